@@ -1,0 +1,216 @@
+/*
+ * kynema_b200.h -- C ABI of the B200-native per-step beam path.
+ *
+ * This library replaces the device side of Kynema's (formerly OpenTurbine's)
+ * per-time-step beam path: the GEBT beam quadrature-point kernels, node-pair
+ * integration, assembly of the bordered constraint system, the linear solve and
+ * the Lie-group generalized-alpha Newton predictor/update.  The host keeps the
+ * reference's Model / Elements / State / Constraints / Solver / Step() surface
+ * and calls the path through the entry points below.
+ *
+ * Conventions
+ *   - Plain C types only; every array is row-major and caller-owned.  The
+ *     library copies inputs in and results out and never retains caller
+ *     pointers.
+ *   - Quaternions are (w, x, y, z), as in src/math/quaternion_operations.hpp.
+ *   - Node state rows: position/rotation fields have 7 components
+ *     (x, y, z, w, i, j, k); velocity-like fields have 6.
+ *   - Every entry point returns an int status: KYN_OK (0) on success, a
+ *     negative KYN_ERR_* code on failure (kyn_last_error() gives the text).
+ *     kyn_step() additionally reports per-model step status, where
+ *     KYN_NOT_CONVERGED (1) is the reference's `Step() == false`.
+ *   - One context per host thread; all work of a context is serialised on its
+ *     own CUDA stream.  kyn_step() returns after results are resident on the
+ *     device and the per-model status has been copied back.
+ */
+#ifndef KYNEMA_B200_H
+#define KYNEMA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+    KYN_OK = 0,
+    KYN_NOT_CONVERGED = 1,   /* Newton loop hit max_iter: Step() returned false
+                                (src/step/step.hpp:55-57) */
+    KYN_ERR_INVALID = -1,    /* bad argument or malformed model description */
+    KYN_ERR_UNSUPPORTED = -2,/* topology or constraint type outside this path */
+    KYN_ERR_CUDA = -3,       /* a CUDA runtime call failed */
+    KYN_ERR_BUDGET = -4,     /* model admission refused: HBM budget exceeded */
+    KYN_ERR_NONFINITE = -5,  /* a non-finite value appeared in the Newton loop */
+    KYN_ERR_SINGULAR = -6,   /* zero pivot in the linear solve */
+    KYN_ERR_NOT_FOUND = -7,  /* unknown model id */
+    KYN_ERR_NO_DEVICE = -8   /* no CUDA device / library built without it */
+};
+
+/* Constraint types: same numbering as constraints::ConstraintType
+ * (src/constraints/constraint_type.hpp:9-24).  This path implements the two
+ * single-node boundary conditions used by beams and rotors. */
+enum {
+    KYN_CONSTRAINT_FIXED_BC = 1,
+    KYN_CONSTRAINT_PRESCRIBED_BC = 2
+};
+
+/* Node-state fields readable with kyn_get_state (src/state/state.hpp:18-68,
+ * src/constraints/constraints.hpp lambda). */
+enum {
+    KYN_FIELD_X0 = 0,      /* [nodes][7] initial position/orientation      */
+    KYN_FIELD_X = 1,       /* [nodes][7] current global position           */
+    KYN_FIELD_Q = 2,       /* [nodes][7] displacement                      */
+    KYN_FIELD_Q_PREV = 3,  /* [nodes][7] displacement at the previous step */
+    KYN_FIELD_Q_DELTA = 4, /* [nodes][6] displacement increment            */
+    KYN_FIELD_V = 5,       /* [nodes][6] velocity                          */
+    KYN_FIELD_VD = 6,      /* [nodes][6] acceleration                      */
+    KYN_FIELD_A = 7,       /* [nodes][6] algorithmic acceleration          */
+    KYN_FIELD_F = 8,       /* [nodes][6] external nodal forces (state.f)   */
+    KYN_FIELD_LAMBDA = 9,  /* [constraints][6] Lagrange multipliers        */
+    KYN_FIELD_TANGENT = 10 /* [nodes][6][6] tangent operator, stored
+                              transposed as in CalculateTangentOperator     */
+};
+
+/* Load channels for kyn_model_set_loads. */
+enum {
+    KYN_LOAD_NODE_FX = 0,  /* Beams::node_FX: [element nodes][6] in the order
+                              of desc.beam_node_ids (element, node-in-element) */
+    KYN_LOAD_STATE_F = 1   /* State::f: [nodes][6] */
+};
+
+/* Arithmetic of the tangent blocks and the linear solve. */
+enum {
+    KYN_PRECISION_FP64 = 0,          /* plain form: everything FP64            */
+    KYN_PRECISION_FP32_REFINED = 1   /* FP32 tangent + FP32 LU, FP64 residual,
+                                        rotation update and refinement        */
+};
+
+/* Model description: the data Model::AddNode / AddBeamElement /
+ * AddFixedBC / AddPrescribedBC / SetGravity collect on the host
+ * (src/model/model.hpp:74-693, src/model/node.hpp:35-60,
+ * src/elements/beams/beam_section.hpp, src/constraints/constraint.hpp). */
+typedef struct kyn_model_desc {
+    int32_t num_nodes;
+    const double* node_x0;  /* [num_nodes][7] Node::x0                    */
+    const double* node_u;   /* [num_nodes][7] Node::u   (NULL: identity)  */
+    const double* node_v;   /* [num_nodes][6] Node::v   (NULL: zero)      */
+    const double* node_vd;  /* [num_nodes][6] Node::vd  (NULL: zero)      */
+    const double* node_s;   /* [num_nodes]    Node::s, element location   */
+
+    int32_t num_beams;
+    const int32_t* beam_node_offsets;    /* [num_beams+1] into beam_node_ids */
+    const int32_t* beam_node_ids;        /* node ids of each beam element    */
+    const int32_t* beam_section_offsets; /* [num_beams+1]                    */
+    const double* section_position;      /* BeamSection::position in [0,1]   */
+    const double* section_mass;          /* [sections][6][6] M_star          */
+    const double* section_stiffness;     /* [sections][6][6] C_star          */
+    const int32_t* beam_qp_offsets;      /* [num_beams+1]                    */
+    const double* qp_xi;                 /* quadrature locations in [-1,1]   */
+    const double* qp_weight;             /* quadrature weights               */
+
+    int32_t num_constraints;
+    const int32_t* constraint_type;        /* KYN_CONSTRAINT_*               */
+    const int32_t* constraint_base_node;   /* Constraint::node_ids[0]        */
+    const int32_t* constraint_target_node; /* Constraint::node_ids[1]        */
+    const double* constraint_axis;         /* [constraints][3] or NULL       */
+    const double* constraint_initial_displacement; /* [constraints][7] or NULL */
+
+    double gravity[3];
+} kyn_model_desc;
+
+/* Step controls: the arguments of the StepParameters constructor
+ * (src/step/step_parameters.hpp:37-52) plus the arithmetic choice. */
+typedef struct kyn_step_params {
+    int32_t is_dynamic_solve;
+    int32_t max_iter;
+    double h;
+    double rho_inf;
+    double absolute_convergence_tol; /* reference default 1e-5 */
+    double relative_convergence_tol; /* reference default 1e-3 */
+    int32_t precision;               /* KYN_PRECISION_*         */
+    int32_t reserved;
+} kyn_step_params;
+
+/* Sizes of one model's system (Solver::num_system_dofs / num_dofs / nnz). */
+typedef struct kyn_model_info {
+    int32_t num_nodes;
+    int32_t num_beams;
+    int32_t num_constraints;
+    int32_t num_system_dofs;
+    int32_t num_dofs;
+    int32_t nnz;
+    int32_t max_beam_nodes;
+    int32_t max_beam_qps;
+    int64_t device_bytes;   /* HBM held by this model's resident state */
+} kyn_model_info;
+
+typedef struct kyn_ctx kyn_ctx;
+
+/* Context: owns every device buffer.  hbm_budget_bytes caps the resident
+ * model state admitted by kyn_model_create (0 = no cap).
+ * Replaces the Kokkos::initialize + per-model View allocation done by
+ * Model::CreateSystemWithSolver (src/model/model.hpp:647-656). */
+kyn_ctx* kyn_ctx_create(int device, size_t hbm_budget_bytes);
+void kyn_ctx_destroy(kyn_ctx* ctx);
+const char* kyn_last_error(const kyn_ctx* ctx);
+/* Device bytes currently held by admitted models. */
+size_t kyn_ctx_used_bytes(const kyn_ctx* ctx);
+
+/* Replaces Model::CreateSystemWithSolver (src/model/model.hpp:647-656):
+ * copies the nodes to resident state (src/model/copy_nodes_to_state.hpp),
+ * builds beam geometry (src/elements/beams/create_beams.hpp:27-165), the
+ * constraints (src/constraints/constraints.hpp:76-266), the DOF map and the
+ * CRS graph (src/model/model.hpp:42-63, src/solver/create_full_matrix.hpp).
+ * Returns the model id (>= 0) or a negative KYN_ERR_* code. */
+int kyn_model_create(kyn_ctx* ctx, const kyn_model_desc* desc);
+int kyn_model_destroy(kyn_ctx* ctx, int model_id);
+int kyn_model_info_get(kyn_ctx* ctx, int model_id, kyn_model_info* info);
+
+/* Replaces writes of Beams::node_FX (tests/regression_tests/regression/
+ * test_cantilever_beam.cpp:105-107) or State::f. */
+int kyn_model_set_loads(kyn_ctx* ctx, int model_id, int which, const double* values);
+
+/* Replaces Constraints::UpdateDisplacement (src/constraints/constraints.hpp:338-343). */
+int kyn_model_set_prescribed(kyn_ctx* ctx, int model_id, int constraint_id, const double u[7]);
+
+/* Replaces kynema::Step (src/step/step.hpp:42-124) for a batch of models:
+ * every listed model advances one time step.  status_out[i] is KYN_OK,
+ * KYN_NOT_CONVERGED or a negative code; iters_out[i] is the Newton iteration
+ * count (= solver.convergence_err.size()).  Either output may be NULL. */
+int kyn_step(kyn_ctx* ctx, const int* model_ids, int n, const kyn_step_params* params,
+             int* status_out, int* iters_out);
+
+/* Asynchronous form used by the serving loop: enqueue the step on the
+ * context stream and return; kyn_step_wait() blocks until it is complete and
+ * fills status/iterations for the models of the last kyn_step_async call. */
+int kyn_step_async(kyn_ctx* ctx, const int* model_ids, int n, const kyn_step_params* params);
+int kyn_step_wait(kyn_ctx* ctx, int* status_out, int* iters_out);
+
+/* Replaces host reads of State / Constraints views after Step(). */
+int kyn_get_state(kyn_ctx* ctx, int model_id, int field, double* out);
+
+/* Replaces reads of solver.convergence_err (src/solver/solver.hpp:83):
+ * errs must hold max_iter values; *n receives the count. */
+int kyn_get_convergence(kyn_ctx* ctx, int model_id, double* errs, int* n);
+
+/* Replaces solver.A / solver.b / solver.x reads (src/solver/solver.hpp:79-81).
+ * row_ptrs [num_dofs+1] and col_inds [nnz] are the reference's CRS graph
+ * (src/solver/create_full_matrix.hpp:47-72), bit-exact.  values [nnz], rhs
+ * [num_dofs] and solution [num_dofs] are the system of the last Newton
+ * iteration of the last step; they are only recorded while the context
+ * option KYN_OPT_RECORD_SYSTEM is set (any pointer may be NULL). */
+int kyn_get_crs(kyn_ctx* ctx, int model_id, int* row_ptrs, int* col_inds, double* values);
+int kyn_get_system_vectors(kyn_ctx* ctx, int model_id, double* rhs, double* solution);
+
+enum {
+    KYN_OPT_RECORD_SYSTEM = 1  /* keep the last assembled system for kyn_get_crs */
+};
+int kyn_ctx_set_option(kyn_ctx* ctx, int option, int64_t value);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KYNEMA_B200_H */

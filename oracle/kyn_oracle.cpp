@@ -1,0 +1,1429 @@
+// kyn_oracle.cpp -- CPU FP64 oracle for the per-step beam path.
+//
+// TEST INFRASTRUCTURE ONLY: the checker for the CUDA path and the timed CPU
+// baseline.  It restates the reference (Kynema) algorithm in the reference's
+// own operation order so that results can be compared at the 1e-13 level of
+// the reference's regression tests.  Each function cites the reference file it
+// follows; paths are relative to the reference project root.
+//
+// Third-party arithmetic restated here (not vendored by the reference,
+// versions not pinned): KokkosKernels SerialGemm / SerialGemv / serial_axpy /
+// serial_nrm2 (textbook loops: C = beta*C; C(i,j) += alpha * sum_p A(i,p)B(p,j)),
+// KokkosSparse::sort_crs_graph (per-row ascending sort) and findRelOffset
+// (position of a column in a sorted row).  The sparse direct solve (KLU /
+// SuperLU / cuDSS) is replaced by a dense LU with partial pivoting; its result
+// is pinned end to end by test_solver.cpp and test_rotor.cpp.
+
+#include "kyn_oracle.h"
+
+#include <algorithm>
+#include <array>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+using V3 = std::array<double, 3>;
+using V4 = std::array<double, 4>;
+using M3 = std::array<double, 9>;
+using M6 = std::array<double, 36>;
+
+// KokkosBatched::SerialGemm restated (row-major, strided, optional transposes).
+void gemm(bool ta, bool tb, int m, int n, int k, double alpha, const double* A, int lda,
+          const double* B, int ldb, double beta, double* C, int ldc) {
+    if (beta == 0.) {
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < n; ++j) C[i * ldc + j] = 0.;
+    } else if (beta != 1.) {
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < n; ++j) C[i * ldc + j] *= beta;
+    }
+    if (alpha == 0.) return;
+    for (int i = 0; i < m; ++i) {
+        for (int j = 0; j < n; ++j) {
+            double c = 0.;
+            for (int p = 0; p < k; ++p) {
+                const double a = ta ? A[p * lda + i] : A[i * lda + p];
+                const double b = tb ? B[j * ldb + p] : B[p * ldb + j];
+                c += a * b;
+            }
+            C[i * ldc + j] += alpha * c;
+        }
+    }
+}
+
+// KokkosBlas::SerialGemv restated: y = beta*y; y(i) += alpha * sum_j op(A)(i,j) x(j).
+void gemv(bool ta, int m, int n, double alpha, const double* A, int lda, const double* x,
+          double beta, double* y) {
+    if (beta == 0.) {
+        for (int i = 0; i < m; ++i) y[i] = 0.;
+    } else if (beta != 1.) {
+        for (int i = 0; i < m; ++i) y[i] *= beta;
+    }
+    if (alpha == 0.) return;
+    for (int i = 0; i < m; ++i) {
+        double t = 0.;
+        for (int j = 0; j < n; ++j) t += (ta ? A[j * lda + i] : A[i * lda + j]) * x[j];
+        y[i] += alpha * t;
+    }
+}
+
+// src/math/vector_operations.hpp:11-21 VecTilde
+M3 tilde(const double* v) {
+    return M3{0., -v[2], v[1], v[2], 0., -v[0], -v[1], v[0], 0.};
+}
+
+// src/math/quaternion_operations.hpp:20-32 QuaternionToRotationMatrix
+M3 quat_to_rot(const double* q) {
+    return M3{q[0] * q[0] + q[1] * q[1] - q[2] * q[2] - q[3] * q[3],
+              2. * (q[1] * q[2] - q[0] * q[3]),
+              2. * (q[1] * q[3] + q[0] * q[2]),
+              2. * (q[1] * q[2] + q[0] * q[3]),
+              q[0] * q[0] - q[1] * q[1] + q[2] * q[2] - q[3] * q[3],
+              2. * (q[2] * q[3] - q[0] * q[1]),
+              2. * (q[1] * q[3] - q[0] * q[2]),
+              2. * (q[2] * q[3] + q[0] * q[1]),
+              q[0] * q[0] - q[1] * q[1] - q[2] * q[2] + q[3] * q[3]};
+}
+
+// src/math/quaternion_operations.hpp:118-129 RotateVectorByQuaternion
+V3 rotate_vec(const double* q, const double* v) {
+    V3 r;
+    r[0] = (q[0] * q[0] + q[1] * q[1] - q[2] * q[2] - q[3] * q[3]) * v[0] +
+           2. * (q[1] * q[2] - q[0] * q[3]) * v[1] + 2. * (q[1] * q[3] + q[0] * q[2]) * v[2];
+    r[1] = 2. * (q[1] * q[2] + q[0] * q[3]) * v[0] +
+           (q[0] * q[0] - q[1] * q[1] + q[2] * q[2] - q[3] * q[3]) * v[1] +
+           2. * (q[2] * q[3] - q[0] * q[1]) * v[2];
+    r[2] = 2. * (q[1] * q[3] - q[0] * q[2]) * v[0] + 2. * (q[2] * q[3] + q[0] * q[1]) * v[1] +
+           (q[0] * q[0] - q[1] * q[1] - q[2] * q[2] + q[3] * q[3]) * v[2];
+    return r;
+}
+
+// src/math/quaternion_operations.hpp:204-211 QuaternionCompose
+V4 quat_compose(const double* a, const double* b) {
+    return V4{a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3],
+              a[0] * b[1] + a[1] * b[0] + a[2] * b[3] - a[3] * b[2],
+              a[0] * b[2] - a[1] * b[3] + a[2] * b[0] + a[3] * b[1],
+              a[0] * b[3] + a[1] * b[2] - a[2] * b[1] + a[3] * b[0]};
+}
+
+// src/math/quaternion_operations.hpp:176-186 QuaternionInverse (device form)
+V4 quat_inverse(const double* q) {
+    const double len = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    return V4{q[0] / len, -q[1] / len, -q[2] / len, -q[3] / len};
+}
+
+// src/math/quaternion_operations.hpp:231-242 RotationVectorToQuaternion (device form)
+V4 rotvec_to_quat(const double* phi) {
+    const double angle = std::sqrt(phi[0] * phi[0] + phi[1] * phi[1] + phi[2] * phi[2]);
+    const double cos_angle = std::cos(angle / 2.);
+    const double factor = (std::abs(angle) < 1.e-12) ? 0. : std::sin(angle / 2.) / angle;
+    return V4{cos_angle, phi[0] * factor, phi[1] * factor, phi[2] * factor};
+}
+
+// src/math/quaternion_operations.hpp:153-166 QuaternionDerivative (3x4)
+std::array<double, 12> quat_derivative(const double* q) {
+    return {-q[1], q[0], -q[3], q[2], -q[2], q[3], q[0], -q[1], -q[3], -q[2], q[1], q[0]};
+}
+
+// src/math/matrix_operations.hpp:19-33 AX_Matrix
+M3 ax_matrix(const M3& A) {
+    double trace = 0.;
+    for (int i = 0; i < 3; ++i) trace += A[i * 4];
+    trace /= 2.;
+    M3 out{};
+    for (int i = 0; i < 3; ++i) {
+        for (int j = 0; j < 3; ++j) out[i * 3 + j] = -A[i * 3 + j] / 2.;
+        out[i * 4] += trace;
+    }
+    return out;
+}
+
+// src/math/matrix_operations.hpp:47-51 AxialVectorOfMatrix
+V3 axial(const M3& m) {
+    return V3{(m[7] - m[5]) / 2., (m[2] - m[6]) / 2., (m[3] - m[1]) / 2.};
+}
+
+double nrm2(const double* v, int n) {
+    double s = 0.;
+    for (int i = 0; i < n; ++i) s += v[i] * v[i];
+    return std::sqrt(s);
+}
+
+// src/system/masses/rotate_section_matrix.hpp:17-51 RotateSectionMatrix
+void rotate_section(const double* xr, const double* cstar, double* cuu) {
+    const M3 R = quat_to_rot(xr);
+    M6 tmp{};
+    gemm(false, false, 3, 6, 3, 1., R.data(), 3, cstar, 6, 0., tmp.data(), 6);
+    gemm(false, false, 3, 6, 3, 1., R.data(), 3, cstar + 18, 6, 0., tmp.data() + 18, 6);
+    gemm(false, true, 6, 3, 3, 1., tmp.data(), 6, R.data(), 3, 0., cuu, 6);
+    gemm(false, true, 6, 3, 3, 1., tmp.data() + 3, 6, R.data(), 3, 0., cuu + 3, 6);
+}
+
+// src/system/masses/calculate_inertial_force.hpp:16-53 CalculateInertialForce
+void inertial_force(double mass, const double* uddot, const double* omega, const double* omegadot,
+                    const double* eta, const M3& eta_t, const M3& rho, const M3& om_t,
+                    const M3& omd_t, double* FI) {
+    M3 M1{};
+    V3 V1{};
+    gemm(false, false, 3, 3, 3, mass, om_t.data(), 3, om_t.data(), 3, 0., M1.data(), 3);
+    for (int i = 0; i < 9; ++i) M1[i] += mass * omd_t[i];
+    gemv(false, 3, 3, 1., M1.data(), 3, eta, 0., FI);
+    for (int i = 0; i < 3; ++i) FI[i] += mass * uddot[i];
+    for (int i = 0; i < 3; ++i) V1[i] += mass * uddot[i];
+    gemv(false, 3, 3, 1., eta_t.data(), 3, V1.data(), 0., FI + 3);
+    gemv(false, 3, 3, 1., rho.data(), 3, omegadot, 1., FI + 3);
+    gemm(false, false, 3, 3, 3, 1., om_t.data(), 3, rho.data(), 3, 0., M1.data(), 3);
+    gemv(false, 3, 3, 1., M1.data(), 3, omega, 1., FI + 3);
+}
+
+// src/system/masses/calculate_gravity_force.hpp:15-27 CalculateGravityForce
+void gravity_force(double mass, const double* g, const M3& eta_t, double* FG) {
+    for (int i = 0; i < 6; ++i) FG[i] = 0.;
+    for (int i = 0; i < 3; ++i) FG[i] += mass * g[i];
+    gemv(false, 3, 3, 1., eta_t.data(), 3, FG, 0., FG + 3);
+}
+
+// src/system/masses/calculate_gyroscopic_matrix.hpp:20-60 CalculateGyroscopicMatrix
+void gyroscopic_matrix(double mass, const double* omega, const double* eta, const M3& rho,
+                       const M3& om_t, double* Guu) {
+    V3 V1{}, V2{};
+    for (int i = 0; i < 36; ++i) Guu[i] = 0.;
+    for (int i = 0; i < 3; ++i) V1[i] += mass * eta[i];
+    gemv(false, 3, 3, 1., om_t.data(), 3, V1.data(), 0., V2.data());
+    M3 M1 = tilde(V2.data());
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Guu[i * 6 + 3 + j] = M1[j * 3 + i];
+    M1 = tilde(V1.data());
+    gemm(false, true, 3, 3, 3, 1., om_t.data(), 3, M1.data(), 3, 1., Guu + 3, 6);
+    gemv(false, 3, 3, 1., rho.data(), 3, omega, 0., V1.data());
+    M1 = tilde(V1.data());
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Guu[(3 + i) * 6 + 3 + j] = M1[i * 3 + j];
+    gemm(false, false, 3, 3, 3, 1., om_t.data(), 3, rho.data(), 3, -1., Guu + 21, 6);
+}
+
+// src/system/masses/calculate_inertia_stiffness_matrix.hpp:19-60
+void inertia_stiffness_matrix(double mass, const double* uddot, const double* omegadot,
+                              const double* omega, const double* eta, const M3& rho,
+                              const M3& om_t, const M3& omd_t, double* Kuu) {
+    V3 V1{};
+    M3 M1{}, M2{};
+    for (int i = 0; i < 36; ++i) Kuu[i] = 0.;
+    for (int i = 0; i < 9; ++i) M1[i] += 1. * omd_t[i];
+    gemm(false, false, 3, 3, 3, 1., om_t.data(), 3, om_t.data(), 3, 1., M1.data(), 3);
+    for (int i = 0; i < 3; ++i) V1[i] += mass * eta[i];
+    M2 = tilde(V1.data());
+    gemm(false, true, 3, 3, 3, 1., M1.data(), 3, M2.data(), 3, 0., Kuu + 3, 6);
+    M1 = tilde(uddot);
+    gemm(false, false, 3, 3, 3, 1., rho.data(), 3, omd_t.data(), 3, 0., Kuu + 21, 6);
+    gemm(false, false, 3, 3, 3, 1., M1.data(), 3, M2.data(), 3, 1., Kuu + 21, 6);
+    gemv(false, 3, 3, 1., rho.data(), 3, omegadot, 0., V1.data());
+    M2 = tilde(V1.data());
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Kuu[(3 + i) * 6 + 3 + j] += -1. * M2[i * 3 + j];
+    gemv(false, 3, 3, 1., rho.data(), 3, omega, 0., V1.data());
+    M1 = tilde(V1.data());
+    gemm(false, false, 3, 3, 3, 1., rho.data(), 3, om_t.data(), 3, -1., M1.data(), 3);
+    gemm(false, false, 3, 3, 3, 1., om_t.data(), 3, M1.data(), 3, 1., Kuu + 21, 6);
+}
+
+// src/system/beams/calculate_inertial_quadrature_point_values.hpp:44-126
+// (from the QuaternionCompose(r, r0) onward; r already interpolated and normalised)
+void inertial_qp(const double* mstar, const double* r0, const double* r, const double* uddot,
+                 const double* omega, const double* omegadot, const double* g, double* FI,
+                 double* FG, double* Muu, double* Guu, double* Kuu) {
+    const V4 xr = quat_compose(r, r0);
+    rotate_section(xr.data(), mstar, Muu);
+    const double mass = Muu[0];
+    // src/system/masses/calculate_mass_matrix_components.hpp CalculateEta / CalculateRho
+    const V3 eta{Muu[5 * 6 + 1] / mass, -Muu[5 * 6 + 0] / mass, Muu[4 * 6 + 0] / mass};
+    const M3 eta_t = tilde(eta.data());
+    M3 rho;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) rho[i * 3 + j] = Muu[(3 + i) * 6 + 3 + j];
+    const M3 om_t = tilde(omega);
+    const M3 omd_t = tilde(omegadot);
+    inertial_force(mass, uddot, omega, omegadot, eta.data(), eta_t, rho, om_t, omd_t, FI);
+    gravity_force(mass, g, eta_t, FG);
+    gyroscopic_matrix(mass, omega, eta.data(), rho, om_t, Guu);
+    inertia_stiffness_matrix(mass, uddot, omegadot, omega, eta.data(), rho, om_t, omd_t, Kuu);
+}
+
+// src/system/beams/calculate_strain.hpp:17-47
+void calc_strain(const double* x0p, const double* up, const double* r, const double* rp,
+                 double* strain) {
+    V3 R = rotate_vec(r, x0p);
+    for (int i = 0; i < 3; ++i) R[i] += -1. * up[i];
+    for (int i = 0; i < 3; ++i) R[i] += -1. * x0p[i];
+    const auto E = quat_derivative(r);
+    double e2[3];
+    gemv(false, 3, 4, 2., E.data(), 4, rp, 0., e2);
+    strain[0] = -R[0];
+    strain[1] = -R[1];
+    strain[2] = -R[2];
+    strain[3] = e2[0];
+    strain[4] = e2[1];
+    strain[5] = e2[2];
+}
+
+// src/system/beams/calculate_Ouu.hpp:17-37
+void calc_ouu(const double* cuu, const double* ss, const double* mt, const double* nt,
+              double* O) {
+    for (int i = 0; i < 36; ++i) O[i] = 0.;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) O[i * 6 + 3 + j] += 1. * nt[i * 3 + j];
+    gemm(false, false, 3, 3, 3, 1., cuu, 6, ss, 3, -1., O + 3, 6);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) O[(3 + i) * 6 + 3 + j] += 1. * mt[i * 3 + j];
+    gemm(false, false, 3, 3, 3, 1., cuu + 18, 6, ss, 3, -1., O + 21, 6);
+}
+
+// src/system/beams/calculate_Puu.hpp:17-36
+void calc_puu(const double* cuu, const double* ss, const double* nt, double* P) {
+    for (int i = 0; i < 36; ++i) P[i] = 0.;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) P[(3 + i) * 6 + j] += 1. * nt[i * 3 + j];
+    gemm(true, false, 3, 3, 3, 1., ss, 3, cuu, 6, 1., P + 18, 6);
+    gemm(true, false, 3, 3, 3, 1., ss, 3, cuu + 3, 6, 0., P + 21, 6);
+}
+
+// src/system/beams/calculate_Quu.hpp:17-38
+void calc_quu(const double* cuu, const double* ss, const double* nt, double* Qm) {
+    M3 M1{};
+    for (int i = 0; i < 36; ++i) Qm[i] = 0.;
+    for (int i = 0; i < 9; ++i) M1[i] += 1. * nt[i];
+    gemm(false, false, 3, 3, 3, 1., cuu, 6, ss, 3, -1., M1.data(), 3);
+    gemm(true, false, 3, 3, 3, 1., ss, 3, M1.data(), 3, 0., Qm + 21, 6);
+}
+
+// src/system/beams/calculate_stiffness_quadrature_point_values.hpp:47-128
+void stiffness_qp(const double* cstar, const double* r0, const double* x0p, const double* up,
+                  const double* r, const double* rp, double* FC, double* FD, double* Cuu,
+                  double* Ouu, double* Puu, double* Quu) {
+    const V4 xr = quat_compose(r, r0);
+    rotate_section(xr.data(), cstar, Cuu);
+    double strain[6];
+    calc_strain(x0p, up, r, rp, strain);
+    // calculate_temporary_variables.hpp:17-28
+    double x0pup[3] = {x0p[0], x0p[1], x0p[2]};
+    for (int i = 0; i < 3; ++i) x0pup[i] += 1. * up[i];
+    const M3 ss = tilde(x0pup);
+    // calculate_force_FC.hpp / calculate_force_FD.hpp
+    gemv(false, 6, 6, 1., Cuu, 6, strain, 0., FC);
+    for (int i = 0; i < 6; ++i) FD[i] = 0.;
+    gemv(true, 3, 3, 1., ss.data(), 3, FC, 0., FD + 3);
+    const M3 nt = tilde(FC);
+    const M3 mt = tilde(FC + 3);
+    calc_ouu(Cuu, ss.data(), mt.data(), nt.data(), Ouu);
+    calc_puu(Cuu, ss.data(), nt.data(), Puu);
+    calc_quu(Cuu, ss.data(), nt.data(), Quu);
+}
+
+// src/system/calculate_tangent_operator.hpp:26-65 (output stored transposed)
+void tangent_operator(double h, const double* qd, double* Tg) {
+    M6 T{};
+    for (int k = 0; k < 6; ++k) T[k * 7] = 1.;
+    double rv[3] = {0., 0., 0.};
+    for (int i = 0; i < 3; ++i) rv[i] += h * qd[3 + i];
+    const double phi = nrm2(rv, 3);
+    const double tmp1 = (phi > 1.e-16) ? (std::cos(phi) - 1.) / (phi * phi) : 0.;
+    const double tmp2 = (phi > 1.e-16) ? (1. - std::sin(phi) / phi) / (phi * phi) : 0.;
+    const M3 m2 = tilde(rv);
+    M3 m1 = m2;
+    gemm(false, false, 3, 3, 3, tmp2, m2.data(), 3, m2.data(), 3, tmp1, m1.data(), 3);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) T[(3 + i) * 6 + 3 + j] += 1. * m1[i * 3 + j];
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) Tg[i * 6 + j] = T[j * 6 + i];
+}
+
+// src/math/interpolation.hpp LagrangePolynomialInterpWeights
+void lagrange_interp(double x, const std::vector<double>& xs, std::vector<double>& w) {
+    const size_t n = xs.size();
+    w.assign(n, 1.);
+    std::vector<double> xm(n);
+    for (size_t m = 0; m < n; ++m) xm[m] = x - xs[m];
+    for (size_t j = 0; j < n; ++j)
+        for (size_t m = 0; m < n; ++m)
+            if (j != m) w[j] *= xm[m] / (xs[j] - xs[m]);
+}
+
+// src/math/interpolation.hpp LagrangePolynomialDerivWeights
+void lagrange_deriv(double x, const std::vector<double>& xs, std::vector<double>& w) {
+    const size_t n = xs.size();
+    w.assign(n, 0.);
+    for (size_t i = 0; i < n; ++i) {
+        const double xi = xs[i];
+        double weight = 0.;
+        for (size_t j = 0; j < n; ++j) {
+            if (j == i) continue;
+            double prod = 1.;
+            for (size_t k = 0; k < n; ++k) {
+                if (k == i || k == j) continue;
+                prod = prod * ((x - xs[k]) / (xi - xs[k]));
+            }
+            weight += prod / (xi - xs[j]);
+        }
+        w[i] = weight;
+    }
+}
+
+// src/math/interpolation.hpp LinearInterpWeights
+void linear_interp(double x, const std::vector<double>& xs, std::vector<double>& w) {
+    const size_t n = xs.size();
+    w.assign(n, 0.);
+    const auto lower = std::lower_bound(xs.begin(), xs.end(), x);
+    if (lower == xs.begin()) {
+        w.front() = 1.;
+        return;
+    }
+    if (lower == xs.end()) {
+        w.back() = 1.;
+        return;
+    }
+    const auto index = static_cast<size_t>(std::distance(xs.begin(), lower));
+    const double lo = xs[index - 1];
+    const double hi = xs[index];
+    const double wu = (x - lo) / (hi - lo);
+    w[index - 1] = 1. - wu;
+    w[index] = wu;
+}
+
+int count_bits(unsigned sig) {
+    int c = 0;
+    for (unsigned v = sig; v > 0; v >>= 1) c += static_cast<int>(v & 1U);
+    return c;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Model
+// ---------------------------------------------------------------------------
+
+struct OBeam {
+    int N = 0, Q = 0;
+    std::vector<int> node_ids;
+    std::vector<double> phi, dphi;      // [N][Q]
+    std::vector<double> w, jac;         // [Q]
+    std::vector<double> x0p;            // [Q][3]
+    std::vector<double> r0;             // [Q][4]
+    std::vector<double> mstar, cstar;   // [Q][36]
+    std::vector<double> fx;             // [N][6]  node_FX
+    std::vector<double> fe;             // [Q][6]  qp_Fe (zero)
+    std::vector<double> residual;       // [N][6]
+    std::vector<double> sysmat;         // [N][N][36]
+    std::vector<long> eft;              // [N][6]
+};
+
+struct OConstraint {
+    int type = 0;
+    int base = 0, target = 0;
+    double X0[3] = {0., 0., 0.};
+    double input[7] = {0., 0., 0., 1., 0., 0., 0.};
+    double lambda[6] = {0., 0., 0., 0., 0., 0.};
+    double res[6] = {};
+    double t_lambda_res[6] = {};
+    double sys_res[6] = {};
+    double t_grad_tan[36] = {};
+    double t_grad_trans[36] = {};
+    long row_first = 0, row_last = 0;
+    long base_active = 0, target_active = 0;
+    long base_table[6] = {};
+    long target_table[6] = {};
+};
+
+struct orc_model {
+    int num_nodes = 0;
+    std::vector<double> x0, x, q, q_prev, q_delta, v, vd, a, f, tangent;
+    std::vector<unsigned> sig;
+    std::vector<long> active, fmap;
+    std::vector<OBeam> beams;
+    std::vector<OConstraint> cons;
+    double gravity[3] = {0., 0., 0.};
+    long nsys = 0, ndofs = 0;
+    std::vector<long> row_ptrs, col_inds;
+    std::vector<double> values, b, xsol;
+    std::vector<double> conv;
+};
+
+namespace {
+
+// src/state/calculate_next_state.hpp:27-37
+void calculate_next_state(orc_model& m, double h, double af, double am, double beta,
+                          double gamma) {
+    for (int n = 0; n < m.num_nodes; ++n) {
+        for (int c = 0; c < 6; ++c) {
+            const double v_p = m.v[n * 6 + c];
+            const double vd_p = m.vd[n * 6 + c];
+            const double a_p = m.a[n * 6 + c];
+            m.vd[n * 6 + c] = 0.;
+            m.a[n * 6 + c] = (af * vd_p - am * a_p) / (1. - am);
+            m.v[n * 6 + c] = v_p + h * (1. - gamma) * a_p + gamma * h * m.a[n * 6 + c];
+            m.q_delta[n * 6 + c] = v_p + (0.5 - beta) * h * a_p + beta * h * m.a[n * 6 + c];
+        }
+    }
+}
+
+// src/state/calculate_displacement.hpp:25-50
+void calculate_displacement(orc_model& m, double h) {
+    for (int n = 0; n < m.num_nodes; ++n) {
+        for (int c = 0; c < 3; ++c)
+            m.q[n * 7 + c] = m.q_prev[n * 7 + c] + h * m.q_delta[n * 6 + c];
+        const double delta[3] = {h * m.q_delta[n * 6 + 3], h * m.q_delta[n * 6 + 4],
+                                 h * m.q_delta[n * 6 + 5]};
+        const V4 qd = rotvec_to_quat(delta);
+        const V4 qn = quat_compose(qd.data(), &m.q_prev[n * 7 + 3]);
+        for (int c = 0; c < 4; ++c) m.q[n * 7 + 3 + c] = qn[c];
+    }
+}
+
+// src/state/update_global_position.hpp:25-45
+void update_global_position(orc_model& m) {
+    for (int n = 0; n < m.num_nodes; ++n) {
+        for (int c = 0; c < 3; ++c) m.x[n * 7 + c] = m.x0[n * 7 + c] + m.q[n * 7 + c];
+        const V4 r = quat_compose(&m.q[n * 7 + 3], &m.x0[n * 7 + 3]);
+        for (int c = 0; c < 4; ++c) m.x[n * 7 + 3 + c] = r[c];
+    }
+}
+
+long find_offset(const orc_model& m, long row, long col) {
+    const long* b = m.col_inds.data() + m.row_ptrs[row];
+    const long* e = m.col_inds.data() + m.row_ptrs[row + 1];
+    const long* p = std::lower_bound(b, e, col);
+    return (p != e && *p == col) ? (p - m.col_inds.data()) : -1;
+}
+
+// src/system/beams/calculate_quadrature_point_values.hpp:51-172 for one element
+void update_beam(orc_model& m, OBeam& B, double beta_prime, double gamma_prime) {
+    const int N = B.N, Q = B.Q;
+    std::vector<double> Fc(Q * 6), Fd(Q * 6), Fi(Q * 6), Fg(Q * 6);
+    std::vector<double> Kuu(Q * 36), Puu(Q * 36), Cuu(Q * 36), Ouu(Q * 36), Quu(Q * 36),
+        Muu(Q * 36), Guu(Q * 36);
+    for (int qp = 0; qp < Q; ++qp) {
+        // interpolate_to_quadrature_point_for_inertia.hpp:19-40
+        double r[4] = {0, 0, 0, 0}, ud[3] = {0, 0, 0}, om[3] = {0, 0, 0}, omd[3] = {0, 0, 0};
+        for (int n = 0; n < N; ++n) {
+            const int s = B.node_ids[n];
+            const double phi = B.phi[n * Q + qp];
+            for (int c = 0; c < 3; ++c) {
+                ud[c] += m.vd[s * 6 + c] * phi;
+                om[c] += m.v[s * 6 + c + 3] * phi;
+                omd[c] += m.vd[s * 6 + c + 3] * phi;
+            }
+            for (int c = 0; c < 4; ++c) r[c] += m.q[s * 7 + c + 3] * phi;
+        }
+        const double rl = nrm2(r, 4);
+        for (int c = 0; c < 4; ++c) r[c] /= rl;
+        inertial_qp(&B.mstar[qp * 36], &B.r0[qp * 4], r, ud, om, omd, m.gravity, &Fi[qp * 6],
+                    &Fg[qp * 6], &Muu[qp * 36], &Guu[qp * 36], &Kuu[qp * 36]);
+        // interpolate_to_quadrature_point_for_stiffness.hpp:19-41
+        double u[3] = {0, 0, 0}, up[3] = {0, 0, 0}, r2[4] = {0, 0, 0, 0}, rp[4] = {0, 0, 0, 0};
+        for (int n = 0; n < N; ++n) {
+            const int s = B.node_ids[n];
+            const double phi = B.phi[n * Q + qp];
+            const double dphiJ = B.dphi[n * Q + qp] / B.jac[qp];
+            for (int c = 0; c < 3; ++c) {
+                u[c] += m.q[s * 7 + c] * phi;
+                up[c] += m.q[s * 7 + c] * dphiJ;
+            }
+            for (int c = 0; c < 4; ++c) {
+                r2[c] += m.q[s * 7 + c + 3] * phi;
+                rp[c] += m.q[s * 7 + c + 3] * dphiJ;
+            }
+        }
+        const double rl2 = nrm2(r2, 4);
+        for (int c = 0; c < 4; ++c) r2[c] /= rl2;
+        stiffness_qp(&B.cstar[qp * 36], &B.r0[qp * 4], &B.x0p[qp * 3], up, r2, rp, &Fc[qp * 6],
+                     &Fd[qp * 6], &Cuu[qp * 36], &Ouu[qp * 36], &Puu[qp * 36], &Quu[qp * 36]);
+    }
+    orc_integrate_residual(N, Q, B.w.data(), B.jac.data(), B.phi.data(), B.dphi.data(),
+                           B.fx.data(), Fc.data(), Fd.data(), Fi.data(), B.fe.data(), Fg.data(),
+                           B.residual.data());
+    std::vector<double> S(N * N * 36), I(N * N * 36);
+    orc_integrate_stiffness(N, Q, B.w.data(), B.jac.data(), B.phi.data(), B.dphi.data(),
+                            Kuu.data(), Puu.data(), Cuu.data(), Ouu.data(), Quu.data(), S.data());
+    orc_integrate_inertia(N, Q, B.w.data(), B.jac.data(), B.phi.data(), Muu.data(), Guu.data(),
+                          beta_prime, gamma_prime, I.data());
+    // calculate_system_matrix.hpp:25-53
+    for (int i = 0; i < N; ++i) {
+        for (int j = 0; j < N; ++j) {
+            const int nT = B.node_ids[j];
+            double* out = &B.sysmat[(i * N + j) * 36];
+            for (int k = 0; k < 36; ++k) out[k] = I[(i * N + j) * 36 + k];
+            gemm(false, false, 6, 6, 6, 1., &S[(i * N + j) * 36], 6, &m.tangent[nT * 36], 6, 1.,
+                 out, 6);
+        }
+    }
+}
+
+// src/constraints/calculate_constraint_residual_gradient.hpp:60-199 (FixedBC, PrescribedBC)
+void update_constraint(orc_model& m, OConstraint& C) {
+    const double* nu = &m.q[C.target * 7];
+    double u1[3] = {0., 0., 0.};
+    double R1[4] = {1., 0., 0., 0.};
+    if (C.type == KYN_CONSTRAINT_PRESCRIBED_BC) {
+        for (int i = 0; i < 3; ++i) u1[i] = C.input[i];
+        for (int i = 0; i < 4; ++i) R1[i] = C.input[3 + i];
+    }
+    const double u2[3] = {nu[0], nu[1], nu[2]};
+    const double R2[4] = {nu[3], nu[4], nu[5], nu[6]};
+    const V4 R1t = quat_inverse(R1);
+    const V3 R1X0 = rotate_vec(R1, C.X0);
+    for (int c = 0; c < 3; ++c) C.res[c] = u2[c] + C.X0[c] - u1[c] - R1X0[c];
+    const V4 R2R1t = quat_compose(R2, R1t.data());
+    const M3 Cm = quat_to_rot(R2R1t.data());
+    const V3 ax = axial(Cm);
+    for (int c = 0; c < 3; ++c) C.res[3 + c] = ax[c];
+    M6 grad{};
+    for (int c = 0; c < 3; ++c) grad[c * 7] = 1.;
+    const M3 A = ax_matrix(Cm);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) grad[(3 + i) * 6 + 3 + j] = A[j * 3 + i];
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) C.t_grad_trans[i * 6 + j] = grad[j * 6 + i];
+    gemm(false, false, 6, 6, 6, 1., grad.data(), 6, &m.tangent[C.target * 36], 6, 0.,
+         C.t_grad_tan, 6);
+    gemv(false, 6, 6, 1., C.t_grad_trans, 6, C.lambda, 0., C.t_lambda_res);
+}
+
+void solve_dense(orc_model& m) {
+    // Dense LU with partial pivoting of the CRS system A x = b.
+    const long n = m.ndofs;
+    std::vector<double> A(n * n, 0.);
+    for (long r = 0; r < n; ++r)
+        for (long k = m.row_ptrs[r]; k < m.row_ptrs[r + 1]; ++k) A[r * n + m.col_inds[k]] = m.values[k];
+    std::vector<double> x(m.b);
+    std::vector<long> piv(n);
+    for (long k = 0; k < n; ++k) {
+        long p = k;
+        double best = std::abs(A[k * n + k]);
+        for (long i = k + 1; i < n; ++i) {
+            if (std::abs(A[i * n + k]) > best) {
+                best = std::abs(A[i * n + k]);
+                p = i;
+            }
+        }
+        if (p != k) {
+            for (long j = 0; j < n; ++j) std::swap(A[k * n + j], A[p * n + j]);
+            std::swap(x[k], x[p]);
+        }
+        const double d = A[k * n + k];
+        for (long i = k + 1; i < n; ++i) {
+            const double l = A[i * n + k] / d;
+            A[i * n + k] = l;
+            if (l == 0.) continue;
+            for (long j = k + 1; j < n; ++j) A[i * n + j] -= l * A[k * n + j];
+            x[i] -= l * x[k];
+        }
+    }
+    for (long i = n - 1; i >= 0; --i) {
+        double s = x[i];
+        for (long j = i + 1; j < n; ++j) s -= A[i * n + j] * x[j];
+        x[i] = s / A[i * n + i];
+    }
+    m.xsol = x;
+}
+
+struct Params {
+    bool dynamic;
+    int max_iter;
+    double h, am, af, gamma, beta, gp, bp, cond, atol, rtol;
+};
+
+// src/step/step_parameters.hpp:37-52
+Params make_params(const kyn_step_params* p) {
+    Params q{};
+    q.dynamic = p->is_dynamic_solve != 0;
+    q.max_iter = p->max_iter;
+    q.h = p->h;
+    const double rho = p->rho_inf;
+    q.am = (2. * rho - 1.) / (rho + 1.);
+    q.af = rho / (rho + 1.);
+    q.gamma = 0.5 + q.af - q.am;
+    q.beta = 0.25 * (q.gamma + 0.5) * (q.gamma + 0.5);
+    q.gp = q.dynamic ? q.gamma / (q.h * q.beta) : 0.;
+    q.bp = q.dynamic ? (1. - q.am) / (q.h * q.h * q.beta * (1. - q.af)) : 0.;
+    q.cond = q.beta * q.h * q.h;
+    q.atol = p->absolute_convergence_tol;
+    q.rtol = p->relative_convergence_tol;
+    return q;
+}
+
+// src/step/predict_next_state.hpp:14-47
+void predict(orc_model& m, const Params& P) {
+    m.q_prev = m.q;
+    calculate_next_state(m, P.h, P.af, P.am, P.beta, P.gamma);
+    calculate_displacement(m, P.h);
+}
+
+void assemble(orc_model& m, const Params& P) {
+    // src/step/reset_solver.hpp
+    std::fill(m.values.begin(), m.values.end(), 0.);
+    std::fill(m.b.begin(), m.b.end(), 0.);
+    // src/step/update_tangent_operator.hpp
+    for (int n = 0; n < m.num_nodes; ++n) tangent_operator(P.h, &m.q_delta[n * 6], &m.tangent[n * 36]);
+    // src/step/update_system_variables_beams.hpp
+    for (auto& B : m.beams) update_beam(m, B, P.bp, P.gp);
+    // src/step/assemble_system_residual.hpp:17-64 (forces, then beams)
+    for (int n = 0; n < m.num_nodes; ++n) {
+        const long d = m.fmap[n];
+        const unsigned s = m.sig[n];
+        if (s == 0b111111U) {
+            for (int c = 0; c < 6; ++c) m.b[d + c] -= m.f[n * 6 + c];
+        } else if (s == 0b111000U) {
+            for (int c = 0; c < 3; ++c) m.b[d + c] -= m.f[n * 6 + c];
+        } else if (s == 0b000111U) {
+            for (int c = 0; c < 3; ++c) m.b[d + c] -= m.f[n * 6 + 3 + c];
+        }
+    }
+    for (auto& B : m.beams)
+        for (int n = 0; n < B.N; ++n)
+            for (int c = 0; c < 6; ++c) m.b[B.eft[n * 6 + c]] += B.residual[n * 6 + c];
+    // src/step/assemble_system_matrix.hpp -> contribute_beams_to_sparse_matrix.hpp:34-73
+    for (auto& B : m.beams) {
+        for (int n2 = 0; n2 < B.N; ++n2) {
+            for (int n1 = 0; n1 < B.N; ++n1) {
+                const long first_col = B.eft[n2 * 6];
+                for (int c1 = 0; c1 < 6; ++c1) {
+                    const long row = B.eft[n1 * 6 + c1];
+                    long off = find_offset(m, row, first_col);
+                    for (int c2 = 0; c2 < 6; ++c2, ++off)
+                        m.values[off] += B.sysmat[(n1 * B.N + n2) * 36 + c1 * 6 + c2] * P.cond;
+                }
+            }
+        }
+    }
+    // src/step/update_constraint_variables.hpp
+    for (auto& C : m.cons) update_constraint(m, C);
+    // src/step/assemble_constraints_matrix.hpp
+    for (auto& C : m.cons) {
+        for (long i = C.row_first; i < C.row_last; ++i) {
+            const long rn = i - C.row_first;
+            const long row = m.nsys + i;
+            long off = find_offset(m, row, C.target_table[0]);
+            for (long e = 0; e < C.target_active; ++e, ++off) m.values[off] += C.t_grad_tan[rn * 6 + e];
+        }
+        const long first_col = C.row_first + m.nsys;
+        const long ncols = C.row_last - C.row_first;
+        for (long i = C.target_table[0]; i < C.target_table[0] + C.target_active; ++i) {
+            const long rn = i - C.target_table[0];
+            long off = find_offset(m, i, first_col);
+            for (long e = 0; e < ncols; ++e, ++off) m.values[off] += C.t_grad_trans[rn * 6 + e];
+        }
+    }
+    // src/step/assemble_constraints_residual.hpp
+    for (auto& C : m.cons)
+        for (long c = 0; c < C.target_active; ++c) m.b[C.target_table[c]] += C.sys_res[c];
+    for (auto& C : m.cons)
+        for (long c = 0; c < C.target_active; ++c) m.b[C.target_table[0] + c] += C.t_lambda_res[c];
+    for (auto& C : m.cons)
+        for (long c = 0; c < C.row_last - C.row_first; ++c) m.b[m.nsys + C.row_first + c] += C.res[c];
+}
+
+// src/step/step.hpp:42-124
+int step_impl(orc_model& m, const Params& P, int* iters) {
+    predict(m, P);
+    // src/step/reset_constraints.hpp
+    for (auto& C : m.cons) {
+        for (int c = 0; c < 6; ++c) {
+            C.lambda[c] = 0.;
+            C.sys_res[c] = 0.;
+        }
+    }
+    m.conv.clear();
+    double err = 1000.;
+    for (int iter = 0; err > 1.; ++iter) {
+        if (iter >= P.max_iter) {
+            if (iters) *iters = iter;
+            return KYN_NOT_CONVERGED;
+        }
+        assemble(m, P);
+        // src/step/solve_system.hpp:15-39
+        for (long i = 0; i < m.nsys; ++i) m.b[i] *= P.cond;
+        for (long i = 0; i < m.ndofs; ++i) m.b[i] = -1. * m.b[i];
+        solve_dense(m);
+        for (long i = m.nsys; i < m.ndofs; ++i) m.xsol[i] /= P.cond;
+        // src/step/calculate_convergence_error.hpp:16-54
+        double sum_sys = 0.;
+        for (int n = 0; n < m.num_nodes; ++n) {
+            for (long c = 0; c < m.active[n]; ++c) {
+                const double pi = m.xsol[m.fmap[n] + c];
+                const double xi = m.q_delta[n * 6 + c] * P.h;
+                const double e = pi / (P.atol + P.rtol * std::abs(xi));
+                sum_sys += e * e;
+            }
+        }
+        double sum_con = 0.;
+        for (auto& C : m.cons) {
+            for (long r = C.row_first; r < C.row_last; ++r) {
+                const double pi = m.xsol[m.nsys + r];
+                const double xi = C.lambda[r - C.row_first];
+                const double e = pi / (P.atol + P.rtol * std::abs(xi));
+                sum_con += e * e;
+            }
+        }
+        err = std::sqrt((sum_sys + sum_con) / static_cast<double>(m.ndofs));
+        m.conv.push_back(err);
+        // src/step/update_state_prediction.hpp
+        for (int n = 0; n < m.num_nodes; ++n) {
+            const int nd = count_bits(m.sig[n]);
+            const long fd = m.fmap[n];
+            for (int c = 0; c < nd; ++c) {
+                const double delta = m.xsol[fd + c];
+                m.q_delta[n * 6 + c] += delta / P.h;
+                if (P.dynamic) {
+                    m.v[n * 6 + c] += P.gp * delta;
+                    m.vd[n * 6 + c] += P.bp * delta;
+                }
+            }
+        }
+        calculate_displacement(m, P.h);
+        // src/constraints/update_lambda_prediction.hpp:27-42
+        for (auto& C : m.cons)
+            for (long r = C.row_first; r < C.row_last; ++r)
+                C.lambda[r - C.row_first] += m.xsol[m.nsys + r];
+    }
+    // src/state/update_algorithmic_acceleration.hpp:19-23, update_global_position.hpp
+    for (int n = 0; n < m.num_nodes; ++n)
+        for (int c = 0; c < 6; ++c) m.a[n * 6 + c] += (1. - P.af) / (1. - P.am) * m.vd[n * 6 + c];
+    update_global_position(m);
+    if (iters) *iters = static_cast<int>(m.conv.size());
+    return KYN_OK;
+}
+
+bool bad(char* err, int errlen, const char* msg) {
+    if (err && errlen > 0) std::snprintf(err, static_cast<size_t>(errlen), "%s", msg);
+    return false;
+}
+
+}  // namespace
+
+extern "C" {
+
+long orc_crs_build(int num_system_dofs, int num_dofs, int num_nodes, const long* active_dofs,
+                   const long* fmap, int num_elems, int max_nodes, const long* nodes_per_elem,
+                   const long* elem_nodes, int num_constraints, const long* base_active,
+                   const long* target_active, const long* base_table, const long* target_table,
+                   const long* row_range, long* row_ptrs, long* col_inds, int sort_rows) {
+    // src/solver/compute_system_row_entries.hpp:75-102
+    auto elem_contains = [&](int e, long node) {
+        for (long k = 0; k < nodes_per_elem[e]; ++k)
+            if (elem_nodes[e * max_nodes + k] == node) return true;
+        return false;
+    };
+    auto con_contains = [&](int c, long dof) {
+        const bool b = dof == base_table[c * 6] && base_active[c] != 0;
+        const bool t = dof == target_table[c * 6] && target_active[c] != 0;
+        return b || t;
+    };
+    std::vector<long> entries(num_dofs, 0);
+    for (long node = 0; node < num_nodes; ++node) {
+        const long nd = active_dofs[node];
+        const long di = fmap[node];
+        long e_row = nd;
+        for (int e = 0; e < num_elems; ++e) {
+            if (!elem_contains(e, node)) continue;
+            long ent = 0;
+            for (long k = 0; k < nodes_per_elem[e]; ++k) ent += active_dofs[elem_nodes[e * max_nodes + k]];
+            e_row += ent - nd;
+        }
+        for (int c = 0; c < num_constraints; ++c) {
+            if (!con_contains(c, di)) continue;
+            e_row += row_range[c * 2 + 1] - row_range[c * 2];
+        }
+        for (long k = 0; k < nd; ++k) entries[di + k] = e_row;
+    }
+    // src/solver/compute_constraints_row_entries.hpp:26-34
+    for (int c = 0; c < num_constraints; ++c)
+        for (long r = row_range[c * 2]; r < row_range[c * 2 + 1]; ++r)
+            entries[r + num_system_dofs] = base_active[c] + target_active[c];
+    // src/solver/scan_row_entries.hpp
+    std::vector<long> rp(num_dofs + 1, 0);
+    for (int i = 0; i < num_dofs; ++i) rp[i + 1] = rp[i] + entries[i];
+    if (row_ptrs) std::copy(rp.begin(), rp.end(), row_ptrs);
+    const long nnz = rp[num_dofs];
+    if (!col_inds) return nnz;
+    // src/solver/compute_system_col_inds.hpp:91-131
+    for (long node = 0; node < num_nodes; ++node) {
+        const long nd = active_dofs[node];
+        const long di = fmap[node];
+        long cur[6] = {0, 0, 0, 0, 0, 0};
+        for (long c1 = 0; c1 < nd; ++c1) {
+            long idx = rp[di + c1];
+            for (long c2 = 0; c2 < nd; ++c2, ++idx) col_inds[idx] = di + c2;
+            cur[c1] = nd;
+        }
+        for (int e = 0; e < num_elems; ++e) {
+            if (!elem_contains(e, node)) continue;
+            for (long c = 0; c < nd; ++c) {
+                long idx = rp[di + c] + cur[c];
+                const long start = idx;
+                for (long k = 0; k < nodes_per_elem[e]; ++k) {
+                    const long s = elem_nodes[e * max_nodes + k];
+                    if (s == node) continue;
+                    for (long cc = 0; cc < active_dofs[s]; ++cc, ++idx) col_inds[idx] = fmap[s] + cc;
+                }
+                cur[c] += idx - start;
+            }
+        }
+        for (int cn = 0; cn < num_constraints; ++cn) {
+            if (!con_contains(cn, di)) continue;
+            for (long c = 0; c < nd; ++c) {
+                long idx = rp[di + c] + cur[c];
+                const long start = idx;
+                for (long k = row_range[cn * 2]; k < row_range[cn * 2 + 1]; ++k, ++idx)
+                    col_inds[idx] = num_system_dofs + k;
+                cur[c] += idx - start;
+            }
+        }
+    }
+    // src/solver/compute_constraints_col_inds.hpp:51-59
+    for (int c = 0; c < num_constraints; ++c) {
+        for (long r = row_range[c * 2]; r < row_range[c * 2 + 1]; ++r) {
+            long idx = rp[r + num_system_dofs];
+            for (long k = 0; k < target_active[c]; ++k, ++idx) col_inds[idx] = target_table[c * 6 + k];
+            for (long k = 0; k < base_active[c]; ++k, ++idx) col_inds[idx] = base_table[c * 6 + k];
+        }
+    }
+    // KokkosSparse::sort_crs_graph (src/solver/create_full_matrix.hpp:62)
+    if (sort_rows)
+        for (int r = 0; r < num_dofs; ++r) std::sort(col_inds + rp[r], col_inds + rp[r + 1]);
+    return nnz;
+}
+
+orc_model* orc_model_create(const kyn_model_desc* d, char* err, int errlen) {
+    if (!d || d->num_nodes <= 0) {
+        bad(err, errlen, "empty model");
+        return nullptr;
+    }
+    auto* m = new orc_model();
+    const int nn = d->num_nodes;
+    m->num_nodes = nn;
+    m->x0.assign(d->node_x0, d->node_x0 + nn * 7);
+    m->q.resize(nn * 7);
+    for (int n = 0; n < nn; ++n) {
+        const double id[7] = {0., 0., 0., 1., 0., 0., 0.};
+        for (int c = 0; c < 7; ++c) m->q[n * 7 + c] = d->node_u ? d->node_u[n * 7 + c] : id[c];
+    }
+    m->v.assign(nn * 6, 0.);
+    m->vd.assign(nn * 6, 0.);
+    if (d->node_v) m->v.assign(d->node_v, d->node_v + nn * 6);
+    if (d->node_vd) m->vd.assign(d->node_vd, d->node_vd + nn * 6);
+    // src/model/copy_nodes_to_state.hpp:14-60
+    m->a = m->vd;
+    m->f.assign(nn * 6, 0.);
+    m->q_prev = m->q;
+    m->q_delta.assign(nn * 6, 0.);
+    m->x.assign(nn * 7, 0.);
+    m->tangent.assign(nn * 36, 0.);
+    update_global_position(*m);
+    for (int c = 0; c < 3; ++c) m->gravity[c] = d->gravity[c];
+
+    // src/elements/beams/create_beams.hpp:27-165
+    m->beams.resize(d->num_beams);
+    for (int e = 0; e < d->num_beams; ++e) {
+        OBeam& B = m->beams[e];
+        const int n0 = d->beam_node_offsets[e], n1 = d->beam_node_offsets[e + 1];
+        const int s0 = d->beam_section_offsets[e], s1 = d->beam_section_offsets[e + 1];
+        const int q0 = d->beam_qp_offsets[e], q1 = d->beam_qp_offsets[e + 1];
+        B.N = n1 - n0;
+        B.Q = q1 - q0;
+        if (B.N < 2 || B.Q < 1 || s1 - s0 < 1) {
+            bad(err, errlen, "beam needs >= 2 nodes, >= 1 qp, >= 1 section");
+            delete m;
+            return nullptr;
+        }
+        B.node_ids.assign(d->beam_node_ids + n0, d->beam_node_ids + n1);
+        for (int id : B.node_ids) {
+            if (id < 0 || id >= nn) {
+                bad(err, errlen, "beam node id out of range");
+                delete m;
+                return nullptr;
+            }
+        }
+        const int N = B.N, Q = B.Q;
+        std::vector<double> node_xi(N);
+        for (int n = 0; n < N; ++n) node_xi[n] = 2. * d->node_s[B.node_ids[n]] - 1.;
+        B.phi.resize(N * Q);
+        B.dphi.resize(N * Q);
+        B.w.resize(Q);
+        std::vector<double> wts;
+        for (int qp = 0; qp < Q; ++qp) {
+            const double xi = d->qp_xi[q0 + qp];
+            B.w[qp] = d->qp_weight[q0 + qp];
+            lagrange_interp(xi, node_xi, wts);
+            for (int n = 0; n < N; ++n) B.phi[n * Q + qp] = wts[n];
+            lagrange_deriv(xi, node_xi, wts);
+            for (int n = 0; n < N; ++n) B.dphi[n * Q + qp] = wts[n];
+        }
+        // populate_element_views.hpp:90-141 (linear section interpolation)
+        std::vector<double> sec_xi(s1 - s0);
+        for (int s = s0; s < s1; ++s) sec_xi[s - s0] = 2. * d->section_position[s] - 1.;
+        B.mstar.assign(Q * 36, 0.);
+        B.cstar.assign(Q * 36, 0.);
+        for (int qp = 0; qp < Q; ++qp) {
+            linear_interp(d->qp_xi[q0 + qp], sec_xi, wts);
+            for (int s = 0; s < s1 - s0; ++s) {
+                for (int k = 0; k < 36; ++k) {
+                    B.mstar[qp * 36 + k] += d->section_mass[(s0 + s) * 36 + k] * wts[s];
+                    B.cstar[qp * 36 + k] += d->section_stiffness[(s0 + s) * 36 + k] * wts[s];
+                }
+            }
+        }
+        // interpolate_QP_rotation.hpp / interpolation_operations.hpp InterpQuaternion
+        B.r0.resize(Q * 4);
+        for (int qp = 0; qp < Q; ++qp) {
+            double t[4] = {0., 0., 0., 0.};
+            for (int n = 0; n < N; ++n) {
+                const double phi = B.phi[n * Q + qp];
+                for (int c = 0; c < 4; ++c) t[c] += m->x0[B.node_ids[n] * 7 + 3 + c] * phi;
+            }
+            const double len = std::sqrt(std::pow(t[0], 2) + std::pow(t[1], 2) +
+                                         std::pow(t[2], 2) + std::pow(t[3], 2));
+            if (len == 0.) {
+                B.r0[qp * 4] = 1.;
+                B.r0[qp * 4 + 1] = B.r0[qp * 4 + 2] = B.r0[qp * 4 + 3] = 0.;
+            } else {
+                for (int c = 0; c < 4; ++c) B.r0[qp * 4 + c] = t[c] / len;
+            }
+        }
+        // calculate_jacobian.hpp:36-76
+        std::vector<double> nx0(N * 7);
+        for (int n = 0; n < N; ++n)
+            for (int c = 0; c < 7; ++c) nx0[n * 7 + c] = m->x0[B.node_ids[n] * 7 + c];
+        B.x0p.resize(Q * 3);
+        B.jac.resize(Q);
+        orc_calc_jacobian(N, Q, B.dphi.data(), nx0.data(), B.x0p.data(), B.jac.data());
+        B.fx.assign(N * 6, 0.);
+        B.fe.assign(Q * 6, 0.);
+        B.residual.assign(N * 6, 0.);
+        B.sysmat.assign(N * N * 36, 0.);
+        B.eft.assign(N * 6, 0);
+    }
+
+    // src/constraints/constraints.hpp:76-266
+    m->cons.resize(d->num_constraints);
+    long start_row = 0;
+    for (int c = 0; c < d->num_constraints; ++c) {
+        OConstraint& C = m->cons[c];
+        C.type = d->constraint_type[c];
+        if (C.type != KYN_CONSTRAINT_FIXED_BC && C.type != KYN_CONSTRAINT_PRESCRIBED_BC) {
+            bad(err, errlen, "constraint type outside this path");
+            delete m;
+            return nullptr;
+        }
+        C.base = d->constraint_base_node ? d->constraint_base_node[c] : 0;
+        C.target = d->constraint_target_node[c];
+        if (C.target < 0 || C.target >= nn) {
+            bad(err, errlen, "constraint node out of range");
+            delete m;
+            return nullptr;
+        }
+        C.base_active = 0;
+        C.target_active = 6;
+        C.row_first = start_row;
+        C.row_last = start_row + 6;
+        start_row += 6;
+        const double axis[3] = {d->constraint_axis ? d->constraint_axis[c * 3] : 0.,
+                                d->constraint_axis ? d->constraint_axis[c * 3 + 1] : 0.,
+                                d->constraint_axis ? d->constraint_axis[c * 3 + 2] : 0.};
+        if (C.type == KYN_CONSTRAINT_FIXED_BC) {
+            for (int k = 0; k < 3; ++k) C.X0[k] = m->x0[C.target * 7 + k] - axis[k];
+        } else {
+            const double idq[7] = {0., 0., 0., 1., 0., 0., 0.};
+            for (int k = 0; k < 7; ++k)
+                C.input[k] = d->constraint_initial_displacement
+                                 ? d->constraint_initial_displacement[c * 7 + k]
+                                 : idq[k];
+        }
+    }
+
+    // src/dof_management/assemble_node_freedom_allocation_table.hpp
+    m->sig.assign(nn, 0U);
+    for (auto& B : m->beams)
+        for (int id : B.node_ids) m->sig[id] |= 0b111111U;
+    for (auto& C : m->cons) m->sig[C.target] |= 0b111111U;
+    m->active.resize(nn);
+    for (int n = 0; n < nn; ++n) m->active[n] = count_bits(m->sig[n]);
+    // compute_node_freedom_map_table.hpp
+    m->fmap.assign(nn, 0);
+    for (int n = 0; n + 1 < nn; ++n) m->fmap[n + 1] = m->fmap[n] + m->active[n];
+    // create_element_freedom_table.hpp / create_constraint_freedom_table.hpp
+    for (auto& B : m->beams)
+        for (int n = 0; n < B.N; ++n)
+            for (int c = 0; c < 6; ++c) B.eft[n * 6 + c] = m->fmap[B.node_ids[n]] + c;
+    for (auto& C : m->cons) {
+        for (long c = 0; c < m->active[C.target]; ++c) C.target_table[c] = m->fmap[C.target] + c;
+        for (int c = 0; c < 6; ++c) C.base_table[c] = 0;
+    }
+    m->nsys = 0;
+    for (int n = 0; n < nn; ++n) m->nsys += m->active[n];
+    m->ndofs = m->nsys + start_row;
+
+    // src/solver/create_full_matrix.hpp:27-73
+    int maxn = 1;
+    for (auto& B : m->beams) maxn = std::max(maxn, B.N);
+    std::vector<long> npe(m->beams.size()), en(m->beams.size() * maxn, 0);
+    for (size_t e = 0; e < m->beams.size(); ++e) {
+        npe[e] = m->beams[e].N;
+        for (int k = 0; k < m->beams[e].N; ++k) en[e * maxn + k] = m->beams[e].node_ids[k];
+    }
+    const int nc = static_cast<int>(m->cons.size());
+    std::vector<long> ba(nc), ta(nc), bt(nc * 6), tt(nc * 6), rr(nc * 2);
+    for (int c = 0; c < nc; ++c) {
+        ba[c] = m->cons[c].base_active;
+        ta[c] = m->cons[c].target_active;
+        for (int k = 0; k < 6; ++k) {
+            bt[c * 6 + k] = m->cons[c].base_table[k];
+            tt[c * 6 + k] = m->cons[c].target_table[k];
+        }
+        rr[c * 2] = m->cons[c].row_first;
+        rr[c * 2 + 1] = m->cons[c].row_last;
+    }
+    m->row_ptrs.resize(m->ndofs + 1);
+    const long nnz = orc_crs_build(static_cast<int>(m->nsys), static_cast<int>(m->ndofs), nn,
+                                   m->active.data(), m->fmap.data(),
+                                   static_cast<int>(m->beams.size()), maxn, npe.data(), en.data(),
+                                   nc, ba.data(), ta.data(), bt.data(), tt.data(), rr.data(),
+                                   m->row_ptrs.data(), nullptr, 1);
+    m->col_inds.resize(nnz);
+    orc_crs_build(static_cast<int>(m->nsys), static_cast<int>(m->ndofs), nn, m->active.data(),
+                  m->fmap.data(), static_cast<int>(m->beams.size()), maxn, npe.data(), en.data(),
+                  nc, ba.data(), ta.data(), bt.data(), tt.data(), rr.data(), m->row_ptrs.data(),
+                  m->col_inds.data(), 1);
+    m->values.assign(nnz, 0.);
+    m->b.assign(m->ndofs, 0.);
+    m->xsol.assign(m->ndofs, 0.);
+    return m;
+}
+
+void orc_model_destroy(orc_model* m) { delete m; }
+
+int orc_model_info(const orc_model* m, kyn_model_info* info) {
+    if (!m || !info) return KYN_ERR_INVALID;
+    info->num_nodes = m->num_nodes;
+    info->num_beams = static_cast<int32_t>(m->beams.size());
+    info->num_constraints = static_cast<int32_t>(m->cons.size());
+    info->num_system_dofs = static_cast<int32_t>(m->nsys);
+    info->num_dofs = static_cast<int32_t>(m->ndofs);
+    info->nnz = static_cast<int32_t>(m->col_inds.size());
+    int mn = 0, mq = 0;
+    for (auto& B : m->beams) {
+        mn = std::max(mn, B.N);
+        mq = std::max(mq, B.Q);
+    }
+    info->max_beam_nodes = mn;
+    info->max_beam_qps = mq;
+    info->device_bytes = 0;
+    return KYN_OK;
+}
+
+int orc_set_loads(orc_model* m, int which, const double* values) {
+    if (!m || !values) return KYN_ERR_INVALID;
+    if (which == KYN_LOAD_NODE_FX) {
+        long k = 0;
+        for (auto& B : m->beams)
+            for (int n = 0; n < B.N; ++n)
+                for (int c = 0; c < 6; ++c) B.fx[n * 6 + c] = values[k++ ];
+        return KYN_OK;
+    }
+    if (which == KYN_LOAD_STATE_F) {
+        std::copy(values, values + m->num_nodes * 6, m->f.begin());
+        return KYN_OK;
+    }
+    return KYN_ERR_INVALID;
+}
+
+int orc_set_prescribed(orc_model* m, int cid, const double u[7]) {
+    if (!m || cid < 0 || cid >= static_cast<int>(m->cons.size())) return KYN_ERR_INVALID;
+    for (int k = 0; k < 7; ++k) m->cons[cid].input[k] = u[k];
+    return KYN_OK;
+}
+
+int orc_step(orc_model* m, const kyn_step_params* p, int* iters) {
+    if (!m || !p) return KYN_ERR_INVALID;
+    return step_impl(*m, make_params(p), iters);
+}
+
+int orc_predict_and_assemble(orc_model* m, const kyn_step_params* p) {
+    if (!m || !p) return KYN_ERR_INVALID;
+    const Params P = make_params(p);
+    predict(*m, P);
+    for (auto& C : m->cons)
+        for (int c = 0; c < 6; ++c) C.lambda[c] = C.sys_res[c] = 0.;
+    assemble(*m, P);
+    return KYN_OK;
+}
+
+int orc_get_state(const orc_model* m, int field, double* out) {
+    if (!m || !out) return KYN_ERR_INVALID;
+    const std::vector<double>* src = nullptr;
+    switch (field) {
+        case KYN_FIELD_X0: src = &m->x0; break;
+        case KYN_FIELD_X: src = &m->x; break;
+        case KYN_FIELD_Q: src = &m->q; break;
+        case KYN_FIELD_Q_PREV: src = &m->q_prev; break;
+        case KYN_FIELD_Q_DELTA: src = &m->q_delta; break;
+        case KYN_FIELD_V: src = &m->v; break;
+        case KYN_FIELD_VD: src = &m->vd; break;
+        case KYN_FIELD_A: src = &m->a; break;
+        case KYN_FIELD_F: src = &m->f; break;
+        case KYN_FIELD_TANGENT: src = &m->tangent; break;
+        case KYN_FIELD_LAMBDA: {
+            for (size_t c = 0; c < m->cons.size(); ++c)
+                for (int k = 0; k < 6; ++k) out[c * 6 + k] = m->cons[c].lambda[k];
+            return KYN_OK;
+        }
+        default: return KYN_ERR_INVALID;
+    }
+    std::copy(src->begin(), src->end(), out);
+    return KYN_OK;
+}
+
+int orc_get_crs(const orc_model* m, int* rp, int* ci, double* vals) {
+    if (!m) return KYN_ERR_INVALID;
+    if (rp)
+        for (size_t i = 0; i < m->row_ptrs.size(); ++i) rp[i] = static_cast<int>(m->row_ptrs[i]);
+    if (ci)
+        for (size_t i = 0; i < m->col_inds.size(); ++i) ci[i] = static_cast<int>(m->col_inds[i]);
+    if (vals) std::copy(m->values.begin(), m->values.end(), vals);
+    return KYN_OK;
+}
+
+int orc_get_system_vectors(const orc_model* m, double* rhs, double* sol) {
+    if (!m) return KYN_ERR_INVALID;
+    if (rhs) std::copy(m->b.begin(), m->b.end(), rhs);
+    if (sol) std::copy(m->xsol.begin(), m->xsol.end(), sol);
+    return KYN_OK;
+}
+
+int orc_get_convergence(const orc_model* m, double* errs, int* n) {
+    if (!m) return KYN_ERR_INVALID;
+    if (errs) std::copy(m->conv.begin(), m->conv.end(), errs);
+    if (n) *n = static_cast<int>(m->conv.size());
+    return KYN_OK;
+}
+
+int orc_get_element_terms(const orc_model* m, int e, double* residual, double* sysmat) {
+    if (!m || e < 0 || e >= static_cast<int>(m->beams.size())) return KYN_ERR_INVALID;
+    const OBeam& B = m->beams[e];
+    if (residual) std::copy(B.residual.begin(), B.residual.end(), residual);
+    if (sysmat) std::copy(B.sysmat.begin(), B.sysmat.end(), sysmat);
+    return KYN_OK;
+}
+
+long orc_run_batch(orc_model** models, int n, const kyn_step_params* p, int steps,
+                   const double* amp, const double* freq, int nthreads, double* seconds,
+                   int* iters_total) {
+    const Params P = make_params(p);
+    long converged = 0;
+    long iters = 0;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+    const auto t0 = std::chrono::steady_clock::now();
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : converged, iters)
+    for (int i = 0; i < n; ++i) {
+        orc_model& m = *models[i];
+        for (int k = 0; k < steps; ++k) {
+            if (amp && freq && !m.beams.empty()) {
+                OBeam& B = m.beams[0];
+                const double t = P.h * static_cast<double>(k + 1);
+                B.fx[(B.N - 1) * 6 + 2] = amp[i] * std::sin(2. * M_PI * freq[i] * t);
+            }
+            int it = 0;
+            const int st = step_impl(m, P, &it);
+            iters += it;
+            if (st == KYN_OK) ++converged;
+        }
+    }
+    const auto t1 = std::chrono::steady_clock::now();
+    if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+    if (iters_total) *iters_total = static_cast<int>(iters);
+    return converged;
+}
+
+// ---- kernel-level entry points --------------------------------------------
+
+void orc_lagrange_interp_weights(double x, const double* xs, int n, double* w) {
+    std::vector<double> v(xs, xs + n), out;
+    lagrange_interp(x, v, out);
+    std::copy(out.begin(), out.end(), w);
+}
+
+void orc_lagrange_deriv_weights(double x, const double* xs, int n, double* w) {
+    std::vector<double> v(xs, xs + n), out;
+    lagrange_deriv(x, v, out);
+    std::copy(out.begin(), out.end(), w);
+}
+
+// src/math/interpolation.hpp GenerateGLLPoints
+void orc_gll_points(int order, double* pts) {
+    const int nn = order + 1;
+    std::vector<double> g(nn, 0.);
+    g.front() = -1.;
+    g.back() = 1.;
+    auto legendre = [](int n, double x) {
+        if (n == 0) return 1.;
+        if (n == 1) return x;
+        double p2 = 1., p1 = x, p = 0.;
+        for (int i = 2; i <= n; ++i) {
+            const double id = static_cast<double>(i);
+            p = ((2. * id - 1.) * x * p1 - (id - 1.) * p2) / id;
+            p2 = p1;
+            p1 = p;
+        }
+        return p;
+    };
+    for (int i = 1; i < order; ++i) {
+        double x = -std::cos(static_cast<double>(i) * M_PI / static_cast<double>(order));
+        for (int it = 0; it < 1000; ++it) {
+            const double xo = x;
+            const double pn = legendre(nn - 1, x), pm = legendre(nn - 2, x);
+            const double num = x * pn - pm;
+            const double den = static_cast<double>(nn) * pn;
+            x -= num / den;
+            if (std::abs(x - xo) <= std::numeric_limits<double>::epsilon()) break;
+        }
+        g[i] = x;
+    }
+    std::copy(g.begin(), g.end(), pts);
+}
+
+void orc_rotate_section(const double xr[4], const double cstar[36], double out[36]) {
+    rotate_section(xr, cstar, out);
+}
+
+void orc_calc_strain(const double x0p[3], const double up[3], const double r[4],
+                     const double rp[4], double strain[6]) {
+    calc_strain(x0p, up, r, rp, strain);
+}
+
+void orc_calc_fc(const double cuu[36], const double strain[6], double fc[6]) {
+    gemv(false, 6, 6, 1., cuu, 6, strain, 0., fc);
+}
+
+void orc_calc_fd(const double ss[9], const double fc[6], double fd[6]) {
+    for (int i = 0; i < 6; ++i) fd[i] = 0.;
+    gemv(true, 3, 3, 1., ss, 3, fc, 0., fd + 3);
+}
+
+void orc_calc_ouu(const double cuu[36], const double ss[9], const double mt[9],
+                  const double nt[9], double out[36]) {
+    calc_ouu(cuu, ss, mt, nt, out);
+}
+
+void orc_calc_puu(const double cuu[36], const double ss[9], const double nt[9], double out[36]) {
+    calc_puu(cuu, ss, nt, out);
+}
+
+void orc_calc_quu(const double cuu[36], const double ss[9], const double nt[9], double out[36]) {
+    calc_quu(cuu, ss, nt, out);
+}
+
+// src/elements/beams/calculate_jacobian.hpp:36-76
+void orc_calc_jacobian(int nn, int nq, const double* sd, const double* nx0, double* x0p,
+                       double* jac) {
+    for (int qp = 0; qp < nq; ++qp) {
+        double t[3] = {0., 0., 0.};
+        for (int n = 0; n < nn; ++n) {
+            const double phi = sd[n * nq + qp];
+            for (int c = 0; c < 3; ++c) t[c] += nx0[n * 7 + c] * phi;
+        }
+        for (int c = 0; c < 3; ++c) x0p[qp * 3 + c] = t[c];
+    }
+    for (int qp = 0; qp < nq; ++qp) {
+        const double j = std::sqrt(std::pow(x0p[qp * 3], 2.) + std::pow(x0p[qp * 3 + 1], 2.) +
+                                   std::pow(x0p[qp * 3 + 2], 2.));
+        jac[qp] = j;
+        for (int c = 0; c < 3; ++c) x0p[qp * 3 + c] /= j;
+    }
+}
+
+// src/system/beams/integrate_residual_vector.hpp:33-50
+void orc_integrate_residual(int nn, int nq, const double* w, const double* jac,
+                            const double* phi, const double* dphi, const double* fx,
+                            const double* fc, const double* fd, const double* fi,
+                            const double* fe, const double* fg, double* out) {
+    for (int n = 0; n < nn; ++n) {
+        double loc[6] = {0, 0, 0, 0, 0, 0};
+        for (int qp = 0; qp < nq; ++qp) {
+            const double weight = w[qp];
+            const double cc = weight * dphi[n * nq + qp];
+            const double cd = weight * jac[qp] * phi[n * nq + qp];
+            for (int c = 0; c < 6; ++c)
+                loc[c] += cc * fc[qp * 6 + c] +
+                          cd * (fd[qp * 6 + c] + fi[qp * 6 + c] - fe[qp * 6 + c] - fg[qp * 6 + c]);
+        }
+        for (int c = 0; c < 6; ++c) out[n * 6 + c] = loc[c] - fx[n * 6 + c];
+    }
+}
+
+// src/system/beams/integrate_stiffness_matrix.hpp:35-96
+void orc_integrate_stiffness(int nn, int nq, const double* w, const double* jac,
+                             const double* phi, const double* dphi, const double* kuu,
+                             const double* puu, const double* cuu, const double* ouu,
+                             const double* quu, double* out) {
+    for (int i = 0; i < nn; ++i) {
+        for (int j = 0; j < nn; ++j) {
+            double loc[36] = {};
+            for (int qp = 0; qp < nq; ++qp) {
+                const double ww = w[qp], J = jac[qp];
+                const double p1 = phi[i * nq + qp], p2 = phi[j * nq + qp];
+                const double d1 = dphi[i * nq + qp], d2 = dphi[j * nq + qp];
+                const double K = (p1 * p2) * (ww * J);
+                const double P = (p1 * d2) * ww;
+                const double C = (d1 * d2) * (ww / J);
+                const double O = (d1 * p2) * ww;
+                for (int c = 0; c < 36; ++c)
+                    loc[c] = loc[c] + K * (kuu[qp * 36 + c] + quu[qp * 36 + c]) +
+                             P * puu[qp * 36 + c] + C * cuu[qp * 36 + c] + O * ouu[qp * 36 + c];
+            }
+            for (int c = 0; c < 36; ++c) out[(i * nn + j) * 36 + c] = loc[c];
+        }
+    }
+}
+
+// src/system/beams/integrate_inertia_matrix.hpp:32-78
+void orc_integrate_inertia(int nn, int nq, const double* w, const double* jac,
+                           const double* phi, const double* muu, const double* guu,
+                           double bp, double gp, double* out) {
+    for (int i = 0; i < nn; ++i) {
+        for (int j = 0; j < nn; ++j) {
+            double loc[36] = {};
+            for (int qp = 0; qp < nq; ++qp) {
+                const double coeff = phi[i * nq + qp] * phi[j * nq + qp] * w[qp] * jac[qp];
+                for (int c = 0; c < 36; ++c) {
+                    const double contribution = bp * muu[qp * 36 + c] + gp * guu[qp * 36 + c];
+                    loc[c] = loc[c] + coeff * contribution;
+                }
+            }
+            for (int c = 0; c < 36; ++c) out[(i * nn + j) * 36 + c] = loc[c];
+        }
+    }
+}
+
+void orc_inertial_qp(double, const double mstar[36], const double r0[4], const double r[4],
+                     const double uddot[3], const double omega[3], const double omegadot[3],
+                     const double gravity[3], double fi[6], double fg[6], double muu[36],
+                     double guu[36], double kuu[36]) {
+    inertial_qp(mstar, r0, r, uddot, omega, omegadot, gravity, fi, fg, muu, guu, kuu);
+}
+
+void orc_tangent_operator(double h, const double qdelta[6], double t_stored[36]) {
+    tangent_operator(h, qdelta, t_stored);
+}
+
+}  // extern "C"

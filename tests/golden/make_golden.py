@@ -1,0 +1,193 @@
+"""Extract the reference's golden vectors into JSON fixtures.
+
+Run in the build container (where the reference tree is mounted):
+    python tests/golden/make_golden.py /root/reference
+It reads the reference's own test sources as text, pulls the numeric
+literals of the named initialisers, and writes tests/golden/*.json.  The GPU
+box never reads the reference; tests use only the committed JSON.
+
+Sources (paths relative to the reference project root):
+  tests/regression_tests/regression/iea15_rotor_data.hpp   IEA-15 rotor inputs
+  tests/regression_tests/regression/test_rotor.cpp:150-189   IEA-15 expected q
+  tests/regression_tests/regression/test_cantilever_beam.cpp expected tip q
+  tests/regression_tests/regression/test_solver.cpp          assembled b, x, err
+  tests/regression_tests/regression/test_rotating_beam.cpp   expected q
+  tests/unit_tests/system/beams/test_curved_beam.hpp         kernel-level data
+"""
+from __future__ import annotations
+
+import json
+import os
+import re
+import sys
+
+NUM = r"[-+]?(?:\d+\.\d*|\.\d+|\d+)(?:[eE][-+]?\d+)?"
+
+
+def strip_comments(text: str) -> str:
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return re.sub(r"//[^\n]*", "", text)
+
+
+def _block(text: str, start: int) -> str:
+    """Return the balanced {...} block beginning at the first '{' after start."""
+    i = text.index("{", start)
+    depth = 0
+    for j in range(i, len(text)):
+        if text[j] == "{":
+            depth += 1
+        elif text[j] == "}":
+            depth -= 1
+            if depth == 0:
+                return text[i : j + 1]
+    raise ValueError("unbalanced braces")
+
+
+def numbers_of(text: str, name: str, known: dict | None = None) -> list[float]:
+    m = re.search(r"\b" + re.escape(name) + r"\b[^=;{]*=", text)
+    if not m:
+        raise KeyError(name)
+    blk = _block(text, m.end())
+    # resolve element references to other initialisers, e.g. kStrainInterpolationHolder[2]
+    if known:
+        def sub(mm):
+            return repr(known[mm.group(1)][int(mm.group(2))])
+        blk = re.sub(r"\b(\w+)\[(\d+)\]", lambda mm: sub(mm) if mm.group(1) in known
+                     else mm.group(0), blk)
+        blk = re.sub(r"-\s*-", "", blk)
+    # drop template arguments like std::array<double, 3> inside initialisers
+    blk = re.sub(r"std::array<[^>]*>", "", blk)
+    blk = re.sub(r"std::array\b", "", blk)
+    return [float(x) for x in re.findall(NUM, blk)]
+
+
+def expect_near_values(text: str, start_pat: str, stop_pat: str) -> list[tuple[str, float]]:
+    i = text.index(start_pat)
+    j = text.index(stop_pat, i)
+    out = []
+    for m in re.finditer(r"EXPECT_NEAR\(\s*q\((\d+),\s*(\d+)\),\s*(" + NUM + r"|q\(\d+,\s*\d+\))",
+                         text[i:j]):
+        out.append((m.group(1), m.group(2), m.group(3)))
+    return out
+
+
+def view_after(text: str, anchor: str, occurrence: int = 0) -> list[float]:
+    """Numbers of the brace block passed to the expect_* call after `anchor`."""
+    pos = -1
+    for _ in range(occurrence + 1):
+        pos = text.index(anchor, pos + 1)
+    return [float(x) for x in re.findall(NUM, _block(text, pos))]
+
+
+def main(ref: str) -> None:
+    out_dir = os.path.dirname(os.path.abspath(__file__))
+    reg = os.path.join(ref, "tests", "regression_tests", "regression")
+    unit = os.path.join(ref, "tests", "unit_tests", "system", "beams")
+
+    # ---- IEA-15 rotor ----------------------------------------------------
+    rd = strip_comments(open(os.path.join(reg, "iea15_rotor_data.hpp")).read())
+    node_xi = numbers_of(rd, "node_xi")
+    coords = numbers_of(rd, "node_coords")
+    quad = numbers_of(rd, "trapz_quadrature")
+    secs = numbers_of(rd, "material_sections")
+    assert len(coords) == 7 * len(node_xi)
+    assert len(secs) % 73 == 0
+    sections = []
+    for k in range(len(secs) // 73):
+        s = secs[73 * k : 73 * (k + 1)]
+        sections.append({"position": s[0], "M_star": s[1:37], "C_star": s[37:73]})
+    rt = strip_comments(open(os.path.join(reg, "test_rotor.cpp")).read())
+    exp = []
+    for node, comp, val in expect_near_values(rt, "TEST(RotorTest, IEA15Rotor)",
+                                              "TEST(RotorTest, IEA15RotorHub)"):
+        ref_m = re.match(r"q\((\d+),\s*(\d+)\)", val)
+        exp.append([int(node), int(comp),
+                    [int(ref_m.group(1)), int(ref_m.group(2))] if ref_m else float(val)])
+    rotor = {
+        "source": "tests/regression_tests/regression/iea15_rotor_data.hpp, test_rotor.cpp",
+        "node_xi": node_xi,
+        "node_coords": [coords[7 * i : 7 * i + 7] for i in range(len(node_xi))],
+        "quadrature": [quad[2 * i : 2 * i + 2] for i in range(len(quad) // 2)],
+        "sections": sections,
+        "omega": [0.0, 0.0, -0.79063415025],
+        "hub_radius": 3.97,
+        "gravity": [-9.81, 0.0, 0.0],
+        "max_iter": 6, "h": 0.01, "rho_inf": 0.0, "num_steps": 11,
+        "tolerance": 1e-13,
+        "expected_q": exp,
+    }
+    json.dump(rotor, open(os.path.join(out_dir, "iea15_rotor.json"), "w"), indent=1)
+
+    # ---- cantilever ----------------------------------------------------------
+    ct = strip_comments(open(os.path.join(reg, "test_cantilever_beam.cpp")).read())
+    tips = [view_after(ct, "expect_kokkos_view_1D_equal", k) for k in range(3)]
+    json.dump({"source": "tests/regression_tests/regression/test_cantilever_beam.cpp",
+               "tip_q": tips, "tolerance": 1e-6},
+              open(os.path.join(out_dir, "cantilever.json"), "w"), indent=1)
+
+    # ---- solver ----------------------------------------------------------------
+    st = strip_comments(open(os.path.join(reg, "test_solver.cpp")).read())
+    s1 = st.index("inline void SetUpSolverAndAssemble")
+    s2 = st.index("inline void SetupAndTakeNoSteps")
+    s3 = st.index("inline auto SetupAndTakeTwoSteps")
+    t1, t2, t3 = st[s1:s2], st[s2:s3], st[s3:]
+    solver = {
+        "source": "tests/regression_tests/regression/test_solver.cpp",
+        "predict": {
+            "residual_terms": view_after(t1, "constraints.residual_terms"),
+            "b": view_after(t1, "Kokkos::subview(solver.b"),
+            "q": view_after(t1, "state.q,"),
+            "q_delta": view_after(t1, "state.q_delta,"),
+            "v": view_after(t1, "state.v,"),
+        },
+        "one_iteration": {
+            "x": view_after(t2, "Kokkos::subview(solver.x"),
+            "convergence_err": float(re.search(r"convergence_err\[0\],\s*(" + NUM + ")",
+                                               t2).group(1)),
+            "q_delta": view_after(t2, "state.q_delta,"),
+            "v": view_after(t2, "state.v,"),
+            "vd": view_after(t2, "state.vd,"),
+            "q": view_after(t2, "state.q,"),
+            "lambda": view_after(t2, "constraints.lambda,"),
+        },
+        "two_iterations": {
+            "residual_terms": view_after(t3, "constraints.residual_terms"),
+            "b": view_after(t3, "Kokkos::subview(solver.b"),
+            "x": view_after(t3, "Kokkos::subview(solver.x"),
+        },
+        "tolerance": 1e-6,
+    }
+    json.dump(solver, open(os.path.join(out_dir, "solver.json"), "w"), indent=1)
+
+    # ---- rotating beam -----------------------------------------------------------
+    rb = strip_comments(open(os.path.join(reg, "test_rotating_beam.cpp")).read())
+    r0 = rb.index("TEST(RotatingBeamTest, StepConvergence)")
+    json.dump({"source": "tests/regression_tests/regression/test_rotating_beam.cpp",
+               "q": view_after(rb[r0:], "state.q,"), "tolerance": 1e-6},
+              open(os.path.join(out_dir, "rotating_beam.json"), "w"), indent=1)
+
+    # ---- curved beam (kernel level) --------------------------------------------
+    cb = strip_comments(open(os.path.join(unit, "test_curved_beam.hpp")).read())
+    names = ["kCurvedBeamNodes_data", "kGaussQuadraturePoints", "kGaussQuadratureWeights",
+             "kExpectedInterpWeights", "kExpectedDerivWeights", "kExpectedJacobians",
+             "kCurvedBeamCuu_data", "kCurvedBeamStrain_data", "kExpectedFc_data",
+             "kX0pupSS_data", "kExpectedFd_data", "kInterpWeightsFlat", "kDerivWeightsFlat",
+             "kFc", "kFd", "kFi", "kExpectedResidualVector", "xr_data", "Cstar_data",
+             "kExpectedCuu_data", "kCurvedBeamM_tilde_data", "kCurvedBeamN_tilde_data",
+             "kExpectedOuu_data", "kExpectedPuu_data", "kExpectedQuu_data", "kKuu", "kOuu",
+             "kPuu", "kQuu", "kCuu", "kExpectedStiffnessMatrix_data"]
+    curved = {"source": "tests/unit_tests/system/beams/test_curved_beam.hpp"}
+    known = {"kStrainInterpolationHolder": numbers_of(cb, "kStrainInterpolationHolder")}
+    for n in names:
+        curved[n] = numbers_of(cb, n, known)
+    ctcpp = open(os.path.join(unit, "test_curved_beam.cpp")).read()
+    gll = re.search(r"kGLLNodes\s*\{([^}]*)\}", cb)
+    curved["kGLLNodes"] = [float(x) for x in re.findall(NUM, gll.group(1))]
+    curved["tolerance"] = 1e-12
+    curved["test_source_lines"] = len(ctcpp.splitlines())
+    json.dump(curved, open(os.path.join(out_dir, "curved_beam.json"), "w"), indent=1)
+    print("wrote fixtures to", out_dir)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

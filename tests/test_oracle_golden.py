@@ -1,0 +1,101 @@
+"""The oracle against the reference's own regression-test golden values.
+
+Fixtures come from tests/golden/make_golden.py (reference test sources read as
+text).  Tolerances are the reference tests' own.
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle_py import OracleModel
+from openturbine_b200.model import StepParameters
+from tests.workloads_ref import (cantilever_test_loads, cantilever_test_model,
+                                 iea15_hub_displacement, iea15_rotor_model, load_golden,
+                                 rotating_beam_root_displacement, rotating_beam_test_model,
+                                 solver_test_model, solver_test_root_displacement)
+
+
+def test_iea15_rotor_q_1e13():
+    """test_rotor.cpp:87-189: 3 blades, 11 GLL nodes, 51-pt trapezoid, 11 steps."""
+    d = load_golden("iea15_rotor.json")
+    m, p, bc = iea15_rotor_model(d)
+    o = OracleModel(m.pack())
+    assert (o.info.num_dofs, o.info.num_system_dofs) == (216, 198)
+    for i in range(d["num_steps"]):
+        u = iea15_hub_displacement(i, d)
+        for c in bc:
+            o.set_prescribed(c, u)
+        st, _ = o.step(p)
+        assert st == 0
+    q = o.state("q")
+    for node, comp, val in d["expected_q"]:
+        ev = q[val[0], val[1]] if isinstance(val, list) else val
+        assert abs(q[node, comp] - ev) <= d["tolerance"], (node, comp, q[node, comp], ev)
+
+
+def test_cantilever_tip():
+    """test_cantilever_beam.cpp:31-138."""
+    g = load_golden("cantilever.json")
+    m, p = cantilever_test_model()
+    o = OracleModel(m.pack())
+    for k in range(3):
+        o.set_node_fx(cantilever_test_loads(k))
+        st, _ = o.step(p)
+        assert st == 0
+        np.testing.assert_allclose(o.state("q")[4, :3], g["tip_q"][k], rtol=0, atol=g["tolerance"])
+
+
+def test_solver_predict_assembly():
+    """test_solver.cpp:18-243: state and b after predict + assemble."""
+    g = load_golden("solver.json")["predict"]
+    m = solver_test_model(2.0)
+    o = OracleModel(m.pack())
+    o.set_prescribed(0, solver_test_root_displacement(2.0))
+    o.predict_and_assemble(StepParameters(True, 10, 0.01, 0.9))
+    b, _ = o.system_vectors()
+    np.testing.assert_allclose(b, g["b"], rtol=0, atol=1e-6)
+    np.testing.assert_allclose(o.state("q").ravel(), g["q"], rtol=0, atol=1e-6)
+    np.testing.assert_allclose(o.state("q_delta").ravel(), g["q_delta"], rtol=0, atol=1e-6)
+    np.testing.assert_allclose(o.state("v").ravel(), g["v"], rtol=0, atol=1e-6)
+
+
+def test_solver_one_iteration():
+    """test_solver.cpp:247-440: x, convergence_err[0] and state after one iteration."""
+    g = load_golden("solver.json")["one_iteration"]
+    m = solver_test_model(2.0)
+    o = OracleModel(m.pack())
+    o.set_prescribed(0, solver_test_root_displacement(2.0))
+    st, it = o.step(StepParameters(True, 1, 0.01, 0.9))
+    assert (st, it) == (1, 1)  # max_iter 1 -> Step() returns false after one iteration
+    _, x = o.system_vectors()
+    np.testing.assert_allclose(x, g["x"], rtol=0, atol=1e-6)
+    assert abs(o.convergence()[0] - g["convergence_err"]) <= 1e-6 * g["convergence_err"]
+    for f in ("q_delta", "v", "vd", "q"):
+        np.testing.assert_allclose(o.state(f).ravel(), g[f], rtol=0, atol=1e-6)
+    np.testing.assert_allclose(o.state("lambda").ravel(), g["lambda"], rtol=0, atol=1e-6)
+
+
+def test_solver_two_iterations():
+    """test_solver.cpp:444-605: b and x of the second iteration."""
+    g = load_golden("solver.json")["two_iterations"]
+    m = solver_test_model(0.0)
+    o = OracleModel(m.pack())
+    q = StepParameters(True, 2, 0.01, 0.9)
+    from openturbine_b200.model import RotationVectorToQuaternion
+    u = RotationVectorToQuaternion([0., 0., 0.1 * 0.01])
+    o.set_prescribed(0, [0., 0., 0., *u])
+    o.step(q)
+    b, x = o.system_vectors()
+    np.testing.assert_allclose(b, g["b"], rtol=0, atol=1e-6)
+    np.testing.assert_allclose(x, g["x"], rtol=0, atol=1e-6)
+
+
+def test_rotating_beam_ten_steps():
+    """test_rotating_beam.cpp:93-150."""
+    g = load_golden("rotating_beam.json")
+    m, p = rotating_beam_test_model()
+    o = OracleModel(m.pack())
+    for i in range(10):
+        o.set_prescribed(0, rotating_beam_root_displacement(i))
+        st, _ = o.step(p)
+        assert st == 0
+    np.testing.assert_allclose(o.state("q").ravel(), g["q"], rtol=0, atol=g["tolerance"])

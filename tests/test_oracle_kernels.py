@@ -1,0 +1,106 @@
+"""Kernel-level oracle functions against test_curved_beam.hpp (Mathematica data)
+and the reference's math unit tests."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle.oracle_py import lib
+from tests.workloads_ref import load_golden
+
+D = ctypes.POINTER(ctypes.c_double)
+
+
+def p(a):
+    return np.ascontiguousarray(a, dtype=np.float64).ctypes.data_as(D)
+
+
+@pytest.fixture(scope="module")
+def cb():
+    return {k: (np.array(v) if isinstance(v, list) else v)
+            for k, v in load_golden("curved_beam.json").items()}
+
+
+def test_lagrange_weights(cb):
+    L = lib()
+    gll = np.array(cb["kGLLNodes"])
+    for qp, x in enumerate(cb["kGaussQuadraturePoints"]):
+        w = np.zeros(3)
+        L.orc_lagrange_interp_weights(ctypes.c_double(x), p(gll), 3, p(w) if False else w.ctypes.data_as(D))
+        np.testing.assert_allclose(w, cb["kExpectedInterpWeights"].reshape(7, 3)[qp], atol=1e-12)
+        L.orc_lagrange_deriv_weights(ctypes.c_double(x), p(gll), 3, w.ctypes.data_as(D))
+        np.testing.assert_allclose(w, cb["kExpectedDerivWeights"].reshape(7, 3)[qp], atol=1e-12)
+
+
+def test_jacobian(cb):
+    L = lib()
+    nodes = cb["kCurvedBeamNodes_data"].reshape(3, 7)
+    dphi = cb["kDerivWeightsFlat"].reshape(3, 7)
+    x0p = np.zeros((7, 3))
+    jac = np.zeros(7)
+    L.orc_calc_jacobian(3, 7, p(dphi), p(nodes), x0p.ctypes.data_as(D), jac.ctypes.data_as(D))
+    np.testing.assert_allclose(jac, cb["kExpectedJacobians"], atol=1e-12)
+    np.testing.assert_allclose(np.linalg.norm(x0p, axis=1), 1.0, atol=1e-12)
+
+
+def test_forces_and_matrices(cb):
+    L = lib()
+    fc = np.zeros(6)
+    L.orc_calc_fc(p(cb["kCurvedBeamCuu_data"]), p(cb["kCurvedBeamStrain_data"]), fc.ctypes.data_as(D))
+    np.testing.assert_allclose(fc, cb["kExpectedFc_data"], atol=1e-6)
+    fd = np.zeros(6)
+    L.orc_calc_fd(p(cb["kX0pupSS_data"]), p(cb["kExpectedFc_data"]), fd.ctypes.data_as(D))
+    np.testing.assert_allclose(fd, cb["kExpectedFd_data"], atol=1e-6)
+    cuu = np.zeros(36)
+    L.orc_rotate_section(p(cb["xr_data"]), p(cb["Cstar_data"]), cuu.ctypes.data_as(D))
+    np.testing.assert_allclose(cuu, cb["kExpectedCuu_data"], atol=1e-6)
+    out = np.zeros(36)
+    L.orc_calc_ouu(p(cb["kCurvedBeamCuu_data"]), p(cb["kX0pupSS_data"]),
+                   p(cb["kCurvedBeamM_tilde_data"]), p(cb["kCurvedBeamN_tilde_data"]),
+                   out.ctypes.data_as(D))
+    np.testing.assert_allclose(out, cb["kExpectedOuu_data"], atol=1e-6)
+    L.orc_calc_puu(p(cb["kCurvedBeamCuu_data"]), p(cb["kX0pupSS_data"]),
+                   p(cb["kCurvedBeamN_tilde_data"]), out.ctypes.data_as(D))
+    np.testing.assert_allclose(out, cb["kExpectedPuu_data"], atol=1e-6)
+    L.orc_calc_quu(p(cb["kCurvedBeamCuu_data"]), p(cb["kX0pupSS_data"]),
+                   p(cb["kCurvedBeamN_tilde_data"]), out.ctypes.data_as(D))
+    np.testing.assert_allclose(out, cb["kExpectedQuu_data"], atol=1e-6)
+
+
+def test_integrate_residual(cb):
+    L = lib()
+    out = np.zeros((3, 6))
+    z6 = np.zeros((7, 6))
+    L.orc_integrate_residual(3, 7, p(cb["kGaussQuadratureWeights"]), p(cb["kExpectedJacobians"]),
+                             p(cb["kInterpWeightsFlat"].reshape(3, 7)),
+                             p(cb["kDerivWeightsFlat"].reshape(3, 7)), p(np.zeros((3, 6))),
+                             p(cb["kFc"]), p(cb["kFd"]), p(cb["kFi"]), p(z6), p(z6),
+                             out.ctypes.data_as(D))
+    np.testing.assert_allclose(out.ravel(), cb["kExpectedResidualVector"], atol=1e-8)
+
+
+def test_integrate_stiffness(cb):
+    L = lib()
+    out = np.zeros((3, 3, 36))
+    L.orc_integrate_stiffness(3, 7, p(cb["kGaussQuadratureWeights"]), p(cb["kExpectedJacobians"]),
+                              p(cb["kInterpWeightsFlat"].reshape(3, 7)),
+                              p(cb["kDerivWeightsFlat"].reshape(3, 7)), p(cb["kKuu"]),
+                              p(cb["kPuu"]), p(cb["kCuu"]), p(cb["kOuu"]), p(cb["kQuu"]),
+                              out.ctypes.data_as(D))
+    np.testing.assert_allclose(out.ravel(), cb["kExpectedStiffnessMatrix_data"], atol=1e-7)
+
+
+def test_gll_points_match_rotor_nodes():
+    """GenerateGLLPoints(10) reproduces the IEA-15 node_xi literals."""
+    L = lib()
+    pts = np.zeros(11)
+    L.orc_gll_points(10, pts.ctypes.data_as(D))
+    np.testing.assert_allclose(pts, load_golden("iea15_rotor.json")["node_xi"], atol=1e-15)
+
+
+def test_tangent_operator_small_angle():
+    """calculate_tangent_operator.hpp: identity below phi = 1e-16."""
+    L = lib()
+    T = np.zeros(36)
+    L.orc_tangent_operator(ctypes.c_double(0.01), p(np.zeros(6)), T.ctypes.data_as(D))
+    np.testing.assert_array_equal(T.reshape(6, 6), np.eye(6))

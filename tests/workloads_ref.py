@@ -1,0 +1,138 @@
+"""Model builders that restate the reference's regression-test setups.
+
+Each builder follows the cited reference test so that the oracle (and the GPU
+path) can be checked against the reference's golden values.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+
+import numpy as np
+
+from openturbine_b200.model import (BeamSection, Model, RotateVectorByQuaternion,
+                                    RotationVectorToQuaternion, StepParameters)
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def load_golden(name: str) -> dict:
+    with open(os.path.join(GOLDEN, name)) as f:
+        return json.load(f)
+
+
+# Uniform composite section of test_cantilever_beam.cpp / test_solver.cpp.
+COMPOSITE_MASS = np.diag([8.538e-2, 8.538e-2, 8.538e-2, 1.4433e-2, 0.40972e-2, 1.0336e-2])
+COMPOSITE_STIFF = np.array([
+    [1368.17e3, 0., 0., 0., 0., 0.],
+    [0., 88.56e3, 0., 0., 0., 0.],
+    [0., 0., 38.78e3, 0., 0., 0.],
+    [0., 0., 0., 16.9600e3, 17.6100e3, -0.3510e3],
+    [0., 0., 0., 17.6100e3, 59.1200e3, -0.3700e3],
+    [0., 0., 0., -0.3510e3, -0.3700e3, 141.470e3],
+])
+GAUSS7 = [
+    [-0.9491079123427585, 0.1294849661688697], [-0.7415311855993943, 0.27970539148927664],
+    [-0.40584515137739696, 0.3818300505051189], [6.123233995736766e-17, 0.4179591836734694],
+    [0.4058451513773971, 0.3818300505051189], [0.7415311855993945, 0.27970539148927664],
+    [0.9491079123427585, 0.1294849661688697],
+]
+GLL6_S = [0., 0.11747233803526763, 0.35738424175967748, 0.64261575824032247,
+          0.88252766196473242, 1.]
+
+
+def cantilever_test_model():
+    """tests/regression_tests/regression/test_cantilever_beam.cpp:31-100."""
+    node_s = [0., 0.17267316464601146, 0.5, 0.8273268353539885, 1.]
+    m = Model()
+    m.SetGravity(0., 0., 0.)
+    ids = [m.AddNode().SetElemLocation(s).SetPosition(10 * s, 0., 0., 1., 0., 0., 0.).Build()
+           for s in node_s]
+    m.AddBeamElement(ids, [BeamSection(0., COMPOSITE_MASS, COMPOSITE_STIFF),
+                           BeamSection(1., COMPOSITE_MASS, COMPOSITE_STIFF)], GAUSS7)
+    m.AddFixedBC(ids[0])
+    return m, StepParameters(True, 5, 0.005, 0.0)
+
+
+def cantilever_test_loads(step: int) -> np.ndarray:
+    fx = np.zeros((5, 6))
+    fx[4, 2] = 100. * math.sin(10.0 * 0.005 * (step + 1))
+    return fx
+
+
+def solver_test_model(x_root: float = 2.0, with_velocity: bool = True):
+    """tests/regression_tests/regression/test_solver.cpp:18-110 (6-node rotating beam)."""
+    omega = 0.1
+    m = Model()
+    m.SetGravity(0., 0., 0.)
+    ids = []
+    for s in GLL6_S:
+        x = 10 * s + x_root
+        b = m.AddNode().SetElemLocation(s).SetPosition(x, 0., 0., 1., 0., 0., 0.)
+        if with_velocity:
+            b.SetVelocity(0., x * omega, 0., 0., 0., omega)
+        ids.append(b.Build())
+    m.AddBeamElement(ids, [BeamSection(0., COMPOSITE_MASS, COMPOSITE_STIFF),
+                           BeamSection(1., COMPOSITE_MASS, COMPOSITE_STIFF)], GAUSS7)
+    m.AddPrescribedBC(ids[0])
+    return m
+
+
+def solver_test_root_displacement(x_root: float = 2.0, omega: float = 0.1, h: float = 0.01):
+    u_rot = RotationVectorToQuaternion([0., 0., omega * h])
+    xr = RotateVectorByQuaternion(u_rot, [x_root, 0., 0.])
+    return [xr[0] - x_root, xr[1] - 0., xr[2] - 0., *u_rot]
+
+
+def rotating_beam_test_model():
+    """tests/regression_tests/regression/test_rotating_beam.cpp:93-125."""
+    m = Model()
+    m.SetGravity(0., 0., 0.)
+    ids = [m.AddNode().SetElemLocation(s).SetPosition(10 * s, 0., 0., 1., 0., 0., 0.).Build()
+           for s in GLL6_S]
+    m.AddBeamElement(ids, [BeamSection(0., COMPOSITE_MASS, COMPOSITE_STIFF),
+                           BeamSection(1., COMPOSITE_MASS, COMPOSITE_STIFF)], GAUSS7)
+    m.TranslateBeam(0, [2.0, 0., 0.])
+    m.SetBeamVelocityAboutPoint(0, [0., 0., 0., 0., 0., 0.1], [0., 0., 0.])
+    m.AddPrescribedBC(ids[0])
+    return m, StepParameters(True, 5, 0.01, 0.9)
+
+
+def rotating_beam_root_displacement(i: int, omega: float = 0.1, h: float = 0.01):
+    x0_root = [2., 0., 0.]
+    q = RotationVectorToQuaternion([0., 0., omega * h * (i + 1)])
+    xr = RotateVectorByQuaternion(q, x0_root)
+    return [xr[0] - x0_root[0], xr[1] - x0_root[1], xr[2] - x0_root[2], *q]
+
+
+def iea15_rotor_model(data: dict | None = None):
+    """tests/regression_tests/regression/test_rotor.cpp:25-65 (CreateIEA15Blades)."""
+    d = data or load_golden("iea15_rotor.json")
+    m = Model()
+    m.SetGravity(*d["gravity"])
+    node_loc = [(xi + 1.) / 2. for xi in d["node_xi"]]
+    sections = [BeamSection(s["position"], np.array(s["M_star"]).reshape(6, 6),
+                            np.array(s["C_star"]).reshape(6, 6)) for s in d["sections"]]
+    omega = d["omega"]
+    velocity = [0., 0., 0., omega[0], omega[1], omega[2]]
+    hub = [d["hub_radius"], 0., 0.]
+    nb = 3
+    for b in range(nb):
+        rq = RotationVectorToQuaternion([0., 0., -2. * math.pi * b / nb])
+        ids = [m.AddNode().SetElemLocation(node_loc[j]).SetPosition(d["node_coords"][j]).Build()
+               for j in range(len(node_loc))]
+        e = m.AddBeamElement(ids, sections, d["quadrature"])
+        m.TranslateBeam(e, hub)
+        m.RotateBeamAboutPoint(e, rq, [0., 0., 0.])
+        m.SetBeamVelocityAboutPoint(e, velocity, [0., 0., 0.])
+    bc = [m.AddPrescribedBC(be.node_ids[0]) for be in m.GetBeamElements()]
+    params = StepParameters(True, d["max_iter"], d["h"], d["rho_inf"])
+    return m, params, bc
+
+
+def iea15_hub_displacement(i: int, data: dict | None = None):
+    d = data or load_golden("iea15_rotor.json")
+    w, h = d["omega"], d["h"]
+    q = RotationVectorToQuaternion([w[0] * h * (i + 1), w[1] * h * (i + 1), w[2] * h * (i + 1)])
+    return [0., 0., 0., *q]
