@@ -1,0 +1,341 @@
+"""Benchmark of the B200 beam-step path (one JSON line on rank 0).
+
+Workload: the 4096-beam batch -- 4096 independent cantilevers, nodes U{5..21}
+(order = nodes - 1, Gauss points = nodes + 2), lengths U(5, 100) m, tapered
+seeded sections, tip loads A sin(2 pi f t) with A ~ U(1e3, 1e5) N and
+f ~ U(0.1, 5) Hz, FP64, h = 0.01 s.  One bench step = every beam advanced one
+time step (all Newton iterations to convergence or max_iter).
+
+Metric: converged beam-steps/s (non-converged beam-steps are excluded), with
+p50/p99 step latency.  `value` is measured with the loads already resident in
+HBM (device-timed with CUDA events on the library's stream); `e2e` goes
+through the public C ABI with host buffers: per step one pinned H2D of every
+beam's loads, the step, and one D2H of every node's displacement.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from openturbine_b200 import workloads as W  # noqa: E402
+
+L2_FLUSH_BYTES = 256 << 20
+
+
+def algorithmic_flops(N: int, Q: int, iters: int, f_qp: float) -> float:
+    """FLOPs of one beam for `iters` Newton iterations (per-iteration count:
+    Q*F_qp + 410 N^2 Q + 468 N^2 + 48 N Q + (2/3) n^3 + 2 n^2, n = 6N + 6)."""
+    n = 6 * N + 6
+    per = Q * f_qp + 410.0 * N * N * Q + 468.0 * N * N + 48.0 * N * Q + (2.0 / 3.0) * n ** 3 + 2.0 * n * n
+    return per * iters
+
+
+F_QP = 2500.0  # flops of the quadrature-point physics per point (frozen estimate)
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_fp64_peak(torch, device) -> float:
+    """cuBLAS FP64 GEMM (8192^3) best of 3, TFLOP/s: the FP64 roof on this GPU."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=device)
+    b = torch.randn(n, n, dtype=torch.float64, device=device)
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(3):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = max(best, 2.0 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+def cpu_baseline(draws, params, steps: int, threads: int) -> dict:
+    """The oracle (FP64 C++ port of the reference, OpenMP over beams) on a sample."""
+    from oracle.oracle_py import OracleModel, run_batch
+    models = [OracleModel(W.batch_cantilever_model(d).pack()) for d in draws]
+    conv, secs, iters = run_batch(models, params, steps, [d.amp for d in draws],
+                                  [d.freq for d in draws], threads)
+    return {"value": conv / secs, "unit": "beam-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{len(draws)} beams of the batch x {steps} steps ({secs:.1f} s)",
+            "newton_iters": iters}
+
+
+def run_reference(args) -> None:
+    """--impl reference: the reference's CPU path (the oracle port: the reference
+    itself needs Kokkos/KokkosKernels/a sparse solver, absent here) on the host
+    cores, each step a bounded sample of the batch."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle.oracle_py import OracleModel, run_batch
+    threads = os.cpu_count() or 1
+    sample = args.ref_sample
+    draws = W.draw_batch(sample)
+    models = [OracleModel(W.batch_cantilever_model(d).pack()) for d in draws]
+    params = W.batch_params()
+    amp = [d.amp for d in draws]
+    freq = [d.freq for d in draws]
+    # warm-up steps, then K timed steps; each step advances the sample one step
+    for _ in range(args.warmup):
+        run_batch(models, params, 1, amp, freq, threads)
+    total_conv, total_secs, lat = 0, 0.0, []
+    for _ in range(args.steps):
+        conv, secs, _ = run_batch(models, params, 1, amp, freq, threads)
+        total_conv += conv
+        total_secs += secs
+        lat.append(secs * 1e3)
+    value = total_conv / total_secs
+    line = {
+        "impl": "reference", "metric": "converged beam-steps/s", "value": value,
+        "unit": "beam-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_secs * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"4096-beam batch, sample of {sample} beams per step (CPU)",
+                   "beams": sample, "h": 0.01},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "cpu_baseline": {"value": value, "unit": "beam-steps/s", "cores": threads, "kind": "port",
+                         "sample": f"{sample} beams x {args.steps} steps"},
+        "e2e": {"value": value, "unit": "beam-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--beams", type=int, default=4096)
+    ap.add_argument("--ref-sample", type=int, default=512)
+    ap.add_argument("--cpu-sample", type=int, default=256)
+    ap.add_argument("--cpu-steps", type=int, default=40)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+
+    from openturbine_b200.runtime import LOAD_NODE_FX, Context
+
+    # ---- build the shard: weak scaling, each rank owns its own 4096 beams ----
+    draws = W.draw_batch(args.beams, first_id=rank * args.beams)
+    ctx = Context(local)
+    t_setup = time.perf_counter()
+    ids = np.array([ctx.create_model(W.batch_cantilever_model(d).pack()) for d in draws],
+                   dtype=np.int32)
+    t_setup = time.perf_counter() - t_setup
+    params = W.batch_params()
+    nodes = np.array([d.num_nodes for d in draws])
+    qps = nodes + 2
+    elem_nodes = int(nodes.sum())
+    tip_index = np.cumsum(nodes) - 1          # element-node row of each tip
+    total_steps = args.warmup + 2 * args.steps
+    # loads for every step (resident on the device for `value`, pinned host for e2e)
+    loads_host = torch.zeros((total_steps, elem_nodes, 6), dtype=torch.float64).pin_memory()
+    for k in range(total_steps):
+        loads_host[k, tip_index, 2] = torch.from_numpy(W.tip_loads(draws, k))
+    loads_dev = loads_host.to(dev)
+    q_host = torch.zeros((elem_nodes, 7), dtype=torch.float64).pin_memory()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    ext = torch.cuda.ExternalStream(ctx.stream_handle, device=dev)
+    fp64_peak = measured_fp64_peak(torch, dev)
+
+    def do_step(k: int, device_loads: bool):
+        if device_loads:
+            ctx.set_loads_batch(ids, LOAD_NODE_FX, loads_dev[k].data_ptr(), True)
+        else:
+            ctx.set_loads_batch(ids, LOAD_NODE_FX, loads_host[k].data_ptr(), False)
+        return ctx.step(ids, params)
+
+    # ---- warm-up (also advances the trajectory like the timed steps) ----------
+    for k in range(args.warmup):
+        do_step(k, True)
+    torch.cuda.synchronize()
+
+    # ---- value: device-resident inputs, device time per step ------------------
+    conv_v, flops_v, dev_ms = 0, 0.0, []
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = ctx.kernel_launches
+    with ClockSampler(local) as clocks:
+        for j in range(args.steps):
+            k = args.warmup + j
+            with torch.cuda.stream(ext):
+                flush.zero_()
+                s = torch.cuda.Event(enable_timing=True)
+                e = torch.cuda.Event(enable_timing=True)
+                s.record(ext)
+            st, it = do_step(k, True)
+            with torch.cuda.stream(ext):
+                e.record(ext)
+            e.synchronize()
+            dev_ms.append(s.elapsed_time(e))
+            ok = st == 0
+            conv_v += int(ok.sum())
+            flops_v += sum(algorithmic_flops(int(nodes[i]), int(qps[i]), int(it[i]), F_QP)
+                           for i in range(len(ids)))
+    torch.cuda.synchronize()
+    launches = ctx.kernel_launches - launches0
+    t_value_ms = float(sum(dev_ms))
+    if dist:
+        t = torch.tensor([t_value_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_value_ms = float(t.item())
+        c = torch.tensor([conv_v], device=dev, dtype=torch.float64)
+        dist.all_reduce(c)
+        conv_all = int(c.item())
+    else:
+        conv_all = conv_v
+    value = conv_all / (t_value_ms * 1e-3)
+
+    # ---- e2e: host buffers through the C ABI, wall time per step --------------
+    e2e_ms, conv_e = [], 0
+    for j in range(args.steps):
+        k = args.warmup + args.steps + j
+        with torch.cuda.stream(ext):
+            flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st, it = do_step(k, False)
+        ctx.get_state_batch(ids, "q", q_host.data_ptr(), False)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        conv_e += int((st == 0).sum())
+    t_e2e_ms = float(sum(e2e_ms))
+    if dist:
+        t = torch.tensor([t_e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e_ms = float(t.item())
+        c = torch.tensor([conv_e], device=dev, dtype=torch.float64)
+        dist.all_reduce(c)
+        conv_e = int(c.item())
+    e2e = conv_e / (t_e2e_ms * 1e-3)
+
+    if rank == 0:
+        achieved = flops_v / (sum(dev_ms) * 1e-3) / 1e12
+        line = {
+            "metric": "converged beam-steps/s", "value": value, "unit": "beam-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_value_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "4096-beam batch of uneven cantilevers (nodes U{5..21}, "
+                                   "Gauss nodes+2, L U(5,100) m, tip A sin(2 pi f t))",
+                       "beams_per_gpu": args.beams, "h": 0.01, "rho_inf": 0.9,
+                       "max_iter": params.max_iter, "a_tol": 1e-7, "r_tol": 1e-3,
+                       "precision": "plain FP64", "l2": "flushed (256 MB write) before each step",
+                       "parallelism": f"independent beam shards x{world}"},
+            "latency_ms": {"p50": float(np.percentile(dev_ms, 50)),
+                           "p99": float(np.percentile(dev_ms, 99)),
+                           "e2e_p50": float(np.percentile(e2e_ms, 50)),
+                           "e2e_p99": float(np.percentile(e2e_ms, 99))},
+            "converged_fraction": conv_v / (args.steps * len(ids)),
+            "e2e": {"value": e2e, "unit": "beam-steps/s",
+                    "h2d_bytes_per_step": int(elem_nodes * 6 * 8),
+                    "d2h_bytes_per_step": int(elem_nodes * 7 * 8 + 2 * 4 * len(ids))},
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak,
+                         "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": None,
+                         "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run"},
+            "gpu_launches": launches,
+            "setup_s": t_setup,
+        }
+        line["clocks"] = clocks.summary()
+        if not args.no_cpu and world == 1:
+            line["cpu_baseline"] = cpu_baseline(draws[: args.cpu_sample], params, args.cpu_steps,
+                                                os.cpu_count() or 1)
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

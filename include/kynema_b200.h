@@ -29,6 +29,12 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#if defined(__GNUC__)
+#define KYN_API __attribute__((visibility("default")))
+#else
+#define KYN_API
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -152,11 +158,14 @@ typedef struct kyn_ctx kyn_ctx;
  * model state admitted by kyn_model_create (0 = no cap).
  * Replaces the Kokkos::initialize + per-model View allocation done by
  * Model::CreateSystemWithSolver (src/model/model.hpp:647-656). */
-kyn_ctx* kyn_ctx_create(int device, size_t hbm_budget_bytes);
-void kyn_ctx_destroy(kyn_ctx* ctx);
-const char* kyn_last_error(const kyn_ctx* ctx);
+KYN_API kyn_ctx* kyn_ctx_create(int device, size_t hbm_budget_bytes);
+KYN_API void kyn_ctx_destroy(kyn_ctx* ctx);
+KYN_API const char* kyn_last_error(const kyn_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that order their own
+ * work or timing events against the library's work. */
+KYN_API void* kyn_ctx_stream(kyn_ctx* ctx);
 /* Device bytes currently held by admitted models. */
-size_t kyn_ctx_used_bytes(const kyn_ctx* ctx);
+KYN_API size_t kyn_ctx_used_bytes(const kyn_ctx* ctx);
 
 /* Replaces Model::CreateSystemWithSolver (src/model/model.hpp:647-656):
  * copies the nodes to resident state (src/model/copy_nodes_to_state.hpp),
@@ -164,36 +173,48 @@ size_t kyn_ctx_used_bytes(const kyn_ctx* ctx);
  * constraints (src/constraints/constraints.hpp:76-266), the DOF map and the
  * CRS graph (src/model/model.hpp:42-63, src/solver/create_full_matrix.hpp).
  * Returns the model id (>= 0) or a negative KYN_ERR_* code. */
-int kyn_model_create(kyn_ctx* ctx, const kyn_model_desc* desc);
-int kyn_model_destroy(kyn_ctx* ctx, int model_id);
-int kyn_model_info_get(kyn_ctx* ctx, int model_id, kyn_model_info* info);
+KYN_API int kyn_model_create(kyn_ctx* ctx, const kyn_model_desc* desc);
+KYN_API int kyn_model_destroy(kyn_ctx* ctx, int model_id);
+KYN_API int kyn_model_info_get(kyn_ctx* ctx, int model_id, kyn_model_info* info);
 
 /* Replaces writes of Beams::node_FX (tests/regression_tests/regression/
  * test_cantilever_beam.cpp:105-107) or State::f. */
-int kyn_model_set_loads(kyn_ctx* ctx, int model_id, int which, const double* values);
+KYN_API int kyn_model_set_loads(kyn_ctx* ctx, int model_id, int which, const double* values);
 
 /* Replaces Constraints::UpdateDisplacement (src/constraints/constraints.hpp:338-343). */
-int kyn_model_set_prescribed(kyn_ctx* ctx, int model_id, int constraint_id, const double u[7]);
+KYN_API int kyn_model_set_prescribed(kyn_ctx* ctx, int model_id, int constraint_id, const double u[7]);
 
 /* Replaces kynema::Step (src/step/step.hpp:42-124) for a batch of models:
  * every listed model advances one time step.  status_out[i] is KYN_OK,
  * KYN_NOT_CONVERGED or a negative code; iters_out[i] is the Newton iteration
  * count (= solver.convergence_err.size()).  Either output may be NULL. */
-int kyn_step(kyn_ctx* ctx, const int* model_ids, int n, const kyn_step_params* params,
+KYN_API int kyn_step(kyn_ctx* ctx, const int* model_ids, int n, const kyn_step_params* params,
              int* status_out, int* iters_out);
 
 /* Asynchronous form used by the serving loop: enqueue the step on the
  * context stream and return; kyn_step_wait() blocks until it is complete and
  * fills status/iterations for the models of the last kyn_step_async call. */
-int kyn_step_async(kyn_ctx* ctx, const int* model_ids, int n, const kyn_step_params* params);
-int kyn_step_wait(kyn_ctx* ctx, int* status_out, int* iters_out);
+KYN_API int kyn_step_async(kyn_ctx* ctx, const int* model_ids, int n, const kyn_step_params* params);
+KYN_API int kyn_step_wait(kyn_ctx* ctx, int* status_out, int* iters_out);
+
+/* Batched forms of kyn_model_set_loads / kyn_get_state for many models in one
+ * transfer: `values` / `out` hold the models' arrays back to back in the order
+ * of model_ids (NODE_FX: [element nodes][6]; STATE_F and node fields:
+ * [nodes][width]).  With on_device != 0 the pointer is device memory and no
+ * host copy is made; otherwise it is host memory (pinned memory is fastest).
+ * These replace the per-model Kokkos::deep_copy of node_FX / state.f before
+ * Step() and of state.q after it (src/interfaces/cfd/interface.cpp:283-309). */
+KYN_API int kyn_set_loads_batch(kyn_ctx* ctx, const int* model_ids, int n, int which,
+                                const double* values, int on_device);
+KYN_API int kyn_get_state_batch(kyn_ctx* ctx, const int* model_ids, int n, int field,
+                                double* out, int on_device);
 
 /* Replaces host reads of State / Constraints views after Step(). */
-int kyn_get_state(kyn_ctx* ctx, int model_id, int field, double* out);
+KYN_API int kyn_get_state(kyn_ctx* ctx, int model_id, int field, double* out);
 
 /* Replaces reads of solver.convergence_err (src/solver/solver.hpp:83):
  * errs must hold max_iter values; *n receives the count. */
-int kyn_get_convergence(kyn_ctx* ctx, int model_id, double* errs, int* n);
+KYN_API int kyn_get_convergence(kyn_ctx* ctx, int model_id, double* errs, int* n);
 
 /* Replaces solver.A / solver.b / solver.x reads (src/solver/solver.hpp:79-81).
  * row_ptrs [num_dofs+1] and col_inds [nnz] are the reference's CRS graph
@@ -201,13 +222,25 @@ int kyn_get_convergence(kyn_ctx* ctx, int model_id, double* errs, int* n);
  * [num_dofs] and solution [num_dofs] are the system of the last Newton
  * iteration of the last step; they are only recorded while the context
  * option KYN_OPT_RECORD_SYSTEM is set (any pointer may be NULL). */
-int kyn_get_crs(kyn_ctx* ctx, int model_id, int* row_ptrs, int* col_inds, double* values);
-int kyn_get_system_vectors(kyn_ctx* ctx, int model_id, double* rhs, double* solution);
+KYN_API int kyn_get_crs(kyn_ctx* ctx, int model_id, int* row_ptrs, int* col_inds, double* values);
+KYN_API int kyn_get_system_vectors(kyn_ctx* ctx, int model_id, double* rhs, double* solution);
 
 enum {
-    KYN_OPT_RECORD_SYSTEM = 1  /* keep the last assembled system for kyn_get_crs */
+    KYN_OPT_RECORD_SYSTEM = 1, /* keep the last assembled system for kyn_get_crs */
+    KYN_OPT_PHASE_TIMING = 2   /* count SM cycles per step-kernel phase (tracing) */
 };
-int kyn_ctx_set_option(kyn_ctx* ctx, int option, int64_t value);
+KYN_API int kyn_ctx_set_option(kyn_ctx* ctx, int option, int64_t value);
+
+/* Context counters (diagnostics; no counterpart in the reference). */
+enum {
+    KYN_STAT_KERNEL_LAUNCHES = 1,  /* kernels launched by this context so far */
+    KYN_STAT_STEP_BUCKETS = 2,     /* step-kernel launches of the last step call */
+    KYN_STAT_PHASE_CYCLES = 100    /* + phase (0..8): SM cycles summed over beams since
+                                      KYN_OPT_PHASE_TIMING was set: load/predict,
+                                      quadrature, integrate, constraints, eliminate,
+                                      factor, substitute, update, store */
+};
+KYN_API int kyn_ctx_stat(kyn_ctx* ctx, int stat, int64_t* value);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,851 @@
+// kyn_capi.cu -- C ABI of the B200 beam path (declared in include/kynema_b200.h).
+//
+// A context owns a CUDA stream, the resident state of every admitted model and
+// cached launch plans.  A step over a list of models launches the fused step
+// kernel once per bucket of beams: beams are grouped by cluster size (beams per
+// model) and by shared-memory class, and each bucket runs on its own stream so
+// the buckets share the GPU.  There is no CPU fallback: without a device every
+// entry point fails with KYN_ERR_NO_DEVICE.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/kynema_b200.h"
+#include "kyn_host.hpp"
+#include "kyn_step_kernel.cuh"
+#include "kyn_types.h"
+
+using namespace kyn;
+
+namespace {
+
+constexpr int kMaxDynSmem = 232448 - 1024;  // 227 KB per CTA on sm_100, minus static use
+constexpr int kSmemPerSM = 233472;      // 228 KB per SM
+constexpr int kBucketStreams = 8;
+
+struct DevModel {
+    HostModel host;
+    std::vector<double*> d_slab;     // per beam
+    std::vector<int> smem;           // per beam: dynamic shared memory of the step kernel
+    double* d_conv = nullptr;        // [kMaxNewtonIters]
+    double* d_dump = nullptr;        // per-beam system dumps (recording mode)
+    std::vector<size_t> dump_off;    // per beam offset into d_dump (doubles)
+    size_t bytes = 0;
+    int last_status = KYN_OK;
+    int last_iters = 0;
+};
+
+struct Bucket {
+    int cluster = 1;
+    int smem = 0;
+    int first = 0;     // first beam in the plan's beam array
+    int count = 0;     // beams
+};
+
+struct Plan {
+    std::vector<int> ids;
+    std::vector<Bucket> buckets;
+    KBeam* d_kbeams = nullptr;
+    int* d_status = nullptr;      // [nmodels]
+    int* d_iters = nullptr;
+    int* h_status = nullptr;      // pinned
+    int* h_iters = nullptr;
+    int nbeams = 0;
+    bool record = false;
+    ~Plan() {
+        if (d_kbeams) cudaFree(d_kbeams);
+        if (d_status) cudaFree(d_status);
+        if (d_iters) cudaFree(d_iters);
+        if (h_status) cudaFreeHost(h_status);
+        if (h_iters) cudaFreeHost(h_iters);
+    }
+};
+
+// One beam of a batched host<->device transfer.
+struct XferBeam {
+    double* slab_field;   // slab + field offset
+    long long ext_off;    // offset of this beam's first row in the external array
+    int map_off;          // offset into the node map
+    int N;
+};
+
+struct XferPlan {
+    std::vector<int> ids;
+    int kind = -1;        // load channel (0/1) or 100 + state field
+    int width = 0;
+    long long total = 0;  // doubles in the external array
+    XferBeam* d_beams = nullptr;
+    int* d_map = nullptr;
+    int nbeams = 0;
+    ~XferPlan() {
+        if (d_beams) cudaFree(d_beams);
+        if (d_map) cudaFree(d_map);
+    }
+};
+
+// Copies rows between the external array and the beams' slabs.
+// to_slab != 0: external -> slab (loads); else slab -> external (state read).
+__global__ void xfer_kernel(const XferBeam* __restrict__ beams, const int* __restrict__ map,
+                            double* ext, int width, int to_slab) {
+    const XferBeam b = beams[blockIdx.x];
+    const int n = b.N * width;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const int k = t / width, c = t - k * width;
+        const long long e = b.ext_off + static_cast<long long>(map[b.map_off + k]) * width + c;
+        if (to_slab) b.slab_field[t] = ext[e];
+        else ext[e] = b.slab_field[t];
+    }
+}
+
+}  // namespace
+
+struct kyn_ctx {
+    int device = 0;
+    size_t budget = 0;
+    size_t used = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t bstream[kBucketStreams] = {};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join[kBucketStreams] = {};
+    std::map<int, std::unique_ptr<DevModel>> models;
+    int next_id = 0;
+    std::string err;
+    bool record = false;
+    std::unique_ptr<Plan> plan;           // last launch plan (cache)
+    std::vector<int> pending;             // models of the last kyn_step_async
+    int smem_configured = 0;
+    double* h_stage = nullptr;            // pinned staging for loads
+    size_t h_stage_len = 0;
+    std::unique_ptr<XferPlan> xfer[4];    // cached transfer plans
+    double* d_stage = nullptr;            // device staging for batched transfers
+    size_t d_stage_len = 0;
+    int64_t launches = 0;                 // kernels launched so far
+    int64_t last_buckets = 0;
+    unsigned long long* d_prof = nullptr; // phase timing counters (KYN_OPT_PHASE_TIMING)
+};
+
+namespace {
+
+int set_err(kyn_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+#define KYN_CUDA(ctx, call)                                                              \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return set_err((ctx), KYN_ERR_CUDA,                                          \
+                           std::string(#call) + ": " + cudaGetErrorString(e_));          \
+    } while (0)
+
+DevModel* find_model(kyn_ctx* c, int id) {
+    auto it = c->models.find(id);
+    return it == c->models.end() ? nullptr : it->second.get();
+}
+
+StepCoeffs make_coeffs(const kyn_step_params* p) {
+    StepCoeffs P{};
+    const double rho = p->rho_inf;
+    P.h = p->h;
+    P.alpha_m = (2. * rho - 1.) / (rho + 1.);
+    P.alpha_f = rho / (rho + 1.);
+    P.gamma = 0.5 + P.alpha_f - P.alpha_m;
+    P.beta = 0.25 * (P.gamma + 0.5) * (P.gamma + 0.5);
+    P.dynamic = p->is_dynamic_solve ? 1 : 0;
+    P.gamma_prime = P.dynamic ? P.gamma / (P.h * P.beta) : 0.;
+    P.beta_prime = P.dynamic ? (1. - P.alpha_m) / (P.h * P.h * P.beta * (1. - P.alpha_f)) : 0.;
+    P.conditioner = P.beta * P.h * P.h;
+    P.atol = p->absolute_convergence_tol;
+    P.rtol = p->relative_convergence_tol;
+    P.max_iter = std::min<int>(p->max_iter, kMaxNewtonIters);
+    return P;
+}
+
+int beam_smem(int N, int Q, int nc, int real_bytes) { return make_smem(N, Q, nc, real_bytes).bytes; }
+
+// Resident CTAs per SM for a shared-memory size; the step kernel's register
+// budget (__launch_bounds__(kThreads, 2)) allows at most two.
+int ctas_per_sm(int smem) {
+    const int per = smem + 1024;
+    return std::max(1, std::min(2, kSmemPerSM / per));
+}
+
+// Builds (or reuses) the launch plan for this id list.
+int get_plan(kyn_ctx* c, const int* ids, int n, Plan** out) {
+    if (c->plan && c->plan->record == c->record &&
+        static_cast<int>(c->plan->ids.size()) == n &&
+        std::equal(ids, ids + n, c->plan->ids.begin())) {
+        *out = c->plan.get();
+        return KYN_OK;
+    }
+    auto plan = std::make_unique<Plan>();
+    plan->ids.assign(ids, ids + n);
+    plan->record = c->record;
+    // bucket key: (cluster size, CTAs per SM class); larger work first
+    struct Entry {
+        int model_index;
+        int cluster;
+        int cls;
+        int smem;
+        double work;
+    };
+    std::vector<Entry> entries;
+    for (int i = 0; i < n; ++i) {
+        DevModel* m = find_model(c, ids[i]);
+        if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id in step list");
+        int smem = 0;
+        double work = 0.;
+        for (size_t b = 0; b < m->host.beams.size(); ++b) {
+            smem = std::max(smem, m->smem[b]);
+            const double N = m->host.beams[b].N, Q = m->host.beams[b].Q;
+            work = std::max(work, N * N * Q + 72. * (N - 1) * (N - 1) * (N - 1));
+        }
+        entries.push_back({i, static_cast<int>(m->host.beams.size()), ctas_per_sm(smem), smem, work});
+    }
+    std::stable_sort(entries.begin(), entries.end(), [](const Entry& a, const Entry& b) {
+        if (a.cluster != b.cluster) return a.cluster > b.cluster;
+        if (a.cls != b.cls) return a.cls < b.cls;
+        return a.work > b.work;
+    });
+    std::vector<KBeam> kb;
+    for (size_t e = 0; e < entries.size(); ++e) {
+        const Entry& en = entries[e];
+        if (plan->buckets.empty() || plan->buckets.back().cluster != en.cluster ||
+            ctas_per_sm(plan->buckets.back().smem) != en.cls) {
+            Bucket bk;
+            bk.cluster = en.cluster;
+            bk.first = static_cast<int>(kb.size());
+            plan->buckets.push_back(bk);
+        }
+        Bucket& bk = plan->buckets.back();
+        bk.smem = std::max(bk.smem, en.smem);
+        DevModel* m = find_model(c, ids[en.model_index]);
+        int model_dofs = m->host.ndofs;
+        for (size_t b = 0; b < m->host.beams.size(); ++b) {
+            const HostBeam& hb = m->host.beams[b];
+            KBeam k{};
+            k.slab = m->d_slab[b];
+            k.N = hb.N;
+            k.Q = hb.Q;
+            k.nc = hb.nc;
+            k.plan_model = en.model_index;
+            k.rank = static_cast<int>(b);
+            k.model_beams = static_cast<int>(m->host.beams.size());
+            k.model_dofs = model_dofs;
+            for (int s = 0; s < kMaxBeamConstraints; ++s) {
+                k.con_node[s] = hb.con_node[s];
+                k.con_type[s] = hb.con_type[s];
+                k.con_row[s] = hb.con_row[s];
+                for (int d = 0; d < 3; ++d) k.con_X0[s][d] = hb.con_X0[s][d];
+            }
+            for (int d = 0; d < 3; ++d) k.gravity[d] = m->host.gravity[d];
+            k.conv = m->d_conv;
+            k.dump = (c->record && m->d_dump) ? m->d_dump + m->dump_off[b] : nullptr;
+            k.prof = c->d_prof;
+            kb.push_back(k);
+            bk.count++;
+        }
+    }
+    plan->nbeams = static_cast<int>(kb.size());
+    KYN_CUDA(c, cudaMalloc(&plan->d_kbeams, sizeof(KBeam) * std::max<size_t>(1, kb.size())));
+    KYN_CUDA(c, cudaMemcpyAsync(plan->d_kbeams, kb.data(), sizeof(KBeam) * kb.size(),
+                                cudaMemcpyHostToDevice, c->stream));
+    KYN_CUDA(c, cudaMalloc(&plan->d_status, sizeof(int) * std::max(1, n)));
+    KYN_CUDA(c, cudaMalloc(&plan->d_iters, sizeof(int) * std::max(1, n)));
+    KYN_CUDA(c, cudaMallocHost(&plan->h_status, sizeof(int) * std::max(1, n)));
+    KYN_CUDA(c, cudaMallocHost(&plan->h_iters, sizeof(int) * std::max(1, n)));
+    KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->plan = std::move(plan);
+    *out = c->plan.get();
+    return KYN_OK;
+}
+
+int launch_plan(kyn_ctx* c, Plan* plan, const kyn_step_params* p) {
+    const StepCoeffs P = make_coeffs(p);
+    if (c->smem_configured < kMaxDynSmem) {
+        KYN_CUDA(c, cudaFuncSetAttribute(step_kernel<double>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
+        c->smem_configured = kMaxDynSmem;
+    }
+    KYN_CUDA(c, cudaEventRecord(c->fork, c->stream));
+    const int nb = static_cast<int>(plan->buckets.size());
+    for (int b = 0; b < nb; ++b) {
+        const Bucket& bk = plan->buckets[b];
+        cudaStream_t s = c->bstream[b % kBucketStreams];
+        KYN_CUDA(c, cudaStreamWaitEvent(s, c->fork, 0));
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(bk.count, 1, 1);
+        cfg.blockDim = dim3(kThreads, 1, 1);
+        cfg.dynamicSmemBytes = bk.smem;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        if (bk.cluster > 1) {
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = bk.cluster;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+        }
+        const KBeam* beams = plan->d_kbeams + bk.first;
+        KYN_CUDA(c, cudaLaunchKernelEx(&cfg, step_kernel<double>, beams, P,
+                                       plan->record ? 1 : 0, plan->d_status, plan->d_iters));
+        c->launches++;
+    }
+    c->last_buckets = nb;
+    for (int b = 0; b < std::min(nb, kBucketStreams); ++b) {
+        KYN_CUDA(c, cudaEventRecord(c->join[b], c->bstream[b]));
+        KYN_CUDA(c, cudaStreamWaitEvent(c->stream, c->join[b], 0));
+    }
+    const int n = static_cast<int>(plan->ids.size());
+    KYN_CUDA(c, cudaMemcpyAsync(plan->h_status, plan->d_status, sizeof(int) * n,
+                                cudaMemcpyDeviceToHost, c->stream));
+    KYN_CUDA(c, cudaMemcpyAsync(plan->h_iters, plan->d_iters, sizeof(int) * n,
+                                cudaMemcpyDeviceToHost, c->stream));
+    return KYN_OK;
+}
+
+int finish_plan(kyn_ctx* c, Plan* plan, int* status_out, int* iters_out) {
+    KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+    const int n = static_cast<int>(plan->ids.size());
+    for (int i = 0; i < n; ++i) {
+        DevModel* m = find_model(c, plan->ids[i]);
+        if (m) {
+            m->last_status = plan->h_status[i];
+            m->last_iters = plan->h_iters[i];
+        }
+        if (status_out) status_out[i] = plan->h_status[i];
+        if (iters_out) iters_out[i] = plan->h_iters[i];
+    }
+    return KYN_OK;
+}
+
+int field_slot(int field, const SlabLayout& L, int* width) {
+    switch (field) {
+        case KYN_FIELD_X0: *width = 7; return L.x0;
+        case KYN_FIELD_X: *width = 7; return L.x;
+        case KYN_FIELD_Q: *width = 7; return L.q;
+        case KYN_FIELD_Q_PREV: *width = 7; return L.q_prev;
+        case KYN_FIELD_Q_DELTA: *width = 6; return L.q_delta;
+        case KYN_FIELD_V: *width = 6; return L.v;
+        case KYN_FIELD_VD: *width = 6; return L.vd;
+        case KYN_FIELD_A: *width = 6; return L.a;
+        case KYN_FIELD_F: *width = 6; return L.f;
+        default: return -1;
+    }
+}
+
+// kind: KYN_LOAD_NODE_FX (0), KYN_LOAD_STATE_F (1), or 100 + node field.
+int get_xfer(kyn_ctx* c, const int* ids, int n, int kind, XferPlan** out) {
+    const int slot = (kind == KYN_LOAD_NODE_FX) ? 0 : (kind == KYN_LOAD_STATE_F) ? 1
+                                                     : (kind == 100 + KYN_FIELD_Q) ? 2 : 3;
+    auto& cached = c->xfer[slot];
+    if (cached && cached->kind == kind && static_cast<int>(cached->ids.size()) == n &&
+        std::equal(ids, ids + n, cached->ids.begin())) {
+        *out = cached.get();
+        return KYN_OK;
+    }
+    auto xp = std::make_unique<XferPlan>();
+    xp->ids.assign(ids, ids + n);
+    xp->kind = kind;
+    std::vector<XferBeam> beams;
+    std::vector<int> map;
+    long long off = 0;
+    for (int i = 0; i < n; ++i) {
+        DevModel* m = find_model(c, ids[i]);
+        if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id in batch");
+        long long elem = 0;
+        for (size_t bi = 0; bi < m->host.beams.size(); ++bi) {
+            const HostBeam& b = m->host.beams[bi];
+            const SlabLayout L = make_slab_layout(b.N, b.Q);
+            XferBeam xb{};
+            xb.N = b.N;
+            xb.map_off = static_cast<int>(map.size());
+            int width = 6, fo;
+            if (kind == KYN_LOAD_NODE_FX) {
+                fo = L.fx;
+                xb.ext_off = off + elem * 6;
+                for (int k = 0; k < b.N; ++k) map.push_back(k);
+            } else {
+                fo = (kind == KYN_LOAD_STATE_F) ? L.f : field_slot(kind - 100, L, &width);
+                if (fo < 0) return set_err(c, KYN_ERR_INVALID, "field not available in batch form");
+                xb.ext_off = off;
+                for (int k = 0; k < b.N; ++k) map.push_back(b.node_ids[k]);
+            }
+            xp->width = width;
+            xb.slab_field = m->d_slab[bi] + fo;
+            beams.push_back(xb);
+            elem += b.N;
+        }
+        off += (kind == KYN_LOAD_NODE_FX) ? elem * 6 : static_cast<long long>(m->host.num_nodes) * xp->width;
+    }
+    if (xp->width == 0) xp->width = 6;
+    xp->total = off;
+    xp->nbeams = static_cast<int>(beams.size());
+    KYN_CUDA(c, cudaMalloc(&xp->d_beams, sizeof(XferBeam) * std::max<size_t>(1, beams.size())));
+    KYN_CUDA(c, cudaMalloc(&xp->d_map, sizeof(int) * std::max<size_t>(1, map.size())));
+    KYN_CUDA(c, cudaMemcpyAsync(xp->d_beams, beams.data(), sizeof(XferBeam) * beams.size(),
+                                cudaMemcpyHostToDevice, c->stream));
+    KYN_CUDA(c, cudaMemcpyAsync(xp->d_map, map.data(), sizeof(int) * map.size(),
+                                cudaMemcpyHostToDevice, c->stream));
+    KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+    cached = std::move(xp);
+    *out = cached.get();
+    return KYN_OK;
+}
+
+int ensure_stage(kyn_ctx* c, long long doubles) {
+    if (c->d_stage_len >= static_cast<size_t>(doubles)) return KYN_OK;
+    if (c->d_stage) {
+        KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+        cudaFree(c->d_stage);
+        c->d_stage = nullptr;
+    }
+    KYN_CUDA(c, cudaMalloc(&c->d_stage, sizeof(double) * std::max<long long>(1, doubles)));
+    c->d_stage_len = static_cast<size_t>(std::max<long long>(1, doubles));
+    return KYN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+kyn_ctx* kyn_ctx_create(int device, size_t hbm_budget_bytes) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= device || device < 0) return nullptr;
+    if (cudaSetDevice(device) != cudaSuccess) return nullptr;
+    auto* c = new kyn_ctx();
+    c->device = device;
+    c->budget = hbm_budget_bytes;
+    bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess;
+    for (int i = 0; i < kBucketStreams && ok; ++i) {
+        ok = cudaStreamCreateWithFlags(&c->bstream[i], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming) == cudaSuccess;
+    }
+    ok = ok && cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+        kyn_ctx_destroy(c);
+        return nullptr;
+    }
+    return c;
+}
+
+void kyn_ctx_destroy(kyn_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    c->plan.reset();
+    for (auto& kv : c->models) {
+        for (double* p : kv.second->d_slab) cudaFree(p);
+        if (kv.second->d_conv) cudaFree(kv.second->d_conv);
+        if (kv.second->d_dump) cudaFree(kv.second->d_dump);
+    }
+    c->models.clear();
+    if (c->h_stage) cudaFreeHost(c->h_stage);
+    for (auto& x : c->xfer) x.reset();
+    if (c->d_stage) cudaFree(c->d_stage);
+    for (int i = 0; i < kBucketStreams; ++i) {
+        if (c->bstream[i]) cudaStreamDestroy(c->bstream[i]);
+        if (c->join[i]) cudaEventDestroy(c->join[i]);
+    }
+    if (c->fork) cudaEventDestroy(c->fork);
+    if (c->d_prof) cudaFree(c->d_prof);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char* kyn_last_error(const kyn_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+size_t kyn_ctx_used_bytes(const kyn_ctx* c) { return c ? c->used : 0; }
+
+void* kyn_ctx_stream(kyn_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
+int kyn_ctx_stat(kyn_ctx* c, int stat, int64_t* value) {
+    if (!c || !value) return KYN_ERR_INVALID;
+    if (stat == KYN_STAT_KERNEL_LAUNCHES) *value = c->launches;
+    else if (stat == KYN_STAT_STEP_BUCKETS) *value = c->last_buckets;
+    else if (stat >= KYN_STAT_PHASE_CYCLES && stat < KYN_STAT_PHASE_CYCLES + kNumPhases) {
+        if (!c->d_prof) return set_err(c, KYN_ERR_INVALID, "KYN_OPT_PHASE_TIMING is not set");
+        unsigned long long v = 0;
+        KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+        KYN_CUDA(c, cudaMemcpy(&v, c->d_prof + (stat - KYN_STAT_PHASE_CYCLES), sizeof(v),
+                               cudaMemcpyDeviceToHost));
+        *value = static_cast<int64_t>(v);
+    } else return set_err(c, KYN_ERR_INVALID, "unknown statistic");
+    return KYN_OK;
+}
+
+int kyn_ctx_set_option(kyn_ctx* c, int option, int64_t value) {
+    if (!c) return KYN_ERR_INVALID;
+    if (option == KYN_OPT_RECORD_SYSTEM) {
+        c->record = value != 0;
+        if (c->record) {
+            for (auto& kv : c->models) {
+                DevModel* m = kv.second.get();
+                if (m->d_dump) continue;
+                size_t tot = 0;
+                m->dump_off.clear();
+                for (auto& b : m->host.beams) {
+                    const size_t nl = 6 * b.N + 6 * b.nc;
+                    m->dump_off.push_back(tot);
+                    tot += nl * nl + 2 * nl;
+                }
+                KYN_CUDA(c, cudaMalloc(&m->d_dump, tot * sizeof(double)));
+                KYN_CUDA(c, cudaMemset(m->d_dump, 0, tot * sizeof(double)));
+            }
+        }
+        c->plan.reset();
+        return KYN_OK;
+    }
+    if (option == KYN_OPT_PHASE_TIMING) {
+        KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+        if (value && !c->d_prof) {
+            KYN_CUDA(c, cudaMalloc(&c->d_prof, 16 * sizeof(unsigned long long)));
+        }
+        if (c->d_prof) KYN_CUDA(c, cudaMemset(c->d_prof, 0, 16 * sizeof(unsigned long long)));
+        if (!value && c->d_prof) {
+            cudaFree(c->d_prof);
+            c->d_prof = nullptr;
+        }
+        c->plan.reset();
+        return KYN_OK;
+    }
+    return set_err(c, KYN_ERR_INVALID, "unknown option");
+}
+
+int kyn_model_create(kyn_ctx* c, const kyn_model_desc* desc) {
+    if (!c) return KYN_ERR_INVALID;
+    cudaSetDevice(c->device);
+    auto m = std::make_unique<DevModel>();
+    std::string err;
+    const int rc = build_host_model(desc, m->host, err);
+    if (rc != KYN_OK) return set_err(c, rc, err);
+    size_t bytes = kMaxNewtonIters * sizeof(double);
+    for (auto& b : m->host.beams) {
+        const int sm = beam_smem(b.N, b.Q, b.nc, sizeof(double));
+        if (sm > kMaxDynSmem)
+            return set_err(c, KYN_ERR_UNSUPPORTED, "beam system does not fit in shared memory");
+        m->smem.push_back(sm);
+        bytes += b.slab.size() * sizeof(double);
+    }
+    if (c->budget && c->used + bytes > c->budget)
+        return set_err(c, KYN_ERR_BUDGET, "HBM budget exceeded");
+    for (auto& b : m->host.beams) {
+        double* p = nullptr;
+        KYN_CUDA(c, cudaMallocAsync(&p, b.slab.size() * sizeof(double), c->stream));
+        KYN_CUDA(c, cudaMemcpyAsync(p, b.slab.data(), b.slab.size() * sizeof(double),
+                                    cudaMemcpyHostToDevice, c->stream));
+        m->d_slab.push_back(p);
+    }
+    KYN_CUDA(c, cudaMallocAsync(&m->d_conv, kMaxNewtonIters * sizeof(double), c->stream));
+    KYN_CUDA(c, cudaMemsetAsync(m->d_conv, 0, kMaxNewtonIters * sizeof(double), c->stream));
+    if (c->record) {
+        size_t tot = 0;
+        for (auto& b : m->host.beams) {
+            const size_t nl = 6 * b.N + 6 * b.nc;
+            m->dump_off.push_back(tot);
+            tot += nl * nl + 2 * nl;
+        }
+        KYN_CUDA(c, cudaMallocAsync(&m->d_dump, tot * sizeof(double), c->stream));
+        KYN_CUDA(c, cudaMemsetAsync(m->d_dump, 0, tot * sizeof(double), c->stream));
+    }
+    KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+    m->bytes = bytes;
+    c->used += bytes;
+    const int id = c->next_id++;
+    c->models[id] = std::move(m);
+    return id;
+}
+
+int kyn_model_destroy(kyn_ctx* c, int id) {
+    if (!c) return KYN_ERR_INVALID;
+    DevModel* m = find_model(c, id);
+    if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
+    KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (double* p : m->d_slab) KYN_CUDA(c, cudaFreeAsync(p, c->stream));
+    if (m->d_conv) KYN_CUDA(c, cudaFreeAsync(m->d_conv, c->stream));
+    if (m->d_dump) KYN_CUDA(c, cudaFreeAsync(m->d_dump, c->stream));
+    c->used -= m->bytes;
+    c->models.erase(id);
+    if (c->plan && std::find(c->plan->ids.begin(), c->plan->ids.end(), id) != c->plan->ids.end())
+        c->plan.reset();
+    return KYN_OK;
+}
+
+int kyn_model_info_get(kyn_ctx* c, int id, kyn_model_info* info) {
+    if (!c || !info) return KYN_ERR_INVALID;
+    DevModel* m = find_model(c, id);
+    if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
+    info->num_nodes = m->host.num_nodes;
+    info->num_beams = static_cast<int32_t>(m->host.beams.size());
+    info->num_constraints = m->host.num_constraints;
+    info->num_system_dofs = m->host.nsys;
+    info->num_dofs = m->host.ndofs;
+    info->nnz = static_cast<int32_t>(m->host.col_inds.size());
+    int mn = 0, mq = 0;
+    for (auto& b : m->host.beams) {
+        mn = std::max(mn, b.N);
+        mq = std::max(mq, b.Q);
+    }
+    info->max_beam_nodes = mn;
+    info->max_beam_qps = mq;
+    info->device_bytes = static_cast<int64_t>(m->bytes);
+    return KYN_OK;
+}
+
+int kyn_model_set_loads(kyn_ctx* c, int id, int which, const double* values) {
+    if (!c || !values) return KYN_ERR_INVALID;
+    DevModel* m = find_model(c, id);
+    if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
+    if (which != KYN_LOAD_NODE_FX && which != KYN_LOAD_STATE_F)
+        return set_err(c, KYN_ERR_INVALID, "unknown load channel");
+    // Stage in pinned memory in beam-local order, then one copy per beam.
+    size_t need = 0;
+    for (auto& b : m->host.beams) need += 6 * b.N;
+    if (c->h_stage_len < need) {
+        if (c->h_stage) {
+            KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+            cudaFreeHost(c->h_stage);
+        }
+        KYN_CUDA(c, cudaMallocHost(&c->h_stage, need * sizeof(double)));
+        c->h_stage_len = need;
+    }
+    KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+    size_t off = 0, elem = 0;
+    for (size_t bi = 0; bi < m->host.beams.size(); ++bi) {
+        const HostBeam& b = m->host.beams[bi];
+        const SlabLayout L = make_slab_layout(b.N, b.Q);
+        for (int k = 0; k < b.N; ++k)
+            for (int cc = 0; cc < 6; ++cc)
+                c->h_stage[off + k * 6 + cc] = (which == KYN_LOAD_NODE_FX)
+                                                   ? values[(elem + k) * 6 + cc]
+                                                   : values[b.node_ids[k] * 6 + cc];
+        KYN_CUDA(c, cudaMemcpyAsync(m->d_slab[bi] + (which == KYN_LOAD_NODE_FX ? L.fx : L.f),
+                                    c->h_stage + off, 6 * b.N * sizeof(double),
+                                    cudaMemcpyHostToDevice, c->stream));
+        off += 6 * b.N;
+        elem += b.N;
+    }
+    KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KYN_OK;
+}
+
+int kyn_model_set_prescribed(kyn_ctx* c, int id, int cid, const double u[7]) {
+    if (!c || !u) return KYN_ERR_INVALID;
+    DevModel* m = find_model(c, id);
+    if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
+    if (cid < 0 || cid >= m->host.num_constraints)
+        return set_err(c, KYN_ERR_INVALID, "constraint id out of range");
+    const int bi = m->host.con_beam[cid], slot = m->host.con_slot[cid];
+    const HostBeam& b = m->host.beams[bi];
+    const SlabLayout L = make_slab_layout(b.N, b.Q);
+    KYN_CUDA(c, cudaMemcpyAsync(m->d_slab[bi] + L.con_input + slot * 7, u, 7 * sizeof(double),
+                                cudaMemcpyHostToDevice, c->stream));
+    KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KYN_OK;
+}
+
+int kyn_step(kyn_ctx* c, const int* ids, int n, const kyn_step_params* p, int* status_out,
+             int* iters_out) {
+    int rc = kyn_step_async(c, ids, n, p);
+    if (rc != KYN_OK) return rc;
+    return kyn_step_wait(c, status_out, iters_out);
+}
+
+int kyn_step_async(kyn_ctx* c, const int* ids, int n, const kyn_step_params* p) {
+    if (!c || !p || n < 0 || (n > 0 && !ids)) return KYN_ERR_INVALID;
+    if (p->max_iter < 1 || !(p->h > 0.)) return set_err(c, KYN_ERR_INVALID, "bad step parameters");
+    if (p->precision != KYN_PRECISION_FP64)
+        return set_err(c, KYN_ERR_UNSUPPORTED, "precision mode not available in this build");
+    cudaSetDevice(c->device);
+    c->pending.assign(ids, ids + n);
+    if (n == 0) return KYN_OK;
+    Plan* plan = nullptr;
+    int rc = get_plan(c, ids, n, &plan);
+    if (rc != KYN_OK) return rc;
+    return launch_plan(c, plan, p);
+}
+
+int kyn_step_wait(kyn_ctx* c, int* status_out, int* iters_out) {
+    if (!c) return KYN_ERR_INVALID;
+    if (c->pending.empty()) return KYN_OK;
+    if (!c->plan) return set_err(c, KYN_ERR_INVALID, "no step in flight");
+    return finish_plan(c, c->plan.get(), status_out, iters_out);
+}
+
+int kyn_get_state(kyn_ctx* c, int id, int field, double* out) {
+    if (!c || !out) return KYN_ERR_INVALID;
+    DevModel* m = find_model(c, id);
+    if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
+    KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (size_t bi = 0; bi < m->host.beams.size(); ++bi) {
+        const HostBeam& b = m->host.beams[bi];
+        const SlabLayout L = make_slab_layout(b.N, b.Q);
+        std::vector<double> h(L.total);
+        KYN_CUDA(c, cudaMemcpy(h.data(), m->d_slab[bi], L.total * sizeof(double),
+                               cudaMemcpyDeviceToHost));
+        if (field == KYN_FIELD_LAMBDA) {
+            for (int s = 0; s < b.nc; ++s)
+                for (int k = 0; k < 6; ++k) out[b.con_row[s] * 6 + k] = h[L.lambda + s * 6 + k];
+            continue;
+        }
+        int src = -1, w = 0;
+        switch (field) {
+            case KYN_FIELD_X0: src = L.x0; w = 7; break;
+            case KYN_FIELD_X: src = L.x; w = 7; break;
+            case KYN_FIELD_Q: src = L.q; w = 7; break;
+            case KYN_FIELD_Q_PREV: src = L.q_prev; w = 7; break;
+            case KYN_FIELD_Q_DELTA: src = L.q_delta; w = 6; break;
+            case KYN_FIELD_V: src = L.v; w = 6; break;
+            case KYN_FIELD_VD: src = L.vd; w = 6; break;
+            case KYN_FIELD_A: src = L.a; w = 6; break;
+            case KYN_FIELD_F: src = L.f; w = 6; break;
+            case KYN_FIELD_TANGENT: src = L.tangent; w = 36; break;
+            default: return set_err(c, KYN_ERR_INVALID, "unknown state field");
+        }
+        for (int k = 0; k < b.N; ++k) {
+            double* o = out + static_cast<size_t>(b.node_ids[k]) * w;
+            if (field == KYN_FIELD_TANGENT) {
+                for (int e = 0; e < 36; ++e) o[e] = 0.;
+                for (int d = 0; d < 3; ++d) o[d * 7] = 1.;
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) o[(3 + i) * 6 + 3 + j] = h[src + k * 9 + i * 3 + j];
+            } else {
+                for (int e = 0; e < w; ++e) o[e] = h[src + k * w + e];
+            }
+        }
+    }
+    return KYN_OK;
+}
+
+int kyn_get_convergence(kyn_ctx* c, int id, double* errs, int* n) {
+    if (!c) return KYN_ERR_INVALID;
+    DevModel* m = find_model(c, id);
+    if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
+    KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+    const int cnt = std::min(m->last_iters, kMaxNewtonIters);
+    if (errs && cnt > 0)
+        KYN_CUDA(c, cudaMemcpy(errs, m->d_conv, cnt * sizeof(double), cudaMemcpyDeviceToHost));
+    if (n) *n = cnt;
+    return KYN_OK;
+}
+
+int kyn_get_crs(kyn_ctx* c, int id, int* row_ptrs, int* col_inds, double* values) {
+    if (!c) return KYN_ERR_INVALID;
+    DevModel* m = find_model(c, id);
+    if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
+    const HostModel& H = m->host;
+    if (row_ptrs) std::copy(H.row_ptrs.begin(), H.row_ptrs.end(), row_ptrs);
+    if (col_inds) std::copy(H.col_inds.begin(), H.col_inds.end(), col_inds);
+    if (!values) return KYN_OK;
+    if (!m->d_dump) return set_err(c, KYN_ERR_INVALID, "KYN_OPT_RECORD_SYSTEM was not set");
+    KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+    std::fill(values, values + H.col_inds.size(), 0.);
+    for (size_t bi = 0; bi < H.beams.size(); ++bi) {
+        const HostBeam& b = H.beams[bi];
+        const int nl = 6 * b.N + 6 * b.nc;
+        std::vector<double> D(static_cast<size_t>(nl) * nl);
+        KYN_CUDA(c, cudaMemcpy(D.data(), m->d_dump + m->dump_off[bi], D.size() * sizeof(double),
+                               cudaMemcpyDeviceToHost));
+        auto gdof = [&](int l) {
+            if (l < 6 * b.N) return H.fmap[b.node_ids[l / 6]] + l % 6;
+            const int s = (l - 6 * b.N) / 6;
+            return H.nsys + 6 * b.con_row[s] + (l - 6 * b.N) % 6;
+        };
+        for (int r = 0; r < nl; ++r) {
+            const int gr = gdof(r);
+            const int* beg = H.col_inds.data() + H.row_ptrs[gr];
+            const int* end = H.col_inds.data() + H.row_ptrs[gr + 1];
+            for (int cc = 0; cc < nl; ++cc) {
+                const double v = D[static_cast<size_t>(r) * nl + cc];
+                if (v == 0.) continue;
+                const int gc = gdof(cc);
+                const int* p = std::lower_bound(beg, end, gc);
+                if (p != end && *p == gc) values[p - H.col_inds.data()] = v;
+            }
+        }
+    }
+    return KYN_OK;
+}
+
+int kyn_get_system_vectors(kyn_ctx* c, int id, double* rhs, double* solution) {
+    if (!c) return KYN_ERR_INVALID;
+    DevModel* m = find_model(c, id);
+    if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
+    if (!m->d_dump) return set_err(c, KYN_ERR_INVALID, "KYN_OPT_RECORD_SYSTEM was not set");
+    KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+    const HostModel& H = m->host;
+    for (size_t bi = 0; bi < H.beams.size(); ++bi) {
+        const HostBeam& b = H.beams[bi];
+        const int nl = 6 * b.N + 6 * b.nc;
+        std::vector<double> V(2 * nl);
+        KYN_CUDA(c, cudaMemcpy(V.data(), m->d_dump + m->dump_off[bi] + static_cast<size_t>(nl) * nl,
+                               V.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int l = 0; l < nl; ++l) {
+            int g;
+            if (l < 6 * b.N) g = H.fmap[b.node_ids[l / 6]] + l % 6;
+            else g = H.nsys + 6 * b.con_row[(l - 6 * b.N) / 6] + (l - 6 * b.N) % 6;
+            if (rhs) rhs[g] = V[l];
+            if (solution) solution[g] = V[nl + l];
+        }
+    }
+    return KYN_OK;
+}
+
+int kyn_set_loads_batch(kyn_ctx* c, const int* ids, int n, int which, const double* values,
+                        int on_device) {
+    if (!c || n < 0 || (n > 0 && (!ids || !values))) return KYN_ERR_INVALID;
+    if (which != KYN_LOAD_NODE_FX && which != KYN_LOAD_STATE_F)
+        return set_err(c, KYN_ERR_INVALID, "unknown load channel");
+    if (n == 0) return KYN_OK;
+    cudaSetDevice(c->device);
+    XferPlan* xp = nullptr;
+    int rc = get_xfer(c, ids, n, which, &xp);
+    if (rc != KYN_OK) return rc;
+    const double* src = values;
+    if (!on_device) {
+        rc = ensure_stage(c, xp->total);
+        if (rc != KYN_OK) return rc;
+        KYN_CUDA(c, cudaMemcpyAsync(c->d_stage, values, sizeof(double) * xp->total,
+                                    cudaMemcpyHostToDevice, c->stream));
+        src = c->d_stage;
+    }
+    xfer_kernel<<<xp->nbeams, 128, 0, c->stream>>>(xp->d_beams, xp->d_map,
+                                                   const_cast<double*>(src), 6, 1);
+    KYN_CUDA(c, cudaGetLastError());
+    c->launches++;
+    return KYN_OK;
+}
+
+int kyn_get_state_batch(kyn_ctx* c, const int* ids, int n, int field, double* out, int on_device) {
+    if (!c || n < 0 || (n > 0 && (!ids || !out))) return KYN_ERR_INVALID;
+    if (n == 0) return KYN_OK;
+    cudaSetDevice(c->device);
+    XferPlan* xp = nullptr;
+    int rc = get_xfer(c, ids, n, 100 + field, &xp);
+    if (rc != KYN_OK) return rc;
+    double* dst = out;
+    if (!on_device) {
+        rc = ensure_stage(c, xp->total);
+        if (rc != KYN_OK) return rc;
+        dst = c->d_stage;
+    }
+    xfer_kernel<<<xp->nbeams, 128, 0, c->stream>>>(xp->d_beams, xp->d_map, dst, xp->width, 0);
+    KYN_CUDA(c, cudaGetLastError());
+    c->launches++;
+    if (!on_device) {
+        KYN_CUDA(c, cudaMemcpyAsync(out, c->d_stage, sizeof(double) * xp->total,
+                                    cudaMemcpyDeviceToHost, c->stream));
+        KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    return KYN_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,260 @@
+// kyn_host.cpp -- host-side model setup for the B200 beam path (see kyn_host.hpp).
+#include "kyn_host.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+
+namespace kyn {
+
+namespace {
+
+// Hamilton product and rotation of a vector (src/math/quaternion_operations.hpp).
+void qmul(const double* a, const double* b, double* o) {
+    o[0] = a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3];
+    o[1] = a[0] * b[1] + a[1] * b[0] + a[2] * b[3] - a[3] * b[2];
+    o[2] = a[0] * b[2] - a[1] * b[3] + a[2] * b[0] + a[3] * b[1];
+    o[3] = a[0] * b[3] + a[1] * b[2] - a[2] * b[1] + a[3] * b[0];
+}
+
+int fail(std::string& err, int code, const char* msg) {
+    err = msg;
+    return code;
+}
+
+}  // namespace
+
+void lagrange_basis(double x, const std::vector<double>& xs, std::vector<double>& val,
+                    std::vector<double>& der) {
+    // l_i(x) = prod_{m != i} (x - x_m) / (x_i - x_m)
+    // l_i'(x) = sum_{j != i} 1/(x_i - x_j) prod_{k != i,j} (x - x_k)/(x_i - x_k)
+    // (src/math/interpolation.hpp LagrangePolynomial{Interp,Deriv}Weights)
+    const size_t n = xs.size();
+    val.assign(n, 1.);
+    der.assign(n, 0.);
+    for (size_t i = 0; i < n; ++i) {
+        for (size_t m = 0; m < n; ++m)
+            if (m != i) val[i] *= (x - xs[m]) / (xs[i] - xs[m]);
+        double d = 0.;
+        for (size_t j = 0; j < n; ++j) {
+            if (j == i) continue;
+            double p = 1.;
+            for (size_t k = 0; k < n; ++k)
+                if (k != i && k != j) p *= (x - xs[k]) / (xs[i] - xs[k]);
+            d += p / (xs[i] - xs[j]);
+        }
+        der[i] = d;
+    }
+}
+
+int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
+    if (!d) return fail(err, KYN_ERR_INVALID, "null model description");
+    if (d->num_nodes <= 0 || !d->node_x0 || !d->node_s)
+        return fail(err, KYN_ERR_INVALID, "model needs nodes with x0 and s");
+    if (d->num_beams <= 0 || !d->beam_node_offsets || !d->beam_node_ids ||
+        !d->beam_section_offsets || !d->beam_qp_offsets || !d->section_position ||
+        !d->section_mass || !d->section_stiffness || !d->qp_xi || !d->qp_weight)
+        return fail(err, KYN_ERR_INVALID, "model needs at least one fully described beam");
+    if (d->num_beams > kMaxClusterBeams)
+        return fail(err, KYN_ERR_UNSUPPORTED, "more than 8 beam elements in one model");
+    const int nn = d->num_nodes;
+    M.num_nodes = nn;
+    M.num_constraints = d->num_constraints;
+    for (int c = 0; c < 3; ++c) M.gravity[c] = d->gravity[c];
+    M.node_beam.assign(nn, -1);
+    M.node_local.assign(nn, -1);
+    M.beams.resize(d->num_beams);
+
+    for (int e = 0; e < d->num_beams; ++e) {
+        HostBeam& B = M.beams[e];
+        const int n0 = d->beam_node_offsets[e], n1 = d->beam_node_offsets[e + 1];
+        const int s0 = d->beam_section_offsets[e], s1 = d->beam_section_offsets[e + 1];
+        const int q0 = d->beam_qp_offsets[e], q1 = d->beam_qp_offsets[e + 1];
+        B.N = n1 - n0;
+        B.Q = q1 - q0;
+        if (B.N < 2 || B.Q < 1 || s1 - s0 < 1)
+            return fail(err, KYN_ERR_INVALID, "beam needs >= 2 nodes, >= 1 qp, >= 1 section");
+        if (B.N > 32 || B.Q > 64)
+            return fail(err, KYN_ERR_UNSUPPORTED, "beam larger than 32 nodes or 64 qps");
+        for (int s = s0 + 1; s < s1; ++s)
+            if (!(d->section_position[s] > d->section_position[s - 1]))
+                return fail(err, KYN_ERR_INVALID, "section positions must increase");
+        B.node_ids.assign(d->beam_node_ids + n0, d->beam_node_ids + n1);
+        for (int k = 0; k < B.N; ++k) {
+            const int id = B.node_ids[k];
+            if (id < 0 || id >= nn) return fail(err, KYN_ERR_INVALID, "beam node id out of range");
+            if (M.node_beam[id] != -1)
+                return fail(err, KYN_ERR_UNSUPPORTED,
+                            "node shared between beam elements (multi-element beams)");
+            M.node_beam[id] = e;
+            M.node_local[id] = k;
+        }
+        const int N = B.N, Q = B.Q;
+        const SlabLayout L = make_slab_layout(N, Q);
+        B.slab.assign(L.total, 0.);
+        double* S = B.slab.data();
+
+        // shape functions on node locations xi = 2 s - 1 (populate_element_views.hpp:45-78)
+        std::vector<double> node_xi(N), val, der;
+        for (int k = 0; k < N; ++k) node_xi[k] = 2. * d->node_s[B.node_ids[k]] - 1.;
+        for (int a = 0; a < N; ++a)
+            for (int b = a + 1; b < N; ++b)
+                if (node_xi[a] == node_xi[b])
+                    return fail(err, KYN_ERR_INVALID, "two beam nodes share an element location");
+        std::vector<double> sec_xi(s1 - s0);
+        for (int s = s0; s < s1; ++s) sec_xi[s - s0] = 2. * d->section_position[s] - 1.;
+        for (int q = 0; q < Q; ++q) {
+            const double xi = d->qp_xi[q0 + q];
+            lagrange_basis(xi, node_xi, val, der);
+            for (int k = 0; k < N; ++k) {
+                S[L.phi + q * N + k] = val[k];
+                S[L.dphi + q * N + k] = der[k];
+            }
+            // sections: linear interpolation in xi, clamped at the ends
+            // (populate_element_views.hpp:90-141, interpolation.hpp LinearInterpWeights)
+            std::vector<double> wsec(sec_xi.size(), 0.);
+            const auto lo = std::lower_bound(sec_xi.begin(), sec_xi.end(), xi);
+            if (lo == sec_xi.begin()) {
+                wsec.front() = 1.;
+            } else if (lo == sec_xi.end()) {
+                wsec.back() = 1.;
+            } else {
+                const size_t idx = static_cast<size_t>(lo - sec_xi.begin());
+                const double wu = (xi - sec_xi[idx - 1]) / (sec_xi[idx] - sec_xi[idx - 1]);
+                wsec[idx - 1] = 1. - wu;
+                wsec[idx] = wu;
+            }
+            for (int k = 0; k < 36; ++k) {
+                double m = 0., c = 0.;
+                for (size_t s = 0; s < sec_xi.size(); ++s) {
+                    m += d->section_mass[(s0 + s) * 36 + k] * wsec[s];
+                    c += d->section_stiffness[(s0 + s) * 36 + k] * wsec[s];
+                }
+                S[L.mstar + q * 36 + k] = m;
+                S[L.cstar + q * 36 + k] = c;
+            }
+            // reference rotation: normalised interpolated node orientation
+            // (interpolation_operations.hpp InterpQuaternion)
+            double r[4] = {0., 0., 0., 0.};
+            double xp[3] = {0., 0., 0.};
+            for (int k = 0; k < N; ++k) {
+                const double* x0 = d->node_x0 + B.node_ids[k] * 7;
+                for (int c = 0; c < 4; ++c) r[c] += x0[3 + c] * val[k];
+                for (int c = 0; c < 3; ++c) xp[c] += x0[c] * der[k];
+            }
+            const double rl = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3]);
+            if (rl == 0.) {
+                S[L.r0 + q * 4] = 1.;
+            } else {
+                for (int c = 0; c < 4; ++c) S[L.r0 + q * 4 + c] = r[c] / rl;
+            }
+            // Jacobian |dx0/dxi| and unit tangent (calculate_jacobian.hpp:36-76)
+            const double J = std::sqrt(xp[0] * xp[0] + xp[1] * xp[1] + xp[2] * xp[2]);
+            if (!(J > 0.)) return fail(err, KYN_ERR_INVALID, "degenerate beam reference line");
+            for (int c = 0; c < 3; ++c) S[L.x0p + q * 3 + c] = xp[c] / J;
+            const double w = d->qp_weight[q0 + q];
+            S[L.qpw + q * 4 + 0] = w;
+            S[L.qpw + q * 4 + 1] = J;
+            S[L.qpw + q * 4 + 2] = w * J;
+            S[L.qpw + q * 4 + 3] = w / J;
+        }
+        // node state (src/model/copy_nodes_to_state.hpp:14-60)
+        static const double ident[7] = {0., 0., 0., 1., 0., 0., 0.};
+        for (int k = 0; k < N; ++k) {
+            const int id = B.node_ids[k];
+            const double* x0 = d->node_x0 + id * 7;
+            const double* u = d->node_u ? d->node_u + id * 7 : ident;
+            for (int c = 0; c < 7; ++c) {
+                S[L.x0 + k * 7 + c] = x0[c];
+                S[L.q + k * 7 + c] = u[c];
+                S[L.q_prev + k * 7 + c] = u[c];
+            }
+            for (int c = 0; c < 3; ++c) S[L.x + k * 7 + c] = x0[c] + u[c];
+            qmul(u + 3, x0 + 3, S + L.x + k * 7 + 3);
+            for (int c = 0; c < 6; ++c) {
+                S[L.v + k * 6 + c] = d->node_v ? d->node_v[id * 6 + c] : 0.;
+                S[L.vd + k * 6 + c] = d->node_vd ? d->node_vd[id * 6 + c] : 0.;
+                S[L.a + k * 6 + c] = S[L.vd + k * 6 + c];
+            }
+            for (int c = 0; c < 3; ++c) S[L.tangent + k * 9 + c * 4] = 1.;
+        }
+    }
+    for (int n = 0; n < nn; ++n)
+        if (M.node_beam[n] < 0)
+            return fail(err, KYN_ERR_UNSUPPORTED, "node not attached to any beam element");
+
+    // constraints (src/constraints/constraints.hpp:76-266)
+    M.con_beam.assign(d->num_constraints, -1);
+    M.con_slot.assign(d->num_constraints, -1);
+    if (d->num_constraints > 0 && (!d->constraint_type || !d->constraint_target_node))
+        return fail(err, KYN_ERR_INVALID, "constraints need type and target node");
+    std::vector<int> node_con(nn, -1);
+    for (int c = 0; c < d->num_constraints; ++c) {
+        const int t = d->constraint_type[c];
+        if (t != KYN_CONSTRAINT_FIXED_BC && t != KYN_CONSTRAINT_PRESCRIBED_BC)
+            return fail(err, KYN_ERR_UNSUPPORTED, "only FixedBC and PrescribedBC constraints");
+        const int node = d->constraint_target_node[c];
+        if (node < 0 || node >= nn) return fail(err, KYN_ERR_INVALID, "constraint node out of range");
+        if (node_con[node] >= 0)
+            return fail(err, KYN_ERR_UNSUPPORTED, "two constraints on one node");
+        node_con[node] = c;
+        const int e = M.node_beam[node];
+        HostBeam& B = M.beams[e];
+        if (B.nc >= kMaxBeamConstraints)
+            return fail(err, KYN_ERR_UNSUPPORTED, "more than 4 constraints on one beam");
+        const int slot = B.nc++;
+        M.con_beam[c] = e;
+        M.con_slot[c] = slot;
+        B.con_node[slot] = M.node_local[node];
+        B.con_type[slot] = t;
+        B.con_row[slot] = c;
+        const SlabLayout L = make_slab_layout(B.N, B.Q);
+        static const double ident[7] = {0., 0., 0., 1., 0., 0., 0.};
+        if (t == KYN_CONSTRAINT_FIXED_BC) {
+            const double* x0 = d->node_x0 + node * 7;
+            for (int k = 0; k < 3; ++k)
+                B.con_X0[slot][k] = x0[k] - (d->constraint_axis ? d->constraint_axis[c * 3 + k] : 0.);
+            for (int k = 0; k < 7; ++k) B.slab[L.con_input + slot * 7 + k] = ident[k];
+        } else {
+            for (int k = 0; k < 3; ++k) B.con_X0[slot][k] = 0.;
+            const double* u = d->constraint_initial_displacement
+                                  ? d->constraint_initial_displacement + c * 7
+                                  : ident;
+            for (int k = 0; k < 7; ++k) B.slab[L.con_input + slot * 7 + k] = u[k];
+        }
+    }
+
+    // DOF map: every node carries 6 DOFs, exclusive scan in node-id order
+    // (compute_node_freedom_map_table.hpp); constraint rows follow in order.
+    M.fmap.resize(nn);
+    for (int n = 0; n < nn; ++n) M.fmap[n] = 6 * n;
+    M.nsys = 6 * nn;
+    M.ndofs = M.nsys + 6 * d->num_constraints;
+
+    // CRS graph: each row lists the DOFs it couples to, sorted ascending
+    // (compute_row_ptrs.hpp, compute_col_inds.hpp, sort_crs_graph).
+    M.row_ptrs.assign(M.ndofs + 1, 0);
+    M.col_inds.clear();
+    std::vector<int> cols;
+    for (int row = 0; row < M.ndofs; ++row) {
+        cols.clear();
+        if (row < M.nsys) {
+            const int node = row / 6;
+            const HostBeam& B = M.beams[M.node_beam[node]];
+            for (int k = 0; k < B.N; ++k)
+                for (int c = 0; c < 6; ++c) cols.push_back(M.fmap[B.node_ids[k]] + c);
+            if (node_con[node] >= 0)
+                for (int c = 0; c < 6; ++c) cols.push_back(M.nsys + 6 * node_con[node] + c);
+        } else {
+            const int con = (row - M.nsys) / 6;
+            const int node = d->constraint_target_node[con];
+            for (int c = 0; c < 6; ++c) cols.push_back(M.fmap[node] + c);
+        }
+        std::sort(cols.begin(), cols.end());
+        M.col_inds.insert(M.col_inds.end(), cols.begin(), cols.end());
+        M.row_ptrs[row + 1] = static_cast<int>(M.col_inds.size());
+    }
+    return KYN_OK;
+}
+
+}  // namespace kyn

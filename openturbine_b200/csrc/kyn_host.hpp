@@ -1,0 +1,49 @@
+// kyn_host.hpp -- host-side model setup for the B200 beam path.
+//
+// Turns a kyn_model_desc into per-beam slabs (constant geometry plus initial
+// state, see SlabLayout) and the reference's CRS graph of the model.  This is
+// the once-per-model work that Model::CreateSystemWithSolver does on the host
+// and in setup kernels (src/model/model.hpp:42-63, 647-656;
+// src/elements/beams/create_beams.hpp:27-165; src/dof_management/*;
+// src/solver/create_full_matrix.hpp:27-73).
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "../../include/kynema_b200.h"
+#include "kyn_types.h"
+
+namespace kyn {
+
+struct HostBeam {
+    int N = 0, Q = 0, nc = 0;
+    std::vector<int> node_ids;        // global node ids in element order
+    std::vector<double> slab;         // SlabLayout-ordered doubles
+    int con_node[kMaxBeamConstraints] = {};
+    int con_type[kMaxBeamConstraints] = {};
+    int con_row[kMaxBeamConstraints] = {};   // constraint index in the model
+    double con_X0[kMaxBeamConstraints][3] = {};
+};
+
+struct HostModel {
+    int num_nodes = 0;
+    int num_constraints = 0;
+    std::vector<HostBeam> beams;
+    std::vector<int> node_beam, node_local;   // node -> (beam, local index)
+    std::vector<int> con_beam, con_slot;      // constraint -> (beam, slot)
+    std::vector<int> fmap;                    // node -> first DOF
+    int nsys = 0, ndofs = 0;
+    std::vector<int> row_ptrs, col_inds;      // reference CRS graph (sorted rows)
+    double gravity[3] = {0., 0., 0.};
+};
+
+// Validates the description and builds the host model.  Returns KYN_OK or a
+// negative KYN_ERR_* code with a message in `err`.
+int build_host_model(const kyn_model_desc* d, HostModel& out, std::string& err);
+
+// Lagrange basis on nodes xs evaluated at x: values and first derivatives.
+void lagrange_basis(double x, const std::vector<double>& xs, std::vector<double>& val,
+                    std::vector<double>& der);
+
+}  // namespace kyn

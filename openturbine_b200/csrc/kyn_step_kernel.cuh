@@ -1,0 +1,1015 @@
+// kyn_step_kernel.cuh -- fused per-beam time-step kernel for sm_100a.
+//
+// One CTA owns one beam element for a whole time step: predictor, every
+// Newton iteration (tangent operator, quadrature-point physics, node-pair
+// integration, assembly of the bordered constraint system, linear solve,
+// convergence test, update) and the post-step update.  The beam system lives
+// in shared memory for the whole step; HBM is touched only to read the beam's
+// constant data and to read/write its resident state.  The beams of one model
+// form a thread-block cluster and sum the model's convergence error through
+// distributed shared memory, so every beam of a model takes the same Newton
+// iterations as the reference's model-wide loop (src/step/step.hpp:54-83).
+//
+// Linear solve: the reference factors the whole bordered system with a
+// sparse direct solver (src/step/solve_system.hpp:27-31).  Here the
+// single-node boundary conditions are eliminated exactly: their gradient
+// B = grad*T and transpose grad^T are block-diagonal with an identity
+// translational block (src/constraints/calculate_fixed_bc_constraint.hpp,
+// calculate_prescribed_bc_constraint.hpp), so the constrained node's
+// correction follows from a 3x3 solve, the free-node block is factored by LU
+// in shared memory, and the multipliers follow from the constrained rows.
+#pragma once
+
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include "../../include/kynema_b200.h"
+#include "kyn_types.h"
+
+namespace kyn {
+
+namespace cg = cooperative_groups;
+
+// ---- small math (src/math/quaternion_operations.hpp, vector_operations.hpp) --
+__device__ __forceinline__ void quat_compose(const double* a, const double* b, double* o) {
+    o[0] = a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3];
+    o[1] = a[0] * b[1] + a[1] * b[0] + a[2] * b[3] - a[3] * b[2];
+    o[2] = a[0] * b[2] - a[1] * b[3] + a[2] * b[0] + a[3] * b[1];
+    o[3] = a[0] * b[3] + a[1] * b[2] - a[2] * b[1] + a[3] * b[0];
+}
+
+// Entry (i,j) of the rotation matrix of unit quaternion q.
+__device__ __forceinline__ double rot_entry(const double* q, int i, int j) {
+    const double w = q[0], x = q[1], y = q[2], z = q[3];
+    switch (i * 3 + j) {
+        case 0: return w * w + x * x - y * y - z * z;
+        case 1: return 2. * (x * y - w * z);
+        case 2: return 2. * (x * z + w * y);
+        case 3: return 2. * (x * y + w * z);
+        case 4: return w * w - x * x + y * y - z * z;
+        case 5: return 2. * (y * z - w * x);
+        case 6: return 2. * (x * z - w * y);
+        case 7: return 2. * (y * z + w * x);
+        default: return w * w - x * x - y * y + z * z;
+    }
+}
+
+// Entry (i,j) of tilde(v) (VecTilde).
+__device__ __forceinline__ double tilde_e(const double* v, int i, int j) {
+    if (i == j) return 0.;
+    const int k = 3 - i - j;
+    const double s = ((i + 1) % 3 == j) ? -1. : 1.;
+    return s * v[k];
+}
+
+__device__ __forceinline__ void cross3(const double* a, const double* b, double* c) {
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// Exponential map: rotation vector -> quaternion (RotationVectorToQuaternion,
+// device form with factor 0 below 1e-12).
+__device__ __forceinline__ void rotvec_to_quat(const double* phi, double* q) {
+    const double angle = sqrt(phi[0] * phi[0] + phi[1] * phi[1] + phi[2] * phi[2]);
+    double s, c;
+    sincos(angle / 2., &s, &c);
+    const double f = (fabs(angle) < 1.e-12) ? 0. : s / angle;
+    q[0] = c;
+    q[1] = phi[0] * f;
+    q[2] = phi[1] * f;
+    q[3] = phi[2] * f;
+}
+
+// Solve the 3x3 system M y = r (row-major M) by elimination with partial pivoting.
+__device__ inline bool solve3(const double* Min, const double* r, double* y) {
+    double M[3][4];
+    for (int i = 0; i < 3; ++i) {
+        for (int j = 0; j < 3; ++j) M[i][j] = Min[i * 3 + j];
+        M[i][3] = r[i];
+    }
+    for (int k = 0; k < 3; ++k) {
+        int p = k;
+        for (int i = k + 1; i < 3; ++i)
+            if (fabs(M[i][k]) > fabs(M[p][k])) p = i;
+        if (M[p][k] == 0.) return false;
+        if (p != k)
+            for (int j = 0; j < 4; ++j) {
+                const double t = M[k][j];
+                M[k][j] = M[p][j];
+                M[p][j] = t;
+            }
+        for (int i = k + 1; i < 3; ++i) {
+            const double l = M[i][k] / M[k][k];
+            for (int j = k; j < 4; ++j) M[i][j] -= l * M[k][j];
+        }
+    }
+    for (int i = 2; i >= 0; --i) {
+        double s = M[i][3];
+        for (int j = i + 1; j < 3; ++j) s -= M[i][j] * y[j];
+        y[i] = s / M[i][i];
+    }
+    return true;
+}
+
+// ---- shared-memory plan of one CTA --------------------------------------------
+constexpr int kWarps = kThreads / 32;
+constexpr int kGroups = kThreads / 16;  // 16-thread groups, one quadrature point each
+constexpr int kGroupScratch = 136;      // doubles of per-group scratch for QP math
+constexpr int kPanel = 8;               // LU panel width
+constexpr int kConStride = 96;      // doubles per constraint record in smem
+
+struct Smem {
+    int A;              // TR [n6][ldA]
+    int XK, XP, XO;     // double [Q][18]  nonzero halves
+    int XC, XI;         // double [Q][36]
+    int Fc, Fdig;       // double [Q][6]
+    int phi, dphi;      // double [Q][N]
+    int qpw;            // double [Q][4]
+    int q, q_prev, v, vd, a, qd;  // node state
+    int T;              // double [N][9]
+    int resid;          // double [N][6]
+    int b;              // double [n6]  permuted rhs
+    int xs;             // double [n6]  permuted solution
+    int rpiv;           // double [n6]  reciprocal pivots
+    int con;            // double [nc][kConStride]
+    int grp;            // double [kGroups][kGroupScratch]
+    int red;            // double [2][kWarps + 8]
+    int pos;            // int [N]
+    int bytes;
+    int ldA;
+};
+
+__host__ __device__ inline Smem make_smem(int N, int Q, int nc, int real_bytes) {
+    Smem S{};
+    int o = 0;
+    auto take = [&](int bytes) {
+        const int r = o;
+        o += (bytes + 15) & ~15;
+        return r;
+    };
+    const int n6 = 6 * N;
+    S.ldA = n6 + 1;
+    S.A = take(n6 * S.ldA * real_bytes);
+    S.XK = take(Q * 18 * 8);
+    S.XP = take(Q * 18 * 8);
+    S.XO = take(Q * 18 * 8);
+    S.XC = take(Q * 36 * 8);
+    S.XI = take(Q * 36 * 8);
+    S.Fc = take(Q * 6 * 8);
+    S.Fdig = take(Q * 6 * 8);
+    S.phi = take(Q * N * 8);
+    S.dphi = take(Q * N * 8);
+    S.qpw = take(Q * 4 * 8);
+    S.q = take(N * 7 * 8);
+    S.q_prev = take(N * 7 * 8);
+    S.v = take(N * 6 * 8);
+    S.vd = take(N * 6 * 8);
+    S.a = take(N * 6 * 8);
+    S.qd = take(N * 6 * 8);
+    S.T = take(N * 9 * 8);
+    S.resid = take(N * 6 * 8);
+    S.b = take(n6 * 8);
+    S.xs = take(n6 * 8);
+    S.rpiv = take(n6 * 8);
+    S.con = take((nc > 0 ? nc : 1) * kConStride * 8);
+    S.grp = take(kGroups * kGroupScratch * 8);
+    S.red = take(2 * (kWarps + 8) * 8);
+    S.pos = take(N * 4);
+    S.bytes = o;
+    return S;
+}
+
+// Constraint record layout inside Smem::con (doubles).
+namespace conrec {
+constexpr int Phi = 0;     // [6] residual
+constexpr int Brot = 6;    // [9] rotational block of B = grad*T (row-major)
+constexpr int AX = 15;     // [9] rotational block of grad^T  (= AX(C))
+constexpr int Gl = 24;     // [6] grad^T lambda
+constexpr int xl = 30;     // [6] multiplier correction
+constexpr int lam = 36;    // [6] lambda
+constexpr int inp = 42;    // [7] prescribed input
+constexpr int yr = 49;     // [6] constrained-row residual b_r - A_r x
+}  // namespace conrec
+
+// ---- the kernel ------------------------------------------------------------------
+template <typename TR>
+__global__ void __launch_bounds__(kThreads, 2)
+    step_kernel(const KBeam* __restrict__ beams, StepCoeffs P, int record,
+                int* __restrict__ status_out, int* __restrict__ iters_out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const KBeam& KB = beams[blockIdx.x];
+    const int N = KB.N, Q = KB.Q, nc = KB.nc;
+    const int n6 = 6 * N;
+    const int m = 6 * (N - nc);   // free-node block size
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const Smem S = make_smem(N, Q, nc, sizeof(TR));
+    const SlabLayout L = make_slab_layout(N, Q);
+    double* __restrict__ slab = KB.slab;
+
+    TR* A = reinterpret_cast<TR*>(smem_raw + S.A);
+    const int ldA = S.ldA;
+    double* XK = reinterpret_cast<double*>(smem_raw + S.XK);
+    double* XP = reinterpret_cast<double*>(smem_raw + S.XP);
+    double* XO = reinterpret_cast<double*>(smem_raw + S.XO);
+    double* XC = reinterpret_cast<double*>(smem_raw + S.XC);
+    double* XI = reinterpret_cast<double*>(smem_raw + S.XI);
+    double* Fc = reinterpret_cast<double*>(smem_raw + S.Fc);
+    double* Fdig = reinterpret_cast<double*>(smem_raw + S.Fdig);
+    double* phi = reinterpret_cast<double*>(smem_raw + S.phi);
+    double* dphi = reinterpret_cast<double*>(smem_raw + S.dphi);
+    double* qpw = reinterpret_cast<double*>(smem_raw + S.qpw);
+    double* sq = reinterpret_cast<double*>(smem_raw + S.q);
+    double* sqp = reinterpret_cast<double*>(smem_raw + S.q_prev);
+    double* sv = reinterpret_cast<double*>(smem_raw + S.v);
+    double* svd = reinterpret_cast<double*>(smem_raw + S.vd);
+    double* sa = reinterpret_cast<double*>(smem_raw + S.a);
+    double* sqd = reinterpret_cast<double*>(smem_raw + S.qd);
+    double* sT = reinterpret_cast<double*>(smem_raw + S.T);
+    double* resid = reinterpret_cast<double*>(smem_raw + S.resid);
+    double* bp = reinterpret_cast<double*>(smem_raw + S.b);
+    double* xs = reinterpret_cast<double*>(smem_raw + S.xs);
+    double* rpiv = reinterpret_cast<double*>(smem_raw + S.rpiv);
+    double* con = reinterpret_cast<double*>(smem_raw + S.con);
+    double* gscr = reinterpret_cast<double*>(smem_raw + S.grp);
+    double* red = reinterpret_cast<double*>(smem_raw + S.red);
+    int* pos = reinterpret_cast<int*>(smem_raw + S.pos);
+    __shared__ int s_flag;
+
+    const double h = P.h;
+    // Optional phase timing: thread 0 reads the SM clock at phase boundaries
+    // (after a CTA barrier) and adds the cycles to prof[phase] at the end.
+    unsigned long long ph_acc[kNumPhases];
+    for (int k = 0; k < kNumPhases; ++k) ph_acc[k] = 0ull;
+    long long ph_t = clock64();
+    const bool timing = KB.prof != nullptr;
+    auto mark = [&](int phase) {
+        if (timing && tid == 0) {
+            const long long t = clock64();
+            ph_acc[phase] += static_cast<unsigned long long>(t - ph_t);
+            ph_t = t;
+        }
+    };
+
+    // ---- load constants and state ------------------------------------------
+    for (int k = tid; k < Q * N; k += kThreads) {
+        phi[k] = slab[L.phi + k];
+        dphi[k] = slab[L.dphi + k];
+    }
+    for (int k = tid; k < Q * 4; k += kThreads) qpw[k] = slab[L.qpw + k];
+    for (int k = tid; k < N * 7; k += kThreads) sq[k] = slab[L.q + k];
+    for (int k = tid; k < N * 6; k += kThreads) {
+        sv[k] = slab[L.v + k];
+        svd[k] = slab[L.vd + k];
+        sa[k] = slab[L.a + k];
+    }
+    if (tid < nc) {
+        double* c = con + tid * kConStride;
+        for (int k = 0; k < 7; ++k) c[conrec::inp + k] = slab[L.con_input + tid * 7 + k];
+        for (int k = 0; k < 6; ++k) c[conrec::lam + k] = 0.;  // ResetConstraints
+    }
+    if (tid == 0) {
+        // Free nodes first, constrained nodes last (in constraint order).
+        int p = 0;
+        for (int n = 0; n < N; ++n) {
+            bool constrained = false;
+            for (int c = 0; c < nc; ++c) constrained |= (KB.con_node[c] == n);
+            if (!constrained) pos[n] = p++;
+        }
+        for (int c = 0; c < nc; ++c) pos[KB.con_node[c]] = p++;
+        s_flag = 0;
+    }
+    __syncthreads();
+
+    // ---- PredictNextState (src/step/predict_next_state.hpp:14-47) ------------
+    for (int k = tid; k < N * 7; k += kThreads) sqp[k] = sq[k];
+    for (int k = tid; k < N * 6; k += kThreads) {
+        const double v_p = sv[k], vd_p = svd[k], a_p = sa[k];
+        svd[k] = 0.;
+        const double an = (P.alpha_f * vd_p - P.alpha_m * a_p) / (1. - P.alpha_m);
+        sa[k] = an;
+        sv[k] = v_p + h * (1. - P.gamma) * a_p + P.gamma * h * an;
+        sqd[k] = v_p + (0.5 - P.beta) * h * a_p + P.beta * h * an;
+    }
+    __syncthreads();
+    // CalculateDisplacement (src/state/calculate_displacement.hpp:25-50)
+    auto displacement = [&]() {
+        for (int n = tid; n < N; n += kThreads) {
+            for (int c = 0; c < 3; ++c) sq[n * 7 + c] = sqp[n * 7 + c] + h * sqd[n * 6 + c];
+            const double d[3] = {h * sqd[n * 6 + 3], h * sqd[n * 6 + 4], h * sqd[n * 6 + 5]};
+            double qd4[4], qn[4];
+            rotvec_to_quat(d, qd4);
+            quat_compose(qd4, sqp + n * 7 + 3, qn);
+            for (int c = 0; c < 4; ++c) sq[n * 7 + 3 + c] = qn[c];
+        }
+    };
+    displacement();
+    __syncthreads();
+    mark(kPhaseLoadPredict);
+
+    int status = KYN_NOT_CONVERGED;
+    int iters = 0;
+    const cg::cluster_group cluster = cg::this_cluster();
+    const bool clustered = KB.model_beams > 1;
+
+    for (int iter = 0; iter < P.max_iter; ++iter) {
+        // ---- tangent operator (src/system/calculate_tangent_operator.hpp:26-65)
+        // Only the rotational 3x3 block of the stored (transposed) operator is kept.
+        for (int n = tid; n < N; n += kThreads) {
+            const double rv[3] = {h * sqd[n * 6 + 3], h * sqd[n * 6 + 4], h * sqd[n * 6 + 5]};
+            const double ph = sqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
+            double sn, cs;
+            sincos(ph, &sn, &cs);
+            const double t1 = (ph > 1.e-16) ? (cs - 1.) / (ph * ph) : 0.;
+            const double t2 = (ph > 1.e-16) ? (1. - sn / ph) / (ph * ph) : 0.;
+            for (int i = 0; i < 3; ++i) {
+                for (int j = 0; j < 3; ++j) {
+                    // m1 = t2*(rv~ rv~) + t1*rv~ ; T_rot = I + m1 ; stored transposed
+                    double rr = 0.;
+                    for (int k = 0; k < 3; ++k) rr += tilde_e(rv, j, k) * tilde_e(rv, k, i);
+                    sT[n * 9 + i * 3 + j] = (i == j ? 1. : 0.) + (t1 * tilde_e(rv, j, i) + t2 * rr);
+                }
+            }
+        }
+
+        // ---- quadrature-point values (calculate_quadrature_point_values.hpp) ---
+        // 16 threads per quadrature point; a CTA covers 16 points per pass.  Each
+        // stage gives every lane of a group the same formula on its own entries,
+        // so the half-warps run without divergence.
+        {
+            const int grp = tid >> 4;
+            const int g = tid & 15;
+            double* gs = gscr + grp * kGroupScratch;
+            double* rn = gs + 20;   // [4] normalised r
+            double* Rx = gs + 24;   // [9] R(r o r0)
+            double* Rr = gs + 33;   // [9] R(r)
+            double* st = gs + 42;   // [6] strain
+            double* Mu = gs + 48;   // [36] Muu
+            double* ms = gs + 84;   // mass, eta[3], s = x0'+u' [3] at 88..90
+            double* O12 = gs + 92;  // [9]
+            double* Gu = gs + 101;  // [18]
+            double* Kk = gs + 119;  // [9]
+            double* fcv = gs + 128; // [6]
+            for (int q0 = 0; q0 < Q; q0 += 16) {
+                const int qp = q0 + grp;
+                const bool act = qp < Q;
+                const double* ph_q = phi + qp * N;
+                const double* dp_q = dphi + qp * N;
+                const double* r0 = slab + L.r0 + qp * 4;
+                const double* x0p = slab + L.x0p + qp * 3;
+                // (1) interpolation: r, u_ddot, omega, omega_dot, u', r'
+                if (act) {
+                    const double Jq = qpw[qp * 4 + 1];
+                    for (int k = g; k < 20; k += 16) {
+                        double acc = 0.;
+                        for (int n = 0; n < N; ++n) {
+                            const double p = ph_q[n];
+                            const double dpJ = dp_q[n] / Jq;
+                            double val;
+                            if (k < 4) val = sq[n * 7 + 3 + k] * p;
+                            else if (k < 7) val = svd[n * 6 + (k - 4)] * p;
+                            else if (k < 10) val = sv[n * 6 + 3 + (k - 7)] * p;
+                            else if (k < 13) val = svd[n * 6 + 3 + (k - 10)] * p;
+                            else if (k < 16) val = sq[n * 7 + (k - 13)] * dpJ;
+                            else val = sq[n * 7 + 3 + (k - 16)] * dpJ;
+                            acc += val;
+                        }
+                        gs[k] = acc;
+                    }
+                }
+                __syncwarp();
+                if (act && g < 4) {
+                    const double nr = sqrt(gs[0] * gs[0] + gs[1] * gs[1] + gs[2] * gs[2] + gs[3] * gs[3]);
+                    rn[g] = gs[g] / nr;
+                }
+                __syncwarp();
+                // (2) R(xr), R(r), rotational strain 2 E(r) r', s = x0' + u'
+                if (act) {
+                    for (int k = g; k < 24; k += 16) {
+                        if (k < 9) {
+                            double xr[4];
+                            quat_compose(rn, r0, xr);
+                            Rx[k] = rot_entry(xr, k / 3, k % 3);
+                        } else if (k < 18) {
+                            Rr[k - 9] = rot_entry(rn, (k - 9) / 3, (k - 9) % 3);
+                        } else if (k < 21) {
+                            const int i = k - 18;
+                            const double* rp = gs + 16;
+                            const double E[3][4] = {{-rn[1], rn[0], -rn[3], rn[2]},
+                                                    {-rn[2], rn[3], rn[0], -rn[1]},
+                                                    {-rn[3], -rn[2], rn[1], rn[0]}};
+                            double e = 0.;
+                            for (int j = 0; j < 4; ++j) e += E[i][j] * rp[j];
+                            st[3 + i] = 2. * e;
+                        } else {
+                            ms[4 + (k - 21)] = x0p[k - 21] + gs[13 + (k - 21)];
+                        }
+                    }
+                }
+                __syncwarp();
+                // (3) Muu = R M* R^T, Cuu = R C* R^T; translational strain
+                if (act) {
+                    const double* mst = slab + L.mstar + qp * 36;
+                    const double* cst = slab + L.cstar + qp * 36;
+                    for (int o = g; o < 75; o += 16) {
+                        if (o < 72) {
+                            const int e = o % 36;
+                            const int i = e / 6, j = e % 6;
+                            const int bi = i / 3, bj = j / 3, ii = i % 3, jj = j % 3;
+                            const double* Cs = (o < 36) ? mst : cst;
+                            double acc = 0.;
+                            for (int pp = 0; pp < 3; ++pp) {
+                                double t = 0.;
+                                for (int ss = 0; ss < 3; ++ss)
+                                    t += Cs[(3 * bi + pp) * 6 + 3 * bj + ss] * Rx[jj * 3 + ss];
+                                acc += Rx[ii * 3 + pp] * t;
+                            }
+                            if (o < 36) Mu[e] = acc;
+                            else XC[qp * 36 + e] = acc;
+                        } else {
+                            // strain[i] = x0' + u' - R(r) x0'  (calculate_strain.hpp:27-46)
+                            const int i = o - 72;
+                            double rx = 0.;
+                            for (int j = 0; j < 3; ++j) rx += Rr[i * 3 + j] * x0p[j];
+                            st[i] = x0p[i] + gs[13 + i] - rx;
+                        }
+                    }
+                }
+                __syncwarp();
+                // (4) FC = Cuu eps (calculate_force_FC.hpp); mass and eta (CalculateEta)
+                const double* Cu = XC + qp * 36;
+                if (act && g < 6) {
+                    double f = 0.;
+                    for (int j = 0; j < 6; ++j) f += Cu[g * 6 + j] * st[j];
+                    fcv[g] = f;
+                    Fc[qp * 6 + g] = f;
+                } else if (act && g == 6) {
+                    const double mass = Mu[0];
+                    ms[0] = mass;
+                    ms[1] = Mu[5 * 6 + 1] / mass;
+                    ms[2] = -Mu[5 * 6 + 0] / mass;
+                    ms[3] = Mu[4 * 6 + 0] / mass;
+                }
+                __syncwarp();
+                const double* ud = gs + 4;
+                const double* om = gs + 7;
+                const double* omd = gs + 10;
+                const double* sv3 = ms + 4;  // x0' + u'
+                if (act && g < 9) {
+                    // (5) entry (i,j) of every 3x3 block: Ouu, Puu (calculate_Ouu/Puu.hpp),
+                    //     Guu (calculate_gyroscopic_matrix.hpp), Kuu
+                    //     (calculate_inertia_stiffness_matrix.hpp)
+                    const int i = g / 3, j = g % 3;
+                    const double mass = ms[0];
+                    const double meta[3] = {mass * ms[1], mass * ms[2], mass * ms[3]};
+                    double rw[3], rwd[3], wme[3];
+                    for (int r = 0; r < 3; ++r) {
+                        rw[r] = Mu[(3 + r) * 6 + 3] * om[0] + Mu[(3 + r) * 6 + 4] * om[1] +
+                                Mu[(3 + r) * 6 + 5] * om[2];
+                        rwd[r] = Mu[(3 + r) * 6 + 3] * omd[0] + Mu[(3 + r) * 6 + 4] * omd[1] +
+                                 Mu[(3 + r) * 6 + 5] * omd[2];
+                    }
+                    cross3(om, meta, wme);
+                    double o12 = -tilde_e(fcv, i, j), o22 = -tilde_e(fcv + 3, i, j);
+                    double p21 = tilde_e(fcv, i, j), p22 = 0.;
+                    double g12 = -tilde_e(wme, i, j), g22 = -tilde_e(rw, i, j);
+                    double k12 = 0., k22 = -tilde_e(rwd, i, j);
+                    for (int k = 0; k < 3; ++k) {
+                        const double s_kj = tilde_e(sv3, k, j);
+                        const double s_ki = tilde_e(sv3, k, i);
+                        o12 += Cu[i * 6 + k] * s_kj;
+                        o22 += Cu[(3 + i) * 6 + k] * s_kj;
+                        p21 += s_ki * Cu[k * 6 + j];
+                        p22 += s_ki * Cu[k * 6 + 3 + j];
+                        const double w_ik = tilde_e(om, i, k);
+                        const double me_kj = tilde_e(meta, k, j);
+                        g12 -= w_ik * me_kj;
+                        g22 += w_ik * Mu[(3 + k) * 6 + 3 + j];
+                        double ww = 0.;
+                        for (int l = 0; l < 3; ++l) ww += tilde_e(om, i, l) * tilde_e(om, l, k);
+                        k12 -= (tilde_e(omd, i, k) + ww) * me_kj;
+                        k22 += Mu[(3 + i) * 6 + 3 + k] * tilde_e(omd, k, j);
+                        k22 += tilde_e(ud, i, k) * me_kj;
+                        double inner = -tilde_e(rw, k, j);
+                        for (int l = 0; l < 3; ++l) inner += Mu[(3 + k) * 6 + 3 + l] * tilde_e(om, l, j);
+                        k22 += w_ik * inner;
+                    }
+                    O12[g] = o12;
+                    XO[qp * 18 + g] = o12;
+                    XO[qp * 18 + 9 + g] = o22;
+                    XP[qp * 18 + g] = p21;
+                    XP[qp * 18 + 9 + g] = p22;
+                    Gu[g] = g12;
+                    Gu[9 + g] = g22;
+                    XK[qp * 18 + g] = k12;
+                    Kk[g] = k22;
+                } else if (act && g < 15) {
+                    // Fd + Fi - Fe - Fg (calculate_force_FD.hpp, calculate_inertial_force.hpp,
+                    // calculate_gravity_force.hpp; Fe = 0)
+                    const int c = g - 9;
+                    const double mass = ms[0];
+                    const double eta[3] = {ms[1], ms[2], ms[3]};
+                    double fd = 0., fi, fgv;
+                    if (c < 3) {
+                        double wxe[3], wxwxe[3], wdxe[3];
+                        cross3(om, eta, wxe);
+                        cross3(om, wxe, wxwxe);
+                        cross3(omd, eta, wdxe);
+                        fi = mass * ud[c] + mass * (wxwxe[c] + wdxe[c]);
+                        fgv = mass * KB.gravity[c];
+                    } else {
+                        const int i = c - 3;
+                        for (int k = 0; k < 3; ++k) fd += tilde_e(sv3, k, i) * fcv[k];
+                        double exu[3], rw[3], rwd[3], wxrw[3];
+                        cross3(eta, ud, exu);
+                        for (int r = 0; r < 3; ++r) {
+                            rw[r] = Mu[(3 + r) * 6 + 3] * om[0] + Mu[(3 + r) * 6 + 4] * om[1] +
+                                    Mu[(3 + r) * 6 + 5] * om[2];
+                            rwd[r] = Mu[(3 + r) * 6 + 3] * omd[0] + Mu[(3 + r) * 6 + 4] * omd[1] +
+                                     Mu[(3 + r) * 6 + 5] * omd[2];
+                        }
+                        cross3(om, rw, wxrw);
+                        fi = mass * exu[i] + rwd[i] + wxrw[i];
+                        const double mg[3] = {mass * KB.gravity[0], mass * KB.gravity[1],
+                                              mass * KB.gravity[2]};
+                        double exg[3];
+                        cross3(eta, mg, exg);
+                        fgv = exg[i];
+                    }
+                    Fdig[qp * 6 + c] = fd + fi - fgv;
+                }
+                __syncwarp();
+                // (6) Quu_22 = SS^T (C11 SS - N~) joins Kuu_22; XI = beta' Muu + gamma' Guu
+                if (act) {
+                    if (g < 9) {
+                        const int i = g / 3, j = g % 3;
+                        double qv = 0.;
+                        for (int k = 0; k < 3; ++k) qv += tilde_e(sv3, k, i) * O12[k * 3 + j];
+                        XK[qp * 18 + 9 + g] = Kk[g] + qv;
+                    }
+                    for (int e = g; e < 36; e += 16) {
+                        const int i = e / 6, j = e % 6;
+                        double gg = 0.;
+                        if (j >= 3) gg = Gu[(i < 3 ? 0 : 9) + (i % 3) * 3 + (j - 3)];
+                        XI[qp * 36 + e] = P.beta_prime * Mu[e] + P.gamma_prime * gg;
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        mark(kPhaseQuadrature);
+
+        // ---- residual integration (integrate_residual_vector.hpp:33-50) ----------
+        for (int t = tid; t < N * 6; t += kThreads) {
+            const int n = t / 6, c = t % 6;
+            double acc = 0.;
+            for (int qp = 0; qp < Q; ++qp) {
+                const double w = qpw[qp * 4], wJ = qpw[qp * 4 + 2];
+                acc += (w * dphi[qp * N + n]) * Fc[qp * 6 + c] +
+                       (wJ * phi[qp * N + n]) * Fdig[qp * 6 + c];
+            }
+            resid[t] = acc - slab[L.fx + t];
+        }
+
+        // ---- stiffness + inertia integration and S T + I (integrate_*_matrix.hpp,
+        //      calculate_system_matrix.hpp), scaled by the conditioner into A ----------
+        for (int item = tid; item < 2 * N * N; item += kThreads) {
+            const int hh = item & 1;
+            const int pair = item >> 1;
+            const int i = pair / N, j = pair % N;
+            double Sacc[18], Iacc[18];
+#pragma unroll
+            for (int k = 0; k < 18; ++k) Sacc[k] = Iacc[k] = 0.;
+            for (int qp = 0; qp < Q; ++qp) {
+                const double w = qpw[qp * 4], wJ = qpw[qp * 4 + 2], wdJ = qpw[qp * 4 + 3];
+                const double p1 = phi[qp * N + i], p2 = phi[qp * N + j];
+                const double d1 = dphi[qp * N + i], d2 = dphi[qp * N + j];
+                const double cK = (p1 * p2) * wJ;
+                const double cP = (p1 * d2) * w;
+                const double cC = (d1 * d2) * wdJ;
+                const double cO = (d1 * p2) * w;
+                const double* xc = XC + qp * 36 + hh * 18;
+                const double* xi = XI + qp * 36 + hh * 18;
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) {
+                        double v = cC * xc[r * 6 + c];
+                        if (c >= 3) {
+                            const int e = r * 3 + (c - 3);
+                            v += cK * XK[qp * 18 + hh * 9 + e] + cO * XO[qp * 18 + hh * 9 + e];
+                        }
+                        if (hh == 1) v += cP * XP[qp * 18 + (c >= 3 ? 9 : 0) + r * 3 + (c % 3)];
+                        Sacc[r * 6 + c] += v;
+                        Iacc[r * 6 + c] += cK * xi[r * 6 + c];
+                    }
+                }
+            }
+            const double* Tj = sT + j * 9;
+            const int row0 = 6 * pos[i] + 3 * hh;
+            const int col0 = 6 * pos[j];
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+#pragma unroll
+                for (int c = 0; c < 6; ++c) {
+                    double sm;
+                    if (c < 3) {
+                        sm = Sacc[r * 6 + c] + Iacc[r * 6 + c];
+                    } else {
+                        sm = Iacc[r * 6 + c];
+                        for (int k = 0; k < 3; ++k) sm += Sacc[r * 6 + 3 + k] * Tj[k * 3 + (c - 3)];
+                    }
+                    A[(row0 + r) * ldA + col0 + c] = static_cast<TR>(sm * P.conditioner);
+                }
+            }
+        }
+
+        __syncthreads();
+        mark(kPhaseIntegrate);
+
+        // ---- constraints (calculate_constraint_residual_gradient.hpp:60-199) -------
+        if (warp == kWarps - 1 && lane < nc) {
+            double* cr = con + lane * kConStride;
+            const int tn = KB.con_node[lane];
+            const double* nu = sq + tn * 7;
+            double u1[3] = {0., 0., 0.}, R1[4] = {1., 0., 0., 0.};
+            if (KB.con_type[lane] == KYN_CONSTRAINT_PRESCRIBED_BC) {
+                for (int k = 0; k < 3; ++k) u1[k] = cr[conrec::inp + k];
+                for (int k = 0; k < 4; ++k) R1[k] = cr[conrec::inp + 3 + k];
+            }
+            const double* X0 = KB.con_X0[lane];
+            const double len = sqrt(R1[0] * R1[0] + R1[1] * R1[1] + R1[2] * R1[2] + R1[3] * R1[3]);
+            const double R1t[4] = {R1[0] / len, -R1[1] / len, -R1[2] / len, -R1[3] / len};
+            double R1X0[3];
+            for (int i = 0; i < 3; ++i) {
+                R1X0[i] = 0.;
+                for (int j = 0; j < 3; ++j) R1X0[i] += rot_entry(R1, i, j) * X0[j];
+            }
+            for (int i = 0; i < 3; ++i) cr[conrec::Phi + i] = nu[i] + X0[i] - u1[i] - R1X0[i];
+            double R2R1t[4];
+            quat_compose(nu + 3, R1t, R2R1t);
+            double C[9];
+            for (int e = 0; e < 9; ++e) C[e] = rot_entry(R2R1t, e / 3, e % 3);
+            cr[conrec::Phi + 3] = (C[7] - C[5]) / 2.;
+            cr[conrec::Phi + 4] = (C[2] - C[6]) / 2.;
+            cr[conrec::Phi + 5] = (C[3] - C[1]) / 2.;
+            // AX(C) = tr(C)/2 I - C/2 ; grad rotational block = AX^T ; grad^T block = AX
+            const double tr = (C[0] + C[4] + C[8]) / 2.;
+            double AXm[9];
+            for (int e = 0; e < 9; ++e) AXm[e] = -C[e] / 2. + ((e % 4 == 0) ? tr : 0.);
+            for (int e = 0; e < 9; ++e) cr[conrec::AX + e] = AXm[e];
+            // B rotational block = AX^T * Rt  (Rt = stored tangent block of the node)
+            const double* Rt = sT + tn * 9;
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    double acc = 0.;
+                    for (int k = 0; k < 3; ++k) acc += AXm[k * 3 + i] * Rt[k * 3 + j];
+                    cr[conrec::Brot + i * 3 + j] = acc;
+                }
+            // grad^T lambda
+            for (int i = 0; i < 3; ++i) cr[conrec::Gl + i] = cr[conrec::lam + i];
+            for (int i = 0; i < 3; ++i) {
+                double acc = 0.;
+                for (int k = 0; k < 3; ++k) acc += AXm[i * 3 + k] * cr[conrec::lam + 3 + k];
+                cr[conrec::Gl + 3 + i] = acc;
+            }
+        }
+        __syncthreads();
+
+        // ---- right-hand side: b = -cond (-f + R + G^T lambda) (assemble_system_residual.hpp,
+        //      solve_system.hpp:20-24) in permuted order --------------------------------
+        for (int t = tid; t < n6; t += kThreads) {
+            const int n = t / 6, c = t % 6;
+            double val = -slab[L.f + t] + resid[t];
+            for (int k = 0; k < nc; ++k)
+                if (KB.con_node[k] == n) val += con[k * kConStride + conrec::Gl + c];
+            bp[6 * pos[n] + c] = -(val * P.conditioner);
+        }
+        if (record && KB.dump) {
+            // Dump of the assembled local system (natural node order, then constraints):
+            // matrix [nl][nl], then rhs [nl], then solution [nl]; nl = n6 + 6 nc.
+            const int nl = n6 + 6 * nc;
+            double* D = KB.dump;
+            for (int t = tid; t < nl * nl; t += kThreads) D[t] = 0.;
+        }
+        __syncthreads();
+        if (record && KB.dump) {
+            const int nl = n6 + 6 * nc;
+            double* D = KB.dump;
+            for (int t = tid; t < n6 * n6; t += kThreads) {
+                const int r = t / n6, c = t % n6;
+                D[r * nl + c] = static_cast<double>(A[(6 * pos[r / 6] + r % 6) * ldA + 6 * pos[c / 6] + c % 6]);
+            }
+            for (int t = tid; t < n6; t += kThreads) D[nl * nl + t] = bp[6 * pos[t / 6] + t % 6];
+            if (tid < nc) {
+                const double* cr = con + tid * kConStride;
+                const int tn = KB.con_node[tid];
+                const int r0 = n6 + 6 * tid;
+                for (int k = 0; k < 3; ++k) {
+                    D[(r0 + k) * nl + 6 * tn + k] = 1.;            // B translational block
+                    D[(6 * tn + k) * nl + r0 + k] = 1.;            // grad^T translational block
+                }
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) {
+                        D[(r0 + 3 + i) * nl + 6 * tn + 3 + j] = cr[conrec::Brot + i * 3 + j];
+                        D[(6 * tn + 3 + i) * nl + r0 + 3 + j] = cr[conrec::AX + i * 3 + j];
+                    }
+                for (int k = 0; k < 6; ++k) D[nl * nl + r0 + k] = -cr[conrec::Phi + k];
+            }
+        }
+
+        __syncthreads();
+        mark(kPhaseConstraints);
+
+        // ---- solve -----------------------------------------------------------------
+        // (S1) constrained node corrections: B x_r = -Phi
+        if (tid < nc) {
+            const double* cr = con + tid * kConStride;
+            const int pr = 6 * pos[KB.con_node[tid]];
+            for (int k = 0; k < 3; ++k) xs[pr + k] = -cr[conrec::Phi + k];
+            const double rhs[3] = {-cr[conrec::Phi + 3], -cr[conrec::Phi + 4], -cr[conrec::Phi + 5]};
+            double y[3] = {0., 0., 0.};
+            if (!solve3(cr + conrec::Brot, rhs, y)) atomicOr(&s_flag, 2);
+            for (int k = 0; k < 3; ++k) xs[pr + 3 + k] = y[k];
+        }
+        __syncthreads();
+        // (S2) free-row right-hand side, folded into column m of A
+        for (int i = tid; i < m; i += kThreads) {
+            double r = bp[i];
+            for (int j = m; j < n6; ++j) r -= static_cast<double>(A[i * ldA + j]) * xs[j];
+            A[i * ldA + m] = static_cast<TR>(r);
+        }
+        __syncthreads();
+        mark(kPhaseEliminate);
+        // (S3) blocked LU without pivoting of the free block A[0:m][0:m]; the
+        //      right-hand side in column m is eliminated with it.  Multipliers
+        //      are stored scaled; rpiv keeps the reciprocal pivots.
+        for (int k0 = 0; k0 < m; k0 += kPanel) {
+            const int kb = min(kPanel, m - k0);
+            // (a) panel factorisation by warp 0 (lanes over rows)
+            if (warp == 0) {
+                for (int j = 0; j < kb; ++j) {
+                    const int kk = k0 + j;
+                    const double d = static_cast<double>(A[kk * ldA + kk]);
+                    const double rp = 1. / d;
+                    if (lane == 0) {
+                        rpiv[kk] = rp;
+                        if (!(fabs(d) > 0.)) s_flag |= 2;
+                    }
+                    for (int i = kk + 1 + lane; i < m; i += 32) {
+                        const double l = static_cast<double>(A[i * ldA + kk]) * rp;
+                        A[i * ldA + kk] = static_cast<TR>(l);
+                        for (int c = j + 1; c < kb; ++c)
+                            A[i * ldA + k0 + c] = static_cast<TR>(
+                                static_cast<double>(A[i * ldA + k0 + c]) -
+                                l * static_cast<double>(A[kk * ldA + k0 + c]));
+                    }
+                    __syncwarp();
+                }
+            }
+            __syncthreads();
+            // (b) U12 = L11^{-1} A12 for columns k0+kb .. m (rhs included)
+            for (int c = k0 + kb + tid; c <= m; c += kThreads) {
+                double u[kPanel];
+#pragma unroll
+                for (int j = 0; j < kPanel; ++j)
+                    u[j] = (j < kb) ? static_cast<double>(A[(k0 + j) * ldA + c]) : 0.;
+#pragma unroll
+                for (int j = 1; j < kPanel; ++j) {
+                    if (j < kb) {
+                        double sacc = u[j];
+                        for (int t = 0; t < j; ++t)
+                            sacc -= static_cast<double>(A[(k0 + j) * ldA + k0 + t]) * u[t];
+                        u[j] = sacc;
+                        A[(k0 + j) * ldA + c] = static_cast<TR>(sacc);
+                    }
+                }
+            }
+            __syncthreads();
+            // (c) trailing update A22 -= L21 U12 with 4x4 register tiles on a
+            //     16x16 thread grid (rows r0+ty+16a, cols r0+tx+16b); the rhs
+            //     column is updated by the first threads.
+            const int r0 = k0 + kb;
+            const int R = m - r0;
+            if (R > 0) {
+                const int ty = tid >> 4, tx = tid & 15;
+                for (int ra = 0; ra * 16 < R; ra += 4) {
+                    for (int cb = 0; cb * 16 < R; cb += 4) {
+                        double acc[4][4];
+                        int rows[4], cols[4];
+#pragma unroll
+                        for (int a = 0; a < 4; ++a) {
+                            rows[a] = r0 + ty + 16 * (ra + a);
+                            cols[a] = r0 + tx + 16 * (cb + a);
+                        }
+#pragma unroll
+                        for (int a = 0; a < 4; ++a)
+#pragma unroll
+                            for (int b = 0; b < 4; ++b)
+                                acc[a][b] = (rows[a] < m && cols[b] < m)
+                                                ? static_cast<double>(A[rows[a] * ldA + cols[b]])
+                                                : 0.;
+                        for (int pk = 0; pk < kb; ++pk) {
+                            double lv[4], uv[4];
+#pragma unroll
+                            for (int a = 0; a < 4; ++a) {
+                                lv[a] = rows[a] < m ? static_cast<double>(A[rows[a] * ldA + k0 + pk]) : 0.;
+                                uv[a] = cols[a] < m ? static_cast<double>(A[(k0 + pk) * ldA + cols[a]]) : 0.;
+                            }
+#pragma unroll
+                            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                                for (int b = 0; b < 4; ++b) acc[a][b] -= lv[a] * uv[b];
+                        }
+#pragma unroll
+                        for (int a = 0; a < 4; ++a)
+#pragma unroll
+                            for (int b = 0; b < 4; ++b)
+                                if (rows[a] < m && cols[b] < m)
+                                    A[rows[a] * ldA + cols[b]] = static_cast<TR>(acc[a][b]);
+                    }
+                }
+                for (int i = r0 + tid; i < m; i += kThreads) {
+                    double y = static_cast<double>(A[i * ldA + m]);
+                    for (int pk = 0; pk < kb; ++pk)
+                        y -= static_cast<double>(A[i * ldA + k0 + pk]) *
+                             static_cast<double>(A[(k0 + pk) * ldA + m]);
+                    A[i * ldA + m] = static_cast<TR>(y);
+                }
+            }
+            __syncthreads();
+        }
+        mark(kPhaseFactor);
+        // (S4) blocked back substitution U x = y (y in column m)
+        for (int i = tid; i < m; i += kThreads) xs[i] = static_cast<double>(A[i * ldA + m]);
+        __syncthreads();
+        for (int k0 = ((m - 1) / kPanel) * kPanel; k0 >= 0 && m > 0; k0 -= kPanel) {
+            const int kb = min(kPanel, m - k0);
+            if (tid == 0) {
+                for (int j = kb - 1; j >= 0; --j) {
+                    double sacc = xs[k0 + j];
+                    for (int t = j + 1; t < kb; ++t)
+                        sacc -= static_cast<double>(A[(k0 + j) * ldA + k0 + t]) * xs[k0 + t];
+                    xs[k0 + j] = sacc * rpiv[k0 + j];
+                }
+            }
+            __syncthreads();
+            for (int i = tid; i < k0; i += kThreads) {
+                double sacc = xs[i];
+                for (int t = 0; t < kb; ++t)
+                    sacc -= static_cast<double>(A[i * ldA + k0 + t]) * xs[k0 + t];
+                xs[i] = sacc;
+            }
+            __syncthreads();
+        }
+        // (S5) multipliers from the constrained rows: grad^T x_l = b_r - A_r x
+        for (int rowi = warp; rowi < 6 * nc; rowi += kWarps) {
+            const int c = rowi / 6, k = rowi % 6;
+            const int pr = 6 * pos[KB.con_node[c]];
+            double sacc = 0.;
+            for (int j = lane; j < n6; j += 32) sacc += static_cast<double>(A[(pr + k) * ldA + j]) * xs[j];
+            for (int o = 16; o > 0; o >>= 1) sacc += __shfl_xor_sync(0xffffffffu, sacc, o);
+            if (lane == 0) con[c * kConStride + conrec::yr + k] = bp[pr + k] - sacc;
+        }
+        __syncthreads();
+        if (tid < nc) {
+            double* cr = con + tid * kConStride;
+            const double* y = cr + conrec::yr;
+            double yr[3] = {0., 0., 0.};
+            if (!solve3(cr + conrec::AX, y + 3, yr)) atomicOr(&s_flag, 2);
+            // UnconditionSolution (condition_system.hpp): x_lambda /= conditioner
+            for (int k = 0; k < 3; ++k) cr[conrec::xl + k] = y[k] / P.conditioner;
+            for (int k = 0; k < 3; ++k) cr[conrec::xl + 3 + k] = yr[k] / P.conditioner;
+        }
+        __syncthreads();
+        if (record && KB.dump) {
+            const int nl = n6 + 6 * nc;
+            double* D = KB.dump + nl * nl + nl;
+            for (int t = tid; t < n6; t += kThreads) D[t] = xs[6 * pos[t / 6] + t % 6];
+            if (tid < nc)
+                for (int k = 0; k < 6; ++k) D[n6 + 6 * tid + k] = con[tid * kConStride + conrec::xl + k];
+        }
+
+        __syncthreads();
+        mark(kPhaseSubstitute);
+
+        // ---- convergence error (calculate_error_sum_squares.hpp:33-79) --------------
+        double part = 0.;
+        for (int t = tid; t < n6; t += kThreads) {
+            const double pi = xs[6 * pos[t / 6] + t % 6];
+            const double xi = sqd[t] * h;
+            const double e = pi / (P.atol + P.rtol * fabs(xi));
+            part += e * e;
+        }
+        if (tid < 6 * nc) {
+            const double* cr = con + (tid / 6) * kConStride;
+            const double pi = cr[conrec::xl + tid % 6];
+            const double xi = cr[conrec::lam + tid % 6];
+            const double e = pi / (P.atol + P.rtol * fabs(xi));
+            part += e * e;
+        }
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+        double* slot = red + (iter & 1) * (kWarps + 8);
+        if (lane == 0) slot[warp] = part;
+        __syncthreads();
+        if (tid == 0) {
+            double s = 0.;
+            for (int w2 = 0; w2 < kWarps; ++w2) s += slot[w2];
+            slot[kWarps] = s;
+            slot[kWarps + 1] = static_cast<double>(s_flag);
+        }
+        double total, flags;
+        if (clustered) {
+            cluster.sync();
+            total = 0.;
+            flags = 0.;
+            for (int r = 0; r < KB.model_beams; ++r) {
+                const double* peer = cluster.map_shared_rank(slot, r);
+                total += peer[kWarps];
+                flags = fmax(flags, peer[kWarps + 1]);
+            }
+        } else {
+            __syncthreads();
+            total = slot[kWarps];
+            flags = slot[kWarps + 1];
+        }
+        const double err = sqrt(total / static_cast<double>(KB.model_dofs));
+        if (KB.rank == 0 && tid == 0 && iter < kMaxNewtonIters) KB.conv[iter] = err;
+        iters = iter + 1;
+
+        // ---- update (update_dynamic_prediction.hpp, calculate_displacement.hpp,
+        //      update_lambda_prediction.hpp) ----------------------------------------------
+        for (int t = tid; t < n6; t += kThreads) {
+            const double delta = xs[6 * pos[t / 6] + t % 6];
+            sqd[t] += delta / h;
+            if (P.dynamic) {
+                sv[t] += P.gamma_prime * delta;
+                svd[t] += P.beta_prime * delta;
+            }
+        }
+        if (tid < 6 * nc) {
+            double* cr = con + (tid / 6) * kConStride;
+            cr[conrec::lam + tid % 6] += cr[conrec::xl + tid % 6];
+        }
+        __syncthreads();
+        displacement();
+        __syncthreads();
+        mark(kPhaseUpdate);
+
+        if (flags != 0.) {
+            status = KYN_ERR_SINGULAR;
+            break;
+        }
+        if (!(err == err) || isinf(err)) {
+            status = KYN_ERR_NONFINITE;
+            break;
+        }
+        if (err <= 1.) {
+            status = KYN_OK;
+            break;
+        }
+    }
+
+    // ---- post-step (step.hpp:86-121) ---------------------------------------------------
+    if (status == KYN_OK) {
+        const double fac = (1. - P.alpha_f) / (1. - P.alpha_m);
+        for (int t = tid; t < n6; t += kThreads) sa[t] += fac * svd[t];
+    }
+    __syncthreads();
+    for (int k = tid; k < N * 7; k += kThreads) {
+        slab[L.q + k] = sq[k];
+        slab[L.q_prev + k] = sqp[k];
+    }
+    for (int k = tid; k < N * 6; k += kThreads) {
+        slab[L.v + k] = sv[k];
+        slab[L.vd + k] = svd[k];
+        slab[L.a + k] = sa[k];
+        slab[L.q_delta + k] = sqd[k];
+    }
+    if (status == KYN_OK) {
+        for (int n = tid; n < N; n += kThreads) {
+            const double* x0 = slab + L.x0 + n * 7;
+            for (int c = 0; c < 3; ++c) slab[L.x + n * 7 + c] = x0[c] + sq[n * 7 + c];
+            double r[4];
+            quat_compose(sq + n * 7 + 3, x0 + 3, r);
+            for (int c = 0; c < 4; ++c) slab[L.x + n * 7 + 3 + c] = r[c];
+        }
+    }
+    for (int k = tid; k < N * 9; k += kThreads) slab[L.tangent + k] = sT[k];
+    if (tid < 6 * nc) {
+        const double* cr = con + (tid / 6) * kConStride;
+        slab[L.lambda + tid] = cr[conrec::lam + tid % 6];
+    }
+    if (KB.rank == 0 && tid == 0) {
+        status_out[KB.plan_model] = status;
+        iters_out[KB.plan_model] = iters;
+    }
+    __syncthreads();
+    mark(kPhaseStore);
+    if (timing && tid == 0)
+        for (int k = 0; k < kNumPhases; ++k) atomicAdd(KB.prof + k, ph_acc[k]);
+    if (clustered) cluster.sync();  // peers may still read this CTA's slot
+}
+
+}  // namespace kyn

@@ -1,0 +1,114 @@
+// kyn_types.h -- data structures shared by the host setup and the CUDA kernels.
+//
+// Layout in HBM: every beam element owns one contiguous "slab" of doubles
+// holding its constant geometry (shape tables, quadrature data, sectional
+// 6x6 matrices) followed by its resident node state in beam-local node order.
+// A model is a set of independent beam blocks (no node shared between beams),
+// so one beam's slab is everything its CTA reads and writes during a step.
+#pragma once
+
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define KYN_HD __host__ __device__
+#else
+#define KYN_HD
+#endif
+
+namespace kyn {
+
+constexpr int kMaxBeamConstraints = 4;   // FixedBC / PrescribedBC per beam
+constexpr int kMaxClusterBeams = 8;      // beams per model (portable cluster size)
+constexpr int kMaxNewtonIters = 64;      // convergence-history capacity
+constexpr int kThreads = 256;            // threads per CTA of the step kernel
+
+// Offsets (in doubles) of the arrays inside one beam slab.
+struct SlabLayout {
+    int32_t phi, dphi;          // [Q][N] shape values / derivatives (qp-major)
+    int32_t qpw;                // [Q][4]  w, J, w*J, w/J
+    int32_t x0p;                // [Q][3]  unit tangent of the reference line
+    int32_t r0;                 // [Q][4]  reference rotation
+    int32_t mstar, cstar;       // [Q][36] sectional mass / stiffness (material frame)
+    int32_t x0;                 // [N][7]
+    int32_t q, q_prev, x;       // [N][7]
+    int32_t v, vd, a, q_delta;  // [N][6]
+    int32_t fx, f;              // [N][6]  node_FX and state.f
+    int32_t tangent;            // [N][9]  rotational block of the stored tangent
+    int32_t con_input;          // [kMaxBeamConstraints][7]
+    int32_t lambda;             // [kMaxBeamConstraints][6]
+    int32_t total;
+};
+
+KYN_HD inline SlabLayout make_slab_layout(int N, int Q) {
+    SlabLayout L{};
+    int o = 0;
+    auto take = [&](int n) {
+        const int r = o;
+        o += (n + 1) & ~1;  // keep 16-byte alignment of every array
+        return r;
+    };
+    L.phi = take(Q * N);
+    L.dphi = take(Q * N);
+    L.qpw = take(Q * 4);
+    L.x0p = take(Q * 3);
+    L.r0 = take(Q * 4);
+    L.mstar = take(Q * 36);
+    L.cstar = take(Q * 36);
+    L.x0 = take(N * 7);
+    L.q = take(N * 7);
+    L.q_prev = take(N * 7);
+    L.x = take(N * 7);
+    L.v = take(N * 6);
+    L.vd = take(N * 6);
+    L.a = take(N * 6);
+    L.q_delta = take(N * 6);
+    L.fx = take(N * 6);
+    L.f = take(N * 6);
+    L.tangent = take(N * 9);
+    L.con_input = take(kMaxBeamConstraints * 7);
+    L.lambda = take(kMaxBeamConstraints * 6);
+    L.total = o;
+    return L;
+}
+
+// One beam as seen by the step kernel (built per launch plan).
+struct KBeam {
+    double* slab;             // device slab of this beam
+    int32_t N, Q, nc;         // nodes, quadrature points, constraints on this beam
+    int32_t plan_model;       // model index inside the launch plan
+    int32_t rank;             // beam index inside its model (cluster rank)
+    int32_t model_beams;      // beams of the model (= cluster size of the launch)
+    int32_t model_dofs;       // Solver::num_dofs of the model
+    int32_t con_node[kMaxBeamConstraints];   // beam-local target node
+    int32_t con_type[kMaxBeamConstraints];   // KYN_CONSTRAINT_*
+    int32_t con_row[kMaxBeamConstraints];    // constraint index within the model
+    double con_X0[kMaxBeamConstraints][3];
+    double gravity[3];
+    double* conv;             // [kMaxNewtonIters] model convergence history (rank 0)
+    double* dump;             // optional: last assembled system (see kyn_capi.cu)
+    unsigned long long* prof; // optional: per-phase SM cycles, summed over beams
+};
+
+// Phases of the step kernel timed when KYN_OPT_PHASE_TIMING is set.
+enum Phase {
+    kPhaseLoadPredict = 0,
+    kPhaseQuadrature = 1,   // tangent operator + quadrature-point physics
+    kPhaseIntegrate = 2,    // residual + stiffness/inertia integration into A
+    kPhaseConstraints = 3,  // constraint residual/gradient + right-hand side
+    kPhaseEliminate = 4,    // boundary-condition elimination
+    kPhaseFactor = 5,       // LU of the free block
+    kPhaseSubstitute = 6,   // back substitution + multipliers
+    kPhaseUpdate = 7,       // convergence error + Newton update
+    kPhaseStore = 8,        // post-step and write-back
+    kNumPhases = 9
+};
+
+// Step coefficients (src/step/step_parameters.hpp:37-52).
+struct StepCoeffs {
+    double h, alpha_m, alpha_f, gamma, beta, gamma_prime, beta_prime, conditioner;
+    double atol, rtol;
+    int32_t max_iter;
+    int32_t dynamic;
+};
+
+}  // namespace kyn

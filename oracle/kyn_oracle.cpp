@@ -456,6 +456,7 @@ struct orc_model {
     std::vector<long> row_ptrs, col_inds;
     std::vector<double> values, b, xsol;
     std::vector<double> conv;
+    int solver_mode = 0;
 };
 
 namespace {
@@ -548,14 +549,40 @@ void update_beam(orc_model& m, OBeam& B, double beta_prime, double gamma_prime) 
         stiffness_qp(&B.cstar[qp * 36], &B.r0[qp * 4], &B.x0p[qp * 3], up, r2, rp, &Fc[qp * 6],
                      &Fd[qp * 6], &Cuu[qp * 36], &Ouu[qp * 36], &Puu[qp * 36], &Quu[qp * 36]);
     }
-    orc_integrate_residual(N, Q, B.w.data(), B.jac.data(), B.phi.data(), B.dphi.data(),
-                           B.fx.data(), Fc.data(), Fd.data(), Fi.data(), B.fe.data(), Fg.data(),
-                           B.residual.data());
     std::vector<double> S(N * N * 36), I(N * N * 36);
-    orc_integrate_stiffness(N, Q, B.w.data(), B.jac.data(), B.phi.data(), B.dphi.data(),
-                            Kuu.data(), Puu.data(), Cuu.data(), Ouu.data(), Quu.data(), S.data());
-    orc_integrate_inertia(N, Q, B.w.data(), B.jac.data(), B.phi.data(), Muu.data(), Guu.data(),
-                          beta_prime, gamma_prime, I.data());
+    if (m.solver_mode & 2) {
+        // Cross-check ordering: the same sums with the quadrature points reversed.
+        auto rev = [Q](const std::vector<double>& a, int w) {
+            std::vector<double> r(a.size());
+            for (int q = 0; q < Q; ++q)
+                for (int k = 0; k < w; ++k) r[(Q - 1 - q) * w + k] = a[q * w + k];
+            return r;
+        };
+        auto revn = [N, Q](const std::vector<double>& a) {
+            std::vector<double> r(a.size());
+            for (int n = 0; n < N; ++n)
+                for (int q = 0; q < Q; ++q) r[n * Q + (Q - 1 - q)] = a[n * Q + q];
+            return r;
+        };
+        const auto w = rev(B.w, 1), jac = rev(B.jac, 1), phi = revn(B.phi), dphi = revn(B.dphi);
+        orc_integrate_residual(N, Q, w.data(), jac.data(), phi.data(), dphi.data(), B.fx.data(),
+                               rev(Fc, 6).data(), rev(Fd, 6).data(), rev(Fi, 6).data(),
+                               B.fe.data(), rev(Fg, 6).data(), B.residual.data());
+        orc_integrate_stiffness(N, Q, w.data(), jac.data(), phi.data(), dphi.data(),
+                                rev(Kuu, 36).data(), rev(Puu, 36).data(), rev(Cuu, 36).data(),
+                                rev(Ouu, 36).data(), rev(Quu, 36).data(), S.data());
+        orc_integrate_inertia(N, Q, w.data(), jac.data(), phi.data(), rev(Muu, 36).data(),
+                              rev(Guu, 36).data(), beta_prime, gamma_prime, I.data());
+    } else {
+        orc_integrate_residual(N, Q, B.w.data(), B.jac.data(), B.phi.data(), B.dphi.data(),
+                               B.fx.data(), Fc.data(), Fd.data(), Fi.data(), B.fe.data(),
+                               Fg.data(), B.residual.data());
+        orc_integrate_stiffness(N, Q, B.w.data(), B.jac.data(), B.phi.data(), B.dphi.data(),
+                                Kuu.data(), Puu.data(), Cuu.data(), Ouu.data(), Quu.data(),
+                                S.data());
+        orc_integrate_inertia(N, Q, B.w.data(), B.jac.data(), B.phi.data(), Muu.data(),
+                              Guu.data(), beta_prime, gamma_prime, I.data());
+    }
     // calculate_system_matrix.hpp:25-53
     for (int i = 0; i < N; ++i) {
         for (int j = 0; j < N; ++j) {
@@ -598,7 +625,19 @@ void update_constraint(orc_model& m, OConstraint& C) {
     gemv(false, 6, 6, 1., C.t_grad_trans, 6, C.lambda, 0., C.t_lambda_res);
 }
 
+// Solver of the oracle (bit flags of orc_model::solver_mode): 0 = dense LU
+// with partial pivoting of the whole bordered system (default); bit 1 =
+// elimination of the single-node boundary conditions followed by LU without
+// pivoting of the free block; bit 2 = quadrature sums taken in reverse order.
+// The flagged variants are the same FP64 algorithm in another summation order;
+// their distance from the default measures the rounding-noise floor.
+void solve_eliminated(orc_model& m);
+
 void solve_dense(orc_model& m) {
+    if (m.solver_mode & 1) {
+        solve_eliminated(m);
+        return;
+    }
     // Dense LU with partial pivoting of the CRS system A x = b.
     const long n = m.ndofs;
     std::vector<double> A(n * n, 0.);
@@ -632,6 +671,89 @@ void solve_dense(orc_model& m) {
         double s = x[i];
         for (long j = i + 1; j < n; ++j) s -= A[i * n + j] * x[j];
         x[i] = s / A[i * n + i];
+    }
+    m.xsol = x;
+}
+
+void solve_eliminated(orc_model& m) {
+    const long n = m.ndofs;
+    std::vector<double> A(n * n, 0.);
+    for (long r = 0; r < n; ++r)
+        for (long k = m.row_ptrs[r]; k < m.row_ptrs[r + 1]; ++k) A[r * n + m.col_inds[k]] = m.values[k];
+    std::vector<char> constrained(m.nsys, 0);
+    for (auto& C : m.cons)
+        for (int c = 0; c < 6; ++c) constrained[C.target_table[c]] = 1;
+    std::vector<long> fr;
+    for (long i = 0; i < m.nsys; ++i)
+        if (!constrained[i]) fr.push_back(i);
+    std::vector<double> x(n, 0.);
+    // B x_r = b_lambda for each constraint (6x6 dense solve with pivoting)
+    for (auto& C : m.cons) {
+        double M[6][7];
+        for (int i = 0; i < 6; ++i) {
+            for (int j = 0; j < 6; ++j) M[i][j] = A[(m.nsys + C.row_first + i) * n + C.target_table[j]];
+            M[i][6] = m.b[m.nsys + C.row_first + i];
+        }
+        for (int k = 0; k < 6; ++k) {
+            int p = k;
+            for (int i = k + 1; i < 6; ++i) if (std::abs(M[i][k]) > std::abs(M[p][k])) p = i;
+            for (int j = 0; j < 7; ++j) std::swap(M[k][j], M[p][j]);
+            for (int i = k + 1; i < 6; ++i) {
+                const double l = M[i][k] / M[k][k];
+                for (int j = k; j < 7; ++j) M[i][j] -= l * M[k][j];
+            }
+        }
+        for (int i = 5; i >= 0; --i) {
+            double s2 = M[i][6];
+            for (int j = i + 1; j < 6; ++j) s2 -= M[i][j] * x[C.target_table[j]];
+            x[C.target_table[i]] = s2 / M[i][i];
+        }
+    }
+    const long mf = static_cast<long>(fr.size());
+    std::vector<double> F(mf * mf), y(mf);
+    for (long a = 0; a < mf; ++a) {
+        double r = m.b[fr[a]];
+        for (long j = 0; j < m.nsys; ++j) if (constrained[j]) r -= A[fr[a] * n + j] * x[j];
+        y[a] = r;
+        for (long c = 0; c < mf; ++c) F[a * mf + c] = A[fr[a] * n + fr[c]];
+    }
+    for (long k = 0; k < mf; ++k) {
+        const double rp = 1. / F[k * mf + k];
+        for (long i = k + 1; i < mf; ++i) {
+            const double l = F[i * mf + k] * rp;
+            for (long j = k + 1; j < mf; ++j) F[i * mf + j] -= l * F[k * mf + j];
+            y[i] -= l * y[k];
+        }
+    }
+    for (long i = mf - 1; i >= 0; --i) {
+        double s2 = y[i];
+        for (long j = i + 1; j < mf; ++j) s2 -= F[i * mf + j] * x[fr[j]];
+        x[fr[i]] = s2 / F[i * mf + i];
+    }
+    // multipliers from the constrained rows: G^T x_lambda = b_r - A_r x
+    for (auto& C : m.cons) {
+        double M[6][7];
+        for (int i = 0; i < 6; ++i) {
+            const long row = C.target_table[i];
+            double r = m.b[row];
+            for (long j = 0; j < m.nsys; ++j) r -= A[row * n + j] * x[j];
+            for (int j = 0; j < 6; ++j) M[i][j] = A[row * n + m.nsys + C.row_first + j];
+            M[i][6] = r;
+        }
+        for (int k = 0; k < 6; ++k) {
+            int p = k;
+            for (int i = k + 1; i < 6; ++i) if (std::abs(M[i][k]) > std::abs(M[p][k])) p = i;
+            for (int j = 0; j < 7; ++j) std::swap(M[k][j], M[p][j]);
+            for (int i = k + 1; i < 6; ++i) {
+                const double l = M[i][k] / M[k][k];
+                for (int j = k; j < 7; ++j) M[i][j] -= l * M[k][j];
+            }
+        }
+        for (int i = 5; i >= 0; --i) {
+            double s2 = M[i][6];
+            for (int j = i + 1; j < 6; ++j) s2 -= M[i][j] * x[m.nsys + C.row_first + j];
+            x[m.nsys + C.row_first + i] = s2 / M[i][i];
+        }
     }
     m.xsol = x;
 }
@@ -1110,6 +1232,10 @@ orc_model* orc_model_create(const kyn_model_desc* d, char* err, int errlen) {
 }
 
 void orc_model_destroy(orc_model* m) { delete m; }
+
+void orc_set_solver_mode(orc_model* m, int mode) {
+    if (m) m->solver_mode = mode;
+}
 
 int orc_model_info(const orc_model* m, kyn_model_info* info) {
     if (!m || !info) return KYN_ERR_INVALID;

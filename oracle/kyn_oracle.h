@@ -27,6 +27,10 @@ typedef struct orc_model orc_model;
 /* Model::CreateSystemWithSolver restated (host FP64). NULL on error. */
 orc_model* orc_model_create(const kyn_model_desc* desc, char* err, int errlen);
 void orc_model_destroy(orc_model* m);
+/* Bit flags: 0 = dense partial-pivot LU of the bordered system (default);
+ * 1 = boundary-condition elimination + LU without pivoting; 2 = quadrature
+ * sums in reverse order.  Flagged runs are cross-checks of rounding noise. */
+void orc_set_solver_mode(orc_model* m, int mode);
 int orc_model_info(const orc_model* m, kyn_model_info* info);
 int orc_set_loads(orc_model* m, int which, const double* values);
 int orc_set_prescribed(orc_model* m, int constraint_id, const double u[7]);

@@ -42,6 +42,7 @@ def lib():
         L.orc_model_create.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int]
         L.orc_model_destroy.argtypes = [ctypes.c_void_p]
         L.orc_model_info.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_set_solver_mode.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_set_loads.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
         L.orc_set_prescribed.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
         L.orc_step.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _ip]
@@ -70,7 +71,9 @@ def _d(a: np.ndarray):
 class OracleModel:
     """One model in the oracle; mirrors State/Solver reads of the reference."""
 
-    def __init__(self, packed):
+    def __init__(self, packed, solver_mode: int = 0):
+        """solver_mode 0: dense partial-pivot LU of the bordered system;
+        1: boundary-condition elimination + LU without pivoting."""
         self.packed = packed  # keeps numpy arrays alive
         err = ctypes.create_string_buffer(256)
         h = lib().orc_model_create(ctypes.byref(packed.desc), err, 256)
@@ -81,6 +84,8 @@ class OracleModel:
         info = KynModelInfo()
         lib().orc_model_info(self.h, ctypes.byref(info))
         self.info = info
+        if solver_mode:
+            lib().orc_set_solver_mode(self.h, solver_mode)
 
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:

@@ -1,0 +1,300 @@
+"""CUDA path (through the C ABI) against the oracle and the reference's goldens.
+
+Bar: identical Newton iteration counts and status, bit-exact CRS graph,
+states within 1e-10 relative (max-abs difference over max-abs value of the
+field) of the FP64 oracle, and the reference's own golden tolerances.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle.oracle_py import OracleModel
+from openturbine_b200 import workloads as W
+from openturbine_b200.model import StepParameters
+from tests.workloads_ref import (cantilever_test_loads, cantilever_test_model,
+                                 iea15_hub_displacement, iea15_rotor_model, load_golden,
+                                 rotating_beam_root_displacement, rotating_beam_test_model,
+                                 solver_test_model, solver_test_root_displacement)
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-10
+FIELDS = ("q", "v", "vd", "a", "q_delta", "x")
+STRICT = ("q", "v", "q_delta", "x")   # always within REL of the oracle
+
+
+class Twin:
+    """The oracle run twice: mode 0 (dense partial-pivot LU of the bordered
+    system, the checker) and mode 3 (the same FP64 algorithm with quadrature
+    sums reversed and the boundary conditions eliminated before an unpivoted
+    LU).  Their disagreement is the
+    rounding-noise floor of a field; accelerations and multipliers amplify the
+    last Newton correction by 1/h^2 and 1/(beta h^2), so their floor can exceed
+    1e-10 on stiff, heavily loaded beams."""
+
+    def __init__(self, pm):
+        self.o = OracleModel(pm)
+        self.alt = OracleModel(pm, solver_mode=3)
+        self.info = self.o.info
+
+    def set_node_fx(self, fx):
+        self.o.set_node_fx(fx)
+        self.alt.set_node_fx(fx)
+
+    def set_prescribed(self, c, u):
+        self.o.set_prescribed(c, u)
+        self.alt.set_prescribed(c, u)
+
+    def step(self, p):
+        self.alt.step(p)
+        return self.o.step(p)
+
+    def state(self, f):
+        return self.o.state(f)
+
+    def floor(self, f):
+        return rel_err(self.alt.state(f), self.o.state(f))
+
+    def convergence(self):
+        return self.o.convergence()
+
+    def crs(self):
+        return self.o.crs()
+
+    def system_vectors(self):
+        return self.o.system_vectors()
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from openturbine_b200.runtime import Context
+    c = Context(0)
+    yield c
+    c.close()
+
+
+def rel_err(a, b):
+    scale = max(np.abs(b).max(), 1e-300)
+    return float(np.abs(a - b).max() / scale)
+
+
+def assert_convergence_close(gpu, orc):
+    """Same Newton history: equal length, same converge decision at every
+    iteration, and equal error norms wherever the norm is above rounding noise
+    (a final norm ~1e-6 means a correction ~1e-11, set by rounding in the solve)."""
+    assert len(gpu) == len(orc)
+    for a, b in zip(gpu, orc):
+        assert (a <= 1.0) == (b <= 1.0)
+        if b > 1e-2:
+            assert abs(a - b) <= 1e-6 * b, (a, b)
+
+
+def assert_state_close(ctx, mid, orc, fields=FIELDS, rel=REL, lam=True):
+    """q, v, q_delta, x within `rel`; vd, a, lambda within max(rel, 10 x the
+    oracle's own noise floor) when `orc` is a Twin."""
+    fl = list(fields) + (["lambda"] if lam and orc.info.num_constraints else [])
+    for f in fl:
+        e = rel_err(ctx.state(mid, f), orc.state(f))
+        tol = rel
+        if f not in STRICT and isinstance(orc, Twin):
+            tol = max(rel, 10.0 * orc.floor(f))
+        assert e <= tol, (f, e, tol)
+
+
+def test_crs_graph_bit_exact(ctx):
+    for m in (cantilever_test_model()[0], solver_test_model(), iea15_rotor_model()[0],
+              W.rotor_model(1)[0], W.batch_cantilever_model(W.draw_batch(1)[0])):
+        pm = m.pack()
+        mid = ctx.create_model(pm)
+        o = OracleModel(pm)
+        rp, ci, _ = ctx.crs(mid, values=False)
+        orp, oci, _ = o.crs()
+        assert np.array_equal(rp, orp)
+        assert np.array_equal(ci, oci)
+        ctx.destroy_model(mid)
+
+
+def test_cantilever_golden_and_oracle(ctx):
+    g = load_golden("cantilever.json")
+    m, p = cantilever_test_model()
+    pm = m.pack()
+    mid = ctx.create_model(pm)
+    o = Twin(pm)
+    for k in range(3):
+        fx = cantilever_test_loads(k)
+        ctx.set_node_fx(mid, fx)
+        o.set_node_fx(fx)
+        st, it = ctx.step([mid], p)
+        ost, oit = o.step(p)
+        assert (st[0], it[0]) == (ost, oit) == (0, oit)
+        np.testing.assert_allclose(ctx.state(mid, "q")[4, :3], g["tip_q"][k], rtol=0,
+                                   atol=g["tolerance"])
+        assert_state_close(ctx, mid, o)
+        assert_convergence_close(ctx.convergence(mid), o.convergence())
+
+
+def test_solver_one_iteration_system(ctx):
+    """test_solver.cpp:247-440 shape: one iteration, CRS values, b and x."""
+    ctx.set_record_system(True)
+    try:
+        m = solver_test_model(2.0)
+        pm = m.pack()
+        mid = ctx.create_model(pm)
+        o = OracleModel(pm)
+        u = solver_test_root_displacement(2.0)
+        ctx.set_prescribed(mid, 0, u)
+        o.set_prescribed(0, u)
+        p = StepParameters(True, 1, 0.01, 0.9)
+        st, it = ctx.step([mid], p)
+        ost, oit = o.step(p)
+        assert (st[0], it[0]) == (ost, oit) == (1, 1)
+        _, _, vals = ctx.crs(mid)
+        _, _, ovals = o.crs()
+        assert rel_err(vals, ovals) <= 1e-13
+        b, x = ctx.system_vectors(mid)
+        ob, ox = o.system_vectors()
+        assert rel_err(b, ob) <= 1e-13
+        assert rel_err(x, ox) <= REL
+        g = load_golden("solver.json")["one_iteration"]
+        np.testing.assert_allclose(x, g["x"], rtol=0, atol=1e-6)
+        assert abs(ctx.convergence(mid)[0] - g["convergence_err"]) <= 1e-6 * g["convergence_err"]
+        assert_state_close(ctx, mid, o)
+        ctx.destroy_model(mid)
+    finally:
+        ctx.set_record_system(False)
+
+
+def test_iea15_rotor_golden(ctx):
+    """test_rotor.cpp:87-189 on the GPU: 3 beams in one cluster, 1e-13 absolute."""
+    d = load_golden("iea15_rotor.json")
+    m, p, bc = iea15_rotor_model(d)
+    pm = m.pack()
+    mid = ctx.create_model(pm)
+    o = Twin(pm)
+    for i in range(d["num_steps"]):
+        u = iea15_hub_displacement(i, d)
+        for c in bc:
+            ctx.set_prescribed(mid, c, u)
+            o.set_prescribed(c, u)
+        st, it = ctx.step([mid], p)
+        ost, oit = o.step(p)
+        assert (st[0], it[0]) == (ost, oit) and ost == 0
+    q = ctx.state(mid, "q")
+    for node, comp, val in d["expected_q"]:
+        ev = q[val[0], val[1]] if isinstance(val, list) else val
+        assert abs(q[node, comp] - ev) <= d["tolerance"], (node, comp, q[node, comp], ev)
+    assert_state_close(ctx, mid, o)
+
+
+def test_rotating_beam_golden(ctx):
+    g = load_golden("rotating_beam.json")
+    m, p = rotating_beam_test_model()
+    pm = m.pack()
+    mid = ctx.create_model(pm)
+    o = Twin(pm)
+    for i in range(10):
+        u = rotating_beam_root_displacement(i)
+        ctx.set_prescribed(mid, 0, u)
+        o.set_prescribed(0, u)
+        st, it = ctx.step([mid], p)
+        assert (st[0], it[0]) == o.step(p)
+    np.testing.assert_allclose(ctx.state(mid, "q").ravel(), g["q"], rtol=0, atol=g["tolerance"])
+    assert_state_close(ctx, mid, o)
+
+
+def test_config_cantilever_100_steps(ctx):
+    m = W.cantilever_model()
+    pm = m.pack()
+    mid = ctx.create_model(pm)
+    o = Twin(pm)
+    p = W.cantilever_params()
+    for k in range(100):
+        fx = np.zeros((5, 6))
+        fx[4, 2] = W.cantilever_tip_load(k)
+        ctx.set_node_fx(mid, fx)
+        o.set_node_fx(fx)
+        st, it = ctx.step([mid], p)
+        assert (st[0], it[0]) == o.step(p)
+    assert_state_close(ctx, mid, o)
+
+
+def test_config_rotor_with_gravity(ctx):
+    m, bcs = W.rotor_model(3)
+    pm = m.pack()
+    mid = ctx.create_model(pm)
+    o = Twin(pm)
+    p = W.rotor_params()
+    for k in range(40):
+        for c, u in zip(bcs, W.rotor_root_inputs(m, bcs, k)):
+            ctx.set_prescribed(mid, c, u)
+            o.set_prescribed(c, u)
+        st, it = ctx.step([mid], p)
+        assert (st[0], it[0]) == o.step(p)
+    assert_state_close(ctx, mid, o)
+
+
+def test_batch_uneven_cantilevers(ctx):
+    """64 uneven beams stepped together; each equals its own oracle run."""
+    draws = W.draw_batch(64)
+    pms = [W.batch_cantilever_model(d).pack() for d in draws]
+    ids = [ctx.create_model(pm) for pm in pms]
+    orcs = [Twin(pm) for pm in pms]
+    p = W.batch_params()
+    alive = np.ones(len(draws), dtype=bool)
+    for k in range(8):
+        fz = W.tip_loads(draws, k)
+        for i, d in enumerate(draws):
+            fx = W.node_fx_for(d, fz[i])
+            ctx.set_node_fx(ids[i], fx)
+            orcs[i].set_node_fx(fx)
+        st, it = ctx.step(ids, p)
+        for i in range(len(draws)):
+            ost, oit = orcs[i].step(p)
+            if alive[i]:
+                assert (st[i], it[i]) == (ost, oit), (i, k, st[i], it[i], ost, oit)
+                if ost != 0:
+                    alive[i] = False
+    checked = 0
+    for i in range(len(draws)):
+        if alive[i]:
+            assert_state_close(ctx, ids[i], orcs[i])
+            checked += 1
+    assert checked >= 32
+    for i in ids:
+        ctx.destroy_model(i)
+
+
+def test_not_converged_status(ctx):
+    m, _ = cantilever_test_model()
+    mid = ctx.create_model(m)
+    ctx.set_node_fx(mid, cantilever_test_loads(0) * 1e3)
+    st, it = ctx.step([mid], StepParameters(True, 1, 0.005, 0.0))
+    assert (st[0], it[0]) == (1, 1)
+
+
+def test_errors(ctx):
+    from openturbine_b200.runtime import KynError
+    with pytest.raises(KynError):
+        ctx.step([12345], W.cantilever_params())
+    st, it = ctx.step([], W.cantilever_params())
+    assert len(st) == 0
+    # a node shared by two beam elements is outside this path
+    m = W.cantilever_model()
+    m.AddBeamElement([0, 1], m.GetBeamElements()[0].sections, [[0.0, 2.0]])
+    with pytest.raises(KynError) as e:
+        ctx.create_model(m)
+    assert e.value.code == -2
+
+
+def test_budget_admission():
+    from openturbine_b200.runtime import Context, KynError
+    c = Context(0, hbm_budget_bytes=40_000)
+    try:
+        c.create_model(W.cantilever_model())
+        with pytest.raises(KynError) as e:
+            for _ in range(10):
+                c.create_model(W.cantilever_model())
+        assert e.value.code == -4
+    finally:
+        c.close()
