@@ -153,6 +153,7 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
             if (!(J > 0.)) return fail(err, KYN_ERR_INVALID, "degenerate beam reference line");
             for (int c = 0; c < 3; ++c) S[L.x0p + q * 3 + c] = xp[c] / J;
             const double w = d->qp_weight[q0 + q];
+            for (int k = 0; k < N; ++k) S[L.dphiJ + q * N + k] = S[L.dphi + q * N + k] / J;
             S[L.qpw + q * 4 + 0] = w;
             S[L.qpw + q * 4 + 1] = J;
             S[L.qpw + q * 4 + 2] = w * J;

@@ -81,50 +81,57 @@ __device__ __forceinline__ void rotvec_to_quat(const double* phi, double* q) {
     q[3] = phi[2] * f;
 }
 
-// Solve the 3x3 system M y = r (row-major M) by elimination with partial pivoting.
-__device__ inline bool solve3(const double* Min, const double* r, double* y) {
-    double M[3][4];
-    for (int i = 0; i < 3; ++i) {
-        for (int j = 0; j < 3; ++j) M[i][j] = Min[i * 3 + j];
-        M[i][3] = r[i];
-    }
-    for (int k = 0; k < 3; ++k) {
-        int p = k;
-        for (int i = k + 1; i < 3; ++i)
-            if (fabs(M[i][k]) > fabs(M[p][k])) p = i;
-        if (M[p][k] == 0.) return false;
-        if (p != k)
-            for (int j = 0; j < 4; ++j) {
-                const double t = M[k][j];
-                M[k][j] = M[p][j];
-                M[p][j] = t;
-            }
-        for (int i = k + 1; i < 3; ++i) {
-            const double l = M[i][k] / M[k][k];
-            for (int j = k; j < 4; ++j) M[i][j] -= l * M[k][j];
-        }
-    }
-    for (int i = 2; i >= 0; --i) {
-        double s = M[i][3];
-        for (int j = i + 1; j < 3; ++j) s -= M[i][j] * y[j];
-        y[i] = s / M[i][i];
-    }
+// Solve the 3x3 system M y = r (row-major M) by Cramer's rule; the matrices
+// solved here (rotational blocks of the boundary-condition gradient) are
+// close to rotations, so the determinant is far from zero.
+__device__ inline bool solve3(const double* M, const double* r, double* y) {
+    const double c00 = M[4] * M[8] - M[5] * M[7];
+    const double c01 = M[5] * M[6] - M[3] * M[8];
+    const double c02 = M[3] * M[7] - M[4] * M[6];
+    const double det = M[0] * c00 + M[1] * c01 + M[2] * c02;
+    if (!(fabs(det) > 0.)) return false;
+    const double id = 1. / det;
+    y[0] = (r[0] * c00 + M[1] * (M[5] * r[2] - r[1] * M[8]) + M[2] * (r[1] * M[7] - M[4] * r[2])) * id;
+    y[1] = (M[0] * (r[1] * M[8] - M[5] * r[2]) + r[0] * c01 + M[2] * (M[3] * r[2] - r[1] * M[6])) * id;
+    y[2] = (M[0] * (M[4] * r[2] - r[1] * M[7]) + M[1] * (r[1] * M[6] - M[3] * r[2]) + r[0] * c02) * id;
     return true;
+}
+
+// Reciprocal of a pivot: single-precision estimate refined by two Newton-Raphson
+// steps r <- r + r (1 - d r) (quadratic convergence: 1e-7 -> 1e-14 -> below
+// double rounding).  Falls back to division outside the float range.
+__device__ __forceinline__ double pivot_rcp(double d) {
+    const float f = static_cast<float>(d);
+    if (!(fabsf(f) > 1e-30f && fabsf(f) < 1e30f)) return 1. / d;
+    double r = static_cast<double>(__frcp_rn(f));
+    r = fma(r, fma(-d, r, 1.), r);
+    r = fma(r, fma(-d, r, 1.), r);
+    return r;
+}
+
+// FP64 tensor-core product D += A B for one 8x8x4 tile (mma.sync m8n8k4 .f64).
+// Fragment layout per lane l: a = A[l/4][l%4], b = B[l%4][l/4],
+// d0/d1 = D[l/4][2(l%4)] / D[l/4][2(l%4)+1].
+__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
 }
 
 // ---- shared-memory plan of one CTA --------------------------------------------
 constexpr int kWarps = kThreads / 32;
 constexpr int kGroups = kThreads / 16;  // 16-thread groups, one quadrature point each
-constexpr int kGroupScratch = 136;      // doubles of per-group scratch for QP math
+constexpr int kGroupScratch = 176;      // doubles of per-group scratch for QP math
+constexpr int kPairChunk = 64;          // node pairs per integration GEMM chunk
 constexpr int kPanel = 8;               // LU panel width
 constexpr int kConStride = 96;      // doubles per constraint record in smem
 
 struct Smem {
     int A;              // TR [n6][ldA]
-    int XK, XP, XO;     // double [Q][18]  nonzero halves
-    int XC, XI;         // double [Q][36]
+    int G;              // double [4Q][56] weighted quadrature blocks (integration GEMM)
     int Fc, Fdig;       // double [Q][6]
     int phi, dphi;      // double [Q][N]
+    int dphiJ;          // double [Q][N]
     int qpw;            // double [Q][4]
     int q, q_prev, v, vd, a, qd;  // node state
     int T;              // double [N][9]
@@ -133,7 +140,8 @@ struct Smem {
     int xs;             // double [n6]  permuted solution
     int rpiv;           // double [n6]  reciprocal pivots
     int con;            // double [nc][kConStride]
-    int grp;            // double [kGroups][kGroupScratch]
+    int grp;            // double [kGroups][kGroupScratch]  (quadrature phase)
+    int stg;            // double [64][56] GEMM output staging (integration; aliases grp)
     int red;            // double [2][kWarps + 8]
     int pos;            // int [N]
     int bytes;
@@ -151,15 +159,12 @@ __host__ __device__ inline Smem make_smem(int N, int Q, int nc, int real_bytes) 
     const int n6 = 6 * N;
     S.ldA = n6 + 1;
     S.A = take(n6 * S.ldA * real_bytes);
-    S.XK = take(Q * 18 * 8);
-    S.XP = take(Q * 18 * 8);
-    S.XO = take(Q * 18 * 8);
-    S.XC = take(Q * 36 * 8);
-    S.XI = take(Q * 36 * 8);
+    S.G = take(4 * Q * 56 * 8);
     S.Fc = take(Q * 6 * 8);
     S.Fdig = take(Q * 6 * 8);
     S.phi = take(Q * N * 8);
     S.dphi = take(Q * N * 8);
+    S.dphiJ = take(Q * N * 8);
     S.qpw = take(Q * 4 * 8);
     S.q = take(N * 7 * 8);
     S.q_prev = take(N * 7 * 8);
@@ -173,7 +178,12 @@ __host__ __device__ inline Smem make_smem(int N, int Q, int nc, int real_bytes) 
     S.xs = take(n6 * 8);
     S.rpiv = take(n6 * 8);
     S.con = take((nc > 0 ? nc : 1) * kConStride * 8);
-    S.grp = take(kGroups * kGroupScratch * 8);
+    {
+        const int grp_bytes = kGroups * kGroupScratch * 8;
+        const int stg_bytes = kPairChunk * 56 * 8;
+        S.grp = take(grp_bytes > stg_bytes ? grp_bytes : stg_bytes);
+        S.stg = S.grp;
+    }
     S.red = take(2 * (kWarps + 8) * 8);
     S.pos = take(N * 4);
     S.bytes = o;
@@ -209,15 +219,12 @@ __global__ void __launch_bounds__(kThreads, 2)
 
     TR* A = reinterpret_cast<TR*>(smem_raw + S.A);
     const int ldA = S.ldA;
-    double* XK = reinterpret_cast<double*>(smem_raw + S.XK);
-    double* XP = reinterpret_cast<double*>(smem_raw + S.XP);
-    double* XO = reinterpret_cast<double*>(smem_raw + S.XO);
-    double* XC = reinterpret_cast<double*>(smem_raw + S.XC);
-    double* XI = reinterpret_cast<double*>(smem_raw + S.XI);
+    double* G = reinterpret_cast<double*>(smem_raw + S.G);
     double* Fc = reinterpret_cast<double*>(smem_raw + S.Fc);
     double* Fdig = reinterpret_cast<double*>(smem_raw + S.Fdig);
     double* phi = reinterpret_cast<double*>(smem_raw + S.phi);
     double* dphi = reinterpret_cast<double*>(smem_raw + S.dphi);
+    double* dphiJ = reinterpret_cast<double*>(smem_raw + S.dphiJ);
     double* qpw = reinterpret_cast<double*>(smem_raw + S.qpw);
     double* sq = reinterpret_cast<double*>(smem_raw + S.q);
     double* sqp = reinterpret_cast<double*>(smem_raw + S.q_prev);
@@ -232,21 +239,25 @@ __global__ void __launch_bounds__(kThreads, 2)
     double* rpiv = reinterpret_cast<double*>(smem_raw + S.rpiv);
     double* con = reinterpret_cast<double*>(smem_raw + S.con);
     double* gscr = reinterpret_cast<double*>(smem_raw + S.grp);
+    double* Stg = reinterpret_cast<double*>(smem_raw + S.stg);
     double* red = reinterpret_cast<double*>(smem_raw + S.red);
     int* pos = reinterpret_cast<int*>(smem_raw + S.pos);
     __shared__ int s_flag;
+    __shared__ unsigned long long s_ph[kNumPhases];
 
     const double h = P.h;
     // Optional phase timing: thread 0 reads the SM clock at phase boundaries
     // (after a CTA barrier) and adds the cycles to prof[phase] at the end.
-    unsigned long long ph_acc[kNumPhases];
-    for (int k = 0; k < kNumPhases; ++k) ph_acc[k] = 0ull;
-    long long ph_t = clock64();
     const bool timing = KB.prof != nullptr;
+    long long ph_t = 0;
+    if (timing && tid == 0) {
+        for (int k = 0; k < kNumPhases; ++k) s_ph[k] = 0ull;
+        ph_t = clock64();
+    }
     auto mark = [&](int phase) {
         if (timing && tid == 0) {
             const long long t = clock64();
-            ph_acc[phase] += static_cast<unsigned long long>(t - ph_t);
+            s_ph[phase] += static_cast<unsigned long long>(t - ph_t);
             ph_t = t;
         }
     };
@@ -255,8 +266,10 @@ __global__ void __launch_bounds__(kThreads, 2)
     for (int k = tid; k < Q * N; k += kThreads) {
         phi[k] = slab[L.phi + k];
         dphi[k] = slab[L.dphi + k];
+        dphiJ[k] = slab[L.dphiJ + k];
     }
     for (int k = tid; k < Q * 4; k += kThreads) qpw[k] = slab[L.qpw + k];
+
     for (int k = tid; k < N * 7; k += kThreads) sq[k] = slab[L.q + k];
     for (int k = tid; k < N * 6; k += kThreads) {
         sv[k] = slab[L.v + k];
@@ -350,30 +363,39 @@ __global__ void __launch_bounds__(kThreads, 2)
             double* Gu = gs + 101;  // [18]
             double* Kk = gs + 119;  // [9]
             double* fcv = gs + 128; // [6]
+            double* Cu = gs + 136;  // [36] Cuu (rotated stiffness)
             for (int q0 = 0; q0 < Q; q0 += 16) {
                 const int qp = q0 + grp;
                 const bool act = qp < Q;
                 const double* ph_q = phi + qp * N;
-                const double* dp_q = dphi + qp * N;
                 const double* r0 = slab + L.r0 + qp * 4;
                 const double* x0p = slab + L.x0p + qp * 3;
+                // structural zeros of this point's G rows
+                if (act) {
+                    double* Gq = G + 4 * qp * 56;
+                    for (int t = g; t < 4 * 56; t += 16) {
+                        const int mm = t / 56, col = t % 56;
+                        bool zero = col >= 54;
+                        if (mm == 1) zero |= (col < 9) || (col >= 18 && col < 27) || col >= 36;
+                        if (mm == 2) zero |= col >= 36;
+                        if (mm == 3) zero |= col < 18 || col >= 36;
+                        if (zero) Gq[t] = 0.;
+                    }
+                }
                 // (1) interpolation: r, u_ddot, omega, omega_dot, u', r'
                 if (act) {
-                    const double Jq = qpw[qp * 4 + 1];
                     for (int k = g; k < 20; k += 16) {
+                        // source column of node state and shape table for sum k
+                        const double* src = (k < 4) ? sq + 3 + k
+                                          : (k < 7) ? svd + (k - 4)
+                                          : (k < 10) ? sv + 3 + (k - 7)
+                                          : (k < 13) ? svd + 3 + (k - 10)
+                                          : (k < 16) ? sq + (k - 13)
+                                                     : sq + 3 + (k - 16);
+                        const int stride = (k < 4 || k >= 13) ? 7 : 6;
+                        const double* shp = (k < 13) ? ph_q : dphiJ + qp * N;
                         double acc = 0.;
-                        for (int n = 0; n < N; ++n) {
-                            const double p = ph_q[n];
-                            const double dpJ = dp_q[n] / Jq;
-                            double val;
-                            if (k < 4) val = sq[n * 7 + 3 + k] * p;
-                            else if (k < 7) val = svd[n * 6 + (k - 4)] * p;
-                            else if (k < 10) val = sv[n * 6 + 3 + (k - 7)] * p;
-                            else if (k < 13) val = svd[n * 6 + 3 + (k - 10)] * p;
-                            else if (k < 16) val = sq[n * 7 + (k - 13)] * dpJ;
-                            else val = sq[n * 7 + 3 + (k - 16)] * dpJ;
-                            acc += val;
-                        }
+                        for (int n = 0; n < N; ++n) acc += src[n * stride] * shp[n];
                         gs[k] = acc;
                     }
                 }
@@ -393,13 +415,13 @@ __global__ void __launch_bounds__(kThreads, 2)
                         } else if (k < 18) {
                             Rr[k - 9] = rot_entry(rn, (k - 9) / 3, (k - 9) % 3);
                         } else if (k < 21) {
+                            // 2 E(r) r' with E = QuaternionDerivative (3x4)
                             const int i = k - 18;
                             const double* rp = gs + 16;
-                            const double E[3][4] = {{-rn[1], rn[0], -rn[3], rn[2]},
-                                                    {-rn[2], rn[3], rn[0], -rn[1]},
-                                                    {-rn[3], -rn[2], rn[1], rn[0]}};
-                            double e = 0.;
-                            for (int j = 0; j < 4; ++j) e += E[i][j] * rp[j];
+                            double e;
+                            if (i == 0) e = -rn[1] * rp[0] + rn[0] * rp[1] - rn[3] * rp[2] + rn[2] * rp[3];
+                            else if (i == 1) e = -rn[2] * rp[0] + rn[3] * rp[1] + rn[0] * rp[2] - rn[1] * rp[3];
+                            else e = -rn[3] * rp[0] - rn[2] * rp[1] + rn[1] * rp[2] + rn[0] * rp[3];
                             st[3 + i] = 2. * e;
                         } else {
                             ms[4 + (k - 21)] = x0p[k - 21] + gs[13 + (k - 21)];
@@ -425,7 +447,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                                 acc += Rx[ii * 3 + pp] * t;
                             }
                             if (o < 36) Mu[e] = acc;
-                            else XC[qp * 36 + e] = acc;
+                            else Cu[e] = acc;
                         } else {
                             // strain[i] = x0' + u' - R(r) x0'  (calculate_strain.hpp:27-46)
                             const int i = o - 72;
@@ -437,7 +459,6 @@ __global__ void __launch_bounds__(kThreads, 2)
                 }
                 __syncwarp();
                 // (4) FC = Cuu eps (calculate_force_FC.hpp); mass and eta (CalculateEta)
-                const double* Cu = XC + qp * 36;
                 if (act && g < 6) {
                     double f = 0.;
                     for (int j = 0; j < 6; ++j) f += Cu[g * 6 + j] * st[j];
@@ -494,14 +515,19 @@ __global__ void __launch_bounds__(kThreads, 2)
                         for (int l = 0; l < 3; ++l) inner += Mu[(3 + k) * 6 + 3 + l] * tilde_e(om, l, j);
                         k22 += w_ik * inner;
                     }
+                    // G rows of this quadrature point (see the integration GEMM):
+                    //   4q+1: w [Puu left | Puu right | 0], 4q+3: w [0 | Ouu right | 0]
+                    const double w = qpw[qp * 4], wJ = qpw[qp * 4 + 2];
+                    double* G1 = G + (4 * qp + 1) * 56;
+                    double* G3 = G + (4 * qp + 3) * 56;
                     O12[g] = o12;
-                    XO[qp * 18 + g] = o12;
-                    XO[qp * 18 + 9 + g] = o22;
-                    XP[qp * 18 + g] = p21;
-                    XP[qp * 18 + 9 + g] = p22;
+                    G3[18 + g] = w * o12;
+                    G3[18 + 9 + g] = w * o22;
+                    G1[9 + g] = w * p21;
+                    G1[18 + 9 + g] = w * p22;
                     Gu[g] = g12;
                     Gu[9 + g] = g22;
-                    XK[qp * 18 + g] = k12;
+                    G[(4 * qp) * 56 + 18 + g] = wJ * k12;
                     Kk[g] = k22;
                 } else if (act && g < 15) {
                     // Fd + Fi - Fe - Fg (calculate_force_FD.hpp, calculate_inertial_force.hpp,
@@ -539,19 +565,26 @@ __global__ void __launch_bounds__(kThreads, 2)
                     Fdig[qp * 6 + c] = fd + fi - fgv;
                 }
                 __syncwarp();
-                // (6) Quu_22 = SS^T (C11 SS - N~) joins Kuu_22; XI = beta' Muu + gamma' Guu
+                // (6) Quu_22 = SS^T (C11 SS - N~) joins Kuu_22; XI = beta' Muu + gamma' Guu;
+                //     G rows 4q+0: wJ [XI left | XK right | XI right], 4q+2: (w/J) [Cuu]
                 if (act) {
+                    const double wJ = qpw[qp * 4 + 2], wdJ = qpw[qp * 4 + 3];
+                    double* G0 = G + (4 * qp) * 56;
+                    double* G2 = G + (4 * qp + 2) * 56;
                     if (g < 9) {
                         const int i = g / 3, j = g % 3;
                         double qv = 0.;
                         for (int k = 0; k < 3; ++k) qv += tilde_e(sv3, k, i) * O12[k * 3 + j];
-                        XK[qp * 18 + 9 + g] = Kk[g] + qv;
+                        G0[18 + 9 + g] = wJ * (Kk[g] + qv);
                     }
                     for (int e = g; e < 36; e += 16) {
                         const int i = e / 6, j = e % 6;
                         double gg = 0.;
                         if (j >= 3) gg = Gu[(i < 3 ? 0 : 9) + (i % 3) * 3 + (j - 3)];
-                        XI[qp * 36 + e] = P.beta_prime * Mu[e] + P.gamma_prime * gg;
+                        const double xi = P.beta_prime * Mu[e] + P.gamma_prime * gg;
+                        const int col = (j < 3) ? i * 3 + j : 36 + i * 3 + (j - 3);
+                        G0[col] = wJ * xi;
+                        G2[(j < 3) ? i * 3 + j : 18 + i * 3 + (j - 3)] = wdJ * Cu[e];
                     }
                 }
                 __syncwarp();
@@ -573,58 +606,61 @@ __global__ void __launch_bounds__(kThreads, 2)
         }
 
         // ---- stiffness + inertia integration and S T + I (integrate_*_matrix.hpp,
-        //      calculate_system_matrix.hpp), scaled by the conditioner into A ----------
-        for (int item = tid; item < 2 * N * N; item += kThreads) {
-            const int hh = item & 1;
-            const int pair = item >> 1;
-            const int i = pair / N, j = pair % N;
-            double Sacc[18], Iacc[18];
+        //      calculate_system_matrix.hpp), scaled by the conditioner into A.
+        //      For node pair (i,j):  C_ij = sum_q sum_m coef_m(i,j,q) G[4q+m]  with
+        //      coef = (phi_i phi_j, phi_i phi'_j, phi'_i phi'_j, phi'_i phi_j) and G the
+        //      weighted blocks written by the quadrature phase (K/inertia, P, C, O
+        //      terms).  C_ij holds [S+I left | S right | I right]; then
+        //      SM_ij = [C_L | C_RS T_j + C_RI] (T_j is identity on the translational
+        //      block).  The pair GEMM runs on the FP64 tensor cores: each warp owns 8
+        //      pairs and all 7 column tiles, one k-step of 4 (m = 0..3) per point.
+        __syncthreads();
+        const int P2 = N * N;
+        for (int p0 = 0; p0 < P2; p0 += kPairChunk) {
+            {
+                const int prow = p0 + 8 * warp + (lane >> 2);
+                const bool valid = prow < P2;
+                const int i = valid ? prow / N : 0, jn = valid ? prow % N : 0;
+                const int mm = lane & 3;
+                const double* fi_tab = (mm < 2) ? phi : dphi;
+                const double* fj_tab = (mm == 0 || mm == 3) ? phi : dphi;
+                double acc[7][2];
 #pragma unroll
-            for (int k = 0; k < 18; ++k) Sacc[k] = Iacc[k] = 0.;
-            for (int qp = 0; qp < Q; ++qp) {
-                const double w = qpw[qp * 4], wJ = qpw[qp * 4 + 2], wdJ = qpw[qp * 4 + 3];
-                const double p1 = phi[qp * N + i], p2 = phi[qp * N + j];
-                const double d1 = dphi[qp * N + i], d2 = dphi[qp * N + j];
-                const double cK = (p1 * p2) * wJ;
-                const double cP = (p1 * d2) * w;
-                const double cC = (d1 * d2) * wdJ;
-                const double cO = (d1 * p2) * w;
-                const double* xc = XC + qp * 36 + hh * 18;
-                const double* xi = XI + qp * 36 + hh * 18;
+                for (int nt = 0; nt < 7; ++nt) acc[nt][0] = acc[nt][1] = 0.;
+                if (p0 + 8 * warp < P2) {
+                    for (int q = 0; q < Q; ++q) {
+                        const double a = valid ? fi_tab[q * N + i] * fj_tab[q * N + jn] : 0.;
+                        const double* gq = G + (4 * q + (lane & 3)) * 56 + (lane >> 2);
 #pragma unroll
-                for (int r = 0; r < 3; ++r) {
-#pragma unroll
-                    for (int c = 0; c < 6; ++c) {
-                        double v = cC * xc[r * 6 + c];
-                        if (c >= 3) {
-                            const int e = r * 3 + (c - 3);
-                            v += cK * XK[qp * 18 + hh * 9 + e] + cO * XO[qp * 18 + hh * 9 + e];
-                        }
-                        if (hh == 1) v += cP * XP[qp * 18 + (c >= 3 ? 9 : 0) + r * 3 + (c % 3)];
-                        Sacc[r * 6 + c] += v;
-                        Iacc[r * 6 + c] += cK * xi[r * 6 + c];
+                        for (int nt = 0; nt < 7; ++nt) dmma884(acc[nt][0], acc[nt][1], a, gq[nt * 8]);
                     }
                 }
-            }
-            const double* Tj = sT + j * 9;
-            const int row0 = 6 * pos[i] + 3 * hh;
-            const int col0 = 6 * pos[j];
+                double* cw = Stg + (8 * warp + (lane >> 2)) * 56 + 2 * (lane & 3);
 #pragma unroll
-            for (int r = 0; r < 3; ++r) {
-#pragma unroll
-                for (int c = 0; c < 6; ++c) {
-                    double sm;
-                    if (c < 3) {
-                        sm = Sacc[r * 6 + c] + Iacc[r * 6 + c];
-                    } else {
-                        sm = Iacc[r * 6 + c];
-                        for (int k = 0; k < 3; ++k) sm += Sacc[r * 6 + 3 + k] * Tj[k * 3 + (c - 3)];
-                    }
-                    A[(row0 + r) * ldA + col0 + c] = static_cast<TR>(sm * P.conditioner);
+                for (int nt = 0; nt < 7; ++nt) {
+                    cw[nt * 8] = acc[nt][0];
+                    cw[nt * 8 + 1] = acc[nt][1];
                 }
             }
+            __syncthreads();
+            const int np = min(kPairChunk, P2 - p0);
+            for (int t = tid; t < np * 36; t += kThreads) {
+                const int pl = t / 36, e = t % 36, r = e / 6, c = e % 6;
+                const int pr = p0 + pl;
+                const int i = pr / N, jn = pr % N;
+                const double* cr = Stg + pl * 56;
+                double val;
+                if (c < 3) {
+                    val = cr[r * 3 + c];
+                } else {
+                    const double* Tj = sT + jn * 9;
+                    val = cr[36 + r * 3 + (c - 3)];
+                    for (int k = 0; k < 3; ++k) val += cr[18 + r * 3 + k] * Tj[k * 3 + (c - 3)];
+                }
+                A[(6 * pos[i] + r) * ldA + 6 * pos[jn] + c] = static_cast<TR>(val * P.conditioner);
+            }
+            __syncthreads();
         }
-
         __syncthreads();
         mark(kPhaseIntegrate);
 
@@ -747,87 +783,101 @@ __global__ void __launch_bounds__(kThreads, 2)
         //      are stored scaled; rpiv keeps the reciprocal pivots.
         for (int k0 = 0; k0 < m; k0 += kPanel) {
             const int kb = min(kPanel, m - k0);
-            // (a) panel factorisation by warp 0 (lanes over rows)
+            // (a) diagonal block L11 U11 (kb x kb) by warp 0: lane r holds row k0+r in
+            //     registers; pivot rows are broadcast with shuffles.
             if (warp == 0) {
-                for (int j = 0; j < kb; ++j) {
-                    const int kk = k0 + j;
-                    const double d = static_cast<double>(A[kk * ldA + kk]);
-                    const double rp = 1. / d;
-                    if (lane == 0) {
-                        rpiv[kk] = rp;
-                        if (!(fabs(d) > 0.)) s_flag |= 2;
-                    }
-                    for (int i = kk + 1 + lane; i < m; i += 32) {
-                        const double l = static_cast<double>(A[i * ldA + kk]) * rp;
-                        A[i * ldA + kk] = static_cast<TR>(l);
-                        for (int c = j + 1; c < kb; ++c)
-                            A[i * ldA + k0 + c] = static_cast<TR>(
-                                static_cast<double>(A[i * ldA + k0 + c]) -
-                                l * static_cast<double>(A[kk * ldA + k0 + c]));
-                    }
-                    __syncwarp();
-                }
-            }
-            __syncthreads();
-            // (b) U12 = L11^{-1} A12 for columns k0+kb .. m (rhs included)
-            for (int c = k0 + kb + tid; c <= m; c += kThreads) {
-                double u[kPanel];
+                double v[kPanel];
 #pragma unroll
-                for (int j = 0; j < kPanel; ++j)
-                    u[j] = (j < kb) ? static_cast<double>(A[(k0 + j) * ldA + c]) : 0.;
+                for (int c = 0; c < kPanel; ++c)
+                    v[c] = (lane < kb && c < kb) ? static_cast<double>(A[(k0 + lane) * ldA + k0 + c]) : 0.;
 #pragma unroll
-                for (int j = 1; j < kPanel; ++j) {
+                for (int j = 0; j < kPanel; ++j) {
                     if (j < kb) {
-                        double sacc = u[j];
-                        for (int t = 0; t < j; ++t)
-                            sacc -= static_cast<double>(A[(k0 + j) * ldA + k0 + t]) * u[t];
-                        u[j] = sacc;
-                        A[(k0 + j) * ldA + c] = static_cast<TR>(sacc);
+                        const double d = __shfl_sync(0xffffffffu, v[j], j);
+                        const double rp = pivot_rcp(d);
+                        if (lane == 0) {
+                            rpiv[k0 + j] = rp;
+                            if (!(fabs(d) > 0.)) s_flag |= 2;
+                        }
+                        const double l = v[j] * rp;
+#pragma unroll
+                        for (int c = j + 1; c < kPanel; ++c) {
+                            const double u = __shfl_sync(0xffffffffu, v[c], j);
+                            if (lane > j) v[c] -= l * u;
+                        }
+                        if (lane > j) v[j] = l;
+                    }
+                }
+                if (lane < kb)
+#pragma unroll
+                    for (int c = 0; c < kPanel; ++c)
+                        if (c < kb) A[(k0 + lane) * ldA + k0 + c] = static_cast<TR>(v[c]);
+            }
+            __syncthreads();
+            // (b) panel rows below the block (L21 = A21 U11^{-1}) and U12 = L11^{-1} A12
+            //     (rhs column included), one row or column per thread
+            {
+                const int nrow = m - (k0 + kb);
+                const int ncol = m + 1 - (k0 + kb);
+                for (int t = tid; t < nrow + ncol; t += kThreads) {
+                    double u[kPanel];
+                    if (t < nrow) {
+                        const int i = k0 + kb + t;
+#pragma unroll
+                        for (int j = 0; j < kPanel; ++j) {
+                            if (j < kb) {
+                                double a = static_cast<double>(A[i * ldA + k0 + j]);
+                                for (int q2 = 0; q2 < j; ++q2)
+                                    a -= u[q2] * static_cast<double>(A[(k0 + q2) * ldA + k0 + j]);
+                                u[j] = a * rpiv[k0 + j];
+                                A[i * ldA + k0 + j] = static_cast<TR>(u[j]);
+                            }
+                        }
+                    } else {
+                        const int c = k0 + kb + (t - nrow);
+#pragma unroll
+                        for (int j = 0; j < kPanel; ++j) {
+                            if (j < kb) {
+                                double a = static_cast<double>(A[(k0 + j) * ldA + c]);
+                                for (int q2 = 0; q2 < j; ++q2)
+                                    a -= static_cast<double>(A[(k0 + j) * ldA + k0 + q2]) * u[q2];
+                                u[j] = a;
+                                if (j > 0) A[(k0 + j) * ldA + c] = static_cast<TR>(a);
+                            }
+                        }
                     }
                 }
             }
             __syncthreads();
-            // (c) trailing update A22 -= L21 U12 with 4x4 register tiles on a
-            //     16x16 thread grid (rows r0+ty+16a, cols r0+tx+16b); the rhs
-            //     column is updated by the first threads.
+            // (c) trailing update A22 -= L21 U12: 8x8 tiles on the FP64 tensor cores
+            //     (two k-steps of 4 over the panel); rows/cols >= m are masked.
+            //     The rhs column is updated by the first threads.
             const int r0 = k0 + kb;
             const int R = m - r0;
             if (R > 0) {
-                const int ty = tid >> 4, tx = tid & 15;
-                for (int ra = 0; ra * 16 < R; ra += 4) {
-                    for (int cb = 0; cb * 16 < R; cb += 4) {
-                        double acc[4][4];
-                        int rows[4], cols[4];
+                const int RT = (R + 7) / 8;
+                for (int rt = warp; rt < RT; rt += kWarps) {
+                    const int row = r0 + 8 * rt + (lane >> 2);
+                    double a[kPanel / 4];
 #pragma unroll
-                        for (int a = 0; a < 4; ++a) {
-                            rows[a] = r0 + ty + 16 * (ra + a);
-                            cols[a] = r0 + tx + 16 * (cb + a);
+                    for (int ks = 0; ks < kPanel / 4; ++ks) {
+                        const int kk = k0 + 4 * ks + (lane & 3);
+                        a[ks] = (row < m && kk < k0 + kb) ? -static_cast<double>(A[row * ldA + kk]) : 0.;
+                    }
+#pragma unroll 2
+                    for (int ct = 0; ct < RT; ++ct) {
+                        const int col = r0 + 8 * ct + 2 * (lane & 3);
+                        const int bcol = r0 + 8 * ct + (lane >> 2);
+                        double d0 = (row < m && col < m) ? static_cast<double>(A[row * ldA + col]) : 0.;
+                        double d1 = (row < m && col + 1 < m) ? static_cast<double>(A[row * ldA + col + 1]) : 0.;
+#pragma unroll
+                        for (int ks = 0; ks < kPanel / 4; ++ks) {
+                            const int kk = k0 + 4 * ks + (lane & 3);
+                            const double b = (bcol < m && kk < k0 + kb) ? static_cast<double>(A[kk * ldA + bcol]) : 0.;
+                            dmma884(d0, d1, a[ks], b);
                         }
-#pragma unroll
-                        for (int a = 0; a < 4; ++a)
-#pragma unroll
-                            for (int b = 0; b < 4; ++b)
-                                acc[a][b] = (rows[a] < m && cols[b] < m)
-                                                ? static_cast<double>(A[rows[a] * ldA + cols[b]])
-                                                : 0.;
-                        for (int pk = 0; pk < kb; ++pk) {
-                            double lv[4], uv[4];
-#pragma unroll
-                            for (int a = 0; a < 4; ++a) {
-                                lv[a] = rows[a] < m ? static_cast<double>(A[rows[a] * ldA + k0 + pk]) : 0.;
-                                uv[a] = cols[a] < m ? static_cast<double>(A[(k0 + pk) * ldA + cols[a]]) : 0.;
-                            }
-#pragma unroll
-                            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                                for (int b = 0; b < 4; ++b) acc[a][b] -= lv[a] * uv[b];
-                        }
-#pragma unroll
-                        for (int a = 0; a < 4; ++a)
-#pragma unroll
-                            for (int b = 0; b < 4; ++b)
-                                if (rows[a] < m && cols[b] < m)
-                                    A[rows[a] * ldA + cols[b]] = static_cast<TR>(acc[a][b]);
+                        if (row < m && col < m) A[row * ldA + col] = static_cast<TR>(d0);
+                        if (row < m && col + 1 < m) A[row * ldA + col + 1] = static_cast<TR>(d1);
                     }
                 }
                 for (int i = r0 + tid; i < m; i += kThreads) {
@@ -846,13 +896,14 @@ __global__ void __launch_bounds__(kThreads, 2)
         __syncthreads();
         for (int k0 = ((m - 1) / kPanel) * kPanel; k0 >= 0 && m > 0; k0 -= kPanel) {
             const int kb = min(kPanel, m - k0);
-            if (tid == 0) {
+            if (warp == 0) {
+                double xv = (lane < kb) ? xs[k0 + lane] : 0.;
                 for (int j = kb - 1; j >= 0; --j) {
-                    double sacc = xs[k0 + j];
-                    for (int t = j + 1; t < kb; ++t)
-                        sacc -= static_cast<double>(A[(k0 + j) * ldA + k0 + t]) * xs[k0 + t];
-                    xs[k0 + j] = sacc * rpiv[k0 + j];
+                    const double xj = __shfl_sync(0xffffffffu, xv, j) * rpiv[k0 + j];
+                    if (lane == j) xv = xj;
+                    if (lane < j) xv -= static_cast<double>(A[(k0 + lane) * ldA + k0 + j]) * xj;
                 }
+                if (lane < kb) xs[k0 + lane] = xv;
             }
             __syncthreads();
             for (int i = tid; i < k0; i += kThreads) {
@@ -1008,7 +1059,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     __syncthreads();
     mark(kPhaseStore);
     if (timing && tid == 0)
-        for (int k = 0; k < kNumPhases; ++k) atomicAdd(KB.prof + k, ph_acc[k]);
+        for (int k = 0; k < kNumPhases; ++k) atomicAdd(KB.prof + k, s_ph[k]);
     if (clustered) cluster.sync();  // peers may still read this CTA's slot
 }
 

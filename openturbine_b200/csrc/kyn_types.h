@@ -25,6 +25,7 @@ constexpr int kThreads = 256;            // threads per CTA of the step kernel
 // Offsets (in doubles) of the arrays inside one beam slab.
 struct SlabLayout {
     int32_t phi, dphi;          // [Q][N] shape values / derivatives (qp-major)
+    int32_t dphiJ;              // [Q][N] derivatives divided by the Jacobian
     int32_t qpw;                // [Q][4]  w, J, w*J, w/J
     int32_t x0p;                // [Q][3]  unit tangent of the reference line
     int32_t r0;                 // [Q][4]  reference rotation
@@ -49,6 +50,7 @@ KYN_HD inline SlabLayout make_slab_layout(int N, int Q) {
     };
     L.phi = take(Q * N);
     L.dphi = take(Q * N);
+    L.dphiJ = take(Q * N);
     L.qpw = take(Q * 4);
     L.x0p = take(Q * 3);
     L.r0 = take(Q * 4);
