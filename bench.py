@@ -181,9 +181,11 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--beams", type=int, default=4096)
     ap.add_argument("--ref-sample", type=int, default=512)
-    ap.add_argument("--cpu-sample", type=int, default=256)
-    ap.add_argument("--cpu-steps", type=int, default=40)
+    ap.add_argument("--cpu-sample", type=int, default=1024)
+    ap.add_argument("--cpu-steps", type=int, default=100)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--nodes", type=int, default=0,
+                    help="uniform nodes per beam (0: the batch's U{5..21}); for profiling one bucket")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -207,6 +209,8 @@ def main() -> None:
 
     # ---- build the shard: weak scaling, each rank owns its own 4096 beams ----
     draws = W.draw_batch(args.beams, first_id=rank * args.beams)
+    if args.nodes:
+        draws = [W.BeamDraw(d.model_id, args.nodes, d.length, d.amp, d.freq) for d in draws]
     ctx = Context(local)
     t_setup = time.perf_counter()
     ids = np.array([ctx.create_model(W.batch_cantilever_model(d).pack()) for d in draws],
@@ -306,8 +310,10 @@ def main() -> None:
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_value_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "4096-beam batch of uneven cantilevers (nodes U{5..21}, "
-                                   "Gauss nodes+2, L U(5,100) m, tip A sin(2 pi f t))",
+            "config": {"workload": (f"{args.beams}-beam batch of cantilevers with {args.nodes} nodes"
+                                    if args.nodes else
+                                    f"{args.beams}-beam batch of uneven cantilevers (nodes U{{5..21}}, "
+                                    "Gauss nodes+2, L U(5,100) m, tip A sin(2 pi f t))"),
                        "beams_per_gpu": args.beams, "h": 0.01, "rho_inf": 0.9,
                        "max_iter": params.max_iter, "a_tol": 1e-7, "r_tol": 1e-3,
                        "precision": "plain FP64", "l2": "flushed (256 MB write) before each step",

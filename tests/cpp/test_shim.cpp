@@ -1,0 +1,93 @@
+// The reference's regression drivers written against the C++ shim (kynema_b200.hpp):
+// test_cantilever_beam.cpp:31-138 and test_rotating_beam.cpp:93-150, same inputs,
+// same golden tolerances.  Exit code 0 on success.
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "kynema_b200.hpp"
+
+using namespace kynema_b200;
+
+static int failures = 0;
+static void expect_near(double a, double b, double tol, const char* what) {
+    if (!(std::abs(a - b) <= tol)) {
+        std::printf("FAIL %s: %.17g vs %.17g\n", what, a, b);
+        ++failures;
+    }
+}
+
+constexpr std::array<std::array<double, 6>, 6> kMass = {{
+    {8.538e-2, 0., 0., 0., 0., 0.}, {0., 8.538e-2, 0., 0., 0., 0.}, {0., 0., 8.538e-2, 0., 0., 0.},
+    {0., 0., 0., 1.4433e-2, 0., 0.}, {0., 0., 0., 0., 0.40972e-2, 0.}, {0., 0., 0., 0., 0., 1.0336e-2}}};
+constexpr std::array<std::array<double, 6>, 6> kStiff = {{
+    {1368.17e3, 0., 0., 0., 0., 0.}, {0., 88.56e3, 0., 0., 0., 0.}, {0., 0., 38.78e3, 0., 0., 0.},
+    {0., 0., 0., 16.9600e3, 17.6100e3, -0.3510e3}, {0., 0., 0., 17.6100e3, 59.1200e3, -0.3700e3},
+    {0., 0., 0., -0.3510e3, -0.3700e3, 141.470e3}}};
+const std::vector<std::array<double, 2>> kGauss7 = {
+    {-0.9491079123427585, 0.1294849661688697}, {-0.7415311855993943, 0.27970539148927664},
+    {-0.40584515137739696, 0.3818300505051189}, {6.123233995736766e-17, 0.4179591836734694},
+    {0.4058451513773971, 0.3818300505051189}, {0.7415311855993945, 0.27970539148927664},
+    {0.9491079123427585, 0.1294849661688697}};
+
+static void cantilever(const Context& ctx) {
+    const std::vector<double> node_s{0., 0.17267316464601146, 0.5, 0.8273268353539885, 1.};
+    Model model;
+    model.SetGravity(0., 0., 0.);
+    std::vector<size_t> ids;
+    for (double s : node_s) ids.push_back(model.AddNode().SetElemLocation(s).SetPosition(10 * s, 0., 0., 1., 0., 0., 0.).Build());
+    const std::vector<BeamSection> sections{BeamSection(0., kMass, kStiff), BeamSection(1., kMass, kStiff)};
+    model.AddBeamElement(ids, sections, kGauss7);
+    model.AddFixedBC(ids[0]);
+    auto parameters = StepParameters(true, 5, 0.005, 0.0);
+    auto [state, elements, constraints, solver] = model.CreateSystemWithSolver(ctx);
+    const double expected[3][3] = {{-8.15173937E-08, -1.86549248E-07, 6.97278045E-04},
+                                   {-1.00926258E-06, -7.91711079E-07, 2.65017558E-03},
+                                   {-5.05830945E-06, -2.29457246E-06, 6.30508154E-03}};
+    for (int k = 0; k < 3; ++k) {
+        elements.SetNodeFX(0, ids.back(), 2, 100. * std::sin(10.0 * 0.005 * (k + 1)));
+        const bool converged = Step(parameters, solver, elements, state, constraints);
+        if (!converged) { std::printf("FAIL cantilever step %d not converged\n", k); ++failures; }
+        const auto q = state.q();
+        for (int c = 0; c < 3; ++c) expect_near(q[4 * 7 + c], expected[k][c], 1e-6, "cantilever tip q");
+    }
+}
+
+static void rotating_beam(const Context& ctx) {
+    const std::vector<double> node_s{0., 0.11747233803526763, 0.35738424175967748, 0.64261575824032247, 0.88252766196473242, 1.};
+    Model model;
+    model.SetGravity(0., 0., 0.);
+    std::vector<size_t> ids;
+    for (double s : node_s) ids.push_back(model.AddNode().SetElemLocation(s).SetPosition(10 * s, 0., 0., 1., 0., 0., 0.).Build());
+    const std::vector<BeamSection> sections{BeamSection(0., kMass, kStiff), BeamSection(1., kMass, kStiff)};
+    model.AddBeamElement(ids, sections, kGauss7);
+    model.TranslateBeam(0, {2., 0., 0.});
+    model.SetBeamVelocityAboutPoint(0, {0., 0., 0., 0., 0., 0.1}, {0., 0., 0.});
+    model.AddPrescribedBC(ids[0]);
+    auto [state, elements, constraints, solver] = model.CreateSystemWithSolver(ctx);
+    auto parameters = StepParameters(true, 5, 0.01, 0.9);
+    for (int i = 0; i < 10; ++i) {
+        const auto q = RotationVectorToQuaternion({0., 0., 0.1 * 0.01 * (i + 1)});
+        const auto xr = RotateVectorByQuaternion(q, {2., 0., 0.});
+        constraints.UpdateDisplacement(0, {xr[0] - 2., xr[1], xr[2], q[0], q[1], q[2], q[3]});
+        if (!Step(parameters, solver, elements, state, constraints)) { std::printf("FAIL rotating step %d\n", i); ++failures; }
+    }
+    // first row of the golden q (test_rotating_beam.cpp:142-150)
+    const auto q = state.q();
+    const double root[7] = {-0.000099999166669473282, 0.019999666668333329, 0., 0.99998750002604219, 0., 0., 0.0049999791666927116};
+    for (int c = 0; c < 7; ++c) expect_near(q[c], root[c], 1e-6, "rotating beam root q");
+    if (solver.convergence_err().empty()) { std::printf("FAIL empty convergence history\n"); ++failures; }
+}
+
+int main() {
+    try {
+        Context ctx(0);
+        cantilever(ctx);
+        rotating_beam(ctx);
+    } catch (const std::exception& e) {
+        std::printf("FAIL exception: %s\n", e.what());
+        return 2;
+    }
+    std::printf("%s (%d failures)\n", failures ? "FAILED" : "OK", failures);
+    return failures ? 1 : 0;
+}

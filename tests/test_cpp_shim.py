@@ -1,0 +1,40 @@
+"""The reference's cantilever and rotating-beam drivers written against the
+C++ host shim (include/kynema_b200.hpp), compiled with g++ and run on the GPU.
+
+The CPU test only compiles the driver, so a broken header fails without a GPU.
+"""
+import os
+import subprocess
+
+import pytest
+
+from openturbine_b200 import build as kbuild
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+SRC = os.path.join(ROOT, "tests", "cpp", "test_shim.cpp")
+OUT_DIR = os.path.join(ROOT, "tests", "cpp", "_build")
+LIB_DIR = os.path.join(ROOT, "openturbine_b200", "_lib")
+
+
+def _compile() -> str:
+    kbuild.build()
+    os.makedirs(OUT_DIR, exist_ok=True)
+    exe = os.path.join(OUT_DIR, "test_shim")
+    gxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+    cmd = [gxx, "-std=c++20", "-O1", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), SRC,
+           "-L", LIB_DIR, "-lkynema_b200", "-Wl,-rpath," + LIB_DIR, "-o", exe]
+    subprocess.run(cmd, check=True)
+    return exe
+
+
+def test_shim_compiles():
+    assert os.path.exists(_compile())
+
+
+@pytest.mark.gpu
+def test_shim_cantilever_and_rotating_beam():
+    exe = _compile()
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    print(r.stdout)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "OK (0 failures)" in r.stdout
