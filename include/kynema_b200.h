@@ -209,6 +209,22 @@ KYN_API int kyn_set_loads_batch(kyn_ctx* ctx, const int* model_ids, int n, int w
 KYN_API int kyn_get_state_batch(kyn_ctx* ctx, const int* model_ids, int n, int field,
                                 double* out, int on_device);
 
+/* kyn_set_loads_batch without any allocation (no counterpart in the reference).
+ * For callers that cannot let a library allocate while they run, e.g. a CFD
+ * solver that owns the device memory through its own pool and shares the GPU:
+ * device staging comes from one fixed 9.19 MiB array inside the library instead
+ * of cudaMalloc'd buffers.  Limits per call: 8192 beam elements, 262144 node
+ * rows, and (host values) 1048576 load doubles; larger batches return
+ * KYN_ERR_INVALID with a message and change nothing.  The first call on each
+ * device does a one-time set-up (looks up the array's device address, which
+ * may load the library's device code): make it before any stream capture.
+ * The array is shared by every call and context on the device and keeps the
+ * last call's contents: calls that overlap in time (two host threads, or two
+ * contexts' streams) race on it; serialise them.  Results equal those of
+ * kyn_set_loads_batch. */
+KYN_API int kyn_set_loads_batch_static(kyn_ctx* ctx, const int* model_ids, int n, int which,
+                                       const double* values, int on_device);
+
 /* Replaces host reads of State / Constraints views after Step(). */
 KYN_API int kyn_get_state(kyn_ctx* ctx, int model_id, int field, double* out);
 

@@ -13,6 +13,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -845,6 +846,138 @@ int kyn_get_state_batch(kyn_ctx* c, const int* ids, int n, int field, double* ou
                                     cudaMemcpyDeviceToHost, c->stream));
         KYN_CUDA(c, cudaStreamSynchronize(c->stream));
     }
+    return KYN_OK;
+}
+
+}  // extern "C"
+
+// ---- batched load scatter through a static staging array (no allocation) ----
+//
+// kyn_set_loads_batch stages host loads in a device buffer that the context
+// grows with cudaMalloc, and builds its per-beam copy plan in cudaMalloc'd
+// memory.  Some callers cannot let a library allocate while they run: a CFD
+// solver that couples to the beams usually owns the device memory through its
+// own pool and shares the GPU with this library, and cudaMalloc/cudaFree there
+// would fail for lack of memory or stall the solver's streams with an implicit
+// device synchronisation.  kyn_set_loads_batch_static does the same scatter
+// (same kernel, same results) with every byte it needs on the device taken from
+// one file-scope array of fixed size, and its host-side plan built in fixed
+// static host arrays, so a call allocates nothing.
+namespace {
+
+constexpr int kStaticStageBeams = 8192;          // beam elements per call
+constexpr int kStaticStageRows = 8192 * 32;      // node rows per call (8192 beams x 32 nodes)
+constexpr long long kStaticStageValues = 1LL << 20;  // load doubles per call (8 MiB)
+constexpr size_t kStaticBeamBytes = sizeof(XferBeam) * kStaticStageBeams;
+constexpr size_t kStaticMapBytes = sizeof(int) * kStaticStageRows;
+constexpr size_t kStaticValuesOffset = kStaticBeamBytes + kStaticMapBytes;
+constexpr size_t kStaticStageBytes = kStaticValuesOffset + sizeof(double) * kStaticStageValues;
+static_assert(kStaticBeamBytes % 256 == 0 && kStaticValuesOffset % 256 == 0,
+              "static staging regions must stay 256-byte aligned");
+
+// [copy plan: XferBeam x 8192 | node map: int x 262144 | load values: double x 2^20],
+// 9.19 MiB in all.  Shared by every call on a device (and by every context on
+// it); each call writes the part it reads before its kernel runs, so nothing
+// has to start at zero and stale contents of an earlier call are never read.
+static __device__ __align__(256) unsigned char g_static_stage[kStaticStageBytes];
+
+constexpr int kStaticMaxDevices = 64;
+std::mutex g_static_stage_mu;                        // guards the tables below
+unsigned char* g_static_stage_addr[kStaticMaxDevices] = {};
+XferBeam g_static_host_beams[kStaticStageBeams];     // host side of the copy plan
+int g_static_host_map[kStaticStageRows];
+
+// Set-up, once per device with that device current: the device address of
+// g_static_stage.  Runs inside the first call on each device.
+int static_stage_address(kyn_ctx* c, unsigned char** out) {
+    if (c->device < 0 || c->device >= kStaticMaxDevices)
+        return set_err(c, KYN_ERR_UNSUPPORTED, "static staging supports device ordinals below 64");
+    if (!g_static_stage_addr[c->device]) {
+        unsigned char* ptr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_static_stage);
+        if (e != cudaSuccess || !ptr)
+            return set_err(c, KYN_ERR_CUDA,
+                           std::string("cudaGetSymbolAddress(static staging): ") + cudaGetErrorString(e));
+        g_static_stage_addr[c->device] = ptr;
+    }
+    *out = g_static_stage_addr[c->device];
+    return KYN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int kyn_set_loads_batch_static(kyn_ctx* c, const int* ids, int n, int which,
+                               const double* values, int on_device) {
+    if (!c || n < 0 || (n > 0 && (!ids || !values))) return KYN_ERR_INVALID;
+    if (which != KYN_LOAD_NODE_FX && which != KYN_LOAD_STATE_F)
+        return set_err(c, KYN_ERR_INVALID, "unknown load channel");
+    if (n == 0) return KYN_OK;
+    KYN_CUDA(c, cudaSetDevice(c->device));
+    std::lock_guard<std::mutex> lock(g_static_stage_mu);
+    unsigned char* base = nullptr;
+    int rc = static_stage_address(c, &base);
+    if (rc != KYN_OK) return rc;
+
+    // Copy plan on the host (same rows and offsets as kyn_set_loads_batch).
+    int nb = 0, rows = 0;
+    long long off = 0;
+    for (int i = 0; i < n; ++i) {
+        DevModel* m = find_model(c, ids[i]);
+        if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id in batch");
+        long long elem = 0;
+        for (size_t bi = 0; bi < m->host.beams.size(); ++bi) {
+            const HostBeam& b = m->host.beams[bi];
+            if (nb == kStaticStageBeams)
+                return set_err(c, KYN_ERR_INVALID,
+                               "kyn_set_loads_batch_static: more than 8192 beam elements in one call");
+            if (rows + b.N > kStaticStageRows)
+                return set_err(c, KYN_ERR_INVALID,
+                               "kyn_set_loads_batch_static: more than 262144 node rows in one call");
+            const SlabLayout L = make_slab_layout(b.N, b.Q);
+            XferBeam xb{};
+            xb.N = b.N;
+            xb.map_off = rows;
+            if (which == KYN_LOAD_NODE_FX) {
+                xb.slab_field = m->d_slab[bi] + L.fx;
+                xb.ext_off = off + elem * 6;
+                for (int k = 0; k < b.N; ++k) g_static_host_map[rows + k] = k;
+            } else {
+                xb.slab_field = m->d_slab[bi] + L.f;
+                xb.ext_off = off;
+                for (int k = 0; k < b.N; ++k) g_static_host_map[rows + k] = b.node_ids[k];
+            }
+            g_static_host_beams[nb++] = xb;
+            rows += b.N;
+            elem += b.N;
+        }
+        off += (which == KYN_LOAD_NODE_FX) ? elem * 6 : static_cast<long long>(m->host.num_nodes) * 6;
+    }
+    if (!on_device && off > kStaticStageValues)
+        return set_err(c, KYN_ERR_INVALID,
+                       "kyn_set_loads_batch_static: " + std::to_string(off) +
+                           " load values exceed the static staging maximum of 1048576 doubles");
+    if (nb == 0) return KYN_OK;
+
+    // Pageable host arrays: each copy returns once the driver holds the data,
+    // so the next call may refill them.
+    XferBeam* d_beams = reinterpret_cast<XferBeam*>(base);
+    int* d_map = reinterpret_cast<int*>(base + kStaticBeamBytes);
+    KYN_CUDA(c, cudaMemcpyAsync(d_beams, g_static_host_beams, sizeof(XferBeam) * nb,
+                                cudaMemcpyHostToDevice, c->stream));
+    KYN_CUDA(c, cudaMemcpyAsync(d_map, g_static_host_map, sizeof(int) * rows,
+                                cudaMemcpyHostToDevice, c->stream));
+    const double* src = values;
+    if (!on_device) {
+        double* d_values = reinterpret_cast<double*>(base + kStaticValuesOffset);
+        KYN_CUDA(c, cudaMemcpyAsync(d_values, values, sizeof(double) * off,
+                                    cudaMemcpyHostToDevice, c->stream));
+        src = d_values;
+    }
+    xfer_kernel<<<nb, 128, 0, c->stream>>>(d_beams, d_map, const_cast<double*>(src), 6, 1);
+    KYN_CUDA(c, cudaGetLastError());
+    c->launches++;
     return KYN_OK;
 }
 

@@ -71,6 +71,8 @@ def load_library():
                                       ctypes.c_void_p, ctypes.c_int]
     L.kyn_get_state_batch.argtypes = [ctypes.c_void_p, _ip, ctypes.c_int, ctypes.c_int,
                                       ctypes.c_void_p, ctypes.c_int]
+    L.kyn_set_loads_batch_static.argtypes = [ctypes.c_void_p, _ip, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_void_p, ctypes.c_int]
     L.kyn_ctx_stat.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
     L.kyn_ctx_stream.restype = ctypes.c_void_p
     L.kyn_ctx_stream.argtypes = [ctypes.c_void_p]
@@ -188,6 +190,14 @@ class Context:
         """Loads for many models from one array at address `ptr` (host or device)."""
         self._check(self.lib.kyn_set_loads_batch(self.h, ids.ctypes.data_as(_ip), ids.shape[0],
                                                  which, ctypes.c_void_p(ptr), int(on_device)))
+
+    def set_loads_batch_static(self, ids: np.ndarray, which: int, ptr: int,
+                               on_device: bool) -> None:
+        """set_loads_batch that allocates nothing: staging in the library's fixed
+        device array (limits and sharing rules in include/kynema_b200.h)."""
+        self._check(self.lib.kyn_set_loads_batch_static(
+            self.h, ids.ctypes.data_as(_ip), ids.shape[0], which, ctypes.c_void_p(ptr),
+            int(on_device)))
 
     def get_state_batch(self, ids: np.ndarray, field: str, ptr: int, on_device: bool) -> None:
         self._check(self.lib.kyn_get_state_batch(self.h, ids.ctypes.data_as(_ip), ids.shape[0],
