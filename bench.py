@@ -182,7 +182,7 @@ def main() -> None:
     ap.add_argument("--beams", type=int, default=4096)
     ap.add_argument("--ref-sample", type=int, default=512)
     ap.add_argument("--cpu-sample", type=int, default=1024)
-    ap.add_argument("--cpu-steps", type=int, default=100)
+    ap.add_argument("--cpu-steps", type=int, default=150)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--nodes", type=int, default=0,
                     help="uniform nodes per beam (0: the batch's U{5..21}); for profiling one bucket")

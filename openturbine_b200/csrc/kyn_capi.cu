@@ -33,7 +33,7 @@ constexpr int kBucketStreams = 8;
 struct DevModel {
     HostModel host;
     std::vector<double*> d_slab;     // per beam
-    std::vector<int> smem;           // per beam: dynamic shared memory of the step kernel
+    std::vector<int> nt;             // per beam: threads per CTA of the step kernel
     double* d_conv = nullptr;        // [kMaxNewtonIters]
     double* d_dump = nullptr;        // per-beam system dumps (recording mode)
     std::vector<size_t> dump_off;    // per beam offset into d_dump (doubles)
@@ -44,6 +44,7 @@ struct DevModel {
 
 struct Bucket {
     int cluster = 1;
+    int nt = 256;      // threads per CTA (step_kernel instance)
     int smem = 0;
     int first = 0;     // first beam in the plan's beam array
     int count = 0;     // beams
@@ -169,11 +170,21 @@ StepCoeffs make_coeffs(const kyn_step_params* p) {
     return P;
 }
 
-int beam_smem(int N, int Q, int nc, int real_bytes) { return make_smem(N, Q, nc, real_bytes).bytes; }
+// Threads per CTA for a beam: 256 when two such CTAs fit on an SM (their
+// serial phases overlap), else 512 so the one resident CTA has 16 warps.
+int beam_threads(int N, int Q, int nc, int real_bytes) {
+    const int s256 = make_smem(N, Q, nc, real_bytes, 256).bytes;
+    return (2 * (s256 + 1024) <= kSmemPerSM) ? 256 : 512;
+}
 
-// Resident CTAs per SM for a shared-memory size; the step kernel's register
-// budget (__launch_bounds__(kThreads, 2)) allows at most two.
-int ctas_per_sm(int smem) {
+int beam_smem(int N, int Q, int nc, int real_bytes, int nt) {
+    return make_smem(N, Q, nc, real_bytes, nt).bytes;
+}
+
+// Resident CTAs per SM for a thread count and shared-memory size; the step
+// kernel's register budget (128 per thread) allows two CTAs of 256 threads.
+int ctas_per_sm(int nt, int smem) {
+    if (nt == 512) return 1;
     const int per = smem + 1024;
     return std::max(1, std::min(2, kSmemPerSM / per));
 }
@@ -193,6 +204,7 @@ int get_plan(kyn_ctx* c, const int* ids, int n, Plan** out) {
     struct Entry {
         int model_index;
         int cluster;
+        int nt;
         int cls;
         int smem;
         double work;
@@ -201,17 +213,22 @@ int get_plan(kyn_ctx* c, const int* ids, int n, Plan** out) {
     for (int i = 0; i < n; ++i) {
         DevModel* m = find_model(c, ids[i]);
         if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id in step list");
-        int smem = 0;
+        int nt = 256;
         double work = 0.;
         for (size_t b = 0; b < m->host.beams.size(); ++b) {
-            smem = std::max(smem, m->smem[b]);
+            nt = std::max(nt, m->nt[b]);
             const double N = m->host.beams[b].N, Q = m->host.beams[b].Q;
             work = std::max(work, N * N * Q + 72. * (N - 1) * (N - 1) * (N - 1));
         }
-        entries.push_back({i, static_cast<int>(m->host.beams.size()), ctas_per_sm(smem), smem, work});
+        int smem = 0;
+        for (const HostBeam& hb : m->host.beams)
+            smem = std::max(smem, beam_smem(hb.N, hb.Q, hb.nc, sizeof(double), nt));
+        entries.push_back({i, static_cast<int>(m->host.beams.size()), nt, ctas_per_sm(nt, smem), smem,
+                           work});
     }
     std::stable_sort(entries.begin(), entries.end(), [](const Entry& a, const Entry& b) {
         if (a.cluster != b.cluster) return a.cluster > b.cluster;
+        if (a.nt != b.nt) return a.nt > b.nt;
         if (a.cls != b.cls) return a.cls < b.cls;
         return a.work > b.work;
     });
@@ -219,9 +236,11 @@ int get_plan(kyn_ctx* c, const int* ids, int n, Plan** out) {
     for (size_t e = 0; e < entries.size(); ++e) {
         const Entry& en = entries[e];
         if (plan->buckets.empty() || plan->buckets.back().cluster != en.cluster ||
-            ctas_per_sm(plan->buckets.back().smem) != en.cls) {
+            plan->buckets.back().nt != en.nt ||
+            ctas_per_sm(en.nt, plan->buckets.back().smem) != en.cls) {
             Bucket bk;
             bk.cluster = en.cluster;
+            bk.nt = en.nt;
             bk.first = static_cast<int>(kb.size());
             plan->buckets.push_back(bk);
         }
@@ -271,7 +290,9 @@ int get_plan(kyn_ctx* c, const int* ids, int n, Plan** out) {
 int launch_plan(kyn_ctx* c, Plan* plan, const kyn_step_params* p) {
     const StepCoeffs P = make_coeffs(p);
     if (c->smem_configured < kMaxDynSmem) {
-        KYN_CUDA(c, cudaFuncSetAttribute(step_kernel<double>,
+        KYN_CUDA(c, cudaFuncSetAttribute(step_kernel<double, 256>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
+        KYN_CUDA(c, cudaFuncSetAttribute(step_kernel<double, 512>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
         c->smem_configured = kMaxDynSmem;
     }
@@ -283,7 +304,7 @@ int launch_plan(kyn_ctx* c, Plan* plan, const kyn_step_params* p) {
         KYN_CUDA(c, cudaStreamWaitEvent(s, c->fork, 0));
         cudaLaunchConfig_t cfg{};
         cfg.gridDim = dim3(bk.count, 1, 1);
-        cfg.blockDim = dim3(kThreads, 1, 1);
+        cfg.blockDim = dim3(bk.nt, 1, 1);
         cfg.dynamicSmemBytes = bk.smem;
         cfg.stream = s;
         cudaLaunchAttribute attr[1];
@@ -296,8 +317,12 @@ int launch_plan(kyn_ctx* c, Plan* plan, const kyn_step_params* p) {
             cfg.numAttrs = 1;
         }
         const KBeam* beams = plan->d_kbeams + bk.first;
-        KYN_CUDA(c, cudaLaunchKernelEx(&cfg, step_kernel<double>, beams, P,
-                                       plan->record ? 1 : 0, plan->d_status, plan->d_iters));
+        if (bk.nt == 512)
+            KYN_CUDA(c, cudaLaunchKernelEx(&cfg, step_kernel<double, 512>, beams, P,
+                                           plan->record ? 1 : 0, plan->d_status, plan->d_iters));
+        else
+            KYN_CUDA(c, cudaLaunchKernelEx(&cfg, step_kernel<double, 256>, beams, P,
+                                           plan->record ? 1 : 0, plan->d_status, plan->d_iters));
         c->launches++;
     }
     c->last_buckets = nb;
@@ -530,10 +555,12 @@ int kyn_model_create(kyn_ctx* c, const kyn_model_desc* desc) {
     if (rc != KYN_OK) return set_err(c, rc, err);
     size_t bytes = kMaxNewtonIters * sizeof(double);
     for (auto& b : m->host.beams) {
-        const int sm = beam_smem(b.N, b.Q, b.nc, sizeof(double));
+        const int nt = beam_threads(b.N, b.Q, b.nc, sizeof(double));
+        const int sm = std::max(beam_smem(b.N, b.Q, b.nc, sizeof(double), 512),
+                                beam_smem(b.N, b.Q, b.nc, sizeof(double), nt));
         if (sm > kMaxDynSmem)
             return set_err(c, KYN_ERR_UNSUPPORTED, "beam system does not fit in shared memory");
-        m->smem.push_back(sm);
+        m->nt.push_back(nt);
         bytes += b.slab.size() * sizeof(double);
     }
     if (c->budget && c->used + bytes > c->budget)

@@ -119,15 +119,35 @@ __device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double
 }
 
 // ---- shared-memory plan of one CTA --------------------------------------------
-constexpr int kWarps = kThreads / 32;
-constexpr int kGroups = kThreads / 16;  // 16-thread groups, one quadrature point each
-constexpr int kGroupScratch = 176;      // doubles of per-group scratch for QP math
-constexpr int kPairChunk = 64;          // node pairs per integration GEMM chunk
+// The kernel runs with NT = 256 threads (two CTAs per SM, beams up to ~14 nodes)
+// or NT = 512 threads (one CTA per SM, larger beams); NT/16 quadrature points
+// are processed per pass and NT/32 warps share the GEMM-shaped phases.
+constexpr int kGroupScratch = 256;      // doubles of per-group scratch for QP math
 constexpr int kPanel = 8;               // LU panel width
-constexpr int kConStride = 96;      // doubles per constraint record in smem
+constexpr int kConStride = 96;          // doubles per constraint record in smem
+
+// Per-group scratch (doubles) of the quadrature phase.
+namespace grec {
+constexpr int interp = 0;   // [20] interpolated sums
+constexpr int rn = 20;      // [4] normalised r
+constexpr int Rx = 24;      // [9] R(r o r0)
+constexpr int Rr = 33;      // [9] R(r)
+constexpr int st = 42;      // [6] strain
+constexpr int Mu = 48;      // [36] Muu
+constexpr int ms = 84;      // mass, eta[3], s = x0'+u' [3] at 88..90
+constexpr int O12 = 92;     // [9]
+constexpr int Gu = 101;     // [18]
+constexpr int Kk = 119;     // [9]
+constexpr int fcv = 128;    // [6]
+constexpr int Cu = 136;     // [36] Cuu (rotated stiffness)
+constexpr int mstar = 172;  // [36] sectional mass (material frame), staged from HBM
+constexpr int cstar = 208;  // [36] sectional stiffness
+constexpr int r0 = 244;     // [4]
+constexpr int x0p = 248;    // [3]
+}  // namespace grec
 
 struct Smem {
-    int A;              // TR [n6][ldA]
+    int A;              // TR [n6][ldA]; aliased by the per-group QP scratch
     int G;              // double [4Q][56] weighted quadrature blocks (integration GEMM)
     int Fc, Fdig;       // double [Q][6]
     int phi, dphi;      // double [Q][N]
@@ -140,15 +160,16 @@ struct Smem {
     int xs;             // double [n6]  permuted solution
     int rpiv;           // double [n6]  reciprocal pivots
     int con;            // double [nc][kConStride]
-    int grp;            // double [kGroups][kGroupScratch]  (quadrature phase)
-    int stg;            // double [64][56] GEMM output staging (integration; aliases grp)
-    int red;            // double [2][kWarps + 8]
+    int red;            // double [2][NT/32 + 8]
     int pos;            // int [N]
     int bytes;
     int ldA;
 };
 
-__host__ __device__ inline Smem make_smem(int N, int Q, int nc, int real_bytes) {
+// The system matrix and the quadrature scratch never live at the same time:
+// A is assembled after the quadrature phase and consumed by the solve, so the
+// two share one region.
+__host__ __device__ inline Smem make_smem(int N, int Q, int nc, int real_bytes, int nt) {
     Smem S{};
     int o = 0;
     auto take = [&](int bytes) {
@@ -158,7 +179,11 @@ __host__ __device__ inline Smem make_smem(int N, int Q, int nc, int real_bytes) 
     };
     const int n6 = 6 * N;
     S.ldA = n6 + 1;
-    S.A = take(n6 * S.ldA * real_bytes);
+    {
+        const int a_bytes = n6 * S.ldA * real_bytes;
+        const int g_bytes = (nt / 16) * kGroupScratch * 8;
+        S.A = take(a_bytes > g_bytes ? a_bytes : g_bytes);
+    }
     S.G = take(4 * Q * 56 * 8);
     S.Fc = take(Q * 6 * 8);
     S.Fdig = take(Q * 6 * 8);
@@ -178,16 +203,31 @@ __host__ __device__ inline Smem make_smem(int N, int Q, int nc, int real_bytes) 
     S.xs = take(n6 * 8);
     S.rpiv = take(n6 * 8);
     S.con = take((nc > 0 ? nc : 1) * kConStride * 8);
-    {
-        const int grp_bytes = kGroups * kGroupScratch * 8;
-        const int stg_bytes = kPairChunk * 56 * 8;
-        S.grp = take(grp_bytes > stg_bytes ? grp_bytes : stg_bytes);
-        S.stg = S.grp;
-    }
-    S.red = take(2 * (kWarps + 8) * 8);
+    S.red = take(2 * (nt / 32 + 8) * 8);
     S.pos = take(N * 4);
     S.bytes = o;
     return S;
+}
+
+// Column layout of the integration GEMM's B operand G (56 columns).  The 54
+// quantities of a node pair are L[r][c] (left 6x3 block, logical r*3+c),
+// RS[r][k] (right block before the tangent, 18 + r*3+k) and RI[r][c] (right
+// inertia block, 36 + r*3+c).  m8n8k4 leaves column 8*nt + 2*s + e of a tile
+// row in lane s = lane%4, slot 2*nt + e; the layout puts the six values of
+// two right-block rows (RS and RI) in one lane, so SM_ij = C_RS T_j + C_RI is
+// formed from registers: lanes 0..2 own rows {2s, 2s+1} in slots 0..11 and two
+// L values in slots 12..13 (lane 2: padding), lane 3 owns L[0..13].
+__host__ __device__ inline int gcol_slot(int s, int t) { return 8 * (t >> 1) + 2 * s + (t & 1); }
+__host__ __device__ inline int gcol(int logical) {
+    if (logical < 18) {
+        if (logical < 14) return gcol_slot(3, logical);
+        if (logical < 16) return gcol_slot(0, 12 + logical - 14);
+        return gcol_slot(1, 12 + logical - 16);
+    }
+    const bool ri = logical >= 36;
+    const int e = logical - (ri ? 36 : 18);
+    const int r = e / 3, k = e % 3;
+    return gcol_slot(r >> 1, (r & 1) * 6 + (ri ? 3 : 0) + k);
 }
 
 // Constraint record layout inside Smem::con (doubles).
@@ -203,17 +243,20 @@ constexpr int yr = 49;     // [6] constrained-row residual b_r - A_r x
 }  // namespace conrec
 
 // ---- the kernel ------------------------------------------------------------------
-template <typename TR>
-__global__ void __launch_bounds__(kThreads, 2)
+template <typename TR, int NT>
+__global__ void __launch_bounds__(NT, (NT == 256) ? 2 : 1)
     step_kernel(const KBeam* __restrict__ beams, StepCoeffs P, int record,
                 int* __restrict__ status_out, int* __restrict__ iters_out) {
+    static_assert(NT == 256 || NT == 512, "step kernel runs with 256 or 512 threads");
+    constexpr int NW = NT / 32;  // warps
+    constexpr int NG = NT / 16;  // quadrature-point groups of 16 threads
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const KBeam& KB = beams[blockIdx.x];
     const int N = KB.N, Q = KB.Q, nc = KB.nc;
     const int n6 = 6 * N;
     const int m = 6 * (N - nc);   // free-node block size
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const Smem S = make_smem(N, Q, nc, sizeof(TR));
+    const Smem S = make_smem(N, Q, nc, sizeof(TR), NT);
     const SlabLayout L = make_slab_layout(N, Q);
     double* __restrict__ slab = KB.slab;
 
@@ -238,8 +281,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     double* xs = reinterpret_cast<double*>(smem_raw + S.xs);
     double* rpiv = reinterpret_cast<double*>(smem_raw + S.rpiv);
     double* con = reinterpret_cast<double*>(smem_raw + S.con);
-    double* gscr = reinterpret_cast<double*>(smem_raw + S.grp);
-    double* Stg = reinterpret_cast<double*>(smem_raw + S.stg);
+    double* gscr = reinterpret_cast<double*>(smem_raw + S.A);  // quadrature phase only
     double* red = reinterpret_cast<double*>(smem_raw + S.red);
     int* pos = reinterpret_cast<int*>(smem_raw + S.pos);
     __shared__ int s_flag;
@@ -263,15 +305,15 @@ __global__ void __launch_bounds__(kThreads, 2)
     };
 
     // ---- load constants and state ------------------------------------------
-    for (int k = tid; k < Q * N; k += kThreads) {
+    for (int k = tid; k < Q * N; k += NT) {
         phi[k] = slab[L.phi + k];
         dphi[k] = slab[L.dphi + k];
         dphiJ[k] = slab[L.dphiJ + k];
     }
-    for (int k = tid; k < Q * 4; k += kThreads) qpw[k] = slab[L.qpw + k];
+    for (int k = tid; k < Q * 4; k += NT) qpw[k] = slab[L.qpw + k];
 
-    for (int k = tid; k < N * 7; k += kThreads) sq[k] = slab[L.q + k];
-    for (int k = tid; k < N * 6; k += kThreads) {
+    for (int k = tid; k < N * 7; k += NT) sq[k] = slab[L.q + k];
+    for (int k = tid; k < N * 6; k += NT) {
         sv[k] = slab[L.v + k];
         svd[k] = slab[L.vd + k];
         sa[k] = slab[L.a + k];
@@ -295,8 +337,8 @@ __global__ void __launch_bounds__(kThreads, 2)
     __syncthreads();
 
     // ---- PredictNextState (src/step/predict_next_state.hpp:14-47) ------------
-    for (int k = tid; k < N * 7; k += kThreads) sqp[k] = sq[k];
-    for (int k = tid; k < N * 6; k += kThreads) {
+    for (int k = tid; k < N * 7; k += NT) sqp[k] = sq[k];
+    for (int k = tid; k < N * 6; k += NT) {
         const double v_p = sv[k], vd_p = svd[k], a_p = sa[k];
         svd[k] = 0.;
         const double an = (P.alpha_f * vd_p - P.alpha_m * a_p) / (1. - P.alpha_m);
@@ -307,7 +349,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     __syncthreads();
     // CalculateDisplacement (src/state/calculate_displacement.hpp:25-50)
     auto displacement = [&]() {
-        for (int n = tid; n < N; n += kThreads) {
+        for (int n = tid; n < N; n += NT) {
             for (int c = 0; c < 3; ++c) sq[n * 7 + c] = sqp[n * 7 + c] + h * sqd[n * 6 + c];
             const double d[3] = {h * sqd[n * 6 + 3], h * sqd[n * 6 + 4], h * sqd[n * 6 + 5]};
             double qd4[4], qn[4];
@@ -328,7 +370,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     for (int iter = 0; iter < P.max_iter; ++iter) {
         // ---- tangent operator (src/system/calculate_tangent_operator.hpp:26-65)
         // Only the rotational 3x3 block of the stored (transposed) operator is kept.
-        for (int n = tid; n < N; n += kThreads) {
+        for (int n = tid; n < N; n += NT) {
             const double rv[3] = {h * sqd[n * 6 + 3], h * sqd[n * 6 + 4], h * sqd[n * 6 + 5]};
             const double ph = sqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
             double sn, cs;
@@ -346,41 +388,46 @@ __global__ void __launch_bounds__(kThreads, 2)
         }
 
         // ---- quadrature-point values (calculate_quadrature_point_values.hpp) ---
-        // 16 threads per quadrature point; a CTA covers 16 points per pass.  Each
+        // 16 threads per quadrature point; a CTA covers NT/16 points per pass.  Each
         // stage gives every lane of a group the same formula on its own entries,
         // so the half-warps run without divergence.
         {
             const int grp = tid >> 4;
             const int g = tid & 15;
             double* gs = gscr + grp * kGroupScratch;
-            double* rn = gs + 20;   // [4] normalised r
-            double* Rx = gs + 24;   // [9] R(r o r0)
-            double* Rr = gs + 33;   // [9] R(r)
-            double* st = gs + 42;   // [6] strain
-            double* Mu = gs + 48;   // [36] Muu
-            double* ms = gs + 84;   // mass, eta[3], s = x0'+u' [3] at 88..90
-            double* O12 = gs + 92;  // [9]
-            double* Gu = gs + 101;  // [18]
-            double* Kk = gs + 119;  // [9]
-            double* fcv = gs + 128; // [6]
-            double* Cu = gs + 136;  // [36] Cuu (rotated stiffness)
-            for (int q0 = 0; q0 < Q; q0 += 16) {
+            double* rn = gs + grec::rn;
+            double* Rx = gs + grec::Rx;
+            double* Rr = gs + grec::Rr;
+            double* st = gs + grec::st;
+            double* Mu = gs + grec::Mu;
+            double* ms = gs + grec::ms;
+            double* O12 = gs + grec::O12;
+            double* Gu = gs + grec::Gu;
+            double* Kk = gs + grec::Kk;
+            double* fcv = gs + grec::fcv;
+            double* Cu = gs + grec::Cu;
+            const double* mst = gs + grec::mstar;
+            const double* cst = gs + grec::cstar;
+            const double* r0 = gs + grec::r0;
+            const double* x0p = gs + grec::x0p;
+            for (int q0 = 0; q0 < Q; q0 += NG) {
                 const int qp = q0 + grp;
                 const bool act = qp < Q;
                 const double* ph_q = phi + qp * N;
-                const double* r0 = slab + L.r0 + qp * 4;
-                const double* x0p = slab + L.x0p + qp * 3;
-                // structural zeros of this point's G rows
                 if (act) {
-                    double* Gq = G + 4 * qp * 56;
-                    for (int t = g; t < 4 * 56; t += 16) {
-                        const int mm = t / 56, col = t % 56;
-                        bool zero = col >= 54;
-                        if (mm == 1) zero |= (col < 9) || (col >= 18 && col < 27) || col >= 36;
-                        if (mm == 2) zero |= col >= 36;
-                        if (mm == 3) zero |= col < 18 || col >= 36;
-                        if (zero) Gq[t] = 0.;
+                    // stage this point's sections and reference frame from the slab
+                    // (read early: the loads overlap the interpolation below)
+                    for (int k = g; k < 79; k += 16) {
+                        double v;
+                        if (k < 36) v = slab[L.mstar + qp * 36 + k];
+                        else if (k < 72) v = slab[L.cstar + qp * 36 + (k - 36)];
+                        else if (k < 76) v = slab[L.r0 + qp * 4 + (k - 72)];
+                        else v = slab[L.x0p + qp * 3 + (k - 76)];
+                        gs[grec::mstar + k] = v;
                     }
+                    // this point's G rows start at zero (structural zeros, padding)
+                    double* Gq = G + 4 * qp * 56;
+                    for (int t = g; t < 4 * 56; t += 16) Gq[t] = 0.;
                 }
                 // (1) interpolation: r, u_ddot, omega, omega_dot, u', r'
                 if (act) {
@@ -431,8 +478,6 @@ __global__ void __launch_bounds__(kThreads, 2)
                 __syncwarp();
                 // (3) Muu = R M* R^T, Cuu = R C* R^T; translational strain
                 if (act) {
-                    const double* mst = slab + L.mstar + qp * 36;
-                    const double* cst = slab + L.cstar + qp * 36;
                     for (int o = g; o < 75; o += 16) {
                         if (o < 72) {
                             const int e = o % 36;
@@ -521,13 +566,13 @@ __global__ void __launch_bounds__(kThreads, 2)
                     double* G1 = G + (4 * qp + 1) * 56;
                     double* G3 = G + (4 * qp + 3) * 56;
                     O12[g] = o12;
-                    G3[18 + g] = w * o12;
-                    G3[18 + 9 + g] = w * o22;
-                    G1[9 + g] = w * p21;
-                    G1[18 + 9 + g] = w * p22;
+                    G3[gcol(18 + g)] = w * o12;
+                    G3[gcol(18 + 9 + g)] = w * o22;
+                    G1[gcol(9 + g)] = w * p21;
+                    G1[gcol(18 + 9 + g)] = w * p22;
                     Gu[g] = g12;
                     Gu[9 + g] = g22;
-                    G[(4 * qp) * 56 + 18 + g] = wJ * k12;
+                    G[(4 * qp) * 56 + gcol(18 + g)] = wJ * k12;
                     Kk[g] = k22;
                 } else if (act && g < 15) {
                     // Fd + Fi - Fe - Fg (calculate_force_FD.hpp, calculate_inertial_force.hpp,
@@ -575,7 +620,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                         const int i = g / 3, j = g % 3;
                         double qv = 0.;
                         for (int k = 0; k < 3; ++k) qv += tilde_e(sv3, k, i) * O12[k * 3 + j];
-                        G0[18 + 9 + g] = wJ * (Kk[g] + qv);
+                        G0[gcol(18 + 9 + g)] = wJ * (Kk[g] + qv);
                     }
                     for (int e = g; e < 36; e += 16) {
                         const int i = e / 6, j = e % 6;
@@ -583,8 +628,8 @@ __global__ void __launch_bounds__(kThreads, 2)
                         if (j >= 3) gg = Gu[(i < 3 ? 0 : 9) + (i % 3) * 3 + (j - 3)];
                         const double xi = P.beta_prime * Mu[e] + P.gamma_prime * gg;
                         const int col = (j < 3) ? i * 3 + j : 36 + i * 3 + (j - 3);
-                        G0[col] = wJ * xi;
-                        G2[(j < 3) ? i * 3 + j : 18 + i * 3 + (j - 3)] = wdJ * Cu[e];
+                        G0[gcol(col)] = wJ * xi;
+                        G2[gcol((j < 3) ? i * 3 + j : 18 + i * 3 + (j - 3))] = wdJ * Cu[e];
                     }
                 }
                 __syncwarp();
@@ -594,7 +639,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         mark(kPhaseQuadrature);
 
         // ---- residual integration (integrate_residual_vector.hpp:33-50) ----------
-        for (int t = tid; t < N * 6; t += kThreads) {
+        for (int t = tid; t < N * 6; t += NT) {
             const int n = t / 6, c = t % 6;
             double acc = 0.;
             for (int qp = 0; qp < Q; ++qp) {
@@ -612,60 +657,74 @@ __global__ void __launch_bounds__(kThreads, 2)
         //      weighted blocks written by the quadrature phase (K/inertia, P, C, O
         //      terms).  C_ij holds [S+I left | S right | I right]; then
         //      SM_ij = [C_L | C_RS T_j + C_RI] (T_j is identity on the translational
-        //      block).  The pair GEMM runs on the FP64 tensor cores: each warp owns 8
-        //      pairs and all 7 column tiles, one k-step of 4 (m = 0..3) per point.
+        //      block).  The pair GEMM runs on the FP64 tensor cores: each warp owns
+        //      tiles of 8 pairs and all 7 column tiles, one k-step of 4 (m = 0..3) per
+        //      point, and writes SM_ij from its accumulators (column layout: gcol).
         __syncthreads();
-        const int P2 = N * N;
-        for (int p0 = 0; p0 < P2; p0 += kPairChunk) {
-            {
-                const int prow = p0 + 8 * warp + (lane >> 2);
+        {
+            const int P2 = N * N;
+            const int s4 = lane & 3;
+            const int mm = lane & 3;
+            const double* fi_tab = (mm < 2) ? phi : dphi;
+            const double* fj_tab = (mm == 0 || mm == 3) ? phi : dphi;
+            const double cond = P.conditioner;
+            for (int p0 = 8 * warp; p0 < P2; p0 += 8 * NW) {
+                const int prow = p0 + (lane >> 2);
                 const bool valid = prow < P2;
                 const int i = valid ? prow / N : 0, jn = valid ? prow % N : 0;
-                const int mm = lane & 3;
-                const double* fi_tab = (mm < 2) ? phi : dphi;
-                const double* fj_tab = (mm == 0 || mm == 3) ? phi : dphi;
                 double acc[7][2];
 #pragma unroll
                 for (int nt = 0; nt < 7; ++nt) acc[nt][0] = acc[nt][1] = 0.;
-                if (p0 + 8 * warp < P2) {
-                    for (int q = 0; q < Q; ++q) {
-                        const double a = valid ? fi_tab[q * N + i] * fj_tab[q * N + jn] : 0.;
-                        const double* gq = G + (4 * q + (lane & 3)) * 56 + (lane >> 2);
+                for (int q = 0; q < Q; ++q) {
+                    const double av = valid ? fi_tab[q * N + i] * fj_tab[q * N + jn] : 0.;
+                    const double* gq = G + (4 * q + (lane & 3)) * 56 + (lane >> 2);
 #pragma unroll
-                        for (int nt = 0; nt < 7; ++nt) dmma884(acc[nt][0], acc[nt][1], a, gq[nt * 8]);
+                    for (int nt = 0; nt < 7; ++nt) dmma884(acc[nt][0], acc[nt][1], av, gq[nt * 8]);
+                }
+                if (valid) {
+                    TR* Arow = A + (6 * pos[i]) * ldA + 6 * pos[jn];
+                    if (s4 < 3) {
+                        const double* Tj = sT + jn * 9;
+#pragma unroll
+                        for (int rr = 0; rr < 2; ++rr) {
+                            const int r = 2 * s4 + rr;
+                            // slots 6rr..6rr+2: RS[r][0..2]; 6rr+3..6rr+5: RI[r][0..2]
+                            double rs[3], ri[3];
+#pragma unroll
+                            for (int k = 0; k < 3; ++k) {
+                                rs[k] = acc[(6 * rr + k) >> 1][(6 * rr + k) & 1];
+                                ri[k] = acc[(6 * rr + 3 + k) >> 1][(6 * rr + 3 + k) & 1];
+                            }
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) {
+                                double val = ri[c];
+#pragma unroll
+                                for (int k = 0; k < 3; ++k) val += rs[k] * Tj[k * 3 + c];
+                                Arow[r * ldA + 3 + c] = static_cast<TR>(val * cond);
+                            }
+                        }
+                        if (s4 < 2) {
+                            // slots 12, 13: L[14 + 2 s4 + e]
+#pragma unroll
+                            for (int e = 0; e < 2; ++e) {
+                                const int l = 14 + 2 * s4 + e;
+                                Arow[(l / 3) * ldA + l % 3] = static_cast<TR>(acc[6][e] * cond);
+                            }
+                        }
+                    } else {
+                        // slots 0..13: L[0..13]
+#pragma unroll
+                        for (int t = 0; t < 14; ++t)
+                            Arow[(t / 3) * ldA + t % 3] = static_cast<TR>(acc[t >> 1][t & 1] * cond);
                     }
                 }
-                double* cw = Stg + (8 * warp + (lane >> 2)) * 56 + 2 * (lane & 3);
-#pragma unroll
-                for (int nt = 0; nt < 7; ++nt) {
-                    cw[nt * 8] = acc[nt][0];
-                    cw[nt * 8 + 1] = acc[nt][1];
-                }
             }
-            __syncthreads();
-            const int np = min(kPairChunk, P2 - p0);
-            for (int t = tid; t < np * 36; t += kThreads) {
-                const int pl = t / 36, e = t % 36, r = e / 6, c = e % 6;
-                const int pr = p0 + pl;
-                const int i = pr / N, jn = pr % N;
-                const double* cr = Stg + pl * 56;
-                double val;
-                if (c < 3) {
-                    val = cr[r * 3 + c];
-                } else {
-                    const double* Tj = sT + jn * 9;
-                    val = cr[36 + r * 3 + (c - 3)];
-                    for (int k = 0; k < 3; ++k) val += cr[18 + r * 3 + k] * Tj[k * 3 + (c - 3)];
-                }
-                A[(6 * pos[i] + r) * ldA + 6 * pos[jn] + c] = static_cast<TR>(val * P.conditioner);
-            }
-            __syncthreads();
         }
         __syncthreads();
         mark(kPhaseIntegrate);
 
         // ---- constraints (calculate_constraint_residual_gradient.hpp:60-199) -------
-        if (warp == kWarps - 1 && lane < nc) {
+        if (warp == NW - 1 && lane < nc) {
             double* cr = con + lane * kConStride;
             const int tn = KB.con_node[lane];
             const double* nu = sq + tn * 7;
@@ -715,7 +774,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 
         // ---- right-hand side: b = -cond (-f + R + G^T lambda) (assemble_system_residual.hpp,
         //      solve_system.hpp:20-24) in permuted order --------------------------------
-        for (int t = tid; t < n6; t += kThreads) {
+        for (int t = tid; t < n6; t += NT) {
             const int n = t / 6, c = t % 6;
             double val = -slab[L.f + t] + resid[t];
             for (int k = 0; k < nc; ++k)
@@ -727,17 +786,17 @@ __global__ void __launch_bounds__(kThreads, 2)
             // matrix [nl][nl], then rhs [nl], then solution [nl]; nl = n6 + 6 nc.
             const int nl = n6 + 6 * nc;
             double* D = KB.dump;
-            for (int t = tid; t < nl * nl; t += kThreads) D[t] = 0.;
+            for (int t = tid; t < nl * nl; t += NT) D[t] = 0.;
         }
         __syncthreads();
         if (record && KB.dump) {
             const int nl = n6 + 6 * nc;
             double* D = KB.dump;
-            for (int t = tid; t < n6 * n6; t += kThreads) {
+            for (int t = tid; t < n6 * n6; t += NT) {
                 const int r = t / n6, c = t % n6;
                 D[r * nl + c] = static_cast<double>(A[(6 * pos[r / 6] + r % 6) * ldA + 6 * pos[c / 6] + c % 6]);
             }
-            for (int t = tid; t < n6; t += kThreads) D[nl * nl + t] = bp[6 * pos[t / 6] + t % 6];
+            for (int t = tid; t < n6; t += NT) D[nl * nl + t] = bp[6 * pos[t / 6] + t % 6];
             if (tid < nc) {
                 const double* cr = con + tid * kConStride;
                 const int tn = KB.con_node[tid];
@@ -771,7 +830,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         }
         __syncthreads();
         // (S2) free-row right-hand side, folded into column m of A
-        for (int i = tid; i < m; i += kThreads) {
+        for (int i = tid; i < m; i += NT) {
             double r = bp[i];
             for (int j = m; j < n6; ++j) r -= static_cast<double>(A[i * ldA + j]) * xs[j];
             A[i * ldA + m] = static_cast<TR>(r);
@@ -814,12 +873,13 @@ __global__ void __launch_bounds__(kThreads, 2)
                         if (c < kb) A[(k0 + lane) * ldA + k0 + c] = static_cast<TR>(v[c]);
             }
             __syncthreads();
+            mark(kPhaseLUDiag);
             // (b) panel rows below the block (L21 = A21 U11^{-1}) and U12 = L11^{-1} A12
             //     (rhs column included), one row or column per thread
             {
                 const int nrow = m - (k0 + kb);
                 const int ncol = m + 1 - (k0 + kb);
-                for (int t = tid; t < nrow + ncol; t += kThreads) {
+                for (int t = tid; t < nrow + ncol; t += NT) {
                     double u[kPanel];
                     if (t < nrow) {
                         const int i = k0 + kb + t;
@@ -849,6 +909,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                 }
             }
             __syncthreads();
+            mark(kPhaseLUPanel);
             // (c) trailing update A22 -= L21 U12: 8x8 tiles on the FP64 tensor cores
             //     (two k-steps of 4 over the panel); rows/cols >= m are masked.
             //     The rhs column is updated by the first threads.
@@ -856,7 +917,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             const int R = m - r0;
             if (R > 0) {
                 const int RT = (R + 7) / 8;
-                for (int rt = warp; rt < RT; rt += kWarps) {
+                for (int rt = warp; rt < RT; rt += NW) {
                     const int row = r0 + 8 * rt + (lane >> 2);
                     double a[kPanel / 4];
 #pragma unroll
@@ -880,7 +941,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                         if (row < m && col + 1 < m) A[row * ldA + col + 1] = static_cast<TR>(d1);
                     }
                 }
-                for (int i = r0 + tid; i < m; i += kThreads) {
+                for (int i = r0 + tid; i < m; i += NT) {
                     double y = static_cast<double>(A[i * ldA + m]);
                     for (int pk = 0; pk < kb; ++pk)
                         y -= static_cast<double>(A[i * ldA + k0 + pk]) *
@@ -889,10 +950,10 @@ __global__ void __launch_bounds__(kThreads, 2)
                 }
             }
             __syncthreads();
+            mark(kPhaseFactor);
         }
-        mark(kPhaseFactor);
         // (S4) blocked back substitution U x = y (y in column m)
-        for (int i = tid; i < m; i += kThreads) xs[i] = static_cast<double>(A[i * ldA + m]);
+        for (int i = tid; i < m; i += NT) xs[i] = static_cast<double>(A[i * ldA + m]);
         __syncthreads();
         for (int k0 = ((m - 1) / kPanel) * kPanel; k0 >= 0 && m > 0; k0 -= kPanel) {
             const int kb = min(kPanel, m - k0);
@@ -906,7 +967,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                 if (lane < kb) xs[k0 + lane] = xv;
             }
             __syncthreads();
-            for (int i = tid; i < k0; i += kThreads) {
+            for (int i = tid; i < k0; i += NT) {
                 double sacc = xs[i];
                 for (int t = 0; t < kb; ++t)
                     sacc -= static_cast<double>(A[i * ldA + k0 + t]) * xs[k0 + t];
@@ -915,7 +976,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             __syncthreads();
         }
         // (S5) multipliers from the constrained rows: grad^T x_l = b_r - A_r x
-        for (int rowi = warp; rowi < 6 * nc; rowi += kWarps) {
+        for (int rowi = warp; rowi < 6 * nc; rowi += NW) {
             const int c = rowi / 6, k = rowi % 6;
             const int pr = 6 * pos[KB.con_node[c]];
             double sacc = 0.;
@@ -937,7 +998,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         if (record && KB.dump) {
             const int nl = n6 + 6 * nc;
             double* D = KB.dump + nl * nl + nl;
-            for (int t = tid; t < n6; t += kThreads) D[t] = xs[6 * pos[t / 6] + t % 6];
+            for (int t = tid; t < n6; t += NT) D[t] = xs[6 * pos[t / 6] + t % 6];
             if (tid < nc)
                 for (int k = 0; k < 6; ++k) D[n6 + 6 * tid + k] = con[tid * kConStride + conrec::xl + k];
         }
@@ -947,7 +1008,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 
         // ---- convergence error (calculate_error_sum_squares.hpp:33-79) --------------
         double part = 0.;
-        for (int t = tid; t < n6; t += kThreads) {
+        for (int t = tid; t < n6; t += NT) {
             const double pi = xs[6 * pos[t / 6] + t % 6];
             const double xi = sqd[t] * h;
             const double e = pi / (P.atol + P.rtol * fabs(xi));
@@ -961,14 +1022,14 @@ __global__ void __launch_bounds__(kThreads, 2)
             part += e * e;
         }
         for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-        double* slot = red + (iter & 1) * (kWarps + 8);
+        double* slot = red + (iter & 1) * (NW + 8);
         if (lane == 0) slot[warp] = part;
         __syncthreads();
         if (tid == 0) {
             double s = 0.;
-            for (int w2 = 0; w2 < kWarps; ++w2) s += slot[w2];
-            slot[kWarps] = s;
-            slot[kWarps + 1] = static_cast<double>(s_flag);
+            for (int w2 = 0; w2 < NW; ++w2) s += slot[w2];
+            slot[NW] = s;
+            slot[NW + 1] = static_cast<double>(s_flag);
         }
         double total, flags;
         if (clustered) {
@@ -977,13 +1038,13 @@ __global__ void __launch_bounds__(kThreads, 2)
             flags = 0.;
             for (int r = 0; r < KB.model_beams; ++r) {
                 const double* peer = cluster.map_shared_rank(slot, r);
-                total += peer[kWarps];
-                flags = fmax(flags, peer[kWarps + 1]);
+                total += peer[NW];
+                flags = fmax(flags, peer[NW + 1]);
             }
         } else {
             __syncthreads();
-            total = slot[kWarps];
-            flags = slot[kWarps + 1];
+            total = slot[NW];
+            flags = slot[NW + 1];
         }
         const double err = sqrt(total / static_cast<double>(KB.model_dofs));
         if (KB.rank == 0 && tid == 0 && iter < kMaxNewtonIters) KB.conv[iter] = err;
@@ -991,7 +1052,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 
         // ---- update (update_dynamic_prediction.hpp, calculate_displacement.hpp,
         //      update_lambda_prediction.hpp) ----------------------------------------------
-        for (int t = tid; t < n6; t += kThreads) {
+        for (int t = tid; t < n6; t += NT) {
             const double delta = xs[6 * pos[t / 6] + t % 6];
             sqd[t] += delta / h;
             if (P.dynamic) {
@@ -1025,21 +1086,21 @@ __global__ void __launch_bounds__(kThreads, 2)
     // ---- post-step (step.hpp:86-121) ---------------------------------------------------
     if (status == KYN_OK) {
         const double fac = (1. - P.alpha_f) / (1. - P.alpha_m);
-        for (int t = tid; t < n6; t += kThreads) sa[t] += fac * svd[t];
+        for (int t = tid; t < n6; t += NT) sa[t] += fac * svd[t];
     }
     __syncthreads();
-    for (int k = tid; k < N * 7; k += kThreads) {
+    for (int k = tid; k < N * 7; k += NT) {
         slab[L.q + k] = sq[k];
         slab[L.q_prev + k] = sqp[k];
     }
-    for (int k = tid; k < N * 6; k += kThreads) {
+    for (int k = tid; k < N * 6; k += NT) {
         slab[L.v + k] = sv[k];
         slab[L.vd + k] = svd[k];
         slab[L.a + k] = sa[k];
         slab[L.q_delta + k] = sqd[k];
     }
     if (status == KYN_OK) {
-        for (int n = tid; n < N; n += kThreads) {
+        for (int n = tid; n < N; n += NT) {
             const double* x0 = slab + L.x0 + n * 7;
             for (int c = 0; c < 3; ++c) slab[L.x + n * 7 + c] = x0[c] + sq[n * 7 + c];
             double r[4];
@@ -1047,7 +1108,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             for (int c = 0; c < 4; ++c) slab[L.x + n * 7 + 3 + c] = r[c];
         }
     }
-    for (int k = tid; k < N * 9; k += kThreads) slab[L.tangent + k] = sT[k];
+    for (int k = tid; k < N * 9; k += NT) slab[L.tangent + k] = sT[k];
     if (tid < 6 * nc) {
         const double* cr = con + (tid / 6) * kConStride;
         slab[L.lambda + tid] = cr[conrec::lam + tid % 6];

@@ -102,7 +102,10 @@ enum Phase {
     kPhaseSubstitute = 6,   // back substitution + multipliers
     kPhaseUpdate = 7,       // convergence error + Newton update
     kPhaseStore = 8,        // post-step and write-back
-    kNumPhases = 9
+    kPhaseLUDiag = 9,       // LU: diagonal-block factorisation (part of the factor phase)
+    kPhaseLUPanel = 10,     // LU: panel solves (part of the factor phase)
+    kPhaseIntEpilogue = 11, // integration: S T + I epilogue into A (part of integrate)
+    kNumPhases = 12
 };
 
 // Step coefficients (src/step/step_parameters.hpp:37-52).
