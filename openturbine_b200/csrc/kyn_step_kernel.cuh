@@ -97,18 +97,6 @@ __device__ inline bool solve3(const double* M, const double* r, double* y) {
     return true;
 }
 
-// Reciprocal of a pivot: single-precision estimate refined by two Newton-Raphson
-// steps r <- r + r (1 - d r) (quadratic convergence: 1e-7 -> 1e-14 -> below
-// double rounding).  Falls back to division outside the float range.
-__device__ __forceinline__ double pivot_rcp(double d) {
-    const float f = static_cast<float>(d);
-    if (!(fabsf(f) > 1e-30f && fabsf(f) < 1e30f)) return 1. / d;
-    double r = static_cast<double>(__frcp_rn(f));
-    r = fma(r, fma(-d, r, 1.), r);
-    r = fma(r, fma(-d, r, 1.), r);
-    return r;
-}
-
 // FP64 tensor-core product D += A B for one 8x8x4 tile (mma.sync m8n8k4 .f64).
 // Fragment layout per lane l: a = A[l/4][l%4], b = B[l%4][l/4],
 // d0/d1 = D[l/4][2(l%4)] / D[l/4][2(l%4)+1].
@@ -241,6 +229,243 @@ constexpr int lam = 36;    // [6] lambda
 constexpr int inp = 42;    // [7] prescribed input
 constexpr int yr = 49;     // [6] constrained-row residual b_r - A_r x
 }  // namespace conrec
+
+// ---- dense LU pieces (free block of the beam system, FP64 in shared memory) ------
+// Reciprocal of a pivot: hardware approximation refined by two Newton-Raphson
+// steps r <- r + r (1 - d r) (each step squares the relative error).
+__device__ __forceinline__ double pivot_rcp(double d) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+    r = fma(r, fma(-d, r, 1.), r);
+    r = fma(r, fma(-d, r, 1.), r);
+    return r;
+}
+
+// Warp-level factorisation of the kb x kb diagonal block of the panel of
+// columns [p0, p0+kb): lane r holds row p0+r; pivots broadcast by shuffles.
+template <typename TR>
+__device__ __forceinline__ void factor_diag(TR* A, int ldA, int m, int p0, double* rpiv, int lane,
+                                            int* flag) {
+    const int kb = min(kPanel, m - p0);
+    double v[kPanel];
+#pragma unroll
+    for (int c = 0; c < kPanel; ++c)
+        v[c] = (lane < kb && c < kb) ? static_cast<double>(A[(p0 + lane) * ldA + p0 + c]) : 0.;
+#pragma unroll
+    for (int j = 0; j < kPanel; ++j) {
+        if (j < kb) {
+            const double d = __shfl_sync(0xffffffffu, v[j], j);
+            double u[kPanel];
+#pragma unroll
+            for (int c = j + 1; c < kPanel; ++c) u[c] = __shfl_sync(0xffffffffu, v[c], j);
+            const double rp = pivot_rcp(d);
+            if (lane == 0) {
+                rpiv[p0 + j] = rp;
+                if (!(fabs(d) > 0.) || !isfinite(rp)) *flag |= 2;
+            }
+            if (lane > j) {
+                const double l = v[j] * rp;
+                v[j] = l;
+#pragma unroll
+                for (int c = j + 1; c < kPanel; ++c) v[c] -= l * u[c];
+            }
+        }
+    }
+    if (lane < kb) {
+#pragma unroll
+        for (int c = 0; c < kPanel; ++c)
+            if (c < kb) A[(p0 + lane) * ldA + p0 + c] = static_cast<TR>(v[c]);
+    }
+}
+
+// L21 = A21 U11^{-1} for rows [r_begin, m) of the panel [p0, p0+kb), rows
+// strided by `stride` starting at r_begin + idx.
+template <typename TR>
+__device__ __forceinline__ void solve_l21(TR* A, int ldA, int m, int p0, const double* rpiv,
+                                          int r_begin, int idx, int stride) {
+    const int kb = min(kPanel, m - p0);
+#pragma unroll 2
+    for (int r = r_begin + idx; r < m; r += stride) {
+        double u[kPanel];
+#pragma unroll
+        for (int c = 0; c < kPanel; ++c) u[c] = (c < kb) ? static_cast<double>(A[r * ldA + p0 + c]) : 0.;
+#pragma unroll
+        for (int j = 0; j < kPanel; ++j) {
+            if (j < kb) {
+                u[j] *= rpiv[p0 + j];
+#pragma unroll
+                for (int k = j + 1; k < kPanel; ++k)
+                    if (k < kb) u[k] -= u[j] * static_cast<double>(A[(p0 + j) * ldA + p0 + k]);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < kPanel; ++c)
+            if (c < kb) A[r * ldA + p0 + c] = static_cast<TR>(u[c]);
+    }
+}
+
+// Warp-level factorisation of the panel of columns [p0, p0+kb): diagonal
+// block, then L21 for the rows below (one row per lane per pass).
+template <typename TR>
+__device__ __forceinline__ void factor_panel(TR* A, int ldA, int m, int p0, double* rpiv, int lane,
+                                             int* flag) {
+    factor_diag(A, ldA, m, p0, rpiv, lane, flag);
+    __syncwarp();
+    solve_l21(A, ldA, m, p0, rpiv, p0 + min(kPanel, m - p0), lane, 32);
+}
+
+// One warp applies panel [k0, k0+kb) to the column tile [c0, c0+8) (columns
+// beyond m masked) for rows [rb0, rb1): U12 = L11^{-1} A12 for the tile, then
+// A22 -= L21 U12 on the FP64 tensor cores (8x8x4 tiles, two k-steps).
+// Where U12 goes:
+//   kU12InPlace  - lanes 0..7 solve one column each and overwrite A12 (the
+//                  tile of U12 is part of the factorisation);
+//   kU12ToStage  - same, but into stage[8][8]; the caller copies it into A once
+//                  no other warp reads that A12 tile any more;
+//   kU12InRegs   - every lane solves column c0 + lane/4 in registers and
+//                  nothing is written (a helper warp on rows of a tile whose
+//                  U12 another warp stores).
+enum U12Mode { kU12InPlace = 0, kU12ToStage = 1, kU12InRegs = 2 };
+
+template <int kMode, typename TR>
+__device__ __forceinline__ void update_tile(TR* A, int ldA, int m, int k0, int kb, int c0, int rb0,
+                                            int rb1, double* stage, int lane) {
+    const int r0 = k0 + kb;
+    const int s4 = lane & 3;
+    const int kk0 = k0 + s4, kk1 = k0 + 4 + s4;
+    double b0, b1;
+    if (kMode != kU12InRegs) {
+        if (lane < 8 && c0 + lane <= m) {
+            const int c = c0 + lane;
+            double u[kPanel];
+#pragma unroll
+            for (int j = 0; j < kPanel; ++j) u[j] = (j < kb) ? static_cast<double>(A[(k0 + j) * ldA + c]) : 0.;
+#pragma unroll
+            for (int q = 0; q < kPanel - 1; ++q) {
+#pragma unroll
+                for (int j = q + 1; j < kPanel; ++j)
+                    if (j < kb) u[j] -= static_cast<double>(A[(k0 + j) * ldA + k0 + q]) * u[q];
+            }
+            if (kMode == kU12InPlace) {
+#pragma unroll
+                for (int j = 1; j < kPanel; ++j)
+                    if (j < kb) A[(k0 + j) * ldA + c] = static_cast<TR>(u[j]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < kPanel; ++j) stage[j * 8 + lane] = u[j];
+            }
+        }
+        __syncwarp();
+        const int bcol = c0 + (lane >> 2);
+        const bool bok = bcol <= m;
+        if (kMode == kU12InPlace) {
+            b0 = (kk0 < r0 && bok) ? static_cast<double>(A[kk0 * ldA + bcol]) : 0.;
+            b1 = (kk1 < r0 && bok) ? static_cast<double>(A[kk1 * ldA + bcol]) : 0.;
+        } else {
+            b0 = (kk0 < r0 && bok) ? stage[s4 * 8 + (lane >> 2)] : 0.;
+            b1 = (kk1 < r0 && bok) ? stage[(4 + s4) * 8 + (lane >> 2)] : 0.;
+        }
+    } else {
+        const int col = c0 + (lane >> 2);
+        const bool cok = col <= m;
+        double u[kPanel];
+#pragma unroll
+        for (int j = 0; j < kPanel; ++j)
+            u[j] = (j < kb && cok) ? static_cast<double>(A[(k0 + j) * ldA + (cok ? col : c0)]) : 0.;
+#pragma unroll
+        for (int q = 0; q < kPanel - 1; ++q) {
+#pragma unroll
+            for (int j = q + 1; j < kPanel; ++j)
+                if (j < kb) u[j] -= static_cast<double>(A[(k0 + j) * ldA + k0 + q]) * u[q];
+        }
+        b0 = u[0];
+        b1 = u[4];
+#pragma unroll
+        for (int t = 1; t < 4; ++t) {
+            b0 = (s4 == t) ? u[t] : b0;
+            b1 = (s4 == t) ? u[4 + t] : b1;
+        }
+        if (kk0 >= r0) b0 = 0.;
+        if (kk1 >= r0) b1 = 0.;
+    }
+    const int dcol = c0 + 2 * s4;
+    const bool c0ok = dcol <= m, c1ok = dcol + 1 <= m;
+#pragma unroll 2
+    for (int rb = rb0; rb < rb1; rb += 8) {
+        const int row = rb + (lane >> 2);
+        const bool rv = row < rb1;
+        const double a0 = (rv && kk0 < r0) ? -static_cast<double>(A[row * ldA + kk0]) : 0.;
+        const double a1 = (rv && kk1 < r0) ? -static_cast<double>(A[row * ldA + kk1]) : 0.;
+        double d0 = (rv && c0ok) ? static_cast<double>(A[row * ldA + dcol]) : 0.;
+        double d1 = (rv && c1ok) ? static_cast<double>(A[row * ldA + dcol + 1]) : 0.;
+        dmma884(d0, d1, a0, b0);
+        dmma884(d0, d1, a1, b1);
+        if (rv && c0ok) A[row * ldA + dcol] = static_cast<TR>(d0);
+        if (rv && c1ok) A[row * ldA + dcol + 1] = static_cast<TR>(d1);
+    }
+}
+
+// Replaces the kb x kb upper-triangular diagonal block of panel p0 (pivots in
+// rpiv) by its inverse; lane j < kb computes column j by back substitution
+// (lanes >= kb compute on padding and store nothing).
+template <typename TR>
+__device__ __forceinline__ void invert_diag_block(TR* A, int ldA, int m, int p0, const double* rpiv,
+                                                  int lane) {
+    const int kb = min(kPanel, m - p0);
+    const int jc = lane & 7;
+    double x[kPanel];
+#pragma unroll
+    for (int i = 0; i < kPanel; ++i) x[i] = (i == jc) ? 1. : 0.;
+#pragma unroll
+    for (int c = kPanel - 1; c >= 0; --c) {
+        if (c < kb) {  // warp-uniform; x[c] = 0 for c > jc, so no lane test is needed
+            x[c] *= rpiv[p0 + c];
+#pragma unroll
+            for (int i = 0; i < c; ++i) x[i] = fma(-static_cast<double>(A[(p0 + i) * ldA + p0 + c]), x[c], x[i]);
+        }
+    }
+    __syncwarp();
+    if (lane < kb) {
+#pragma unroll
+        for (int i = 0; i < kPanel; ++i)
+            if (i <= lane) A[(p0 + i) * ldA + p0 + lane] = static_cast<TR>(x[i]);
+    }
+}
+
+// Block back substitution U x = y by one warp (y in column m), with the
+// diagonal blocks already inverted: x_b = U_bb^{-1} y_b, then the rows above
+// the block take y_i -= U_i,b x_b.
+template <typename TR>
+__device__ __forceinline__ void back_substitute_blocked(const TR* A, int ldA, int m, double* xs, int lane) {
+    for (int i = lane; i < m; i += 32) xs[i] = static_cast<double>(A[i * ldA + m]);
+    __syncwarp();
+    const int nblk = (m + kPanel - 1) / kPanel;
+    for (int b = nblk - 1; b >= 0; --b) {
+        const int k0 = b * kPanel, kb = min(kPanel, m - k0);
+        double xv = 0.;
+        if (lane < kb) {
+#pragma unroll
+            for (int c = 0; c < kPanel; ++c)
+                if (c >= lane && c < kb)
+                    xv += static_cast<double>(A[(k0 + lane) * ldA + k0 + c]) * xs[k0 + c];
+        }
+        __syncwarp();
+        if (lane < kb) xs[k0 + lane] = xv;
+        __syncwarp();
+        double xb[kPanel];
+#pragma unroll
+        for (int c = 0; c < kPanel; ++c) xb[c] = (c < kb) ? xs[k0 + c] : 0.;
+#pragma unroll 2
+        for (int i = lane; i < k0; i += 32) {
+            double acc = xs[i];
+#pragma unroll
+            for (int c = 0; c < kPanel; ++c)
+                if (c < kb) acc -= static_cast<double>(A[i * ldA + k0 + c]) * xb[c];
+            xs[i] = acc;
+        }
+        __syncwarp();
+    }
+}
 
 // ---- the kernel ------------------------------------------------------------------
 template <typename TR, int NT>
@@ -837,144 +1062,41 @@ __global__ void __launch_bounds__(NT, (NT == 256) ? 2 : 1)
         }
         __syncthreads();
         mark(kPhaseEliminate);
-        // (S3) blocked LU without pivoting of the free block A[0:m][0:m]; the
-        //      right-hand side in column m is eliminated with it.  Multipliers
-        //      are stored scaled; rpiv keeps the reciprocal pivots.
-        for (int k0 = 0; k0 < m; k0 += kPanel) {
-            const int kb = min(kPanel, m - k0);
-            // (a) diagonal block L11 U11 (kb x kb) by warp 0: lane r holds row k0+r in
-            //     registers; pivot rows are broadcast with shuffles.
-            if (warp == 0) {
-                double v[kPanel];
-#pragma unroll
-                for (int c = 0; c < kPanel; ++c)
-                    v[c] = (lane < kb && c < kb) ? static_cast<double>(A[(k0 + lane) * ldA + k0 + c]) : 0.;
-#pragma unroll
-                for (int j = 0; j < kPanel; ++j) {
-                    if (j < kb) {
-                        const double d = __shfl_sync(0xffffffffu, v[j], j);
-                        const double rp = pivot_rcp(d);
-                        if (lane == 0) {
-                            rpiv[k0 + j] = rp;
-                            if (!(fabs(d) > 0.)) s_flag |= 2;
-                        }
-                        const double l = v[j] * rp;
-#pragma unroll
-                        for (int c = j + 1; c < kPanel; ++c) {
-                            const double u = __shfl_sync(0xffffffffu, v[c], j);
-                            if (lane > j) v[c] -= l * u;
-                        }
-                        if (lane > j) v[j] = l;
-                    }
-                }
-                if (lane < kb)
-#pragma unroll
-                    for (int c = 0; c < kPanel; ++c)
-                        if (c < kb) A[(k0 + lane) * ldA + k0 + c] = static_cast<TR>(v[c]);
-            }
+        // (S3) LU without pivoting of the free block A[0:m][0:m]; the right-hand
+        //      side in column m is eliminated with it.  Right-looking with panels
+        //      of kPanel columns and one CTA barrier per panel: warp 0 updates the
+        //      next panel's columns and factors that panel (look-ahead) while the
+        //      other warps apply the current panel to the columns right of it.
+        //      Multipliers are stored scaled; rpiv keeps the reciprocal pivots.
+        if (m > 0) {
+            if (warp == 0) factor_panel(A, ldA, m, 0, rpiv, lane, &s_flag);
             __syncthreads();
-            mark(kPhaseLUDiag);
-            // (b) panel rows below the block (L21 = A21 U11^{-1}) and U12 = L11^{-1} A12
-            //     (rhs column included), one row or column per thread
-            {
-                const int nrow = m - (k0 + kb);
-                const int ncol = m + 1 - (k0 + kb);
-                for (int t = tid; t < nrow + ncol; t += NT) {
-                    double u[kPanel];
-                    if (t < nrow) {
-                        const int i = k0 + kb + t;
-#pragma unroll
-                        for (int j = 0; j < kPanel; ++j) {
-                            if (j < kb) {
-                                double a = static_cast<double>(A[i * ldA + k0 + j]);
-                                for (int q2 = 0; q2 < j; ++q2)
-                                    a -= u[q2] * static_cast<double>(A[(k0 + q2) * ldA + k0 + j]);
-                                u[j] = a * rpiv[k0 + j];
-                                A[i * ldA + k0 + j] = static_cast<TR>(u[j]);
-                            }
-                        }
-                    } else {
-                        const int c = k0 + kb + (t - nrow);
-#pragma unroll
-                        for (int j = 0; j < kPanel; ++j) {
-                            if (j < kb) {
-                                double a = static_cast<double>(A[(k0 + j) * ldA + c]);
-                                for (int q2 = 0; q2 < j; ++q2)
-                                    a -= static_cast<double>(A[(k0 + j) * ldA + k0 + q2]) * u[q2];
-                                u[j] = a;
-                                if (j > 0) A[(k0 + j) * ldA + c] = static_cast<TR>(a);
-                            }
-                        }
+            for (int k0 = 0; k0 < m; k0 += kPanel) {
+                const int kb = min(kPanel, m - k0);
+                const int r0 = k0 + kb;
+                const int nct = (m + 1 - r0 + 7) / 8;  // column tiles of [r0, m], rhs included
+                if (warp == 0) {
+                    update_tile<kU12InPlace>(A, ldA, m, k0, kb, r0, r0, m, nullptr, lane);
+                    mark(kPhaseLUDiag);
+                    if (r0 < m) {
+                        __syncwarp();
+                        factor_panel(A, ldA, m, r0, rpiv, lane, &s_flag);
                     }
+                    mark(kPhaseLUPanel);
+                } else {
+                    for (int ct = warp; ct < nct; ct += NW - 1)
+                        update_tile<kU12InPlace>(A, ldA, m, k0, kb, r0 + 8 * ct, r0, m, nullptr, lane);
                 }
+                __syncthreads();
+                mark(kPhaseFactor);
             }
-            __syncthreads();
-            mark(kPhaseLUPanel);
-            // (c) trailing update A22 -= L21 U12: 8x8 tiles on the FP64 tensor cores
-            //     (two k-steps of 4 over the panel); rows/cols >= m are masked.
-            //     The rhs column is updated by the first threads.
-            const int r0 = k0 + kb;
-            const int R = m - r0;
-            if (R > 0) {
-                const int RT = (R + 7) / 8;
-                for (int rt = warp; rt < RT; rt += NW) {
-                    const int row = r0 + 8 * rt + (lane >> 2);
-                    double a[kPanel / 4];
-#pragma unroll
-                    for (int ks = 0; ks < kPanel / 4; ++ks) {
-                        const int kk = k0 + 4 * ks + (lane & 3);
-                        a[ks] = (row < m && kk < k0 + kb) ? -static_cast<double>(A[row * ldA + kk]) : 0.;
-                    }
-#pragma unroll 2
-                    for (int ct = 0; ct < RT; ++ct) {
-                        const int col = r0 + 8 * ct + 2 * (lane & 3);
-                        const int bcol = r0 + 8 * ct + (lane >> 2);
-                        double d0 = (row < m && col < m) ? static_cast<double>(A[row * ldA + col]) : 0.;
-                        double d1 = (row < m && col + 1 < m) ? static_cast<double>(A[row * ldA + col + 1]) : 0.;
-#pragma unroll
-                        for (int ks = 0; ks < kPanel / 4; ++ks) {
-                            const int kk = k0 + 4 * ks + (lane & 3);
-                            const double b = (bcol < m && kk < k0 + kb) ? static_cast<double>(A[kk * ldA + bcol]) : 0.;
-                            dmma884(d0, d1, a[ks], b);
-                        }
-                        if (row < m && col < m) A[row * ldA + col] = static_cast<TR>(d0);
-                        if (row < m && col + 1 < m) A[row * ldA + col + 1] = static_cast<TR>(d1);
-                    }
-                }
-                for (int i = r0 + tid; i < m; i += NT) {
-                    double y = static_cast<double>(A[i * ldA + m]);
-                    for (int pk = 0; pk < kb; ++pk)
-                        y -= static_cast<double>(A[i * ldA + k0 + pk]) *
-                             static_cast<double>(A[(k0 + pk) * ldA + m]);
-                    A[i * ldA + m] = static_cast<TR>(y);
-                }
-            }
-            __syncthreads();
-            mark(kPhaseFactor);
         }
-        // (S4) blocked back substitution U x = y (y in column m)
-        for (int i = tid; i < m; i += NT) xs[i] = static_cast<double>(A[i * ldA + m]);
+        // (S4) back substitution U x = y (y in column m): every warp inverts some
+        //      diagonal blocks, then warp 0 substitutes block by block.
+        for (int b = warp; b * kPanel < m; b += NW) invert_diag_block(A, ldA, m, b * kPanel, rpiv, lane);
         __syncthreads();
-        for (int k0 = ((m - 1) / kPanel) * kPanel; k0 >= 0 && m > 0; k0 -= kPanel) {
-            const int kb = min(kPanel, m - k0);
-            if (warp == 0) {
-                double xv = (lane < kb) ? xs[k0 + lane] : 0.;
-                for (int j = kb - 1; j >= 0; --j) {
-                    const double xj = __shfl_sync(0xffffffffu, xv, j) * rpiv[k0 + j];
-                    if (lane == j) xv = xj;
-                    if (lane < j) xv -= static_cast<double>(A[(k0 + lane) * ldA + k0 + j]) * xj;
-                }
-                if (lane < kb) xs[k0 + lane] = xv;
-            }
-            __syncthreads();
-            for (int i = tid; i < k0; i += NT) {
-                double sacc = xs[i];
-                for (int t = 0; t < kb; ++t)
-                    sacc -= static_cast<double>(A[i * ldA + k0 + t]) * xs[k0 + t];
-                xs[i] = sacc;
-            }
-            __syncthreads();
-        }
+        if (warp == 0 && m > 0) back_substitute_blocked(A, ldA, m, xs, lane);
+        __syncthreads();
         // (S5) multipliers from the constrained rows: grad^T x_l = b_r - A_r x
         for (int rowi = warp; rowi < 6 * nc; rowi += NW) {
             const int c = rowi / 6, k = rowi % 6;
