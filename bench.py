@@ -31,6 +31,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from openturbine_b200 import sharding as S
 from openturbine_b200 import workloads as W  # noqa: E402
 
 L2_FLUSH_BYTES = 256 << 20
@@ -208,7 +209,7 @@ def main() -> None:
     from openturbine_b200.runtime import LOAD_NODE_FX, Context
 
     # ---- build the shard: weak scaling, each rank owns its own 4096 beams ----
-    draws = W.draw_batch(args.beams, first_id=rank * args.beams)
+    draws = W.draw_batch(args.beams, first_id=S.weak_shard_first_id(rank, args.beams))
     if args.nodes:
         draws = [W.BeamDraw(d.model_id, args.nodes, d.length, d.amp, d.freq) for d in draws]
     ctx = Context(local)
@@ -269,16 +270,8 @@ def main() -> None:
                            for i in range(len(ids)))
     torch.cuda.synchronize()
     launches = ctx.kernel_launches - launches0
-    t_value_ms = float(sum(dev_ms))
-    if dist:
-        t = torch.tensor([t_value_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_value_ms = float(t.item())
-        c = torch.tensor([conv_v], device=dev, dtype=torch.float64)
-        dist.all_reduce(c)
-        conv_all = int(c.item())
-    else:
-        conv_all = conv_v
+    t_value_ms = S.max_over_ranks(float(sum(dev_ms)), dist, dev)
+    conv_all = int(S.sum_over_ranks(conv_v, dist, dev))
     value = conv_all / (t_value_ms * 1e-3)
 
     # ---- e2e: host buffers through the C ABI, wall time per step --------------
@@ -293,14 +286,8 @@ def main() -> None:
         ctx.get_state_batch(ids, "q", q_host.data_ptr(), False)
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
         conv_e += int((st == 0).sum())
-    t_e2e_ms = float(sum(e2e_ms))
-    if dist:
-        t = torch.tensor([t_e2e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e_ms = float(t.item())
-        c = torch.tensor([conv_e], device=dev, dtype=torch.float64)
-        dist.all_reduce(c)
-        conv_e = int(c.item())
+    t_e2e_ms = S.max_over_ranks(float(sum(e2e_ms)), dist, dev)
+    conv_e = int(S.sum_over_ranks(conv_e, dist, dev))
     e2e = conv_e / (t_e2e_ms * 1e-3)
 
     if rank == 0:
