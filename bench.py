@@ -185,6 +185,9 @@ def main() -> None:
     ap.add_argument("--cpu-sample", type=int, default=1024)
     ap.add_argument("--cpu-steps", type=int, default=150)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true", help="skip the FP32 + refinement form")
+    ap.add_argument("--refine", type=int, default=0,
+                    help="refinement corrections of the FP32 form after convergence")
     ap.add_argument("--nodes", type=int, default=0,
                     help="uniform nodes per beam (0: the batch's U{5..21}); for profiling one bucket")
     args = ap.parse_args()
@@ -240,18 +243,24 @@ def main() -> None:
             ctx.set_loads_batch(ids, LOAD_NODE_FX, loads_host[k].data_ptr(), False)
         return ctx.step(ids, params)
 
-    # ---- warm-up (also advances the trajectory like the timed steps) ----------
-    for k in range(args.warmup):
-        do_step(k, True)
-    torch.cuda.synchronize()
-
-    # ---- value: device-resident inputs, device time per step ------------------
-    conv_v, flops_v, dev_ms = 0, 0.0, []
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    launches0 = ctx.kernel_launches
-    with ClockSampler(local) as clocks:
+    def device_leg(step_ids, step_params, clocks_on: bool):
+        """W warm-up steps, then K device-timed steps (device-resident loads, L2
+        flushed before each step).  Returns per-step ms, converged counts,
+        algorithmic flops, launches, clock summary and the final states."""
+        def step(k):
+            ctx.set_loads_batch(step_ids, LOAD_NODE_FX, loads_dev[k].data_ptr(), True)
+            return ctx.step(step_ids, step_params)
+        for k in range(args.warmup):
+            step(k)
+        torch.cuda.synchronize()
+        conv, flops, ms, iters = 0, 0.0, [], 0
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        l0 = ctx.kernel_launches
+        sampler = ClockSampler(local) if clocks_on else None
+        if sampler:
+            sampler.__enter__()
         for j in range(args.steps):
             k = args.warmup + j
             with torch.cuda.stream(ext):
@@ -259,20 +268,62 @@ def main() -> None:
                 s = torch.cuda.Event(enable_timing=True)
                 e = torch.cuda.Event(enable_timing=True)
                 s.record(ext)
-            st, it = do_step(k, True)
+            st, it = step(k)
             with torch.cuda.stream(ext):
                 e.record(ext)
             e.synchronize()
-            dev_ms.append(s.elapsed_time(e))
-            ok = st == 0
-            conv_v += int(ok.sum())
-            flops_v += sum(algorithmic_flops(int(nodes[i]), int(qps[i]), int(it[i]), F_QP)
-                           for i in range(len(ids)))
-    torch.cuda.synchronize()
-    launches = ctx.kernel_launches - launches0
+            ms.append(s.elapsed_time(e))
+            conv += int((st == 0).sum())
+            iters += int(it.sum())
+            flops += sum(algorithmic_flops(int(nodes[i]), int(qps[i]), int(it[i]), F_QP)
+                         for i in range(len(step_ids)))
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        clk = None
+        if sampler:
+            sampler.__exit__(None, None, None)
+            clk = sampler.summary()
+        q = torch.zeros((elem_nodes, 7), dtype=torch.float64).pin_memory()
+        ctx.get_state_batch(step_ids, "q", q.data_ptr(), False)
+        return {"ms": ms, "conv": conv, "flops": flops, "iters": iters,
+                "launches": ctx.kernel_launches - l0, "clocks": clk, "q": q.numpy().copy()}
+
+    # ---- value: plain FP64 form, device-resident inputs, device time per step --
+    r64 = device_leg(ids, params, True)
+    dev_ms, conv_v, flops_v, launches = r64["ms"], r64["conv"], r64["flops"], r64["launches"]
     t_value_ms = S.max_over_ranks(float(sum(dev_ms)), dist, dev)
     conv_all = int(S.sum_over_ranks(conv_v, dist, dev))
     value = conv_all / (t_value_ms * 1e-3)
+
+    # ---- the FP32 + refinement form on its own copy of the batch ---------------
+    prec = None
+    if not args.no_fp32:
+        ids32 = np.array([ctx.create_model(W.batch_cantilever_model(d).pack()) for d in draws],
+                         dtype=np.int32)
+        p32 = W.batch_params()
+        p32.precision, p32.refine_iters = 1, args.refine
+        r32 = device_leg(ids32, p32, False)
+        t32 = S.max_over_ranks(float(sum(r32["ms"])), dist, dev)
+        v32 = S.sum_over_ranks(r32["conv"], dist, dev) / (t32 * 1e-3)
+        tips = np.cumsum(nodes) - 1
+        a, b = r64["q"][tips, :3], r32["q"][tips, :3]
+        rel = np.abs(b - a).max(axis=1) / np.maximum(np.abs(a).max(axis=1), 1e-300)
+        rel = rel[np.isfinite(rel)]
+        prec = {"form": "FP32 tangent/LU (3xTF32 integration GEMM) + FP64 residual, update "
+                        f"and {args.refine} refinement correction(s)",
+                "value": v32, "unit": "beam-steps/s", "ratio_vs_fp64": v32 / value,
+                "ms_per_step": t32 / args.steps,
+                "newton_iters_per_beam_step": r32["iters"] / (args.steps * len(ids32)),
+                "fp64_newton_iters_per_beam_step": r64["iters"] / (args.steps * len(ids)),
+                "converged_fraction": r32["conv"] / (args.steps * len(ids32)),
+                "tip_rel_err_vs_fp64": {"median": float(np.median(rel)) if rel.size else None,
+                                        "p99": float(np.percentile(rel, 99)) if rel.size else None,
+                                        "max": float(rel.max()) if rel.size else None},
+                "latency_ms": {"p50": float(np.percentile(r32["ms"], 50)),
+                               "p99": float(np.percentile(r32["ms"], 99))}}
+        for i in ids32:
+            ctx.destroy_model(int(i))
 
     # ---- e2e: host buffers through the C ABI, wall time per step --------------
     e2e_ms, conv_e = [], 0
@@ -319,7 +370,9 @@ def main() -> None:
             "gpu_launches": launches,
             "setup_s": t_setup,
         }
-        line["clocks"] = clocks.summary()
+        line["clocks"] = r64["clocks"]
+        if prec is not None:
+            line["precision_form"] = prec
         if not args.no_cpu and world == 1:
             line["cpu_baseline"] = cpu_baseline(draws[: args.cpu_sample], params, args.cpu_steps,
                                                 os.cpu_count() or 1)

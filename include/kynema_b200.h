@@ -136,7 +136,9 @@ typedef struct kyn_step_params {
     double absolute_convergence_tol; /* reference default 1e-5 */
     double relative_convergence_tol; /* reference default 1e-3 */
     int32_t precision;               /* KYN_PRECISION_*         */
-    int32_t reserved;
+    int32_t refine_iters;            /* FP32 form: extra Newton corrections after
+                                        the convergence test passes (each with
+                                        the FP64 residual); ignored in FP64 */
 } kyn_step_params;
 
 /* Sizes of one model's system (Solver::num_system_dofs / num_dofs / nnz). */
@@ -224,6 +226,17 @@ KYN_API int kyn_get_state_batch(kyn_ctx* ctx, const int* model_ids, int n, int f
  * kyn_set_loads_batch. */
 KYN_API int kyn_set_loads_batch_static(kyn_ctx* ctx, const int* model_ids, int n, int which,
                                        const double* values, int on_device);
+
+/* Autotuner (no counterpart in the reference): for every size class of the
+ * listed models (beams per model, nodes, quadrature points, constraints,
+ * precision), times the step kernel with 128, 256 and 512 threads per CTA on
+ * temporary copies of up to 8 x SMs models of that class (two steps after one
+ * warm-up step) and keeps the fastest for later kyn_step calls on this
+ * context.  The listed models' states are not changed. */
+KYN_API int kyn_autotune(kyn_ctx* ctx, const int* model_ids, int n, const kyn_step_params* params);
+
+/* Threads per CTA kyn_step uses for a model at a precision (tuned or default). */
+KYN_API int kyn_tuned_threads(kyn_ctx* ctx, int model_id, int precision);
 
 /* Replaces host reads of State / Constraints views after Step(). */
 KYN_API int kyn_get_state(kyn_ctx* ctx, int model_id, int field, double* out);

@@ -143,13 +143,14 @@ struct StepParameters {  // src/step/step_parameters.hpp:12-53
     size_t max_iter;
     double h, rho_inf, absolute_convergence_tol, relative_convergence_tol;
     int precision = KYN_PRECISION_FP64;
+    int refine_iters = 0;
     StepParameters(bool dyn, size_t max_it, double h_, double rho, double a_tol = 1e-5,
                    double r_tol = 1e-3)
         : is_dynamic_solve(dyn), max_iter(max_it), h(h_), rho_inf(rho),
           absolute_convergence_tol(a_tol), relative_convergence_tol(r_tol) {}
     kyn_step_params c() const {
         return {is_dynamic_solve ? 1 : 0, static_cast<int32_t>(max_iter), h, rho_inf,
-                absolute_convergence_tol, relative_convergence_tol, precision, 0};
+                absolute_convergence_tol, relative_convergence_tol, precision, refine_iters};
     }
 };
 

@@ -42,6 +42,17 @@ struct DevModel {
     int last_iters = 0;
 };
 
+struct ClassKey {
+    int beams, N, Q, nc, precision;
+    bool operator<(const ClassKey& o) const {
+        if (beams != o.beams) return beams < o.beams;
+        if (N != o.N) return N < o.N;
+        if (Q != o.Q) return Q < o.Q;
+        if (nc != o.nc) return nc < o.nc;
+        return precision < o.precision;
+    }
+};
+
 struct Bucket {
     int cluster = 1;
     int nt = 256;      // threads per CTA (step_kernel instance)
@@ -52,6 +63,7 @@ struct Bucket {
 
 struct Plan {
     std::vector<int> ids;
+    int precision = KYN_PRECISION_FP64;
     std::vector<Bucket> buckets;
     KBeam* d_kbeams = nullptr;
     int* d_status = nullptr;      // [nmodels]
@@ -130,6 +142,7 @@ struct kyn_ctx {
     int64_t launches = 0;                 // kernels launched so far
     int64_t last_buckets = 0;
     unsigned long long* d_prof = nullptr; // phase timing counters (KYN_OPT_PHASE_TIMING)
+    std::map<ClassKey, int> tuned;        // threads per CTA chosen by kyn_autotune
 };
 
 namespace {
@@ -167,11 +180,14 @@ StepCoeffs make_coeffs(const kyn_step_params* p) {
     P.atol = p->absolute_convergence_tol;
     P.rtol = p->relative_convergence_tol;
     P.max_iter = std::min<int>(p->max_iter, kMaxNewtonIters);
+    P.refine_iters = (p->precision == KYN_PRECISION_FP32_REFINED)
+                         ? std::max(0, std::min<int>(p->refine_iters, 4)) : 0;
     return P;
 }
 
-// Threads per CTA for a beam: 256 when two such CTAs fit on an SM (their
-// serial phases overlap), else 512 so the one resident CTA has 16 warps.
+// Default threads per CTA for a beam: 256 when two such CTAs fit on an SM
+// (their serial phases overlap), else 512 so the one resident CTA has 16
+// warps.  kyn_autotune replaces the default per size class by measurement.
 int beam_threads(int N, int Q, int nc, int real_bytes) {
     const int s256 = make_smem(N, Q, nc, real_bytes, 256).bytes;
     return (2 * (s256 + 1024) <= kSmemPerSM) ? 256 : 512;
@@ -182,16 +198,27 @@ int beam_smem(int N, int Q, int nc, int real_bytes, int nt) {
 }
 
 // Resident CTAs per SM for a thread count and shared-memory size; the step
-// kernel's register budget (128 per thread) allows two CTAs of 256 threads.
+// kernel's register budget (128 per thread) allows 65536 / (128 nt) CTAs.
 int ctas_per_sm(int nt, int smem) {
-    if (nt == 512) return 1;
+    const int by_regs = 65536 / (128 * nt);
     const int per = smem + 1024;
-    return std::max(1, std::min(2, kSmemPerSM / per));
+    return std::max(1, std::min(by_regs, kSmemPerSM / per));
+}
+
+// Size class of a model for the tuned thread-count table.
+ClassKey class_key(const HostModel& h, int precision) {
+    ClassKey k{static_cast<int>(h.beams.size()), 0, 0, 0, precision};
+    for (const HostBeam& b : h.beams) {
+        k.N = std::max(k.N, b.N);
+        k.Q = std::max(k.Q, b.Q);
+        k.nc = std::max(k.nc, b.nc);
+    }
+    return k;
 }
 
 // Builds (or reuses) the launch plan for this id list.
-int get_plan(kyn_ctx* c, const int* ids, int n, Plan** out) {
-    if (c->plan && c->plan->record == c->record &&
+int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
+    if (c->plan && c->plan->record == c->record && c->plan->precision == precision &&
         static_cast<int>(c->plan->ids.size()) == n &&
         std::equal(ids, ids + n, c->plan->ids.begin())) {
         *out = c->plan.get();
@@ -200,6 +227,8 @@ int get_plan(kyn_ctx* c, const int* ids, int n, Plan** out) {
     auto plan = std::make_unique<Plan>();
     plan->ids.assign(ids, ids + n);
     plan->record = c->record;
+    plan->precision = precision;
+    const int rb = (precision == KYN_PRECISION_FP32_REFINED) ? 4 : 8;
     // bucket key: (cluster size, CTAs per SM class); larger work first
     struct Entry {
         int model_index;
@@ -213,16 +242,18 @@ int get_plan(kyn_ctx* c, const int* ids, int n, Plan** out) {
     for (int i = 0; i < n; ++i) {
         DevModel* m = find_model(c, ids[i]);
         if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id in step list");
-        int nt = 256;
+        int nt = 128;
         double work = 0.;
+        const auto tuned = c->tuned.find(class_key(m->host, precision));
         for (size_t b = 0; b < m->host.beams.size(); ++b) {
-            nt = std::max(nt, m->nt[b]);
+            const HostBeam& hb = m->host.beams[b];
+            nt = std::max(nt, tuned != c->tuned.end() ? tuned->second : beam_threads(hb.N, hb.Q, hb.nc, rb));
             const double N = m->host.beams[b].N, Q = m->host.beams[b].Q;
             work = std::max(work, N * N * Q + 72. * (N - 1) * (N - 1) * (N - 1));
         }
         int smem = 0;
         for (const HostBeam& hb : m->host.beams)
-            smem = std::max(smem, beam_smem(hb.N, hb.Q, hb.nc, sizeof(double), nt));
+            smem = std::max(smem, beam_smem(hb.N, hb.Q, hb.nc, rb, nt));
         entries.push_back({i, static_cast<int>(m->host.beams.size()), nt, ctas_per_sm(nt, smem), smem,
                            work});
     }
@@ -287,13 +318,20 @@ int get_plan(kyn_ctx* c, const int* ids, int n, Plan** out) {
     return KYN_OK;
 }
 
+template <typename K>
+cudaError_t set_smem_attr(K kernel) {
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+}
+
 int launch_plan(kyn_ctx* c, Plan* plan, const kyn_step_params* p) {
     const StepCoeffs P = make_coeffs(p);
     if (c->smem_configured < kMaxDynSmem) {
-        KYN_CUDA(c, cudaFuncSetAttribute(step_kernel<double, 256>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
-        KYN_CUDA(c, cudaFuncSetAttribute(step_kernel<double, 512>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
+        KYN_CUDA(c, set_smem_attr(step_kernel<double, 128>));
+        KYN_CUDA(c, set_smem_attr(step_kernel<double, 256>));
+        KYN_CUDA(c, set_smem_attr(step_kernel<double, 512>));
+        KYN_CUDA(c, set_smem_attr(step_kernel<float, 128>));
+        KYN_CUDA(c, set_smem_attr(step_kernel<float, 256>));
+        KYN_CUDA(c, set_smem_attr(step_kernel<float, 512>));
         c->smem_configured = kMaxDynSmem;
     }
     KYN_CUDA(c, cudaEventRecord(c->fork, c->stream));
@@ -317,12 +355,13 @@ int launch_plan(kyn_ctx* c, Plan* plan, const kyn_step_params* p) {
             cfg.numAttrs = 1;
         }
         const KBeam* beams = plan->d_kbeams + bk.first;
-        if (bk.nt == 512)
-            KYN_CUDA(c, cudaLaunchKernelEx(&cfg, step_kernel<double, 512>, beams, P,
-                                           plan->record ? 1 : 0, plan->d_status, plan->d_iters));
-        else
-            KYN_CUDA(c, cudaLaunchKernelEx(&cfg, step_kernel<double, 256>, beams, P,
-                                           plan->record ? 1 : 0, plan->d_status, plan->d_iters));
+        const int rec = plan->record ? 1 : 0;
+        const bool fp32 = plan->precision == KYN_PRECISION_FP32_REFINED;
+        auto kern = fp32 ? (bk.nt == 128 ? step_kernel<float, 128>
+                            : bk.nt == 256 ? step_kernel<float, 256> : step_kernel<float, 512>)
+                         : (bk.nt == 128 ? step_kernel<double, 128>
+                            : bk.nt == 256 ? step_kernel<double, 256> : step_kernel<double, 512>);
+        KYN_CUDA(c, cudaLaunchKernelEx(&cfg, kern, beams, P, rec, plan->d_status, plan->d_iters));
         c->launches++;
     }
     c->last_buckets = nb;
@@ -690,13 +729,13 @@ int kyn_step(kyn_ctx* c, const int* ids, int n, const kyn_step_params* p, int* s
 int kyn_step_async(kyn_ctx* c, const int* ids, int n, const kyn_step_params* p) {
     if (!c || !p || n < 0 || (n > 0 && !ids)) return KYN_ERR_INVALID;
     if (p->max_iter < 1 || !(p->h > 0.)) return set_err(c, KYN_ERR_INVALID, "bad step parameters");
-    if (p->precision != KYN_PRECISION_FP64)
-        return set_err(c, KYN_ERR_UNSUPPORTED, "precision mode not available in this build");
+    if (p->precision != KYN_PRECISION_FP64 && p->precision != KYN_PRECISION_FP32_REFINED)
+        return set_err(c, KYN_ERR_INVALID, "unknown precision mode");
     cudaSetDevice(c->device);
     c->pending.assign(ids, ids + n);
     if (n == 0) return KYN_OK;
     Plan* plan = nullptr;
-    int rc = get_plan(c, ids, n, &plan);
+    int rc = get_plan(c, ids, n, p->precision, &plan);
     if (rc != KYN_OK) return rc;
     return launch_plan(c, plan, p);
 }
@@ -877,6 +916,117 @@ int kyn_get_state_batch(kyn_ctx* c, const int* ids, int n, int field, double* ou
 }
 
 }  // extern "C"
+
+// ---- autotuner: threads per CTA per model size class -----------------------------
+namespace {
+
+// Copy of a model (description and current device state) for tuning runs.
+int clone_model(kyn_ctx* c, int id) {
+    DevModel* src = find_model(c, id);
+    if (!src) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
+    auto m = std::make_unique<DevModel>();
+    m->host = src->host;
+    m->nt = src->nt;
+    size_t bytes = kMaxNewtonIters * sizeof(double);
+    for (auto& b : m->host.beams) bytes += b.slab.size() * sizeof(double);
+    if (c->budget && c->used + bytes > c->budget)
+        return set_err(c, KYN_ERR_BUDGET, "HBM budget exceeded");
+    for (size_t bi = 0; bi < m->host.beams.size(); ++bi) {
+        double* p = nullptr;
+        const size_t len = m->host.beams[bi].slab.size() * sizeof(double);
+        KYN_CUDA(c, cudaMallocAsync(&p, len, c->stream));
+        KYN_CUDA(c, cudaMemcpyAsync(p, src->d_slab[bi], len, cudaMemcpyDeviceToDevice, c->stream));
+        m->d_slab.push_back(p);
+    }
+    KYN_CUDA(c, cudaMallocAsync(&m->d_conv, kMaxNewtonIters * sizeof(double), c->stream));
+    m->bytes = bytes;
+    c->used += bytes;
+    const int nid = c->next_id++;
+    c->models[nid] = std::move(m);
+    return nid;
+}
+
+}  // namespace
+
+extern "C" int kyn_autotune(kyn_ctx* c, const int* ids, int n, const kyn_step_params* p) {
+    if (!c || !p || n < 0 || (n > 0 && !ids)) return KYN_ERR_INVALID;
+    if (p->precision != KYN_PRECISION_FP64 && p->precision != KYN_PRECISION_FP32_REFINED)
+        return set_err(c, KYN_ERR_INVALID, "unknown precision mode");
+    if (n == 0) return KYN_OK;
+    KYN_CUDA(c, cudaSetDevice(c->device));
+    const int rb = (p->precision == KYN_PRECISION_FP32_REFINED) ? 4 : 8;
+    int sms = 148;
+    KYN_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+    const size_t sample_max = static_cast<size_t>(8) * sms;
+    std::map<ClassKey, std::vector<int>> classes;
+    for (int i = 0; i < n; ++i) {
+        DevModel* m = find_model(c, ids[i]);
+        if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id in autotune list");
+        classes[class_key(m->host, p->precision)].push_back(ids[i]);
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    KYN_CUDA(c, cudaEventCreate(&e0));
+    KYN_CUDA(c, cudaEventCreate(&e1));
+    int rc = KYN_OK;
+    for (auto& kv : classes) {
+        const ClassKey& key = kv.first;
+        std::vector<int> clones;
+        for (size_t j = 0; j < std::min(kv.second.size(), sample_max); ++j) {
+            const int cid = clone_model(c, kv.second[j]);
+            if (cid < 0) break;
+            clones.push_back(cid);
+        }
+        if (clones.empty()) continue;
+        const HostModel& h = c->models[clones[0]]->host;
+        int best_nt = -1;
+        float best_ms = 0.f;
+        for (int nt : {128, 256, 512}) {
+            bool fits = true;
+            for (const HostBeam& b : h.beams) fits &= beam_smem(b.N, b.Q, b.nc, rb, nt) <= kMaxDynSmem;
+            if (!fits || (key.beams > 1 && key.beams * nt > 1024 * 8)) continue;
+            c->tuned[key] = nt;
+            c->plan.reset();
+            Plan* plan = nullptr;
+            rc = get_plan(c, clones.data(), static_cast<int>(clones.size()), p->precision, &plan);
+            if (rc != KYN_OK) break;
+            rc = launch_plan(c, plan, p);  // warm-up step
+            if (rc == KYN_OK) rc = finish_plan(c, plan, nullptr, nullptr);
+            if (rc != KYN_OK) break;
+            KYN_CUDA(c, cudaEventRecord(e0, c->stream));
+            for (int r = 0; r < 2 && rc == KYN_OK; ++r) rc = launch_plan(c, plan, p);
+            KYN_CUDA(c, cudaEventRecord(e1, c->stream));
+            if (rc == KYN_OK) rc = finish_plan(c, plan, nullptr, nullptr);
+            if (rc != KYN_OK) break;
+            float ms = 0.f;
+            KYN_CUDA(c, cudaEventElapsedTime(&ms, e0, e1));
+            if (best_nt < 0 || ms < best_ms) {
+                best_nt = nt;
+                best_ms = ms;
+            }
+        }
+        if (best_nt > 0) c->tuned[key] = best_nt;
+        else c->tuned.erase(key);
+        c->plan.reset();
+        for (int cid : clones) kyn_model_destroy(c, cid);
+        if (rc != KYN_OK) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->plan.reset();
+    return rc;
+}
+
+extern "C" int kyn_tuned_threads(kyn_ctx* c, int model_id, int precision) {
+    if (!c) return KYN_ERR_INVALID;
+    DevModel* m = find_model(c, model_id);
+    if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
+    const auto it = c->tuned.find(class_key(m->host, precision));
+    if (it != c->tuned.end()) return it->second;
+    const int rb = (precision == KYN_PRECISION_FP32_REFINED) ? 4 : 8;
+    int nt = 128;
+    for (const HostBeam& b : m->host.beams) nt = std::max(nt, beam_threads(b.N, b.Q, b.nc, rb));
+    return nt;
+}
 
 // ---- batched load scatter through a static staging array (no allocation) ----
 //

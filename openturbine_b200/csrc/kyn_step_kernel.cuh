@@ -107,9 +107,11 @@ __device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double
 }
 
 // ---- shared-memory plan of one CTA --------------------------------------------
-// The kernel runs with NT = 256 threads (two CTAs per SM, beams up to ~14 nodes)
-// or NT = 512 threads (one CTA per SM, larger beams); NT/16 quadrature points
-// are processed per pass and NT/32 warps share the GEMM-shaped phases.
+// The kernel runs with NT = 128, 256 or 512 threads (up to four, two or one
+// CTAs per SM within the 128-register budget); NT/16 quadrature points are
+// processed per pass and NT/32 warps share the GEMM-shaped phases.  More
+// resident CTAs overlap more beams' serial sections (LU pivots); more warps
+// per CTA shorten the parallel phases of one beam.
 constexpr int kGroupScratch = 256;      // doubles of per-group scratch for QP math
 constexpr int kPanel = 8;               // LU panel width
 constexpr int kConStride = 96;          // doubles per constraint record in smem
@@ -172,7 +174,9 @@ __host__ __device__ inline Smem make_smem(int N, int Q, int nc, int real_bytes, 
         const int g_bytes = (nt / 16) * kGroupScratch * 8;
         S.A = take(a_bytes > g_bytes ? a_bytes : g_bytes);
     }
-    S.G = take(4 * Q * 56 * 8);
+    // FP64 form: G in FP64, one k-step per point.  FP32 form: G in FP32 and
+    // k-steps of two points (m16n8k8), so an odd Q gets one zero pad point.
+    S.G = take(4 * (real_bytes == 4 ? (Q + 1) & ~1 : Q) * 56 * real_bytes);
     S.Fc = take(Q * 6 * 8);
     S.Fdig = take(Q * 6 * 8);
     S.phi = take(Q * N * 8);
@@ -230,15 +234,87 @@ constexpr int inp = 42;    // [7] prescribed input
 constexpr int yr = 49;     // [6] constrained-row residual b_r - A_r x
 }  // namespace conrec
 
-// ---- dense LU pieces (free block of the beam system, FP64 in shared memory) ------
-// Reciprocal of a pivot: hardware approximation refined by two Newton-Raphson
-// steps r <- r + r (1 - d r) (each step squares the relative error).
+// TF32 tensor-core product D += A B for one 16x8x8 tile (mma.sync m16n8k8).
+// Fragment layout per lane l (g = l/4, t = l%4): a = {A[g][t], A[g+8][t],
+// A[g][t+4], A[g+8][t+4]}, b = {B[t][g], B[t+4][g]}, d = {D[g][2t], D[g][2t+1],
+// D[g+8][2t], D[g+8][2t+1]}.
+__device__ __forceinline__ void mma_tf32(float* d, const unsigned* a, const unsigned* b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+        "{%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// x = hi + lo with hi, lo representable in TF32 (round to nearest, ties away).
+__device__ __forceinline__ void split_tf32(float x, unsigned& hi, unsigned& lo) {
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(x));
+    const float r = x - __uint_as_float(hi);
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(r));
+}
+
+// Writes SM_ij = [C_L | C_RS T_j + C_RI] of node pair (i, j), scaled by the
+// conditioner, into the system matrix from one lane's integration-GEMM slots
+// (column layout: gcol; slot(t) returns the lane's slot t).
+template <typename TR, typename Slot>
+__device__ __forceinline__ void store_pair_block(TR* A, int ldA, const int* pos, const double* sT,
+                                                 int i, int jn, int s4, double cond, Slot slot) {
+    TR* Arow = A + (6 * pos[i]) * ldA + 6 * pos[jn];
+    if (s4 < 3) {
+        const double* Tj = sT + jn * 9;
+#pragma unroll
+        for (int rr = 0; rr < 2; ++rr) {
+            const int r = 2 * s4 + rr;
+            // slots 6rr..6rr+2: RS[r][0..2]; 6rr+3..6rr+5: RI[r][0..2]
+            double rs[3], ri[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                rs[k] = slot(6 * rr + k);
+                ri[k] = slot(6 * rr + 3 + k);
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                double val = ri[c];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) val += rs[k] * Tj[k * 3 + c];
+                Arow[r * ldA + 3 + c] = static_cast<TR>(val * cond);
+            }
+        }
+        if (s4 < 2) {
+            // slots 12, 13: L[14 + 2 s4 + e]
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int l = 14 + 2 * s4 + e;
+                Arow[(l / 3) * ldA + l % 3] = static_cast<TR>(slot(12 + e) * cond);
+            }
+        }
+    } else {
+        // slots 0..13: L[0..13]
+#pragma unroll
+        for (int t = 0; t < 14; ++t) Arow[(t / 3) * ldA + t % 3] = static_cast<TR>(slot(t) * cond);
+    }
+}
+
+// ---- dense LU pieces (free block of the beam system in shared memory) -------------
+// The pivot chains (diagonal blocks, panel solves, block back substitution)
+// compute in the storage type TR: FP64 in the plain form, FP32 in the FP32
+// form.  Trailing updates run on the FP64 tensor cores in both forms (FP32
+// operands are exact in FP64; the result is rounded once to TR on store).
+
+// Reciprocal of a pivot: hardware approximation refined by Newton-Raphson
+// steps r <- r + r (1 - d r) (each step squares the relative error): two in
+// FP64 (exact to the last bit on all tested inputs), one in FP32.
 __device__ __forceinline__ double pivot_rcp(double d) {
     double r;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
     r = fma(r, fma(-d, r, 1.), r);
     r = fma(r, fma(-d, r, 1.), r);
     return r;
+}
+__device__ __forceinline__ float pivot_rcp(float d) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d));
+    return fmaf(r, fmaf(-d, r, 1.f), r);
 }
 
 // Warp-level factorisation of the kb x kb diagonal block of the panel of
@@ -247,24 +323,23 @@ template <typename TR>
 __device__ __forceinline__ void factor_diag(TR* A, int ldA, int m, int p0, double* rpiv, int lane,
                                             int* flag) {
     const int kb = min(kPanel, m - p0);
-    double v[kPanel];
+    TR v[kPanel];
 #pragma unroll
-    for (int c = 0; c < kPanel; ++c)
-        v[c] = (lane < kb && c < kb) ? static_cast<double>(A[(p0 + lane) * ldA + p0 + c]) : 0.;
+    for (int c = 0; c < kPanel; ++c) v[c] = (lane < kb && c < kb) ? A[(p0 + lane) * ldA + p0 + c] : TR(0);
 #pragma unroll
     for (int j = 0; j < kPanel; ++j) {
         if (j < kb) {
-            const double d = __shfl_sync(0xffffffffu, v[j], j);
-            double u[kPanel];
+            const TR d = __shfl_sync(0xffffffffu, v[j], j);
+            TR u[kPanel];
 #pragma unroll
             for (int c = j + 1; c < kPanel; ++c) u[c] = __shfl_sync(0xffffffffu, v[c], j);
-            const double rp = pivot_rcp(d);
+            const TR rp = pivot_rcp(d);
             if (lane == 0) {
-                rpiv[p0 + j] = rp;
-                if (!(fabs(d) > 0.) || !isfinite(rp)) *flag |= 2;
+                rpiv[p0 + j] = static_cast<double>(rp);
+                if (!(fabs(d) > TR(0)) || !isfinite(rp)) *flag |= 2;
             }
             if (lane > j) {
-                const double l = v[j] * rp;
+                const TR l = v[j] * rp;
                 v[j] = l;
 #pragma unroll
                 for (int c = j + 1; c < kPanel; ++c) v[c] -= l * u[c];
@@ -274,7 +349,7 @@ __device__ __forceinline__ void factor_diag(TR* A, int ldA, int m, int p0, doubl
     if (lane < kb) {
 #pragma unroll
         for (int c = 0; c < kPanel; ++c)
-            if (c < kb) A[(p0 + lane) * ldA + p0 + c] = static_cast<TR>(v[c]);
+            if (c < kb) A[(p0 + lane) * ldA + p0 + c] = v[c];
     }
 }
 
@@ -286,21 +361,21 @@ __device__ __forceinline__ void solve_l21(TR* A, int ldA, int m, int p0, const d
     const int kb = min(kPanel, m - p0);
 #pragma unroll 2
     for (int r = r_begin + idx; r < m; r += stride) {
-        double u[kPanel];
+        TR u[kPanel];
 #pragma unroll
-        for (int c = 0; c < kPanel; ++c) u[c] = (c < kb) ? static_cast<double>(A[r * ldA + p0 + c]) : 0.;
+        for (int c = 0; c < kPanel; ++c) u[c] = (c < kb) ? A[r * ldA + p0 + c] : TR(0);
 #pragma unroll
         for (int j = 0; j < kPanel; ++j) {
             if (j < kb) {
-                u[j] *= rpiv[p0 + j];
+                u[j] *= static_cast<TR>(rpiv[p0 + j]);
 #pragma unroll
                 for (int k = j + 1; k < kPanel; ++k)
-                    if (k < kb) u[k] -= u[j] * static_cast<double>(A[(p0 + j) * ldA + p0 + k]);
+                    if (k < kb) u[k] -= u[j] * A[(p0 + j) * ldA + p0 + k];
             }
         }
 #pragma unroll
         for (int c = 0; c < kPanel; ++c)
-            if (c < kb) A[r * ldA + p0 + c] = static_cast<TR>(u[c]);
+            if (c < kb) A[r * ldA + p0 + c] = u[c];
     }
 }
 
@@ -337,22 +412,22 @@ __device__ __forceinline__ void update_tile(TR* A, int ldA, int m, int k0, int k
     if (kMode != kU12InRegs) {
         if (lane < 8 && c0 + lane <= m) {
             const int c = c0 + lane;
-            double u[kPanel];
+            TR u[kPanel];
 #pragma unroll
-            for (int j = 0; j < kPanel; ++j) u[j] = (j < kb) ? static_cast<double>(A[(k0 + j) * ldA + c]) : 0.;
+            for (int j = 0; j < kPanel; ++j) u[j] = (j < kb) ? A[(k0 + j) * ldA + c] : TR(0);
 #pragma unroll
             for (int q = 0; q < kPanel - 1; ++q) {
 #pragma unroll
                 for (int j = q + 1; j < kPanel; ++j)
-                    if (j < kb) u[j] -= static_cast<double>(A[(k0 + j) * ldA + k0 + q]) * u[q];
+                    if (j < kb) u[j] -= A[(k0 + j) * ldA + k0 + q] * u[q];
             }
             if (kMode == kU12InPlace) {
 #pragma unroll
                 for (int j = 1; j < kPanel; ++j)
-                    if (j < kb) A[(k0 + j) * ldA + c] = static_cast<TR>(u[j]);
+                    if (j < kb) A[(k0 + j) * ldA + c] = u[j];
             } else {
 #pragma unroll
-                for (int j = 0; j < kPanel; ++j) stage[j * 8 + lane] = u[j];
+                for (int j = 0; j < kPanel; ++j) stage[j * 8 + lane] = static_cast<double>(u[j]);
             }
         }
         __syncwarp();
@@ -368,15 +443,14 @@ __device__ __forceinline__ void update_tile(TR* A, int ldA, int m, int k0, int k
     } else {
         const int col = c0 + (lane >> 2);
         const bool cok = col <= m;
-        double u[kPanel];
+        TR u[kPanel];
 #pragma unroll
-        for (int j = 0; j < kPanel; ++j)
-            u[j] = (j < kb && cok) ? static_cast<double>(A[(k0 + j) * ldA + (cok ? col : c0)]) : 0.;
+        for (int j = 0; j < kPanel; ++j) u[j] = (j < kb && cok) ? A[(k0 + j) * ldA + (cok ? col : c0)] : TR(0);
 #pragma unroll
         for (int q = 0; q < kPanel - 1; ++q) {
 #pragma unroll
             for (int j = q + 1; j < kPanel; ++j)
-                if (j < kb) u[j] -= static_cast<double>(A[(k0 + j) * ldA + k0 + q]) * u[q];
+                if (j < kb) u[j] -= A[(k0 + j) * ldA + k0 + q] * u[q];
         }
         b0 = u[0];
         b1 = u[4];
@@ -413,28 +487,29 @@ __device__ __forceinline__ void invert_diag_block(TR* A, int ldA, int m, int p0,
                                                   int lane) {
     const int kb = min(kPanel, m - p0);
     const int jc = lane & 7;
-    double x[kPanel];
+    TR x[kPanel];
 #pragma unroll
-    for (int i = 0; i < kPanel; ++i) x[i] = (i == jc) ? 1. : 0.;
+    for (int i = 0; i < kPanel; ++i) x[i] = (i == jc) ? TR(1) : TR(0);
 #pragma unroll
     for (int c = kPanel - 1; c >= 0; --c) {
         if (c < kb) {  // warp-uniform; x[c] = 0 for c > jc, so no lane test is needed
-            x[c] *= rpiv[p0 + c];
+            x[c] *= static_cast<TR>(rpiv[p0 + c]);
 #pragma unroll
-            for (int i = 0; i < c; ++i) x[i] = fma(-static_cast<double>(A[(p0 + i) * ldA + p0 + c]), x[c], x[i]);
+            for (int i = 0; i < c; ++i) x[i] -= A[(p0 + i) * ldA + p0 + c] * x[c];
         }
     }
     __syncwarp();
     if (lane < kb) {
 #pragma unroll
         for (int i = 0; i < kPanel; ++i)
-            if (i <= lane) A[(p0 + i) * ldA + p0 + lane] = static_cast<TR>(x[i]);
+            if (i <= lane) A[(p0 + i) * ldA + p0 + lane] = x[i];
     }
 }
 
 // Block back substitution U x = y by one warp (y in column m), with the
 // diagonal blocks already inverted: x_b = U_bb^{-1} y_b, then the rows above
-// the block take y_i -= U_i,b x_b.
+// the block take y_i -= U_i,b x_b.  Arithmetic in TR; the solution is written
+// to xs in FP64.
 template <typename TR>
 __device__ __forceinline__ void back_substitute_blocked(const TR* A, int ldA, int m, double* xs, int lane) {
     for (int i = lane; i < m; i += 32) xs[i] = static_cast<double>(A[i * ldA + m]);
@@ -442,26 +517,25 @@ __device__ __forceinline__ void back_substitute_blocked(const TR* A, int ldA, in
     const int nblk = (m + kPanel - 1) / kPanel;
     for (int b = nblk - 1; b >= 0; --b) {
         const int k0 = b * kPanel, kb = min(kPanel, m - k0);
-        double xv = 0.;
+        TR xv = TR(0);
         if (lane < kb) {
 #pragma unroll
             for (int c = 0; c < kPanel; ++c)
-                if (c >= lane && c < kb)
-                    xv += static_cast<double>(A[(k0 + lane) * ldA + k0 + c]) * xs[k0 + c];
+                if (c >= lane && c < kb) xv += A[(k0 + lane) * ldA + k0 + c] * static_cast<TR>(xs[k0 + c]);
         }
         __syncwarp();
-        if (lane < kb) xs[k0 + lane] = xv;
+        if (lane < kb) xs[k0 + lane] = static_cast<double>(xv);
         __syncwarp();
-        double xb[kPanel];
+        TR xb[kPanel];
 #pragma unroll
-        for (int c = 0; c < kPanel; ++c) xb[c] = (c < kb) ? xs[k0 + c] : 0.;
+        for (int c = 0; c < kPanel; ++c) xb[c] = (c < kb) ? static_cast<TR>(xs[k0 + c]) : TR(0);
 #pragma unroll 2
         for (int i = lane; i < k0; i += 32) {
-            double acc = xs[i];
+            TR acc = static_cast<TR>(xs[i]);
 #pragma unroll
             for (int c = 0; c < kPanel; ++c)
-                if (c < kb) acc -= static_cast<double>(A[i * ldA + k0 + c]) * xb[c];
-            xs[i] = acc;
+                if (c < kb) acc -= A[i * ldA + k0 + c] * xb[c];
+            xs[i] = static_cast<double>(acc);
         }
         __syncwarp();
     }
@@ -469,10 +543,10 @@ __device__ __forceinline__ void back_substitute_blocked(const TR* A, int ldA, in
 
 // ---- the kernel ------------------------------------------------------------------
 template <typename TR, int NT>
-__global__ void __launch_bounds__(NT, (NT == 256) ? 2 : 1)
+__global__ void __launch_bounds__(NT, (NT == 128) ? 4 : (NT == 256) ? 2 : 1)
     step_kernel(const KBeam* __restrict__ beams, StepCoeffs P, int record,
                 int* __restrict__ status_out, int* __restrict__ iters_out) {
-    static_assert(NT == 256 || NT == 512, "step kernel runs with 256 or 512 threads");
+    static_assert(NT == 128 || NT == 256 || NT == 512, "step kernel runs with 128, 256 or 512 threads");
     constexpr int NW = NT / 32;  // warps
     constexpr int NG = NT / 16;  // quadrature-point groups of 16 threads
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -487,7 +561,8 @@ __global__ void __launch_bounds__(NT, (NT == 256) ? 2 : 1)
 
     TR* A = reinterpret_cast<TR*>(smem_raw + S.A);
     const int ldA = S.ldA;
-    double* G = reinterpret_cast<double*>(smem_raw + S.G);
+    using TG = TR;  // element type of G: FP64 form double, FP32 form float
+    TG* G = reinterpret_cast<TG*>(smem_raw + S.G);
     double* Fc = reinterpret_cast<double*>(smem_raw + S.Fc);
     double* Fdig = reinterpret_cast<double*>(smem_raw + S.Fdig);
     double* phi = reinterpret_cast<double*>(smem_raw + S.phi);
@@ -561,6 +636,9 @@ __global__ void __launch_bounds__(NT, (NT == 256) ? 2 : 1)
     }
     __syncthreads();
 
+    if (sizeof(TR) == 4 && (Q & 1))  // zero pad point of the FP32 integration GEMM
+        for (int k = tid; k < 4 * 56; k += NT) G[4 * Q * 56 + k] = TG(0);
+
     // ---- PredictNextState (src/step/predict_next_state.hpp:14-47) ------------
     for (int k = tid; k < N * 7; k += NT) sqp[k] = sq[k];
     for (int k = tid; k < N * 6; k += NT) {
@@ -592,7 +670,8 @@ __global__ void __launch_bounds__(NT, (NT == 256) ? 2 : 1)
     const cg::cluster_group cluster = cg::this_cluster();
     const bool clustered = KB.model_beams > 1;
 
-    for (int iter = 0; iter < P.max_iter; ++iter) {
+    int extra = 0;  // refinement corrections taken after convergence (FP32 form)
+    for (int iter = 0; iter < P.max_iter + extra; ++iter) {
         // ---- tangent operator (src/system/calculate_tangent_operator.hpp:26-65)
         // Only the rotational 3x3 block of the stored (transposed) operator is kept.
         for (int n = tid; n < N; n += NT) {
@@ -651,8 +730,8 @@ __global__ void __launch_bounds__(NT, (NT == 256) ? 2 : 1)
                         gs[grec::mstar + k] = v;
                     }
                     // this point's G rows start at zero (structural zeros, padding)
-                    double* Gq = G + 4 * qp * 56;
-                    for (int t = g; t < 4 * 56; t += 16) Gq[t] = 0.;
+                    TG* Gq = G + 4 * qp * 56;
+                    for (int t = g; t < 4 * 56; t += 16) Gq[t] = TG(0);
                 }
                 // (1) interpolation: r, u_ddot, omega, omega_dot, u', r'
                 if (act) {
@@ -788,16 +867,16 @@ __global__ void __launch_bounds__(NT, (NT == 256) ? 2 : 1)
                     // G rows of this quadrature point (see the integration GEMM):
                     //   4q+1: w [Puu left | Puu right | 0], 4q+3: w [0 | Ouu right | 0]
                     const double w = qpw[qp * 4], wJ = qpw[qp * 4 + 2];
-                    double* G1 = G + (4 * qp + 1) * 56;
-                    double* G3 = G + (4 * qp + 3) * 56;
+                    TG* G1 = G + (4 * qp + 1) * 56;
+                    TG* G3 = G + (4 * qp + 3) * 56;
                     O12[g] = o12;
-                    G3[gcol(18 + g)] = w * o12;
-                    G3[gcol(18 + 9 + g)] = w * o22;
-                    G1[gcol(9 + g)] = w * p21;
-                    G1[gcol(18 + 9 + g)] = w * p22;
+                    G3[gcol(18 + g)] = static_cast<TG>(w * o12);
+                    G3[gcol(18 + 9 + g)] = static_cast<TG>(w * o22);
+                    G1[gcol(9 + g)] = static_cast<TG>(w * p21);
+                    G1[gcol(18 + 9 + g)] = static_cast<TG>(w * p22);
                     Gu[g] = g12;
                     Gu[9 + g] = g22;
-                    G[(4 * qp) * 56 + gcol(18 + g)] = wJ * k12;
+                    G[(4 * qp) * 56 + gcol(18 + g)] = static_cast<TG>(wJ * k12);
                     Kk[g] = k22;
                 } else if (act && g < 15) {
                     // Fd + Fi - Fe - Fg (calculate_force_FD.hpp, calculate_inertial_force.hpp,
@@ -839,13 +918,13 @@ __global__ void __launch_bounds__(NT, (NT == 256) ? 2 : 1)
                 //     G rows 4q+0: wJ [XI left | XK right | XI right], 4q+2: (w/J) [Cuu]
                 if (act) {
                     const double wJ = qpw[qp * 4 + 2], wdJ = qpw[qp * 4 + 3];
-                    double* G0 = G + (4 * qp) * 56;
-                    double* G2 = G + (4 * qp + 2) * 56;
+                    TG* G0 = G + (4 * qp) * 56;
+                    TG* G2 = G + (4 * qp + 2) * 56;
                     if (g < 9) {
                         const int i = g / 3, j = g % 3;
                         double qv = 0.;
                         for (int k = 0; k < 3; ++k) qv += tilde_e(sv3, k, i) * O12[k * 3 + j];
-                        G0[gcol(18 + 9 + g)] = wJ * (Kk[g] + qv);
+                        G0[gcol(18 + 9 + g)] = static_cast<TG>(wJ * (Kk[g] + qv));
                     }
                     for (int e = g; e < 36; e += 16) {
                         const int i = e / 6, j = e % 6;
@@ -853,8 +932,8 @@ __global__ void __launch_bounds__(NT, (NT == 256) ? 2 : 1)
                         if (j >= 3) gg = Gu[(i < 3 ? 0 : 9) + (i % 3) * 3 + (j - 3)];
                         const double xi = P.beta_prime * Mu[e] + P.gamma_prime * gg;
                         const int col = (j < 3) ? i * 3 + j : 36 + i * 3 + (j - 3);
-                        G0[gcol(col)] = wJ * xi;
-                        G2[gcol((j < 3) ? i * 3 + j : 18 + i * 3 + (j - 3))] = wdJ * Cu[e];
+                        G0[gcol(col)] = static_cast<TG>(wJ * xi);
+                        G2[gcol((j < 3) ? i * 3 + j : 18 + i * 3 + (j - 3))] = static_cast<TG>(wdJ * Cu[e]);
                     }
                 }
                 __syncwarp();
@@ -889,59 +968,72 @@ __global__ void __launch_bounds__(NT, (NT == 256) ? 2 : 1)
         {
             const int P2 = N * N;
             const int s4 = lane & 3;
-            const int mm = lane & 3;
-            const double* fi_tab = (mm < 2) ? phi : dphi;
-            const double* fj_tab = (mm == 0 || mm == 3) ? phi : dphi;
+            const double* fi_tab = (s4 < 2) ? phi : dphi;
+            const double* fj_tab = (s4 == 0 || s4 == 3) ? phi : dphi;
             const double cond = P.conditioner;
-            for (int p0 = 8 * warp; p0 < P2; p0 += 8 * NW) {
-                const int prow = p0 + (lane >> 2);
-                const bool valid = prow < P2;
-                const int i = valid ? prow / N : 0, jn = valid ? prow % N : 0;
-                double acc[7][2];
+            if constexpr (sizeof(TR) == 8) {
+                // FP64 tensor cores, m8n8k4: 8 pairs per tile, one point per k-step
+                for (int p0 = 8 * warp; p0 < P2; p0 += 8 * NW) {
+                    const int prow = p0 + (lane >> 2);
+                    const bool valid = prow < P2;
+                    const int i = valid ? prow / N : 0, jn = valid ? prow % N : 0;
+                    double acc[7][2];
 #pragma unroll
-                for (int nt = 0; nt < 7; ++nt) acc[nt][0] = acc[nt][1] = 0.;
-                for (int q = 0; q < Q; ++q) {
-                    const double av = valid ? fi_tab[q * N + i] * fj_tab[q * N + jn] : 0.;
-                    const double* gq = G + (4 * q + (lane & 3)) * 56 + (lane >> 2);
+                    for (int nt = 0; nt < 7; ++nt) acc[nt][0] = acc[nt][1] = 0.;
+                    for (int q = 0; q < Q; ++q) {
+                        const double av = valid ? fi_tab[q * N + i] * fj_tab[q * N + jn] : 0.;
+                        const TG* gq = G + (4 * q + s4) * 56 + (lane >> 2);
 #pragma unroll
-                    for (int nt = 0; nt < 7; ++nt) dmma884(acc[nt][0], acc[nt][1], av, gq[nt * 8]);
-                }
-                if (valid) {
-                    TR* Arow = A + (6 * pos[i]) * ldA + 6 * pos[jn];
-                    if (s4 < 3) {
-                        const double* Tj = sT + jn * 9;
-#pragma unroll
-                        for (int rr = 0; rr < 2; ++rr) {
-                            const int r = 2 * s4 + rr;
-                            // slots 6rr..6rr+2: RS[r][0..2]; 6rr+3..6rr+5: RI[r][0..2]
-                            double rs[3], ri[3];
-#pragma unroll
-                            for (int k = 0; k < 3; ++k) {
-                                rs[k] = acc[(6 * rr + k) >> 1][(6 * rr + k) & 1];
-                                ri[k] = acc[(6 * rr + 3 + k) >> 1][(6 * rr + 3 + k) & 1];
-                            }
-#pragma unroll
-                            for (int c = 0; c < 3; ++c) {
-                                double val = ri[c];
-#pragma unroll
-                                for (int k = 0; k < 3; ++k) val += rs[k] * Tj[k * 3 + c];
-                                Arow[r * ldA + 3 + c] = static_cast<TR>(val * cond);
-                            }
-                        }
-                        if (s4 < 2) {
-                            // slots 12, 13: L[14 + 2 s4 + e]
-#pragma unroll
-                            for (int e = 0; e < 2; ++e) {
-                                const int l = 14 + 2 * s4 + e;
-                                Arow[(l / 3) * ldA + l % 3] = static_cast<TR>(acc[6][e] * cond);
-                            }
-                        }
-                    } else {
-                        // slots 0..13: L[0..13]
-#pragma unroll
-                        for (int t = 0; t < 14; ++t)
-                            Arow[(t / 3) * ldA + t % 3] = static_cast<TR>(acc[t >> 1][t & 1] * cond);
+                        for (int nt = 0; nt < 7; ++nt) dmma884(acc[nt][0], acc[nt][1], av, gq[nt * 8]);
                     }
+                    if (valid)
+                        store_pair_block(A, ldA, pos, sT, i, jn, s4, cond,
+                                         [&](int t) { return acc[t >> 1][t & 1]; });
+                }
+            } else {
+                // FP32 form: TF32 tensor cores with the 3-term split (hi*hi + hi*lo +
+                // lo*hi, FP32 accumulation), m16n8k8: 16 pairs per tile, two points
+                // per k-step (an odd Q reads the zero pad point).
+                const int g8 = lane >> 2;
+                const int QK = (Q + 1) >> 1;
+                for (int p0 = 16 * warp; p0 < P2; p0 += 16 * NW) {
+                    const int pa = p0 + g8, pb = p0 + g8 + 8;
+                    const bool va = pa < P2, vb = pb < P2;
+                    const int ia = va ? pa / N : 0, ja = va ? pa % N : 0;
+                    const int ib = vb ? pb / N : 0, jb = vb ? pb % N : 0;
+                    float acc[7][4];
+#pragma unroll
+                    for (int nt = 0; nt < 7; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+                    for (int ks = 0; ks < QK; ++ks) {
+                        const int q0 = 2 * ks, q1 = 2 * ks + 1;
+                        const bool q1ok = q1 < Q;
+                        const int q1c = q1ok ? q1 : q0;
+                        float av[4];
+                        av[0] = va ? static_cast<float>(fi_tab[q0 * N + ia] * fj_tab[q0 * N + ja]) : 0.f;
+                        av[1] = vb ? static_cast<float>(fi_tab[q0 * N + ib] * fj_tab[q0 * N + jb]) : 0.f;
+                        av[2] = (va && q1ok) ? static_cast<float>(fi_tab[q1c * N + ia] * fj_tab[q1c * N + ja]) : 0.f;
+                        av[3] = (vb && q1ok) ? static_cast<float>(fi_tab[q1c * N + ib] * fj_tab[q1c * N + jb]) : 0.f;
+                        unsigned ah[4], al[4];
+#pragma unroll
+                        for (int r = 0; r < 4; ++r) split_tf32(av[r], ah[r], al[r]);
+                        const TG* g0 = G + (4 * q0 + s4) * 56 + g8;
+                        const TG* g1 = G + (4 * q1 + s4) * 56 + g8;
+#pragma unroll
+                        for (int nt = 0; nt < 7; ++nt) {
+                            unsigned bh[2], bl[2];
+                            split_tf32(static_cast<float>(g0[nt * 8]), bh[0], bl[0]);
+                            split_tf32(static_cast<float>(g1[nt * 8]), bh[1], bl[1]);
+                            mma_tf32(acc[nt], al, bh);
+                            mma_tf32(acc[nt], ah, bl);
+                            mma_tf32(acc[nt], ah, bh);
+                        }
+                    }
+                    if (va)
+                        store_pair_block(A, ldA, pos, sT, ia, ja, s4, cond,
+                                         [&](int t) { return static_cast<double>(acc[t >> 1][t & 1]); });
+                    if (vb)
+                        store_pair_block(A, ldA, pos, sT, ib, jb, s4, cond,
+                                         [&](int t) { return static_cast<double>(acc[t >> 1][2 + (t & 1)]); });
                 }
             }
         }
@@ -1200,6 +1292,10 @@ __global__ void __launch_bounds__(NT, (NT == 256) ? 2 : 1)
             break;
         }
         if (err <= 1.) {
+            if (extra < P.refine_iters) {
+                ++extra;  // one more correction from the FP64 residual
+                continue;
+            }
             status = KYN_OK;
             break;
         }

@@ -114,6 +114,7 @@ struct StepCoeffs {
     double atol, rtol;
     int32_t max_iter;
     int32_t dynamic;
+    int32_t refine_iters;  // extra corrections after convergence (FP32 form)
 };
 
 }  // namespace kyn

@@ -252,7 +252,8 @@ class StepParameters:
     """src/step/step_parameters.hpp:12-53 (derived coefficients kept for tests)."""
 
     def __init__(self, is_dynamic_solve: bool, max_iter: int, h: float, rho_inf: float,
-                 a_tol: float = 1e-5, r_tol: float = 1e-3, precision: int = 0):
+                 a_tol: float = 1e-5, r_tol: float = 1e-3, precision: int = 0,
+                 refine_iters: int = 0):
         self.is_dynamic_solve = bool(is_dynamic_solve)
         self.max_iter = int(max_iter)
         self.h = float(h)
@@ -268,11 +269,12 @@ class StepParameters:
         self.absolute_convergence_tol = float(a_tol)
         self.relative_convergence_tol = float(r_tol)
         self.precision = int(precision)
+        self.refine_iters = int(refine_iters)
 
     def to_c(self) -> "KynStepParams":
         return KynStepParams(int(self.is_dynamic_solve), self.max_iter, self.h, self.rho_inf,
                              self.absolute_convergence_tol, self.relative_convergence_tol,
-                             self.precision, 0)
+                             self.precision, self.refine_iters)
 
 
 # ---- C structs (include/kynema_b200.h) -------------------------------------
@@ -301,7 +303,7 @@ class KynStepParams(ctypes.Structure):
         ("h", ctypes.c_double), ("rho_inf", ctypes.c_double),
         ("absolute_convergence_tol", ctypes.c_double),
         ("relative_convergence_tol", ctypes.c_double),
-        ("precision", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("precision", ctypes.c_int32), ("refine_iters", ctypes.c_int32),
     ]
 
 

@@ -71,6 +71,8 @@ def load_library():
                                       ctypes.c_void_p, ctypes.c_int]
     L.kyn_get_state_batch.argtypes = [ctypes.c_void_p, _ip, ctypes.c_int, ctypes.c_int,
                                       ctypes.c_void_p, ctypes.c_int]
+    L.kyn_autotune.argtypes = [ctypes.c_void_p, _ip, ctypes.c_int, ctypes.c_void_p]
+    L.kyn_tuned_threads.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     L.kyn_set_loads_batch_static.argtypes = [ctypes.c_void_p, _ip, ctypes.c_int, ctypes.c_int,
                                              ctypes.c_void_p, ctypes.c_int]
     L.kyn_ctx_stat.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
@@ -190,6 +192,17 @@ class Context:
         """Loads for many models from one array at address `ptr` (host or device)."""
         self._check(self.lib.kyn_set_loads_batch(self.h, ids.ctypes.data_as(_ip), ids.shape[0],
                                                  which, ctypes.c_void_p(ptr), int(on_device)))
+
+    def autotune(self, ids, params) -> None:
+        """Pick threads per CTA for each size class of these models by timing
+        copies of them (the models themselves are not advanced)."""
+        arr = np.ascontiguousarray(ids, dtype=np.int32)
+        c = params.to_c()
+        self._check(self.lib.kyn_autotune(self.h, arr.ctypes.data_as(_ip), arr.shape[0],
+                                          ctypes.byref(c)))
+
+    def tuned_threads(self, mid: int, precision: int = 0) -> int:
+        return self._check(self.lib.kyn_tuned_threads(self.h, mid, precision))
 
     def set_loads_batch_static(self, ids: np.ndarray, which: int, ptr: int,
                                on_device: bool) -> None:
