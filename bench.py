@@ -186,6 +186,9 @@ def main() -> None:
     ap.add_argument("--cpu-steps", type=int, default=150)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32 + refinement form")
+    ap.add_argument("--serve", type=float, default=5.0,
+                    help="seconds of the serving workload per form (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=2000.0, help="request arrivals per second")
     ap.add_argument("--refine", type=int, default=0,
                     help="refinement corrections of the FP32 form after convergence")
     ap.add_argument("--nodes", type=int, default=0,
@@ -341,6 +344,29 @@ def main() -> None:
     conv_e = int(S.sum_over_ranks(conv_e, dist, dev))
     e2e = conv_e / (t_e2e_ms * 1e-3)
 
+    # ---- serving: Poisson request stream, continuous batching, both forms --------
+    serving = None
+    if args.serve > 0 and world == 1:
+        from openturbine_b200.serving import StepServer, poisson_requests, request_pool
+        pool_b, pool_r = request_pool(256, 32)
+        serving = {"workload": f"Poisson arrivals at {args.serve_rate:g}/s for {args.serve:g} s, "
+                               "90% single beams (nodes U{5..21}), 10% three-blade rotors (11 nodes "
+                               "per blade, prescribed hub rotation), U{50..500} steps per request",
+                   "hbm_budget_gb": 150}
+        for name, form in (("fp64", 0), ("fp32_refined", 1)):
+            sctx = Context(local, 150 * 10**9)
+            sp = W.batch_params()
+            sp.precision = form
+            srv = StepServer(sctx, sp)
+            for r in poisson_requests(args.serve_rate, args.serve, pool_b, pool_r):
+                srv.submit(r)
+            srv.run(until_s=args.serve)
+            serving[name] = srv.summary()
+            sctx.close()
+        if serving["fp64"]["converged_beam_steps_per_s"] > 0:
+            serving["fp32_vs_fp64"] = (serving["fp32_refined"]["converged_beam_steps_per_s"] /
+                                       serving["fp64"]["converged_beam_steps_per_s"])
+
     if rank == 0:
         achieved = flops_v / (sum(dev_ms) * 1e-3) / 1e12
         line = {
@@ -373,6 +399,8 @@ def main() -> None:
         line["clocks"] = r64["clocks"]
         if prec is not None:
             line["precision_form"] = prec
+        if serving is not None:
+            line["serving"] = serving
         if not args.no_cpu and world == 1:
             line["cpu_baseline"] = cpu_baseline(draws[: args.cpu_sample], params, args.cpu_steps,
                                                 os.cpu_count() or 1)

@@ -238,6 +238,13 @@ KYN_API int kyn_autotune(kyn_ctx* ctx, const int* model_ids, int n, const kyn_st
 /* Threads per CTA kyn_step uses for a model at a precision (tuned or default). */
 KYN_API int kyn_tuned_threads(kyn_ctx* ctx, int model_id, int precision);
 
+/* Batched Constraints::UpdateDisplacement for many models: values holds
+ * [sum of the listed models' constraints][7] (model order, then constraint
+ * order).  Replaces the per-blade prescribed hub motion updates of
+ * src/interfaces/turbine/turbine_interface.cpp:117-150. */
+KYN_API int kyn_set_prescribed_batch(kyn_ctx* ctx, const int* model_ids, int n, const double* values,
+                                     int on_device);
+
 /* Replaces host reads of State / Constraints views after Step(). */
 KYN_API int kyn_get_state(kyn_ctx* ctx, int model_id, int field, double* out);
 

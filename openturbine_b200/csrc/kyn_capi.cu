@@ -72,12 +72,7 @@ struct Plan {
     int* h_iters = nullptr;
     int nbeams = 0;
     bool record = false;
-    ~Plan() {
-        if (d_kbeams) cudaFree(d_kbeams);
-        if (d_status) cudaFree(d_status);
-        if (d_iters) cudaFree(d_iters);
-        if (h_status) cudaFreeHost(h_status);
-        if (h_iters) cudaFreeHost(h_iters);
+    ~Plan() {  // buffers belong to the context's plan pool
     }
 };
 
@@ -96,6 +91,7 @@ struct XferPlan {
     long long total = 0;  // doubles in the external array
     XferBeam* d_beams = nullptr;
     int* d_map = nullptr;
+    size_t beams_cap = 0, map_cap = 0;  // device buffers are reused when a slot is rebuilt
     int nbeams = 0;
     ~XferPlan() {
         if (d_beams) cudaFree(d_beams);
@@ -143,6 +139,18 @@ struct kyn_ctx {
     int64_t last_buckets = 0;
     unsigned long long* d_prof = nullptr; // phase timing counters (KYN_OPT_PHASE_TIMING)
     std::map<ClassKey, int> tuned;        // threads per CTA chosen by kyn_autotune
+    // Plan buffers, grown on demand and reused by every plan (one step in
+    // flight at a time), so rebuilding a plan for a changed model set (the
+    // serving loop does it every iteration) allocates nothing in steady state.
+    KBeam* pool_kbeams = nullptr;
+    size_t pool_kbeams_cap = 0;
+    int* pool_status = nullptr;           // device [2][cap]: status, iterations
+    int* pool_hstatus = nullptr;          // pinned [2][cap]
+    size_t pool_status_cap = 0;
+    std::vector<int> presc_ids;           // batched prescribed motion: cached targets
+    double** presc_targets = nullptr;     // device [count] slab addresses of con_input slots
+    size_t presc_cap = 0;
+    int presc_count = 0;
 };
 
 namespace {
@@ -305,14 +313,31 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
         }
     }
     plan->nbeams = static_cast<int>(kb.size());
-    KYN_CUDA(c, cudaMalloc(&plan->d_kbeams, sizeof(KBeam) * std::max<size_t>(1, kb.size())));
+    if (c->pool_kbeams_cap < kb.size()) {
+        if (c->pool_kbeams) KYN_CUDA(c, cudaFree(c->pool_kbeams));
+        c->pool_kbeams = nullptr;
+        const size_t cap = std::max<size_t>(kb.size() + kb.size() / 2, 256);
+        KYN_CUDA(c, cudaMalloc(&c->pool_kbeams, sizeof(KBeam) * cap));
+        c->pool_kbeams_cap = cap;
+    }
+    if (c->pool_status_cap < static_cast<size_t>(n)) {
+        if (c->pool_status) KYN_CUDA(c, cudaFree(c->pool_status));
+        if (c->pool_hstatus) KYN_CUDA(c, cudaFreeHost(c->pool_hstatus));
+        c->pool_status = nullptr;
+        c->pool_hstatus = nullptr;
+        const size_t cap = std::max<size_t>(n + n / 2, 256);
+        KYN_CUDA(c, cudaMalloc(&c->pool_status, sizeof(int) * 2 * cap));
+        KYN_CUDA(c, cudaMallocHost(&c->pool_hstatus, sizeof(int) * 2 * cap));
+        c->pool_status_cap = cap;
+    }
+    plan->d_kbeams = c->pool_kbeams;
+    plan->d_status = c->pool_status;
+    plan->d_iters = c->pool_status + c->pool_status_cap;
+    plan->h_status = c->pool_hstatus;
+    plan->h_iters = c->pool_hstatus + c->pool_status_cap;
+    // pageable source: the copy is staged before this call returns
     KYN_CUDA(c, cudaMemcpyAsync(plan->d_kbeams, kb.data(), sizeof(KBeam) * kb.size(),
                                 cudaMemcpyHostToDevice, c->stream));
-    KYN_CUDA(c, cudaMalloc(&plan->d_status, sizeof(int) * std::max(1, n)));
-    KYN_CUDA(c, cudaMalloc(&plan->d_iters, sizeof(int) * std::max(1, n)));
-    KYN_CUDA(c, cudaMallocHost(&plan->h_status, sizeof(int) * std::max(1, n)));
-    KYN_CUDA(c, cudaMallocHost(&plan->h_iters, sizeof(int) * std::max(1, n)));
-    KYN_CUDA(c, cudaStreamSynchronize(c->stream));
     c->plan = std::move(plan);
     *out = c->plan.get();
     return KYN_OK;
@@ -417,8 +442,10 @@ int get_xfer(kyn_ctx* c, const int* ids, int n, int kind, XferPlan** out) {
         *out = cached.get();
         return KYN_OK;
     }
-    auto xp = std::make_unique<XferPlan>();
+    // Reuse the slot's device buffers (the id set changes every serving iteration).
+    std::unique_ptr<XferPlan> xp = cached ? std::move(cached) : std::make_unique<XferPlan>();
     xp->ids.assign(ids, ids + n);
+    xp->width = 0;
     xp->kind = kind;
     std::vector<XferBeam> beams;
     std::vector<int> map;
@@ -454,13 +481,23 @@ int get_xfer(kyn_ctx* c, const int* ids, int n, int kind, XferPlan** out) {
     if (xp->width == 0) xp->width = 6;
     xp->total = off;
     xp->nbeams = static_cast<int>(beams.size());
-    KYN_CUDA(c, cudaMalloc(&xp->d_beams, sizeof(XferBeam) * std::max<size_t>(1, beams.size())));
-    KYN_CUDA(c, cudaMalloc(&xp->d_map, sizeof(int) * std::max<size_t>(1, map.size())));
+    if (xp->beams_cap < beams.size()) {
+        if (xp->d_beams) KYN_CUDA(c, cudaFree(xp->d_beams));
+        xp->d_beams = nullptr;
+        xp->beams_cap = std::max<size_t>(beams.size() + beams.size() / 2, 64);
+        KYN_CUDA(c, cudaMalloc(&xp->d_beams, sizeof(XferBeam) * xp->beams_cap));
+    }
+    if (xp->map_cap < map.size()) {
+        if (xp->d_map) KYN_CUDA(c, cudaFree(xp->d_map));
+        xp->d_map = nullptr;
+        xp->map_cap = std::max<size_t>(map.size() + map.size() / 2, 256);
+        KYN_CUDA(c, cudaMalloc(&xp->d_map, sizeof(int) * xp->map_cap));
+    }
+    // pageable sources: staged before the calls return; stream order does the rest
     KYN_CUDA(c, cudaMemcpyAsync(xp->d_beams, beams.data(), sizeof(XferBeam) * beams.size(),
                                 cudaMemcpyHostToDevice, c->stream));
     KYN_CUDA(c, cudaMemcpyAsync(xp->d_map, map.data(), sizeof(int) * map.size(),
                                 cudaMemcpyHostToDevice, c->stream));
-    KYN_CUDA(c, cudaStreamSynchronize(c->stream));
     cached = std::move(xp);
     *out = cached.get();
     return KYN_OK;
@@ -513,6 +550,10 @@ void kyn_ctx_destroy(kyn_ctx* c) {
         if (kv.second->d_dump) cudaFree(kv.second->d_dump);
     }
     c->models.clear();
+    if (c->pool_kbeams) cudaFree(c->pool_kbeams);
+    if (c->pool_status) cudaFree(c->pool_status);
+    if (c->pool_hstatus) cudaFreeHost(c->pool_hstatus);
+    if (c->presc_targets) cudaFree(c->presc_targets);
     if (c->h_stage) cudaFreeHost(c->h_stage);
     for (auto& x : c->xfer) x.reset();
     if (c->d_stage) cudaFree(c->d_stage);
@@ -623,7 +664,9 @@ int kyn_model_create(kyn_ctx* c, const kyn_model_desc* desc) {
         KYN_CUDA(c, cudaMallocAsync(&m->d_dump, tot * sizeof(double), c->stream));
         KYN_CUDA(c, cudaMemsetAsync(m->d_dump, 0, tot * sizeof(double), c->stream));
     }
-    KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+    // Stream-ordered: the uploads (from the model's own host copy, which it
+    // keeps) complete before any later work on the context stream, so a step
+    // in flight is not waited for.
     m->bytes = bytes;
     c->used += bytes;
     const int id = c->next_id++;
@@ -635,7 +678,8 @@ int kyn_model_destroy(kyn_ctx* c, int id) {
     if (!c) return KYN_ERR_INVALID;
     DevModel* m = find_model(c, id);
     if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
-    KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+    // Stream-ordered frees: a step in flight that uses the model (its bucket
+    // streams join the context stream) completes before the memory is reused.
     for (double* p : m->d_slab) KYN_CUDA(c, cudaFreeAsync(p, c->stream));
     if (m->d_conv) KYN_CUDA(c, cudaFreeAsync(m->d_conv, c->stream));
     if (m->d_dump) KYN_CUDA(c, cudaFreeAsync(m->d_dump, c->stream));
@@ -643,6 +687,10 @@ int kyn_model_destroy(kyn_ctx* c, int id) {
     c->models.erase(id);
     if (c->plan && std::find(c->plan->ids.begin(), c->plan->ids.end(), id) != c->plan->ids.end())
         c->plan.reset();
+    if (std::find(c->presc_ids.begin(), c->presc_ids.end(), id) != c->presc_ids.end())
+        c->presc_ids.clear();
+    for (auto& x : c->xfer)
+        if (x && std::find(x->ids.begin(), x->ids.end(), id) != x->ids.end()) x->ids.clear();
     return KYN_OK;
 }
 
@@ -916,6 +964,63 @@ int kyn_get_state_batch(kyn_ctx* c, const int* ids, int n, int field, double* ou
 }
 
 }  // extern "C"
+
+// ---- batched prescribed motion -------------------------------------------------
+namespace {
+
+__global__ void prescribed_kernel(double* const* __restrict__ targets, const double* __restrict__ vals,
+                                  int count) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < count * 7) targets[t / 7][t % 7] = vals[t];
+}
+
+}  // namespace
+
+extern "C" int kyn_set_prescribed_batch(kyn_ctx* c, const int* ids, int n, const double* values,
+                                        int on_device) {
+    if (!c || n < 0 || (n > 0 && (!ids || !values))) return KYN_ERR_INVALID;
+    if (n == 0) return KYN_OK;
+    KYN_CUDA(c, cudaSetDevice(c->device));
+    if (!(static_cast<int>(c->presc_ids.size()) == n && std::equal(ids, ids + n, c->presc_ids.begin()))) {
+        std::vector<double*> t;
+        for (int i = 0; i < n; ++i) {
+            DevModel* m = find_model(c, ids[i]);
+            if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id in batch");
+            for (int k = 0; k < m->host.num_constraints; ++k) {
+                const int bi = m->host.con_beam[k], slot = m->host.con_slot[k];
+                const HostBeam& b = m->host.beams[bi];
+                const SlabLayout L = make_slab_layout(b.N, b.Q);
+                t.push_back(m->d_slab[bi] + L.con_input + slot * 7);
+            }
+        }
+        if (c->presc_cap < t.size()) {
+            if (c->presc_targets) KYN_CUDA(c, cudaFree(c->presc_targets));
+            c->presc_targets = nullptr;
+            const size_t cap = std::max<size_t>(t.size() + t.size() / 2, 64);
+            KYN_CUDA(c, cudaMalloc(&c->presc_targets, sizeof(double*) * cap));
+            c->presc_cap = cap;
+        }
+        if (!t.empty())
+            KYN_CUDA(c, cudaMemcpyAsync(c->presc_targets, t.data(), sizeof(double*) * t.size(),
+                                        cudaMemcpyHostToDevice, c->stream));
+        c->presc_count = static_cast<int>(t.size());
+        c->presc_ids.assign(ids, ids + n);
+    }
+    const int cnt = c->presc_count;
+    if (cnt == 0) return KYN_OK;
+    const double* src = values;
+    if (!on_device) {
+        int rc = ensure_stage(c, static_cast<long long>(cnt) * 7);
+        if (rc != KYN_OK) return rc;
+        KYN_CUDA(c, cudaMemcpyAsync(c->d_stage, values, sizeof(double) * 7 * cnt,
+                                    cudaMemcpyHostToDevice, c->stream));
+        src = c->d_stage;
+    }
+    prescribed_kernel<<<(cnt * 7 + 255) / 256, 256, 0, c->stream>>>(c->presc_targets, src, cnt);
+    KYN_CUDA(c, cudaGetLastError());
+    c->launches++;
+    return KYN_OK;
+}
 
 // ---- autotuner: threads per CTA per model size class -----------------------------
 namespace {

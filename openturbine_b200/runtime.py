@@ -71,6 +71,8 @@ def load_library():
                                       ctypes.c_void_p, ctypes.c_int]
     L.kyn_get_state_batch.argtypes = [ctypes.c_void_p, _ip, ctypes.c_int, ctypes.c_int,
                                       ctypes.c_void_p, ctypes.c_int]
+    L.kyn_set_prescribed_batch.argtypes = [ctypes.c_void_p, _ip, ctypes.c_int, ctypes.c_void_p,
+                                           ctypes.c_int]
     L.kyn_autotune.argtypes = [ctypes.c_void_p, _ip, ctypes.c_int, ctypes.c_void_p]
     L.kyn_tuned_threads.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     L.kyn_set_loads_batch_static.argtypes = [ctypes.c_void_p, _ip, ctypes.c_int, ctypes.c_int,
@@ -192,6 +194,11 @@ class Context:
         """Loads for many models from one array at address `ptr` (host or device)."""
         self._check(self.lib.kyn_set_loads_batch(self.h, ids.ctypes.data_as(_ip), ids.shape[0],
                                                  which, ctypes.c_void_p(ptr), int(on_device)))
+
+    def set_prescribed_batch(self, ids: np.ndarray, ptr: int, on_device: bool) -> None:
+        """Prescribed motion [constraints of the listed models][7] from one array."""
+        self._check(self.lib.kyn_set_prescribed_batch(self.h, ids.ctypes.data_as(_ip), ids.shape[0],
+                                                      ctypes.c_void_p(ptr), int(on_device)))
 
     def autotune(self, ids, params) -> None:
         """Pick threads per CTA for each size class of these models by timing
