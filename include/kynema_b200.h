@@ -245,6 +245,26 @@ KYN_API int kyn_tuned_threads(kyn_ctx* ctx, int model_id, int precision);
 KYN_API int kyn_set_prescribed_batch(kyn_ctx* ctx, const int* model_ids, int n, const double* values,
                                      int on_device);
 
+/* Writes one node field ([nodes][7] or [nodes][6], model node order) into the
+ * resident state: the inverse of kyn_get_state for x0, x, q, q_prev, q_delta,
+ * v, vd, a and f. */
+KYN_API int kyn_set_state(kyn_ctx* ctx, int model_id, int field, const double* values);
+
+/* Restart record of WriteStateToFile / ReadStateFromFile
+ * (src/state/write_state_to_file.hpp:20-58, read_state_from_file.hpp:23-65):
+ * size_t num_system_nodes, then x0, x, q_delta, q_prev, q, v, vd, a, f as
+ * doubles, node-major.  kyn_state_write with buf NULL only reports the size;
+ * kyn_state_read rejects a record whose node count differs from the model's
+ * (the reference's std::length_error) with KYN_ERR_INVALID. */
+KYN_API int kyn_state_write(kyn_ctx* ctx, int model_id, void* buf, size_t capacity, size_t* bytes);
+KYN_API int kyn_state_read(kyn_ctx* ctx, int model_id, const void* buf, size_t size);
+
+/* CopyStateData (src/state/copy_state_data.hpp:21-34) between two models of the
+ * same structure: x, q_delta, q_prev, q, v, vd, a, f and the tangent blocks
+ * (the save / restore of the CFD predictor-corrector loop,
+ * src/interfaces/cfd/interface.cpp:312-327). */
+KYN_API int kyn_state_copy(kyn_ctx* ctx, int dst_model_id, int src_model_id);
+
 /* Replaces host reads of State / Constraints views after Step(). */
 KYN_API int kyn_get_state(kyn_ctx* ctx, int model_id, int field, double* out);
 

@@ -1022,6 +1022,129 @@ extern "C" int kyn_set_prescribed_batch(kyn_ctx* c, const int* ids, int n, const
     return KYN_OK;
 }
 
+// ---- state save / restore / copy (restart files, predictor-corrector) -----------
+namespace {
+
+// Slab offset and row width of a node field.
+int field_offset(int field, const SlabLayout& L, int* w) {
+    switch (field) {
+        case KYN_FIELD_X0: *w = 7; return L.x0;
+        case KYN_FIELD_X: *w = 7; return L.x;
+        case KYN_FIELD_Q: *w = 7; return L.q;
+        case KYN_FIELD_Q_PREV: *w = 7; return L.q_prev;
+        case KYN_FIELD_Q_DELTA: *w = 6; return L.q_delta;
+        case KYN_FIELD_V: *w = 6; return L.v;
+        case KYN_FIELD_VD: *w = 6; return L.vd;
+        case KYN_FIELD_A: *w = 6; return L.a;
+        case KYN_FIELD_F: *w = 6; return L.f;
+        default: return -1;
+    }
+}
+
+// Fields of the restart record, in file order (src/state/write_state_to_file.hpp:50-58).
+constexpr int kRestartFields[9] = {KYN_FIELD_X0, KYN_FIELD_X, KYN_FIELD_Q_DELTA, KYN_FIELD_Q_PREV,
+                                   KYN_FIELD_Q, KYN_FIELD_V, KYN_FIELD_VD, KYN_FIELD_A, KYN_FIELD_F};
+constexpr int kRestartWidth[9] = {7, 7, 6, 7, 7, 6, 6, 6, 6};
+
+}  // namespace
+
+extern "C" int kyn_set_state(kyn_ctx* c, int id, int field, const double* values) {
+    if (!c || !values) return KYN_ERR_INVALID;
+    DevModel* m = find_model(c, id);
+    if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
+    KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (size_t bi = 0; bi < m->host.beams.size(); ++bi) {
+        const HostBeam& b = m->host.beams[bi];
+        const SlabLayout L = make_slab_layout(b.N, b.Q);
+        int w = 0;
+        const int off = field_offset(field, L, &w);
+        if (off < 0) return set_err(c, KYN_ERR_INVALID, "field cannot be set");
+        std::vector<double> h(static_cast<size_t>(b.N) * w);
+        for (int k = 0; k < b.N; ++k)
+            for (int e = 0; e < w; ++e) h[k * w + e] = values[static_cast<size_t>(b.node_ids[k]) * w + e];
+        KYN_CUDA(c, cudaMemcpy(m->d_slab[bi] + off, h.data(), h.size() * sizeof(double),
+                               cudaMemcpyHostToDevice));
+    }
+    return KYN_OK;
+}
+
+extern "C" int kyn_state_write(kyn_ctx* c, int id, void* buf, size_t capacity, size_t* bytes) {
+    if (!c || !bytes) return KYN_ERR_INVALID;
+    DevModel* m = find_model(c, id);
+    if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
+    const size_t nn = static_cast<size_t>(m->host.num_nodes);
+    size_t need = sizeof(size_t);
+    for (int w : kRestartWidth) need += w * nn * sizeof(double);
+    *bytes = need;
+    if (!buf) return KYN_OK;
+    if (capacity < need) return set_err(c, KYN_ERR_INVALID, "restart buffer too small");
+    unsigned char* p = static_cast<unsigned char*>(buf);
+    std::memcpy(p, &nn, sizeof(size_t));
+    p += sizeof(size_t);
+    std::vector<double> tmp(7 * nn);
+    for (int f = 0; f < 9; ++f) {
+        const int rc = kyn_get_state(c, id, kRestartFields[f], tmp.data());
+        if (rc != KYN_OK) return rc;
+        const size_t len = kRestartWidth[f] * nn * sizeof(double);
+        std::memcpy(p, tmp.data(), len);
+        p += len;
+    }
+    return KYN_OK;
+}
+
+extern "C" int kyn_state_read(kyn_ctx* c, int id, const void* buf, size_t size) {
+    if (!c || !buf) return KYN_ERR_INVALID;
+    DevModel* m = find_model(c, id);
+    if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
+    const size_t nn = static_cast<size_t>(m->host.num_nodes);
+    if (size < sizeof(size_t)) return set_err(c, KYN_ERR_INVALID, "restart record too short");
+    size_t file_nodes = 0;
+    std::memcpy(&file_nodes, buf, sizeof(size_t));
+    if (file_nodes != nn)
+        return set_err(c, KYN_ERR_INVALID, "Number of system nodes in file is not the same as in model");
+    size_t need = sizeof(size_t);
+    for (int w : kRestartWidth) need += w * nn * sizeof(double);
+    if (size < need) return set_err(c, KYN_ERR_INVALID, "restart record too short");
+    const unsigned char* p = static_cast<const unsigned char*>(buf) + sizeof(size_t);
+    std::vector<double> tmp(7 * nn);
+    for (int f = 0; f < 9; ++f) {
+        const size_t len = kRestartWidth[f] * nn * sizeof(double);
+        std::memcpy(tmp.data(), p, len);
+        p += len;
+        const int rc = kyn_set_state(c, id, kRestartFields[f], tmp.data());
+        if (rc != KYN_OK) return rc;
+    }
+    return KYN_OK;
+}
+
+extern "C" int kyn_state_copy(kyn_ctx* c, int dst, int src) {
+    if (!c) return KYN_ERR_INVALID;
+    DevModel* d = find_model(c, dst);
+    DevModel* s = find_model(c, src);
+    if (!d || !s) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
+    if (d->host.beams.size() != s->host.beams.size())
+        return set_err(c, KYN_ERR_INVALID, "models differ in structure");
+    for (size_t bi = 0; bi < d->host.beams.size(); ++bi) {
+        const HostBeam& a = d->host.beams[bi];
+        const HostBeam& b = s->host.beams[bi];
+        if (a.N != b.N || a.Q != b.Q || a.nc != b.nc)
+            return set_err(c, KYN_ERR_INVALID, "models differ in structure");
+    }
+    // CopyStateData (src/state/copy_state_data.hpp:21-34): x, q_delta, q_prev, q, v,
+    // vd, a, f, tangent -- the slab's state arrays from x through the tangent block
+    for (size_t bi = 0; bi < d->host.beams.size(); ++bi) {
+        const HostBeam& b = d->host.beams[bi];
+        const SlabLayout L = make_slab_layout(b.N, b.Q);
+        const int fields[] = {L.x, L.q, L.q_prev, L.q_delta, L.v, L.vd, L.a, L.f, L.tangent};
+        const int widths[] = {7, 7, 7, 6, 6, 6, 6, 6, 9};
+        for (int k = 0; k < 9; ++k)
+            KYN_CUDA(c, cudaMemcpyAsync(d->d_slab[bi] + fields[k], s->d_slab[bi] + fields[k],
+                                        sizeof(double) * widths[k] * b.N, cudaMemcpyDeviceToDevice,
+                                        c->stream));
+    }
+    return KYN_OK;
+}
+
 // ---- autotuner: threads per CTA per model size class -----------------------------
 namespace {
 

@@ -73,6 +73,11 @@ def load_library():
                                       ctypes.c_void_p, ctypes.c_int]
     L.kyn_set_prescribed_batch.argtypes = [ctypes.c_void_p, _ip, ctypes.c_int, ctypes.c_void_p,
                                            ctypes.c_int]
+    L.kyn_set_state.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp]
+    L.kyn_state_write.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t,
+                                  ctypes.POINTER(ctypes.c_size_t)]
+    L.kyn_state_read.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]
+    L.kyn_state_copy.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     L.kyn_autotune.argtypes = [ctypes.c_void_p, _ip, ctypes.c_int, ctypes.c_void_p]
     L.kyn_tuned_threads.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     L.kyn_set_loads_batch_static.argtypes = [ctypes.c_void_p, _ip, ctypes.c_int, ctypes.c_int,
@@ -199,6 +204,24 @@ class Context:
         """Prescribed motion [constraints of the listed models][7] from one array."""
         self._check(self.lib.kyn_set_prescribed_batch(self.h, ids.ctypes.data_as(_ip), ids.shape[0],
                                                       ctypes.c_void_p(ptr), int(on_device)))
+
+    def set_state(self, mid: int, field: str, values: np.ndarray) -> None:
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        self._check(self.lib.kyn_set_state(self.h, mid, FIELD[field], v.ctypes.data_as(_dp)))
+
+    def write_restart(self, mid: int) -> bytes:
+        """The model's restart record (WriteStateToFile format)."""
+        n = ctypes.c_size_t(0)
+        self._check(self.lib.kyn_state_write(self.h, mid, None, 0, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value)
+        self._check(self.lib.kyn_state_write(self.h, mid, buf, n.value, ctypes.byref(n)))
+        return buf.raw
+
+    def read_restart(self, mid: int, record: bytes) -> None:
+        self._check(self.lib.kyn_state_read(self.h, mid, record, len(record)))
+
+    def copy_state(self, dst: int, src: int) -> None:
+        self._check(self.lib.kyn_state_copy(self.h, dst, src))
 
     def autotune(self, ids, params) -> None:
         """Pick threads per CTA for each size class of these models by timing
