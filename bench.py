@@ -186,6 +186,7 @@ def main() -> None:
     ap.add_argument("--cpu-steps", type=int, default=150)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32 + refinement form")
+    ap.add_argument("--no-graph", action="store_true", help="launch steps directly (no CUDA graph)")
     ap.add_argument("--serve", type=float, default=5.0,
                     help="seconds of the serving workload per form (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="request arrivals per second")
@@ -219,6 +220,8 @@ def main() -> None:
     if args.nodes:
         draws = [W.BeamDraw(d.model_id, args.nodes, d.length, d.amp, d.freq) for d in draws]
     ctx = Context(local)
+    if not args.no_graph:
+        ctx.set_cuda_graph(True)   # each step replays the captured bucket launches
     t_setup = time.perf_counter()
     ids = np.array([ctx.create_model(W.batch_cantilever_model(d).pack()) for d in draws],
                    dtype=np.int32)
@@ -381,6 +384,7 @@ def main() -> None:
                        "beams_per_gpu": args.beams, "h": 0.01, "rho_inf": 0.9,
                        "max_iter": params.max_iter, "a_tol": 1e-7, "r_tol": 1e-3,
                        "precision": "plain FP64", "l2": "flushed (256 MB write) before each step",
+                       "launch": "direct" if args.no_graph else "CUDA graph replay per step",
                        "parallelism": f"independent beam shards x{world}"},
             "latency_ms": {"p50": float(np.percentile(dev_ms, 50)),
                            "p99": float(np.percentile(dev_ms, 99)),

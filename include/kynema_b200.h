@@ -283,7 +283,10 @@ KYN_API int kyn_get_system_vectors(kyn_ctx* ctx, int model_id, double* rhs, doub
 
 enum {
     KYN_OPT_RECORD_SYSTEM = 1, /* keep the last assembled system for kyn_get_crs */
-    KYN_OPT_PHASE_TIMING = 2   /* count SM cycles per step-kernel phase (tracing) */
+    KYN_OPT_PHASE_TIMING = 2,  /* count SM cycles per step-kernel phase (tracing) */
+    KYN_OPT_CUDA_GRAPH = 3     /* capture each model set's step launches in a CUDA
+                                  graph and replay it (re-captured when the model
+                                  set or the step coefficients change) */
 };
 KYN_API int kyn_ctx_set_option(kyn_ctx* ctx, int option, int64_t value);
 

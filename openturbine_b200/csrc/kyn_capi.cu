@@ -72,7 +72,10 @@ struct Plan {
     int* h_iters = nullptr;
     int nbeams = 0;
     bool record = false;
+    cudaGraphExec_t graph = nullptr;  // captured step (KYN_OPT_CUDA_GRAPH)
+    StepCoeffs graph_coeffs{};        // coefficients baked into the captured launches
     ~Plan() {  // buffers belong to the context's plan pool
+        if (graph) cudaGraphExecDestroy(graph);
     }
 };
 
@@ -130,6 +133,7 @@ struct kyn_ctx {
     std::unique_ptr<Plan> plan;           // last launch plan (cache)
     std::vector<int> pending;             // models of the last kyn_step_async
     int smem_configured = 0;
+    bool use_graph = false;               // KYN_OPT_CUDA_GRAPH
     double* h_stage = nullptr;            // pinned staging for loads
     size_t h_stage_len = 0;
     std::unique_ptr<XferPlan> xfer[4];    // cached transfer plans
@@ -348,8 +352,7 @@ cudaError_t set_smem_attr(K kernel) {
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
 }
 
-int launch_plan(kyn_ctx* c, Plan* plan, const kyn_step_params* p) {
-    const StepCoeffs P = make_coeffs(p);
+int configure_smem(kyn_ctx* c) {
     if (c->smem_configured < kMaxDynSmem) {
         KYN_CUDA(c, set_smem_attr(step_kernel<double, 128>));
         KYN_CUDA(c, set_smem_attr(step_kernel<double, 256>));
@@ -359,6 +362,13 @@ int launch_plan(kyn_ctx* c, Plan* plan, const kyn_step_params* p) {
         KYN_CUDA(c, set_smem_attr(step_kernel<float, 512>));
         c->smem_configured = kMaxDynSmem;
     }
+    return KYN_OK;
+}
+
+int launch_plan(kyn_ctx* c, Plan* plan, const kyn_step_params* p) {
+    const StepCoeffs P = make_coeffs(p);
+    int rc = configure_smem(c);
+    if (rc != KYN_OK) return rc;
     KYN_CUDA(c, cudaEventRecord(c->fork, c->stream));
     const int nb = static_cast<int>(plan->buckets.size());
     for (int b = 0; b < nb; ++b) {
@@ -610,6 +620,11 @@ int kyn_ctx_set_option(kyn_ctx* c, int option, int64_t value) {
         c->plan.reset();
         return KYN_OK;
     }
+    if (option == KYN_OPT_CUDA_GRAPH) {
+        c->use_graph = value != 0;
+        c->plan.reset();
+        return KYN_OK;
+    }
     if (option == KYN_OPT_PHASE_TIMING) {
         KYN_CUDA(c, cudaStreamSynchronize(c->stream));
         if (value && !c->d_prof) {
@@ -785,7 +800,37 @@ int kyn_step_async(kyn_ctx* c, const int* ids, int n, const kyn_step_params* p) 
     Plan* plan = nullptr;
     int rc = get_plan(c, ids, n, p->precision, &plan);
     if (rc != KYN_OK) return rc;
-    return launch_plan(c, plan, p);
+    if (!c->use_graph) return launch_plan(c, plan, p);
+    // CUDA graph: capture the step's launch sequence (fork, bucket kernels,
+    // join, status copies) once per plan and coefficient set, then replay it.
+    const StepCoeffs P = make_coeffs(p);
+    if (!plan->graph || std::memcmp(&P, &plan->graph_coeffs, sizeof(P)) != 0) {
+        rc = configure_smem(c);
+        if (rc != KYN_OK) return rc;
+        if (plan->graph) {
+            KYN_CUDA(c, cudaGraphExecDestroy(plan->graph));
+            plan->graph = nullptr;
+        }
+        KYN_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        const int64_t before = c->launches;
+        rc = launch_plan(c, plan, p);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+        c->launches = before;
+        if (rc != KYN_OK) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        KYN_CUDA(c, ce);
+        const cudaError_t ie = cudaGraphInstantiate(&plan->graph, g, 0);
+        cudaGraphDestroy(g);
+        KYN_CUDA(c, ie);
+        plan->graph_coeffs = P;
+    }
+    KYN_CUDA(c, cudaGraphLaunch(plan->graph, c->stream));
+    c->launches += static_cast<int64_t>(plan->buckets.size());
+    c->last_buckets = static_cast<int64_t>(plan->buckets.size());
+    return KYN_OK;
 }
 
 int kyn_step_wait(kyn_ctx* c, int* status_out, int* iters_out) {

@@ -24,7 +24,7 @@ FIELD = {"x0": 0, "x": 1, "q": 2, "q_prev": 3, "q_delta": 4, "v": 5, "vd": 6, "a
 WIDTH = {"x0": 7, "x": 7, "q": 7, "q_prev": 7, "q_delta": 6, "v": 6, "vd": 6, "a": 6, "f": 6,
          "lambda": 6, "tangent": 36}
 LOAD_NODE_FX, LOAD_STATE_F = 0, 1
-OPT_RECORD_SYSTEM = 1
+OPT_RECORD_SYSTEM, OPT_PHASE_TIMING, OPT_CUDA_GRAPH = 1, 2, 3
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -116,6 +116,10 @@ class Context:
         if rc < 0:
             raise KynError(rc, self.lib.kyn_last_error(self.h).decode())
         return rc
+
+    def set_cuda_graph(self, on: bool = True) -> None:
+        """Replay each model set's step launches from a captured CUDA graph."""
+        self._check(self.lib.kyn_ctx_set_option(self.h, OPT_CUDA_GRAPH, int(on)))
 
     def set_record_system(self, on: bool = True) -> None:
         self._check(self.lib.kyn_ctx_set_option(self.h, OPT_RECORD_SYSTEM, int(on)))

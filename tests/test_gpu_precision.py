@@ -128,3 +128,30 @@ def test_autotune_keeps_results(ctx):
     for (s0, i0), (s1, i1) in zip(r0, r1):
         assert np.array_equal(s0, s1) and np.array_equal(i0, i1)
     assert np.abs(q0 - q1).max() <= 1e-12 * max(1.0, np.abs(q0).max())
+
+
+def test_cuda_graph_replay_matches_direct_launches():
+    """Steps replayed from the captured graph give the same results and
+    launch counts as direct launches."""
+    from openturbine_b200.runtime import Context
+    draws = W.draw_batch(40, first_id=9100)
+    pms = [W.batch_cantilever_model(d).pack() for d in draws]
+    p = W.batch_params()
+    runs = []
+    for graph in (False, True):
+        c = Context(0)
+        c.set_cuda_graph(graph)
+        ids = np.array([c.create_model(pm) for pm in pms], dtype=np.int32)
+        res = []
+        for k in range(5):
+            fz = W.tip_loads(draws, k)
+            for i, d in enumerate(draws):
+                c.set_node_fx(int(ids[i]), W.node_fx_for(d, fz[i]))
+            l0 = c.kernel_launches
+            res.append(c.step(ids, p) + (c.kernel_launches - l0,))
+        runs.append((res, np.concatenate([c.state(int(i), "q") for i in ids])))
+        c.close()
+    (r0, q0), (r1, q1) = runs
+    for (s0, i0, n0), (s1, i1, n1) in zip(r0, r1):
+        assert np.array_equal(s0, s1) and np.array_equal(i0, i1) and n0 == n1 > 0
+    np.testing.assert_array_equal(q0, q1)
