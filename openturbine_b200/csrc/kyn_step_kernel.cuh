@@ -149,6 +149,7 @@ struct Smem {
     int b;              // double [n6]  permuted rhs
     int xs;             // double [n6]  permuted solution
     int rpiv;           // double [n6]  reciprocal pivots
+    int stage;          // double [64]  U12 tile staged by warp 0 during the LU
     int con;            // double [nc][kConStride]
     int red;            // double [2][NT/32 + 8]
     int pos;            // int [N]
@@ -194,6 +195,7 @@ __host__ __device__ inline Smem make_smem(int N, int Q, int nc, int real_bytes, 
     S.b = take(n6 * 8);
     S.xs = take(n6 * 8);
     S.rpiv = take(n6 * 8);
+    S.stage = take(64 * 8);
     S.con = take((nc > 0 ? nc : 1) * kConStride * 8);
     S.red = take(2 * (nt / 32 + 8) * 8);
     S.pos = take(N * 4);
@@ -580,6 +582,7 @@ __global__ void __launch_bounds__(NT, (NT == 128) ? 4 : (NT == 256) ? 2 : 1)
     double* bp = reinterpret_cast<double*>(smem_raw + S.b);
     double* xs = reinterpret_cast<double*>(smem_raw + S.xs);
     double* rpiv = reinterpret_cast<double*>(smem_raw + S.rpiv);
+    double* stage = reinterpret_cast<double*>(smem_raw + S.stage);
     double* con = reinterpret_cast<double*>(smem_raw + S.con);
     double* gscr = reinterpret_cast<double*>(smem_raw + S.A);  // quadrature phase only
     double* red = reinterpret_cast<double*>(smem_raw + S.red);
@@ -1155,32 +1158,53 @@ __global__ void __launch_bounds__(NT, (NT == 128) ? 4 : (NT == 256) ? 2 : 1)
         __syncthreads();
         mark(kPhaseEliminate);
         // (S3) LU without pivoting of the free block A[0:m][0:m]; the right-hand
-        //      side in column m is eliminated with it.  Right-looking with panels
-        //      of kPanel columns and one CTA barrier per panel: warp 0 updates the
-        //      next panel's columns and factors that panel (look-ahead) while the
-        //      other warps apply the current panel to the columns right of it.
+        //      side in column m is eliminated with it.  Right-looking, panels of
+        //      kPanel columns, two CTA barriers per panel:
+        //      phase 1 - warp 0 applies panel k to the next panel's diagonal rows
+        //                (its U12 tile goes to a stage) and factors the next
+        //                diagonal block; the other warps apply panel k to the rows
+        //                below it and to every other column tile;
+        //      phase 2 - the stage is copied into A and all threads solve the next
+        //                panel's L21 rows (one row per thread).
         //      Multipliers are stored scaled; rpiv keeps the reciprocal pivots.
         if (m > 0) {
-            if (warp == 0) factor_panel(A, ldA, m, 0, rpiv, lane, &s_flag);
+            if (warp == 0) factor_diag(A, ldA, m, 0, rpiv, lane, &s_flag);
+            __syncthreads();
+            solve_l21(A, ldA, m, 0, rpiv, min(kPanel, m), tid, NT);
             __syncthreads();
             for (int k0 = 0; k0 < m; k0 += kPanel) {
                 const int kb = min(kPanel, m - k0);
                 const int r0 = k0 + kb;
                 const int nct = (m + 1 - r0 + 7) / 8;  // column tiles of [r0, m], rhs included
+                const int top = min(r0 + kPanel, m);   // rows of the next diagonal block
                 if (warp == 0) {
-                    update_tile<kU12InPlace>(A, ldA, m, k0, kb, r0, r0, m, nullptr, lane);
+                    update_tile<kU12ToStage>(A, ldA, m, k0, kb, r0, r0, top, stage, lane);
                     mark(kPhaseLUDiag);
                     if (r0 < m) {
                         __syncwarp();
-                        factor_panel(A, ldA, m, r0, rpiv, lane, &s_flag);
+                        factor_diag(A, ldA, m, r0, rpiv, lane, &s_flag);
                     }
                     mark(kPhaseLUPanel);
                 } else {
-                    for (int ct = warp; ct < nct; ct += NW - 1)
-                        update_tile<kU12InPlace>(A, ldA, m, k0, kb, r0 + 8 * ct, r0, m, nullptr, lane);
+                    // unit 0: tile 0 below the next diagonal block; unit u >= 1: tile u
+                    for (int u = warp - 1; u < nct; u += NW - 1) {
+                        if (u == 0) {
+                            if (top < m)
+                                update_tile<kU12InRegs>(A, ldA, m, k0, kb, r0, top, m, nullptr, lane);
+                        } else {
+                            update_tile<kU12InPlace>(A, ldA, m, k0, kb, r0 + 8 * u, r0, m, nullptr, lane);
+                        }
+                    }
                 }
                 __syncthreads();
                 mark(kPhaseFactor);
+                if (tid < 64) {  // tile 0 of U12 (rows k0+1 .. k0+kb-1) from the stage
+                    const int j = tid >> 3, c = r0 + (tid & 7);
+                    if (j >= 1 && j < kb && c <= m) A[(k0 + j) * ldA + c] = static_cast<TR>(stage[tid]);
+                }
+                if (top < m) solve_l21(A, ldA, m, r0, rpiv, top, tid, NT);
+                __syncthreads();
+                mark(kPhaseIntEpilogue);
             }
         }
         // (S4) back substitution U x = y (y in column m): every warp inverts some

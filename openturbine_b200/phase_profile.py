@@ -18,8 +18,8 @@ from . import workloads as W
 from .runtime import LOAD_NODE_FX, OPT_PHASE_TIMING, Context
 
 PHASES = ["load_predict", "quadrature", "integrate_gemm", "constraints", "eliminate",
-          "lu_barrier_wait", "substitute", "update", "store", "lu_next_panel_update",
-          "lu_panel_factor", "unused"]
+          "lu_barrier_wait", "substitute", "update", "store", "lu_warp0_next_rows",
+          "lu_warp0_diag_factor", "lu_l21_all_threads"]
 
 
 def main() -> None:
@@ -54,7 +54,7 @@ def main() -> None:
     print(json.dumps({"beams": args.beams, "nodes": args.nodes or "mixed",
                       "precision": args.precision, "beam_iterations": iters,
                       "cycles_per_beam_iteration": {n: round(c / max(iters, 1))
-                                                    for n, c in zip(PHASES, cyc) if n != "unused"}}))
+                                                    for n, c in zip(PHASES, cyc)}}))
     ctx.close()
 
 
