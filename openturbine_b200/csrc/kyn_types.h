@@ -104,7 +104,7 @@ enum Phase {
     kPhaseStore = 8,        // post-step and write-back
     kPhaseLUDiag = 9,       // LU: diagonal-block factorisation (part of the factor phase)
     kPhaseLUPanel = 10,     // LU: panel solves (part of the factor phase)
-    kPhaseIntEpilogue = 11, // integration: S T + I epilogue into A (part of integrate)
+    kPhaseIntEpilogue = 11, // LU: L21 rows solved by all threads (part of the factor phase)
     kNumPhases = 12
 };
 
