@@ -59,7 +59,9 @@ enum {
  * single-node boundary conditions used by beams and rotors. */
 enum {
     KYN_CONSTRAINT_FIXED_BC = 1,
-    KYN_CONSTRAINT_PRESCRIBED_BC = 2
+    KYN_CONSTRAINT_PRESCRIBED_BC = 2,
+    KYN_CONSTRAINT_RIGID_JOINT = 3   /* base node (hub) to target node, six DOFs
+                                        (src/constraints/calculate_rigid_joint_constraint.hpp) */
 };
 
 /* Node-state fields readable with kyn_get_state (src/state/state.hpp:18-68,

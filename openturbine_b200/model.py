@@ -29,6 +29,7 @@ import numpy as np
 # ---- constraint types (src/constraints/constraint_type.hpp:9-24) ----------
 FIXED_BC = 1
 PRESCRIBED_BC = 2
+RIGID_JOINT = 3
 INVALID_NODE_ID = 0  # Model::InvalidNodeID
 
 
@@ -411,6 +412,12 @@ class Model:
         self.constraints_.append(Constraint(cid, PRESCRIBED_BC, (INVALID_NODE_ID, int(node_id)),
                                             (0.0, 0.0, 0.0),
                                             tuple(float(x) for x in initial_displacement)))
+        return cid
+
+    def AddRigidJointConstraint(self, node_ids) -> int:
+        """src/model/model.hpp AddRigidJointConstraint({base, target})."""
+        cid = len(self.constraints_)
+        self.constraints_.append(Constraint(cid, RIGID_JOINT, (int(node_ids[0]), int(node_ids[1]))))
         return cid
 
     def NumConstraints(self) -> int:

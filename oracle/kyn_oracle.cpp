@@ -438,6 +438,9 @@ struct OConstraint {
     double sys_res[6] = {};
     double t_grad_tan[36] = {};
     double t_grad_trans[36] = {};
+    double b_grad_tan[36] = {};      // rigid joint: base-node blocks
+    double b_grad_trans[36] = {};
+    double b_lambda_res[6] = {};
     long row_first = 0, row_last = 0;
     long base_active = 0, target_active = 0;
     long base_table[6] = {};
@@ -596,7 +599,13 @@ void update_beam(orc_model& m, OBeam& B, double beta_prime, double gamma_prime) 
 }
 
 // src/constraints/calculate_constraint_residual_gradient.hpp:60-199 (FixedBC, PrescribedBC)
+void update_rigid_joint(orc_model& m, OConstraint& C);
+
 void update_constraint(orc_model& m, OConstraint& C) {
+    if (C.type == KYN_CONSTRAINT_RIGID_JOINT) {
+        update_rigid_joint(m, C);
+        return;
+    }
     const double* nu = &m.q[C.target * 7];
     double u1[3] = {0., 0., 0.};
     double R1[4] = {1., 0., 0., 0.};
@@ -622,6 +631,45 @@ void update_constraint(orc_model& m, OConstraint& C) {
         for (int j = 0; j < 6; ++j) C.t_grad_trans[i * 6 + j] = grad[j * 6 + i];
     gemm(false, false, 6, 6, 6, 1., grad.data(), 6, &m.tangent[C.target * 36], 6, 0.,
          C.t_grad_tan, 6);
+    gemv(false, 6, 6, 1., C.t_grad_trans, 6, C.lambda, 0., C.t_lambda_res);
+}
+
+// src/constraints/calculate_rigid_joint_constraint.hpp:17-113 and the RigidJoint
+// branch of calculate_constraint_residual_gradient.hpp:251-320
+void update_rigid_joint(orc_model& m, OConstraint& C) {
+    const double* bu = &m.q[C.base * 7];
+    const double* tu = &m.q[C.target * 7];
+    const double u1[3] = {bu[0], bu[1], bu[2]};
+    const double R1[4] = {bu[3], bu[4], bu[5], bu[6]};
+    const double u2[3] = {tu[0], tu[1], tu[2]};
+    const double R2[4] = {tu[3], tu[4], tu[5], tu[6]};
+    const V4 R1t = quat_inverse(R1);
+    const V3 R1X0 = rotate_vec(R1, C.X0);
+    for (int c = 0; c < 3; ++c) C.res[c] = u2[c] + C.X0[c] - u1[c] - R1X0[c];
+    const V4 R2R1t = quat_compose(R2, R1t.data());
+    const M3 Cm = quat_to_rot(R2R1t.data());
+    const V3 ax = axial(Cm);
+    for (int c = 0; c < 3; ++c) C.res[3 + c] = ax[c];
+    const M3 A = ax_matrix(Cm);
+    M6 tg{}, bg{};
+    for (int c = 0; c < 3; ++c) tg[c * 7] = 1.;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) tg[(3 + i) * 6 + 3 + j] = A[j * 3 + i];
+    for (int c = 0; c < 3; ++c) bg[c * 7] = -1.;
+    // B(0:3,3:6) = tilde(R1 X0)
+    const double tl[9] = {0., -R1X0[2], R1X0[1], R1X0[2], 0., -R1X0[0], -R1X0[1], R1X0[0], 0.};
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) bg[i * 6 + 3 + j] = tl[i * 3 + j];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) bg[(3 + i) * 6 + 3 + j] = -A[i * 3 + j];
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) {
+            C.t_grad_trans[i * 6 + j] = tg[j * 6 + i];
+            C.b_grad_trans[i * 6 + j] = bg[j * 6 + i];
+        }
+    gemm(false, false, 6, 6, 6, 1., bg.data(), 6, &m.tangent[C.base * 36], 6, 0., C.b_grad_tan, 6);
+    gemm(false, false, 6, 6, 6, 1., tg.data(), 6, &m.tangent[C.target * 36], 6, 0., C.t_grad_tan, 6);
+    gemv(false, 6, 6, 1., C.b_grad_trans, 6, C.lambda, 0., C.b_lambda_res);
     gemv(false, 6, 6, 1., C.t_grad_trans, 6, C.lambda, 0., C.t_lambda_res);
 }
 
@@ -834,11 +882,20 @@ void assemble(orc_model& m, const Params& P) {
         for (long i = C.row_first; i < C.row_last; ++i) {
             const long rn = i - C.row_first;
             const long row = m.nsys + i;
+            if (C.base_active) {  // src/solver/copy_constraints_to_sparse_matrix.hpp:37-84
+                long boff = find_offset(m, row, C.base_table[0]);
+                for (long e = 0; e < C.base_active; ++e, ++boff) m.values[boff] += C.b_grad_tan[rn * 6 + e];
+            }
             long off = find_offset(m, row, C.target_table[0]);
             for (long e = 0; e < C.target_active; ++e, ++off) m.values[off] += C.t_grad_tan[rn * 6 + e];
         }
         const long first_col = C.row_first + m.nsys;
         const long ncols = C.row_last - C.row_first;
+        for (long i = C.base_table[0]; C.base_active && i < C.base_table[0] + C.base_active; ++i) {
+            const long rn = i - C.base_table[0];
+            long off = find_offset(m, i, first_col);
+            for (long e = 0; e < ncols; ++e, ++off) m.values[off] += C.b_grad_trans[rn * 6 + e];
+        }
         for (long i = C.target_table[0]; i < C.target_table[0] + C.target_active; ++i) {
             const long rn = i - C.target_table[0];
             long off = find_offset(m, i, first_col);
@@ -848,6 +905,8 @@ void assemble(orc_model& m, const Params& P) {
     // src/step/assemble_constraints_residual.hpp
     for (auto& C : m.cons)
         for (long c = 0; c < C.target_active; ++c) m.b[C.target_table[c]] += C.sys_res[c];
+    for (auto& C : m.cons)  // src/solver/contribute_lambda_to_vector.hpp:34-51
+        for (long c = 0; c < C.base_active; ++c) m.b[C.base_table[0] + c] += C.b_lambda_res[c];
     for (auto& C : m.cons)
         for (long c = 0; c < C.target_active; ++c) m.b[C.target_table[0] + c] += C.t_lambda_res[c];
     for (auto& C : m.cons)
@@ -1141,7 +1200,8 @@ orc_model* orc_model_create(const kyn_model_desc* d, char* err, int errlen) {
     for (int c = 0; c < d->num_constraints; ++c) {
         OConstraint& C = m->cons[c];
         C.type = d->constraint_type[c];
-        if (C.type != KYN_CONSTRAINT_FIXED_BC && C.type != KYN_CONSTRAINT_PRESCRIBED_BC) {
+        if (C.type != KYN_CONSTRAINT_FIXED_BC && C.type != KYN_CONSTRAINT_PRESCRIBED_BC &&
+            C.type != KYN_CONSTRAINT_RIGID_JOINT) {
             bad(err, errlen, "constraint type outside this path");
             delete m;
             return nullptr;
@@ -1153,7 +1213,12 @@ orc_model* orc_model_create(const kyn_model_desc* d, char* err, int errlen) {
             delete m;
             return nullptr;
         }
-        C.base_active = 0;
+        if (C.type == KYN_CONSTRAINT_RIGID_JOINT && (C.base < 0 || C.base >= nn || C.base == C.target)) {
+            bad(err, errlen, "rigid joint base node out of range");
+            delete m;
+            return nullptr;
+        }
+        C.base_active = (C.type == KYN_CONSTRAINT_RIGID_JOINT) ? 6 : 0;
         C.target_active = 6;
         C.row_first = start_row;
         C.row_last = start_row + 6;
@@ -1163,6 +1228,9 @@ orc_model* orc_model_create(const kyn_model_desc* d, char* err, int errlen) {
                                 d->constraint_axis ? d->constraint_axis[c * 3 + 2] : 0.};
         if (C.type == KYN_CONSTRAINT_FIXED_BC) {
             for (int k = 0; k < 3; ++k) C.X0[k] = m->x0[C.target * 7 + k] - axis[k];
+        } else if (C.type == KYN_CONSTRAINT_RIGID_JOINT) {
+            // src/constraints/constraints.hpp:268-290: relative position target - base
+            for (int k = 0; k < 3; ++k) C.X0[k] = m->x0[C.target * 7 + k] - m->x0[C.base * 7 + k];
         } else {
             const double idq[7] = {0., 0., 0., 1., 0., 0., 0.};
             for (int k = 0; k < 7; ++k)
@@ -1176,7 +1244,10 @@ orc_model* orc_model_create(const kyn_model_desc* d, char* err, int errlen) {
     m->sig.assign(nn, 0U);
     for (auto& B : m->beams)
         for (int id : B.node_ids) m->sig[id] |= 0b111111U;
-    for (auto& C : m->cons) m->sig[C.target] |= 0b111111U;
+    for (auto& C : m->cons) {
+        m->sig[C.target] |= 0b111111U;
+        if (C.base_active) m->sig[C.base] |= 0b111111U;
+    }
     m->active.resize(nn);
     for (int n = 0; n < nn; ++n) m->active[n] = count_bits(m->sig[n]);
     // compute_node_freedom_map_table.hpp
@@ -1188,7 +1259,7 @@ orc_model* orc_model_create(const kyn_model_desc* d, char* err, int errlen) {
             for (int c = 0; c < 6; ++c) B.eft[n * 6 + c] = m->fmap[B.node_ids[n]] + c;
     for (auto& C : m->cons) {
         for (long c = 0; c < m->active[C.target]; ++c) C.target_table[c] = m->fmap[C.target] + c;
-        for (int c = 0; c < 6; ++c) C.base_table[c] = 0;
+        for (int c = 0; c < 6; ++c) C.base_table[c] = C.base_active ? m->fmap[C.base] + c : 0;
     }
     m->nsys = 0;
     for (int n = 0; n < nn; ++n) m->nsys += m->active[n];

@@ -99,3 +99,27 @@ def test_rotating_beam_ten_steps():
         st, _ = o.step(p)
         assert st == 0
     np.testing.assert_allclose(o.state("q").ravel(), g["q"], rtol=0, atol=g["tolerance"])
+
+
+def test_iea15_hub_rotor_converges_and_holds_the_joints():
+    """test_rotor.cpp:191-243 (IEA15RotorHub): every step converges within
+    max_iter = 6, the hub follows its prescribed rotation, and every blade root
+    stays rigidly attached: u_root = R_hub X0 - X0 and R_root = R_hub R0."""
+    from openturbine_b200.model import QuaternionCompose, RotateVectorByQuaternion
+    from tests.workloads_ref import iea15_hub_rotor_model
+    d = load_golden("iea15_rotor.json")
+    m, p, hub_bc, hub_id = iea15_hub_rotor_model(d)
+    o = OracleModel(m.pack())
+    assert o.info.num_dofs == 3 * 66 + 6 + 4 * 6
+    for i in range(d["num_steps"]):
+        o.set_prescribed(hub_bc, iea15_hub_displacement(i, d))
+        st, it = o.step(p)
+        assert st == 0 and it <= 6
+    q, x0 = o.state("q"), o.state("x0")
+    qh = q[hub_id, 3:]
+    np.testing.assert_allclose(q[hub_id], iea15_hub_displacement(d["num_steps"] - 1, d), atol=1e-12)
+    for be in m.GetBeamElements():
+        r = be.node_ids[0]
+        X0 = x0[r, :3] - x0[hub_id, :3]
+        np.testing.assert_allclose(q[r, :3], np.array(RotateVectorByQuaternion(qh, X0)) - X0, atol=1e-6)
+        np.testing.assert_allclose(np.abs(np.dot(q[r, 3:], qh)), 1.0, atol=1e-9)

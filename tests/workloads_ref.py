@@ -136,3 +136,32 @@ def iea15_hub_displacement(i: int, data: dict | None = None):
     w, h = d["omega"], d["h"]
     q = RotationVectorToQuaternion([w[0] * h * (i + 1), w[1] * h * (i + 1), w[2] * h * (i + 1)])
     return [0., 0., 0., *q]
+
+
+def iea15_hub_rotor_model(data: dict | None = None):
+    """test_rotor.cpp:191-243 (IEA15RotorHub): the IEA-15 blades of
+    CreateIEA15Blades, a hub node at the origin, a rigid joint from the hub to
+    every blade root and a prescribed hub motion."""
+    d = data or load_golden("iea15_rotor.json")
+    m = Model()
+    m.SetGravity(*d["gravity"])
+    node_loc = [(xi + 1.) / 2. for xi in d["node_xi"]]
+    sections = [BeamSection(s["position"], np.array(s["M_star"]).reshape(6, 6),
+                            np.array(s["C_star"]).reshape(6, 6)) for s in d["sections"]]
+    omega = d["omega"]
+    velocity = [0., 0., 0., omega[0], omega[1], omega[2]]
+    hub = [d["hub_radius"], 0., 0.]
+    for b in range(3):
+        rq = RotationVectorToQuaternion([0., 0., -2. * math.pi * b / 3])
+        ids = [m.AddNode().SetElemLocation(node_loc[j]).SetPosition(d["node_coords"][j]).Build()
+               for j in range(len(node_loc))]
+        e = m.AddBeamElement(ids, sections, d["quadrature"])
+        m.TranslateBeam(e, hub)
+        m.RotateBeamAboutPoint(e, rq, [0., 0., 0.])
+        m.SetBeamVelocityAboutPoint(e, velocity, [0., 0., 0.])
+    hub_id = m.AddNode().SetPosition(0., 0., 0., 1., 0., 0., 0.).Build()
+    for be in m.GetBeamElements():
+        m.AddRigidJointConstraint([hub_id, be.node_ids[0]])
+    hub_bc = m.AddPrescribedBC(hub_id)
+    params = StepParameters(True, 6, d["h"], 0.0)
+    return m, params, hub_bc, hub_id
