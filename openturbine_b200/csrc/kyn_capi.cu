@@ -153,6 +153,8 @@ struct kyn_ctx {
     size_t pool_status_cap = 0;
     std::vector<int> presc_ids;           // batched prescribed motion: cached targets
     double** presc_targets = nullptr;     // device [count] slab addresses of con_input slots
+    int* presc_vidx = nullptr;            // device [count] row of the caller's array per target
+    int presc_rows = 0;                   // constraint rows of the cached id list
     size_t presc_cap = 0;
     int presc_count = 0;
 };
@@ -200,13 +202,13 @@ StepCoeffs make_coeffs(const kyn_step_params* p) {
 // Default threads per CTA for a beam: 256 when two such CTAs fit on an SM
 // (their serial phases overlap), else 512 so the one resident CTA has 16
 // warps.  kyn_autotune replaces the default per size class by measurement.
-int beam_threads(int N, int Q, int nc, int real_bytes) {
-    const int s256 = make_smem(N, Q, nc, real_bytes, 256).bytes;
+int beam_threads(int N, int Q, int nc, int real_bytes, int hub = 0) {
+    const int s256 = make_smem(N, Q, nc, real_bytes, 256, hub).bytes;
     return (2 * (s256 + 1024) <= kSmemPerSM) ? 256 : 512;
 }
 
-int beam_smem(int N, int Q, int nc, int real_bytes, int nt) {
-    return make_smem(N, Q, nc, real_bytes, nt).bytes;
+int beam_smem(int N, int Q, int nc, int real_bytes, int nt, int hub = 0) {
+    return make_smem(N, Q, nc, real_bytes, nt, hub).bytes;
 }
 
 // Resident CTAs per SM for a thread count and shared-memory size; the step
@@ -259,13 +261,14 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
         const auto tuned = c->tuned.find(class_key(m->host, precision));
         for (size_t b = 0; b < m->host.beams.size(); ++b) {
             const HostBeam& hb = m->host.beams[b];
-            nt = std::max(nt, tuned != c->tuned.end() ? tuned->second : beam_threads(hb.N, hb.Q, hb.nc, rb));
+            nt = std::max(nt, tuned != c->tuned.end() ? tuned->second
+                                                      : beam_threads(hb.N, hb.Q, hb.nc, rb, m->host.hub >= 0));
             const double N = m->host.beams[b].N, Q = m->host.beams[b].Q;
             work = std::max(work, N * N * Q + 72. * (N - 1) * (N - 1) * (N - 1));
         }
         int smem = 0;
         for (const HostBeam& hb : m->host.beams)
-            smem = std::max(smem, beam_smem(hb.N, hb.Q, hb.nc, rb, nt));
+            smem = std::max(smem, beam_smem(hb.N, hb.Q, hb.nc, rb, nt, m->host.hub >= 0));
         entries.push_back({i, static_cast<int>(m->host.beams.size()), nt, ctas_per_sm(nt, smem), smem,
                            work});
     }
@@ -310,7 +313,10 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
             }
             for (int d = 0; d < 3; ++d) k.gravity[d] = m->host.gravity[d];
             k.conv = m->d_conv;
-            k.dump = (c->record && m->d_dump) ? m->d_dump + m->dump_off[b] : nullptr;
+            k.hub = m->host.hub >= 0 ? 1 : 0;
+            k.hub_con_type = m->host.hub_con_type;
+            // the system dump covers single-node constraints only
+            k.dump = (c->record && m->d_dump && !k.hub) ? m->d_dump + m->dump_off[b] : nullptr;
             k.prof = c->d_prof;
             kb.push_back(k);
             bk.count++;
@@ -442,6 +448,22 @@ int field_slot(int field, const SlabLayout& L, int* width) {
     }
 }
 
+// Offset of a node field inside a slab's hub region (-1: not kept for the hub;
+// the hub carries no external load, so its f reads as zero).
+int hub_field_offset(int field, int* w) {
+    switch (field) {
+        case KYN_FIELD_X0: *w = 7; return hubrec::x0;
+        case KYN_FIELD_X: *w = 7; return hubrec::x;
+        case KYN_FIELD_Q: *w = 7; return hubrec::q;
+        case KYN_FIELD_Q_PREV: *w = 7; return hubrec::q_prev;
+        case KYN_FIELD_Q_DELTA: *w = 6; return hubrec::q_delta;
+        case KYN_FIELD_V: *w = 6; return hubrec::v;
+        case KYN_FIELD_VD: *w = 6; return hubrec::vd;
+        case KYN_FIELD_A: *w = 6; return hubrec::a;
+        default: return -1;
+    }
+}
+
 // kind: KYN_LOAD_NODE_FX (0), KYN_LOAD_STATE_F (1), or 100 + node field.
 int get_xfer(kyn_ctx* c, const int* ids, int n, int kind, XferPlan** out) {
     const int slot = (kind == KYN_LOAD_NODE_FX) ? 0 : (kind == KYN_LOAD_STATE_F) ? 1
@@ -485,6 +507,20 @@ int get_xfer(kyn_ctx* c, const int* ids, int n, int kind, XferPlan** out) {
             xb.slab_field = m->d_slab[bi] + fo;
             beams.push_back(xb);
             elem += b.N;
+        }
+        if (m->host.hub >= 0 && kind >= 100) {  // the hub row, from beam 0's copy
+            int hw = 0;
+            const int ho = hub_field_offset(kind - 100, &hw);
+            if (ho < 0) return set_err(c, KYN_ERR_UNSUPPORTED, "field not kept for a hub node");
+            const HostBeam& b0 = m->host.beams[0];
+            const SlabLayout L0 = make_slab_layout(b0.N, b0.Q);
+            XferBeam xb{};
+            xb.N = 1;
+            xb.map_off = static_cast<int>(map.size());
+            xb.ext_off = off;
+            xb.slab_field = m->d_slab[0] + L0.hub + ho;
+            map.push_back(m->host.hub);
+            beams.push_back(xb);
         }
         off += (kind == KYN_LOAD_NODE_FX) ? elem * 6 : static_cast<long long>(m->host.num_nodes) * xp->width;
     }
@@ -564,6 +600,7 @@ void kyn_ctx_destroy(kyn_ctx* c) {
     if (c->pool_status) cudaFree(c->pool_status);
     if (c->pool_hstatus) cudaFreeHost(c->pool_hstatus);
     if (c->presc_targets) cudaFree(c->presc_targets);
+    if (c->presc_vidx) cudaFree(c->presc_vidx);
     if (c->h_stage) cudaFreeHost(c->h_stage);
     for (auto& x : c->xfer) x.reset();
     if (c->d_stage) cudaFree(c->d_stage);
@@ -650,9 +687,10 @@ int kyn_model_create(kyn_ctx* c, const kyn_model_desc* desc) {
     if (rc != KYN_OK) return set_err(c, rc, err);
     size_t bytes = kMaxNewtonIters * sizeof(double);
     for (auto& b : m->host.beams) {
-        const int nt = beam_threads(b.N, b.Q, b.nc, sizeof(double));
-        const int sm = std::max(beam_smem(b.N, b.Q, b.nc, sizeof(double), 512),
-                                beam_smem(b.N, b.Q, b.nc, sizeof(double), nt));
+        const int hubf = m->host.hub >= 0;
+        const int nt = beam_threads(b.N, b.Q, b.nc, sizeof(double), hubf);
+        const int sm = std::max(beam_smem(b.N, b.Q, b.nc, sizeof(double), 512, hubf),
+                                beam_smem(b.N, b.Q, b.nc, sizeof(double), nt, hubf));
         if (sm > kMaxDynSmem)
             return set_err(c, KYN_ERR_UNSUPPORTED, "beam system does not fit in shared memory");
         m->nt.push_back(nt);
@@ -773,6 +811,16 @@ int kyn_model_set_prescribed(kyn_ctx* c, int id, int cid, const double u[7]) {
     if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
     if (cid < 0 || cid >= m->host.num_constraints)
         return set_err(c, KYN_ERR_INVALID, "constraint id out of range");
+    if (cid == m->host.hub_con) {  // the hub BC: every beam keeps a copy
+        for (size_t bi = 0; bi < m->host.beams.size(); ++bi) {
+            const HostBeam& b = m->host.beams[bi];
+            const SlabLayout L = make_slab_layout(b.N, b.Q);
+            KYN_CUDA(c, cudaMemcpyAsync(m->d_slab[bi] + L.hub + hubrec::input, u, 7 * sizeof(double),
+                                        cudaMemcpyHostToDevice, c->stream));
+        }
+        KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+        return KYN_OK;
+    }
     const int bi = m->host.con_beam[cid], slot = m->host.con_slot[cid];
     const HostBeam& b = m->host.beams[bi];
     const SlabLayout L = make_slab_layout(b.N, b.Q);
@@ -854,6 +902,9 @@ int kyn_get_state(kyn_ctx* c, int id, int field, double* out) {
         if (field == KYN_FIELD_LAMBDA) {
             for (int s = 0; s < b.nc; ++s)
                 for (int k = 0; k < 6; ++k) out[b.con_row[s] * 6 + k] = h[L.lambda + s * 6 + k];
+            if (bi == 0 && m->host.hub >= 0)
+                for (int k = 0; k < 6; ++k)
+                    out[m->host.hub_con * 6 + k] = h[L.hub + hubrec::lambda + k];
             continue;
         }
         int src = -1, w = 0;
@@ -881,6 +932,23 @@ int kyn_get_state(kyn_ctx* c, int id, int field, double* out) {
                 for (int e = 0; e < w; ++e) o[e] = h[src + k * w + e];
             }
         }
+        if (bi == 0 && m->host.hub >= 0) {  // the hub node / the hub BC, from beam 0's copy
+            const double* H = h.data() + L.hub;
+            if (field == KYN_FIELD_LAMBDA) continue;
+            double* o = out + static_cast<size_t>(m->host.hub) * w;
+            int hw = 0;
+            const int ho = hub_field_offset(field, &hw);
+            if (field == KYN_FIELD_TANGENT) {
+                for (int e = 0; e < 36; ++e) o[e] = 0.;
+                for (int d = 0; d < 3; ++d) o[d * 7] = 1.;
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) o[(3 + i) * 6 + 3 + j] = H[hubrec::tangent + i * 3 + j];
+            } else if (ho >= 0) {
+                for (int e = 0; e < w; ++e) o[e] = H[ho + e];
+            } else {
+                for (int e = 0; e < w; ++e) o[e] = 0.;
+            }
+        }
     }
     return KYN_OK;
 }
@@ -905,6 +973,8 @@ int kyn_get_crs(kyn_ctx* c, int id, int* row_ptrs, int* col_inds, double* values
     if (row_ptrs) std::copy(H.row_ptrs.begin(), H.row_ptrs.end(), row_ptrs);
     if (col_inds) std::copy(H.col_inds.begin(), H.col_inds.end(), col_inds);
     if (!values) return KYN_OK;
+    if (m->host.hub >= 0)
+        return set_err(c, KYN_ERR_UNSUPPORTED, "system values are not recorded for models with a hub");
     if (!m->d_dump) return set_err(c, KYN_ERR_INVALID, "KYN_OPT_RECORD_SYSTEM was not set");
     KYN_CUDA(c, cudaStreamSynchronize(c->stream));
     std::fill(values, values + H.col_inds.size(), 0.);
@@ -939,6 +1009,8 @@ int kyn_get_system_vectors(kyn_ctx* c, int id, double* rhs, double* solution) {
     if (!c) return KYN_ERR_INVALID;
     DevModel* m = find_model(c, id);
     if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
+    if (m->host.hub >= 0)
+        return set_err(c, KYN_ERR_UNSUPPORTED, "system values are not recorded for models with a hub");
     if (!m->d_dump) return set_err(c, KYN_ERR_INVALID, "KYN_OPT_RECORD_SYSTEM was not set");
     KYN_CUDA(c, cudaStreamSynchronize(c->stream));
     const HostModel& H = m->host;
@@ -1013,10 +1085,12 @@ int kyn_get_state_batch(kyn_ctx* c, const int* ids, int n, int field, double* ou
 // ---- batched prescribed motion -------------------------------------------------
 namespace {
 
-__global__ void prescribed_kernel(double* const* __restrict__ targets, const double* __restrict__ vals,
-                                  int count) {
+// Target e (a constraint input slot, or one beam's copy of a hub BC input)
+// receives the 7 values of row vidx[e] of the caller's array.
+__global__ void prescribed_kernel(double* const* __restrict__ targets, const int* __restrict__ vidx,
+                                  const double* __restrict__ vals, int count) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < count * 7) targets[t / 7][t % 7] = vals[t];
+    if (t < count * 7) targets[t / 7][t % 7] = vals[vidx[t / 7] * 7 + t % 7];
 }
 
 }  // namespace
@@ -1028,40 +1102,60 @@ extern "C" int kyn_set_prescribed_batch(kyn_ctx* c, const int* ids, int n, const
     KYN_CUDA(c, cudaSetDevice(c->device));
     if (!(static_cast<int>(c->presc_ids.size()) == n && std::equal(ids, ids + n, c->presc_ids.begin()))) {
         std::vector<double*> t;
+        std::vector<int> vi;
+        int row = 0;
         for (int i = 0; i < n; ++i) {
             DevModel* m = find_model(c, ids[i]);
             if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id in batch");
-            for (int k = 0; k < m->host.num_constraints; ++k) {
+            for (int k = 0; k < m->host.num_constraints; ++k, ++row) {
+                if (k == m->host.hub_con) {
+                    for (size_t bi = 0; bi < m->host.beams.size(); ++bi) {
+                        const HostBeam& b = m->host.beams[bi];
+                        const SlabLayout L = make_slab_layout(b.N, b.Q);
+                        t.push_back(m->d_slab[bi] + L.hub + hubrec::input);
+                        vi.push_back(row);
+                    }
+                    continue;
+                }
                 const int bi = m->host.con_beam[k], slot = m->host.con_slot[k];
                 const HostBeam& b = m->host.beams[bi];
                 const SlabLayout L = make_slab_layout(b.N, b.Q);
                 t.push_back(m->d_slab[bi] + L.con_input + slot * 7);
+                vi.push_back(row);
             }
         }
         if (c->presc_cap < t.size()) {
             if (c->presc_targets) KYN_CUDA(c, cudaFree(c->presc_targets));
+            if (c->presc_vidx) KYN_CUDA(c, cudaFree(c->presc_vidx));
             c->presc_targets = nullptr;
+            c->presc_vidx = nullptr;
             const size_t cap = std::max<size_t>(t.size() + t.size() / 2, 64);
             KYN_CUDA(c, cudaMalloc(&c->presc_targets, sizeof(double*) * cap));
+            KYN_CUDA(c, cudaMalloc(&c->presc_vidx, sizeof(int) * cap));
             c->presc_cap = cap;
         }
-        if (!t.empty())
+        if (!t.empty()) {
             KYN_CUDA(c, cudaMemcpyAsync(c->presc_targets, t.data(), sizeof(double*) * t.size(),
                                         cudaMemcpyHostToDevice, c->stream));
+            KYN_CUDA(c, cudaMemcpyAsync(c->presc_vidx, vi.data(), sizeof(int) * vi.size(),
+                                        cudaMemcpyHostToDevice, c->stream));
+        }
         c->presc_count = static_cast<int>(t.size());
+        c->presc_rows = row;
         c->presc_ids.assign(ids, ids + n);
     }
     const int cnt = c->presc_count;
     if (cnt == 0) return KYN_OK;
     const double* src = values;
     if (!on_device) {
-        int rc = ensure_stage(c, static_cast<long long>(cnt) * 7);
+        int rc = ensure_stage(c, static_cast<long long>(c->presc_rows) * 7);
         if (rc != KYN_OK) return rc;
-        KYN_CUDA(c, cudaMemcpyAsync(c->d_stage, values, sizeof(double) * 7 * cnt,
+        KYN_CUDA(c, cudaMemcpyAsync(c->d_stage, values, sizeof(double) * 7 * c->presc_rows,
                                     cudaMemcpyHostToDevice, c->stream));
         src = c->d_stage;
     }
-    prescribed_kernel<<<(cnt * 7 + 255) / 256, 256, 0, c->stream>>>(c->presc_targets, src, cnt);
+    prescribed_kernel<<<(cnt * 7 + 255) / 256, 256, 0, c->stream>>>(c->presc_targets, c->presc_vidx,
+                                                                    src, cnt);
     KYN_CUDA(c, cudaGetLastError());
     c->launches++;
     return KYN_OK;
@@ -1109,6 +1203,11 @@ extern "C" int kyn_set_state(kyn_ctx* c, int id, int field, const double* values
             for (int e = 0; e < w; ++e) h[k * w + e] = values[static_cast<size_t>(b.node_ids[k]) * w + e];
         KYN_CUDA(c, cudaMemcpy(m->d_slab[bi] + off, h.data(), h.size() * sizeof(double),
                                cudaMemcpyHostToDevice));
+        int hw = 0;
+        const int ho = hub_field_offset(field, &hw);
+        if (m->host.hub >= 0 && ho >= 0)  // every beam's copy of the hub
+            KYN_CUDA(c, cudaMemcpy(m->d_slab[bi] + L.hub + ho, values + static_cast<size_t>(m->host.hub) * w,
+                                   w * sizeof(double), cudaMemcpyHostToDevice));
     }
     return KYN_OK;
 }
@@ -1167,7 +1266,7 @@ extern "C" int kyn_state_copy(kyn_ctx* c, int dst, int src) {
     DevModel* d = find_model(c, dst);
     DevModel* s = find_model(c, src);
     if (!d || !s) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
-    if (d->host.beams.size() != s->host.beams.size())
+    if (d->host.beams.size() != s->host.beams.size() || (d->host.hub >= 0) != (s->host.hub >= 0))
         return set_err(c, KYN_ERR_INVALID, "models differ in structure");
     for (size_t bi = 0; bi < d->host.beams.size(); ++bi) {
         const HostBeam& a = d->host.beams[bi];
@@ -1185,6 +1284,10 @@ extern "C" int kyn_state_copy(kyn_ctx* c, int dst, int src) {
         for (int k = 0; k < 9; ++k)
             KYN_CUDA(c, cudaMemcpyAsync(d->d_slab[bi] + fields[k], s->d_slab[bi] + fields[k],
                                         sizeof(double) * widths[k] * b.N, cudaMemcpyDeviceToDevice,
+                                        c->stream));
+        if (d->host.hub >= 0)  // the hub's state (its BC input stays the destination's)
+            KYN_CUDA(c, cudaMemcpyAsync(d->d_slab[bi] + L.hub, s->d_slab[bi] + L.hub,
+                                        sizeof(double) * hubrec::input, cudaMemcpyDeviceToDevice,
                                         c->stream));
     }
     return KYN_OK;
@@ -1255,7 +1358,7 @@ extern "C" int kyn_autotune(kyn_ctx* c, const int* ids, int n, const kyn_step_pa
         float best_ms = 0.f;
         for (int nt : {128, 256, 512}) {
             bool fits = true;
-            for (const HostBeam& b : h.beams) fits &= beam_smem(b.N, b.Q, b.nc, rb, nt) <= kMaxDynSmem;
+            for (const HostBeam& b : h.beams) fits &= beam_smem(b.N, b.Q, b.nc, rb, nt, h.hub >= 0) <= kMaxDynSmem;
             if (!fits || (key.beams > 1 && key.beams * nt > 1024 * 8)) continue;
             c->tuned[key] = nt;
             c->plan.reset();
@@ -1297,7 +1400,7 @@ extern "C" int kyn_tuned_threads(kyn_ctx* c, int model_id, int precision) {
     if (it != c->tuned.end()) return it->second;
     const int rb = (precision == KYN_PRECISION_FP32_REFINED) ? 4 : 8;
     int nt = 128;
-    for (const HostBeam& b : m->host.beams) nt = std::max(nt, beam_threads(b.N, b.Q, b.nc, rb));
+    for (const HostBeam& b : m->host.beams) nt = std::max(nt, beam_threads(b.N, b.Q, b.nc, rb, m->host.hub >= 0));
     return nt;
 }
 

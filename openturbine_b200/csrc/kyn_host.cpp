@@ -180,9 +180,18 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
             for (int c = 0; c < 3; ++c) S[L.tangent + k * 9 + c * 4] = 1.;
         }
     }
-    for (int n = 0; n < nn; ++n)
-        if (M.node_beam[n] < 0)
-            return fail(err, KYN_ERR_UNSUPPORTED, "node not attached to any beam element");
+    // A node outside every beam element is allowed only as the hub of a rotor:
+    // the base node of rigid joints, held by one single-node BC.
+    for (int n = 0; n < nn; ++n) {
+        if (M.node_beam[n] >= 0) continue;
+        bool is_hub = false;
+        for (int c = 0; c < d->num_constraints && d->constraint_type; ++c)
+            is_hub |= d->constraint_type[c] == KYN_CONSTRAINT_RIGID_JOINT && d->constraint_base_node &&
+                      d->constraint_base_node[c] == n;
+        if (!is_hub) return fail(err, KYN_ERR_UNSUPPORTED, "node not attached to any beam element");
+        if (M.hub >= 0) return fail(err, KYN_ERR_UNSUPPORTED, "more than one hub node in a model");
+        M.hub = n;
+    }
 
     // constraints (src/constraints/constraints.hpp:76-266)
     M.con_beam.assign(d->num_constraints, -1);
@@ -190,15 +199,38 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
     if (d->num_constraints > 0 && (!d->constraint_type || !d->constraint_target_node))
         return fail(err, KYN_ERR_INVALID, "constraints need type and target node");
     std::vector<int> node_con(nn, -1);
+    std::vector<std::vector<int>> node_cols(nn);   // constraint row blocks coupled to a node
+    static const double ident7[7] = {0., 0., 0., 1., 0., 0., 0.};
+    int joints = 0;
     for (int c = 0; c < d->num_constraints; ++c) {
         const int t = d->constraint_type[c];
-        if (t != KYN_CONSTRAINT_FIXED_BC && t != KYN_CONSTRAINT_PRESCRIBED_BC)
-            return fail(err, KYN_ERR_UNSUPPORTED, "only FixedBC and PrescribedBC constraints");
+        if (t != KYN_CONSTRAINT_FIXED_BC && t != KYN_CONSTRAINT_PRESCRIBED_BC &&
+            t != KYN_CONSTRAINT_RIGID_JOINT)
+            return fail(err, KYN_ERR_UNSUPPORTED,
+                        "only FixedBC, PrescribedBC and RigidJoint constraints");
         const int node = d->constraint_target_node[c];
         if (node < 0 || node >= nn) return fail(err, KYN_ERR_INVALID, "constraint node out of range");
+        if (t == KYN_CONSTRAINT_RIGID_JOINT) {
+            const int base = d->constraint_base_node ? d->constraint_base_node[c] : -1;
+            if (base < 0 || base >= nn) return fail(err, KYN_ERR_INVALID, "joint base node out of range");
+            if (base != M.hub || M.node_beam[node] < 0)
+                return fail(err, KYN_ERR_UNSUPPORTED,
+                            "rigid joints must join a hub node (in no beam) to a beam node");
+            node_cols[base].push_back(c);
+            ++joints;
+        }
+        if (node == M.hub) {  // the hub's own boundary condition
+            if (t == KYN_CONSTRAINT_RIGID_JOINT || M.hub_con >= 0)
+                return fail(err, KYN_ERR_UNSUPPORTED, "the hub needs exactly one FixedBC or PrescribedBC");
+            M.hub_con = c;
+            M.hub_con_type = t;
+            node_cols[node].push_back(c);
+            continue;
+        }
         if (node_con[node] >= 0)
             return fail(err, KYN_ERR_UNSUPPORTED, "two constraints on one node");
         node_con[node] = c;
+        node_cols[node].push_back(c);
         const int e = M.node_beam[node];
         HostBeam& B = M.beams[e];
         if (B.nc >= kMaxBeamConstraints)
@@ -216,12 +248,52 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
             for (int k = 0; k < 3; ++k)
                 B.con_X0[slot][k] = x0[k] - (d->constraint_axis ? d->constraint_axis[c * 3 + k] : 0.);
             for (int k = 0; k < 7; ++k) B.slab[L.con_input + slot * 7 + k] = ident[k];
+        } else if (t == KYN_CONSTRAINT_RIGID_JOINT) {
+            // X0 = target x0 - base x0 (src/constraints/constraints.hpp:268-290)
+            const double* x0 = d->node_x0 + node * 7;
+            const double* xb = d->node_x0 + M.hub * 7;
+            for (int k = 0; k < 3; ++k) B.con_X0[slot][k] = x0[k] - xb[k];
+            for (int k = 0; k < 7; ++k) B.slab[L.con_input + slot * 7 + k] = ident[k];
         } else {
             for (int k = 0; k < 3; ++k) B.con_X0[slot][k] = 0.;
             const double* u = d->constraint_initial_displacement
                                   ? d->constraint_initial_displacement + c * 7
                                   : ident;
             for (int k = 0; k < 7; ++k) B.slab[L.con_input + slot * 7 + k] = u[k];
+        }
+    }
+
+    if (M.hub >= 0 && (M.hub_con < 0 || joints == 0))
+        return fail(err, KYN_ERR_UNSUPPORTED, "a hub node needs one BC and at least one rigid joint");
+    if (M.hub >= 0) {
+        // every beam carries a copy of the hub's state
+        const int h = M.hub;
+        const double* x0 = d->node_x0 + h * 7;
+        const double* u = d->node_u ? d->node_u + h * 7 : ident7;
+        const int c = M.hub_con;
+        for (auto& B : M.beams) {
+            const SlabLayout L = make_slab_layout(B.N, B.Q);
+            double* H = B.slab.data() + L.hub;
+            for (int k = 0; k < 7; ++k) {
+                H[hubrec::x0 + k] = x0[k];
+                H[hubrec::q + k] = u[k];
+                H[hubrec::q_prev + k] = u[k];
+            }
+            for (int k = 0; k < 3; ++k) H[hubrec::x + k] = x0[k] + u[k];
+            qmul(u + 3, x0 + 3, H + hubrec::x + 3);
+            for (int k = 0; k < 6; ++k) {
+                H[hubrec::v + k] = d->node_v ? d->node_v[h * 6 + k] : 0.;
+                H[hubrec::vd + k] = d->node_vd ? d->node_vd[h * 6 + k] : 0.;
+                H[hubrec::a + k] = H[hubrec::vd + k];
+            }
+            for (int k = 0; k < 3; ++k) H[hubrec::tangent + k * 4] = 1.;
+            const double* in = (M.hub_con_type == KYN_CONSTRAINT_PRESCRIBED_BC &&
+                                d->constraint_initial_displacement)
+                                   ? d->constraint_initial_displacement + c * 7 : ident7;
+            for (int k = 0; k < 7; ++k) H[hubrec::input + k] = in[k];
+            for (int k = 0; k < 3; ++k)
+                H[hubrec::X0 + k] = (M.hub_con_type == KYN_CONSTRAINT_FIXED_BC)
+                    ? x0[k] - (d->constraint_axis ? d->constraint_axis[c * 3 + k] : 0.) : 0.;
         }
     }
 
@@ -241,15 +313,23 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
         cols.clear();
         if (row < M.nsys) {
             const int node = row / 6;
-            const HostBeam& B = M.beams[M.node_beam[node]];
-            for (int k = 0; k < B.N; ++k)
-                for (int c = 0; c < 6; ++c) cols.push_back(M.fmap[B.node_ids[k]] + c);
-            if (node_con[node] >= 0)
-                for (int c = 0; c < 6; ++c) cols.push_back(M.nsys + 6 * node_con[node] + c);
+            if (M.node_beam[node] >= 0) {
+                const HostBeam& B = M.beams[M.node_beam[node]];
+                for (int k = 0; k < B.N; ++k)
+                    for (int c = 0; c < 6; ++c) cols.push_back(M.fmap[B.node_ids[k]] + c);
+            } else {
+                // a node in no element still holds its own diagonal block
+                // (compute_system_row_entries.hpp starts every row with it)
+                for (int c = 0; c < 6; ++c) cols.push_back(M.fmap[node] + c);
+            }
+            for (int con : node_cols[node])
+                for (int c = 0; c < 6; ++c) cols.push_back(M.nsys + 6 * con + c);
         } else {
             const int con = (row - M.nsys) / 6;
             const int node = d->constraint_target_node[con];
             for (int c = 0; c < 6; ++c) cols.push_back(M.fmap[node] + c);
+            if (d->constraint_type[con] == KYN_CONSTRAINT_RIGID_JOINT)
+                for (int c = 0; c < 6; ++c) cols.push_back(M.fmap[d->constraint_base_node[con]] + c);
         }
         std::sort(cols.begin(), cols.end());
         M.col_inds.insert(M.col_inds.end(), cols.begin(), cols.end());

@@ -36,6 +36,9 @@ struct HostModel {
     int nsys = 0, ndofs = 0;
     std::vector<int> row_ptrs, col_inds;      // reference CRS graph (sorted rows)
     double gravity[3] = {0., 0., 0.};
+    int hub = -1;                             // hub node (in no beam) or -1
+    int hub_con = -1;                         // the single-node BC holding the hub
+    int hub_con_type = 0;
 };
 
 // Validates the description and builds the host model.  Returns KYN_OK or a

@@ -115,6 +115,7 @@ __device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double
 constexpr int kGroupScratch = 256;      // doubles of per-group scratch for QP math
 constexpr int kPanel = 8;               // LU panel width
 constexpr int kConStride = 96;          // doubles per constraint record in smem
+constexpr int kHubSmem = 200;           // doubles of the hub record (hubsm)
 
 // Per-group scratch (doubles) of the quadrature phase.
 namespace grec {
@@ -151,7 +152,8 @@ struct Smem {
     int rpiv;           // double [n6]  reciprocal pivots
     int stage;          // double [64]  U12 tile staged by warp 0 during the LU
     int con;            // double [nc][kConStride]
-    int red;            // double [2][NT/32 + 8]
+    int red;            // double [2][NT/32 + 8]  (offset 0: cluster exchange)
+    int hub;            // double [kHubSmem] hub state and records, or -1
     int pos;            // int [N]
     int bytes;
     int ldA;
@@ -160,7 +162,7 @@ struct Smem {
 // The system matrix and the quadrature scratch never live at the same time:
 // A is assembled after the quadrature phase and consumed by the solve, so the
 // two share one region.
-__host__ __device__ inline Smem make_smem(int N, int Q, int nc, int real_bytes, int nt) {
+__host__ __device__ inline Smem make_smem(int N, int Q, int nc, int real_bytes, int nt, int hub = 0) {
     Smem S{};
     int o = 0;
     auto take = [&](int bytes) {
@@ -170,6 +172,10 @@ __host__ __device__ inline Smem make_smem(int N, int Q, int nc, int real_bytes, 
     };
     const int n6 = 6 * N;
     S.ldA = n6 + 1;
+    // The cluster exchange areas come first, so that every CTA of a model's
+    // cluster finds them at the same offset whatever its beam's size.
+    S.red = take(2 * (nt / 32 + 8) * 8);
+    S.hub = hub ? take(kHubSmem * 8) : -1;
     {
         const int a_bytes = n6 * S.ldA * real_bytes;
         const int g_bytes = (nt / 16) * kGroupScratch * 8;
@@ -197,7 +203,6 @@ __host__ __device__ inline Smem make_smem(int N, int Q, int nc, int real_bytes, 
     S.rpiv = take(n6 * 8);
     S.stage = take(64 * 8);
     S.con = take((nc > 0 ? nc : 1) * kConStride * 8);
-    S.red = take(2 * (nt / 32 + 8) * 8);
     S.pos = take(N * 4);
     S.bytes = o;
     return S;
@@ -234,7 +239,21 @@ constexpr int xl = 30;     // [6] multiplier correction
 constexpr int lam = 36;    // [6] lambda
 constexpr int inp = 42;    // [7] prescribed input
 constexpr int yr = 49;     // [6] constrained-row residual b_r - A_r x
+constexpr int R1X0 = 55;   // [3] rigid joint: R(hub) X0
+constexpr int Btr = 58;    // [9] rigid joint: base block tilde(R1 X0) T_hub
+constexpr int Brr = 67;    // [9] rigid joint: base block -AX(C) T_hub
 }  // namespace conrec
+
+// Shared-memory record of a model's hub (doubles): the hub state in the slab
+// layout (hubrec), the hub BC's constraint record, the hub correction, the
+// hub multiplier correction, and the per-beam contributions exchanged over
+// the cluster (double-buffered by iteration parity).
+namespace hubsm {
+constexpr int bc = 80;     // [kConStride] constraint record of the hub BC
+constexpr int xh = 176;    // [6] hub correction
+constexpr int xlh = 182;   // [6] hub multiplier correction (unconditioned)
+constexpr int pub = 188;   // [2][6] sum over this beam's joints of G_base^T (lambda + x_lambda)
+}  // namespace hubsm
 
 // TF32 tensor-core product D += A B for one 16x8x8 tile (mma.sync m16n8k8).
 // Fragment layout per lane l (g = l/4, t = l%4): a = {A[g][t], A[g+8][t],
@@ -543,6 +562,85 @@ __device__ __forceinline__ void back_substitute_blocked(const TR* A, int ldA, in
     }
 }
 
+// Residual, gradient blocks and G^T lambda of one constraint on node q `nu`
+// (calculate_constraint_residual_gradient.hpp:60-320 with
+// calculate_{fixed,prescribed}_bc_constraint.hpp and
+// calculate_rigid_joint_constraint.hpp:17-113).  FixedBC: R1 = I, u1 = 0;
+// PrescribedBC: (u1, R1) = the record's input; RigidJoint: (u1, R1) = the hub
+// node's q `hq`, X0 = target x0 - hub x0, and the base-node blocks
+// tilde(R1 X0) T_hub and -AX(C) T_hub are kept for the hub elimination.
+__device__ inline void constraint_record(double* cr, int type, const double* nu, const double* X0,
+                                         const double* Rt, const double* hq, const double* RtHub) {
+    double u1[3] = {0., 0., 0.}, R1[4] = {1., 0., 0., 0.};
+    if (type == KYN_CONSTRAINT_PRESCRIBED_BC) {
+        for (int k = 0; k < 3; ++k) u1[k] = cr[conrec::inp + k];
+        for (int k = 0; k < 4; ++k) R1[k] = cr[conrec::inp + 3 + k];
+    } else if (type == KYN_CONSTRAINT_RIGID_JOINT) {
+        for (int k = 0; k < 3; ++k) u1[k] = hq[k];
+        for (int k = 0; k < 4; ++k) R1[k] = hq[3 + k];
+    }
+    const double len = sqrt(R1[0] * R1[0] + R1[1] * R1[1] + R1[2] * R1[2] + R1[3] * R1[3]);
+    const double R1t[4] = {R1[0] / len, -R1[1] / len, -R1[2] / len, -R1[3] / len};
+    double R1X0[3];
+    for (int i = 0; i < 3; ++i) {
+        R1X0[i] = 0.;
+        for (int j = 0; j < 3; ++j) R1X0[i] += rot_entry(R1, i, j) * X0[j];
+    }
+    for (int i = 0; i < 3; ++i) cr[conrec::Phi + i] = nu[i] + X0[i] - u1[i] - R1X0[i];
+    double R2R1t[4];
+    quat_compose(nu + 3, R1t, R2R1t);
+    double C[9];
+    for (int e = 0; e < 9; ++e) C[e] = rot_entry(R2R1t, e / 3, e % 3);
+    cr[conrec::Phi + 3] = (C[7] - C[5]) / 2.;
+    cr[conrec::Phi + 4] = (C[2] - C[6]) / 2.;
+    cr[conrec::Phi + 5] = (C[3] - C[1]) / 2.;
+    // AX(C) = tr(C)/2 I - C/2 ; grad rotational block = AX^T ; grad^T block = AX
+    const double tr = (C[0] + C[4] + C[8]) / 2.;
+    double AXm[9];
+    for (int e = 0; e < 9; ++e) AXm[e] = -C[e] / 2. + ((e % 4 == 0) ? tr : 0.);
+    for (int e = 0; e < 9; ++e) cr[conrec::AX + e] = AXm[e];
+    // B rotational block = AX^T * Rt  (Rt = stored tangent block of the node)
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double acc = 0.;
+            for (int k = 0; k < 3; ++k) acc += AXm[k * 3 + i] * Rt[k * 3 + j];
+            cr[conrec::Brot + i * 3 + j] = acc;
+        }
+    // grad^T lambda
+    for (int i = 0; i < 3; ++i) cr[conrec::Gl + i] = cr[conrec::lam + i];
+    for (int i = 0; i < 3; ++i) {
+        double acc = 0.;
+        for (int k = 0; k < 3; ++k) acc += AXm[i * 3 + k] * cr[conrec::lam + 3 + k];
+        cr[conrec::Gl + 3 + i] = acc;
+    }
+    if (type == KYN_CONSTRAINT_RIGID_JOINT) {
+        for (int i = 0; i < 3; ++i) cr[conrec::R1X0 + i] = R1X0[i];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                double bt = 0., br = 0.;
+                for (int k = 0; k < 3; ++k) {
+                    bt += tilde_e(R1X0, i, k) * RtHub[k * 3 + j];
+                    br -= AXm[i * 3 + k] * RtHub[k * 3 + j];
+                }
+                cr[conrec::Btr + i * 3 + j] = bt;
+                cr[conrec::Brr + i * 3 + j] = br;
+            }
+    }
+}
+
+// G_base^T w of a rigid joint (base gradient [-I, tilde(R1 X0); 0, -AX]):
+// [-w_t; tilde(R1 X0)^T w_t - AX^T w_r], accumulated into out.
+__device__ inline void joint_base_transpose_add(const double* cr, const double* w, double* out) {
+    const double* r = cr + conrec::R1X0;
+    const double* AX = cr + conrec::AX;
+    for (int i = 0; i < 3; ++i) out[i] -= w[i];
+    for (int i = 0; i < 3; ++i) {
+        double acc = 0.;
+        for (int k = 0; k < 3; ++k) acc += tilde_e(r, k, i) * w[k] - AX[k * 3 + i] * w[3 + k];
+        out[3 + i] += acc;
+    }
+}
+
 // ---- the kernel ------------------------------------------------------------------
 template <typename TR, int NT>
 __global__ void __launch_bounds__(NT, (NT == 128) ? 4 : (NT == 256) ? 2 : 1)
@@ -557,7 +655,8 @@ __global__ void __launch_bounds__(NT, (NT == 128) ? 4 : (NT == 256) ? 2 : 1)
     const int n6 = 6 * N;
     const int m = 6 * (N - nc);   // free-node block size
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const Smem S = make_smem(N, Q, nc, sizeof(TR), NT);
+    const bool hub = KB.hub != 0;
+    const Smem S = make_smem(N, Q, nc, sizeof(TR), NT, hub ? 1 : 0);
     const SlabLayout L = make_slab_layout(N, Q);
     double* __restrict__ slab = KB.slab;
 
@@ -578,6 +677,7 @@ __global__ void __launch_bounds__(NT, (NT == 128) ? 4 : (NT == 256) ? 2 : 1)
     double* sa = reinterpret_cast<double*>(smem_raw + S.a);
     double* sqd = reinterpret_cast<double*>(smem_raw + S.qd);
     double* sT = reinterpret_cast<double*>(smem_raw + S.T);
+    double* hb = hub ? reinterpret_cast<double*>(smem_raw + S.hub) : nullptr;  // hub record
     double* resid = reinterpret_cast<double*>(smem_raw + S.resid);
     double* bp = reinterpret_cast<double*>(smem_raw + S.b);
     double* xs = reinterpret_cast<double*>(smem_raw + S.xs);
@@ -626,6 +726,14 @@ __global__ void __launch_bounds__(NT, (NT == 128) ? 4 : (NT == 256) ? 2 : 1)
         for (int k = 0; k < 7; ++k) c[conrec::inp + k] = slab[L.con_input + tid * 7 + k];
         for (int k = 0; k < 6; ++k) c[conrec::lam + k] = 0.;  // ResetConstraints
     }
+    if (hub) {
+        for (int k = tid; k < kHubDoubles; k += NT) hb[k] = slab[L.hub + k];
+        if (tid == 0) {
+            double* br = hb + hubsm::bc;
+            for (int k = 0; k < 7; ++k) br[conrec::inp + k] = slab[L.hub + hubrec::input + k];
+            for (int k = 0; k < 6; ++k) br[conrec::lam + k] = 0.;  // ResetConstraints
+        }
+    }
     if (tid == 0) {
         // Free nodes first, constrained nodes last (in constraint order).
         int p = 0;
@@ -652,6 +760,17 @@ __global__ void __launch_bounds__(NT, (NT == 128) ? 4 : (NT == 256) ? 2 : 1)
         sv[k] = v_p + h * (1. - P.gamma) * a_p + P.gamma * h * an;
         sqd[k] = v_p + (0.5 - P.beta) * h * a_p + P.beta * h * an;
     }
+    if (hub && tid == NT - 1) {  // the hub node: same predictor
+        for (int k = 0; k < 7; ++k) hb[hubrec::q_prev + k] = hb[hubrec::q + k];
+        for (int k = 0; k < 6; ++k) {
+            const double v_p = hb[hubrec::v + k], vd_p = hb[hubrec::vd + k], a_p = hb[hubrec::a + k];
+            hb[hubrec::vd + k] = 0.;
+            const double an = (P.alpha_f * vd_p - P.alpha_m * a_p) / (1. - P.alpha_m);
+            hb[hubrec::a + k] = an;
+            hb[hubrec::v + k] = v_p + h * (1. - P.gamma) * a_p + P.gamma * h * an;
+            hb[hubrec::q_delta + k] = v_p + (0.5 - P.beta) * h * a_p + P.beta * h * an;
+        }
+    }
     __syncthreads();
     // CalculateDisplacement (src/state/calculate_displacement.hpp:25-50)
     auto displacement = [&]() {
@@ -662,6 +781,17 @@ __global__ void __launch_bounds__(NT, (NT == 128) ? 4 : (NT == 256) ? 2 : 1)
             rotvec_to_quat(d, qd4);
             quat_compose(qd4, sqp + n * 7 + 3, qn);
             for (int c = 0; c < 4; ++c) sq[n * 7 + 3 + c] = qn[c];
+        }
+        if (hub && tid == NT - 1) {
+            double* hq = hb + hubrec::q;
+            const double* hqp = hb + hubrec::q_prev;
+            const double* hqd = hb + hubrec::q_delta;
+            for (int c = 0; c < 3; ++c) hq[c] = hqp[c] + h * hqd[c];
+            const double d[3] = {h * hqd[3], h * hqd[4], h * hqd[5]};
+            double qd4[4], qn[4];
+            rotvec_to_quat(d, qd4);
+            quat_compose(qd4, hqp + 3, qn);
+            for (int c = 0; c < 4; ++c) hq[3 + c] = qn[c];
         }
     };
     displacement();
@@ -677,8 +807,8 @@ __global__ void __launch_bounds__(NT, (NT == 128) ? 4 : (NT == 256) ? 2 : 1)
     for (int iter = 0; iter < P.max_iter + extra; ++iter) {
         // ---- tangent operator (src/system/calculate_tangent_operator.hpp:26-65)
         // Only the rotational 3x3 block of the stored (transposed) operator is kept.
-        for (int n = tid; n < N; n += NT) {
-            const double rv[3] = {h * sqd[n * 6 + 3], h * sqd[n * 6 + 4], h * sqd[n * 6 + 5]};
+        auto tangent_op = [&](const double* qd, double* T) {
+            const double rv[3] = {h * qd[3], h * qd[4], h * qd[5]};
             const double ph = sqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
             double sn, cs;
             sincos(ph, &sn, &cs);
@@ -689,10 +819,12 @@ __global__ void __launch_bounds__(NT, (NT == 128) ? 4 : (NT == 256) ? 2 : 1)
                     // m1 = t2*(rv~ rv~) + t1*rv~ ; T_rot = I + m1 ; stored transposed
                     double rr = 0.;
                     for (int k = 0; k < 3; ++k) rr += tilde_e(rv, j, k) * tilde_e(rv, k, i);
-                    sT[n * 9 + i * 3 + j] = (i == j ? 1. : 0.) + (t1 * tilde_e(rv, j, i) + t2 * rr);
+                    T[i * 3 + j] = (i == j ? 1. : 0.) + (t1 * tilde_e(rv, j, i) + t2 * rr);
                 }
             }
-        }
+        };
+        for (int n = tid; n < N; n += NT) tangent_op(sqd + n * 6, sT + n * 9);
+        if (hub && tid == NT - 1) tangent_op(hb + hubrec::q_delta, hb + hubrec::tangent);
 
         // ---- quadrature-point values (calculate_quadrature_point_values.hpp) ---
         // 16 threads per quadrature point; a CTA covers NT/16 points per pass.  Each
@@ -1043,53 +1175,16 @@ __global__ void __launch_bounds__(NT, (NT == 128) ? 4 : (NT == 256) ? 2 : 1)
         __syncthreads();
         mark(kPhaseIntegrate);
 
-        // ---- constraints (calculate_constraint_residual_gradient.hpp:60-199) -------
+        // ---- constraints (calculate_constraint_residual_gradient.hpp:60-320) -------
         if (warp == NW - 1 && lane < nc) {
-            double* cr = con + lane * kConStride;
             const int tn = KB.con_node[lane];
-            const double* nu = sq + tn * 7;
-            double u1[3] = {0., 0., 0.}, R1[4] = {1., 0., 0., 0.};
-            if (KB.con_type[lane] == KYN_CONSTRAINT_PRESCRIBED_BC) {
-                for (int k = 0; k < 3; ++k) u1[k] = cr[conrec::inp + k];
-                for (int k = 0; k < 4; ++k) R1[k] = cr[conrec::inp + 3 + k];
-            }
-            const double* X0 = KB.con_X0[lane];
-            const double len = sqrt(R1[0] * R1[0] + R1[1] * R1[1] + R1[2] * R1[2] + R1[3] * R1[3]);
-            const double R1t[4] = {R1[0] / len, -R1[1] / len, -R1[2] / len, -R1[3] / len};
-            double R1X0[3];
-            for (int i = 0; i < 3; ++i) {
-                R1X0[i] = 0.;
-                for (int j = 0; j < 3; ++j) R1X0[i] += rot_entry(R1, i, j) * X0[j];
-            }
-            for (int i = 0; i < 3; ++i) cr[conrec::Phi + i] = nu[i] + X0[i] - u1[i] - R1X0[i];
-            double R2R1t[4];
-            quat_compose(nu + 3, R1t, R2R1t);
-            double C[9];
-            for (int e = 0; e < 9; ++e) C[e] = rot_entry(R2R1t, e / 3, e % 3);
-            cr[conrec::Phi + 3] = (C[7] - C[5]) / 2.;
-            cr[conrec::Phi + 4] = (C[2] - C[6]) / 2.;
-            cr[conrec::Phi + 5] = (C[3] - C[1]) / 2.;
-            // AX(C) = tr(C)/2 I - C/2 ; grad rotational block = AX^T ; grad^T block = AX
-            const double tr = (C[0] + C[4] + C[8]) / 2.;
-            double AXm[9];
-            for (int e = 0; e < 9; ++e) AXm[e] = -C[e] / 2. + ((e % 4 == 0) ? tr : 0.);
-            for (int e = 0; e < 9; ++e) cr[conrec::AX + e] = AXm[e];
-            // B rotational block = AX^T * Rt  (Rt = stored tangent block of the node)
-            const double* Rt = sT + tn * 9;
-            for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j) {
-                    double acc = 0.;
-                    for (int k = 0; k < 3; ++k) acc += AXm[k * 3 + i] * Rt[k * 3 + j];
-                    cr[conrec::Brot + i * 3 + j] = acc;
-                }
-            // grad^T lambda
-            for (int i = 0; i < 3; ++i) cr[conrec::Gl + i] = cr[conrec::lam + i];
-            for (int i = 0; i < 3; ++i) {
-                double acc = 0.;
-                for (int k = 0; k < 3; ++k) acc += AXm[i * 3 + k] * cr[conrec::lam + 3 + k];
-                cr[conrec::Gl + 3 + i] = acc;
-            }
+            constraint_record(con + lane * kConStride, KB.con_type[lane], sq + tn * 7, KB.con_X0[lane],
+                              sT + tn * 9, hub ? hb + hubrec::q : nullptr,
+                              hub ? hb + hubrec::tangent : nullptr);
         }
+        if (hub && warp == NW - 1 && lane == nc)  // the hub's own boundary condition
+            constraint_record(hb + hubsm::bc, KB.hub_con_type, hb + hubrec::q, hb + hubrec::X0,
+                              hb + hubrec::tangent, nullptr, nullptr);
         __syncthreads();
 
         // ---- right-hand side: b = -cond (-f + R + G^T lambda) (assemble_system_residual.hpp,
@@ -1138,14 +1233,42 @@ __global__ void __launch_bounds__(NT, (NT == 128) ? 4 : (NT == 256) ? 2 : 1)
         mark(kPhaseConstraints);
 
         // ---- solve -----------------------------------------------------------------
-        // (S1) constrained node corrections: B x_r = -Phi
+        // (S1) constrained node corrections: B x_r = -Phi.  With a hub, its
+        //      correction comes first (its BC rows), then each rigid joint gives
+        //      the root correction: B_t x_root = -Phi - B_base x_hub.
+        if (hub) {
+            if (tid == 0) {
+                const double* br = hb + hubsm::bc;
+                double* xh = hb + hubsm::xh;
+                for (int k = 0; k < 3; ++k) xh[k] = -br[conrec::Phi + k];
+                const double rhs[3] = {-br[conrec::Phi + 3], -br[conrec::Phi + 4], -br[conrec::Phi + 5]};
+                double y[3] = {0., 0., 0.};
+                if (!solve3(br + conrec::Brot, rhs, y)) atomicOr(&s_flag, 2);
+                for (int k = 0; k < 3; ++k) xh[3 + k] = y[k];
+            }
+            __syncthreads();
+        }
         if (tid < nc) {
             const double* cr = con + tid * kConStride;
             const int pr = 6 * pos[KB.con_node[tid]];
-            for (int k = 0; k < 3; ++k) xs[pr + k] = -cr[conrec::Phi + k];
-            const double rhs[3] = {-cr[conrec::Phi + 3], -cr[conrec::Phi + 4], -cr[conrec::Phi + 5]};
+            double rt[3], rr[3];
+            for (int k = 0; k < 3; ++k) {
+                rt[k] = -cr[conrec::Phi + k];
+                rr[k] = -cr[conrec::Phi + 3 + k];
+            }
+            if (KB.con_type[tid] == KYN_CONSTRAINT_RIGID_JOINT) {
+                const double* xh = hb + hubsm::xh;
+                for (int i = 0; i < 3; ++i) {
+                    rt[i] += xh[i];
+                    for (int k = 0; k < 3; ++k) {
+                        rt[i] -= cr[conrec::Btr + i * 3 + k] * xh[3 + k];
+                        rr[i] -= cr[conrec::Brr + i * 3 + k] * xh[3 + k];
+                    }
+                }
+            }
+            for (int k = 0; k < 3; ++k) xs[pr + k] = rt[k];
             double y[3] = {0., 0., 0.};
-            if (!solve3(cr + conrec::Brot, rhs, y)) atomicOr(&s_flag, 2);
+            if (!solve3(cr + conrec::Brot, rr, y)) atomicOr(&s_flag, 2);
             for (int k = 0; k < 3; ++k) xs[pr + 3 + k] = y[k];
         }
         __syncthreads();
@@ -1233,6 +1356,19 @@ __global__ void __launch_bounds__(NT, (NT == 128) ? 4 : (NT == 256) ? 2 : 1)
             for (int k = 0; k < 3; ++k) cr[conrec::xl + 3 + k] = yr[k] / P.conditioner;
         }
         __syncthreads();
+        if (hub && tid == 0) {
+            // this beam's part of the hub rows: sum over its joints of
+            // G_base^T (lambda + x_lambda), exchanged over the cluster below
+            double* pub = hb + hubsm::pub + 6 * (iter & 1);
+            for (int k = 0; k < 6; ++k) pub[k] = 0.;
+            for (int c = 0; c < nc; ++c) {
+                if (KB.con_type[c] != KYN_CONSTRAINT_RIGID_JOINT) continue;
+                const double* cr = con + c * kConStride;
+                double w[6];
+                for (int k = 0; k < 6; ++k) w[k] = cr[conrec::lam + k] + cr[conrec::xl + k];
+                joint_base_transpose_add(cr, w, pub);
+            }
+        }
         if (record && KB.dump) {
             const int nl = n6 + 6 * nc;
             double* D = KB.dump + nl * nl + nl;
@@ -1284,6 +1420,30 @@ __global__ void __launch_bounds__(NT, (NT == 128) ? 4 : (NT == 256) ? 2 : 1)
             total = slot[NW];
             flags = slot[NW + 1];
         }
+        double xlh[6] = {0., 0., 0., 0., 0., 0.};
+        if (hub) {
+            // Hub rows have no element terms: G_hub^T x_lh = -G_hub^T lambda_hub -
+            // sum_j G_base,j^T (lambda_j + x_lj), summed over the beams in rank order.
+            double sum[6] = {0., 0., 0., 0., 0., 0.};
+            for (int r = 0; r < KB.model_beams; ++r) {
+                const double* peer = clustered ? cluster.map_shared_rank(hb + hubsm::pub + 6 * (iter & 1), r)
+                                               : hb + hubsm::pub + 6 * (iter & 1);
+                for (int k = 0; k < 6; ++k) sum[k] += peer[k];
+            }
+            const double* br = hb + hubsm::bc;
+            for (int k = 0; k < 3; ++k) xlh[k] = -br[conrec::lam + k] - sum[k];
+            double yr[3] = {0., 0., 0.};
+            if (!solve3(br + conrec::AX, sum + 3, yr)) flags = 1.;
+            for (int k = 0; k < 3; ++k) xlh[3 + k] = -br[conrec::lam + 3 + k] - yr[k];
+            // the hub's own terms of the error sum (every CTA adds the same values)
+            const double* xh = hb + hubsm::xh;
+            const double* hqd = hb + hubrec::q_delta;
+            for (int k = 0; k < 6; ++k) {
+                const double e1 = xh[k] / (P.atol + P.rtol * fabs(hqd[k] * h));
+                const double e2 = xlh[k] / (P.atol + P.rtol * fabs(br[conrec::lam + k]));
+                total += e1 * e1 + e2 * e2;
+            }
+        }
         const double err = sqrt(total / static_cast<double>(KB.model_dofs));
         if (KB.rank == 0 && tid == 0 && iter < kMaxNewtonIters) KB.conv[iter] = err;
         iters = iter + 1;
@@ -1301,6 +1461,17 @@ __global__ void __launch_bounds__(NT, (NT == 128) ? 4 : (NT == 256) ? 2 : 1)
         if (tid < 6 * nc) {
             double* cr = con + (tid / 6) * kConStride;
             cr[conrec::lam + tid % 6] += cr[conrec::xl + tid % 6];
+        }
+        if (hub && tid == NT - 1) {
+            const double* xh = hb + hubsm::xh;
+            for (int k = 0; k < 6; ++k) {
+                hb[hubrec::q_delta + k] += xh[k] / h;
+                if (P.dynamic) {
+                    hb[hubrec::v + k] += P.gamma_prime * xh[k];
+                    hb[hubrec::vd + k] += P.beta_prime * xh[k];
+                }
+                hb[hubsm::bc + conrec::lam + k] += xlh[k];
+            }
         }
         __syncthreads();
         displacement();
@@ -1330,7 +1501,20 @@ __global__ void __launch_bounds__(NT, (NT == 128) ? 4 : (NT == 256) ? 2 : 1)
         const double fac = (1. - P.alpha_f) / (1. - P.alpha_m);
         for (int t = tid; t < n6; t += NT) sa[t] += fac * svd[t];
     }
+    if (hub && tid == NT - 1) {
+        if (status == KYN_OK) {
+            const double fac = (1. - P.alpha_f) / (1. - P.alpha_m);
+            for (int k = 0; k < 6; ++k) hb[hubrec::a + k] += fac * hb[hubrec::vd + k];
+            const double* x0 = hb + hubrec::x0;
+            for (int c = 0; c < 3; ++c) hb[hubrec::x + c] = x0[c] + hb[hubrec::q + c];
+            quat_compose(hb + hubrec::q + 3, x0 + 3, hb + hubrec::x + 3);
+        }
+        for (int k = 0; k < 6; ++k) hb[hubrec::lambda + k] = hb[hubsm::bc + conrec::lam + k];
+    }
     __syncthreads();
+    if (hub)  // every beam keeps its copy of the hub state (the input is the caller's)
+        for (int k = tid; k < kHubDoubles; k += NT)
+            if (k < hubrec::input || k >= hubrec::input + 7) slab[L.hub + k] = hb[k];
     for (int k = tid; k < N * 7; k += NT) {
         slab[L.q + k] = sq[k];
         slab[L.q_prev + k] = sqp[k];

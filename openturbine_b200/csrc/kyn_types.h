@@ -17,7 +17,7 @@
 
 namespace kyn {
 
-constexpr int kMaxBeamConstraints = 4;   // FixedBC / PrescribedBC per beam
+constexpr int kMaxBeamConstraints = 4;   // FixedBC / PrescribedBC / RigidJoint per beam
 constexpr int kMaxClusterBeams = 8;      // beams per model (portable cluster size)
 constexpr int kMaxNewtonIters = 64;      // convergence-history capacity
 constexpr int kThreads = 256;            // threads per CTA of the step kernel
@@ -37,8 +37,29 @@ struct SlabLayout {
     int32_t tangent;            // [N][9]  rotational block of the stored tangent
     int32_t con_input;          // [kMaxBeamConstraints][7]
     int32_t lambda;             // [kMaxBeamConstraints][6]
+    int32_t hub;                // [kHubDoubles] hub node of a jointed model (see hubrec)
     int32_t total;
 };
+
+// Hub node of a model whose beam roots are rigidly jointed to it: a node in
+// no beam element, held by one FixedBC / PrescribedBC.  Every beam of the
+// model keeps an identical copy of the hub's state in its slab; every CTA of
+// the model's cluster updates its copy with the same arithmetic.
+namespace hubrec {
+constexpr int x0 = 0;       // [7]
+constexpr int q = 7;        // [7]
+constexpr int q_prev = 14;  // [7]
+constexpr int x = 21;       // [7]
+constexpr int v = 28;       // [6]
+constexpr int vd = 34;      // [6]
+constexpr int a = 40;       // [6]
+constexpr int q_delta = 46; // [6]
+constexpr int tangent = 52; // [9] rotational block of the stored tangent
+constexpr int input = 61;   // [7] hub BC input (PrescribedBC displacement)
+constexpr int lambda = 68;  // [6] hub BC multipliers
+constexpr int X0 = 74;      // [3] hub BC X0 (FixedBC)
+}  // namespace hubrec
+constexpr int kHubDoubles = 78;
 
 KYN_HD inline SlabLayout make_slab_layout(int N, int Q) {
     SlabLayout L{};
@@ -69,6 +90,7 @@ KYN_HD inline SlabLayout make_slab_layout(int N, int Q) {
     L.tangent = take(N * 9);
     L.con_input = take(kMaxBeamConstraints * 7);
     L.lambda = take(kMaxBeamConstraints * 6);
+    L.hub = take(kHubDoubles);
     L.total = o;
     return L;
 }
@@ -84,7 +106,9 @@ struct KBeam {
     int32_t con_node[kMaxBeamConstraints];   // beam-local target node
     int32_t con_type[kMaxBeamConstraints];   // KYN_CONSTRAINT_*
     int32_t con_row[kMaxBeamConstraints];    // constraint index within the model
-    double con_X0[kMaxBeamConstraints][3];
+    double con_X0[kMaxBeamConstraints][3];   // RigidJoint: target x0 - hub x0
+    int32_t hub;              // 1: the model has a hub (rigid joints in con_type)
+    int32_t hub_con_type;     // KYN_CONSTRAINT_FIXED_BC / PRESCRIBED_BC on the hub
     double gravity[3];
     double* conv;             // [kMaxNewtonIters] model convergence history (rank 0)
     double* dump;             // optional: last assembled system (see kyn_capi.cu)
