@@ -271,6 +271,11 @@ public:
         cons_.push_back({KYN_CONSTRAINT_PRESCRIBED_BC, node, u0});
         return cons_.size() - 1;
     }
+    // {base (hub), target} (src/model/model.hpp AddRigidJointConstraint)
+    size_t AddRigidJointConstraint(const std::array<size_t, 2>& nodes) {
+        cons_.push_back({KYN_CONSTRAINT_RIGID_JOINT, nodes[1], {0., 0., 0., 1., 0., 0., 0.}, nodes[0]});
+        return cons_.size() - 1;
+    }
 
     std::tuple<State, Elements, Constraints, Solver> CreateSystemWithSolver(const Context& ctx) const {
         std::vector<double> x0, u, v, vd, s, spos, smass, sstiff, qxi, qw, cinit;
@@ -303,7 +308,7 @@ public:
         }
         for (const auto& c : cons_) {
             ctype.push_back(c.type);
-            cbase.push_back(0);
+            cbase.push_back(static_cast<int32_t>(c.base));
             ctarget.push_back(static_cast<int32_t>(c.node));
             cinit.insert(cinit.end(), c.u0.begin(), c.u0.end());
         }
@@ -339,6 +344,7 @@ private:
         int type;
         size_t node;
         std::array<double, 7> u0;
+        size_t base = 0;
     };
     std::array<double, 3> gravity_{0., 0., 0.};
     std::vector<Node> nodes_;
