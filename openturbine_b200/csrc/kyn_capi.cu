@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <unordered_map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -34,6 +35,13 @@ struct DevModel {
     HostModel host;
     std::vector<double*> d_slab;     // per beam
     std::vector<int> nt;             // per beam: threads per CTA of the step kernel
+    // Per-model values every plan needs, computed once (plans are rebuilt
+    // whenever the model set changes, every iteration of a serving loop).
+    std::vector<SlabLayout> lay;     // per beam slab layout
+    std::vector<KBeam> kt;           // per beam launch record (plan fields filled per plan)
+    int def_nt[2] = {0, 0};          // default threads per CTA, FP64 / FP32 form
+    int smem_nt[2][3] = {};          // dynamic smem for 128 / 256 / 512 threads, per form
+    double work = 0.;                // largest beam's N^2 Q + 72 (N-1)^3 (ordering in buckets)
     double* d_conv = nullptr;        // [kMaxNewtonIters]
     double* d_dump = nullptr;        // per-beam system dumps (recording mode)
     std::vector<size_t> dump_off;    // per beam offset into d_dump (doubles)
@@ -126,7 +134,7 @@ struct kyn_ctx {
     cudaStream_t bstream[kBucketStreams] = {};
     cudaEvent_t fork = nullptr;
     cudaEvent_t join[kBucketStreams] = {};
-    std::map<int, std::unique_ptr<DevModel>> models;
+    std::unordered_map<int, std::unique_ptr<DevModel>> models;
     int next_id = 0;
     std::string err;
     bool record = false;
@@ -137,6 +145,8 @@ struct kyn_ctx {
     double* h_stage = nullptr;            // pinned staging for loads
     size_t h_stage_len = 0;
     std::unique_ptr<XferPlan> xfer[4];    // cached transfer plans
+    std::vector<XferBeam> xfer_beams_tmp; // host build buffers of transfer plans (reused)
+    std::vector<int> xfer_map_tmp;
     double* d_stage = nullptr;            // device staging for batched transfers
     size_t d_stage_len = 0;
     int64_t launches = 0;                 // kernels launched so far
@@ -148,6 +158,10 @@ struct kyn_ctx {
     // serving loop does it every iteration) allocates nothing in steady state.
     KBeam* pool_kbeams = nullptr;
     size_t pool_kbeams_cap = 0;
+    KBeam* pool_hkbeams = nullptr;        // pinned staging of the plan's KBeam records
+    size_t pool_hkbeams_cap = 0;
+    cudaEvent_t plan_uploaded = nullptr;  // the staging buffer's last upload
+    bool plan_upload_pending = false;
     int* pool_status = nullptr;           // device [2][cap]: status, iterations
     int* pool_hstatus = nullptr;          // pinned [2][cap]
     size_t pool_status_cap = 0;
@@ -230,6 +244,52 @@ ClassKey class_key(const HostModel& h, int precision) {
     return k;
 }
 
+// Fills the per-model values that plans and transfer plans reuse.
+void prepare_model(DevModel* m) {
+    const HostModel& H = m->host;
+    const int hubf = H.hub >= 0;
+    m->lay.clear();
+    m->kt.clear();
+    m->work = 0.;
+    for (int f = 0; f < 2; ++f) {
+        const int rb = f ? 4 : 8;
+        m->def_nt[f] = 128;
+        for (int k = 0; k < 3; ++k) m->smem_nt[f][k] = 0;
+        for (const HostBeam& hb : H.beams) {
+            m->def_nt[f] = std::max(m->def_nt[f], beam_threads(hb.N, hb.Q, hb.nc, rb, hubf));
+            for (int k = 0; k < 3; ++k)
+                m->smem_nt[f][k] = std::max(m->smem_nt[f][k], beam_smem(hb.N, hb.Q, hb.nc, rb, 128 << k, hubf));
+        }
+    }
+    for (size_t b = 0; b < H.beams.size(); ++b) {
+        const HostBeam& hb = H.beams[b];
+        m->lay.push_back(make_slab_layout(hb.N, hb.Q));
+        const double N = hb.N, Q = hb.Q;
+        m->work = std::max(m->work, N * N * Q + 72. * (N - 1) * (N - 1) * (N - 1));
+        KBeam k{};
+        k.slab = m->d_slab[b];
+        k.N = hb.N;
+        k.Q = hb.Q;
+        k.nc = hb.nc;
+        k.rank = static_cast<int>(b);
+        k.model_beams = static_cast<int>(H.beams.size());
+        k.model_dofs = H.ndofs;
+        for (int s2 = 0; s2 < kMaxBeamConstraints; ++s2) {
+            k.con_node[s2] = hb.con_node[s2];
+            k.con_type[s2] = hb.con_type[s2];
+            k.con_row[s2] = hb.con_row[s2];
+            for (int d = 0; d < 3; ++d) k.con_X0[s2][d] = hb.con_X0[s2][d];
+        }
+        for (int d = 0; d < 3; ++d) k.gravity[d] = H.gravity[d];
+        k.conv = m->d_conv;
+        k.hub = hubf;
+        k.hub_con_type = H.hub_con_type;
+        m->kt.push_back(k);
+    }
+}
+
+int nt_index(int nt) { return nt == 128 ? 0 : nt == 256 ? 1 : 2; }
+
 // Builds (or reuses) the launch plan for this id list.
 int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
     if (c->plan && c->plan->record == c->record && c->plan->precision == precision &&
@@ -242,8 +302,8 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
     plan->ids.assign(ids, ids + n);
     plan->record = c->record;
     plan->precision = precision;
-    const int rb = (precision == KYN_PRECISION_FP32_REFINED) ? 4 : 8;
-    // bucket key: (cluster size, CTAs per SM class); larger work first
+    const int f = (precision == KYN_PRECISION_FP32_REFINED) ? 1 : 0;
+    // bucket key: (cluster size, threads, CTAs per SM class); larger work first
     struct Entry {
         int model_index;
         int cluster;
@@ -251,34 +311,45 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
         int cls;
         int smem;
         double work;
+        DevModel* m;
     };
     std::vector<Entry> entries;
+    entries.reserve(n);
+    size_t nbeams = 0;
     for (int i = 0; i < n; ++i) {
         DevModel* m = find_model(c, ids[i]);
         if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id in step list");
-        int nt = 128;
-        double work = 0.;
-        const auto tuned = c->tuned.find(class_key(m->host, precision));
-        for (size_t b = 0; b < m->host.beams.size(); ++b) {
-            const HostBeam& hb = m->host.beams[b];
-            nt = std::max(nt, tuned != c->tuned.end() ? tuned->second
-                                                      : beam_threads(hb.N, hb.Q, hb.nc, rb, m->host.hub >= 0));
-            const double N = m->host.beams[b].N, Q = m->host.beams[b].Q;
-            work = std::max(work, N * N * Q + 72. * (N - 1) * (N - 1) * (N - 1));
+        int nt = m->def_nt[f];
+        if (!c->tuned.empty()) {
+            const auto tuned = c->tuned.find(class_key(m->host, precision));
+            if (tuned != c->tuned.end()) nt = tuned->second;
         }
-        int smem = 0;
-        for (const HostBeam& hb : m->host.beams)
-            smem = std::max(smem, beam_smem(hb.N, hb.Q, hb.nc, rb, nt, m->host.hub >= 0));
-        entries.push_back({i, static_cast<int>(m->host.beams.size()), nt, ctas_per_sm(nt, smem), smem,
-                           work});
+        const int smem = m->smem_nt[f][nt_index(nt)];
+        entries.push_back({i, static_cast<int>(m->kt.size()), nt, ctas_per_sm(nt, smem), smem, m->work, m});
+        nbeams += m->kt.size();
     }
-    std::stable_sort(entries.begin(), entries.end(), [](const Entry& a, const Entry& b) {
+    std::sort(entries.begin(), entries.end(), [](const Entry& a, const Entry& b) {
         if (a.cluster != b.cluster) return a.cluster > b.cluster;
         if (a.nt != b.nt) return a.nt > b.nt;
         if (a.cls != b.cls) return a.cls < b.cls;
-        return a.work > b.work;
+        if (a.work != b.work) return a.work > b.work;
+        return a.model_index < b.model_index;
     });
-    std::vector<KBeam> kb;
+    // KBeam records go through a pinned staging buffer (one DMA); wait for the
+    // previous plan's upload before refilling it
+    if (c->plan_upload_pending) {
+        KYN_CUDA(c, cudaEventSynchronize(c->plan_uploaded));
+        c->plan_upload_pending = false;
+    }
+    if (c->pool_hkbeams_cap < nbeams) {
+        if (c->pool_hkbeams) KYN_CUDA(c, cudaFreeHost(c->pool_hkbeams));
+        c->pool_hkbeams = nullptr;
+        const size_t cap = std::max<size_t>(nbeams + nbeams / 2, 256);
+        KYN_CUDA(c, cudaMallocHost(&c->pool_hkbeams, sizeof(KBeam) * cap));
+        c->pool_hkbeams_cap = cap;
+    }
+    KBeam* kb = c->pool_hkbeams;
+    size_t nk = 0;
     for (size_t e = 0; e < entries.size(); ++e) {
         const Entry& en = entries[e];
         if (plan->buckets.empty() || plan->buckets.back().cluster != en.cluster ||
@@ -287,46 +358,27 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
             Bucket bk;
             bk.cluster = en.cluster;
             bk.nt = en.nt;
-            bk.first = static_cast<int>(kb.size());
+            bk.first = static_cast<int>(nk);
             plan->buckets.push_back(bk);
         }
         Bucket& bk = plan->buckets.back();
         bk.smem = std::max(bk.smem, en.smem);
-        DevModel* m = find_model(c, ids[en.model_index]);
-        int model_dofs = m->host.ndofs;
-        for (size_t b = 0; b < m->host.beams.size(); ++b) {
-            const HostBeam& hb = m->host.beams[b];
-            KBeam k{};
-            k.slab = m->d_slab[b];
-            k.N = hb.N;
-            k.Q = hb.Q;
-            k.nc = hb.nc;
+        DevModel* m = en.m;
+        for (size_t b = 0; b < m->kt.size(); ++b) {
+            KBeam k = m->kt[b];
             k.plan_model = en.model_index;
-            k.rank = static_cast<int>(b);
-            k.model_beams = static_cast<int>(m->host.beams.size());
-            k.model_dofs = model_dofs;
-            for (int s = 0; s < kMaxBeamConstraints; ++s) {
-                k.con_node[s] = hb.con_node[s];
-                k.con_type[s] = hb.con_type[s];
-                k.con_row[s] = hb.con_row[s];
-                for (int d = 0; d < 3; ++d) k.con_X0[s][d] = hb.con_X0[s][d];
-            }
-            for (int d = 0; d < 3; ++d) k.gravity[d] = m->host.gravity[d];
-            k.conv = m->d_conv;
-            k.hub = m->host.hub >= 0 ? 1 : 0;
-            k.hub_con_type = m->host.hub_con_type;
             // the system dump covers single-node constraints only
             k.dump = (c->record && m->d_dump && !k.hub) ? m->d_dump + m->dump_off[b] : nullptr;
             k.prof = c->d_prof;
-            kb.push_back(k);
+            kb[nk++] = k;
             bk.count++;
         }
     }
-    plan->nbeams = static_cast<int>(kb.size());
-    if (c->pool_kbeams_cap < kb.size()) {
+    plan->nbeams = static_cast<int>(nk);
+    if (c->pool_kbeams_cap < nk) {
         if (c->pool_kbeams) KYN_CUDA(c, cudaFree(c->pool_kbeams));
         c->pool_kbeams = nullptr;
-        const size_t cap = std::max<size_t>(kb.size() + kb.size() / 2, 256);
+        const size_t cap = std::max<size_t>(nk + nk / 2, 256);
         KYN_CUDA(c, cudaMalloc(&c->pool_kbeams, sizeof(KBeam) * cap));
         c->pool_kbeams_cap = cap;
     }
@@ -345,9 +397,10 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
     plan->d_iters = c->pool_status + c->pool_status_cap;
     plan->h_status = c->pool_hstatus;
     plan->h_iters = c->pool_hstatus + c->pool_status_cap;
-    // pageable source: the copy is staged before this call returns
-    KYN_CUDA(c, cudaMemcpyAsync(plan->d_kbeams, kb.data(), sizeof(KBeam) * kb.size(),
-                                cudaMemcpyHostToDevice, c->stream));
+    KYN_CUDA(c, cudaMemcpyAsync(plan->d_kbeams, kb, sizeof(KBeam) * nk, cudaMemcpyHostToDevice,
+                                c->stream));
+    KYN_CUDA(c, cudaEventRecord(c->plan_uploaded, c->stream));
+    c->plan_upload_pending = true;
     c->plan = std::move(plan);
     *out = c->plan.get();
     return KYN_OK;
@@ -479,8 +532,10 @@ int get_xfer(kyn_ctx* c, const int* ids, int n, int kind, XferPlan** out) {
     xp->ids.assign(ids, ids + n);
     xp->width = 0;
     xp->kind = kind;
-    std::vector<XferBeam> beams;
-    std::vector<int> map;
+    std::vector<XferBeam>& beams = c->xfer_beams_tmp;
+    std::vector<int>& map = c->xfer_map_tmp;
+    beams.clear();
+    map.clear();
     long long off = 0;
     for (int i = 0; i < n; ++i) {
         DevModel* m = find_model(c, ids[i]);
@@ -488,7 +543,7 @@ int get_xfer(kyn_ctx* c, const int* ids, int n, int kind, XferPlan** out) {
         long long elem = 0;
         for (size_t bi = 0; bi < m->host.beams.size(); ++bi) {
             const HostBeam& b = m->host.beams[bi];
-            const SlabLayout L = make_slab_layout(b.N, b.Q);
+            const SlabLayout& L = m->lay[bi];
             XferBeam xb{};
             xb.N = b.N;
             xb.map_off = static_cast<int>(map.size());
@@ -578,6 +633,15 @@ kyn_ctx* kyn_ctx_create(int device, size_t hbm_budget_bytes) {
              cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming) == cudaSuccess;
     }
     ok = ok && cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) == cudaSuccess;
+    ok = ok && cudaEventCreateWithFlags(&c->plan_uploaded, cudaEventDisableTiming) == cudaSuccess;
+    // Slabs come from the device's stream-ordered pool; keep freed blocks in
+    // the pool instead of returning them at each synchronisation, so that
+    // models created and destroyed every serving iteration reuse memory.
+    cudaMemPool_t pool = nullptr;
+    if (ok && cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     if (!ok) {
         kyn_ctx_destroy(c);
         return nullptr;
@@ -597,6 +661,8 @@ void kyn_ctx_destroy(kyn_ctx* c) {
     }
     c->models.clear();
     if (c->pool_kbeams) cudaFree(c->pool_kbeams);
+    if (c->pool_hkbeams) cudaFreeHost(c->pool_hkbeams);
+    if (c->plan_uploaded) cudaEventDestroy(c->plan_uploaded);
     if (c->pool_status) cudaFree(c->pool_status);
     if (c->pool_hstatus) cudaFreeHost(c->pool_hstatus);
     if (c->presc_targets) cudaFree(c->presc_targets);
@@ -722,6 +788,7 @@ int kyn_model_create(kyn_ctx* c, const kyn_model_desc* desc) {
     // in flight is not waited for.
     m->bytes = bytes;
     c->used += bytes;
+    prepare_model(m.get());
     const int id = c->next_id++;
     c->models[id] = std::move(m);
     return id;
@@ -1317,6 +1384,7 @@ int clone_model(kyn_ctx* c, int id) {
     KYN_CUDA(c, cudaMallocAsync(&m->d_conv, kMaxNewtonIters * sizeof(double), c->stream));
     m->bytes = bytes;
     c->used += bytes;
+    prepare_model(m.get());
     const int nid = c->next_id++;
     c->models[nid] = std::move(m);
     return nid;

@@ -77,6 +77,9 @@ class StepServer:
         self.beam_steps_converged = 0
         self.beam_steps_total = 0
         self.max_active_seen = 0
+        # host time per iteration part (ms, summed): loads and motion in, step
+        # submission, admission while the step runs, wait for results, retire
+        self.host_ms = {"inputs": 0.0, "submit": 0.0, "admit": 0.0, "wait": 0.0, "retire": 0.0}
         self._pinned = None
         self._ids = np.zeros(0, dtype=np.int32)
         self._rotor = np.zeros(0, dtype=bool)
@@ -171,10 +174,16 @@ class StepServer:
         self.ctx.set_loads_batch(ids, LOAD_NODE_FX, fx.ctypes.data, False)
         if presc is not None:
             self.ctx.set_prescribed_batch(rot_ids, presc.ctypes.data, False)
+        t1 = time.perf_counter()
         self.ctx.step_async(ids, self.params)
+        t2 = time.perf_counter()
         self._admit(now_fn())               # overlaps the step on the GPU (appends after n)
+        t3 = time.perf_counter()
         st, it = self.ctx.step_wait()
-        self.step_ms.append((time.perf_counter() - t0) * 1e3)
+        t4 = time.perf_counter()
+        self.step_ms.append((t4 - t0) * 1e3)
+        for k, dt in (("inputs", t1 - t0), ("submit", t2 - t1), ("admit", t3 - t2), ("wait", t4 - t3)):
+            self.host_ms[k] += dt * 1e3
         self.step_models.append(n)
         self.max_active_seen = max(self.max_active_seen, n)
         conv = st == 0
@@ -186,6 +195,7 @@ class StepServer:
         self._done[:n] += 1
         leave = np.flatnonzero(self._done[:n] >= self._steps[:n])
         if leave.size:
+            t5 = time.perf_counter()
             now = now_fn()
             for i in leave:
                 r = self.active[i]
@@ -195,6 +205,7 @@ class StepServer:
                 r.finished_at = now
                 self.finished.append(r)
             self._remove(leave)
+            self.host_ms["retire"] += (time.perf_counter() - t5) * 1e3
 
     def run(self, until_s: float, drain: bool = False) -> None:
         """Serve in real time for until_s seconds (requests become visible at
@@ -226,6 +237,7 @@ class StepServer:
                 "step_latency_ms": {"p50": float(np.percentile(ms, 50)),
                                     "p99": float(np.percentile(ms, 99))},
                 "max_active": self.max_active_seen,
+                "host_ms_total": {k: round(v, 1) for k, v in self.host_ms.items()},
                 "active_end": len(self.active), "queued_end": len(self.queue),
                 "finished": len(self.finished)}
 
