@@ -187,6 +187,8 @@ def main() -> None:
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32 + refinement form")
     ap.add_argument("--no-graph", action="store_true", help="launch steps directly (no CUDA graph)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="default threads per CTA instead of the autotuned choice per size class")
     ap.add_argument("--serve", type=float, default=5.0,
                     help="seconds of the serving workload per form (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="request arrivals per second")
@@ -249,6 +251,17 @@ def main() -> None:
             ctx.set_loads_batch(ids, LOAD_NODE_FX, loads_host[k].data_ptr(), False)
         return ctx.step(ids, params)
 
+    def tune(step_ids, step_params) -> dict:
+        """Autotune threads per CTA per size class (timed on clones, before the
+        timed region); returns the choice per node count."""
+        if args.no_autotune:
+            return {}
+        ctx.autotune(step_ids, step_params)
+        out = {}
+        for i, d in enumerate(draws):
+            out.setdefault(int(d.num_nodes), ctx.tuned_threads(int(step_ids[i]), step_params.precision))
+        return dict(sorted(out.items()))
+
     def device_leg(step_ids, step_params, clocks_on: bool):
         """W warm-up steps, then K device-timed steps (device-resident loads, L2
         flushed before each step).  Returns per-step ms, converged counts,
@@ -299,6 +312,7 @@ def main() -> None:
                 "ok_all": ok_all}
 
     # ---- value: plain FP64 form, device-resident inputs, device time per step --
+    tuned64 = tune(ids, params)
     r64 = device_leg(ids, params, True)
     dev_ms, conv_v, flops_v, launches = r64["ms"], r64["conv"], r64["flops"], r64["launches"]
     t_value_ms = S.max_over_ranks(float(sum(dev_ms)), dist, dev)
@@ -312,6 +326,7 @@ def main() -> None:
                          dtype=np.int32)
         p32 = W.batch_params()
         p32.precision, p32.refine_iters = 1, args.refine
+        tuned32 = tune(ids32, p32)
         r32 = device_leg(ids32, p32, False)
         t32 = S.max_over_ranks(float(sum(r32["ms"])), dist, dev)
         v32 = S.sum_over_ranks(r32["conv"], dist, dev) / (t32 * 1e-3)
@@ -322,6 +337,7 @@ def main() -> None:
         prec = {"form": "FP32 tangent/LU (3xTF32 integration GEMM) + FP64 residual, update "
                         f"and {args.refine} refinement correction(s)",
                 "value": v32, "unit": "beam-steps/s", "ratio_vs_fp64": v32 / value,
+                "threads_per_cta_by_nodes": tuned32,
                 "ms_per_step": t32 / args.steps,
                 "newton_iters_per_beam_step": r32["iters"] / (args.steps * len(ids32)),
                 "fp64_newton_iters_per_beam_step": r64["iters"] / (args.steps * len(ids)),
@@ -363,6 +379,11 @@ def main() -> None:
             sctx = Context(local, 150 * 10**9)
             sp = W.batch_params()
             sp.precision = form
+            if not args.no_autotune:   # size classes of the request pool, tuned before serving
+                pids = np.array([sctx.create_model(pm) for pm, *_ in pool_b + pool_r], dtype=np.int32)
+                sctx.autotune(pids, sp)
+                for i in pids:
+                    sctx.destroy_model(int(i))
             srv = StepServer(sctx, sp)
             for r in poisson_requests(args.serve_rate, args.serve, pool_b, pool_r):
                 srv.submit(r)
@@ -388,6 +409,7 @@ def main() -> None:
                        "max_iter": params.max_iter, "a_tol": 1e-7, "r_tol": 1e-3,
                        "precision": "plain FP64", "l2": "flushed (256 MB write) before each step",
                        "launch": "direct" if args.no_graph else "CUDA graph replay per step",
+                       "threads_per_cta_by_nodes": tuned64,
                        "parallelism": f"independent beam shards x{world}"},
             "latency_ms": {"p50": float(np.percentile(dev_ms, 50)),
                            "p99": float(np.percentile(dev_ms, 99)),

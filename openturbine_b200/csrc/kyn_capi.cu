@@ -221,14 +221,20 @@ int beam_threads(int N, int Q, int nc, int real_bytes, int hub = 0) {
     return (2 * (s256 + 1024) <= kSmemPerSM) ? 256 : 512;
 }
 
+// Registers per thread of an instance: the budget its launch bounds give,
+// rounded down to the allocation granule of 8.
+int step_regs(int real_bytes, int nt) {
+    const int r = 65536 / (nt * step_min_blocks(real_bytes, nt));
+    return std::min(255, r & ~7);
+}
+
 int beam_smem(int N, int Q, int nc, int real_bytes, int nt, int hub = 0) {
     return make_smem(N, Q, nc, real_bytes, nt, hub).bytes;
 }
 
-// Resident CTAs per SM for a thread count and shared-memory size; the step
-// kernel's register budget (128 per thread) allows 65536 / (128 nt) CTAs.
-int ctas_per_sm(int nt, int smem) {
-    const int by_regs = 65536 / (128 * nt);
+// Resident CTAs per SM for an instance and shared-memory size.
+int ctas_per_sm(int real_bytes, int nt, int smem) {
+    const int by_regs = 65536 / (step_regs(real_bytes, nt) * nt);
     const int per = smem + 1024;
     return std::max(1, std::min(by_regs, kSmemPerSM / per));
 }
@@ -303,6 +309,7 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
     plan->record = c->record;
     plan->precision = precision;
     const int f = (precision == KYN_PRECISION_FP32_REFINED) ? 1 : 0;
+    const int rbytes = f ? 4 : 8;
     // bucket key: (cluster size, threads, CTAs per SM class); larger work first
     struct Entry {
         int model_index;
@@ -325,7 +332,7 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
             if (tuned != c->tuned.end()) nt = tuned->second;
         }
         const int smem = m->smem_nt[f][nt_index(nt)];
-        entries.push_back({i, static_cast<int>(m->kt.size()), nt, ctas_per_sm(nt, smem), smem, m->work, m});
+        entries.push_back({i, static_cast<int>(m->kt.size()), nt, ctas_per_sm(rbytes, nt, smem), smem, m->work, m});
         nbeams += m->kt.size();
     }
     std::sort(entries.begin(), entries.end(), [](const Entry& a, const Entry& b) {
@@ -354,7 +361,7 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
         const Entry& en = entries[e];
         if (plan->buckets.empty() || plan->buckets.back().cluster != en.cluster ||
             plan->buckets.back().nt != en.nt ||
-            ctas_per_sm(en.nt, plan->buckets.back().smem) != en.cls) {
+            ctas_per_sm(rbytes, en.nt, plan->buckets.back().smem) != en.cls) {
             Bucket bk;
             bk.cluster = en.cluster;
             bk.nt = en.nt;

@@ -642,8 +642,17 @@ __device__ inline void joint_base_transpose_add(const double* cr, const double* 
 }
 
 // ---- the kernel ------------------------------------------------------------------
+// Resident CTAs per SM that each instance is compiled for (its register budget
+// is 65536 / (NT * this), 128 registers per thread for all three).  Three
+// 256-thread CTAs per SM in the FP32 form (80 registers) would fit its shared
+// memory up to 16 nodes, but the spills land in the pivot loops and cost more
+// than the third beam per SM hides.
+__host__ __device__ constexpr int step_min_blocks(int real_bytes, int nt) {
+    return (void)real_bytes, nt == 128 ? 4 : nt == 256 ? 2 : 1;
+}
+
 template <typename TR, int NT>
-__global__ void __launch_bounds__(NT, (NT == 128) ? 4 : (NT == 256) ? 2 : 1)
+__global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
     step_kernel(const KBeam* __restrict__ beams, StepCoeffs P, int record,
                 int* __restrict__ status_out, int* __restrict__ iters_out) {
     static_assert(NT == 128 || NT == 256 || NT == 512, "step kernel runs with 128, 256 or 512 threads");
