@@ -56,12 +56,21 @@ enum {
 
 /* Constraint types: same numbering as constraints::ConstraintType
  * (src/constraints/constraint_type.hpp:9-24).  This path implements the two
- * single-node boundary conditions used by beams and rotors. */
+ * single-node boundary conditions used by beams and rotors and the two
+ * six-row joints that tie blade roots to a hub node. */
 enum {
     KYN_CONSTRAINT_FIXED_BC = 1,
     KYN_CONSTRAINT_PRESCRIBED_BC = 2,
-    KYN_CONSTRAINT_RIGID_JOINT = 3   /* base node (hub) to target node, six DOFs
+    KYN_CONSTRAINT_RIGID_JOINT = 3,  /* base node (hub) to target node, six DOFs
                                         (src/constraints/calculate_rigid_joint_constraint.hpp) */
+    KYN_CONSTRAINT_ROTATION_CONTROL = 5  /* a rigid joint whose target is turned by a
+                                        commanded angle about constraint_axis (normalised
+                                        here as in src/constraints/constraints.hpp:321-328);
+                                        the angle is u[0] of kyn_model_set_prescribed, the
+                                        slot Constraints::UpdateViews fills from the control
+                                        pointer (src/constraints/constraints.hpp:345-352;
+                                        src/constraints/calculate_rotation_control_constraint.hpp:17-144,
+                                        src/model/model.hpp:550-562) */
 };
 
 /* Node-state fields readable with kyn_get_state (src/state/state.hpp:18-68,
@@ -185,7 +194,9 @@ KYN_API int kyn_model_info_get(kyn_ctx* ctx, int model_id, kyn_model_info* info)
  * test_cantilever_beam.cpp:105-107) or State::f. */
 KYN_API int kyn_model_set_loads(kyn_ctx* ctx, int model_id, int which, const double* values);
 
-/* Replaces Constraints::UpdateDisplacement (src/constraints/constraints.hpp:338-343). */
+/* Replaces Constraints::UpdateDisplacement (src/constraints/constraints.hpp:338-343).
+ * For a KYN_CONSTRAINT_ROTATION_CONTROL constraint u[0] is the commanded angle
+ * (rad) and u[1..6] are ignored. */
 KYN_API int kyn_model_set_prescribed(kyn_ctx* ctx, int model_id, int constraint_id, const double u[7]);
 
 /* Replaces kynema::Step (src/step/step.hpp:42-124) for a batch of models:

@@ -20,6 +20,7 @@
 #include <stdexcept>
 #include <string>
 #include <tuple>
+#include <utility>
 #include <vector>
 
 #include "kynema_b200.h"
@@ -167,6 +168,7 @@ struct DeviceModel {
     std::vector<size_t> elem_offset;
     bool fx_dirty = false;
     std::vector<double> errs;
+    std::vector<std::pair<int, double*>> controls;  // RotationControl: constraint, signal
     ~DeviceModel() {
         if (id >= 0) kyn_model_destroy(ctx.get(), id);
     }
@@ -277,8 +279,17 @@ public:
         return cons_.size() - 1;
     }
 
+    // {base (hub), target}, rotation axis and the control signal read before
+    // every Step (src/model/model.hpp:550-562 AddRotationControl)
+    size_t AddRotationControl(const std::array<size_t, 2>& nodes, const std::array<double, 3>& axis,
+                              double* control) {
+        cons_.push_back({KYN_CONSTRAINT_ROTATION_CONTROL, nodes[1], {0., 0., 0., 1., 0., 0., 0.},
+                         nodes[0], axis, control});
+        return cons_.size() - 1;
+    }
+
     std::tuple<State, Elements, Constraints, Solver> CreateSystemWithSolver(const Context& ctx) const {
-        std::vector<double> x0, u, v, vd, s, spos, smass, sstiff, qxi, qw, cinit;
+        std::vector<double> x0, u, v, vd, s, spos, smass, sstiff, qxi, qw, cinit, caxis;
         std::vector<int32_t> bno{0}, bni, bso{0}, bqo{0}, ctype, cbase, ctarget;
         for (const auto& n : nodes_) {
             x0.insert(x0.end(), n.x0.begin(), n.x0.end());
@@ -311,6 +322,8 @@ public:
             cbase.push_back(static_cast<int32_t>(c.base));
             ctarget.push_back(static_cast<int32_t>(c.node));
             cinit.insert(cinit.end(), c.u0.begin(), c.u0.end());
+            caxis.insert(caxis.end(), c.axis.begin(), c.axis.end());
+            if (c.control) m->controls.emplace_back(static_cast<int>(ctype.size() - 1), c.control);
         }
         kyn_model_desc d{};
         d.num_nodes = static_cast<int32_t>(nodes_.size());
@@ -323,7 +336,7 @@ public:
         d.beam_qp_offsets = bqo.data(); d.qp_xi = qxi.data(); d.qp_weight = qw.data();
         d.num_constraints = static_cast<int32_t>(cons_.size());
         d.constraint_type = ctype.data(); d.constraint_base_node = cbase.data();
-        d.constraint_target_node = ctarget.data(); d.constraint_axis = nullptr;
+        d.constraint_target_node = ctarget.data(); d.constraint_axis = caxis.data();
         d.constraint_initial_displacement = cinit.data();
         for (int k = 0; k < 3; ++k) d.gravity[k] = gravity_[k];
         const int id = kyn_model_create(ctx.get(), &d);
@@ -345,6 +358,8 @@ private:
         size_t node;
         std::array<double, 7> u0;
         size_t base = 0;
+        std::array<double, 3> axis{0., 0., 0.};
+        double* control = nullptr;
     };
     std::array<double, 3> gravity_{0., 0., 0.};
     std::vector<Node> nodes_;
@@ -359,6 +374,12 @@ inline bool Step(const StepParameters& parameters, Solver& solver, Elements&, St
     if (m->fx_dirty) {
         check(c, kyn_model_set_loads(c, m->id, KYN_LOAD_NODE_FX, m->node_fx.data()));
         m->fx_dirty = false;
+    }
+    // control signals into the constraints' input slot 0
+    // (src/constraints/constraints.hpp:345-352 UpdateViews)
+    for (const auto& [cid, signal] : m->controls) {
+        const double u[7] = {*signal, 0., 0., 1., 0., 0., 0.};
+        check(c, kyn_model_set_prescribed(c, m->id, cid, u));
     }
     const kyn_step_params p = parameters.c();
     int status = 0, iters = 0;

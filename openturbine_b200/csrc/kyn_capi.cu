@@ -285,6 +285,7 @@ void prepare_model(DevModel* m) {
             k.con_type[s2] = hb.con_type[s2];
             k.con_row[s2] = hb.con_row[s2];
             for (int d = 0; d < 3; ++d) k.con_X0[s2][d] = hb.con_X0[s2][d];
+            for (int d = 0; d < 3; ++d) k.con_axis[s2][d] = hb.con_axis[s2][d];
         }
         for (int d = 0; d < 3; ++d) k.gravity[d] = H.gravity[d];
         k.conv = m->d_conv;

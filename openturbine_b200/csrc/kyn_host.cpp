@@ -181,12 +181,12 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
         }
     }
     // A node outside every beam element is allowed only as the hub of a rotor:
-    // the base node of rigid joints, held by one single-node BC.
+    // the base node of the joints, held by one single-node BC.
     for (int n = 0; n < nn; ++n) {
         if (M.node_beam[n] >= 0) continue;
         bool is_hub = false;
         for (int c = 0; c < d->num_constraints && d->constraint_type; ++c)
-            is_hub |= d->constraint_type[c] == KYN_CONSTRAINT_RIGID_JOINT && d->constraint_base_node &&
+            is_hub |= is_hub_joint(d->constraint_type[c]) && d->constraint_base_node &&
                       d->constraint_base_node[c] == n;
         if (!is_hub) return fail(err, KYN_ERR_UNSUPPORTED, "node not attached to any beam element");
         if (M.hub >= 0) return fail(err, KYN_ERR_UNSUPPORTED, "more than one hub node in a model");
@@ -204,23 +204,22 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
     int joints = 0;
     for (int c = 0; c < d->num_constraints; ++c) {
         const int t = d->constraint_type[c];
-        if (t != KYN_CONSTRAINT_FIXED_BC && t != KYN_CONSTRAINT_PRESCRIBED_BC &&
-            t != KYN_CONSTRAINT_RIGID_JOINT)
+        if (t != KYN_CONSTRAINT_FIXED_BC && t != KYN_CONSTRAINT_PRESCRIBED_BC && !is_hub_joint(t))
             return fail(err, KYN_ERR_UNSUPPORTED,
-                        "only FixedBC, PrescribedBC and RigidJoint constraints");
+                        "only FixedBC, PrescribedBC, RigidJoint and RotationControl constraints");
         const int node = d->constraint_target_node[c];
         if (node < 0 || node >= nn) return fail(err, KYN_ERR_INVALID, "constraint node out of range");
-        if (t == KYN_CONSTRAINT_RIGID_JOINT) {
+        if (is_hub_joint(t)) {
             const int base = d->constraint_base_node ? d->constraint_base_node[c] : -1;
             if (base < 0 || base >= nn) return fail(err, KYN_ERR_INVALID, "joint base node out of range");
             if (base != M.hub || M.node_beam[node] < 0)
                 return fail(err, KYN_ERR_UNSUPPORTED,
-                            "rigid joints must join a hub node (in no beam) to a beam node");
+                            "joints must join a hub node (in no beam) to a beam node");
             node_cols[base].push_back(c);
             ++joints;
         }
         if (node == M.hub) {  // the hub's own boundary condition
-            if (t == KYN_CONSTRAINT_RIGID_JOINT || M.hub_con >= 0)
+            if (is_hub_joint(t) || M.hub_con >= 0)
                 return fail(err, KYN_ERR_UNSUPPORTED, "the hub needs exactly one FixedBC or PrescribedBC");
             M.hub_con = c;
             M.hub_con_type = t;
@@ -248,12 +247,20 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
             for (int k = 0; k < 3; ++k)
                 B.con_X0[slot][k] = x0[k] - (d->constraint_axis ? d->constraint_axis[c * 3 + k] : 0.);
             for (int k = 0; k < 7; ++k) B.slab[L.con_input + slot * 7 + k] = ident[k];
-        } else if (t == KYN_CONSTRAINT_RIGID_JOINT) {
+        } else if (is_hub_joint(t)) {
             // X0 = target x0 - base x0 (src/constraints/constraints.hpp:268-290)
             const double* x0 = d->node_x0 + node * 7;
             const double* xb = d->node_x0 + M.hub * 7;
             for (int k = 0; k < 3; ++k) B.con_X0[slot][k] = x0[k] - xb[k];
             for (int k = 0; k < 7; ++k) B.slab[L.con_input + slot * 7 + k] = ident[k];
+            if (t == KYN_CONSTRAINT_ROTATION_CONTROL) {
+                // axes row 0 = UnitVector(axis) (src/constraints/constraints.hpp:321-328)
+                const double* ax = d->constraint_axis ? d->constraint_axis + c * 3 : nullptr;
+                const double nrm = ax ? std::sqrt(ax[0] * ax[0] + ax[1] * ax[1] + ax[2] * ax[2]) : 0.;
+                if (!(nrm > 0.))
+                    return fail(err, KYN_ERR_INVALID, "rotation control needs a nonzero axis");
+                for (int k = 0; k < 3; ++k) B.con_axis[slot][k] = ax[k] / nrm;
+            }
         } else {
             for (int k = 0; k < 3; ++k) B.con_X0[slot][k] = 0.;
             const double* u = d->constraint_initial_displacement
@@ -264,7 +271,7 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
     }
 
     if (M.hub >= 0 && (M.hub_con < 0 || joints == 0))
-        return fail(err, KYN_ERR_UNSUPPORTED, "a hub node needs one BC and at least one rigid joint");
+        return fail(err, KYN_ERR_UNSUPPORTED, "a hub node needs one BC and at least one joint");
     if (M.hub >= 0) {
         // every beam carries a copy of the hub's state
         const int h = M.hub;
@@ -328,7 +335,7 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
             const int con = (row - M.nsys) / 6;
             const int node = d->constraint_target_node[con];
             for (int c = 0; c < 6; ++c) cols.push_back(M.fmap[node] + c);
-            if (d->constraint_type[con] == KYN_CONSTRAINT_RIGID_JOINT)
+            if (is_hub_joint(d->constraint_type[con]))
                 for (int c = 0; c < 6; ++c) cols.push_back(M.fmap[d->constraint_base_node[con]] + c);
         }
         std::sort(cols.begin(), cols.end());

@@ -24,6 +24,7 @@ struct HostBeam {
     int con_type[kMaxBeamConstraints] = {};
     int con_row[kMaxBeamConstraints] = {};   // constraint index in the model
     double con_X0[kMaxBeamConstraints][3] = {};
+    double con_axis[kMaxBeamConstraints][3] = {};  // RotationControl: unit axis
 };
 
 struct HostModel {

@@ -563,19 +563,23 @@ __device__ __forceinline__ void back_substitute_blocked(const TR* A, int ldA, in
 }
 
 // Residual, gradient blocks and G^T lambda of one constraint on node q `nu`
-// (calculate_constraint_residual_gradient.hpp:60-320 with
-// calculate_{fixed,prescribed}_bc_constraint.hpp and
-// calculate_rigid_joint_constraint.hpp:17-113).  FixedBC: R1 = I, u1 = 0;
-// PrescribedBC: (u1, R1) = the record's input; RigidJoint: (u1, R1) = the hub
+// (calculate_constraint_residual_gradient.hpp:60-320 and :468-540 with
+// calculate_{fixed,prescribed}_bc_constraint.hpp,
+// calculate_rigid_joint_constraint.hpp:17-113 and
+// calculate_rotation_control_constraint.hpp:17-144).  FixedBC: R1 = I, u1 = 0;
+// PrescribedBC: (u1, R1) = the record's input; joints: (u1, R1) = the hub
 // node's q `hq`, X0 = target x0 - hub x0, and the base-node blocks
 // tilde(R1 X0) T_hub and -AX(C) T_hub are kept for the hub elimination.
+// RotationControl puts the commanded rotation Rc = exp(angle * axis) (angle =
+// input[0]) between the target and the hub: C = R(R2 Rc^-1 R1^-1).
 __device__ inline void constraint_record(double* cr, int type, const double* nu, const double* X0,
-                                         const double* Rt, const double* hq, const double* RtHub) {
+                                         const double* Rt, const double* hq, const double* RtHub,
+                                         const double* axis) {
     double u1[3] = {0., 0., 0.}, R1[4] = {1., 0., 0., 0.};
     if (type == KYN_CONSTRAINT_PRESCRIBED_BC) {
         for (int k = 0; k < 3; ++k) u1[k] = cr[conrec::inp + k];
         for (int k = 0; k < 4; ++k) R1[k] = cr[conrec::inp + 3 + k];
-    } else if (type == KYN_CONSTRAINT_RIGID_JOINT) {
+    } else if (is_hub_joint(type)) {
         for (int k = 0; k < 3; ++k) u1[k] = hq[k];
         for (int k = 0; k < 4; ++k) R1[k] = hq[3 + k];
     }
@@ -588,7 +592,21 @@ __device__ inline void constraint_record(double* cr, int type, const double* nu,
     }
     for (int i = 0; i < 3; ++i) cr[conrec::Phi + i] = nu[i] + X0[i] - u1[i] - R1X0[i];
     double R2R1t[4];
-    quat_compose(nu + 3, R1t, R2R1t);
+    if (type == KYN_CONSTRAINT_ROTATION_CONTROL) {
+        // quaternion of the rotation vector axis*angle (quaternion_operations.hpp:231-242)
+        const double ang = cr[conrec::inp];
+        const double rv[3] = {axis[0] * ang, axis[1] * ang, axis[2] * ang};
+        const double th = sqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
+        const double fac = (fabs(th) < 1e-12) ? 0. : sin(th / 2.) / th;
+        const double Rc[4] = {cos(th / 2.), rv[0] * fac, rv[1] * fac, rv[2] * fac};
+        const double lc = sqrt(Rc[0] * Rc[0] + Rc[1] * Rc[1] + Rc[2] * Rc[2] + Rc[3] * Rc[3]);
+        const double Rct[4] = {Rc[0] / lc, -Rc[1] / lc, -Rc[2] / lc, -Rc[3] / lc};
+        double R2Rct[4];
+        quat_compose(nu + 3, Rct, R2Rct);
+        quat_compose(R2Rct, R1t, R2R1t);
+    } else {
+        quat_compose(nu + 3, R1t, R2R1t);
+    }
     double C[9];
     for (int e = 0; e < 9; ++e) C[e] = rot_entry(R2R1t, e / 3, e % 3);
     cr[conrec::Phi + 3] = (C[7] - C[5]) / 2.;
@@ -613,7 +631,7 @@ __device__ inline void constraint_record(double* cr, int type, const double* nu,
         for (int k = 0; k < 3; ++k) acc += AXm[i * 3 + k] * cr[conrec::lam + 3 + k];
         cr[conrec::Gl + 3 + i] = acc;
     }
-    if (type == KYN_CONSTRAINT_RIGID_JOINT) {
+    if (is_hub_joint(type)) {
         for (int i = 0; i < 3; ++i) cr[conrec::R1X0 + i] = R1X0[i];
         for (int i = 0; i < 3; ++i)
             for (int j = 0; j < 3; ++j) {
@@ -1189,11 +1207,11 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
             const int tn = KB.con_node[lane];
             constraint_record(con + lane * kConStride, KB.con_type[lane], sq + tn * 7, KB.con_X0[lane],
                               sT + tn * 9, hub ? hb + hubrec::q : nullptr,
-                              hub ? hb + hubrec::tangent : nullptr);
+                              hub ? hb + hubrec::tangent : nullptr, KB.con_axis[lane]);
         }
         if (hub && warp == NW - 1 && lane == nc)  // the hub's own boundary condition
             constraint_record(hb + hubsm::bc, KB.hub_con_type, hb + hubrec::q, hb + hubrec::X0,
-                              hb + hubrec::tangent, nullptr, nullptr);
+                              hb + hubrec::tangent, nullptr, nullptr, nullptr);
         __syncthreads();
 
         // ---- right-hand side: b = -cond (-f + R + G^T lambda) (assemble_system_residual.hpp,
@@ -1265,7 +1283,7 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
                 rt[k] = -cr[conrec::Phi + k];
                 rr[k] = -cr[conrec::Phi + 3 + k];
             }
-            if (KB.con_type[tid] == KYN_CONSTRAINT_RIGID_JOINT) {
+            if (is_hub_joint(KB.con_type[tid])) {
                 const double* xh = hb + hubsm::xh;
                 for (int i = 0; i < 3; ++i) {
                     rt[i] += xh[i];
@@ -1371,7 +1389,7 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
             double* pub = hb + hubsm::pub + 6 * (iter & 1);
             for (int k = 0; k < 6; ++k) pub[k] = 0.;
             for (int c = 0; c < nc; ++c) {
-                if (KB.con_type[c] != KYN_CONSTRAINT_RIGID_JOINT) continue;
+                if (!is_hub_joint(KB.con_type[c])) continue;
                 const double* cr = con + c * kConStride;
                 double w[6];
                 for (int k = 0; k < 6; ++k) w[k] = cr[conrec::lam + k] + cr[conrec::xl + k];

@@ -17,7 +17,7 @@
 
 namespace kyn {
 
-constexpr int kMaxBeamConstraints = 4;   // FixedBC / PrescribedBC / RigidJoint per beam
+constexpr int kMaxBeamConstraints = 4;   // FixedBC / PrescribedBC / joints per beam
 constexpr int kMaxClusterBeams = 8;      // beams per model (portable cluster size)
 constexpr int kMaxNewtonIters = 64;      // convergence-history capacity
 constexpr int kThreads = 256;            // threads per CTA of the step kernel
@@ -96,6 +96,10 @@ KYN_HD inline SlabLayout make_slab_layout(int N, int Q) {
 }
 
 // One beam as seen by the step kernel (built per launch plan).
+// Joints between the hub node and a target node (six rows, base blocks on the
+// hub): KYN_CONSTRAINT_RIGID_JOINT (3) and KYN_CONSTRAINT_ROTATION_CONTROL (5).
+KYN_HD inline bool is_hub_joint(int type) { return type == 3 || type == 5; }
+
 struct KBeam {
     double* slab;             // device slab of this beam
     int32_t N, Q, nc;         // nodes, quadrature points, constraints on this beam
@@ -106,8 +110,9 @@ struct KBeam {
     int32_t con_node[kMaxBeamConstraints];   // beam-local target node
     int32_t con_type[kMaxBeamConstraints];   // KYN_CONSTRAINT_*
     int32_t con_row[kMaxBeamConstraints];    // constraint index within the model
-    double con_X0[kMaxBeamConstraints][3];   // RigidJoint: target x0 - hub x0
-    int32_t hub;              // 1: the model has a hub (rigid joints in con_type)
+    double con_X0[kMaxBeamConstraints][3];   // joints: target x0 - hub x0
+    double con_axis[kMaxBeamConstraints][3]; // RotationControl: unit rotation axis
+    int32_t hub;              // 1: the model has a hub (joints in con_type)
     int32_t hub_con_type;     // KYN_CONSTRAINT_FIXED_BC / PRESCRIBED_BC on the hub
     double gravity[3];
     double* conv;             // [kMaxNewtonIters] model convergence history (rank 0)

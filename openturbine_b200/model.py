@@ -30,6 +30,7 @@ import numpy as np
 FIXED_BC = 1
 PRESCRIBED_BC = 2
 RIGID_JOINT = 3
+ROTATION_CONTROL = 5
 INVALID_NODE_ID = 0  # Model::InvalidNodeID
 
 
@@ -350,7 +351,8 @@ class PackedModel:
 
 
 class Model:
-    """src/model/model.hpp:74-693 (beams, FixedBC, PrescribedBC, gravity)."""
+    """src/model/model.hpp:74-693 (beams, FixedBC, PrescribedBC, RigidJoint,
+    RotationControl, gravity)."""
 
     InvalidNodeID = INVALID_NODE_ID
 
@@ -359,6 +361,7 @@ class Model:
         self.nodes_: list[Node] = []
         self.beam_elements_: list[BeamElement] = []
         self.constraints_: list[Constraint] = []
+        self.controls_: dict = {}
 
     def SetGravity(self, x: float, y: float, z: float) -> None:
         self.gravity_ = [float(x), float(y), float(z)]
@@ -419,6 +422,22 @@ class Model:
         cid = len(self.constraints_)
         self.constraints_.append(Constraint(cid, RIGID_JOINT, (int(node_ids[0]), int(node_ids[1]))))
         return cid
+
+    def AddRotationControl(self, node_ids, axis, control=None) -> int:
+        """src/model/model.hpp:550-562 AddRotationControl({base, target}, axis,
+        control).  `control` stands for the reference's double*: any object
+        that float() reads (a one-element array, for instance); its value at
+        each step is the commanded angle.  Context.set_control(model_id,
+        constraint_id, angle) passes it to a created model."""
+        cid = len(self.constraints_)
+        self.constraints_.append(Constraint(cid, ROTATION_CONTROL, (int(node_ids[0]), int(node_ids[1])),
+                                            tuple(float(x) for x in axis)))
+        self.controls_[cid] = control
+        return cid
+
+    def Controls(self) -> dict:
+        """Constraint id -> control object of the RotationControl constraints."""
+        return dict(self.controls_)
 
     def NumConstraints(self) -> int:
         return len(self.constraints_)

@@ -158,6 +158,11 @@ class Context:
         v = np.ascontiguousarray(u, dtype=np.float64)
         self._check(self.lib.kyn_model_set_prescribed(self.h, mid, cid, v.ctypes.data_as(_dp)))
 
+    def set_control(self, mid: int, cid: int, value: float) -> None:
+        """The commanded angle of a RotationControl constraint (the value the
+        reference reads through its control pointer before each step)."""
+        self.set_prescribed(mid, cid, [float(value), 0.0, 0.0, 1.0, 0.0, 0.0, 0.0])
+
     # stepping
     def step(self, ids, params: StepParameters):
         ids_a = np.ascontiguousarray(ids, dtype=np.int32)

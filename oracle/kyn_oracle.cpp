@@ -431,6 +431,7 @@ struct OConstraint {
     int type = 0;
     int base = 0, target = 0;
     double X0[3] = {0., 0., 0.};
+    double axis[3] = {0., 0., 0.};   // RotationControl: axes row 0 (unit axis)
     double input[7] = {0., 0., 0., 1., 0., 0., 0.};
     double lambda[6] = {0., 0., 0., 0., 0., 0.};
     double res[6] = {};
@@ -602,7 +603,7 @@ void update_beam(orc_model& m, OBeam& B, double beta_prime, double gamma_prime) 
 void update_rigid_joint(orc_model& m, OConstraint& C);
 
 void update_constraint(orc_model& m, OConstraint& C) {
-    if (C.type == KYN_CONSTRAINT_RIGID_JOINT) {
+    if (C.type == KYN_CONSTRAINT_RIGID_JOINT || C.type == KYN_CONSTRAINT_ROTATION_CONTROL) {
         update_rigid_joint(m, C);
         return;
     }
@@ -635,7 +636,10 @@ void update_constraint(orc_model& m, OConstraint& C) {
 }
 
 // src/constraints/calculate_rigid_joint_constraint.hpp:17-113 and the RigidJoint
-// branch of calculate_constraint_residual_gradient.hpp:251-320
+// branch of calculate_constraint_residual_gradient.hpp:251-320.  RotationControl
+// (calculate_rotation_control_constraint.hpp:17-144, branch :468-540) is the same
+// joint with the commanded rotation Rc = exp(input[0] axis) in the rotational
+// residual: C = R(R2 Rc^-1 R1^-1).
 void update_rigid_joint(orc_model& m, OConstraint& C) {
     const double* bu = &m.q[C.base * 7];
     const double* tu = &m.q[C.target * 7];
@@ -646,7 +650,16 @@ void update_rigid_joint(orc_model& m, OConstraint& C) {
     const V4 R1t = quat_inverse(R1);
     const V3 R1X0 = rotate_vec(R1, C.X0);
     for (int c = 0; c < 3; ++c) C.res[c] = u2[c] + C.X0[c] - u1[c] - R1X0[c];
-    const V4 R2R1t = quat_compose(R2, R1t.data());
+    V4 R2R1t;
+    if (C.type == KYN_CONSTRAINT_ROTATION_CONTROL) {
+        const double rv[3] = {C.axis[0] * C.input[0], C.axis[1] * C.input[0], C.axis[2] * C.input[0]};
+        const V4 Rc = rotvec_to_quat(rv);
+        const V4 Rct = quat_inverse(Rc.data());
+        const V4 R2Rct = quat_compose(R2, Rct.data());
+        R2R1t = quat_compose(R2Rct.data(), R1t.data());
+    } else {
+        R2R1t = quat_compose(R2, R1t.data());
+    }
     const M3 Cm = quat_to_rot(R2R1t.data());
     const V3 ax = axial(Cm);
     for (int c = 0; c < 3; ++c) C.res[3 + c] = ax[c];
@@ -1200,8 +1213,8 @@ orc_model* orc_model_create(const kyn_model_desc* d, char* err, int errlen) {
     for (int c = 0; c < d->num_constraints; ++c) {
         OConstraint& C = m->cons[c];
         C.type = d->constraint_type[c];
-        if (C.type != KYN_CONSTRAINT_FIXED_BC && C.type != KYN_CONSTRAINT_PRESCRIBED_BC &&
-            C.type != KYN_CONSTRAINT_RIGID_JOINT) {
+        const bool joint = C.type == KYN_CONSTRAINT_RIGID_JOINT || C.type == KYN_CONSTRAINT_ROTATION_CONTROL;
+        if (C.type != KYN_CONSTRAINT_FIXED_BC && C.type != KYN_CONSTRAINT_PRESCRIBED_BC && !joint) {
             bad(err, errlen, "constraint type outside this path");
             delete m;
             return nullptr;
@@ -1213,12 +1226,12 @@ orc_model* orc_model_create(const kyn_model_desc* d, char* err, int errlen) {
             delete m;
             return nullptr;
         }
-        if (C.type == KYN_CONSTRAINT_RIGID_JOINT && (C.base < 0 || C.base >= nn || C.base == C.target)) {
-            bad(err, errlen, "rigid joint base node out of range");
+        if (joint && (C.base < 0 || C.base >= nn || C.base == C.target)) {
+            bad(err, errlen, "joint base node out of range");
             delete m;
             return nullptr;
         }
-        C.base_active = (C.type == KYN_CONSTRAINT_RIGID_JOINT) ? 6 : 0;
+        C.base_active = joint ? 6 : 0;
         C.target_active = 6;
         C.row_first = start_row;
         C.row_last = start_row + 6;
@@ -1228,9 +1241,19 @@ orc_model* orc_model_create(const kyn_model_desc* d, char* err, int errlen) {
                                 d->constraint_axis ? d->constraint_axis[c * 3 + 2] : 0.};
         if (C.type == KYN_CONSTRAINT_FIXED_BC) {
             for (int k = 0; k < 3; ++k) C.X0[k] = m->x0[C.target * 7 + k] - axis[k];
-        } else if (C.type == KYN_CONSTRAINT_RIGID_JOINT) {
+        } else if (joint) {
             // src/constraints/constraints.hpp:268-290: relative position target - base
             for (int k = 0; k < 3; ++k) C.X0[k] = m->x0[C.target * 7 + k] - m->x0[C.base * 7 + k];
+            if (C.type == KYN_CONSTRAINT_ROTATION_CONTROL) {
+                // axes row 0 = UnitVector(axis) (src/constraints/constraints.hpp:321-328)
+                const double nrm = std::sqrt(axis[0] * axis[0] + axis[1] * axis[1] + axis[2] * axis[2]);
+                if (!(nrm > 0.)) {
+                    bad(err, errlen, "rotation control needs a nonzero axis");
+                    delete m;
+                    return nullptr;
+                }
+                for (int k = 0; k < 3; ++k) C.axis[k] = axis[k] / nrm;
+            }
         } else {
             const double idq[7] = {0., 0., 0., 1., 0., 0., 0.};
             for (int k = 0; k < 7; ++k)

@@ -1,6 +1,6 @@
 // The reference's regression drivers written against the C++ shim (kynema_b200.hpp):
-// test_cantilever_beam.cpp:31-138 and test_rotating_beam.cpp:93-150, same inputs,
-// same golden tolerances.  Exit code 0 on success.
+// test_cantilever_beam.cpp:31-138, test_rotating_beam.cpp:93-150 and :390-456
+// (rotation control), same inputs, same golden tolerances.  Exit code 0 on success.
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -79,11 +79,42 @@ static void rotating_beam(const Context& ctx) {
     if (solver.convergence_err().empty()) { std::printf("FAIL empty convergence history\n"); ++failures; }
 }
 
+// test_rotating_beam.cpp:390-456: pitch through a control signal the shim reads before each Step
+static void rotation_control(const Context& ctx) {
+    const std::vector<double> node_s{0., 0.11747233803526763, 0.35738424175967748, 0.64261575824032247, 0.88252766196473242, 1.};
+    Model model;
+    model.SetGravity(0., 0., 0.);
+    std::vector<size_t> ids;
+    for (double s : node_s) ids.push_back(model.AddNode().SetElemLocation(s).SetPosition(10 * s, 0., 0., 1., 0., 0., 0.).Build());
+    const std::vector<BeamSection> sections{BeamSection(0., kMass, kStiff), BeamSection(1., kMass, kStiff)};
+    model.AddBeamElement(ids, sections, kGauss7);
+    model.TranslateBeam(0, {2., 0., 0.});
+    double pitch = 0.;
+    const size_t hub = model.AddNode().SetPosition(0., 0., 0., 1., 0., 0., 0.).Build();
+    model.AddRotationControl({hub, ids.front()}, {1., 0., 0.}, &pitch);
+    model.AddFixedBC(hub);
+    auto [state, elements, constraints, solver] = model.CreateSystemWithSolver(ctx);
+    auto parameters = StepParameters(true, 5, 0.01, 0.9);
+    for (int i = 0; i < 10; ++i) {
+        pitch = 0.01 * (i + 1) * 3.14159265358979323846 / 2.;
+        if (!Step(parameters, solver, elements, state, constraints)) { std::printf("FAIL rotation control step %d\n", i); ++failures; }
+    }
+    // rows 0 and 5 of the golden q (test_rotating_beam.cpp:436-456)
+    const auto q = state.q();
+    const double root[7] = {-5.7690945215728628E-18, 2.0652319043893875E-18, -2.4953577261422928E-20,
+                            0.99691733356165013, 0.078459097906677058, 5.0946025505270351E-19, 3.3980589449407732E-19};
+    const double tip[7] = {-0.0000058187577280119813, -0.00014174393267219577, 0.0015608892113182621,
+                           0.9972883429355086, 0.073590276246437658, -0.00065565396382017294, -0.000049038763777556399};
+    for (int c = 0; c < 7; ++c) expect_near(q[c], root[c], 1e-6, "rotation control root q");
+    for (int c = 0; c < 7; ++c) expect_near(q[5 * 7 + c], tip[c], 1e-6, "rotation control tip q");
+}
+
 int main() {
     try {
         Context ctx(0);
         cantilever(ctx);
         rotating_beam(ctx);
+        rotation_control(ctx);
     } catch (const std::exception& e) {
         std::printf("FAIL exception: %s\n", e.what());
         return 2;

@@ -11,7 +11,8 @@ Sources (paths relative to the reference project root):
   tests/regression_tests/regression/test_rotor.cpp:150-189   IEA-15 expected q
   tests/regression_tests/regression/test_cantilever_beam.cpp expected tip q
   tests/regression_tests/regression/test_solver.cpp          assembled b, x, err
-  tests/regression_tests/regression/test_rotating_beam.cpp   expected q
+  tests/regression_tests/regression/test_rotating_beam.cpp   expected q (prescribed
+                                                             root; rotation control)
   tests/unit_tests/system/beams/test_curved_beam.hpp         kernel-level data
 """
 from __future__ import annotations
@@ -165,6 +166,19 @@ def main(ref: str) -> None:
     json.dump({"source": "tests/regression_tests/regression/test_rotating_beam.cpp",
                "q": view_after(rb[r0:], "state.q,"), "tolerance": 1e-6},
               open(os.path.join(out_dir, "rotating_beam.json"), "w"), indent=1)
+
+    # ---- rotation control (hub node, pitch about the blade axis) ------------------
+    r1 = rb.index("TEST(RotatingBeamTest, RotationControlConstraint)")
+    r2 = rb.index("TEST(RotatingBeamTest, CompoundRotationControlConstraint)")
+    r3 = rb.index("TEST(", r2 + 5)
+    rv = [float(m.group(2)) for m in
+          re.finditer(r"EXPECT_NEAR\(\s*rv\[(\d)\],\s*(" + NUM + r"),\s*(" + NUM + r")\)", rb[r2:r3])]
+    tol = [float(m.group(3)) for m in
+           re.finditer(r"EXPECT_NEAR\(\s*rv\[(\d)\],\s*(" + NUM + r"),\s*(" + NUM + r")\)", rb[r2:r3])]
+    json.dump({"source": "tests/regression_tests/regression/test_rotating_beam.cpp",
+               "fixed_hub": {"steps": 10, "q": view_after(rb[r1:r2], "state.q,"), "tolerance": 1e-6},
+               "prescribed_hub": {"steps": 100, "rv_root": rv, "tolerance": max(tol)}},
+              open(os.path.join(out_dir, "rotation_control.json"), "w"), indent=1)
 
     # ---- curved beam (kernel level) --------------------------------------------
     cb = strip_comments(open(os.path.join(unit, "test_curved_beam.hpp")).read())

@@ -123,3 +123,46 @@ def test_hub_rotor_restart(ctx, golden):
     drive(b, 4, 7)
     for f in ("q", "v", "vd", "a", "x"):
         np.testing.assert_array_equal(ctx.state(a, f), ctx.state(b, f))
+
+
+@pytest.mark.parametrize("prescribed_hub", [False, True])
+def test_rotation_control_matches_oracle_and_golden(ctx, prescribed_hub):
+    """RotationControl from a hub node to a blade root
+    (test_rotating_beam.cpp:390-512): the root is pitched by t pi/2 about x
+    while the hub is fixed, or turned about z by a PrescribedBC.  Same Newton
+    decisions and states as the oracle; the reference's golden q (fixed hub,
+    10 steps, 1e-6) or root rotation vector (prescribed hub, 100 steps, 1e-8)."""
+    from tests.workloads_ref import (quaternion_to_rotation_vector, rotation_control_inputs,
+                                     rotation_control_test_model)
+    g = load_golden("rotation_control.json")["prescribed_hub" if prescribed_hub else "fixed_hub"]
+    m, p, rc, bc = rotation_control_test_model(prescribed_hub)
+    pm = m.pack()
+    mid = ctx.create_model(pm)
+    rp, ci, _ = ctx.crs(mid, values=False)
+    orp, oci, _ = OracleModel(pm).crs()
+    assert np.array_equal(rp, orp) and np.array_equal(ci, oci)
+    tw = HubTwin(pm)
+    for i in range(g["steps"]):
+        pitch, u_hub = rotation_control_inputs(i)
+        ctx.set_control(mid, rc, pitch)
+        tw.set_prescribed(rc, [pitch, 0., 0., 1., 0., 0., 0.])
+        if prescribed_hub:
+            ctx.set_prescribed(mid, bc, u_hub)
+            tw.set_prescribed(bc, u_hub)
+        st, it = ctx.step([mid], p)
+        ost, oit = tw.step(p)
+        assert (st[0], it[0]) == (ost, oit) == (0, oit)
+        gc, oc = ctx.convergence(mid), tw.convergence()
+        assert len(gc) == len(oc)
+        for a, b in zip(gc, oc):
+            assert (a <= 1.0) == (b <= 1.0)
+            if b > 1.0:
+                assert abs(a - b) <= 1e-6 * b, (a, b)
+    assert_state_close(ctx, mid, tw, fields=FIELDS)
+    q = ctx.state(mid, "q")
+    if prescribed_hub:
+        np.testing.assert_allclose(quaternion_to_rotation_vector(q[0, 3:]), g["rv_root"],
+                                   rtol=0, atol=g["tolerance"])
+    else:
+        np.testing.assert_allclose(q.ravel(), g["q"], rtol=0, atol=g["tolerance"])
+    ctx.destroy_model(mid)

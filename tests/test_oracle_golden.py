@@ -123,3 +123,38 @@ def test_iea15_hub_rotor_converges_and_holds_the_joints():
         X0 = x0[r, :3] - x0[hub_id, :3]
         np.testing.assert_allclose(q[r, :3], np.array(RotateVectorByQuaternion(qh, X0)) - X0, atol=1e-6)
         np.testing.assert_allclose(np.abs(np.dot(q[r, 3:], qh)), 1.0, atol=1e-9)
+
+
+def test_rotation_control_fixed_hub_ten_steps():
+    """test_rotating_beam.cpp:390-456 (RotationControlConstraint): the blade
+    root pitched about x by pitch = t pi/2 from a fixed hub, 10 steps, q of all
+    7 nodes (the hub last) at the test's 1e-6."""
+    from tests.workloads_ref import rotation_control_inputs, rotation_control_test_model
+    g = load_golden("rotation_control.json")["fixed_hub"]
+    m, p, rc, _ = rotation_control_test_model(prescribed_hub=False)
+    o = OracleModel(m.pack())
+    for i in range(g["steps"]):
+        pitch, _ = rotation_control_inputs(i)
+        o.set_prescribed(rc, [pitch, 0., 0., 1., 0., 0., 0.])
+        st, _ = o.step(p)
+        assert st == 0
+    np.testing.assert_allclose(o.state("q").ravel(), g["q"], rtol=0, atol=g["tolerance"])
+
+
+def test_rotation_control_prescribed_hub_hundred_steps():
+    """test_rotating_beam.cpp:458-512 (CompoundRotationControlConstraint): hub
+    turned about z by azimuth = 0.5 t pi/2 while the root pitches by t pi/2;
+    after 100 steps the root's rotation vector matches at the test's 1e-8."""
+    from tests.workloads_ref import (quaternion_to_rotation_vector, rotation_control_inputs,
+                                     rotation_control_test_model)
+    g = load_golden("rotation_control.json")["prescribed_hub"]
+    m, p, rc, bc = rotation_control_test_model(prescribed_hub=True)
+    o = OracleModel(m.pack())
+    for i in range(g["steps"]):
+        pitch, u_hub = rotation_control_inputs(i)
+        o.set_prescribed(rc, [pitch, 0., 0., 1., 0., 0., 0.])
+        o.set_prescribed(bc, u_hub)
+        st, _ = o.step(p)
+        assert st == 0
+    rv = quaternion_to_rotation_vector(o.state("q")[0, 3:])
+    np.testing.assert_allclose(rv, g["rv_root"], rtol=0, atol=g["tolerance"])

@@ -106,6 +106,42 @@ def rotating_beam_root_displacement(i: int, omega: float = 0.1, h: float = 0.01)
     return [xr[0] - x0_root[0], xr[1] - x0_root[1], xr[2] - x0_root[2], *q]
 
 
+def rotation_control_test_model(prescribed_hub: bool = False):
+    """tests/regression_tests/regression/test_rotating_beam.cpp:390-430
+    (RotationControlConstraint: hub held by a FixedBC) and :458-500
+    (CompoundRotationControlConstraint: hub turned by a PrescribedBC).  The
+    blade root is pitched about x by a RotationControl from the hub.  Returns
+    (model, params, rotation-control constraint id, hub BC constraint id)."""
+    m = Model()
+    m.SetGravity(0., 0., 0.)
+    ids = [m.AddNode().SetElemLocation(s).SetPosition(10 * s, 0., 0., 1., 0., 0., 0.).Build()
+           for s in GLL6_S]
+    m.AddBeamElement(ids, [BeamSection(0., COMPOSITE_MASS, COMPOSITE_STIFF),
+                           BeamSection(1., COMPOSITE_MASS, COMPOSITE_STIFF)], GAUSS7)
+    m.TranslateBeam(0, [2.0, 0., 0.])
+    hub = m.AddNode().SetPosition(0., 0., 0., 1., 0., 0., 0.).Build()
+    rc = m.AddRotationControl([hub, ids[0]], [1., 0., 0.])
+    bc = m.AddPrescribedBC(hub) if prescribed_hub else m.AddFixedBC(hub)
+    return m, StepParameters(True, 5, 0.01, 0.9), rc, bc
+
+
+def rotation_control_inputs(i: int, h: float = 0.01):
+    """Pitch angle and hub displacement before step i (0-based) of the two
+    rotation-control tests: pitch = t pi/2, azimuth = 0.5 t pi/2 about z."""
+    t = h * (i + 1)
+    q = RotationVectorToQuaternion([0., 0., 0.5 * t * math.pi / 2.])
+    return t * math.pi / 2., [0., 0., 0., *q]
+
+
+def quaternion_to_rotation_vector(q):
+    """src/math/quaternion_operations.hpp:267-281 QuaternionToRotationVector."""
+    theta = 2. * math.acos(q[0])
+    s = math.sqrt(1. - q[0] * q[0])
+    if s > 1e-12:
+        return [theta * q[1] / s, theta * q[2] / s, theta * q[3] / s]
+    return [0., 0., 0.]
+
+
 def iea15_rotor_model(data: dict | None = None):
     """tests/regression_tests/regression/test_rotor.cpp:25-65 (CreateIEA15Blades)."""
     d = data or load_golden("iea15_rotor.json")
