@@ -105,7 +105,8 @@ enum {
 };
 
 /* Model description: the data Model::AddNode / AddBeamElement /
- * AddFixedBC / AddPrescribedBC / SetGravity collect on the host
+ * AddMassElement / AddSpringElement / AddFixedBC / AddPrescribedBC /
+ * SetGravity collect on the host
  * (src/model/model.hpp:74-693, src/model/node.hpp:35-60,
  * src/elements/beams/beam_section.hpp, src/constraints/constraint.hpp). */
 typedef struct kyn_model_desc {
@@ -135,7 +136,26 @@ typedef struct kyn_model_desc {
     const double* constraint_initial_displacement; /* [constraints][7] or NULL */
 
     double gravity[3];
+
+    /* Point masses and springs (src/model/model.hpp:294-415 AddMassElement,
+     * AddSpringElement).  A model of masses and springs only (num_beams = 0) runs
+     * on the lumped-element kernel; see KYN_LUMPED_* for its limits. */
+    int32_t num_masses;
+    const int32_t* mass_node;          /* [num_masses] MassElement::node_id        */
+    const double* mass_matrix;         /* [num_masses][6][6] M_star, material frame */
+    int32_t num_springs;
+    const int32_t* spring_nodes;       /* [num_springs][2] SpringElement::node_ids */
+    const double* spring_stiffness;    /* [num_springs] k                          */
+    const double* spring_length;       /* [num_springs] undeformed length l_ref    */
 } kyn_model_desc;
+
+/* Limits of a lumped model (masses, springs and single-node boundary
+ * conditions, no beam element): one CTA holds its dense system. */
+enum {
+    KYN_LUMPED_MAX_NODES = 24,
+    KYN_LUMPED_MAX_MASSES = 32,
+    KYN_LUMPED_MAX_SPRINGS = 64
+};
 
 /* Step controls: the arguments of the StepParameters constructor
  * (src/step/step_parameters.hpp:37-52) plus the arithmetic choice. */

@@ -240,6 +240,25 @@ class BeamElement:
 
 
 @dataclass
+class MassElement:
+    """src/elements/masses/mass_element.hpp."""
+
+    id: int
+    node_id: int
+    mass: np.ndarray
+
+
+@dataclass
+class SpringElement:
+    """src/elements/springs/spring_element.hpp."""
+
+    id: int
+    node_ids: tuple
+    stiffness: float
+    undeformed_length: float
+
+
+@dataclass
 class Constraint:
     """src/constraints/constraint.hpp."""
 
@@ -296,6 +315,9 @@ class KynModelDesc(ctypes.Structure):
         ("constraint_type", _ip), ("constraint_base_node", _ip), ("constraint_target_node", _ip),
         ("constraint_axis", _dp), ("constraint_initial_displacement", _dp),
         ("gravity", ctypes.c_double * 3),
+        ("num_masses", ctypes.c_int32), ("mass_node", _ip), ("mass_matrix", _dp),
+        ("num_springs", ctypes.c_int32), ("spring_nodes", _ip), ("spring_stiffness", _dp),
+        ("spring_length", _dp),
     ]
 
 
@@ -330,12 +352,16 @@ class PackedModel:
         d.num_nodes = a["node_x0"].shape[0]
         for k in ("node_x0", "node_u", "node_v", "node_vd", "node_s", "section_position",
                   "section_mass", "section_stiffness", "qp_xi", "qp_weight",
-                  "constraint_axis", "constraint_initial_displacement"):
+                  "constraint_axis", "constraint_initial_displacement", "mass_matrix",
+                  "spring_stiffness", "spring_length"):
             setattr(d, k, a[k].ctypes.data_as(_dp) if a[k].size else None)
         d.num_beams = a["beam_node_offsets"].shape[0] - 1
         d.num_constraints = a["constraint_type"].shape[0]
+        d.num_masses = a["mass_node"].shape[0]
+        d.num_springs = a["spring_nodes"].shape[0]
         for k in ("beam_node_offsets", "beam_node_ids", "beam_section_offsets", "beam_qp_offsets",
-                  "constraint_type", "constraint_base_node", "constraint_target_node"):
+                  "constraint_type", "constraint_base_node", "constraint_target_node",
+                  "mass_node", "spring_nodes"):
             setattr(d, k, a[k].ctypes.data_as(_ip) if a[k].size else None)
         for i in range(3):
             d.gravity[i] = self.gravity[i]
@@ -362,6 +388,8 @@ class Model:
         self.beam_elements_: list[BeamElement] = []
         self.constraints_: list[Constraint] = []
         self.controls_: dict = {}
+        self.mass_elements_: list[MassElement] = []
+        self.spring_elements_: list[SpringElement] = []
 
     def SetGravity(self, x: float, y: float, z: float) -> None:
         self.gravity_ = [float(x), float(y), float(z)]
@@ -402,6 +430,34 @@ class Model:
     def SetBeamVelocityAboutPoint(self, eid: int, velocity, point) -> None:
         for n in self.beam_elements_[eid].node_ids:
             self.nodes_[n].SetVelocityAboutPoint(velocity, point)
+
+    # point masses and springs
+    def AddMassElement(self, node_id: int, mass) -> int:
+        """src/model/model.hpp:305-311: a 6x6 mass matrix (material frame) at a node."""
+        eid = len(self.mass_elements_)
+        self.mass_elements_.append(MassElement(eid, int(node_id), np.asarray(mass, dtype=np.float64)
+                                               .reshape(6, 6)))
+        return eid
+
+    def GetMassElements(self) -> list["MassElement"]:
+        return self.mass_elements_
+
+    def NumMassElements(self) -> int:
+        return len(self.mass_elements_)
+
+    def AddSpringElement(self, node1_id: int, node2_id: int, stiffness: float,
+                         undeformed_length: float) -> int:
+        """src/model/model.hpp:376-389: a translational spring between two nodes."""
+        eid = len(self.spring_elements_)
+        self.spring_elements_.append(SpringElement(eid, (int(node1_id), int(node2_id)),
+                                                   float(stiffness), float(undeformed_length)))
+        return eid
+
+    def GetSpringElements(self) -> list["SpringElement"]:
+        return self.spring_elements_
+
+    def NumSpringElements(self) -> int:
+        return len(self.spring_elements_)
 
     # constraints
     def AddFixedBC(self, node_id: int) -> int:
@@ -488,6 +544,16 @@ class Model:
                                         dtype=f64).reshape(nc, 3),
             "constraint_initial_displacement": np.array(
                 [c.initial_displacement for c in self.constraints_], dtype=f64).reshape(nc, 7),
+        })
+        a.update({
+            "mass_node": np.array([m.node_id for m in self.mass_elements_], dtype=i32),
+            "mass_matrix": np.array([m.mass for m in self.mass_elements_],
+                                    dtype=f64).reshape(-1, 36),
+            "spring_nodes": np.array([s.node_ids for s in self.spring_elements_],
+                                     dtype=i32).reshape(-1, 2),
+            "spring_stiffness": np.array([s.stiffness for s in self.spring_elements_], dtype=f64),
+            "spring_length": np.array([s.undeformed_length for s in self.spring_elements_],
+                                      dtype=f64),
         })
         for k in a:
             a[k] = np.ascontiguousarray(a[k])

@@ -427,6 +427,26 @@ struct OBeam {
     std::vector<long> eft;              // [N][6]
 };
 
+// src/elements/masses/masses.hpp: one 6x6 mass at a node
+struct OMass {
+    int node = 0;
+    double mstar[36] = {};
+    double r0[4] = {1., 0., 0., 0.};   // node x0 rotation
+    double residual[6] = {};
+    double sysmat[36] = {};
+    long eft[6] = {};
+};
+
+// src/elements/springs/springs.hpp: translational spring between two nodes
+struct OSpring {
+    int n1 = 0, n2 = 0;
+    double x0[3] = {};                 // x0(node 2) - x0(node 1)
+    double l_ref = 0., k = 0.;
+    double residual[2][3] = {};
+    double stiff[2][2][9] = {};
+    long eft[2][3] = {};
+};
+
 struct OConstraint {
     int type = 0;
     int base = 0, target = 0;
@@ -454,6 +474,8 @@ struct orc_model {
     std::vector<unsigned> sig;
     std::vector<long> active, fmap;
     std::vector<OBeam> beams;
+    std::vector<OMass> masses;
+    std::vector<OSpring> springs;
     std::vector<OConstraint> cons;
     double gravity[3] = {0., 0., 0.};
     long nsys = 0, ndofs = 0;
@@ -596,6 +618,49 @@ void update_beam(orc_model& m, OBeam& B, double beta_prime, double gamma_prime) 
             gemm(false, false, 6, 6, 6, 1., &S[(i * N + j) * 36], 6, &m.tangent[nT * 36], 6, 1.,
                  out, 6);
         }
+    }
+}
+
+// src/system/masses/calculate_quadrature_point_values.hpp:40-152 (one mass at its
+// node: vd as the acceleration, residual Fi - Fg, matrix b'Muu + g'Guu + Kuu T)
+void update_mass(orc_model& m, OMass& M, double beta_prime, double gamma_prime) {
+    const int n = M.node;
+    const double* q = &m.q[n * 7];
+    const double* v = &m.v[n * 6];
+    const double* vd = &m.vd[n * 6];
+    double FI[6], FG[6], Muu[36], Guu[36], Kuu[36];
+    inertial_qp(M.mstar, M.r0, q + 3, vd, v + 3, vd + 3, m.gravity, FI, FG, Muu, Guu, Kuu);
+    for (int c = 0; c < 6; ++c) M.residual[c] = FI[c] - FG[c];
+    for (int k = 0; k < 36; ++k) M.sysmat[k] = beta_prime * Muu[k] + gamma_prime * Guu[k];
+    gemm(false, false, 6, 6, 6, 1., Kuu, 6, &m.tangent[n * 36], 6, 1., M.sysmat, 6);
+}
+
+// src/system/springs/calculate_quadrature_point_values.hpp:27-92 with
+// calculate_{distance_components,length,force_coefficients,force_vectors,stiffness_matrix}.hpp
+void update_spring(orc_model& m, OSpring& S) {
+    const double* u1 = &m.q[S.n1 * 7];
+    const double* u2 = &m.q[S.n2 * 7];
+    double r[3];
+    for (int c = 0; c < 3; ++c) r[c] = S.x0[c] + u2[c] - u1[c];
+    const double l = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    const double c1 = S.k * (S.l_ref / l - 1.);
+    const double c2 = S.k * S.l_ref / (l * l * l);
+    double f[3];
+    for (int c = 0; c < 3; ++c) f[c] = c1 * r[c];
+    double a[9] = {};
+    const double diag = c1 - c2 * l * l;
+    a[0] = a[4] = a[8] = diag;
+    const M3 rt = tilde(r);
+    gemm(false, false, 3, 3, 3, -c2, rt.data(), 3, rt.data(), 3, 1., a, 3);
+    for (int c = 0; c < 3; ++c) {
+        S.residual[0][c] = f[c];
+        S.residual[1][c] = -f[c];
+    }
+    for (int k = 0; k < 9; ++k) {
+        S.stiff[0][0][k] = a[k];
+        S.stiff[0][1][k] = -a[k];
+        S.stiff[1][0][k] = -a[k];
+        S.stiff[1][1][k] = a[k];
     }
 }
 
@@ -859,7 +924,10 @@ void assemble(orc_model& m, const Params& P) {
     for (int n = 0; n < m.num_nodes; ++n) tangent_operator(P.h, &m.q_delta[n * 6], &m.tangent[n * 36]);
     // src/step/update_system_variables_beams.hpp
     for (auto& B : m.beams) update_beam(m, B, P.bp, P.gp);
-    // src/step/assemble_system_residual.hpp:17-64 (forces, then beams)
+    // src/step/update_system_variables.hpp:23-28 (masses, springs)
+    for (auto& M : m.masses) update_mass(m, M, P.bp, P.gp);
+    for (auto& S : m.springs) update_spring(m, S);
+    // src/step/assemble_system_residual.hpp:17-64 (forces, beams, masses, springs)
     for (int n = 0; n < m.num_nodes; ++n) {
         const long d = m.fmap[n];
         const unsigned s = m.sig[n];
@@ -874,6 +942,13 @@ void assemble(orc_model& m, const Params& P) {
     for (auto& B : m.beams)
         for (int n = 0; n < B.N; ++n)
             for (int c = 0; c < 6; ++c) m.b[B.eft[n * 6 + c]] += B.residual[n * 6 + c];
+    for (auto& M : m.masses)  // src/solver/contribute_masses_to_vector.hpp
+        for (int c = 0; c < 6; ++c) m.b[M.eft[c]] += M.residual[c];
+    for (auto& S : m.springs)  // src/solver/contribute_springs_to_vector.hpp
+        for (int c = 0; c < 3; ++c) {
+            m.b[S.eft[0][c]] += S.residual[0][c];
+            m.b[S.eft[1][c]] += S.residual[1][c];
+        }
     // src/step/assemble_system_matrix.hpp -> contribute_beams_to_sparse_matrix.hpp:34-73
     for (auto& B : m.beams) {
         for (int n2 = 0; n2 < B.N; ++n2) {
@@ -887,6 +962,23 @@ void assemble(orc_model& m, const Params& P) {
                 }
             }
         }
+    }
+    // src/solver/contribute_masses_to_sparse_matrix.hpp
+    for (auto& M : m.masses) {
+        for (int c1 = 0; c1 < 6; ++c1) {
+            long off = find_offset(m, M.eft[c1], M.eft[0]);
+            for (int c2 = 0; c2 < 6; ++c2, ++off) m.values[off] += M.sysmat[c1 * 6 + c2] * P.cond;
+        }
+    }
+    // src/solver/contribute_springs_to_sparse_matrix.hpp
+    for (auto& S : m.springs) {
+        for (int a = 0; a < 2; ++a)
+            for (int b = 0; b < 2; ++b)
+                for (int c1 = 0; c1 < 3; ++c1) {
+                    long off = find_offset(m, S.eft[a][c1], S.eft[b][0]);
+                    for (int c2 = 0; c2 < 3; ++c2, ++off)
+                        m.values[off] += S.stiff[a][b][c1 * 3 + c2] * P.cond;
+                }
     }
     // src/step/update_constraint_variables.hpp
     for (auto& C : m.cons) update_constraint(m, C);
@@ -1207,6 +1299,34 @@ orc_model* orc_model_create(const kyn_model_desc* d, char* err, int errlen) {
         B.eft.assign(N * 6, 0);
     }
 
+    // src/elements/masses/create_masses.hpp, src/elements/springs/create_springs.hpp
+    m->masses.resize(d->num_masses > 0 ? d->num_masses : 0);
+    for (int e = 0; e < d->num_masses; ++e) {
+        OMass& M = m->masses[e];
+        M.node = d->mass_node[e];
+        if (M.node < 0 || M.node >= nn) {
+            bad(err, errlen, "mass node out of range");
+            delete m;
+            return nullptr;
+        }
+        for (int k = 0; k < 36; ++k) M.mstar[k] = d->mass_matrix[e * 36 + k];
+        for (int c = 0; c < 4; ++c) M.r0[c] = m->x0[M.node * 7 + 3 + c];
+    }
+    m->springs.resize(d->num_springs > 0 ? d->num_springs : 0);
+    for (int e = 0; e < d->num_springs; ++e) {
+        OSpring& S = m->springs[e];
+        S.n1 = d->spring_nodes[2 * e];
+        S.n2 = d->spring_nodes[2 * e + 1];
+        if (S.n1 < 0 || S.n1 >= nn || S.n2 < 0 || S.n2 >= nn || S.n1 == S.n2) {
+            bad(err, errlen, "spring nodes out of range");
+            delete m;
+            return nullptr;
+        }
+        for (int c = 0; c < 3; ++c) S.x0[c] = m->x0[S.n2 * 7 + c] - m->x0[S.n1 * 7 + c];
+        S.k = d->spring_stiffness[e];
+        S.l_ref = d->spring_length[e];
+    }
+
     // src/constraints/constraints.hpp:76-266
     m->cons.resize(d->num_constraints);
     long start_row = 0;
@@ -1267,6 +1387,11 @@ orc_model* orc_model_create(const kyn_model_desc* d, char* err, int errlen) {
     m->sig.assign(nn, 0U);
     for (auto& B : m->beams)
         for (int id : B.node_ids) m->sig[id] |= 0b111111U;
+    for (auto& M : m->masses) m->sig[M.node] |= 0b111111U;
+    for (auto& S : m->springs) {  // JustPosition
+        m->sig[S.n1] |= 0b111000U;
+        m->sig[S.n2] |= 0b111000U;
+    }
     for (auto& C : m->cons) {
         m->sig[C.target] |= 0b111111U;
         if (C.base_active) m->sig[C.base] |= 0b111111U;
@@ -1280,6 +1405,13 @@ orc_model* orc_model_create(const kyn_model_desc* d, char* err, int errlen) {
     for (auto& B : m->beams)
         for (int n = 0; n < B.N; ++n)
             for (int c = 0; c < 6; ++c) B.eft[n * 6 + c] = m->fmap[B.node_ids[n]] + c;
+    for (auto& M : m->masses)
+        for (int c = 0; c < 6; ++c) M.eft[c] = m->fmap[M.node] + c;
+    for (auto& S : m->springs)
+        for (int c = 0; c < 3; ++c) {
+            S.eft[0][c] = m->fmap[S.n1] + c;
+            S.eft[1][c] = m->fmap[S.n2] + c;
+        }
     for (auto& C : m->cons) {
         for (long c = 0; c < m->active[C.target]; ++c) C.target_table[c] = m->fmap[C.target] + c;
         for (int c = 0; c < 6; ++c) C.base_table[c] = C.base_active ? m->fmap[C.base] + c : 0;
@@ -1289,12 +1421,26 @@ orc_model* orc_model_create(const kyn_model_desc* d, char* err, int errlen) {
     m->ndofs = m->nsys + start_row;
 
     // src/solver/create_full_matrix.hpp:27-73
-    int maxn = 1;
+    // element connectivity in the order beams, masses, springs
+    int maxn = 2;
     for (auto& B : m->beams) maxn = std::max(maxn, B.N);
-    std::vector<long> npe(m->beams.size()), en(m->beams.size() * maxn, 0);
-    for (size_t e = 0; e < m->beams.size(); ++e) {
-        npe[e] = m->beams[e].N;
-        for (int k = 0; k < m->beams[e].N; ++k) en[e * maxn + k] = m->beams[e].node_ids[k];
+    const size_t ne = m->beams.size() + m->masses.size() + m->springs.size();
+    std::vector<long> npe(ne), en(ne * maxn, 0);
+    size_t e_at = 0;
+    for (size_t e = 0; e < m->beams.size(); ++e, ++e_at) {
+        npe[e_at] = m->beams[e].N;
+        for (int k = 0; k < m->beams[e].N; ++k) en[e_at * maxn + k] = m->beams[e].node_ids[k];
+    }
+    for (auto& M : m->masses) {
+        npe[e_at] = 1;
+        en[e_at * maxn] = M.node;
+        ++e_at;
+    }
+    for (auto& S : m->springs) {
+        npe[e_at] = 2;
+        en[e_at * maxn] = S.n1;
+        en[e_at * maxn + 1] = S.n2;
+        ++e_at;
     }
     const int nc = static_cast<int>(m->cons.size());
     std::vector<long> ba(nc), ta(nc), bt(nc * 6), tt(nc * 6), rr(nc * 2);
@@ -1311,12 +1457,12 @@ orc_model* orc_model_create(const kyn_model_desc* d, char* err, int errlen) {
     m->row_ptrs.resize(m->ndofs + 1);
     const long nnz = orc_crs_build(static_cast<int>(m->nsys), static_cast<int>(m->ndofs), nn,
                                    m->active.data(), m->fmap.data(),
-                                   static_cast<int>(m->beams.size()), maxn, npe.data(), en.data(),
+                                   static_cast<int>(ne), maxn, npe.data(), en.data(),
                                    nc, ba.data(), ta.data(), bt.data(), tt.data(), rr.data(),
                                    m->row_ptrs.data(), nullptr, 1);
     m->col_inds.resize(nnz);
     orc_crs_build(static_cast<int>(m->nsys), static_cast<int>(m->ndofs), nn, m->active.data(),
-                  m->fmap.data(), static_cast<int>(m->beams.size()), maxn, npe.data(), en.data(),
+                  m->fmap.data(), static_cast<int>(ne), maxn, npe.data(), en.data(),
                   nc, ba.data(), ta.data(), bt.data(), tt.data(), rr.data(), m->row_ptrs.data(),
                   m->col_inds.data(), 1);
     m->values.assign(nnz, 0.);

@@ -14,6 +14,8 @@ Sources (paths relative to the reference project root):
   tests/regression_tests/regression/test_rotating_beam.cpp   expected q (prescribed
                                                              root; rotation control)
   tests/unit_tests/system/beams/test_curved_beam.hpp         kernel-level data
+  tests/regression_tests/regression/test_masses.cpp,
+    test_precession.cpp, test_spring_mass_system.cpp          point masses, springs
 """
 from __future__ import annotations
 
@@ -179,6 +181,31 @@ def main(ref: str) -> None:
                "fixed_hub": {"steps": 10, "q": view_after(rb[r1:r2], "state.q,"), "tolerance": 1e-6},
                "prescribed_hub": {"steps": 100, "rv_root": rv, "tolerance": max(tol)}},
               open(os.path.join(out_dir, "rotation_control.json"), "w"), indent=1)
+
+    # ---- point masses and springs -------------------------------------------------
+    def near_calls(text: str, name: str):
+        pat = (r"EXPECT_NEAR\(\s*" + name + r"\((\d+),\s*(\d+)\),\s*(" + NUM + r"),\s*(" + NUM +
+               r")\s*\)")
+        return [(int(m.group(1)), int(m.group(2)), float(m.group(3)), float(m.group(4)))
+                for m in re.finditer(pat, text)]
+    ms = strip_comments(open(os.path.join(reg, "test_masses.cpp")).read())
+    ms = ms[ms.index("TEST(MassesTest, ExternalForce)"):]
+    pr = strip_comments(open(os.path.join(reg, "test_precession.cpp")).read())
+    sm = strip_comments(open(os.path.join(reg, "test_spring_mass_system.cpp")).read())
+    s1 = sm.index("SetUpSpringMassSystem()")
+    s2 = sm.index("SetUpSpringMassChainSystem()")
+    half, full = near_calls(sm[s1:s2], "q")[1], near_calls(sm[s1:s2], "q")[3]
+    json.dump({"source": ["tests/regression_tests/regression/test_masses.cpp",
+                          "tests/regression_tests/regression/test_precession.cpp",
+                          "tests/regression_tests/regression/test_spring_mass_system.cpp"],
+               "mass_external_force": {"steps": 1000, "v": [c[2] for c in near_calls(ms, "v_host")],
+                                       "tolerance": max(c[3] for c in near_calls(ms, "v_host"))},
+               "precession": {"steps": 500, "q": [c[2] for c in near_calls(pr, "q_host")],
+                              "tolerance": max(c[3] for c in near_calls(pr, "q_host"))},
+               "spring_mass": {"steps": 1000, "q1x_half": half[2], "q1x_end": full[2],
+                               "tolerance": max(half[3], full[3])},
+               "spring_mass_chain": {"steps": 1000, "tolerance": 1e-14}},
+              open(os.path.join(out_dir, "masses_springs.json"), "w"), indent=1)
 
     # ---- curved beam (kernel level) --------------------------------------------
     cb = strip_comments(open(os.path.join(unit, "test_curved_beam.hpp")).read())

@@ -158,3 +158,56 @@ def test_rotation_control_prescribed_hub_hundred_steps():
         assert st == 0
     rv = quaternion_to_rotation_vector(o.state("q")[0, 3:])
     np.testing.assert_allclose(rv, g["rv_root"], rtol=0, atol=g["tolerance"])
+
+
+def test_mass_external_force_velocity():
+    """test_masses.cpp:79-144: v after 1000 steps at the test's 1e-12."""
+    from tests.workloads_ref import mass_external_force_model
+    g = load_golden("masses_springs.json")["mass_external_force"]
+    m, p, f = mass_external_force_model()
+    o = OracleModel(m.pack())
+    o.set_state_f(f)
+    for _ in range(g["steps"]):
+        st, _ = o.step(p)
+        assert st == 0
+    np.testing.assert_allclose(o.state("v")[0], g["v"], rtol=0, atol=g["tolerance"])
+
+
+def test_precession_final_rotation():
+    """test_precession.cpp:29-53: q after 500 steps at the test's 1e-12."""
+    from tests.workloads_ref import precession_model
+    g = load_golden("masses_springs.json")["precession"]
+    m, p = precession_model()
+    o = OracleModel(m.pack())
+    for _ in range(g["steps"]):
+        st, _ = o.step(p)
+        assert st == 0
+    np.testing.assert_allclose(o.state("q")[0], g["q"], rtol=0, atol=g["tolerance"])
+
+
+def test_spring_mass_oscillation():
+    """test_spring_mass_system.cpp:62-96: x displacement of the mass at T/2 and T."""
+    from tests.workloads_ref import spring_mass_model
+    g = load_golden("masses_springs.json")["spring_mass"]
+    m, p = spring_mass_model()
+    o = OracleModel(m.pack())
+    for step in range(1, g["steps"] + 1):
+        st, _ = o.step(p)
+        assert st == 0
+        q = o.state("q")
+        if step == g["steps"] // 2:
+            assert abs(q[0, 0]) <= 1e-14
+            assert abs(q[1, 0] - g["q1x_half"]) <= g["tolerance"]
+    assert abs(q[1, 0] - g["q1x_end"]) <= g["tolerance"]
+
+
+def test_spring_mass_chain_stays_in_equilibrium():
+    """test_spring_mass_system.cpp:113-185: every x displacement stays 0 (1e-14)."""
+    from tests.workloads_ref import spring_mass_chain_model
+    g = load_golden("masses_springs.json")["spring_mass_chain"]
+    m, p = spring_mass_chain_model()
+    o = OracleModel(m.pack())
+    for _ in range(g["steps"]):
+        st, _ = o.step(p)
+        assert st == 0
+        assert np.abs(o.state("q")[:, 0]).max() <= g["tolerance"]

@@ -201,3 +201,60 @@ def iea15_hub_rotor_model(data: dict | None = None):
     hub_bc = m.AddPrescribedBC(hub_id)
     params = StepParameters(True, 6, d["h"], 0.0)
     return m, params, hub_bc, hub_id
+
+
+# ---- point masses and springs (tests/regression_tests/regression/) -----------------
+def mass_external_force_model():
+    """test_masses.cpp:79-144 (ExternalForce): a free unit mass, force_x = 5 and
+    torque_y = 3 in state.f, h = 0.001, rho_inf = 0, 1000 steps."""
+    m = Model()
+    m.SetGravity(0., 0., 0.)
+    n = m.AddNode().SetPosition(0, 0, 0, 1, 0, 0, 0).Build()
+    m.AddMassElement(n, np.eye(6))
+    f = np.zeros((1, 6))
+    f[0, 0], f[0, 4] = 5., 3.
+    return m, StepParameters(True, 5, 0.001, 0.0), f
+
+
+def precession_model():
+    """test_precession.cpp:9-40: a free mass spinning with v = (0,0,0,0.5,0.5,1)
+    and inertia diag(1, 1, 0.5); h = 0.01, rho_inf = 1, 500 steps."""
+    m = Model()
+    n = m.AddNode().SetVelocity(0., 0., 0., 0.5, 0.5, 1.0).Build()
+    m.AddMassElement(n, np.diag([1., 1., 1., 1., 1., 0.5]))
+    return m, StepParameters(True, 6, 0.01, 1.0)
+
+
+def spring_mass_model():
+    """test_spring_mass_system.cpp:23-60: a unit mass at x = 2 on a spring
+    (k = 10, l0 = 0) to a fixed node at the origin; h = T/1000 with
+    T = 2 pi sqrt(m/k), rho_inf = 0, 1000 steps."""
+    m = Model()
+    fixed = m.AddNode().SetPosition(0., 0., 0., 1., 0., 0., 0.).Build()
+    mass = m.AddNode().SetPosition(2., 0., 0., 1., 0., 0., 0.).Build()
+    m.AddMassElement(mass, np.eye(6))
+    m.AddFixedBC(fixed)
+    m.AddSpringElement(fixed, mass, 10., 0.)
+    period = 2. * math.pi * math.sqrt(1. / 10.)
+    return m, StepParameters(True, 6, period / 1000., 0.0)
+
+
+def spring_mass_chain_model(number_of_masses: int = 10):
+    """test_spring_mass_system.cpp:113-185: equal unit masses between equal
+    springs (k = 10, l0 = 0) anchored at both ends: static equilibrium."""
+    m = Model()
+    position = 0.
+    m.AddNode().SetPosition(position, 0., 0., 1., 0., 0., 0.)
+    for _ in range(number_of_masses):
+        position += 0.5
+        m.AddNode().SetPosition(position, 0., 0., 1., 0., 0., 0.)
+    position += 0.5
+    m.AddNode().SetPosition(position, 0., 0., 1., 0., 0., 0.)
+    for k in range(number_of_masses):
+        m.AddMassElement(k + 1, np.eye(6))
+    for k in range(number_of_masses + 1):
+        m.AddSpringElement(k, k + 1, 10., 0.)
+    m.AddFixedBC(0)
+    m.AddFixedBC(number_of_masses + 1)
+    final_time = 2. * math.pi * math.sqrt(1. / 10.)
+    return m, StepParameters(True, 6, final_time / 1000., 0.0)
