@@ -288,6 +288,9 @@ void prepare_model(DevModel* m) {
             for (int d = 0; d < 3; ++d) k.con_axis[s2][d] = hb.con_axis[s2][d];
         }
         for (int d = 0; d < 3; ++d) k.gravity[d] = H.gravity[d];
+        k.lumped = (hb.n_mass + hb.n_spring > 0) ? m->d_slab[b] + hb.lumped_off : nullptr;
+        k.n_mass = hb.n_mass;
+        k.n_spring = hb.n_spring;
         k.conv = m->d_conv;
         k.hub = hubf;
         k.hub_con_type = H.hub_con_type;
@@ -826,14 +829,16 @@ int kyn_model_info_get(kyn_ctx* c, int id, kyn_model_info* info) {
     if (!c || !info) return KYN_ERR_INVALID;
     DevModel* m = find_model(c, id);
     if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
+    const bool lumped = !m->host.beams.empty() && m->host.beams[0].lumped;
     info->num_nodes = m->host.num_nodes;
-    info->num_beams = static_cast<int32_t>(m->host.beams.size());
+    info->num_beams = lumped ? 0 : static_cast<int32_t>(m->host.beams.size());
     info->num_constraints = m->host.num_constraints;
     info->num_system_dofs = m->host.nsys;
     info->num_dofs = m->host.ndofs;
     info->nnz = static_cast<int32_t>(m->host.col_inds.size());
     int mn = 0, mq = 0;
     for (auto& b : m->host.beams) {
+        if (b.lumped) continue;
         mn = std::max(mn, b.N);
         mq = std::max(mq, b.Q);
     }
@@ -849,6 +854,8 @@ int kyn_model_set_loads(kyn_ctx* c, int id, int which, const double* values) {
     if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
     if (which != KYN_LOAD_NODE_FX && which != KYN_LOAD_STATE_F)
         return set_err(c, KYN_ERR_INVALID, "unknown load channel");
+    if (which == KYN_LOAD_NODE_FX && m->host.beams[0].lumped)
+        return set_err(c, KYN_ERR_UNSUPPORTED, "a model without beam elements has no node_FX");
     // Stage in pinned memory in beam-local order, then one copy per beam.
     size_t need = 0;
     for (auto& b : m->host.beams) need += 6 * b.N;

@@ -47,14 +47,51 @@ void lagrange_basis(double x, const std::vector<double>& xs, std::vector<double>
     }
 }
 
+// Node state of a beam's (or a lumped model's) slab from the description
+// (src/model/copy_nodes_to_state.hpp:14-60).
+static void init_node_state(const kyn_model_desc* d, const HostBeam& B, const SlabLayout& L,
+                            double* S) {
+    static const double ident[7] = {0., 0., 0., 1., 0., 0., 0.};
+    for (int k = 0; k < B.N; ++k) {
+        const int id = B.node_ids[k];
+        const double* x0 = d->node_x0 + id * 7;
+        const double* u = d->node_u ? d->node_u + id * 7 : ident;
+        for (int c = 0; c < 7; ++c) {
+            S[L.x0 + k * 7 + c] = x0[c];
+            S[L.q + k * 7 + c] = u[c];
+            S[L.q_prev + k * 7 + c] = u[c];
+        }
+        for (int c = 0; c < 3; ++c) S[L.x + k * 7 + c] = x0[c] + u[c];
+        qmul(u + 3, x0 + 3, S + L.x + k * 7 + 3);
+        for (int c = 0; c < 6; ++c) {
+            S[L.v + k * 6 + c] = d->node_v ? d->node_v[id * 6 + c] : 0.;
+            S[L.vd + k * 6 + c] = d->node_vd ? d->node_vd[id * 6 + c] : 0.;
+            S[L.a + k * 6 + c] = S[L.vd + k * 6 + c];
+        }
+        for (int c = 0; c < 3; ++c) S[L.tangent + k * 9 + c * 4] = 1.;
+    }
+}
+
 int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
     if (!d) return fail(err, KYN_ERR_INVALID, "null model description");
     if (d->num_nodes <= 0 || !d->node_x0 || !d->node_s)
         return fail(err, KYN_ERR_INVALID, "model needs nodes with x0 and s");
-    if (d->num_beams <= 0 || !d->beam_node_offsets || !d->beam_node_ids ||
-        !d->beam_section_offsets || !d->beam_qp_offsets || !d->section_position ||
-        !d->section_mass || !d->section_stiffness || !d->qp_xi || !d->qp_weight)
+    const int n_mass = d->num_masses > 0 ? d->num_masses : 0;
+    const int n_spring = d->num_springs > 0 ? d->num_springs : 0;
+    if ((n_mass > 0 && (!d->mass_node || !d->mass_matrix)) ||
+        (n_spring > 0 && (!d->spring_nodes || !d->spring_stiffness || !d->spring_length)))
+        return fail(err, KYN_ERR_INVALID, "mass or spring arrays missing");
+    // A model without beam elements is a lumped model: its masses, springs and
+    // boundary conditions form one dense system over all its nodes.
+    const bool lumped = d->num_beams == 0;
+    if (lumped && n_mass + n_spring == 0)
+        return fail(err, KYN_ERR_INVALID, "model needs beam elements, point masses or springs");
+    if (!lumped && (d->num_beams < 0 || !d->beam_node_offsets || !d->beam_node_ids ||
+                    !d->beam_section_offsets || !d->beam_qp_offsets || !d->section_position ||
+                    !d->section_mass || !d->section_stiffness || !d->qp_xi || !d->qp_weight))
         return fail(err, KYN_ERR_INVALID, "model needs at least one fully described beam");
+    if (lumped && d->num_nodes > KYN_LUMPED_MAX_NODES)
+        return fail(err, KYN_ERR_UNSUPPORTED, "lumped model larger than KYN_LUMPED_MAX_NODES nodes");
     if (d->num_beams > kMaxClusterBeams)
         return fail(err, KYN_ERR_UNSUPPORTED, "more than 8 beam elements in one model");
     const int nn = d->num_nodes;
@@ -159,26 +196,66 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
             S[L.qpw + q * 4 + 2] = w * J;
             S[L.qpw + q * 4 + 3] = w / J;
         }
-        // node state (src/model/copy_nodes_to_state.hpp:14-60)
-        static const double ident[7] = {0., 0., 0., 1., 0., 0., 0.};
-        for (int k = 0; k < N; ++k) {
-            const int id = B.node_ids[k];
-            const double* x0 = d->node_x0 + id * 7;
-            const double* u = d->node_u ? d->node_u + id * 7 : ident;
-            for (int c = 0; c < 7; ++c) {
-                S[L.x0 + k * 7 + c] = x0[c];
-                S[L.q + k * 7 + c] = u[c];
-                S[L.q_prev + k * 7 + c] = u[c];
-            }
-            for (int c = 0; c < 3; ++c) S[L.x + k * 7 + c] = x0[c] + u[c];
-            qmul(u + 3, x0 + 3, S + L.x + k * 7 + 3);
-            for (int c = 0; c < 6; ++c) {
-                S[L.v + k * 6 + c] = d->node_v ? d->node_v[id * 6 + c] : 0.;
-                S[L.vd + k * 6 + c] = d->node_vd ? d->node_vd[id * 6 + c] : 0.;
-                S[L.a + k * 6 + c] = S[L.vd + k * 6 + c];
-            }
-            for (int c = 0; c < 3; ++c) S[L.tangent + k * 9 + c * 4] = 1.;
+        init_node_state(d, B, L, S);
+    }
+    if (lumped) {
+        // one system over all nodes, no quadrature points
+        M.beams.resize(1);
+        HostBeam& B = M.beams[0];
+        B.N = nn;
+        B.Q = 0;
+        B.lumped = true;
+        for (int n = 0; n < nn; ++n) {
+            B.node_ids.push_back(n);
+            M.node_beam[n] = 0;
+            M.node_local[n] = n;
         }
+        const SlabLayout L = make_slab_layout(B.N, 0);
+        B.slab.assign(L.total, 0.);
+        init_node_state(d, B, L, B.slab.data());
+    }
+
+    // point masses and springs join the beam that holds their nodes
+    // (src/elements/masses/create_masses.hpp, src/elements/springs/create_springs.hpp)
+    std::vector<std::vector<double>> lrec_mass(M.beams.size()), lrec_spring(M.beams.size());
+    std::vector<int> node_mass(nn, 0);
+    for (int e = 0; e < n_mass; ++e) {
+        const int node = d->mass_node[e];
+        if (node < 0 || node >= nn) return fail(err, KYN_ERR_INVALID, "mass node out of range");
+        const int b = M.node_beam[node];
+        if (b < 0) return fail(err, KYN_ERR_UNSUPPORTED, "point mass on a node outside the beams");
+        auto& r = lrec_mass[b];
+        r.push_back(static_cast<double>(M.node_local[node]));
+        r.insert(r.end(), d->mass_matrix + e * 36, d->mass_matrix + e * 36 + 36);
+        r.insert(r.end(), d->node_x0 + node * 7 + 3, d->node_x0 + node * 7 + 7);
+        node_mass[node] = 1;
+    }
+    M.spring_nodes.assign(n_spring * 2, 0);
+    for (int e = 0; e < n_spring; ++e) {
+        const int n1 = d->spring_nodes[2 * e], n2 = d->spring_nodes[2 * e + 1];
+        if (n1 < 0 || n1 >= nn || n2 < 0 || n2 >= nn || n1 == n2)
+            return fail(err, KYN_ERR_INVALID, "spring nodes out of range");
+        const int b = M.node_beam[n1];
+        if (b < 0 || M.node_beam[n2] != b)
+            return fail(err, KYN_ERR_UNSUPPORTED, "spring between nodes of different beams");
+        auto& r = lrec_spring[b];
+        r.push_back(static_cast<double>(M.node_local[n1]));
+        r.push_back(static_cast<double>(M.node_local[n2]));
+        for (int c = 0; c < 3; ++c) r.push_back(d->node_x0[n2 * 7 + c] - d->node_x0[n1 * 7 + c]);
+        r.push_back(d->spring_length[e]);
+        r.push_back(d->spring_stiffness[e]);
+        M.spring_nodes[2 * e] = n1;
+        M.spring_nodes[2 * e + 1] = n2;
+    }
+    for (size_t b = 0; b < M.beams.size(); ++b) {
+        HostBeam& B = M.beams[b];
+        B.n_mass = static_cast<int>(lrec_mass[b].size()) / kMassRec;
+        B.n_spring = static_cast<int>(lrec_spring[b].size()) / kSpringRec;
+        if (B.n_mass > KYN_LUMPED_MAX_MASSES || B.n_spring > KYN_LUMPED_MAX_SPRINGS)
+            return fail(err, KYN_ERR_UNSUPPORTED, "more point masses or springs than one system holds");
+        B.lumped_off = static_cast<int>(B.slab.size());
+        B.slab.insert(B.slab.end(), lrec_mass[b].begin(), lrec_mass[b].end());
+        B.slab.insert(B.slab.end(), lrec_spring[b].begin(), lrec_spring[b].end());
     }
     // A node outside every beam element is allowed only as the hub of a rotor:
     // the base node of the joints, held by one single-node BC.
@@ -270,6 +347,11 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
         }
     }
 
+    if (lumped)  // every node of a lumped model needs its 6 DOFs from a mass or a BC
+        for (int n = 0; n < nn; ++n)
+            if (!node_mass[n] && node_con[n] < 0)
+                return fail(err, KYN_ERR_UNSUPPORTED,
+                            "lumped-model node without a point mass or a boundary condition");
     if (M.hub >= 0 && (M.hub_con < 0 || joints == 0))
         return fail(err, KYN_ERR_UNSUPPORTED, "a hub node needs one BC and at least one joint");
     if (M.hub >= 0) {
@@ -320,7 +402,7 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
         cols.clear();
         if (row < M.nsys) {
             const int node = row / 6;
-            if (M.node_beam[node] >= 0) {
+            if (M.node_beam[node] >= 0 && !M.beams[M.node_beam[node]].lumped) {
                 const HostBeam& B = M.beams[M.node_beam[node]];
                 for (int k = 0; k < B.N; ++k)
                     for (int c = 0; c < 6; ++c) cols.push_back(M.fmap[B.node_ids[k]] + c);
@@ -328,6 +410,14 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
                 // a node in no element still holds its own diagonal block
                 // (compute_system_row_entries.hpp starts every row with it)
                 for (int c = 0; c < 6; ++c) cols.push_back(M.fmap[node] + c);
+            }
+            // a spring adds its other node's columns once per spring, also where
+            // another element already added them (compute_system_col_inds.hpp:65-79)
+            for (size_t e = 0; e + 1 < M.spring_nodes.size(); e += 2) {
+                const int n1 = M.spring_nodes[e], n2 = M.spring_nodes[e + 1];
+                if (n1 != node && n2 != node) continue;
+                const int other = (n1 == node) ? n2 : n1;
+                for (int c = 0; c < 6; ++c) cols.push_back(M.fmap[other] + c);
             }
             for (int con : node_cols[node])
                 for (int c = 0; c < 6; ++c) cols.push_back(M.nsys + 6 * con + c);

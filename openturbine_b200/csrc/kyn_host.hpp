@@ -25,6 +25,9 @@ struct HostBeam {
     int con_row[kMaxBeamConstraints] = {};   // constraint index in the model
     double con_X0[kMaxBeamConstraints][3] = {};
     double con_axis[kMaxBeamConstraints][3] = {};  // RotationControl: unit axis
+    bool lumped = false;              // all nodes of a model without beam elements (Q = 0)
+    int n_mass = 0, n_spring = 0;     // point masses / springs at this beam's nodes
+    int lumped_off = 0;               // their records' offset in the slab (kMassRec, kSpringRec)
 };
 
 struct HostModel {
@@ -33,6 +36,7 @@ struct HostModel {
     std::vector<HostBeam> beams;
     std::vector<int> node_beam, node_local;   // node -> (beam, local index)
     std::vector<int> con_beam, con_slot;      // constraint -> (beam, slot)
+    std::vector<int> spring_nodes;            // [springs][2] global node ids
     std::vector<int> fmap;                    // node -> first DOF
     int nsys = 0, ndofs = 0;
     std::vector<int> row_ptrs, col_inds;      // reference CRS graph (sorted rows)

@@ -659,6 +659,154 @@ __device__ inline void joint_base_transpose_add(const double* cr, const double* 
     }
 }
 
+// ---- point masses and springs at the nodes of one CTA's system ---------------------
+// Adds, for local node n, the terms of every point mass at n
+// (src/system/masses/calculate_quadrature_point_values.hpp:40-152: residual
+// Fi - Fg, block b'Muu + g'Guu + Kuu T) and of every spring with an end at n
+// (src/system/springs/calculate_quadrature_point_values.hpp:27-92: residual
+// +-f, translational blocks +-a) to resid[n] and to node n's block row of A
+// (scaled by the conditioner).  One thread per node: each writes only its own
+// rows, and takes its elements in element order.
+template <typename TR>
+__device__ void add_lumped_terms(int n, const double* __restrict__ rec, int n_mass, int n_spring,
+                                 const double* sq, const double* sv, const double* svd,
+                                 const double* sT, const double* grav, double bprime,
+                                 double gprime, double cond, const int* pos, TR* A, int ldA,
+                                 double* resid) {
+    TR* Arow = A + (6 * pos[n]) * ldA;
+    const int cn = 6 * pos[n];
+    for (int e = 0; e < n_mass; ++e) {
+        const double* mr = rec + e * kMassRec;
+        if (static_cast<int>(mr[0]) != n) continue;
+        const double* ms = mr + 1;
+        // Muu = diag(R, R) M* diag(R, R)^T, R = R(r o r0)
+        double xr[4], R[9];
+        quat_compose(sq + n * 7 + 3, mr + 37, xr);
+        for (int e9 = 0; e9 < 9; ++e9) R[e9] = rot_entry(xr, e9 / 3, e9 % 3);
+        double Mu[36];
+        for (int bi = 0; bi < 2; ++bi)
+            for (int bj = 0; bj < 2; ++bj)
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) {
+                        double acc = 0.;
+                        for (int k = 0; k < 3; ++k) {
+                            double t = 0.;
+                            for (int l = 0; l < 3; ++l) t += ms[(3 * bi + k) * 6 + 3 * bj + l] * R[j * 3 + l];
+                            acc += R[i * 3 + k] * t;
+                        }
+                        Mu[(3 * bi + i) * 6 + 3 * bj + j] = acc;
+                    }
+        const double mass = Mu[0];
+        const double eta[3] = {Mu[5 * 6 + 1] / mass, -Mu[5 * 6 + 0] / mass, Mu[4 * 6 + 0] / mass};
+        double rho[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) rho[i * 3 + j] = Mu[(3 + i) * 6 + 3 + j];
+        const double* ud = svd + n * 6;       // u_ddot = vd[0:3], omega_dot = vd[3:6]
+        const double* od = svd + n * 6 + 3;
+        const double* om = sv + n * 6 + 3;
+        const double me[3] = {mass * eta[0], mass * eta[1], mass * eta[2]};
+        auto mat3 = [](const double* a, const double* b, int i, int j) {
+            return a[i * 3] * b[j] + a[i * 3 + 1] * b[3 + j] + a[i * 3 + 2] * b[6 + j];
+        };
+        double omt[9], odt[9], met[9], udt[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                omt[i * 3 + j] = tilde_e(om, i, j);
+                odt[i * 3 + j] = tilde_e(od, i, j);
+                met[i * 3 + j] = tilde_e(me, i, j);
+                udt[i * 3 + j] = tilde_e(ud, i, j);
+            }
+        double oo[9], orho[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                oo[i * 3 + j] = mat3(omt, omt, i, j);
+                orho[i * 3 + j] = mat3(omt, rho, i, j);
+            }
+        // inertial force (calculate_inertial_force.hpp) minus gravity (calculate_gravity_force.hpp)
+        double r6[6];
+        for (int i = 0; i < 3; ++i) {
+            double acc = 0.;
+            for (int k = 0; k < 3; ++k) acc += (mass * oo[i * 3 + k] + mass * odt[i * 3 + k]) * eta[k];
+            r6[i] = acc + mass * ud[i] - mass * grav[i];
+        }
+        for (int i = 0; i < 3; ++i) {
+            double acc = 0.;
+            for (int k = 0; k < 3; ++k)
+                acc += tilde_e(eta, i, k) * (mass * ud[k]) + rho[i * 3 + k] * od[k] + orho[i * 3 + k] * om[k] -
+                       tilde_e(eta, i, k) * (mass * grav[k]);
+            r6[3 + i] = acc;
+        }
+        for (int c = 0; c < 6; ++c) resid[n * 6 + c] += r6[c];
+        // Guu (calculate_gyroscopic_matrix.hpp) and Kuu (calculate_inertia_stiffness_matrix.hpp):
+        // both are zero outside the columns 3..5
+        double wm[3], rw[3], rwd[3];
+        for (int i = 0; i < 3; ++i) {
+            wm[i] = omt[i * 3] * me[0] + omt[i * 3 + 1] * me[1] + omt[i * 3 + 2] * me[2];
+            rw[i] = rho[i * 3] * om[0] + rho[i * 3 + 1] * om[1] + rho[i * 3 + 2] * om[2];
+            rwd[i] = rho[i * 3] * od[0] + rho[i * 3 + 1] * od[1] + rho[i * 3 + 2] * od[2];
+        }
+        double G12[9], G22[9], K12[9], K22[9], M1[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) M1[i * 3 + j] = mat3(rho, omt, i, j) - tilde_e(rw, i, j);
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                double a12 = tilde_e(wm, j, i), k12 = 0., k22 = 0.;
+                for (int k = 0; k < 3; ++k) {
+                    a12 += omt[i * 3 + k] * met[j * 3 + k];
+                    k12 += (odt[i * 3 + k] + oo[i * 3 + k]) * met[j * 3 + k];
+                    k22 += rho[i * 3 + k] * odt[k * 3 + j] + udt[i * 3 + k] * met[k * 3 + j] +
+                           omt[i * 3 + k] * M1[k * 3 + j];
+                }
+                G12[i * 3 + j] = a12;
+                G22[i * 3 + j] = orho[i * 3 + j] - tilde_e(rw, i, j);
+                K12[i * 3 + j] = k12;
+                K22[i * 3 + j] = k22 - tilde_e(rwd, i, j);
+            }
+        // block b'Muu + g'Guu + Kuu T (T = I on the translational block)
+        const double* Tn = sT + n * 9;
+        for (int r = 0; r < 6; ++r) {
+            for (int c = 0; c < 6; ++c) {
+                double val = bprime * Mu[r * 6 + c];
+                if (c >= 3) {
+                    const int cc = c - 3;
+                    const double* G = r < 3 ? G12 + r * 3 : G22 + (r - 3) * 3;
+                    const double* K = r < 3 ? K12 + r * 3 : K22 + (r - 3) * 3;
+                    val += gprime * G[cc];
+                    val += K[0] * Tn[cc] + K[1] * Tn[3 + cc] + K[2] * Tn[6 + cc];
+                }
+                TR* a = Arow + r * ldA + cn + c;
+                *a = static_cast<TR>(static_cast<double>(*a) + val * cond);
+            }
+        }
+    }
+    const double* srec = rec + n_mass * kMassRec;
+    for (int e = 0; e < n_spring; ++e) {
+        const double* sp = srec + e * kSpringRec;
+        const int n1 = static_cast<int>(sp[0]), n2 = static_cast<int>(sp[1]);
+        if (n1 != n && n2 != n) continue;
+        double r[3];
+        for (int c = 0; c < 3; ++c) r[c] = sp[2 + c] + sq[n2 * 7 + c] - sq[n1 * 7 + c];
+        const double l = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+        const double lref = sp[5], k = sp[6];
+        const double c1 = k * (lref / l - 1.);
+        const double c2 = k * lref / (l * l * l);
+        const double sgn = (n == n1) ? 1. : -1.;
+        for (int c = 0; c < 3; ++c) resid[n * 6 + c] += sgn * (c1 * r[c]);
+        const int other = (n == n1) ? n2 : n1;
+        const int co = 6 * pos[other];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                double rr = 0.;
+                for (int t = 0; t < 3; ++t) rr += tilde_e(r, i, t) * tilde_e(r, t, j);
+                const double a = ((i == j) ? c1 - c2 * l * l : 0.) - c2 * rr;
+                TR* d = Arow + i * ldA + cn + j;
+                *d = static_cast<TR>(static_cast<double>(*d) + a * cond);
+                TR* o = Arow + i * ldA + co + j;
+                *o = static_cast<TR>(static_cast<double>(*o) - a * cond);
+            }
+    }
+}
+
 // ---- the kernel ------------------------------------------------------------------
 // Resident CTAs per SM that each instance is compiled for (its register budget
 // is 65536 / (NT * this), 128 registers per thread for all three).  Three
@@ -1200,6 +1348,12 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
             }
         }
         __syncthreads();
+        if (KB.n_mass + KB.n_spring > 0) {  // point masses and springs at this CTA's nodes
+            for (int n = tid; n < N; n += NT)
+                add_lumped_terms(n, KB.lumped, KB.n_mass, KB.n_spring, sq, sv, svd, sT, KB.gravity,
+                                 P.beta_prime, P.gamma_prime, P.conditioner, pos, A, ldA, resid);
+            __syncthreads();
+        }
         mark(kPhaseIntegrate);
 
         // ---- constraints (calculate_constraint_residual_gradient.hpp:60-320) -------

@@ -96,6 +96,12 @@ KYN_HD inline SlabLayout make_slab_layout(int N, int Q) {
 }
 
 // One beam as seen by the step kernel (built per launch plan).
+// Point-mass and spring records behind KBeam::lumped (doubles):
+//   mass   [kMassRec]   = node, M_star[36] (material frame), r0[4] (node x0 rotation)
+//   spring [kSpringRec] = node 1, node 2, x0[3] (x0 of node 2 - x0 of node 1), l_ref, k
+constexpr int kMassRec = 41;
+constexpr int kSpringRec = 7;
+
 // Joints between the hub node and a target node (six rows, base blocks on the
 // hub): KYN_CONSTRAINT_RIGID_JOINT (3) and KYN_CONSTRAINT_ROTATION_CONTROL (5).
 KYN_HD inline bool is_hub_joint(int type) { return type == 3 || type == 5; }
@@ -112,6 +118,8 @@ struct KBeam {
     int32_t con_row[kMaxBeamConstraints];    // constraint index within the model
     double con_X0[kMaxBeamConstraints][3];   // joints: target x0 - hub x0
     double con_axis[kMaxBeamConstraints][3]; // RotationControl: unit rotation axis
+    const double* lumped;     // point masses then springs at this beam's nodes, or null
+    int32_t n_mass, n_spring; // (records of kMassRec / kSpringRec doubles, node-local indices)
     int32_t hub;              // 1: the model has a hub (joints in con_type)
     int32_t hub_con_type;     // KYN_CONSTRAINT_FIXED_BC / PRESCRIBED_BC on the hub
     double gravity[3];
