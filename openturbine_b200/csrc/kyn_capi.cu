@@ -40,6 +40,7 @@ struct DevModel {
     std::vector<SlabLayout> lay;     // per beam slab layout
     std::vector<KBeam> kt;           // per beam launch record (plan fields filled per plan)
     int def_nt[2] = {0, 0};          // default threads per CTA, FP64 / FP32 form
+    bool lump = false;               // some beam carries point masses or springs
     int smem_nt[2][3] = {};          // dynamic smem for 128 / 256 / 512 threads, per form
     double work = 0.;                // largest beam's N^2 Q + 72 (N-1)^3 (ordering in buckets)
     double* d_conv = nullptr;        // [kMaxNewtonIters]
@@ -64,6 +65,7 @@ struct ClassKey {
 struct Bucket {
     int cluster = 1;
     int nt = 256;      // threads per CTA (step_kernel instance)
+    bool lump = false; // some beam carries point masses or springs
     int smem = 0;
     int first = 0;     // first beam in the plan's beam array
     int count = 0;     // beams
@@ -257,6 +259,8 @@ void prepare_model(DevModel* m) {
     m->lay.clear();
     m->kt.clear();
     m->work = 0.;
+    m->lump = false;
+    for (const HostBeam& hb : H.beams) m->lump |= hb.n_mass + hb.n_spring > 0;
     for (int f = 0; f < 2; ++f) {
         const int rb = f ? 4 : 8;
         m->def_nt[f] = 128;
@@ -314,7 +318,8 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
     plan->precision = precision;
     const int f = (precision == KYN_PRECISION_FP32_REFINED) ? 1 : 0;
     const int rbytes = f ? 4 : 8;
-    // bucket key: (cluster size, threads, CTAs per SM class); larger work first
+    // bucket key: (point masses/springs, cluster size, threads, CTAs per SM
+    // class); larger work first
     struct Entry {
         int model_index;
         int cluster;
@@ -323,6 +328,7 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
         int smem;
         double work;
         DevModel* m;
+        bool lump;
     };
     std::vector<Entry> entries;
     entries.reserve(n);
@@ -336,10 +342,12 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
             if (tuned != c->tuned.end()) nt = tuned->second;
         }
         const int smem = m->smem_nt[f][nt_index(nt)];
-        entries.push_back({i, static_cast<int>(m->kt.size()), nt, ctas_per_sm(rbytes, nt, smem), smem, m->work, m});
+        entries.push_back({i, static_cast<int>(m->kt.size()), nt, ctas_per_sm(rbytes, nt, smem), smem,
+                           m->work, m, m->lump});
         nbeams += m->kt.size();
     }
     std::sort(entries.begin(), entries.end(), [](const Entry& a, const Entry& b) {
+        if (a.lump != b.lump) return b.lump;
         if (a.cluster != b.cluster) return a.cluster > b.cluster;
         if (a.nt != b.nt) return a.nt > b.nt;
         if (a.cls != b.cls) return a.cls < b.cls;
@@ -364,11 +372,12 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
     for (size_t e = 0; e < entries.size(); ++e) {
         const Entry& en = entries[e];
         if (plan->buckets.empty() || plan->buckets.back().cluster != en.cluster ||
-            plan->buckets.back().nt != en.nt ||
+            plan->buckets.back().nt != en.nt || plan->buckets.back().lump != en.lump ||
             ctas_per_sm(rbytes, en.nt, plan->buckets.back().smem) != en.cls) {
             Bucket bk;
             bk.cluster = en.cluster;
             bk.nt = en.nt;
+            bk.lump = en.lump;
             bk.first = static_cast<int>(nk);
             plan->buckets.push_back(bk);
         }
@@ -417,6 +426,23 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
     return KYN_OK;
 }
 
+using StepKernelFn = void (*)(const KBeam*, StepCoeffs, int, int*, int*);
+
+// The step kernel instance for an arithmetic form, a thread count and whether
+// point masses or springs are present.
+StepKernelFn pick_kernel(bool fp32, int nt, bool lump) {
+    if (lump) {
+        if (fp32) return nt == 128 ? step_kernel<float, 128, true>
+                       : nt == 256 ? step_kernel<float, 256, true> : step_kernel<float, 512, true>;
+        return nt == 128 ? step_kernel<double, 128, true>
+             : nt == 256 ? step_kernel<double, 256, true> : step_kernel<double, 512, true>;
+    }
+    if (fp32) return nt == 128 ? step_kernel<float, 128, false>
+                   : nt == 256 ? step_kernel<float, 256, false> : step_kernel<float, 512, false>;
+    return nt == 128 ? step_kernel<double, 128, false>
+         : nt == 256 ? step_kernel<double, 256, false> : step_kernel<double, 512, false>;
+}
+
 template <typename K>
 cudaError_t set_smem_attr(K kernel) {
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
@@ -424,12 +450,8 @@ cudaError_t set_smem_attr(K kernel) {
 
 int configure_smem(kyn_ctx* c) {
     if (c->smem_configured < kMaxDynSmem) {
-        KYN_CUDA(c, set_smem_attr(step_kernel<double, 128>));
-        KYN_CUDA(c, set_smem_attr(step_kernel<double, 256>));
-        KYN_CUDA(c, set_smem_attr(step_kernel<double, 512>));
-        KYN_CUDA(c, set_smem_attr(step_kernel<float, 128>));
-        KYN_CUDA(c, set_smem_attr(step_kernel<float, 256>));
-        KYN_CUDA(c, set_smem_attr(step_kernel<float, 512>));
+        for (int k = 0; k < 12; ++k)
+            KYN_CUDA(c, set_smem_attr(pick_kernel(k & 1, 128 << ((k >> 1) % 3), k >= 6)));
         c->smem_configured = kMaxDynSmem;
     }
     return KYN_OK;
@@ -462,11 +484,8 @@ int launch_plan(kyn_ctx* c, Plan* plan, const kyn_step_params* p) {
         const KBeam* beams = plan->d_kbeams + bk.first;
         const int rec = plan->record ? 1 : 0;
         const bool fp32 = plan->precision == KYN_PRECISION_FP32_REFINED;
-        auto kern = fp32 ? (bk.nt == 128 ? step_kernel<float, 128>
-                            : bk.nt == 256 ? step_kernel<float, 256> : step_kernel<float, 512>)
-                         : (bk.nt == 128 ? step_kernel<double, 128>
-                            : bk.nt == 256 ? step_kernel<double, 256> : step_kernel<double, 512>);
-        KYN_CUDA(c, cudaLaunchKernelEx(&cfg, kern, beams, P, rec, plan->d_status, plan->d_iters));
+        KYN_CUDA(c, cudaLaunchKernelEx(&cfg, pick_kernel(fp32, bk.nt, bk.lump), beams, P, rec,
+                                       plan->d_status, plan->d_iters));
         c->launches++;
     }
     c->last_buckets = nb;

@@ -817,7 +817,10 @@ __host__ __device__ constexpr int step_min_blocks(int real_bytes, int nt) {
     return (void)real_bytes, nt == 128 ? 4 : nt == 256 ? 2 : 1;
 }
 
-template <typename TR, int NT>
+// LUMP: the instance that also adds point masses and springs (KBeam::lumped);
+// beams without them run the instance compiled without that code, whose
+// registers it would otherwise crowd.
+template <typename TR, int NT, bool LUMP>
 __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
     step_kernel(const KBeam* __restrict__ beams, StepCoeffs P, int record,
                 int* __restrict__ status_out, int* __restrict__ iters_out) {
@@ -1348,7 +1351,7 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
             }
         }
         __syncthreads();
-        if (KB.n_mass + KB.n_spring > 0) {  // point masses and springs at this CTA's nodes
+        if (LUMP && KB.n_mass + KB.n_spring > 0) {  // point masses and springs at this CTA's nodes
             for (int n = tid; n < N; n += NT)
                 add_lumped_terms(n, KB.lumped, KB.n_mass, KB.n_spring, sq, sv, svd, sT, KB.gravity,
                                  P.beta_prime, P.gamma_prime, P.conditioner, pos, A, ldA, resid);
