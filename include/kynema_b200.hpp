@@ -265,6 +265,16 @@ public:
     void SetBeamVelocityAboutPoint(size_t e, const std::array<double, 6>& v, const std::array<double, 3>& p) {
         for (auto n : beams_[e].nodes) nodes_[n].SetVelocityAboutPoint(v, p);
     }
+    // src/model/model.hpp:305-311 AddMassElement: 6x6 mass (material frame) at a node
+    size_t AddMassElement(size_t node, const std::array<std::array<double, 6>, 6>& mass) {
+        masses_.push_back({node, mass});
+        return masses_.size() - 1;
+    }
+    // src/model/model.hpp:376-389 AddSpringElement
+    size_t AddSpringElement(size_t node1, size_t node2, double stiffness, double undeformed_length) {
+        springs_.push_back({node1, node2, stiffness, undeformed_length});
+        return springs_.size() - 1;
+    }
     size_t AddFixedBC(size_t node) {
         cons_.push_back({KYN_CONSTRAINT_FIXED_BC, node, {0., 0., 0., 1., 0., 0., 0.}});
         return cons_.size() - 1;
@@ -339,6 +349,22 @@ public:
         d.constraint_target_node = ctarget.data(); d.constraint_axis = caxis.data();
         d.constraint_initial_displacement = cinit.data();
         for (int k = 0; k < 3; ++k) d.gravity[k] = gravity_[k];
+        std::vector<int32_t> mnode, snodes;
+        std::vector<double> mmat, sk, sl;
+        for (const auto& ms : masses_) {
+            mnode.push_back(static_cast<int32_t>(ms.node));
+            for (const auto& row : ms.mass) mmat.insert(mmat.end(), row.begin(), row.end());
+        }
+        for (const auto& sp : springs_) {
+            snodes.push_back(static_cast<int32_t>(sp.n1));
+            snodes.push_back(static_cast<int32_t>(sp.n2));
+            sk.push_back(sp.k);
+            sl.push_back(sp.l0);
+        }
+        d.num_masses = static_cast<int32_t>(masses_.size());
+        d.mass_node = mnode.data(); d.mass_matrix = mmat.data();
+        d.num_springs = static_cast<int32_t>(springs_.size());
+        d.spring_nodes = snodes.data(); d.spring_stiffness = sk.data(); d.spring_length = sl.data();
         const int id = kyn_model_create(ctx.get(), &d);
         check(ctx.get(), id);
         m->id = id;
@@ -361,6 +387,16 @@ private:
         std::array<double, 3> axis{0., 0., 0.};
         double* control = nullptr;
     };
+    struct Mass {
+        size_t node;
+        std::array<std::array<double, 6>, 6> mass;
+    };
+    struct Spring {
+        size_t n1, n2;
+        double k, l0;
+    };
+    std::vector<Mass> masses_;
+    std::vector<Spring> springs_;
     std::array<double, 3> gravity_{0., 0., 0.};
     std::vector<Node> nodes_;
     std::vector<Beam> beams_;

@@ -1,6 +1,7 @@
 // The reference's regression drivers written against the C++ shim (kynema_b200.hpp):
 // test_cantilever_beam.cpp:31-138, test_rotating_beam.cpp:93-150 and :390-456
-// (rotation control), same inputs, same golden tolerances.  Exit code 0 on success.
+// (rotation control), test_spring_mass_system.cpp:23-96, same inputs, same golden
+// tolerances.  Exit code 0 on success.
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -109,12 +110,32 @@ static void rotation_control(const Context& ctx) {
     for (int c = 0; c < 7; ++c) expect_near(q[5 * 7 + c], tip[c], 1e-6, "rotation control tip q");
 }
 
+// test_spring_mass_system.cpp:23-96: a mass on a spring to a fixed node, no beam element
+static void spring_mass(const Context& ctx) {
+    Model model;
+    const size_t fixed = model.AddNode().SetPosition(0., 0., 0., 1., 0., 0., 0.).Build();
+    const size_t mass = model.AddNode().SetPosition(2., 0., 0., 1., 0., 0., 0.).Build();
+    model.AddMassElement(mass, {{{1., 0., 0., 0., 0., 0.}, {0., 1., 0., 0., 0., 0.}, {0., 0., 1., 0., 0., 0.},
+                                 {0., 0., 0., 1., 0., 0.}, {0., 0., 0., 0., 1., 0.}, {0., 0., 0., 0., 0., 1.}}});
+    model.AddFixedBC(fixed);
+    model.AddSpringElement(fixed, mass, 10., 0.);
+    const double T = 2. * 3.14159265358979323846 * std::sqrt(1. / 10.);
+    auto parameters = StepParameters(true, 6, T / 1000., 0.);
+    auto [state, elements, constraints, solver] = model.CreateSystemWithSolver(ctx);
+    for (int i = 1; i <= 1000; ++i) {
+        if (!Step(parameters, solver, elements, state, constraints)) { std::printf("FAIL spring-mass step %d\n", i); ++failures; }
+        if (i == 500) expect_near(state.q()[7], -3.9999199193098396, 1e-12, "spring-mass x at T/2");
+    }
+    expect_near(state.q()[7], -8.1226588438437419e-05, 1e-12, "spring-mass x at T");
+}
+
 int main() {
     try {
         Context ctx(0);
         cantilever(ctx);
         rotating_beam(ctx);
         rotation_control(ctx);
+        spring_mass(ctx);
     } catch (const std::exception& e) {
         std::printf("FAIL exception: %s\n", e.what());
         return 2;
