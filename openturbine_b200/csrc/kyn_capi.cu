@@ -579,6 +579,9 @@ int get_xfer(kyn_ctx* c, const int* ids, int n, int kind, XferPlan** out) {
             xb.map_off = static_cast<int>(map.size());
             int width = 6, fo;
             if (kind == KYN_LOAD_NODE_FX) {
+                if (b.elem_ids.size() != 1)
+                    return set_err(c, KYN_ERR_UNSUPPORTED,
+                                   "batched node_FX needs single-element beams (use kyn_model_set_loads)");
                 fo = L.fx;
                 xb.ext_off = off + elem * 6;
                 for (int k = 0; k < b.N; ++k) map.push_back(k);
@@ -850,7 +853,7 @@ int kyn_model_info_get(kyn_ctx* c, int id, kyn_model_info* info) {
     if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
     const bool lumped = !m->host.beams.empty() && m->host.beams[0].lumped;
     info->num_nodes = m->host.num_nodes;
-    info->num_beams = lumped ? 0 : static_cast<int32_t>(m->host.beams.size());
+    info->num_beams = lumped ? 0 : m->host.num_elements;
     info->num_constraints = m->host.num_constraints;
     info->num_system_dofs = m->host.nsys;
     info->num_dofs = m->host.ndofs;
@@ -875,7 +878,8 @@ int kyn_model_set_loads(kyn_ctx* c, int id, int which, const double* values) {
         return set_err(c, KYN_ERR_INVALID, "unknown load channel");
     if (which == KYN_LOAD_NODE_FX && m->host.beams[0].lumped)
         return set_err(c, KYN_ERR_UNSUPPORTED, "a model without beam elements has no node_FX");
-    // Stage in pinned memory in beam-local order, then one copy per beam.
+    // Stage in pinned memory in beam-local order, then one copy per beam; node_FX
+    // rows of the elements of a multi-element beam add up at shared nodes.
     size_t need = 0;
     for (auto& b : m->host.beams) need += 6 * b.N;
     if (c->h_stage_len < need) {
@@ -887,20 +891,31 @@ int kyn_model_set_loads(kyn_ctx* c, int id, int which, const double* values) {
         c->h_stage_len = need;
     }
     KYN_CUDA(c, cudaStreamSynchronize(c->stream));
-    size_t off = 0, elem = 0;
+    size_t off = 0;
     for (size_t bi = 0; bi < m->host.beams.size(); ++bi) {
         const HostBeam& b = m->host.beams[bi];
         const SlabLayout L = make_slab_layout(b.N, b.Q);
-        for (int k = 0; k < b.N; ++k)
-            for (int cc = 0; cc < 6; ++cc)
-                c->h_stage[off + k * 6 + cc] = (which == KYN_LOAD_NODE_FX)
-                                                   ? values[(elem + k) * 6 + cc]
-                                                   : values[b.node_ids[k] * 6 + cc];
+        if (which == KYN_LOAD_NODE_FX && b.elem_ids.size() > 1) {
+            for (int k = 0; k < 6 * b.N; ++k) c->h_stage[off + k] = 0.;
+            for (size_t ei = 0; ei < b.elem_ids.size(); ++ei) {
+                const int row = m->host.elem_row[b.elem_ids[ei]];
+                const auto& loc = b.elem_local[ei];
+                for (size_t k = 0; k < loc.size(); ++k)
+                    for (int cc = 0; cc < 6; ++cc)
+                        c->h_stage[off + loc[k] * 6 + cc] += values[(row + k) * 6 + cc];
+            }
+        } else {
+            const size_t row = (which == KYN_LOAD_NODE_FX) ? m->host.elem_row[b.elem_ids[0]] : 0;
+            for (int k = 0; k < b.N; ++k)
+                for (int cc = 0; cc < 6; ++cc)
+                    c->h_stage[off + k * 6 + cc] = (which == KYN_LOAD_NODE_FX)
+                                                       ? values[(row + k) * 6 + cc]
+                                                       : values[b.node_ids[k] * 6 + cc];
+        }
         KYN_CUDA(c, cudaMemcpyAsync(m->d_slab[bi] + (which == KYN_LOAD_NODE_FX ? L.fx : L.f),
                                     c->h_stage + off, 6 * b.N * sizeof(double),
                                     cudaMemcpyHostToDevice, c->stream));
         off += 6 * b.N;
-        elem += b.N;
     }
     KYN_CUDA(c, cudaStreamSynchronize(c->stream));
     return KYN_OK;
@@ -1595,6 +1610,9 @@ int kyn_set_loads_batch_static(kyn_ctx* c, const int* ids, int n, int which,
             xb.N = b.N;
             xb.map_off = rows;
             if (which == KYN_LOAD_NODE_FX) {
+                if (b.elem_ids.size() != 1)
+                    return set_err(c, KYN_ERR_UNSUPPORTED,
+                                   "batched node_FX needs single-element beams (use kyn_model_set_loads)");
                 xb.slab_field = m->d_slab[bi] + L.fx;
                 xb.ext_off = off + elem * 6;
                 for (int k = 0; k < b.N; ++k) g_static_host_map[rows + k] = k;

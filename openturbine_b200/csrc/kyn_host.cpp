@@ -49,6 +49,85 @@ void lagrange_basis(double x, const std::vector<double>& xs, std::vector<double>
 
 // Node state of a beam's (or a lumped model's) slab from the description
 // (src/model/copy_nodes_to_state.hpp:14-60).
+// Shape tables, quadrature weights, Jacobian, reference line tangent, r0 and
+// interpolated sections of element e's quadrature points, written at points
+// [qo, qo + Q_e) of a slab over N local nodes; element node k is local column
+// loc[k] (global node enode[k]).
+static int fill_element_qps(const kyn_model_desc* d, int e, const std::vector<int>& enode,
+                            const std::vector<int>& loc, int Nloc, int qo, const SlabLayout& L,
+                            double* S, std::string& err) {
+    const int s0 = d->beam_section_offsets[e], s1 = d->beam_section_offsets[e + 1];
+    const int q0 = d->beam_qp_offsets[e], q1 = d->beam_qp_offsets[e + 1];
+    const int N = static_cast<int>(enode.size()), Q = q1 - q0;
+    // shape functions on node locations xi = 2 s - 1 (populate_element_views.hpp:45-78)
+    std::vector<double> node_xi(N), val, der;
+    for (int k = 0; k < N; ++k) node_xi[k] = 2. * d->node_s[enode[k]] - 1.;
+    for (int a = 0; a < N; ++a)
+        for (int b = a + 1; b < N; ++b)
+            if (node_xi[a] == node_xi[b])
+                return fail(err, KYN_ERR_INVALID, "two beam nodes share an element location");
+    std::vector<double> sec_xi(s1 - s0);
+    for (int s = s0; s < s1; ++s) sec_xi[s - s0] = 2. * d->section_position[s] - 1.;
+    for (int q = 0; q < Q; ++q) {
+        const double xi = d->qp_xi[q0 + q];
+        lagrange_basis(xi, node_xi, val, der);
+        for (int k = 0; k < N; ++k) {
+            S[L.phi + (qo + q) * Nloc + loc[k]] = val[k];
+            S[L.dphi + (qo + q) * Nloc + loc[k]] = der[k];
+        }
+        // sections: linear interpolation in xi, clamped at the ends
+        // (populate_element_views.hpp:90-141, interpolation.hpp LinearInterpWeights)
+        std::vector<double> wsec(sec_xi.size(), 0.);
+        const auto lo = std::lower_bound(sec_xi.begin(), sec_xi.end(), xi);
+        if (lo == sec_xi.begin()) {
+            wsec.front() = 1.;
+        } else if (lo == sec_xi.end()) {
+            wsec.back() = 1.;
+        } else {
+            const size_t idx = static_cast<size_t>(lo - sec_xi.begin());
+            const double wu = (xi - sec_xi[idx - 1]) / (sec_xi[idx] - sec_xi[idx - 1]);
+            wsec[idx - 1] = 1. - wu;
+            wsec[idx] = wu;
+        }
+        for (int k = 0; k < 36; ++k) {
+            double m = 0., c = 0.;
+            for (size_t s = 0; s < sec_xi.size(); ++s) {
+                m += d->section_mass[(s0 + s) * 36 + k] * wsec[s];
+                c += d->section_stiffness[(s0 + s) * 36 + k] * wsec[s];
+            }
+            S[L.mstar + (qo + q) * 36 + k] = m;
+            S[L.cstar + (qo + q) * 36 + k] = c;
+        }
+        // reference rotation: normalised interpolated node orientation
+        // (interpolation_operations.hpp InterpQuaternion)
+        double r[4] = {0., 0., 0., 0.};
+        double xp[3] = {0., 0., 0.};
+        for (int k = 0; k < N; ++k) {
+            const double* x0 = d->node_x0 + enode[k] * 7;
+            for (int c = 0; c < 4; ++c) r[c] += x0[3 + c] * val[k];
+            for (int c = 0; c < 3; ++c) xp[c] += x0[c] * der[k];
+        }
+        const double rl = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3]);
+        if (rl == 0.) {
+            S[L.r0 + (qo + q) * 4] = 1.;
+        } else {
+            for (int c = 0; c < 4; ++c) S[L.r0 + (qo + q) * 4 + c] = r[c] / rl;
+        }
+        // Jacobian |dx0/dxi| and unit tangent (calculate_jacobian.hpp:36-76)
+        const double J = std::sqrt(xp[0] * xp[0] + xp[1] * xp[1] + xp[2] * xp[2]);
+        if (!(J > 0.)) return fail(err, KYN_ERR_INVALID, "degenerate beam reference line");
+        for (int c = 0; c < 3; ++c) S[L.x0p + (qo + q) * 3 + c] = xp[c] / J;
+        const double w = d->qp_weight[q0 + q];
+        for (int k = 0; k < N; ++k)
+            S[L.dphiJ + (qo + q) * Nloc + loc[k]] = S[L.dphi + (qo + q) * Nloc + loc[k]] / J;
+        S[L.qpw + (qo + q) * 4 + 0] = w;
+        S[L.qpw + (qo + q) * 4 + 1] = J;
+        S[L.qpw + (qo + q) * 4 + 2] = w * J;
+        S[L.qpw + (qo + q) * 4 + 3] = w / J;
+    }
+    return KYN_OK;
+}
+
 static void init_node_state(const kyn_model_desc* d, const HostBeam& B, const SlabLayout& L,
                             double* S) {
     static const double ident[7] = {0., 0., 0., 1., 0., 0., 0.};
@@ -100,101 +179,100 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
     for (int c = 0; c < 3; ++c) M.gravity[c] = d->gravity[c];
     M.node_beam.assign(nn, -1);
     M.node_local.assign(nn, -1);
-    M.beams.resize(d->num_beams);
-
+    // Elements that share nodes form one system (a multi-element beam): group
+    // them into connected components; each component is one CTA's system over
+    // its nodes, with every element's shape tables spread over the component's
+    // local node columns (zeros outside the element), so that the integration
+    // sums the overlap of elements at shared nodes
+    // (src/solver/compute_system_row_entries.hpp:83-97).
+    std::vector<int> comp(d->num_beams > 0 ? d->num_beams : 0);
+    for (int e = 0; e < d->num_beams; ++e) comp[e] = e;
+    auto find = [&](int e) {
+        while (comp[e] != e) e = comp[e] = comp[comp[e]];
+        return e;
+    };
+    {
+        std::vector<int> node_elem(nn, -1);
+        for (int e = 0; e < d->num_beams; ++e) {
+            const int n0 = d->beam_node_offsets[e], n1 = d->beam_node_offsets[e + 1];
+            if (n1 - n0 < 2) return fail(err, KYN_ERR_INVALID, "beam needs >= 2 nodes, >= 1 qp, >= 1 section");
+            for (int k = n0; k < n1; ++k) {
+                const int id = d->beam_node_ids[k];
+                if (id < 0 || id >= nn) return fail(err, KYN_ERR_INVALID, "beam node id out of range");
+                for (int k2 = n0; k2 < k; ++k2)
+                    if (d->beam_node_ids[k2] == id)
+                        return fail(err, KYN_ERR_INVALID, "node listed twice in one beam element");
+                if (node_elem[id] >= 0) {
+                    const int a = find(node_elem[id]), b = find(e);
+                    if (a != b) comp[std::max(a, b)] = std::min(a, b);
+                } else {
+                    node_elem[id] = e;
+                }
+            }
+        }
+    }
+    std::vector<int> comp_index(d->num_beams > 0 ? d->num_beams : 0, -1);
+    std::vector<std::vector<int>> comp_elems;
     for (int e = 0; e < d->num_beams; ++e) {
-        HostBeam& B = M.beams[e];
-        const int n0 = d->beam_node_offsets[e], n1 = d->beam_node_offsets[e + 1];
-        const int s0 = d->beam_section_offsets[e], s1 = d->beam_section_offsets[e + 1];
-        const int q0 = d->beam_qp_offsets[e], q1 = d->beam_qp_offsets[e + 1];
-        B.N = n1 - n0;
-        B.Q = q1 - q0;
-        if (B.N < 2 || B.Q < 1 || s1 - s0 < 1)
-            return fail(err, KYN_ERR_INVALID, "beam needs >= 2 nodes, >= 1 qp, >= 1 section");
+        const int r = find(e);
+        if (comp_index[r] < 0) {
+            comp_index[r] = static_cast<int>(comp_elems.size());
+            comp_elems.emplace_back();
+        }
+        comp_elems[comp_index[r]].push_back(e);
+    }
+    if (comp_elems.size() > static_cast<size_t>(kMaxClusterBeams))
+        return fail(err, KYN_ERR_UNSUPPORTED, "more than 8 beams in one model");
+    M.num_elements = d->num_beams > 0 ? d->num_beams : 0;
+    M.elem_row.assign(M.num_elements + 1, 0);
+    for (int e = 0; e < M.num_elements; ++e)
+        M.elem_row[e + 1] = M.elem_row[e] + d->beam_node_offsets[e + 1] - d->beam_node_offsets[e];
+    M.beams.resize(comp_elems.size());
+
+    for (size_t ci = 0; ci < comp_elems.size(); ++ci) {
+        HostBeam& B = M.beams[ci];
+        // local nodes in order of first appearance, element by element
+        int qtot = 0;
+        for (int e : comp_elems[ci]) {
+            const int n0 = d->beam_node_offsets[e], n1 = d->beam_node_offsets[e + 1];
+            std::vector<int> loc;
+            for (int k = n0; k < n1; ++k) {
+                const int id = d->beam_node_ids[k];
+                if (M.node_beam[id] < 0) {
+                    M.node_beam[id] = static_cast<int>(ci);
+                    M.node_local[id] = static_cast<int>(B.node_ids.size());
+                    B.node_ids.push_back(id);
+                }
+                loc.push_back(M.node_local[id]);
+            }
+            B.elem_ids.push_back(e);
+            B.elem_local.push_back(loc);
+            qtot += d->beam_qp_offsets[e + 1] - d->beam_qp_offsets[e];
+        }
+        B.N = static_cast<int>(B.node_ids.size());
+        B.Q = qtot;
         if (B.N > 32 || B.Q > 64)
             return fail(err, KYN_ERR_UNSUPPORTED, "beam larger than 32 nodes or 64 qps");
-        for (int s = s0 + 1; s < s1; ++s)
-            if (!(d->section_position[s] > d->section_position[s - 1]))
-                return fail(err, KYN_ERR_INVALID, "section positions must increase");
-        B.node_ids.assign(d->beam_node_ids + n0, d->beam_node_ids + n1);
-        for (int k = 0; k < B.N; ++k) {
-            const int id = B.node_ids[k];
-            if (id < 0 || id >= nn) return fail(err, KYN_ERR_INVALID, "beam node id out of range");
-            if (M.node_beam[id] != -1)
-                return fail(err, KYN_ERR_UNSUPPORTED,
-                            "node shared between beam elements (multi-element beams)");
-            M.node_beam[id] = e;
-            M.node_local[id] = k;
-        }
         const int N = B.N, Q = B.Q;
         const SlabLayout L = make_slab_layout(N, Q);
         B.slab.assign(L.total, 0.);
         double* S = B.slab.data();
-
-        // shape functions on node locations xi = 2 s - 1 (populate_element_views.hpp:45-78)
-        std::vector<double> node_xi(N), val, der;
-        for (int k = 0; k < N; ++k) node_xi[k] = 2. * d->node_s[B.node_ids[k]] - 1.;
-        for (int a = 0; a < N; ++a)
-            for (int b = a + 1; b < N; ++b)
-                if (node_xi[a] == node_xi[b])
-                    return fail(err, KYN_ERR_INVALID, "two beam nodes share an element location");
-        std::vector<double> sec_xi(s1 - s0);
-        for (int s = s0; s < s1; ++s) sec_xi[s - s0] = 2. * d->section_position[s] - 1.;
-        for (int q = 0; q < Q; ++q) {
-            const double xi = d->qp_xi[q0 + q];
-            lagrange_basis(xi, node_xi, val, der);
-            for (int k = 0; k < N; ++k) {
-                S[L.phi + q * N + k] = val[k];
-                S[L.dphi + q * N + k] = der[k];
-            }
-            // sections: linear interpolation in xi, clamped at the ends
-            // (populate_element_views.hpp:90-141, interpolation.hpp LinearInterpWeights)
-            std::vector<double> wsec(sec_xi.size(), 0.);
-            const auto lo = std::lower_bound(sec_xi.begin(), sec_xi.end(), xi);
-            if (lo == sec_xi.begin()) {
-                wsec.front() = 1.;
-            } else if (lo == sec_xi.end()) {
-                wsec.back() = 1.;
-            } else {
-                const size_t idx = static_cast<size_t>(lo - sec_xi.begin());
-                const double wu = (xi - sec_xi[idx - 1]) / (sec_xi[idx] - sec_xi[idx - 1]);
-                wsec[idx - 1] = 1. - wu;
-                wsec[idx] = wu;
-            }
-            for (int k = 0; k < 36; ++k) {
-                double m = 0., c = 0.;
-                for (size_t s = 0; s < sec_xi.size(); ++s) {
-                    m += d->section_mass[(s0 + s) * 36 + k] * wsec[s];
-                    c += d->section_stiffness[(s0 + s) * 36 + k] * wsec[s];
-                }
-                S[L.mstar + q * 36 + k] = m;
-                S[L.cstar + q * 36 + k] = c;
-            }
-            // reference rotation: normalised interpolated node orientation
-            // (interpolation_operations.hpp InterpQuaternion)
-            double r[4] = {0., 0., 0., 0.};
-            double xp[3] = {0., 0., 0.};
-            for (int k = 0; k < N; ++k) {
-                const double* x0 = d->node_x0 + B.node_ids[k] * 7;
-                for (int c = 0; c < 4; ++c) r[c] += x0[3 + c] * val[k];
-                for (int c = 0; c < 3; ++c) xp[c] += x0[c] * der[k];
-            }
-            const double rl = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3]);
-            if (rl == 0.) {
-                S[L.r0 + q * 4] = 1.;
-            } else {
-                for (int c = 0; c < 4; ++c) S[L.r0 + q * 4 + c] = r[c] / rl;
-            }
-            // Jacobian |dx0/dxi| and unit tangent (calculate_jacobian.hpp:36-76)
-            const double J = std::sqrt(xp[0] * xp[0] + xp[1] * xp[1] + xp[2] * xp[2]);
-            if (!(J > 0.)) return fail(err, KYN_ERR_INVALID, "degenerate beam reference line");
-            for (int c = 0; c < 3; ++c) S[L.x0p + q * 3 + c] = xp[c] / J;
-            const double w = d->qp_weight[q0 + q];
-            for (int k = 0; k < N; ++k) S[L.dphiJ + q * N + k] = S[L.dphi + q * N + k] / J;
-            S[L.qpw + q * 4 + 0] = w;
-            S[L.qpw + q * 4 + 1] = J;
-            S[L.qpw + q * 4 + 2] = w * J;
-            S[L.qpw + q * 4 + 3] = w / J;
+        int qo = 0;   // first quadrature point of the element in the component
+        for (size_t ei = 0; ei < comp_elems[ci].size(); ++ei) {
+            const int e = comp_elems[ci][ei];
+            const std::vector<int>& loc = B.elem_local[ei];
+            const int s0 = d->beam_section_offsets[e], s1 = d->beam_section_offsets[e + 1];
+            const int q0 = d->beam_qp_offsets[e], q1 = d->beam_qp_offsets[e + 1];
+            const int NE = static_cast<int>(loc.size()), QE = q1 - q0;
+            if (QE < 1 || s1 - s0 < 1)
+                return fail(err, KYN_ERR_INVALID, "beam needs >= 2 nodes, >= 1 qp, >= 1 section");
+            for (int s = s0 + 1; s < s1; ++s)
+                if (!(d->section_position[s] > d->section_position[s - 1]))
+                    return fail(err, KYN_ERR_INVALID, "section positions must increase");
+            std::vector<int> enode(NE);
+            for (int k = 0; k < NE; ++k) enode[k] = B.node_ids[loc[k]];
+            if (fill_element_qps(d, e, enode, loc, N, qo, L, S, err) != KYN_OK) return KYN_ERR_INVALID;
+            qo += QE;
         }
         init_node_state(d, B, L, S);
     }
@@ -402,14 +480,18 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
         cols.clear();
         if (row < M.nsys) {
             const int node = row / 6;
+            // own block first (compute_system_row_entries.hpp starts every row
+            // with it), then the other nodes of every element holding the node
+            for (int c = 0; c < 6; ++c) cols.push_back(M.fmap[node] + c);
             if (M.node_beam[node] >= 0 && !M.beams[M.node_beam[node]].lumped) {
                 const HostBeam& B = M.beams[M.node_beam[node]];
-                for (int k = 0; k < B.N; ++k)
-                    for (int c = 0; c < 6; ++c) cols.push_back(M.fmap[B.node_ids[k]] + c);
-            } else {
-                // a node in no element still holds its own diagonal block
-                // (compute_system_row_entries.hpp starts every row with it)
-                for (int c = 0; c < 6; ++c) cols.push_back(M.fmap[node] + c);
+                const int ln = M.node_local[node];
+                for (const auto& loc : B.elem_local) {
+                    if (std::find(loc.begin(), loc.end(), ln) == loc.end()) continue;
+                    for (int k : loc)
+                        if (k != ln)
+                            for (int c = 0; c < 6; ++c) cols.push_back(M.fmap[B.node_ids[k]] + c);
+                }
             }
             // a spring adds its other node's columns once per spring, also where
             // another element already added them (compute_system_col_inds.hpp:65-79)

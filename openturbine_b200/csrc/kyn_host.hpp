@@ -16,9 +16,13 @@
 
 namespace kyn {
 
+// One CTA's system: a beam element, or several elements sharing nodes (a
+// multi-element beam), or the nodes of a model without beam elements.
 struct HostBeam {
     int N = 0, Q = 0, nc = 0;
-    std::vector<int> node_ids;        // global node ids in element order
+    std::vector<int> node_ids;        // global node ids (local node order)
+    std::vector<int> elem_ids;        // beam elements in this system (model order)
+    std::vector<std::vector<int>> elem_local;  // local index of each element node
     std::vector<double> slab;         // SlabLayout-ordered doubles
     int con_node[kMaxBeamConstraints] = {};
     int con_type[kMaxBeamConstraints] = {};
@@ -32,6 +36,8 @@ struct HostBeam {
 
 struct HostModel {
     int num_nodes = 0;
+    int num_elements = 0;                     // beam elements of the description
+    std::vector<int> elem_row;                // first node_FX row of each element
     int num_constraints = 0;
     std::vector<HostBeam> beams;
     std::vector<int> node_beam, node_local;   // node -> (beam, local index)

@@ -338,9 +338,11 @@ def test_errors(ctx):
         ctx.step([12345], W.cantilever_params())
     st, it = ctx.step([], W.cantilever_params())
     assert len(st) == 0
-    # a node shared by two beam elements is outside this path
+    # a revolute joint (constraint type 4) is outside this path
+    from openturbine_b200.model import Constraint
     m = W.cantilever_model()
-    m.AddBeamElement([0, 1], m.GetBeamElements()[0].sections, [[0.0, 2.0]])
+    hub = m.AddNode().SetPosition(-1., 0., 0., 1., 0., 0., 0.).Build()
+    m.constraints_.append(Constraint(len(m.constraints_), 4, (hub, 0), (0.0, 0.0, 1.0)))
     with pytest.raises(KynError) as e:
         ctx.create_model(m)
     assert e.value.code == -2

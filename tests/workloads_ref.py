@@ -258,3 +258,32 @@ def spring_mass_chain_model(number_of_masses: int = 10):
     m.AddFixedBC(number_of_masses + 1)
     final_time = 2. * math.pi * math.sqrt(1. / 10.)
     return m, StepParameters(True, 6, final_time / 1000., 0.0)
+
+
+def two_element_cantilever_model():
+    """A 10 m cantilever of two quadratic elements sharing the middle node C:
+    element 1 = (A, B, C) along +x, element 2 = (E, D, C) parametrised from the
+    tip back to C (Node::s is one value per node, so the shared node sits at
+    s = 1 of both elements).  Composite section of test_cantilever_beam.cpp,
+    4 Gauss points per element, FixedBC at A; the tip load goes on E
+    (element 2, local node 0)."""
+    m = Model()
+    m.SetGravity(0., 0., 0.)
+    xs = [0., 2.5, 5., 7.5, 10.]
+    ss = [0., 0.5, 1., 0.5, 0.]
+    ids = [m.AddNode().SetElemLocation(s).SetPosition(x, 0., 0., 1., 0., 0., 0.).Build()
+           for x, s in zip(xs, ss)]
+    secs = [BeamSection(0., COMPOSITE_MASS, COMPOSITE_STIFF),
+            BeamSection(1., COMPOSITE_MASS, COMPOSITE_STIFF)]
+    g4 = [[x, w] for x, w in zip(*np.polynomial.legendre.leggauss(4))]
+    m.AddBeamElement([ids[0], ids[1], ids[2]], secs, g4)
+    m.AddBeamElement([ids[4], ids[3], ids[2]], secs, g4)
+    m.AddFixedBC(ids[0])
+    return m, StepParameters(True, 5, 0.005, 0.0)
+
+
+def two_element_cantilever_loads(step: int) -> np.ndarray:
+    """node_FX rows per element node (element 1: A, B, C; element 2: E, D, C)."""
+    fx = np.zeros((6, 6))
+    fx[3, 2] = 100. * math.sin(10.0 * 0.005 * (step + 1))
+    return fx
