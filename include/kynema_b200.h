@@ -210,6 +210,15 @@ KYN_API int kyn_model_create(kyn_ctx* ctx, const kyn_model_desc* desc);
 KYN_API int kyn_model_destroy(kyn_ctx* ctx, int model_id);
 KYN_API int kyn_model_info_get(kyn_ctx* ctx, int model_id, kyn_model_info* info);
 
+/* A new model that is a copy of an existing one in its current state (same
+ * description, node state, multipliers and loads; its own device memory,
+ * counted against the HBM budget).  No counterpart in the reference: a server
+ * that admits many copies of the same description keeps one resident template
+ * and clones it, which costs a device-to-device copy instead of a rebuild of
+ * the shape tables, sections and CRS graph.  Returns the new id or a negative
+ * KYN_ERR_* code. */
+KYN_API int kyn_model_clone(kyn_ctx* ctx, int model_id);
+
 /* Replaces writes of Beams::node_FX (tests/regression_tests/regression/
  * test_cantilever_beam.cpp:105-107) or State::f. */
 KYN_API int kyn_model_set_loads(kyn_ctx* ctx, int model_id, int which, const double* values);

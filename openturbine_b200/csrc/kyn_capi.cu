@@ -304,6 +304,41 @@ void prepare_model(DevModel* m) {
 
 int nt_index(int nt) { return nt == 128 ? 0 : nt == 256 ? 1 : 2; }
 
+// Per-call device buffers grow by doubling from a floor sized for a serving
+// batch, stream-ordered on the context stream (no device synchronisation: work
+// already queued on the stream still reads the old buffer before it is freed).
+template <typename T>
+int grow_device(kyn_ctx* c, T*& p, size_t& cap, size_t need, size_t floor) {
+    if (cap >= need && p) return KYN_OK;
+    size_t nc = std::max(cap, floor);
+    while (nc < need) nc *= 2;
+    if (p) KYN_CUDA(c, cudaFreeAsync(p, c->stream));
+    p = nullptr;
+    KYN_CUDA(c, cudaMallocAsync(reinterpret_cast<void**>(&p), sizeof(T) * nc, c->stream));
+    cap = nc;
+    return KYN_OK;
+}
+
+// Pinned host staging grows the same way; cudaMallocHost is slow, so growth
+// events are kept rare.  Copies from the old buffer are finished first.
+template <typename T>
+int grow_pinned(kyn_ctx* c, T*& p, size_t& cap, size_t need, size_t floor) {
+    if (cap >= need && p) return KYN_OK;
+    size_t nc = std::max(cap, floor);
+    while (nc < need) nc *= 2;
+    if (p) {
+        KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+        KYN_CUDA(c, cudaFreeHost(p));
+    }
+    p = nullptr;
+    KYN_CUDA(c, cudaMallocHost(reinterpret_cast<void**>(&p), sizeof(T) * nc));
+    cap = nc;
+    return KYN_OK;
+}
+
+constexpr size_t kPoolBeams = 16384;     // growth floor of the per-beam buffers
+constexpr size_t kPoolRows = 16384 * 24; // growth floor of the per-node-row buffers
+
 // Builds (or reuses) the launch plan for this id list.
 int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
     if (c->plan && c->plan->record == c->record && c->plan->precision == precision &&
@@ -360,12 +395,9 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
         KYN_CUDA(c, cudaEventSynchronize(c->plan_uploaded));
         c->plan_upload_pending = false;
     }
-    if (c->pool_hkbeams_cap < nbeams) {
-        if (c->pool_hkbeams) KYN_CUDA(c, cudaFreeHost(c->pool_hkbeams));
-        c->pool_hkbeams = nullptr;
-        const size_t cap = std::max<size_t>(nbeams + nbeams / 2, 256);
-        KYN_CUDA(c, cudaMallocHost(&c->pool_hkbeams, sizeof(KBeam) * cap));
-        c->pool_hkbeams_cap = cap;
+    {
+        const int rc = grow_pinned(c, c->pool_hkbeams, c->pool_hkbeams_cap, nbeams, kPoolBeams);
+        if (rc != KYN_OK) return rc;
     }
     KBeam* kb = c->pool_hkbeams;
     size_t nk = 0;
@@ -395,22 +427,22 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
         }
     }
     plan->nbeams = static_cast<int>(nk);
-    if (c->pool_kbeams_cap < nk) {
-        if (c->pool_kbeams) KYN_CUDA(c, cudaFree(c->pool_kbeams));
-        c->pool_kbeams = nullptr;
-        const size_t cap = std::max<size_t>(nk + nk / 2, 256);
-        KYN_CUDA(c, cudaMalloc(&c->pool_kbeams, sizeof(KBeam) * cap));
-        c->pool_kbeams_cap = cap;
-    }
-    if (c->pool_status_cap < static_cast<size_t>(n)) {
-        if (c->pool_status) KYN_CUDA(c, cudaFree(c->pool_status));
-        if (c->pool_hstatus) KYN_CUDA(c, cudaFreeHost(c->pool_hstatus));
-        c->pool_status = nullptr;
-        c->pool_hstatus = nullptr;
-        const size_t cap = std::max<size_t>(n + n / 2, 256);
-        KYN_CUDA(c, cudaMalloc(&c->pool_status, sizeof(int) * 2 * cap));
-        KYN_CUDA(c, cudaMallocHost(&c->pool_hstatus, sizeof(int) * 2 * cap));
-        c->pool_status_cap = cap;
+    {
+        int rc = grow_device(c, c->pool_kbeams, c->pool_kbeams_cap, nk, kPoolBeams);
+        if (rc != KYN_OK) return rc;
+        if (c->pool_status_cap < static_cast<size_t>(n) || !c->pool_status) {
+            // status and iteration counts share one buffer: [cap] + [cap]
+            size_t cap = std::max(c->pool_status_cap, kPoolBeams);
+            while (cap < static_cast<size_t>(n)) cap *= 2;
+            size_t dcap = 0, hcap = 0;
+            if (c->pool_status) KYN_CUDA(c, cudaFreeAsync(c->pool_status, c->stream));
+            c->pool_status = nullptr;
+            rc = grow_device(c, c->pool_status, dcap, 2 * cap, 2 * cap);
+            if (rc != KYN_OK) return rc;
+            rc = grow_pinned(c, c->pool_hstatus, hcap, 2 * cap, 2 * cap);
+            if (rc != KYN_OK) return rc;
+            c->pool_status_cap = cap;
+        }
     }
     plan->d_kbeams = c->pool_kbeams;
     plan->d_status = c->pool_status;
@@ -615,17 +647,11 @@ int get_xfer(kyn_ctx* c, const int* ids, int n, int kind, XferPlan** out) {
     if (xp->width == 0) xp->width = 6;
     xp->total = off;
     xp->nbeams = static_cast<int>(beams.size());
-    if (xp->beams_cap < beams.size()) {
-        if (xp->d_beams) KYN_CUDA(c, cudaFree(xp->d_beams));
-        xp->d_beams = nullptr;
-        xp->beams_cap = std::max<size_t>(beams.size() + beams.size() / 2, 64);
-        KYN_CUDA(c, cudaMalloc(&xp->d_beams, sizeof(XferBeam) * xp->beams_cap));
-    }
-    if (xp->map_cap < map.size()) {
-        if (xp->d_map) KYN_CUDA(c, cudaFree(xp->d_map));
-        xp->d_map = nullptr;
-        xp->map_cap = std::max<size_t>(map.size() + map.size() / 2, 256);
-        KYN_CUDA(c, cudaMalloc(&xp->d_map, sizeof(int) * xp->map_cap));
+    {
+        int rc = grow_device(c, xp->d_beams, xp->beams_cap, beams.size(), kPoolBeams);
+        if (rc != KYN_OK) return rc;
+        rc = grow_device(c, xp->d_map, xp->map_cap, map.size(), kPoolRows);
+        if (rc != KYN_OK) return rc;
     }
     // pageable sources: staged before the calls return; stream order does the rest
     KYN_CUDA(c, cudaMemcpyAsync(xp->d_beams, beams.data(), sizeof(XferBeam) * beams.size(),
@@ -638,15 +664,8 @@ int get_xfer(kyn_ctx* c, const int* ids, int n, int kind, XferPlan** out) {
 }
 
 int ensure_stage(kyn_ctx* c, long long doubles) {
-    if (c->d_stage_len >= static_cast<size_t>(doubles)) return KYN_OK;
-    if (c->d_stage) {
-        KYN_CUDA(c, cudaStreamSynchronize(c->stream));
-        cudaFree(c->d_stage);
-        c->d_stage = nullptr;
-    }
-    KYN_CUDA(c, cudaMalloc(&c->d_stage, sizeof(double) * std::max<long long>(1, doubles)));
-    c->d_stage_len = static_cast<size_t>(std::max<long long>(1, doubles));
-    return KYN_OK;
+    return grow_device(c, c->d_stage, c->d_stage_len, static_cast<size_t>(std::max<long long>(1, doubles)),
+                       kPoolRows * 6);
 }
 
 }  // namespace
@@ -1240,15 +1259,13 @@ extern "C" int kyn_set_prescribed_batch(kyn_ctx* c, const int* ids, int n, const
                 vi.push_back(row);
             }
         }
-        if (c->presc_cap < t.size()) {
-            if (c->presc_targets) KYN_CUDA(c, cudaFree(c->presc_targets));
-            if (c->presc_vidx) KYN_CUDA(c, cudaFree(c->presc_vidx));
-            c->presc_targets = nullptr;
-            c->presc_vidx = nullptr;
-            const size_t cap = std::max<size_t>(t.size() + t.size() / 2, 64);
-            KYN_CUDA(c, cudaMalloc(&c->presc_targets, sizeof(double*) * cap));
-            KYN_CUDA(c, cudaMalloc(&c->presc_vidx, sizeof(int) * cap));
-            c->presc_cap = cap;
+        if (c->presc_cap < t.size() || !c->presc_targets) {
+            size_t tcap = c->presc_cap, vcap = c->presc_cap;
+            int rc = grow_device(c, c->presc_targets, tcap, t.size(), kPoolBeams);
+            if (rc != KYN_OK) return rc;
+            rc = grow_device(c, c->presc_vidx, vcap, t.size(), kPoolBeams);
+            if (rc != KYN_OK) return rc;
+            c->presc_cap = std::min(tcap, vcap);
         }
         if (!t.empty()) {
             KYN_CUDA(c, cudaMemcpyAsync(c->presc_targets, t.data(), sizeof(double*) * t.size(),
@@ -1431,6 +1448,20 @@ int clone_model(kyn_ctx* c, int id) {
         m->d_slab.push_back(p);
     }
     KYN_CUDA(c, cudaMallocAsync(&m->d_conv, kMaxNewtonIters * sizeof(double), c->stream));
+    KYN_CUDA(c, cudaMemcpyAsync(m->d_conv, src->d_conv, kMaxNewtonIters * sizeof(double),
+                                cudaMemcpyDeviceToDevice, c->stream));
+    if (src->d_dump) {  // the recorded-system buffer, when the source has one
+        m->dump_off = src->dump_off;
+        size_t tot = 0;
+        for (size_t bi = 0; bi < m->host.beams.size(); ++bi) {
+            const size_t nl = 6 * m->host.beams[bi].N + 6 * m->host.beams[bi].nc;
+            tot += nl * nl + 2 * nl;
+        }
+        KYN_CUDA(c, cudaMallocAsync(&m->d_dump, tot * sizeof(double), c->stream));
+        KYN_CUDA(c, cudaMemsetAsync(m->d_dump, 0, tot * sizeof(double), c->stream));
+    }
+    m->last_status = src->last_status;
+    m->last_iters = src->last_iters;
     m->bytes = bytes;
     c->used += bytes;
     prepare_model(m.get());
@@ -1440,6 +1471,12 @@ int clone_model(kyn_ctx* c, int id) {
 }
 
 }  // namespace
+
+extern "C" int kyn_model_clone(kyn_ctx* c, int model_id) {
+    if (!c) return KYN_ERR_INVALID;
+    KYN_CUDA(c, cudaSetDevice(c->device));
+    return clone_model(c, model_id);
+}
 
 extern "C" int kyn_autotune(kyn_ctx* c, const int* ids, int n, const kyn_step_params* p) {
     if (!c || !p || n < 0 || (n > 0 && !ids)) return KYN_ERR_INVALID;

@@ -57,6 +57,7 @@ def load_library():
     L.kyn_ctx_set_option.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64]
     L.kyn_model_create.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
     L.kyn_model_destroy.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.kyn_model_clone.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.kyn_model_info_get.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
     L.kyn_model_set_loads.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp]
     L.kyn_model_set_prescribed.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp]
@@ -137,6 +138,13 @@ class Context:
         self._check(self.lib.kyn_model_info_get(self.h, mid, ctypes.byref(info)))
         self._info[mid] = info
         return mid
+
+    def clone_model(self, mid: int) -> int:
+        """A copy of model `mid` in its current state (kyn_model_clone)."""
+        nid = self._check(self.lib.kyn_model_clone(self.h, mid))
+        self._packed[nid] = self._packed.get(mid)
+        self._info[nid] = self._info[mid]
+        return nid
 
     def destroy_model(self, mid: int) -> None:
         self._check(self.lib.kyn_model_destroy(self.h, mid))

@@ -18,6 +18,7 @@ both per step, src/interfaces/turbine/turbine_interface.cpp:117-150).
 """
 from __future__ import annotations
 
+import gc
 import math
 import time
 from dataclasses import dataclass, field
@@ -62,9 +63,16 @@ class StepServer:
     The active set is kept as arrays (model ids, load parameters, step
     counters, node-row offsets), so building one iteration's loads and
     bookkeeping costs a few vector operations, not a pass over Python
-    objects; only admitted and finishing requests are touched one by one."""
+    objects; only admitted and finishing requests are touched one by one.
 
-    def __init__(self, ctx: Context, params, h: float = 0.01, max_active: int | None = None):
+    Requests that carry the same (pooled) model description share one
+    resident template model: the first one builds it, every admission clones
+    it on the device (kyn_model_clone), so admitting costs a device copy, not
+    a rebuild of shape tables, sections and CRS graph.  Templates count
+    against the HBM budget and are never stepped."""
+
+    def __init__(self, ctx: Context, params, h: float = 0.01, max_active: int | None = None,
+                 reserve_rows: int = 16384 * 22):
         self.ctx = ctx
         self.params = params
         self.h = h
@@ -80,7 +88,12 @@ class StepServer:
         # host time per iteration part (ms, summed): loads and motion in, step
         # submission, admission while the step runs, wait for results, retire
         self.host_ms = {"inputs": 0.0, "submit": 0.0, "admit": 0.0, "wait": 0.0, "retire": 0.0}
-        self._pinned = None
+        # pinned staging of the per-iteration loads, sized up front: growing it
+        # (a page-locked allocation) inside the loop stalls an iteration
+        import torch
+        self._pinned = torch.zeros((max(int(reserve_rows), 1024), 6), dtype=torch.float64).pin_memory()
+        self._templates: dict = {}      # id(packed description) -> resident template model
+        self._template_refs: list = []  # keeps those descriptions alive (their ids stay unique)
         self._ids = np.zeros(0, dtype=np.int32)
         self._rotor = np.zeros(0, dtype=bool)
         self._amp = np.zeros(0)
@@ -103,13 +116,23 @@ class StepServer:
                 keep.append(r)
                 continue
             try:
-                r.model_id = self.ctx.create_model(r.packed)
+                r.model_id = self._new_model(r.packed)
             except KynError as e:
-                if e.code == KYN_ERR_BUDGET:  # wait for memory to free up
-                    blocked = True
+                if e.code != KYN_ERR_BUDGET:
+                    raise
+                # the templates are a cache: give their memory back and build
+                # this model directly before waiting for active models to leave
+                try:
+                    if not self._templates:
+                        raise
+                    self._drop_templates()
+                    r.model_id = self.ctx.create_model(r.packed)
+                except KynError as e2:
+                    if e2.code != KYN_ERR_BUDGET:
+                        raise
+                    blocked = True  # wait for memory to free up
                     keep.append(r)
                     continue
-                raise
             r.admitted_at = now
             new.append(r)
         self.queue = keep
@@ -126,6 +149,22 @@ class StepServer:
             self._roots = np.concatenate(
                 [self._roots, np.stack([r.roots if r.roots is not None else np.zeros((3, 3)) for r in new])])
 
+    def _new_model(self, packed) -> int:
+        """First request of a description builds a resident template; every
+        request then gets a device copy of it."""
+        tid = self._templates.get(id(packed))
+        if tid is None:
+            tid = self.ctx.create_model(packed)
+            self._templates[id(packed)] = tid
+            self._template_refs.append(packed)
+        return self.ctx.clone_model(tid)
+
+    def _drop_templates(self) -> None:
+        for tid in self._templates.values():
+            self.ctx.destroy_model(tid)
+        self._templates.clear()
+        self._template_refs.clear()
+
     def _remove(self, idx: np.ndarray) -> None:
         keep = np.ones(len(self.active), dtype=bool)
         keep[idx] = False
@@ -137,9 +176,9 @@ class StepServer:
     def _loads(self, n: int):
         nodes = self._nodes[:n]
         rows = int(nodes.sum())
-        if self._pinned is None or self._pinned.shape[0] < rows:
+        if self._pinned.shape[0] < rows:
             import torch
-            self._pinned = torch.zeros((max(rows, 1024) * 2, 6), dtype=torch.float64).pin_memory()
+            self._pinned = torch.zeros((2 * rows, 6), dtype=torch.float64).pin_memory()
         fx = self._pinned.numpy()[:rows]
         fx[:] = 0.0
         t = self.h * (self._done[:n] + 1)
@@ -210,6 +249,10 @@ class StepServer:
     def run(self, until_s: float, drain: bool = False) -> None:
         """Serve in real time for until_s seconds (requests become visible at
         their arrival times); with drain, then finish every admitted model."""
+        # The request objects and model descriptions made before serving stay
+        # alive throughout; keep the cyclic collector from walking them inside an
+        # iteration (a full collection over them stalls the loop).
+        gc.freeze()
         t_start = time.perf_counter()
         now = lambda: time.perf_counter() - t_start  # noqa: E731
         while now() < until_s:

@@ -88,3 +88,29 @@ def test_predictor_corrector_with_state_copy(ctx):
     ctx.step([twin], p)
     for f in ("q", "v", "vd", "a"):
         np.testing.assert_array_equal(ctx.state(a, f), ctx.state(twin, f))
+
+
+def test_clone_continues_like_the_original(ctx):
+    """kyn_model_clone of a model part-way through a run: the clone has the
+    original's state and, stepped with the same loads, stays identical to it
+    bit for bit; the source is unaffected and both can be destroyed."""
+    from openturbine_b200 import workloads as W
+    d = W.draw_batch(1, first_id=4242)[0]
+    p = W.batch_params()
+    src = ctx.create_model(W.batch_cantilever_model(d).pack())
+    for k in range(3):
+        ctx.set_node_fx(src, W.node_fx_for(d, W.tip_loads([d], k)[0]))
+        ctx.step([src], p)
+    cl = ctx.clone_model(src)
+    for f in ("q", "v", "vd", "a", "x", "lambda"):
+        np.testing.assert_array_equal(ctx.state(cl, f), ctx.state(src, f))
+    for k in range(3, 8):
+        fx = W.node_fx_for(d, W.tip_loads([d], k)[0])
+        ctx.set_node_fx(src, fx)
+        ctx.set_node_fx(cl, fx)
+        st, it = ctx.step([src, cl], p)
+        assert st[0] == st[1] and it[0] == it[1]
+    for f in ("q", "v", "vd", "a", "x", "lambda"):
+        np.testing.assert_array_equal(ctx.state(cl, f), ctx.state(src, f))
+    ctx.destroy_model(cl)
+    ctx.destroy_model(src)
