@@ -109,6 +109,20 @@ struct Node {  // src/model/node.hpp:35-60
         v = {vel[0] + (w[1] * r[2] - w[2] * r[1]), vel[1] + (w[2] * r[0] - w[0] * r[2]),
              vel[2] + (w[0] * r[1] - w[1] * r[0]), w[0], w[1], w[2]};
     }
+    // src/model/node.hpp:233-262: rigid-body acceleration about a point
+    void SetAccelerationAboutPoint(const std::array<double, 6>& acc, const std::array<double, 3>& omega,
+                                   const std::array<double, 3>& p) {
+        const auto dp = DisplacedPosition();
+        const std::array<double, 3> r{dp[0] - p[0], dp[1] - p[1], dp[2] - p[2]};
+        auto cross = [](const std::array<double, 3>& a, const std::array<double, 3>& b) {
+            return std::array<double, 3>{a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2],
+                                         a[0] * b[1] - a[1] * b[0]};
+        };
+        const auto ar = cross({acc[3], acc[4], acc[5]}, r);
+        const auto wwr = cross(omega, cross(omega, r));
+        vd = {acc[0] + ar[0] + wwr[0], acc[1] + ar[1] + wwr[1], acc[2] + ar[2] + wwr[2],
+              acc[3], acc[4], acc[5]};
+    }
 };
 
 class NodeBuilder {  // src/model/node.hpp:284-538
@@ -264,6 +278,10 @@ public:
     }
     void SetBeamVelocityAboutPoint(size_t e, const std::array<double, 6>& v, const std::array<double, 3>& p) {
         for (auto n : beams_[e].nodes) nodes_[n].SetVelocityAboutPoint(v, p);
+    }
+    void SetBeamAccelerationAboutPoint(size_t e, const std::array<double, 6>& a,
+                                       const std::array<double, 3>& omega, const std::array<double, 3>& p) {
+        for (auto n : beams_[e].nodes) nodes_[n].SetAccelerationAboutPoint(a, omega, p);
     }
     // src/model/model.hpp:305-311 AddMassElement: 6x6 mass (material frame) at a node
     size_t AddMassElement(size_t node, const std::array<std::array<double, 6>, 6>& mass) {

@@ -1,0 +1,579 @@
+// kynema_b200_interfaces.hpp -- the blade interface of Kynema on the B200 path.
+//
+// A code that couples a wind-turbine blade to an aerodynamics or CFD solver
+// uses the reference's BladeInterface (src/interfaces/blade/blade_interface.hpp):
+// it describes the blade by a reference axis, twist and 6x6 sections
+// (BladeInterfaceBuilder / components::BeamBuilder), writes nodal loads into
+// Blade().nodes[i].loads, calls Step(), and reads the nodes' position,
+// displacement, velocity and acceleration back.  This header keeps that
+// surface; the blade becomes one beam element of the requested order built
+// through the C++ shim (kynema_b200.hpp), and each Step() is one kyn_step of
+// the device model.  NetCDF and YAML output of the reference are not part of
+// this path; SetOutputFile only records the path.
+#pragma once
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <limits>
+#include <memory>
+#include <numbers>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "kynema_b200.hpp"
+
+namespace kynema_b200::interfaces {
+
+// ---- geometry helpers (src/math/interpolation.hpp, least_squares_fit.hpp,
+//      project_points_to_target_polynomial.hpp, quaternion_operations.hpp,
+//      matrix_operations.hpp) ----------------------------------------------------------
+namespace math {
+
+using M3 = std::array<std::array<double, 3>, 3>;
+using M6 = std::array<std::array<double, 6>, 6>;
+
+// P_n(x) by the three-term recurrence
+inline double Legendre(size_t n, double x) {
+    if (n == 0) return 1.;
+    double p2 = 1., p1 = x, p = x;
+    for (size_t i = 2; i <= n; ++i) {
+        const double di = static_cast<double>(i);
+        p = ((2. * di - 1.) * x * p1 - (di - 1.) * p2) / di;
+        p2 = p1;
+        p1 = p;
+    }
+    return p;
+}
+
+// Gauss-Lobatto-Legendre points of a polynomial order, ascending: the end
+// points and the roots of (1 - x^2) P'_order, found by Newton's method from the
+// Chebyshev-Lobatto points (interpolation.hpp:169-230).
+inline std::vector<double> GenerateGLLPoints(size_t order) {
+    if (order < 1) throw std::invalid_argument("polynomial order must be >= 1");
+    const size_t n = order + 1;
+    std::vector<double> x(n, 0.);
+    x.front() = -1.;
+    x.back() = 1.;
+    for (size_t i = 1; i < order; ++i) {
+        double xi = -std::cos(static_cast<double>(i) * std::numbers::pi / static_cast<double>(order));
+        bool done = false;
+        for (int it = 0; it < 1000 && !done; ++it) {
+            const double old = xi;
+            const double pn = Legendre(n - 1, xi), pm = Legendre(n - 2, xi);
+            xi -= (xi * pn - pm) / (static_cast<double>(n) * pn);
+            done = std::abs(xi - old) <= std::numeric_limits<double>::epsilon();
+        }
+        if (!done) throw std::runtime_error("GLL point iteration did not converge");
+        x[i] = xi;
+    }
+    return x;
+}
+
+inline std::vector<double> LagrangeWeights(double x, const std::vector<double>& xs) {
+    std::vector<double> w(xs.size(), 1.);
+    for (size_t j = 0; j < xs.size(); ++j)
+        for (size_t m = 0; m < xs.size(); ++m)
+            if (m != j) w[j] *= (x - xs[m]) / (xs[j] - xs[m]);
+    return w;
+}
+
+inline std::vector<double> LagrangeDerivWeights(double x, const std::vector<double>& xs) {
+    std::vector<double> w(xs.size(), 0.);
+    for (size_t j = 0; j < xs.size(); ++j)
+        for (size_t i = 0; i < xs.size(); ++i) {
+            if (i == j) continue;
+            double p = 1. / (xs[j] - xs[i]);
+            for (size_t m = 0; m < xs.size(); ++m)
+                if (m != i && m != j) p *= (x - xs[m]) / (xs[j] - xs[m]);
+            w[j] += p;
+        }
+    return w;
+}
+
+// Linear interpolation on a sorted grid, clamped at its ends.
+inline double LinearInterp(double x, const std::vector<double>& xs, const std::vector<double>& v) {
+    if (xs.empty()) return 0.;
+    if (x <= xs.front()) return v.front();
+    if (x >= xs.back()) return v.back();
+    const size_t k = static_cast<size_t>(std::lower_bound(xs.begin(), xs.end(), x) - xs.begin());
+    const double u = (x - xs[k - 1]) / (xs[k] - xs[k - 1]);
+    return (1. - u) * v[k - 1] + u * v[k];
+}
+
+inline M3 QuaternionToRotationMatrix(const std::array<double, 4>& q) {
+    const double w = q[0], x = q[1], y = q[2], z = q[3];
+    return {{{w * w + x * x - y * y - z * z, 2. * (x * y - w * z), 2. * (x * z + w * y)},
+             {2. * (x * y + w * z), w * w - x * x + y * y - z * z, 2. * (y * z - w * x)},
+             {2. * (x * z - w * y), 2. * (y * z + w * x), w * w - x * x - y * y + z * z}}};
+}
+
+// The quaternion of a rotation matrix, from its largest diagonal combination
+// (quaternion_operations.hpp:63-120).
+inline std::array<double, 4> RotationMatrixToQuaternion(const M3& m) {
+    const double a = m[1][1] + m[2][2], b = m[1][1] - m[2][2];
+    const std::array<double, 4> vals{m[0][0] + a, m[0][0] - a, -m[0][0] + b, -m[0][0] - b};
+    const size_t k = static_cast<size_t>(std::max_element(vals.begin(), vals.end()) - vals.begin());
+    const double t = std::sqrt(vals[k] + 1.), c = 0.5 / t;
+    switch (k) {
+        case 0: return {0.5 * t, (m[2][1] - m[1][2]) * c, (m[0][2] - m[2][0]) * c, (m[1][0] - m[0][1]) * c};
+        case 1: return {(m[2][1] - m[1][2]) * c, 0.5 * t, (m[0][1] + m[1][0]) * c, (m[0][2] + m[2][0]) * c};
+        case 2: return {(m[0][2] - m[2][0]) * c, (m[0][1] + m[1][0]) * c, 0.5 * t, (m[1][2] + m[2][1]) * c};
+        default: return {(m[1][0] - m[0][1]) * c, (m[0][2] + m[2][0]) * c, (m[1][2] + m[2][1]) * c, 0.5 * t};
+    }
+}
+
+inline std::array<double, 3> Unit(const std::array<double, 3>& v) {
+    const double n = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    return {v[0] / n, v[1] / n, v[2] / n};
+}
+
+// Orientation whose first axis is the tangent, turned by twist (degrees) about
+// it; the second axis lies in the plane of the tangent and y (or x when the
+// tangent is near y) (quaternion_operations.hpp:334-362).
+inline std::array<double, 4> TangentTwistToQuaternion(const std::array<double, 3>& tangent, double twist) {
+    const auto e1 = Unit(tangent);
+    std::array<double, 3> t{0., 1., 0.};
+    if (std::abs(e1[0] * t[0] + e1[1] * t[1] + e1[2] * t[2]) > 0.9) t = {1., 0., 0.};
+    const double a = e1[0] * t[0] + e1[1] * t[1] + e1[2] * t[2];
+    const auto e2 = Unit({t[0] - e1[0] * a, t[1] - e1[1] * a, t[2] - e1[2] * a});
+    const std::array<double, 3> e3{e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                                   e1[0] * e2[1] - e1[1] * e2[0]};
+    const auto q_tan = RotationMatrixToQuaternion({{{e1[0], e2[0], e3[0]},
+                                                    {e1[1], e2[1], e3[1]},
+                                                    {e1[2], e2[2], e3[2]}}});
+    const double tw = twist * std::numbers::pi / 180.;
+    const auto q_twist = RotationVectorToQuaternion({e1[0] * tw, e1[1] * tw, e1[2] * tw});
+    return QuaternionCompose(q_twist, q_tan);
+}
+
+// diag(R, R) m diag(R, R)^T
+inline M6 RotateMatrix6(const M6& m, const std::array<double, 4>& q) {
+    const auto R = QuaternionToRotationMatrix(q);
+    auto r = [&](size_t i, size_t k) {
+        return (i / 3 == k / 3) ? R[i % 3][k % 3] : 0.;
+    };
+    M6 t{}, o{};
+    for (size_t i = 0; i < 6; ++i)
+        for (size_t j = 0; j < 6; ++j)
+            for (size_t k = 0; k < 6; ++k) t[i][j] += r(i, k) * m[k][j];
+    for (size_t i = 0; i < 6; ++i)
+        for (size_t j = 0; j < 6; ++j)
+            for (size_t k = 0; k < 6; ++k) o[i][j] += t[i][k] * r(j, k);
+    return o;
+}
+
+// Trapezoidal rule on a grid mapped to [-1, 1] (src/elements/beams/beam_quadrature.hpp:11-28).
+inline std::vector<std::array<double, 2>> CreateTrapezoidalQuadrature(const std::vector<double>& grid) {
+    const size_t n = grid.size();
+    const auto [lo, hi] = std::minmax_element(grid.begin(), grid.end());
+    const double g0 = *lo, range = *hi - *lo;
+    std::vector<std::array<double, 2>> q{{-1., (grid[1] - grid[0]) / range}};
+    for (size_t i = 1; i + 1 < n; ++i)
+        q.push_back({2. * (grid[i] - g0) / range - 1., (grid[i + 1] - grid[i - 1]) / range});
+    q.push_back({1., (grid[n - 1] - grid[n - 2]) / range});
+    return q;
+}
+
+// Node coordinates of a polynomial through key points: least squares with the
+// first and last node held at the first and last key point (interior rows are
+// the normal equations), solved by Gaussian elimination with partial pivoting
+// (least_squares_fit.hpp: MapGeometricLocations, ComputeShapeFunctionValues,
+// PerformLeastSquaresFitting).
+inline std::vector<std::array<double, 3>> FitNodes(const std::vector<double>& node_xi,
+                                                   const std::vector<double>& kp_grid,
+                                                   const std::vector<std::array<double, 3>>& kp) {
+    const size_t p = node_xi.size(), n = kp.size();
+    const double g0 = kp_grid.front(), span = kp_grid.back() - kp_grid.front();
+    if (span == 0.) throw std::invalid_argument("reference axis grid has zero length");
+    std::vector<std::vector<double>> phi(p, std::vector<double>(n));   // phi[node][key point]
+    for (size_t k = 0; k < n; ++k) {
+        const auto w = LagrangeWeights(2. * (kp_grid[k] - g0) / span - 1., node_xi);
+        for (size_t i = 0; i < p; ++i) phi[i][k] = w[i];
+    }
+    std::vector<std::vector<double>> A(p, std::vector<double>(p, 0.));
+    std::vector<std::array<double, 3>> B(p, {0., 0., 0.});
+    A[0][0] = 1.;
+    A[p - 1][p - 1] = 1.;
+    B[0] = kp.front();
+    B[p - 1] = kp.back();
+    for (size_t i = 1; i + 1 < p; ++i) {
+        for (size_t j = 0; j < p; ++j) {
+            double s = 0.;
+            for (size_t k = 0; k < n; ++k) s += phi[i][k] * phi[j][k];
+            A[i][j] = s;
+        }
+        for (size_t k = 0; k < n; ++k)
+            for (int d = 0; d < 3; ++d) B[i][d] += phi[i][k] * kp[k][d];
+    }
+    for (size_t c = 0; c < p; ++c) {
+        size_t piv = c;
+        for (size_t r = c + 1; r < p; ++r)
+            if (std::abs(A[r][c]) > std::abs(A[piv][c])) piv = r;
+        std::swap(A[c], A[piv]);
+        std::swap(B[c], B[piv]);
+        for (size_t r = c + 1; r < p; ++r) {
+            const double l = A[r][c] / A[c][c];
+            for (size_t j = c; j < p; ++j) A[r][j] -= l * A[c][j];
+            for (int d = 0; d < 3; ++d) B[r][d] -= l * B[c][d];
+        }
+    }
+    std::vector<std::array<double, 3>> X(p);
+    for (size_t r = p; r-- > 0;) {
+        for (int d = 0; d < 3; ++d) {
+            double s = B[r][d];
+            for (size_t j = r + 1; j < p; ++j) s -= A[r][j] * X[j][d];
+            X[r][d] = s / A[r][r];
+        }
+    }
+    return X;
+}
+
+// Values of the order (m-1) GLL polynomial through `in` at the points of order
+// (n-1) (project_points_to_target_polynomial.hpp).
+inline std::vector<std::array<double, 3>> ProjectPoints(size_t m, size_t n,
+                                                        const std::vector<std::array<double, 3>>& in) {
+    const auto from = GenerateGLLPoints(m - 1), to = GenerateGLLPoints(n - 1);
+    std::vector<std::array<double, 3>> out(n, {0., 0., 0.});
+    for (size_t o = 0; o < n; ++o) {
+        const auto w = LagrangeWeights(to[o], from);
+        for (size_t i = 0; i < m; ++i)
+            for (int d = 0; d < 3; ++d) out[o][d] += w[i] * in[i][d];
+    }
+    return out;
+}
+
+}  // namespace math
+
+namespace components {
+
+enum class ReferenceAxisOrientation { X, Z };
+
+// src/interfaces/components/beam_input.hpp
+struct ReferenceAxis {
+    std::vector<double> coordinate_grid;
+    std::vector<std::array<double, 3>> coordinates;
+    std::vector<double> twist_grid;
+    std::vector<double> twist;   // degrees
+};
+
+struct Section {
+    double location;
+    math::M6 mass_matrix, stiffness_matrix;
+    Section(double loc, const math::M6& m, const math::M6& k) : location(loc), mass_matrix(m), stiffness_matrix(k) {
+        if (loc < 0. || loc > 1.) throw std::invalid_argument("section location must be in [0, 1]");
+    }
+};
+
+struct Root {
+    bool prescribe_root_motion = false;
+    std::array<double, 7> position{0., 0., 0., 1., 0., 0., 0.};
+    std::array<double, 6> velocity{};
+    std::array<double, 6> acceleration{};
+};
+
+struct BeamInput {
+    size_t element_order = 10;
+    size_t section_refinement = 0;
+    ReferenceAxis ref_axis;
+    Root root;
+    std::vector<Section> sections;
+};
+
+// src/interfaces/node_data.hpp: one node's motion out and loads in
+struct NodeData {
+    size_t id;
+    std::array<double, 7> position{0., 0., 0., 1., 0., 0., 0.};
+    std::array<double, 7> displacement{0., 0., 0., 1., 0., 0., 0.};
+    std::array<double, 6> velocity{};
+    std::array<double, 6> acceleration{};
+    std::array<double, 6> loads{};
+    explicit NodeData(size_t i) : id(i) {}
+    void ClearLoads() { loads = {0., 0., 0., 0., 0., 0.}; }
+};
+
+// The rotation taking a Z-up (WindIO) reference axis to the X axis.
+inline std::array<double, 4> ZToX() { return RotationVectorToQuaternion({0., std::numbers::pi / 2., 0.}); }
+
+// src/interfaces/components/beam_builder.cpp
+class BeamBuilder {
+public:
+    BeamBuilder& SetElementOrder(size_t order) { input_.element_order = order; return *this; }
+    BeamBuilder& SetSectionRefinement(size_t r) { input_.section_refinement = r; return *this; }
+    BeamBuilder& AddRefAxisPoint(double s, const std::array<double, 3>& c,
+                                 ReferenceAxisOrientation o = ReferenceAxisOrientation::X) {
+        input_.ref_axis.coordinate_grid.push_back(s);
+        input_.ref_axis.coordinates.push_back(o == ReferenceAxisOrientation::X
+                                                  ? c : RotateVectorByQuaternion(ZToX(), c));
+        return *this;
+    }
+    BeamBuilder& AddRefAxisTwist(double s, double twist) {
+        input_.ref_axis.twist_grid.push_back(s);
+        input_.ref_axis.twist.push_back(twist);
+        return *this;
+    }
+    BeamBuilder& PrescribedRootMotion(bool on) { input_.root.prescribe_root_motion = on; return *this; }
+    BeamBuilder& SetRootPosition(const std::array<double, 7>& p) { input_.root.position = p; return *this; }
+    BeamBuilder& SetRootVelocity(const std::array<double, 6>& v) { input_.root.velocity = v; return *this; }
+    BeamBuilder& SetRootAcceleration(const std::array<double, 6>& a) { input_.root.acceleration = a; return *this; }
+    BeamBuilder& AddSection(double s, const math::M6& mass, const math::M6& stiffness,
+                            ReferenceAxisOrientation o = ReferenceAxisOrientation::X) {
+        if (o == ReferenceAxisOrientation::X)
+            input_.sections.emplace_back(s, mass, stiffness);
+        else
+            input_.sections.emplace_back(s, math::RotateMatrix6(mass, ZToX()), math::RotateMatrix6(stiffness, ZToX()));
+        return *this;
+    }
+    const BeamInput& Input() const { return input_; }
+
+private:
+    BeamInput input_;
+};
+
+// src/interfaces/components/beam.cpp: the blade as one beam element of the
+// requested order on GLL nodes fitted to the reference axis, trapezoidal
+// quadrature at the section stations, placed at the root.
+class Beam {
+public:
+    static constexpr size_t kMaxGeometryPoints = 10;
+    static constexpr size_t invalid_id = static_cast<size_t>(-1);
+    std::vector<NodeData> nodes;
+    size_t beam_element_id = 0;
+    size_t prescribed_root_constraint_id = invalid_id;
+
+    Beam(const BeamInput& in, Model& model) {
+        if (in.ref_axis.coordinate_grid.size() < 2 || in.ref_axis.coordinates.size() < 2)
+            throw std::invalid_argument("at least two reference axis points are required");
+        if (in.ref_axis.coordinate_grid.size() != in.ref_axis.coordinates.size())
+            throw std::invalid_argument("reference axis grid and coordinates differ in size");
+        if (in.sections.empty()) throw std::invalid_argument("at least one section is required");
+        if (in.element_order < 1) throw std::invalid_argument("element order must be at least 1");
+        node_xi_ = math::GenerateGLLPoints(in.element_order);
+        const size_t n_nodes = in.element_order + 1;
+        const size_t n_geo = std::min({in.ref_axis.coordinate_grid.size(), n_nodes, kMaxGeometryPoints});
+        std::vector<std::array<double, 3>> coords;
+        if (n_geo < n_nodes) {
+            const auto geo = math::FitNodes(math::GenerateGLLPoints(n_geo - 1), in.ref_axis.coordinate_grid,
+                                            in.ref_axis.coordinates);
+            coords = math::ProjectPoints(n_geo, n_nodes, geo);
+        } else {
+            coords = math::FitNodes(node_xi_, in.ref_axis.coordinate_grid, in.ref_axis.coordinates);
+        }
+        // tangents: derivative of the node polynomial at the nodes, normalised
+        std::vector<std::array<double, 3>> tangents(n_nodes, {0., 0., 0.});
+        for (size_t a = 0; a < n_nodes; ++a) {
+            const auto dw = math::LagrangeDerivWeights(node_xi_[a], node_xi_);
+            for (size_t b = 0; b < n_nodes; ++b)
+                for (int d = 0; d < 3; ++d) tangents[a][d] += dw[b] * coords[b][d];
+            tangents[a] = math::Unit(tangents[a]);
+        }
+        std::vector<size_t> ids;
+        for (size_t k = 0; k < n_nodes; ++k) {
+            const auto q = math::TangentTwistToQuaternion(tangents[k], 0.);
+            ids.push_back(model.AddNode()
+                              .SetElemLocation((node_xi_[k] + 1.) / 2.)
+                              .SetPosition(coords[k][0], coords[k][1], coords[k][2], q[0], q[1], q[2], q[3])
+                              .Build());
+            nodes.emplace_back(ids.back());
+        }
+        const auto sections = BuildSections(in);
+        std::vector<double> grid;
+        for (const auto& s : sections) grid.push_back(s.position);
+        const auto quad = math::CreateTrapezoidalQuadrature(grid);
+        beam_element_id = model.AddBeamElement(ids, sections, quad);
+        // place at the root
+        const std::array<double, 3> p{in.root.position[0], in.root.position[1], in.root.position[2]};
+        model.TranslateBeam(beam_element_id, p);
+        model.RotateBeamAboutPoint(beam_element_id, {in.root.position[3], in.root.position[4],
+                                                     in.root.position[5], in.root.position[6]}, p);
+        model.SetBeamVelocityAboutPoint(beam_element_id, in.root.velocity, p);
+        model.SetBeamAccelerationAboutPoint(beam_element_id, in.root.acceleration,
+                                            {in.root.velocity[3], in.root.velocity[4], in.root.velocity[5]}, p);
+        if (in.root.prescribe_root_motion) prescribed_root_constraint_id = model.AddPrescribedBC(ids.front());
+    }
+
+    // Distributes a point load at s in [0, 1] over the nodes with the weights
+    // the reference's Beam::AddPointLoad uses (its GetNodeWeights returns the
+    // Lagrange derivative weights at s, beam.cpp:24-41); kept as it is so that
+    // callers see the same nodal loads.
+    void AddPointLoad(double s, const std::array<double, 6>& loads) {
+        if (s < 0. || s > 1.) throw std::invalid_argument("invalid load position");
+        const auto w = math::LagrangeDerivWeights(2. * s - 1., node_xi_);
+        for (size_t k = 0; k < nodes.size(); ++k)
+            for (int c = 0; c < 6; ++c) nodes[k].loads[c] += w[k] * loads[c];
+    }
+    void ClearLoads() {
+        for (auto& n : nodes) n.ClearLoads();
+    }
+
+private:
+    std::vector<double> node_xi_;
+
+    // Sections rotated by the interpolated twist about x, with optional linear
+    // refinement between stations (Beam::BuildBeamSections).
+    static std::vector<BeamSection> BuildSections(const BeamInput& in) {
+        auto twist_q = [&](double s) {
+            const double tw = math::LinearInterp(s, in.ref_axis.twist_grid, in.ref_axis.twist);
+            return RotationVectorToQuaternion({tw * std::numbers::pi / 180., 0., 0.});
+        };
+        std::vector<BeamSection> out;
+        const auto& s0 = in.sections.front();
+        out.emplace_back(s0.location, math::RotateMatrix6(s0.mass_matrix, twist_q(s0.location)),
+                         math::RotateMatrix6(s0.stiffness_matrix, twist_q(s0.location)));
+        for (size_t i = 1; i < in.sections.size(); ++i) {
+            const auto& L = in.sections[i - 1];
+            const auto& R = in.sections[i];
+            for (size_t r = 0; r < in.section_refinement; ++r) {
+                const double al = static_cast<double>(r + 1) / static_cast<double>(in.section_refinement + 1);
+                math::M6 m{}, k{};
+                for (int a = 0; a < 6; ++a)
+                    for (int b = 0; b < 6; ++b) {
+                        m[a][b] = (1. - al) * L.mass_matrix[a][b] + al * R.mass_matrix[a][b];
+                        k[a][b] = (1. - al) * L.stiffness_matrix[a][b] + al * R.stiffness_matrix[a][b];
+                    }
+                // the reference takes the twist of the right station here
+                const auto q = twist_q(R.location);
+                out.emplace_back((1. - al) * L.location + al * R.location, math::RotateMatrix6(m, q),
+                                 math::RotateMatrix6(k, q));
+            }
+            const auto q = twist_q(R.location);
+            out.emplace_back(R.location, math::RotateMatrix6(R.mass_matrix, q),
+                             math::RotateMatrix6(R.stiffness_matrix, q));
+        }
+        return out;
+    }
+};
+
+// src/interfaces/components/solution_input.hpp
+struct SolutionInput {
+    std::array<double, 3> gravity{0., 0., 0.};
+    bool dynamic_solve = true;
+    double time_step = 0.01;
+    double rho_inf = 0.;
+    size_t max_iter = 5;
+    double absolute_error_tolerance = 1e-5;
+    double relative_error_tolerance = 1e-3;
+    std::string output_file_path;
+    StepParameters Parameters() const {
+        return StepParameters(dynamic_solve, max_iter, time_step, rho_inf, absolute_error_tolerance,
+                              relative_error_tolerance);
+    }
+};
+
+// src/interfaces/components/solution_builder.hpp
+class SolutionBuilder {
+public:
+    SolutionBuilder& EnableDynamicSolve() { in_.dynamic_solve = true; return *this; }
+    SolutionBuilder& EnableStaticSolve() { in_.dynamic_solve = false; return *this; }
+    SolutionBuilder& SetTimeStep(double h) { in_.time_step = h; return *this; }
+    SolutionBuilder& SetDampingFactor(double rho) { in_.rho_inf = rho; return *this; }
+    SolutionBuilder& SetGravity(const std::array<double, 3>& g) { in_.gravity = g; return *this; }
+    SolutionBuilder& SetMaximumNonlinearIterations(size_t n) { in_.max_iter = n; return *this; }
+    SolutionBuilder& SetAbsoluteErrorTolerance(double t) { in_.absolute_error_tolerance = t; return *this; }
+    SolutionBuilder& SetRelativeErrorTolerance(double t) { in_.relative_error_tolerance = t; return *this; }
+    SolutionBuilder& SetOutputFile(const std::string& p) { in_.output_file_path = p; return *this; }
+    const SolutionInput& Input() const { return in_; }
+
+private:
+    SolutionInput in_;
+};
+
+}  // namespace components
+
+// src/interfaces/blade/blade_interface.hpp: a blade with loads in and motion
+// out per step, a saved state for predictor-corrector coupling, and the root
+// motion when it is prescribed.
+class BladeInterface {
+public:
+    BladeInterface(const Context& ctx, const components::SolutionInput& sol, const components::BeamInput& blade)
+        : ctx_(ctx), model_(sol.gravity), blade_(blade, model_), parameters_(sol.Parameters()) {
+        auto [state, elements, constraints, solver] = model_.CreateSystemWithSolver(ctx_);
+        state_ = std::make_unique<State>(state);
+        elements_ = std::make_unique<Elements>(elements);
+        constraints_ = std::make_unique<Constraints>(constraints);
+        solver_ = std::make_unique<Solver>(solver);
+        const int id = solver_->model()->id;
+        saved_ = kyn_model_clone(ctx_.get(), id);   // state_save (CloneState)
+        check(ctx_.get(), saved_);
+        loads_.assign(solver_->model()->info.num_nodes * 6, 0.);
+        GetMotion();
+    }
+    BladeInterface(const BladeInterface&) = delete;
+    BladeInterface& operator=(const BladeInterface&) = delete;
+    BladeInterface(BladeInterface&& o) noexcept
+        : ctx_(o.ctx_), model_(std::move(o.model_)), blade_(std::move(o.blade_)),
+          parameters_(o.parameters_), state_(std::move(o.state_)), elements_(std::move(o.elements_)),
+          constraints_(std::move(o.constraints_)), solver_(std::move(o.solver_)), saved_(o.saved_),
+          loads_(std::move(o.loads_)) {
+        o.saved_ = -1;
+    }
+    ~BladeInterface() {
+        if (saved_ >= 0) kyn_model_destroy(ctx_.get(), saved_);
+    }
+
+    components::Beam& Blade() { return blade_; }
+
+    // Node loads -> state.f, one step, motion of the nodes back (false: the
+    // Newton loop reached max_iter, as the reference's Step()).
+    bool Step() {
+        for (const auto& n : blade_.nodes)
+            for (int c = 0; c < 6; ++c) loads_[n.id * 6 + c] = n.loads[c];
+        state_->SetExternalForces(loads_);
+        if (!kynema_b200::Step(parameters_, *solver_, *elements_, *state_, *constraints_)) return false;
+        GetMotion();
+        return true;
+    }
+    void SaveState() { check(ctx_.get(), kyn_state_copy(ctx_.get(), saved_, solver_->model()->id)); }
+    void RestoreState() {
+        check(ctx_.get(), kyn_state_copy(ctx_.get(), solver_->model()->id, saved_));
+        GetMotion();
+    }
+    void SetRootDisplacement(const std::array<double, 7>& u) const {
+        if (blade_.prescribed_root_constraint_id == components::Beam::invalid_id)
+            throw std::runtime_error("prescribed root motion was not enabled");
+        constraints_->UpdateDisplacement(blade_.prescribed_root_constraint_id, u);
+    }
+
+private:
+    void GetMotion() {
+        const auto x = state_->Get(KYN_FIELD_X), q = state_->q(), v = state_->v(), vd = state_->vd();
+        for (auto& n : blade_.nodes) {
+            for (int c = 0; c < 7; ++c) {
+                n.position[c] = x[n.id * 7 + c];
+                n.displacement[c] = q[n.id * 7 + c];
+            }
+            for (int c = 0; c < 6; ++c) {
+                n.velocity[c] = v[n.id * 6 + c];
+                n.acceleration[c] = vd[n.id * 6 + c];
+            }
+        }
+    }
+
+    Context ctx_;
+    Model model_;
+    components::Beam blade_;
+    StepParameters parameters_;
+    std::unique_ptr<State> state_;
+    std::unique_ptr<Elements> elements_;
+    std::unique_ptr<Constraints> constraints_;
+    std::unique_ptr<Solver> solver_;
+    int saved_ = -1;
+    std::vector<double> loads_;
+};
+
+// src/interfaces/blade/blade_interface_builder.hpp
+class BladeInterfaceBuilder {
+public:
+    components::SolutionBuilder& Solution() { return solution_; }
+    components::BeamBuilder& Blade() { return blade_; }
+    BladeInterface Build(const Context& ctx = Context(0)) const {
+        return BladeInterface(ctx, solution_.Input(), blade_.Input());
+    }
+
+private:
+    components::SolutionBuilder solution_;
+    components::BeamBuilder blade_;
+};
+
+}  // namespace kynema_b200::interfaces

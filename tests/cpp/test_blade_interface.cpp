@@ -1,0 +1,116 @@
+// The reference's blade-interface regression driver written against
+// kynema_b200_interfaces.hpp: BladeInterfaceTest.RotatingBeam
+// (tests/regression_tests/interfaces/test_blade_interface.cpp:132-277), same
+// inputs, same golden values and tolerance (1e-10).  Exit code 0 on success.
+#include <cmath>
+#include <cstdio>
+#include <numbers>
+#include <vector>
+
+#include "kynema_b200_interfaces.hpp"
+
+using namespace kynema_b200;
+using namespace kynema_b200::interfaces;
+
+static int failures = 0;
+static void expect_near(double a, double b, double tol, const char* what, int i) {
+    if (!(std::abs(a - b) <= tol)) {
+        std::printf("FAIL %s[%d]: %.17g vs %.17g\n", what, i, a, b);
+        ++failures;
+    }
+}
+
+int main() {
+    try {
+        const double time_step = 0.01;
+        const std::array<double, 3> omega{0., 0., 1.};
+        const std::array<double, 3> x0_root{2., 0., 0.};
+        const std::array<double, 3> root_vel{omega[1] * x0_root[2] - omega[2] * x0_root[1],
+                                             omega[2] * x0_root[0] - omega[0] * x0_root[2],
+                                             omega[0] * x0_root[1] - omega[1] * x0_root[0]};
+        BladeInterfaceBuilder builder;
+        builder.Solution()
+            .EnableDynamicSolve()
+            .SetTimeStep(time_step)
+            .SetDampingFactor(0.0)
+            .SetMaximumNonlinearIterations(6)
+            .SetAbsoluteErrorTolerance(1e-6)
+            .SetRelativeErrorTolerance(1e-4);
+        const std::vector<double> node_s{0., 0.11747233803526763, 0.35738424175967748,
+                                         0.64261575824032247, 0.88252766196473242, 1.};
+        builder.Blade()
+            .SetElementOrder(5)
+            .PrescribedRootMotion(true)
+            .SetRootPosition({x0_root[0], x0_root[1], x0_root[2], 1., 0., 0., 0.})
+            .SetRootVelocity({root_vel[0], root_vel[1], root_vel[2], omega[0], omega[1], omega[2]})
+            .AddRefAxisTwist(0., 0.)
+            .AddRefAxisTwist(1., 0.);
+        for (double s : node_s)
+            builder.Blade().AddRefAxisPoint(s, {10. * s, 0., 0.}, components::ReferenceAxisOrientation::X);
+        const std::vector<double> section_s{0.0254460438286208, 0.1292344072003028, 0.2970774243113015, 0.5,
+                                            0.7029225756886985, 0.8707655927996972, 0.9745539561713792};
+        const components::ReferenceAxisOrientation X = components::ReferenceAxisOrientation::X;
+        for (double s : section_s)
+            builder.Blade().AddSection(
+                s,
+                {{{8.538e-2, 0., 0., 0., 0., 0.}, {0., 8.538e-2, 0., 0., 0., 0.}, {0., 0., 8.538e-2, 0., 0., 0.},
+                  {0., 0., 0., 1.4433e-2, 0., 0.}, {0., 0., 0., 0., 0.40972e-2, 0.}, {0., 0., 0., 0., 0., 1.0336e-2}}},
+                {{{1368.17e3, 0., 0., 0., 0., 0.}, {0., 88.56e3, 0., 0., 0., 0.}, {0., 0., 38.78e3, 0., 0., 0.},
+                  {0., 0., 0., 16.9600e3, 17.6100e3, -0.3510e3}, {0., 0., 0., 17.6100e3, 59.1200e3, -0.3700e3},
+                  {0., 0., 0., -0.3510e3, -0.3700e3, 141.470e3}}},
+                X);
+        auto interface = builder.Build(Context(0));
+        for (int i = 1; i < 10; ++i) {
+            const double t = static_cast<double>(i) * time_step;
+            const auto u_rot = RotationVectorToQuaternion({omega[0] * t, omega[1] * t, omega[2] * t});
+            const auto x_root = RotateVectorByQuaternion(u_rot, x0_root);
+            interface.SetRootDisplacement({x_root[0] - x0_root[0], x_root[1] - x0_root[1], x_root[2] - x0_root[2],
+                                           u_rot[0], u_rot[1], u_rot[2], u_rot[3]});
+            if (!interface.Step()) {
+                std::printf("FAIL step %d did not converge\n", i);
+                ++failures;
+            }
+        }
+        const auto& root = interface.Blade().nodes[0];
+        const auto& tip = interface.Blade().nodes[5];
+        const double rp[7] = {1.9919054660239885, 0.17975709839602211, 0., 0.99898767084784234, 0., 0.,
+                              0.044984814037660227};
+        const double ru[7] = {-0.0080945339760114532, 0.17975709839602211, 0., 0.99898767084784234, 0., 0.,
+                              0.044984814037660227};
+        const double rv[6] = {-0.17976259212149071, 1.9919719054875213, 0., 0., 0., 1.};
+        const double ra[6] = {-1.9920882238788629, -0.17977158309645525, 0., 0., 0., 0.};
+        const double tp[7] = {11.951460424343411, 1.0785463019560009, 2.2845605555050727E-10, 0.99898766738195299,
+                              2.6570959740959799E-9, -1.0123941616837804E-10, 0.044984891005365443};
+        const double tu[7] = {-0.048539575656588806, 1.0785463019560009, 2.2845605555050727E-10,
+                              0.99898766738195299, 2.6570959740959799E-9, -1.0123941616837804E-10,
+                              0.044984891005365443};
+        const double tv[6] = {-1.0786835619583102, 11.95303967174639, -6.3862048021175104E-8,
+                              0.000003159329892760129, 2.5866107917084571E-7, 1.0001562024381443};
+        const double ta[6] = {-11.955952417551353, -1.0800839943831992, -0.000013544534439173783,
+                              -0.000046709402446003812, 0.000008256203749646939, 0.00020635762959181575};
+        for (int c = 0; c < 7; ++c) {
+            expect_near(root.position[c], rp[c], 1e-10, "root position", c);
+            expect_near(root.displacement[c], ru[c], 1e-10, "root displacement", c);
+            expect_near(tip.position[c], tp[c], 1e-10, "tip position", c);
+            expect_near(tip.displacement[c], tu[c], 1e-10, "tip displacement", c);
+        }
+        for (int c = 0; c < 6; ++c) {
+            expect_near(root.velocity[c], rv[c], 1e-10, "root velocity", c);
+            expect_near(root.acceleration[c], ra[c], 1e-10, "root acceleration", c);
+            expect_near(tip.velocity[c], tv[c], 1e-10, "tip velocity", c);
+            expect_near(tip.acceleration[c], ta[c], 1e-10, "tip acceleration", c);
+        }
+        // save / restore: a step taken after SaveState is undone by RestoreState
+        interface.SaveState();
+        const auto before = tip.position;
+        interface.Blade().nodes[5].loads[2] = 1e3;
+        interface.Step();
+        interface.RestoreState();
+        for (int c = 0; c < 7; ++c) expect_near(interface.Blade().nodes[5].position[c], before[c], 0., "restored", c);
+    } catch (const std::exception& e) {
+        std::printf("FAIL exception: %s\n", e.what());
+        return 2;
+    }
+    std::printf("%s (%d failures)\n", failures ? "FAILED" : "OK", failures);
+    return failures ? 1 : 0;
+}
