@@ -14,6 +14,8 @@ Sources (paths relative to the reference project root):
   tests/regression_tests/regression/test_rotating_beam.cpp   expected q (prescribed
                                                              root; rotation control)
   tests/unit_tests/system/beams/test_curved_beam.hpp         kernel-level data
+  tests/regression_tests/interfaces/test_blade_interface.cpp + its WindIO file
+                                                             IEA-15 blade input, tip
   tests/regression_tests/regression/test_masses.cpp,
     test_precession.cpp, test_spring_mass_system.cpp          point masses, springs
 """
@@ -206,6 +208,42 @@ def main(ref: str) -> None:
                                "tolerance": max(half[3], full[3])},
                "spring_mass_chain": {"steps": 1000, "tolerance": 1e-14}},
               open(os.path.join(out_dir, "masses_springs.json"), "w"), indent=1)
+
+    # ---- IEA-15 blade through the blade interface (WindIO input) ----------------
+    # tests/regression_tests/interfaces/test_blade_interface.cpp:13-128 reads the
+    # WindIO file of interfaces_test_files; its blade axis, twist and 6x6 section
+    # tables go to a plain-number file the C++ driver reads, with the expected
+    # tip position of the test.
+    import yaml
+    itf = os.path.join(ref, "tests", "regression_tests", "interfaces")
+    wio = yaml.safe_load(open(os.path.join(itf, "interfaces_test_files", "IEA-15-240-RWT.yaml")))
+    bl = wio["components"]["blade"]
+    ra = bl["outer_shape_bem"]["reference_axis"]
+    tw = bl["outer_shape_bem"]["twist"]
+    kk = bl["elastic_properties_mb"]["six_x_six"]["stiff_matrix"]
+    mm = bl["elastic_properties_mb"]["six_x_six"]["inertia_matrix"]
+    bt = strip_comments(open(os.path.join(itf, "test_blade_interface.cpp")).read())
+    b0 = bt.index("TEST(BladeInterfaceTest, BladeWindIO)")
+    b1 = bt.index("TEST(", b0 + 5)
+    tip = [float(m.group(2)) for m in
+           re.finditer(r"EXPECT_NEAR\(\s*tip_node\.position\[(\d)\],\s*(" + NUM + r"),", bt[b0:b1])]
+    assert len(tip) == 7
+    lines = [str(len(ra["x"]["grid"]))]
+    for i, g in enumerate(ra["x"]["grid"]):
+        lines.append(" ".join(repr(float(v)) for v in (g, ra["x"]["values"][i], ra["y"]["values"][i],
+                                                        ra["z"]["values"][i])))
+    lines.append(str(len(tw["grid"])))
+    for g, v in zip(tw["grid"], tw["values"]):
+        lines.append(f"{float(g)!r} {float(v)!r}")
+    lines.append(str(len(kk["grid"])))
+    for i, g in enumerate(kk["grid"]):
+        assert abs(mm["grid"][i] - g) <= 1e-8
+        lines.append(" ".join(repr(float(v)) for v in [g] + list(mm["values"][i]) + list(kk["values"][i])))
+    lines.append(" ".join(repr(v) for v in tip))
+    with open(os.path.join(out_dir, "iea15_blade_windio.txt"), "w") as f:
+        f.write("# IEA-15-240-RWT blade (WindIO) for BladeInterfaceTest.BladeWindIO:\n"
+                "# axis points (grid x y z), twist (grid deg), sections (grid inertia[21] stiffness[21]),\n"
+                "# expected tip position [7]\n" + "\n".join(lines) + "\n")
 
     # ---- curved beam (kernel level) --------------------------------------------
     cb = strip_comments(open(os.path.join(unit, "test_curved_beam.hpp")).read())

@@ -37,11 +37,13 @@ def test_shim_compiles():
 
 
 @pytest.mark.gpu
-def test_blade_interface_rotating_beam():
+def test_blade_interface_rotating_beam_and_windio():
     """BladeInterface (include/kynema_b200_interfaces.hpp) on the reference's
-    BladeInterfaceTest.RotatingBeam: root and tip motion at 1e-10."""
+    BladeInterfaceTest.RotatingBeam (root and tip motion) and BladeWindIO (the
+    IEA-15 blade from its WindIO description, tip position), both at 1e-10."""
     exe = _compile(BLADE_SRC, "test_blade_interface")
-    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    fixture = os.path.join(ROOT, "tests", "golden", "iea15_blade_windio.txt")
+    r = subprocess.run([exe, fixture], capture_output=True, text=True, timeout=300)
     print(r.stdout)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "OK (0 failures)" in r.stdout
