@@ -1,8 +1,8 @@
 // The reference's blade-interface regression drivers written against
-// kynema_b200_interfaces.hpp: BladeInterfaceTest.RotatingBeam and
-// BladeInterfaceTest.BladeWindIO
-// (tests/regression_tests/interfaces/test_blade_interface.cpp:13-277), same
-// inputs, same golden values and tolerance (1e-10).  The IEA-15 blade input of
+// kynema_b200_interfaces.hpp: BladeInterfaceTest.RotatingBeam,
+// BladeInterfaceTest.BladeWindIO and BladeInterfaceTest.StaticCurledBeam
+// (tests/regression_tests/interfaces/test_blade_interface.cpp:13-277, 392-492),
+// same inputs, same golden values and tolerances (1e-10; 1e-8 static).  The IEA-15 blade input of
 // the WindIO case is read from the fixture given as argv[1]
 // (tests/golden/iea15_blade_windio.txt).  Exit code 0 on success.
 #include <cmath>
@@ -91,9 +91,54 @@ static void blade_windio(const char* path) {
     for (int c = 0; c < 7; ++c) expect_near(tip.position[c], expected[c], 1e-10, "windio tip position", c);
 }
 
+// StaticCurledBeam: static solves of a straight 10 m blade of order 10 (two key
+// points, sections refined once) under a growing tip moment about y that curls
+// it towards a full circle; tip position after each load at 1e-8.
+static void static_curled_beam() {
+    BladeInterfaceBuilder builder;
+    builder.Solution()
+        .EnableStaticSolve()
+        .SetTimeStep(1.)
+        .SetDampingFactor(1.)
+        .SetMaximumNonlinearIterations(10)
+        .SetAbsoluteErrorTolerance(1e-5)
+        .SetRelativeErrorTolerance(1e-3);
+    builder.Blade().SetElementOrder(10).SetSectionRefinement(1).PrescribedRootMotion(true)
+        .AddRefAxisTwist(0., 0.).AddRefAxisTwist(1., 0.);
+    const auto X = components::ReferenceAxisOrientation::X;
+    for (double s : {0., 1.}) builder.Blade().AddRefAxisPoint(s, {s * 10., 0., 0.}, X);
+    for (int i = 0; i <= 10; ++i)
+        builder.Blade().AddSection(
+            0.1 * i,
+            {{{1., 0., 0., 0., 0., 0.}, {0., 1., 0., 0., 0., 0.}, {0., 0., 1., 0., 0., 0.},
+              {0., 0., 0., 1., 0., 0.}, {0., 0., 0., 0., 1., 0.}, {0., 0., 0., 0., 0., 1.}}},
+            {{{1770.e3, 0., 0., 0., 0., 0.}, {0., 1770.e3, 0., 0., 0., 0.}, {0., 0., 1770.e3, 0., 0., 0.},
+              {0., 0., 0., 8.16e3, 0., 0.}, {0., 0., 0., 0., 86.9e3, 0.}, {0., 0., 0., 0., 0., 215.e3}}},
+            X);
+    auto interface = builder.Build(Context(0));
+    auto& tip = interface.Blade().nodes.back();
+    const double moments[6] = {0., 10920.0, 21840.0, 32761.0, 43681.0, 54601.0};
+    const double expected[6][3] = {{10., 0., 0.},
+                                   {7.5396813678794645, 0., 5.5363879677563252},
+                                   {2.275087482106132, 0., 7.2166560706481686},
+                                   {-1.6222827675944771, 0., 4.7694966546892239},
+                                   {-1.9054629771623546, 0., 1.3243726828814482},
+                                   {0.021386893541979646, 0., 0.0006097054603659835}};
+    for (int k = 0; k < 6; ++k) {
+        tip.loads[4] = -moments[k];
+        if (!interface.Step()) {
+            std::printf("FAIL static curled beam load %d did not converge\n", k);
+            ++failures;
+            return;
+        }
+        for (int c = 0; c < 3; ++c) expect_near(tip.position[c], expected[k][c], 1e-8, "curled tip", 3 * k + c);
+    }
+}
+
 int main(int argc, char** argv) {
     try {
         if (argc > 1) blade_windio(argv[1]);
+        static_curled_beam();
         const double time_step = 0.01;
         const std::array<double, 3> omega{0., 0., 1.};
         const std::array<double, 3> x0_root{2., 0., 0.};
