@@ -39,6 +39,8 @@ struct DevModel {
     // whenever the model set changes, every iteration of a serving loop).
     std::vector<SlabLayout> lay;     // per beam slab layout
     std::vector<KBeam> kt;           // per beam launch record (plan fields filled per plan)
+    KBeam* d_kt = nullptr;           // the same records resident on the device (plans gather them)
+    std::vector<int> node_base;      // per beam: first global node when its nodes are contiguous, else -1
     int def_nt[2] = {0, 0};          // default threads per CTA, FP64 / FP32 form
     bool lump = false;               // some beam carries point masses or springs
     int smem_nt[2][3] = {};          // dynamic smem for 128 / 256 / 512 threads, per form
@@ -82,6 +84,7 @@ struct Plan {
     int* h_iters = nullptr;
     int nbeams = 0;
     bool record = false;
+    unsigned long long epoch = 0;     // model-destroy count when built
     cudaGraphExec_t graph = nullptr;  // captured step (KYN_OPT_CUDA_GRAPH)
     StepCoeffs graph_coeffs{};        // coefficients baked into the captured launches
     ~Plan() {  // buffers belong to the context's plan pool
@@ -93,12 +96,42 @@ struct Plan {
 struct XferBeam {
     double* slab_field;   // slab + field offset
     long long ext_off;    // offset of this beam's first row in the external array
-    int map_off;          // offset into the node map
+    int map_off;          // offset into the node map; -1: rows in order (ext row k = slab row k)
     int N;
 };
 
+// Source of one plan record: a model's resident KBeam and the plan's own fields.
+struct PlanSrc {
+    const KBeam* src;
+    double* dump;
+    int plan_model;
+    int pad;
+};
+static_assert(sizeof(KBeam) % 8 == 0, "KBeam is copied in 8-byte words");
+
+// Fills a plan's KBeam array from the models' resident records (one warp per
+// record), so that a new plan uploads 24 bytes per beam instead of the record.
+__global__ void gather_kbeams(const PlanSrc* __restrict__ srcs, int n, KBeam* __restrict__ out,
+                              unsigned long long* prof) {
+    const int w = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (w >= n) return;
+    const PlanSrc sr = srcs[w];
+    const unsigned long long* a = reinterpret_cast<const unsigned long long*>(sr.src);
+    unsigned long long* b = reinterpret_cast<unsigned long long*>(out + w);
+    constexpr int kWords = static_cast<int>(sizeof(KBeam) / 8);
+    for (int k = lane; k < kWords; k += 32) b[k] = a[k];
+    __syncwarp();
+    if (lane == 0) {
+        out[w].plan_model = sr.plan_model;
+        out[w].dump = sr.dump;
+        out[w].prof = prof;
+    }
+}
+
 struct XferPlan {
     std::vector<int> ids;
+    unsigned long long epoch = 0;  // model-destroy count when built
     int kind = -1;        // load channel (0/1) or 100 + state field
     int width = 0;
     long long total = 0;  // doubles in the external array
@@ -120,7 +153,8 @@ __global__ void xfer_kernel(const XferBeam* __restrict__ beams, const int* __res
     const int n = b.N * width;
     for (int t = threadIdx.x; t < n; t += blockDim.x) {
         const int k = t / width, c = t - k * width;
-        const long long e = b.ext_off + static_cast<long long>(map[b.map_off + k]) * width + c;
+        const int row = (b.map_off < 0) ? k : map[b.map_off + k];
+        const long long e = b.ext_off + static_cast<long long>(row) * width + c;
         if (to_slab) b.slab_field[t] = ext[e];
         else ext[e] = b.slab_field[t];
     }
@@ -160,14 +194,18 @@ struct kyn_ctx {
     // serving loop does it every iteration) allocates nothing in steady state.
     KBeam* pool_kbeams = nullptr;
     size_t pool_kbeams_cap = 0;
-    KBeam* pool_hkbeams = nullptr;        // pinned staging of the plan's KBeam records
-    size_t pool_hkbeams_cap = 0;
+    PlanSrc* pool_hsrc = nullptr;         // pinned staging of the plan's record sources
+    size_t pool_hsrc_cap = 0;
+    PlanSrc* pool_dsrc = nullptr;         // the same on the device
+    size_t pool_dsrc_cap = 0;
+    unsigned long long destroy_epoch = 0; // models destroyed so far (cached plans check it)
     cudaEvent_t plan_uploaded = nullptr;  // the staging buffer's last upload
     bool plan_upload_pending = false;
     int* pool_status = nullptr;           // device [2][cap]: status, iterations
     int* pool_hstatus = nullptr;          // pinned [2][cap]
     size_t pool_status_cap = 0;
     std::vector<int> presc_ids;           // batched prescribed motion: cached targets
+    unsigned long long presc_epoch = 0;   // model-destroy count when they were built
     double** presc_targets = nullptr;     // device [count] slab addresses of con_input slots
     int* presc_vidx = nullptr;            // device [count] row of the caller's array per target
     int presc_rows = 0;                   // constraint rows of the cached id list
@@ -271,6 +309,13 @@ void prepare_model(DevModel* m) {
                 m->smem_nt[f][k] = std::max(m->smem_nt[f][k], beam_smem(hb.N, hb.Q, hb.nc, rb, 128 << k, hubf));
         }
     }
+    m->node_base.clear();
+    for (const HostBeam& hb : H.beams) {
+        int base = hb.node_ids.empty() ? -1 : hb.node_ids[0];
+        for (int k = 0; k < hb.N && base >= 0; ++k)
+            if (hb.node_ids[k] != base + k) base = -1;
+        m->node_base.push_back(base);
+    }
     for (size_t b = 0; b < H.beams.size(); ++b) {
         const HostBeam& hb = H.beams[b];
         m->lay.push_back(make_slab_layout(hb.N, hb.Q));
@@ -303,6 +348,17 @@ void prepare_model(DevModel* m) {
 }
 
 int nt_index(int nt) { return nt == 128 ? 0 : nt == 256 ? 1 : 2; }
+
+// The model's launch records, resident on the device for the plans to gather
+// (stream-ordered; the host copy m->kt stays alive with the model).
+int upload_templates(kyn_ctx* c, DevModel* m) {
+    const size_t len = sizeof(KBeam) * m->kt.size();
+    KYN_CUDA(c, cudaMallocAsync(reinterpret_cast<void**>(&m->d_kt), len, c->stream));
+    KYN_CUDA(c, cudaMemcpyAsync(m->d_kt, m->kt.data(), len, cudaMemcpyHostToDevice, c->stream));
+    m->bytes += len;
+    c->used += len;
+    return KYN_OK;
+}
 
 // Per-call device buffers grow by doubling from a floor sized for a serving
 // batch, stream-ordered on the context stream (no device synchronisation: work
@@ -342,12 +398,13 @@ constexpr size_t kPoolRows = 16384 * 24; // growth floor of the per-node-row buf
 // Builds (or reuses) the launch plan for this id list.
 int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
     if (c->plan && c->plan->record == c->record && c->plan->precision == precision &&
-        static_cast<int>(c->plan->ids.size()) == n &&
+        c->plan->epoch == c->destroy_epoch && static_cast<int>(c->plan->ids.size()) == n &&
         std::equal(ids, ids + n, c->plan->ids.begin())) {
         *out = c->plan.get();
         return KYN_OK;
     }
     auto plan = std::make_unique<Plan>();
+    plan->epoch = c->destroy_epoch;
     plan->ids.assign(ids, ids + n);
     plan->record = c->record;
     plan->precision = precision;
@@ -389,17 +446,17 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
         if (a.work != b.work) return a.work > b.work;
         return a.model_index < b.model_index;
     });
-    // KBeam records go through a pinned staging buffer (one DMA); wait for the
-    // previous plan's upload before refilling it
+    // The record sources go through a pinned staging buffer (one DMA) and a
+    // gather on the device; wait for the previous plan's upload before refilling it
     if (c->plan_upload_pending) {
         KYN_CUDA(c, cudaEventSynchronize(c->plan_uploaded));
         c->plan_upload_pending = false;
     }
     {
-        const int rc = grow_pinned(c, c->pool_hkbeams, c->pool_hkbeams_cap, nbeams, kPoolBeams);
+        const int rc = grow_pinned(c, c->pool_hsrc, c->pool_hsrc_cap, nbeams, kPoolBeams);
         if (rc != KYN_OK) return rc;
     }
-    KBeam* kb = c->pool_hkbeams;
+    PlanSrc* kb = c->pool_hsrc;
     size_t nk = 0;
     for (size_t e = 0; e < entries.size(); ++e) {
         const Entry& en = entries[e];
@@ -417,18 +474,19 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
         bk.smem = std::max(bk.smem, en.smem);
         DevModel* m = en.m;
         for (size_t b = 0; b < m->kt.size(); ++b) {
-            KBeam k = m->kt[b];
+            PlanSrc& k = kb[nk++];
+            k.src = m->d_kt + b;
             k.plan_model = en.model_index;
             // the system dump covers single-node constraints only
-            k.dump = (c->record && m->d_dump && !k.hub) ? m->d_dump + m->dump_off[b] : nullptr;
-            k.prof = c->d_prof;
-            kb[nk++] = k;
+            k.dump = (c->record && m->d_dump && !m->kt[b].hub) ? m->d_dump + m->dump_off[b] : nullptr;
             bk.count++;
         }
     }
     plan->nbeams = static_cast<int>(nk);
     {
         int rc = grow_device(c, c->pool_kbeams, c->pool_kbeams_cap, nk, kPoolBeams);
+        if (rc != KYN_OK) return rc;
+        rc = grow_device(c, c->pool_dsrc, c->pool_dsrc_cap, nk, kPoolBeams);
         if (rc != KYN_OK) return rc;
         if (c->pool_status_cap < static_cast<size_t>(n) || !c->pool_status) {
             // status and iteration counts share one buffer: [cap] + [cap]
@@ -449,9 +507,17 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
     plan->d_iters = c->pool_status + c->pool_status_cap;
     plan->h_status = c->pool_hstatus;
     plan->h_iters = c->pool_hstatus + c->pool_status_cap;
-    KYN_CUDA(c, cudaMemcpyAsync(plan->d_kbeams, kb, sizeof(KBeam) * nk, cudaMemcpyHostToDevice,
+    KYN_CUDA(c, cudaMemcpyAsync(c->pool_dsrc, kb, sizeof(PlanSrc) * nk, cudaMemcpyHostToDevice,
                                 c->stream));
     KYN_CUDA(c, cudaEventRecord(c->plan_uploaded, c->stream));
+    if (nk > 0) {
+        const int threads = 256;
+        const int blocks = static_cast<int>((nk * 32 + threads - 1) / threads);
+        gather_kbeams<<<blocks, threads, 0, c->stream>>>(c->pool_dsrc, static_cast<int>(nk), plan->d_kbeams,
+                                                          c->d_prof);
+        KYN_CUDA(c, cudaGetLastError());
+        c->launches++;
+    }
     c->plan_upload_pending = true;
     c->plan = std::move(plan);
     *out = c->plan.get();
@@ -584,7 +650,8 @@ int get_xfer(kyn_ctx* c, const int* ids, int n, int kind, XferPlan** out) {
     const int slot = (kind == KYN_LOAD_NODE_FX) ? 0 : (kind == KYN_LOAD_STATE_F) ? 1
                                                      : (kind == 100 + KYN_FIELD_Q) ? 2 : 3;
     auto& cached = c->xfer[slot];
-    if (cached && cached->kind == kind && static_cast<int>(cached->ids.size()) == n &&
+    if (cached && cached->kind == kind && cached->epoch == c->destroy_epoch &&
+        static_cast<int>(cached->ids.size()) == n &&
         std::equal(ids, ids + n, cached->ids.begin())) {
         *out = cached.get();
         return KYN_OK;
@@ -592,6 +659,7 @@ int get_xfer(kyn_ctx* c, const int* ids, int n, int kind, XferPlan** out) {
     // Reuse the slot's device buffers (the id set changes every serving iteration).
     std::unique_ptr<XferPlan> xp = cached ? std::move(cached) : std::make_unique<XferPlan>();
     xp->ids.assign(ids, ids + n);
+    xp->epoch = c->destroy_epoch;
     xp->width = 0;
     xp->kind = kind;
     std::vector<XferBeam>& beams = c->xfer_beams_tmp;
@@ -616,12 +684,17 @@ int get_xfer(kyn_ctx* c, const int* ids, int n, int kind, XferPlan** out) {
                                    "batched node_FX needs single-element beams (use kyn_model_set_loads)");
                 fo = L.fx;
                 xb.ext_off = off + elem * 6;
-                for (int k = 0; k < b.N; ++k) map.push_back(k);
+                xb.map_off = -1;   // element rows in order
             } else {
                 fo = (kind == KYN_LOAD_STATE_F) ? L.f : field_slot(kind - 100, L, &width);
                 if (fo < 0) return set_err(c, KYN_ERR_INVALID, "field not available in batch form");
-                xb.ext_off = off;
-                for (int k = 0; k < b.N; ++k) map.push_back(b.node_ids[k]);
+                if (m->node_base[bi] >= 0) {  // the beam's nodes are consecutive model nodes
+                    xb.ext_off = off + static_cast<long long>(m->node_base[bi]) * width;
+                    xb.map_off = -1;
+                } else {
+                    xb.ext_off = off;
+                    for (int k = 0; k < b.N; ++k) map.push_back(b.node_ids[k]);
+                }
             }
             xp->width = width;
             xb.slab_field = m->d_slab[bi] + fo;
@@ -710,10 +783,12 @@ void kyn_ctx_destroy(kyn_ctx* c) {
         for (double* p : kv.second->d_slab) cudaFree(p);
         if (kv.second->d_conv) cudaFree(kv.second->d_conv);
         if (kv.second->d_dump) cudaFree(kv.second->d_dump);
+        if (kv.second->d_kt) cudaFree(kv.second->d_kt);
     }
     c->models.clear();
     if (c->pool_kbeams) cudaFree(c->pool_kbeams);
-    if (c->pool_hkbeams) cudaFreeHost(c->pool_hkbeams);
+    if (c->pool_hsrc) cudaFreeHost(c->pool_hsrc);
+    if (c->pool_dsrc) cudaFree(c->pool_dsrc);
     if (c->plan_uploaded) cudaEventDestroy(c->plan_uploaded);
     if (c->pool_status) cudaFree(c->pool_status);
     if (c->pool_hstatus) cudaFreeHost(c->pool_hstatus);
@@ -841,6 +916,10 @@ int kyn_model_create(kyn_ctx* c, const kyn_model_desc* desc) {
     m->bytes = bytes;
     c->used += bytes;
     prepare_model(m.get());
+    {
+        const int urc = upload_templates(c, m.get());
+        if (urc != KYN_OK) return urc;
+    }
     const int id = c->next_id++;
     c->models[id] = std::move(m);
     return id;
@@ -855,14 +934,13 @@ int kyn_model_destroy(kyn_ctx* c, int id) {
     for (double* p : m->d_slab) KYN_CUDA(c, cudaFreeAsync(p, c->stream));
     if (m->d_conv) KYN_CUDA(c, cudaFreeAsync(m->d_conv, c->stream));
     if (m->d_dump) KYN_CUDA(c, cudaFreeAsync(m->d_dump, c->stream));
+    if (m->d_kt) KYN_CUDA(c, cudaFreeAsync(m->d_kt, c->stream));
     c->used -= m->bytes;
     c->models.erase(id);
-    if (c->plan && std::find(c->plan->ids.begin(), c->plan->ids.end(), id) != c->plan->ids.end())
-        c->plan.reset();
-    if (std::find(c->presc_ids.begin(), c->presc_ids.end(), id) != c->presc_ids.end())
-        c->presc_ids.clear();
-    for (auto& x : c->xfer)
-        if (x && std::find(x->ids.begin(), x->ids.end(), id) != x->ids.end()) x->ids.clear();
+    // Cached plans, transfer plans and prescribed-motion targets built before
+    // this call are not reused (each compares the count with the one it was
+    // built at), so a cached list that held this id is never stepped again.
+    ++c->destroy_epoch;
     return KYN_OK;
 }
 
@@ -1235,7 +1313,8 @@ extern "C" int kyn_set_prescribed_batch(kyn_ctx* c, const int* ids, int n, const
     if (!c || n < 0 || (n > 0 && (!ids || !values))) return KYN_ERR_INVALID;
     if (n == 0) return KYN_OK;
     KYN_CUDA(c, cudaSetDevice(c->device));
-    if (!(static_cast<int>(c->presc_ids.size()) == n && std::equal(ids, ids + n, c->presc_ids.begin()))) {
+    if (!(c->presc_epoch == c->destroy_epoch && static_cast<int>(c->presc_ids.size()) == n &&
+          std::equal(ids, ids + n, c->presc_ids.begin()))) {
         std::vector<double*> t;
         std::vector<int> vi;
         int row = 0;
@@ -1276,6 +1355,7 @@ extern "C" int kyn_set_prescribed_batch(kyn_ctx* c, const int* ids, int n, const
         c->presc_count = static_cast<int>(t.size());
         c->presc_rows = row;
         c->presc_ids.assign(ids, ids + n);
+        c->presc_epoch = c->destroy_epoch;
     }
     const int cnt = c->presc_count;
     if (cnt == 0) return KYN_OK;
@@ -1465,6 +1545,10 @@ int clone_model(kyn_ctx* c, int id) {
     m->bytes = bytes;
     c->used += bytes;
     prepare_model(m.get());
+    {
+        const int urc = upload_templates(c, m.get());
+        if (urc != KYN_OK) return urc;
+    }
     const int nid = c->next_id++;
     c->models[nid] = std::move(m);
     return nid;

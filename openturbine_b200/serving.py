@@ -236,10 +236,17 @@ class StepServer:
         if leave.size:
             t5 = time.perf_counter()
             now = now_fn()
-            for i in leave:
+            # final displacements of all leaving models in one batched read
+            lids = np.ascontiguousarray(self._ids[leave])
+            rows = [self.ctx.info(int(mid)).num_nodes for mid in lids]
+            qall = np.empty((sum(rows), 7))
+            self.ctx.get_state_batch(lids, "q", qall.ctypes.data, False)
+            start = 0
+            for i, nr in zip(leave, rows):
                 r = self.active[i]
                 r.done = int(self._done[i])
-                r.final_q = self.ctx.state(r.model_id, "q")
+                r.final_q = qall[start:start + nr].copy()
+                start += nr
                 self.ctx.destroy_model(r.model_id)
                 r.finished_at = now
                 self.finished.append(r)
