@@ -37,6 +37,22 @@ from openturbine_b200 import workloads as W  # noqa: E402
 L2_FLUSH_BYTES = 256 << 20
 
 
+# DRAM bytes per beam-step of the step kernel from the ncu capture of
+# profiles/step_kernel_fp64_batch.md (53.2 MB for 2048 beams: the slab read once
+# and the state written once per step).
+DRAM_BYTES_PER_BEAM_STEP = 53.2e6 / 2048
+
+
+def _hbm_peak() -> float | None:
+    """Measured HBM copy bandwidth of this pool's B200s, when the file is present."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
 def algorithmic_flops(N: int, Q: int, iters: int, f_qp: float) -> float:
     """FLOPs of one beam for `iters` Newton iterations (per-iteration count:
     Q*F_qp + 410 N^2 Q + 468 N^2 + 48 N Q + (2/3) n^3 + 2 n^2, n = 6N + 6)."""
@@ -419,9 +435,14 @@ def main() -> None:
             "e2e": {"value": e2e, "unit": "beam-steps/s",
                     "h2d_bytes_per_step": int(elem_nodes * 6 * 8),
                     "d2h_bytes_per_step": int(elem_nodes * 7 * 8 + 2 * 4 * len(ids))},
-            "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak,
-                         "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": None,
-                         "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run"},
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": fp64_peak,
+                         "unit": "TFLOP/s", "frac": achieved / fp64_peak,
+                         "traffic": DRAM_BYTES_PER_BEAM_STEP * len(ids),
+                         "peak_source": "cuBLAS FP64 GEMM 8192^3 (FP64 tensor cores) measured in this run",
+                         "traffic_source": "ncu dram bytes read+write per beam-step (2048 beams x 13 nodes, "
+                                           "profiles/step_kernel_fp64_batch.md) x beams per step",
+                         "hbm": {"achieved_gbs": DRAM_BYTES_PER_BEAM_STEP * len(ids) / (t_value_ms / args.steps * 1e-3) / 1e9,
+                                 "peak_gbs": _hbm_peak(), "peak_source": "MEASURED_PEAKS.json hbm_gbs"}},
             "gpu_launches": launches,
             "setup_s": t_setup,
         }
