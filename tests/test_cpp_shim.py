@@ -36,6 +36,49 @@ def test_shim_compiles():
     assert os.path.exists(_compile(BLADE_SRC, "test_blade_interface"))
 
 
+def test_interface_geometry_helpers():
+    """The blade interface's host geometry (no GPU): GLL points, trapezoidal
+    quadrature, the end-point-constrained least-squares fit of the reference
+    axis and the tangent/twist frame, against independent computations."""
+    import numpy as np
+    from openturbine_b200.model import CreateTrapezoidalQuadrature, GenerateGLLPoints
+    exe = _compile(os.path.join(ROOT, "tests", "cpp", "test_interface_math.cpp"), "test_interface_math")
+    out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split("\n")
+    vals = {}
+    for line in out:
+        if line:
+            k, *v = line.split()
+            vals.setdefault(k, []).append([float(x) for x in v])
+    for order in (1, 4, 10):
+        got = [v[1] for v in vals["gll"] if int(v[0]) == order]
+        np.testing.assert_allclose(got, GenerateGLLPoints(order), rtol=0, atol=1e-14)
+    np.testing.assert_allclose(vals["trap"], CreateTrapezoidalQuadrature([0., 0.1, 0.25, 0.6, 1.]),
+                               rtol=0, atol=1e-15)
+    # the fit: interior rows are the normal equations of the key points, the
+    # end rows pin the first and last key point
+    xi = np.array(GenerateGLLPoints(4))
+    s = np.arange(7) / 6.
+    kp = np.stack([10 * s, 0.5 * s * s, 0.1 * s ** 3], axis=1)
+    phi = np.array([[np.prod([(2 * si - 1 - xi[m]) / (xi[j] - xi[m]) for m in range(5) if m != j])
+                     for si in s] for j in range(5)])
+    A = phi @ phi.T
+    B = phi @ kp
+    A[0] = 0; A[0, 0] = 1; B[0] = kp[0]
+    A[-1] = 0; A[-1, -1] = 1; B[-1] = kp[-1]
+    np.testing.assert_allclose(vals["fit"], np.linalg.solve(A, B), rtol=0, atol=1e-12)
+    # the frame: first axis along the tangent, turned by 30 degrees about it
+    w, x, y, z = vals["ttq"][0]
+    R = np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)],
+                  [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
+                  [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
+    t = np.array([1., 2., .5]) / np.linalg.norm([1., 2., .5])
+    np.testing.assert_allclose(R[:, 0], t, atol=1e-14)
+    e2 = np.array([0., 1., 0.]) - t * t[1]
+    e2 /= np.linalg.norm(e2)
+    ang = np.radians(30.)
+    np.testing.assert_allclose(R[:, 1], np.cos(ang) * e2 + np.sin(ang) * np.cross(t, e2), atol=1e-14)
+
+
 @pytest.mark.gpu
 def test_blade_interface_rotating_beam_and_windio():
     """BladeInterface (include/kynema_b200_interfaces.hpp) on the reference's
