@@ -366,6 +366,42 @@ def main() -> None:
         for i in ids32:
             ctx.destroy_model(int(i))
 
+        # accuracy of the FP32 form on the EI-swept batch (EA/EI over three
+        # decades, conditioned tangents ~2e7..3e9): the same steps in both forms,
+        # per-beam tip-displacement and root-load errors against the FP64 form
+        # (which reproduces the FP64 oracle to 1e-10, tests/test_gpu_parity.py)
+        acc_ids = {}
+        for form in (0, 1):
+            acc_ids[form] = np.array([ctx.create_model(W.precision_cantilever_model(d).pack())
+                                      for d in draws], dtype=np.int32)
+        pa = {}
+        for form in (0, 1):
+            pp = W.batch_params()
+            pp.precision, pp.refine_iters = form, args.refine
+            pa[form] = device_leg(acc_ids[form], pp, False)
+        both = pa[0]["ok_all"] & pa[1]["ok_all"]
+        a, b = pa[0]["q"][tips, :3], pa[1]["q"][tips, :3]
+        tip_rel = (np.abs(b - a).max(axis=1) / np.maximum(np.abs(a).max(axis=1), 1e-300))[both]
+        root_rel = []
+        for i in np.flatnonzero(both):
+            la = ctx.state(int(acc_ids[0][i]), "lambda")
+            lb = ctx.state(int(acc_ids[1][i]), "lambda")
+            root_rel.append(float(np.abs(lb - la).max() / max(np.abs(la).max(), 1e-300)))
+        root_rel = np.array(root_rel)
+
+        def stats(x):
+            return {"median": float(np.median(x)), "p99": float(np.percentile(x, 99)),
+                    "max": float(x.max())} if x.size else None
+        prec["accuracy_ei_swept_batch"] = {
+            "workload": f"{args.beams} beams of the batch with bending/torsion stiffness x 10^U(-1,2)",
+            "beams_converged_in_both": int(both.sum()),
+            "ratio_vs_fp64": (pa[1]["conv"] / sum(pa[1]["ms"])) / max(pa[0]["conv"] / sum(pa[0]["ms"]), 1e-300),
+            "tip_rel_err_vs_fp64": stats(tip_rel),
+            "root_load_rel_err_vs_fp64": stats(root_rel)}
+        for form in (0, 1):
+            for i in acc_ids[form]:
+                ctx.destroy_model(int(i))
+
     # ---- e2e: host buffers through the C ABI, wall time per step --------------
     e2e_ms, conv_e = [], 0
     for j in range(args.steps):

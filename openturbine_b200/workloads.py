@@ -14,6 +14,9 @@ stream per model id):
 * ``batch_cantilevers`` -- N cantilevers with nodes U{5..21}, Gauss points
   nodes+2, length U(5, 100) m, rotor-style sections, tip load amplitude
   U(1e3, 1e5) N and frequency U(0.1, 5) Hz.
+* ``precision_cantilever_model`` -- the same batch with the bending and
+  torsion stiffness of each beam scaled log-uniformly in [0.1, 100] (EA/EI
+  swept), for the accuracy report of the FP32 form.
 """
 from __future__ import annotations
 
@@ -163,6 +166,19 @@ def batch_cantilever_model(d: BeamDraw, stiffness_scale: float = 1.0) -> Model:
                      GaussLegendreQuadrature(d.num_nodes + 2))
     m.AddFixedBC(ids[0])
     return m
+
+
+def precision_scale(d: BeamDraw) -> float:
+    """Stiffness scale of the rotational (torsion and bending) block of beam d in
+    the precision batch: log-uniform in [0.1, 100], so that EA/EI sweeps three
+    decades and the conditioned tangent of the first Newton iteration spans
+    ~2e7..3e9 (tests/test_workloads.py measures it on the oracle)."""
+    return float(10.0 ** rng_for(d.model_id + 2_000_000).uniform(-1.0, 2.0))
+
+
+def precision_cantilever_model(d: BeamDraw) -> Model:
+    """The batch cantilever of draw d with its EI scaled by precision_scale(d)."""
+    return batch_cantilever_model(d, stiffness_scale=precision_scale(d))
 
 
 def batch_params(max_iter: int = 10) -> StepParameters:
