@@ -42,6 +42,8 @@ struct DevModel {
     KBeam* d_kt = nullptr;           // the same records resident on the device (plans gather them)
     std::vector<int> node_base;      // per beam: first global node when its nodes are contiguous, else -1
     int def_nt[2] = {0, 0};          // default threads per CTA, FP64 / FP32 form
+    int tuned_nt[2] = {0, 0};        // tuned threads per CTA (0: none), cached per form
+    unsigned long long tuned_gen[2] = {~0ull, ~0ull};  // tuned-table generation of that cache
     bool lump = false;               // some beam carries point masses or springs
     int smem_nt[2][3] = {};          // dynamic smem for 128 / 256 / 512 threads, per form
     double work = 0.;                // largest beam's N^2 Q + 72 (N-1)^3 (ordering in buckets)
@@ -51,6 +53,19 @@ struct DevModel {
     size_t bytes = 0;
     int last_status = KYN_OK;
     int last_iters = 0;
+};
+
+// One model of a plan being built; bucket key: (point masses/springs, cluster
+// size, threads, CTAs per SM class); larger work first.
+struct Entry {
+    int model_index;
+    int cluster;
+    int nt;
+    int cls;
+    int smem;
+    double work;
+    DevModel* m;
+    bool lump;
 };
 
 struct ClassKey {
@@ -171,6 +186,10 @@ struct kyn_ctx {
     cudaEvent_t fork = nullptr;
     cudaEvent_t join[kBucketStreams] = {};
     std::unordered_map<int, std::unique_ptr<DevModel>> models;
+    std::vector<DevModel*> by_id;         // model id -> model (ids are dense and never reused)
+    std::vector<Entry> plan_entries_tmp, plan_sorted_tmp;  // plan build buffers (reused)
+    std::vector<uint64_t> plan_keys_tmp;
+    unsigned long long tuned_gen = 0;     // bumped whenever the tuned table changes
     int next_id = 0;
     std::string err;
     bool record = false;
@@ -229,8 +248,13 @@ int set_err(kyn_ctx* c, int code, const std::string& msg) {
     } while (0)
 
 DevModel* find_model(kyn_ctx* c, int id) {
-    auto it = c->models.find(id);
-    return it == c->models.end() ? nullptr : it->second.get();
+    return (id >= 0 && static_cast<size_t>(id) < c->by_id.size()) ? c->by_id[id] : nullptr;
+}
+
+void register_model(kyn_ctx* c, int id, std::unique_ptr<DevModel> m) {
+    if (c->by_id.size() <= static_cast<size_t>(id)) c->by_id.resize(static_cast<size_t>(id) + 1, nullptr);
+    c->by_id[id] = m.get();
+    c->models[id] = std::move(m);
 }
 
 StepCoeffs make_coeffs(const kyn_step_params* p) {
@@ -410,42 +434,45 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
     plan->precision = precision;
     const int f = (precision == KYN_PRECISION_FP32_REFINED) ? 1 : 0;
     const int rbytes = f ? 4 : 8;
-    // bucket key: (point masses/springs, cluster size, threads, CTAs per SM
-    // class); larger work first
-    struct Entry {
-        int model_index;
-        int cluster;
-        int nt;
-        int cls;
-        int smem;
-        double work;
-        DevModel* m;
-        bool lump;
-    };
-    std::vector<Entry> entries;
-    entries.reserve(n);
+    std::vector<Entry>& all = c->plan_entries_tmp;
+    all.clear();
+    all.reserve(n);
+    std::vector<uint64_t>& keys = c->plan_keys_tmp;
+    keys.clear();
+    keys.reserve(n);
+    if (n >= (1 << 26)) return set_err(c, KYN_ERR_UNSUPPORTED, "more than 2^26 models in one step");
     size_t nbeams = 0;
     for (int i = 0; i < n; ++i) {
         DevModel* m = find_model(c, ids[i]);
         if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id in step list");
         int nt = m->def_nt[f];
         if (!c->tuned.empty()) {
-            const auto tuned = c->tuned.find(class_key(m->host, precision));
-            if (tuned != c->tuned.end()) nt = tuned->second;
+            if (m->tuned_gen[f] != c->tuned_gen) {  // per-model cache of the tuned table
+                const auto tuned = c->tuned.find(class_key(m->host, precision));
+                m->tuned_nt[f] = (tuned != c->tuned.end()) ? tuned->second : 0;
+                m->tuned_gen[f] = c->tuned_gen;
+            }
+            if (m->tuned_nt[f] > 0) nt = m->tuned_nt[f];
         }
         const int smem = m->smem_nt[f][nt_index(nt)];
-        entries.push_back({i, static_cast<int>(m->kt.size()), nt, ctas_per_sm(rbytes, nt, smem), smem,
-                           m->work, m, m->lump});
+        const int cluster = static_cast<int>(m->kt.size());
+        const int cls = ctas_per_sm(rbytes, nt, smem);
+        all.push_back({i, cluster, nt, cls, smem, m->work, m, m->lump});
+        // one 64-bit sort key: masses/springs last, larger clusters first, more
+        // threads first, fewer CTAs per SM first, more work first, then model order
+        const uint64_t work = static_cast<uint64_t>(std::min(m->work, 4194303.));
+        keys.push_back((static_cast<uint64_t>(m->lump) << 63) |
+                       (static_cast<uint64_t>(15 - std::min(cluster, 15)) << 59) |
+                       (static_cast<uint64_t>(2 - nt_index(nt)) << 57) |
+                       (static_cast<uint64_t>(std::min(cls, 15)) << 53) |
+                       ((4194303ull - work) << 31) | static_cast<uint64_t>(i));
         nbeams += m->kt.size();
     }
-    std::sort(entries.begin(), entries.end(), [](const Entry& a, const Entry& b) {
-        if (a.lump != b.lump) return b.lump;
-        if (a.cluster != b.cluster) return a.cluster > b.cluster;
-        if (a.nt != b.nt) return a.nt > b.nt;
-        if (a.cls != b.cls) return a.cls < b.cls;
-        if (a.work != b.work) return a.work > b.work;
-        return a.model_index < b.model_index;
-    });
+    std::sort(keys.begin(), keys.end());
+    std::vector<Entry>& entries = c->plan_sorted_tmp;
+    entries.clear();
+    entries.reserve(n);
+    for (uint64_t k : keys) entries.push_back(all[static_cast<size_t>(k & ((1ull << 31) - 1))]);
     // The record sources go through a pinned staging buffer (one DMA) and a
     // gather on the device; wait for the previous plan's upload before refilling it
     if (c->plan_upload_pending) {
@@ -786,6 +813,7 @@ void kyn_ctx_destroy(kyn_ctx* c) {
         if (kv.second->d_kt) cudaFree(kv.second->d_kt);
     }
     c->models.clear();
+    c->by_id.clear();
     if (c->pool_kbeams) cudaFree(c->pool_kbeams);
     if (c->pool_hsrc) cudaFreeHost(c->pool_hsrc);
     if (c->pool_dsrc) cudaFree(c->pool_dsrc);
@@ -921,7 +949,7 @@ int kyn_model_create(kyn_ctx* c, const kyn_model_desc* desc) {
         if (urc != KYN_OK) return urc;
     }
     const int id = c->next_id++;
-    c->models[id] = std::move(m);
+    register_model(c, id, std::move(m));
     return id;
 }
 
@@ -936,6 +964,7 @@ int kyn_model_destroy(kyn_ctx* c, int id) {
     if (m->d_dump) KYN_CUDA(c, cudaFreeAsync(m->d_dump, c->stream));
     if (m->d_kt) KYN_CUDA(c, cudaFreeAsync(m->d_kt, c->stream));
     c->used -= m->bytes;
+    c->by_id[id] = nullptr;
     c->models.erase(id);
     // Cached plans, transfer plans and prescribed-motion targets built before
     // this call are not reused (each compares the count with the one it was
@@ -1550,7 +1579,7 @@ int clone_model(kyn_ctx* c, int id) {
         if (urc != KYN_OK) return urc;
     }
     const int nid = c->next_id++;
-    c->models[nid] = std::move(m);
+    register_model(c, nid, std::move(m));
     return nid;
 }
 
@@ -1591,8 +1620,8 @@ extern "C" int kyn_autotune(kyn_ctx* c, const int* ids, int n, const kyn_step_pa
             clones.push_back(cid);
         }
         if (clones.empty()) continue;
-        const HostModel& h = c->models[clones[0]]->host;
-        const int def_nt = c->models[clones[0]]->def_nt[rb == 4 ? 1 : 0];
+        const HostModel& h = find_model(c, clones[0])->host;
+        const int def_nt = find_model(c, clones[0])->def_nt[rb == 4 ? 1 : 0];
         // Every candidate is timed on the same two steps from the sources'
         // current state (the clones are reset before the warm-up and before the
         // timed steps), so that Newton iteration counts match across candidates.
@@ -1610,6 +1639,7 @@ extern "C" int kyn_autotune(kyn_ctx* c, const int* ids, int n, const kyn_step_pa
             for (const HostBeam& b : h.beams) fits &= beam_smem(b.N, b.Q, b.nc, rb, nt, h.hub >= 0) <= kMaxDynSmem;
             if (!fits || (key.beams > 1 && key.beams * nt > 1024 * 8)) continue;
             c->tuned[key] = nt;
+            ++c->tuned_gen;
             c->plan.reset();
             Plan* plan = nullptr;
             rc = get_plan(c, clones.data(), static_cast<int>(clones.size()), p->precision, &plan);
@@ -1635,6 +1665,7 @@ extern "C" int kyn_autotune(kyn_ctx* c, const int* ids, int n, const kyn_step_pa
         if (def_ms > 0.f && best_nt != def_nt && best_ms > 0.97f * def_ms) best_nt = def_nt;
         if (best_nt > 0) c->tuned[key] = best_nt;
         else c->tuned.erase(key);
+        ++c->tuned_gen;
         c->plan.reset();
         for (int cid : clones) kyn_model_destroy(c, cid);
         if (rc != KYN_OK) break;
