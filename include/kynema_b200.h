@@ -56,13 +56,22 @@ enum {
 
 /* Constraint types: same numbering as constraints::ConstraintType
  * (src/constraints/constraint_type.hpp:9-24).  This path implements the two
- * single-node boundary conditions used by beams and rotors and the two
- * six-row joints that tie blade roots to a hub node. */
+ * single-node boundary conditions used by beams and rotors, the two six-row
+ * joints that tie blade roots to a hub node, and the five-row revolute joint
+ * that lets a drive train (hub, or azimuth node rigidly holding the hub) turn
+ * about a shaft held by a boundary condition. */
 enum {
     KYN_CONSTRAINT_FIXED_BC = 1,
     KYN_CONSTRAINT_PRESCRIBED_BC = 2,
     KYN_CONSTRAINT_RIGID_JOINT = 3,  /* base node (hub) to target node, six DOFs
                                         (src/constraints/calculate_rigid_joint_constraint.hpp) */
+    KYN_CONSTRAINT_REVOLUTE_JOINT = 4, /* five rows: the target turns freely about the
+                                        joint axis (constraint_axis, or the base-to-target
+                                        direction when it is zero; src/constraints/
+                                        constraints.hpp:294-319); a torque about that axis,
+                                        u[0] of kyn_model_set_prescribed, acts on the target
+                                        (src/constraints/calculate_revolute_joint_constraint.hpp,
+                                        calculate_revolute_joint_force.hpp) */
     KYN_CONSTRAINT_ROTATION_CONTROL = 5  /* a rigid joint whose target is turned by a
                                         commanded angle about constraint_axis (normalised
                                         here as in src/constraints/constraints.hpp:321-328);
@@ -86,8 +95,13 @@ enum {
     KYN_FIELD_A = 7,       /* [nodes][6] algorithmic acceleration          */
     KYN_FIELD_F = 8,       /* [nodes][6] external nodal forces (state.f)   */
     KYN_FIELD_LAMBDA = 9,  /* [constraints][6] Lagrange multipliers        */
-    KYN_FIELD_TANGENT = 10 /* [nodes][6][6] tangent operator, stored
+    KYN_FIELD_TANGENT = 10, /* [nodes][6][6] tangent operator, stored
                               transposed as in CalculateTangentOperator     */
+    KYN_FIELD_CONSTRAINT_OUTPUT = 11 /* [constraints][3] Constraints::output: for a
+                              revolute joint the rotation, angular velocity and
+                              angular acceleration about its axis
+                              (src/constraints/calculate_revolute_joint_output.hpp);
+                              zero for the other types                          */
 };
 
 /* Load channels for kyn_model_set_loads. */
@@ -225,7 +239,8 @@ KYN_API int kyn_model_set_loads(kyn_ctx* ctx, int model_id, int which, const dou
 
 /* Replaces Constraints::UpdateDisplacement (src/constraints/constraints.hpp:338-343).
  * For a KYN_CONSTRAINT_ROTATION_CONTROL constraint u[0] is the commanded angle
- * (rad) and u[1..6] are ignored. */
+ * (rad), for a KYN_CONSTRAINT_REVOLUTE_JOINT the torque about the joint axis;
+ * u[1..6] are ignored for both. */
 KYN_API int kyn_model_set_prescribed(kyn_ctx* ctx, int model_id, int constraint_id, const double u[7]);
 
 /* Replaces kynema::Step (src/step/step.hpp:42-124) for a batch of models:

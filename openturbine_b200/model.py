@@ -30,6 +30,7 @@ import numpy as np
 FIXED_BC = 1
 PRESCRIBED_BC = 2
 RIGID_JOINT = 3
+REVOLUTE_JOINT = 4
 ROTATION_CONTROL = 5
 INVALID_NODE_ID = 0  # Model::InvalidNodeID
 
@@ -491,8 +492,22 @@ class Model:
         self.controls_[cid] = control
         return cid
 
+    def AddRevoluteJointConstraint(self, node_ids, axis, torque=None) -> int:
+        """src/model/model.hpp:529-541 AddRevoluteJointConstraint({base, target},
+        axis, torque): the target turns freely about `axis` (a zero axis takes
+        the base-to-target direction).  `torque` stands for the reference's
+        double*, read like a RotationControl's control before each step;
+        Context.set_control(model_id, constraint_id, torque) passes it to a
+        created model."""
+        cid = len(self.constraints_)
+        self.constraints_.append(Constraint(cid, REVOLUTE_JOINT, (int(node_ids[0]), int(node_ids[1])),
+                                            tuple(float(x) for x in axis)))
+        self.controls_[cid] = torque
+        return cid
+
     def Controls(self) -> dict:
-        """Constraint id -> control object of the RotationControl constraints."""
+        """Constraint id -> control object of the RotationControl and
+        RevoluteJoint constraints."""
         return dict(self.controls_)
 
     def NumConstraints(self) -> int:

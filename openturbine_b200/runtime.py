@@ -20,9 +20,9 @@ OK, NOT_CONVERGED = 0, 1
 ERR = {-1: "INVALID", -2: "UNSUPPORTED", -3: "CUDA", -4: "BUDGET", -5: "NONFINITE",
        -6: "SINGULAR", -7: "NOT_FOUND", -8: "NO_DEVICE"}
 FIELD = {"x0": 0, "x": 1, "q": 2, "q_prev": 3, "q_delta": 4, "v": 5, "vd": 6, "a": 7, "f": 8,
-         "lambda": 9, "tangent": 10}
+         "lambda": 9, "tangent": 10, "output": 11}
 WIDTH = {"x0": 7, "x": 7, "q": 7, "q_prev": 7, "q_delta": 6, "v": 6, "vd": 6, "a": 6, "f": 6,
-         "lambda": 6, "tangent": 36}
+         "lambda": 6, "tangent": 36, "output": 3}
 LOAD_NODE_FX, LOAD_STATE_F = 0, 1
 OPT_RECORD_SYSTEM, OPT_PHASE_TIMING, OPT_CUDA_GRAPH = 1, 2, 3
 
@@ -167,8 +167,9 @@ class Context:
         self._check(self.lib.kyn_model_set_prescribed(self.h, mid, cid, v.ctypes.data_as(_dp)))
 
     def set_control(self, mid: int, cid: int, value: float) -> None:
-        """The commanded angle of a RotationControl constraint (the value the
-        reference reads through its control pointer before each step)."""
+        """The commanded angle of a RotationControl constraint, or the torque
+        of a RevoluteJoint (the value the reference reads through its control
+        pointer before each step)."""
         self.set_prescribed(mid, cid, [float(value), 0.0, 0.0, 1.0, 0.0, 0.0, 0.0])
 
     # stepping
@@ -267,7 +268,7 @@ class Context:
     # results
     def state(self, mid: int, field: str) -> np.ndarray:
         info = self._info[mid]
-        rows = info.num_constraints if field == "lambda" else info.num_nodes
+        rows = info.num_constraints if field in ("lambda", "output") else info.num_nodes
         out = np.zeros((rows, WIDTH[field]))
         self._check(self.lib.kyn_get_state(self.h, mid, FIELD[field], out.ctypes.data_as(_dp)))
         return out

@@ -452,6 +452,8 @@ struct OConstraint {
     int base = 0, target = 0;
     double X0[3] = {0., 0., 0.};
     double axis[3] = {0., 0., 0.};   // RotationControl: axes row 0 (unit axis)
+    double axes[9] = {};             // RevoluteJoint: joint frame, row 0 = joint axis
+    double output[3] = {0., 0., 0.}; // RevoluteJoint: rotation, rate, acceleration
     double input[7] = {0., 0., 0., 1., 0., 0., 0.};
     double lambda[6] = {0., 0., 0., 0., 0., 0.};
     double res[6] = {};
@@ -666,10 +668,15 @@ void update_spring(orc_model& m, OSpring& S) {
 
 // src/constraints/calculate_constraint_residual_gradient.hpp:60-199 (FixedBC, PrescribedBC)
 void update_rigid_joint(orc_model& m, OConstraint& C);
+void update_revolute_joint(orc_model& m, OConstraint& C);
 
 void update_constraint(orc_model& m, OConstraint& C) {
     if (C.type == KYN_CONSTRAINT_RIGID_JOINT || C.type == KYN_CONSTRAINT_ROTATION_CONTROL) {
         update_rigid_joint(m, C);
+        return;
+    }
+    if (C.type == KYN_CONSTRAINT_REVOLUTE_JOINT) {
+        update_revolute_joint(m, C);
         return;
     }
     const double* nu = &m.q[C.target * 7];
@@ -751,6 +758,76 @@ void update_rigid_joint(orc_model& m, OConstraint& C) {
     gemv(false, 6, 6, 1., C.t_grad_trans, 6, C.lambda, 0., C.t_lambda_res);
 }
 
+// src/constraints/calculate_revolute_joint_constraint.hpp:19-113 and
+// calculate_revolute_joint_force.hpp:19-45 with the RevoluteJoint branch of
+// calculate_constraint_residual_gradient.hpp:388-465.  Five rows: the relative
+// translation, and the two dot products (R2 z0).(R1 x0), (R2 y0).(R1 x0) that
+// vanish while the target's frame keeps the joint axis; row 5 of the 6x6
+// blocks stays zero.  The torque input[0] about R2 x0 joins the target's rows.
+void update_revolute_joint(orc_model& m, OConstraint& C) {
+    const double* bu = &m.q[C.base * 7];
+    const double* tu = &m.q[C.target * 7];
+    const double* x0 = C.axes;
+    const double* y0 = C.axes + 3;
+    const double* z0 = C.axes + 6;
+    const double R1[4] = {bu[3], bu[4], bu[5], bu[6]};
+    const double R2[4] = {tu[3], tu[4], tu[5], tu[6]};
+    const V3 R1X0 = rotate_vec(R1, C.X0);
+    for (int c = 0; c < 3; ++c) C.res[c] = tu[c] + C.X0[c] - bu[c] - R1X0[c];
+    const V3 x = rotate_vec(R1, x0);
+    const V3 y = rotate_vec(R2, y0);
+    const V3 z = rotate_vec(R2, z0);
+    C.res[3] = z[0] * x[0] + z[1] * x[1] + z[2] * x[2];
+    C.res[4] = y[0] * x[0] + y[1] * x[1] + y[2] * x[2];
+    C.res[5] = 0.;
+    const double xcz[3] = {x[1] * z[2] - x[2] * z[1], x[2] * z[0] - x[0] * z[2], x[0] * z[1] - x[1] * z[0]};
+    const double xcy[3] = {x[1] * y[2] - x[2] * y[1], x[2] * y[0] - x[0] * y[2], x[0] * y[1] - x[1] * y[0]};
+    M6 tg{}, bg{};
+    for (int c = 0; c < 3; ++c) {
+        tg[c * 7] = 1.;
+        bg[c * 7] = -1.;
+        tg[3 * 6 + 3 + c] = -xcz[c];
+        tg[4 * 6 + 3 + c] = -xcy[c];
+        bg[3 * 6 + 3 + c] = xcz[c];
+        bg[4 * 6 + 3 + c] = xcy[c];
+    }
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) {
+            C.t_grad_trans[i * 6 + j] = tg[j * 6 + i];
+            C.b_grad_trans[i * 6 + j] = bg[j * 6 + i];
+        }
+    gemm(false, false, 6, 6, 6, 1., bg.data(), 6, &m.tangent[C.base * 36], 6, 0., C.b_grad_tan, 6);
+    gemm(false, false, 6, 6, 6, 1., tg.data(), 6, &m.tangent[C.target * 36], 6, 0., C.t_grad_tan, 6);
+    gemv(false, 6, 6, 1., C.b_grad_trans, 6, C.lambda, 0., C.b_lambda_res);
+    gemv(false, 6, 6, 1., C.t_grad_trans, 6, C.lambda, 0., C.t_lambda_res);
+    const V3 ax = rotate_vec(R2, x0);
+    for (int c = 0; c < 3; ++c) {
+        C.sys_res[c] = 0.;
+        C.sys_res[3 + c] = ax[c] * C.input[0];
+    }
+}
+
+// src/constraints/calculate_revolute_joint_output.hpp:24-85: rotation about
+// the joint axis (axis turned by the target's rotation, dotted with the
+// rotation vector of that rotation), angular velocity and acceleration about
+// it.
+void revolute_output(const orc_model& m, OConstraint& C) {
+    const double* u = &m.q[C.target * 7];
+    const double R[4] = {u[3], u[4], u[5], u[6]};
+    const V3 ax = rotate_vec(R, C.axes);
+    double rv[3] = {0., 0., 0.};
+    const double s = std::sqrt(1. - R[0] * R[0]);
+    if (s > 1e-12) {  // src/math/quaternion_operations.hpp QuaternionToRotationVector
+        const double th = 2. * std::acos(R[0]);
+        for (int c = 0; c < 3; ++c) rv[c] = th * R[1 + c] / s;
+    }
+    const double* w = &m.v[C.target * 6 + 3];
+    const double* wd = &m.vd[C.target * 6 + 3];
+    C.output[0] = ax[0] * rv[0] + ax[1] * rv[1] + ax[2] * rv[2];
+    C.output[1] = ax[0] * w[0] + ax[1] * w[1] + ax[2] * w[2];
+    C.output[2] = ax[0] * wd[0] + ax[1] * wd[1] + ax[2] * wd[2];
+}
+
 // Solver of the oracle (bit flags of orc_model::solver_mode): 0 = dense LU
 // with partial pivoting of the whole bordered system (default); bit 1 =
 // elimination of the single-node boundary conditions followed by LU without
@@ -760,7 +837,9 @@ void update_rigid_joint(orc_model& m, OConstraint& C) {
 void solve_eliminated(orc_model& m);
 
 void solve_dense(orc_model& m) {
-    if (m.solver_mode & 1) {
+    bool revolute = false;
+    for (auto& C : m.cons) revolute = revolute || C.type == KYN_CONSTRAINT_REVOLUTE_JOINT;
+    if ((m.solver_mode & 1) && !revolute) {
         solve_eliminated(m);
         return;
     }
@@ -1085,6 +1164,9 @@ int step_impl(orc_model& m, const Params& P, int* iters) {
     for (int n = 0; n < m.num_nodes; ++n)
         for (int c = 0; c < 6; ++c) m.a[n * 6 + c] += (1. - P.af) / (1. - P.am) * m.vd[n * 6 + c];
     update_global_position(m);
+    // src/step/step.hpp:105-115 (CalculateConstraintOutput)
+    for (auto& C : m.cons)
+        if (C.type == KYN_CONSTRAINT_REVOLUTE_JOINT) revolute_output(m, C);
     if (iters) *iters = static_cast<int>(m.conv.size());
     return KYN_OK;
 }
@@ -1333,7 +1415,8 @@ orc_model* orc_model_create(const kyn_model_desc* d, char* err, int errlen) {
     for (int c = 0; c < d->num_constraints; ++c) {
         OConstraint& C = m->cons[c];
         C.type = d->constraint_type[c];
-        const bool joint = C.type == KYN_CONSTRAINT_RIGID_JOINT || C.type == KYN_CONSTRAINT_ROTATION_CONTROL;
+        const bool joint = C.type == KYN_CONSTRAINT_RIGID_JOINT || C.type == KYN_CONSTRAINT_ROTATION_CONTROL ||
+                           C.type == KYN_CONSTRAINT_REVOLUTE_JOINT;
         if (C.type != KYN_CONSTRAINT_FIXED_BC && C.type != KYN_CONSTRAINT_PRESCRIBED_BC && !joint) {
             bad(err, errlen, "constraint type outside this path");
             delete m;
@@ -1353,9 +1436,11 @@ orc_model* orc_model_create(const kyn_model_desc* d, char* err, int errlen) {
         }
         C.base_active = joint ? 6 : 0;
         C.target_active = 6;
+        // src/constraints/constraint_type.hpp NumRowsForConstraint: 5 for a revolute joint
+        const int rows = C.type == KYN_CONSTRAINT_REVOLUTE_JOINT ? 5 : 6;
         C.row_first = start_row;
-        C.row_last = start_row + 6;
-        start_row += 6;
+        C.row_last = start_row + rows;
+        start_row += rows;
         const double axis[3] = {d->constraint_axis ? d->constraint_axis[c * 3] : 0.,
                                 d->constraint_axis ? d->constraint_axis[c * 3 + 1] : 0.,
                                 d->constraint_axis ? d->constraint_axis[c * 3 + 2] : 0.};
@@ -1373,6 +1458,38 @@ orc_model* orc_model_create(const kyn_model_desc* d, char* err, int errlen) {
                     return nullptr;
                 }
                 for (int k = 0; k < 3; ++k) C.axis[k] = axis[k] / nrm;
+            }
+            if (C.type == KYN_CONSTRAINT_REVOLUTE_JOINT) {
+                // src/constraints/constraints.hpp:294-319: x_hat = unit(axis), or
+                // unit(X0) for a zero axis; the frame is the rotation taking
+                // (1, 0, 0) to x_hat, its rows the joint axes.
+                const double na = std::sqrt(axis[0] * axis[0] + axis[1] * axis[1] + axis[2] * axis[2]);
+                const double* src = na != 0. ? axis : C.X0;
+                const double ns = std::sqrt(src[0] * src[0] + src[1] * src[1] + src[2] * src[2]);
+                if (!(ns > 0.)) {
+                    bad(err, errlen, "revolute joint needs an axis or distinct node positions");
+                    delete m;
+                    return nullptr;
+                }
+                const double xh[3] = {src[0] / ns, src[1] / ns, src[2] / ns};
+                const double cp[3] = {0., -xh[2], xh[1]};  // (1, 0, 0) x x_hat
+                const double dp = xh[0];
+                if (!(1. + dp > 0.)) {
+                    bad(err, errlen, "revolute joint axis along -x is outside this path");
+                    delete m;
+                    return nullptr;
+                }
+                const double k = 1. / (1. + dp);
+                double* R = C.axes;
+                R[0] = cp[0] * cp[0] * k + dp;
+                R[1] = cp[1] * cp[0] * k + cp[2];
+                R[2] = cp[2] * cp[0] * k - cp[1];
+                R[3] = cp[0] * cp[1] * k - cp[2];
+                R[4] = cp[1] * cp[1] * k + dp;
+                R[5] = cp[2] * cp[1] * k + cp[0];
+                R[6] = cp[0] * cp[2] * k + cp[1];
+                R[7] = cp[1] * cp[2] * k - cp[0];
+                R[8] = cp[2] * cp[2] * k + dp;
             }
         } else {
             const double idq[7] = {0., 0., 0., 1., 0., 0., 0.};
@@ -1550,6 +1667,11 @@ int orc_get_state(const orc_model* m, int field, double* out) {
         case KYN_FIELD_LAMBDA: {
             for (size_t c = 0; c < m->cons.size(); ++c)
                 for (int k = 0; k < 6; ++k) out[c * 6 + k] = m->cons[c].lambda[k];
+            return KYN_OK;
+        }
+        case KYN_FIELD_CONSTRAINT_OUTPUT: {
+            for (size_t c = 0; c < m->cons.size(); ++c)
+                for (int k = 0; k < 3; ++k) out[c * 3 + k] = m->cons[c].output[k];
             return KYN_OK;
         }
         default: return KYN_ERR_INVALID;

@@ -21,9 +21,9 @@ _ip = ctypes.POINTER(ctypes.c_int)
 _lp = ctypes.POINTER(ctypes.c_long)
 
 FIELD = {"x0": 0, "x": 1, "q": 2, "q_prev": 3, "q_delta": 4, "v": 5, "vd": 6, "a": 7, "f": 8,
-         "lambda": 9, "tangent": 10}
+         "lambda": 9, "tangent": 10, "output": 11}
 WIDTH = {"x0": 7, "x": 7, "q": 7, "q_prev": 7, "q_delta": 6, "v": 6, "vd": 6, "a": 6, "f": 6,
-         "lambda": 6, "tangent": 36}
+         "lambda": 6, "tangent": 36, "output": 3}
 
 
 def build(force: bool = False) -> str:
@@ -115,7 +115,7 @@ class OracleModel:
         lib().orc_predict_and_assemble(self.h, ctypes.byref(c))
 
     def state(self, field: str) -> np.ndarray:
-        rows = self.info.num_constraints if field == "lambda" else self.info.num_nodes
+        rows = self.info.num_constraints if field in ("lambda", "output") else self.info.num_nodes
         out = np.zeros((rows, WIDTH[field]))
         lib().orc_get_state(self.h, FIELD[field], _d(out))
         return out

@@ -12,7 +12,9 @@ Sources (paths relative to the reference project root):
   tests/regression_tests/regression/test_cantilever_beam.cpp expected tip q
   tests/regression_tests/regression/test_solver.cpp          assembled b, x, err
   tests/regression_tests/regression/test_rotating_beam.cpp   expected q (prescribed
-                                                             root; rotation control)
+                                                             root; rotation control;
+                                                             revolute joint, generator
+                                                             torque)
   tests/unit_tests/system/beams/test_curved_beam.hpp         kernel-level data
   tests/regression_tests/interfaces/test_blade_interface.cpp + its WindIO file
                                                              IEA-15 blade input, tip
@@ -183,6 +185,28 @@ def main(ref: str) -> None:
                "fixed_hub": {"steps": 10, "q": view_after(rb[r1:r2], "state.q,"), "tolerance": 1e-6},
                "prescribed_hub": {"steps": 100, "rv_root": rv, "tolerance": max(tol)}},
               open(os.path.join(out_dir, "rotation_control.json"), "w"), indent=1)
+
+    # ---- revolute joint (ground - revolute - hub - rigid - root; generator torque) --
+    j0 = rb.index("TEST(RotatingBeamTest, RevoluteJointConstraint)")
+    j1 = rb.index("void GeneratorTorqueWithAxisTilt(")
+    gen = {}
+    for name, key in (("GeneratorTorque_Tilt0", "tilt0"), ("GeneratorTorque_Tilt90", "tilt90")):
+        t0 = rb.index("TEST(RotatingBeamTest, " + name + ")")
+        call = rb.index("GeneratorTorqueWithAxisTilt(", t0)
+        b1 = _block(rb, call)
+        p2 = rb.index(b1, call) + len(b1)
+        b2 = _block(rb, p2)
+        p3 = rb.index(b2, p2) + len(b2)
+        b3 = _block(rb, p3)
+        gen[key] = {"azimuth_q": [float(x) for x in re.findall(NUM, b1)],
+                    "azimuth_v": [float(x) for x in re.findall(NUM, b2)],
+                    "output": [float(x) for x in re.findall(NUM, b3)]}
+    gen["tilt0"]["tilt"] = 0.0
+    gen["tilt90"]["tilt"] = "pi/2"
+    json.dump({"source": "tests/regression_tests/regression/test_rotating_beam.cpp",
+               "revolute": {"steps": 5, "q": view_after(rb[j0:j1], "state.q,"), "tolerance": 1e-6},
+               "generator_torque": dict(gen, steps=10, torque=100.0, tolerance=1e-6)},
+              open(os.path.join(out_dir, "revolute_joint.json"), "w"), indent=1)
 
     # ---- point masses and springs -------------------------------------------------
     def near_calls(text: str, name: str):

@@ -3,6 +3,8 @@
 Fixtures come from tests/golden/make_golden.py (reference test sources read as
 text).  Tolerances are the reference tests' own.
 """
+import math
+
 import numpy as np
 import pytest
 
@@ -158,6 +160,41 @@ def test_rotation_control_prescribed_hub_hundred_steps():
         assert st == 0
     rv = quaternion_to_rotation_vector(o.state("q")[0, 3:])
     np.testing.assert_allclose(rv, g["rv_root"], rtol=0, atol=g["tolerance"])
+
+
+def test_revolute_joint_five_steps():
+    """test_rotating_beam.cpp:516-579 (RevoluteJointConstraint): q of the 6
+    blade nodes, the hub and the ground after 5 steps at the test's 1e-6."""
+    from tests.workloads_ref import revolute_joint_test_model
+    g = load_golden("revolute_joint.json")["revolute"]
+    m, p, rj = revolute_joint_test_model()
+    o = OracleModel(m.pack())
+    assert o.info.num_dofs == 8 * 6 + 6 + 5 + 6
+    for _ in range(g["steps"]):
+        o.set_prescribed(rj, [0., 0., 0., 1., 0., 0., 0.])
+        st, _ = o.step(p)
+        assert st == 0
+    np.testing.assert_allclose(o.state("q").ravel(), g["q"], rtol=0, atol=g["tolerance"])
+
+
+@pytest.mark.parametrize("key", ["tilt0", "tilt90"])
+def test_generator_torque(key):
+    """test_rotating_beam.cpp:581-680 (GeneratorTorque_Tilt0 / _Tilt90): after
+    10 steps under a 100 N m generator torque, the azimuth node's q and v and
+    the revolute joint's output (rotation, rate, acceleration about the shaft)
+    at the test's 1e-6."""
+    from tests.workloads_ref import generator_torque_model
+    g = load_golden("revolute_joint.json")["generator_torque"]
+    tilt = 0.0 if key == "tilt0" else math.pi / 2.
+    m, p, rj, az = generator_torque_model(tilt)
+    o = OracleModel(m.pack())
+    for _ in range(g["steps"]):
+        o.set_prescribed(rj, [g["torque"], 0., 0., 1., 0., 0., 0.])
+        st, _ = o.step(p)
+        assert st == 0
+    np.testing.assert_allclose(o.state("q")[az], g[key]["azimuth_q"], rtol=0, atol=g["tolerance"])
+    np.testing.assert_allclose(o.state("v")[az], g[key]["azimuth_v"], rtol=0, atol=g["tolerance"])
+    np.testing.assert_allclose(o.state("output")[rj], g[key]["output"], rtol=0, atol=g["tolerance"])
 
 
 def test_mass_external_force_velocity():

@@ -125,6 +125,54 @@ def rotation_control_test_model(prescribed_hub: bool = False):
     return m, StepParameters(True, 5, 0.01, 0.9), rc, bc
 
 
+def revolute_joint_test_model():
+    """tests/regression_tests/regression/test_rotating_beam.cpp:516-560
+    (RevoluteJointConstraint): a blade on a hub node that turns about z on a
+    revolute joint from a fixed ground node one unit below it, zero torque,
+    blade spinning at 0.1 rad/s about z.  Returns (model, params, revolute
+    constraint id); node order: blade (6), hub, ground."""
+    m = Model()
+    m.SetGravity(0., 0., 0.)
+    ids = [m.AddNode().SetElemLocation(s).SetPosition(10 * s, 0., 0., 1., 0., 0., 0.).Build()
+           for s in GLL6_S]
+    m.AddBeamElement(ids, [BeamSection(0., COMPOSITE_MASS, COMPOSITE_STIFF),
+                           BeamSection(1., COMPOSITE_MASS, COMPOSITE_STIFF)], GAUSS7)
+    m.TranslateBeam(0, [2.0, 0., 0.])
+    m.SetBeamVelocityAboutPoint(0, [0., 0., 0., 0., 0., 0.1], [0., 0., 0.])
+    hub = m.AddNode().SetPosition(0., 0., 0., 1., 0., 0., 0.).Build()
+    ground = m.AddNode().SetPosition(0., 0., -1., 1., 0., 0., 0.).Build()
+    m.AddFixedBC(ground)
+    rj = m.AddRevoluteJointConstraint([ground, hub], [0., 0., 0.], np.zeros(1))
+    m.AddRigidJointConstraint([hub, ids[0]])
+    return m, StepParameters(True, 5, 0.01, 0.9), rj
+
+
+def generator_torque_model(tilt: float):
+    """tests/regression_tests/regression/test_rotating_beam.cpp:581-650
+    (GeneratorTorqueWithAxisTilt): the blade, tilted by `tilt` about x, on a
+    hub rigidly held by an azimuth node that turns on a revolute joint about
+    (0, sin tilt, cos tilt) from a fixed shaft base, with a generator torque of
+    100.  Returns (model, params, revolute constraint id, azimuth node id)."""
+    m = Model()
+    m.SetGravity(0., 0., 0.)
+    q_tilt = RotationVectorToQuaternion([tilt, 0., 0.])
+    ids = [m.AddNode().SetElemLocation(s).SetPosition(10 * s, 0., 0., 1., 0., 0., 0.).Build()
+           for s in GLL6_S]
+    m.AddBeamElement(ids, [BeamSection(0., COMPOSITE_MASS, COMPOSITE_STIFF),
+                           BeamSection(1., COMPOSITE_MASS, COMPOSITE_STIFF)], GAUSS7)
+    m.TranslateBeam(0, [2.0, 0., 0.])
+    m.RotateBeamAboutPoint(0, q_tilt, [0., 0., 0.])
+    shaft = m.AddNode().SetPosition(0., 0., 0., 1., 0., 0., 0.).Build()
+    azimuth = m.AddNode().SetPosition(0., 0., 0., 1., 0., 0., 0.).Build()
+    hub = m.AddNode().SetPosition(0., math.sin(tilt), math.cos(tilt), 1., 0., 0., 0.).Build()
+    m.AddFixedBC(shaft)
+    rj = m.AddRevoluteJointConstraint([shaft, azimuth], [0., math.sin(tilt), math.cos(tilt)],
+                                      np.array([100.0]))
+    m.AddRigidJointConstraint([azimuth, hub])
+    m.AddRigidJointConstraint([hub, ids[0]])
+    return m, StepParameters(True, 5, 0.01, 0.0), rj, azimuth
+
+
 def rotation_control_inputs(i: int, h: float = 0.01):
     """Pitch angle and hub displacement before step i (0-based) of the two
     rotation-control tests: pitch = t pi/2, azimuth = 0.5 t pi/2 about z."""
