@@ -235,6 +235,14 @@ public:
         check(m_->ctx.get(), kyn_get_state(m_->ctx.get(), m_->id, KYN_FIELD_LAMBDA, out.data()));
         return out;
     }
+    // Constraints::output, [constraints][3]: a revolute joint's rotation, angular
+    // velocity and angular acceleration about its axis
+    // (src/constraints/calculate_revolute_joint_output.hpp)
+    std::vector<double> output() const {
+        std::vector<double> out(m_->info.num_constraints * 3);
+        check(m_->ctx.get(), kyn_get_state(m_->ctx.get(), m_->id, KYN_FIELD_CONSTRAINT_OUTPUT, out.data()));
+        return out;
+    }
 
 private:
     std::shared_ptr<DeviceModel> m_;
@@ -307,6 +315,15 @@ public:
         return cons_.size() - 1;
     }
 
+    // {base (shaft base), target (azimuth or hub)}, joint axis (zero: the
+    // base-to-target direction) and the torque read before every Step
+    // (src/model/model.hpp:529-541 AddRevoluteJointConstraint)
+    size_t AddRevoluteJointConstraint(const std::array<size_t, 2>& nodes,
+                                      const std::array<double, 3>& axis, double* torque) {
+        cons_.push_back({KYN_CONSTRAINT_REVOLUTE_JOINT, nodes[1], {0., 0., 0., 1., 0., 0., 0.},
+                         nodes[0], axis, torque});
+        return cons_.size() - 1;
+    }
     // {base (hub), target}, rotation axis and the control signal read before
     // every Step (src/model/model.hpp:550-562 AddRotationControl)
     size_t AddRotationControl(const std::array<size_t, 2>& nodes, const std::array<double, 3>& axis,

@@ -303,6 +303,11 @@ int ctas_per_sm(int real_bytes, int nt, int smem) {
     return std::max(1, std::min(by_regs, kSmemPerSM / per));
 }
 
+// Hub record kind of a model for make_smem: 0 none, 1 a hub, 2 a drive train.
+int hub_kind(const HostModel& h) {
+    return h.chain.size() > 1 ? 2 : h.hub >= 0 ? 1 : 0;
+}
+
 // Size class of a model for the tuned thread-count table.
 ClassKey class_key(const HostModel& h, int precision) {
     ClassKey k{static_cast<int>(h.beams.size()), 0, 0, 0, precision};
@@ -317,11 +322,12 @@ ClassKey class_key(const HostModel& h, int precision) {
 // Fills the per-model values that plans and transfer plans reuse.
 void prepare_model(DevModel* m) {
     const HostModel& H = m->host;
-    const int hubf = H.hub >= 0;
+    const int hubf = hub_kind(H);
     m->lay.clear();
     m->kt.clear();
     m->work = 0.;
-    m->lump = false;
+    // masses, springs and drive trains run in the LUMP instance
+    m->lump = H.chain.size() > 1;
     for (const HostBeam& hb : H.beams) m->lump |= hb.n_mass + hb.n_spring > 0;
     for (int f = 0; f < 2; ++f) {
         const int rb = f ? 4 : 8;
@@ -365,7 +371,7 @@ void prepare_model(DevModel* m) {
         k.n_mass = hb.n_mass;
         k.n_spring = hb.n_spring;
         k.conv = m->d_conv;
-        k.hub = hubf;
+        k.hub = static_cast<int>(H.chain.size());
         k.hub_con_type = H.hub_con_type;
         m->kt.push_back(k);
     }
@@ -728,7 +734,7 @@ int get_xfer(kyn_ctx* c, const int* ids, int n, int kind, XferPlan** out) {
             beams.push_back(xb);
             elem += b.N;
         }
-        if (m->host.hub >= 0 && kind >= 100) {  // the hub row, from beam 0's copy
+        for (size_t r = 0; r < m->host.chain.size() && kind >= 100; ++r) {  // hub rows, from beam 0's copy
             int hw = 0;
             const int ho = hub_field_offset(kind - 100, &hw);
             if (ho < 0) return set_err(c, KYN_ERR_UNSUPPORTED, "field not kept for a hub node");
@@ -738,8 +744,8 @@ int get_xfer(kyn_ctx* c, const int* ids, int n, int kind, XferPlan** out) {
             xb.N = 1;
             xb.map_off = static_cast<int>(map.size());
             xb.ext_off = off;
-            xb.slab_field = m->d_slab[0] + L0.hub + ho;
-            map.push_back(m->host.hub);
+            xb.slab_field = m->d_slab[0] + L0.hub + static_cast<int>(r) * kHubDoubles + ho;
+            map.push_back(m->host.chain[r]);
             beams.push_back(xb);
         }
         off += (kind == KYN_LOAD_NODE_FX) ? elem * 6 : static_cast<long long>(m->host.num_nodes) * xp->width;
@@ -908,7 +914,7 @@ int kyn_model_create(kyn_ctx* c, const kyn_model_desc* desc) {
     if (rc != KYN_OK) return set_err(c, rc, err);
     size_t bytes = kMaxNewtonIters * sizeof(double);
     for (auto& b : m->host.beams) {
-        const int hubf = m->host.hub >= 0;
+        const int hubf = hub_kind(m->host);
         const int nt = beam_threads(b.N, b.Q, b.nc, sizeof(double), hubf);
         const int sm = std::max(beam_smem(b.N, b.Q, b.nc, sizeof(double), 512, hubf),
                                 beam_smem(b.N, b.Q, b.nc, sizeof(double), nt, hubf));
@@ -1053,12 +1059,15 @@ int kyn_model_set_prescribed(kyn_ctx* c, int id, int cid, const double u[7]) {
     if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
     if (cid < 0 || cid >= m->host.num_constraints)
         return set_err(c, KYN_ERR_INVALID, "constraint id out of range");
-    if (cid == m->host.hub_con) {  // the hub BC: every beam keeps a copy
+    if (cid == m->host.ah_con) return KYN_OK;  // a rigid joint reads no input
+    if (cid == m->host.hub_con || cid == m->host.rev_con) {
+        // the hub BC, or the revolute joint's torque: every beam keeps a copy
+        const int r = cid == m->host.rev_con ? 1 : 0;
         for (size_t bi = 0; bi < m->host.beams.size(); ++bi) {
             const HostBeam& b = m->host.beams[bi];
             const SlabLayout L = make_slab_layout(b.N, b.Q);
-            KYN_CUDA(c, cudaMemcpyAsync(m->d_slab[bi] + L.hub + hubrec::input, u, 7 * sizeof(double),
-                                        cudaMemcpyHostToDevice, c->stream));
+            KYN_CUDA(c, cudaMemcpyAsync(m->d_slab[bi] + L.hub + r * kHubDoubles + hubrec::input, u,
+                                        7 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         }
         KYN_CUDA(c, cudaStreamSynchronize(c->stream));
         return KYN_OK;
@@ -1135,6 +1144,38 @@ int kyn_get_state(kyn_ctx* c, int id, int field, double* out) {
     DevModel* m = find_model(c, id);
     if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
     KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+    const HostModel& HM = m->host;
+    if (field == KYN_FIELD_CONSTRAINT_OUTPUT) {
+        // Constraints::output (src/step/step.hpp:105-115): the revolute joint's
+        // rotation, rate and acceleration about its axis
+        // (src/constraints/calculate_revolute_joint_output.hpp:24-85), from beam
+        // 0's copy of the azimuth record; zero for the other constraints.
+        for (int k = 0; k < 3 * HM.num_constraints; ++k) out[k] = 0.;
+        if (HM.rev_con < 0) return KYN_OK;
+        const HostBeam& b0 = HM.beams[0];
+        const SlabLayout L0 = make_slab_layout(b0.N, b0.Q);
+        double R[kHubDoubles];
+        KYN_CUDA(c, cudaMemcpy(R, m->d_slab[0] + L0.hub + kHubDoubles, sizeof(R), cudaMemcpyDeviceToHost));
+        const double* q = R + hubrec::q + 3;
+        const double* a0 = R + hubrec::axes;
+        double ax[3], rv[3] = {0., 0., 0.};
+        for (int i = 0; i < 3; ++i) {
+            ax[i] = 0.;
+            for (int j = 0; j < 3; ++j) ax[i] += rot_entry(q, i, j) * a0[j];
+        }
+        const double sh = std::sqrt(1. - q[0] * q[0]);
+        if (sh > 1e-12) {  // QuaternionToRotationVector (src/math/quaternion_operations.hpp:248-262)
+            const double th = 2. * std::acos(q[0]);
+            for (int i = 0; i < 3; ++i) rv[i] = th * q[1 + i] / sh;
+        }
+        double* o = out + 3 * HM.rev_con;
+        for (int i = 0; i < 3; ++i) {
+            o[0] += ax[i] * rv[i];
+            o[1] += ax[i] * R[hubrec::v + 3 + i];
+            o[2] += ax[i] * R[hubrec::vd + 3 + i];
+        }
+        return KYN_OK;
+    }
     for (size_t bi = 0; bi < m->host.beams.size(); ++bi) {
         const HostBeam& b = m->host.beams[bi];
         const SlabLayout L = make_slab_layout(b.N, b.Q);
@@ -1144,9 +1185,12 @@ int kyn_get_state(kyn_ctx* c, int id, int field, double* out) {
         if (field == KYN_FIELD_LAMBDA) {
             for (int s = 0; s < b.nc; ++s)
                 for (int k = 0; k < 6; ++k) out[b.con_row[s] * 6 + k] = h[L.lambda + s * 6 + k];
-            if (bi == 0 && m->host.hub >= 0)
+            // the constraints leading into the hub-chain records: the hub BC, the
+            // revolute joint, the rigid joint inside the drive train
+            const int into[3] = {HM.hub_con, HM.rev_con, HM.ah_con};
+            for (size_t r = 0; bi == 0 && r < HM.chain.size(); ++r)
                 for (int k = 0; k < 6; ++k)
-                    out[m->host.hub_con * 6 + k] = h[L.hub + hubrec::lambda + k];
+                    out[into[r] * 6 + k] = h[L.hub + r * kHubDoubles + hubrec::lambda + k];
             continue;
         }
         int src = -1, w = 0;
@@ -1174,10 +1218,9 @@ int kyn_get_state(kyn_ctx* c, int id, int field, double* out) {
                 for (int e = 0; e < w; ++e) o[e] = h[src + k * w + e];
             }
         }
-        if (bi == 0 && m->host.hub >= 0) {  // the hub node / the hub BC, from beam 0's copy
-            const double* H = h.data() + L.hub;
-            if (field == KYN_FIELD_LAMBDA) continue;
-            double* o = out + static_cast<size_t>(m->host.hub) * w;
+        for (size_t r = 0; bi == 0 && r < HM.chain.size(); ++r) {  // hub-chain nodes, from beam 0's copy
+            const double* H = h.data() + L.hub + r * kHubDoubles;
+            double* o = out + static_cast<size_t>(HM.chain[r]) * w;
             int hw = 0;
             const int ho = hub_field_offset(field, &hw);
             if (field == KYN_FIELD_TANGENT) {
@@ -1351,11 +1394,13 @@ extern "C" int kyn_set_prescribed_batch(kyn_ctx* c, const int* ids, int n, const
             DevModel* m = find_model(c, ids[i]);
             if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id in batch");
             for (int k = 0; k < m->host.num_constraints; ++k, ++row) {
-                if (k == m->host.hub_con) {
+                if (k == m->host.ah_con) continue;  // a rigid joint reads no input
+                if (k == m->host.hub_con || k == m->host.rev_con) {
+                    const int r = k == m->host.rev_con ? 1 : 0;
                     for (size_t bi = 0; bi < m->host.beams.size(); ++bi) {
                         const HostBeam& b = m->host.beams[bi];
                         const SlabLayout L = make_slab_layout(b.N, b.Q);
-                        t.push_back(m->d_slab[bi] + L.hub + hubrec::input);
+                        t.push_back(m->d_slab[bi] + L.hub + r * kHubDoubles + hubrec::input);
                         vi.push_back(row);
                     }
                     continue;
@@ -1447,8 +1492,9 @@ extern "C" int kyn_set_state(kyn_ctx* c, int id, int field, const double* values
                                cudaMemcpyHostToDevice));
         int hw = 0;
         const int ho = hub_field_offset(field, &hw);
-        if (m->host.hub >= 0 && ho >= 0)  // every beam's copy of the hub
-            KYN_CUDA(c, cudaMemcpy(m->d_slab[bi] + L.hub + ho, values + static_cast<size_t>(m->host.hub) * w,
+        for (size_t r = 0; ho >= 0 && r < m->host.chain.size(); ++r)  // every beam's copy of the hub chain
+            KYN_CUDA(c, cudaMemcpy(m->d_slab[bi] + L.hub + r * kHubDoubles + ho,
+                                   values + static_cast<size_t>(m->host.chain[r]) * w,
                                    w * sizeof(double), cudaMemcpyHostToDevice));
     }
     return KYN_OK;
@@ -1508,7 +1554,7 @@ extern "C" int kyn_state_copy(kyn_ctx* c, int dst, int src) {
     DevModel* d = find_model(c, dst);
     DevModel* s = find_model(c, src);
     if (!d || !s) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
-    if (d->host.beams.size() != s->host.beams.size() || (d->host.hub >= 0) != (s->host.hub >= 0))
+    if (d->host.beams.size() != s->host.beams.size() || d->host.chain.size() != s->host.chain.size())
         return set_err(c, KYN_ERR_INVALID, "models differ in structure");
     for (size_t bi = 0; bi < d->host.beams.size(); ++bi) {
         const HostBeam& a = d->host.beams[bi];
@@ -1527,8 +1573,9 @@ extern "C" int kyn_state_copy(kyn_ctx* c, int dst, int src) {
             KYN_CUDA(c, cudaMemcpyAsync(d->d_slab[bi] + fields[k], s->d_slab[bi] + fields[k],
                                         sizeof(double) * widths[k] * b.N, cudaMemcpyDeviceToDevice,
                                         c->stream));
-        if (d->host.hub >= 0)  // the hub's state (its BC input stays the destination's)
-            KYN_CUDA(c, cudaMemcpyAsync(d->d_slab[bi] + L.hub, s->d_slab[bi] + L.hub,
+        for (size_t r = 0; r < d->host.chain.size(); ++r)  // hub-chain states (inputs stay the destination's)
+            KYN_CUDA(c, cudaMemcpyAsync(d->d_slab[bi] + L.hub + r * kHubDoubles,
+                                        s->d_slab[bi] + L.hub + r * kHubDoubles,
                                         sizeof(double) * hubrec::input, cudaMemcpyDeviceToDevice,
                                         c->stream));
     }
@@ -1636,7 +1683,7 @@ extern "C" int kyn_autotune(kyn_ctx* c, const int* ids, int n, const kyn_step_pa
         float best_ms = 0.f, def_ms = -1.f;
         for (int nt : {128, 256, 512}) {
             bool fits = true;
-            for (const HostBeam& b : h.beams) fits &= beam_smem(b.N, b.Q, b.nc, rb, nt, h.hub >= 0) <= kMaxDynSmem;
+            for (const HostBeam& b : h.beams) fits &= beam_smem(b.N, b.Q, b.nc, rb, nt, hub_kind(h)) <= kMaxDynSmem;
             if (!fits || (key.beams > 1 && key.beams * nt > 1024 * 8)) continue;
             c->tuned[key] = nt;
             ++c->tuned_gen;
@@ -1684,7 +1731,7 @@ extern "C" int kyn_tuned_threads(kyn_ctx* c, int model_id, int precision) {
     if (it != c->tuned.end()) return it->second;
     const int rb = (precision == KYN_PRECISION_FP32_REFINED) ? 4 : 8;
     int nt = 128;
-    for (const HostBeam& b : m->host.beams) nt = std::max(nt, beam_threads(b.N, b.Q, b.nc, rb, m->host.hub >= 0));
+    for (const HostBeam& b : m->host.beams) nt = std::max(nt, beam_threads(b.N, b.Q, b.nc, rb, hub_kind(m->host)));
     return nt;
 }
 

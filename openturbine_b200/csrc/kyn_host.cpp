@@ -335,18 +335,52 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
         B.slab.insert(B.slab.end(), lrec_mass[b].begin(), lrec_mass[b].end());
         B.slab.insert(B.slab.end(), lrec_spring[b].begin(), lrec_spring[b].end());
     }
-    // A node outside every beam element is allowed only as the hub of a rotor:
-    // the base node of the joints, held by one single-node BC.
-    for (int n = 0; n < nn; ++n) {
-        if (M.node_beam[n] >= 0) continue;
-        bool is_hub = false;
-        for (int c = 0; c < d->num_constraints && d->constraint_type; ++c)
-            is_hub |= is_hub_joint(d->constraint_type[c]) && d->constraint_base_node &&
-                      d->constraint_base_node[c] == n;
-        if (!is_hub) return fail(err, KYN_ERR_UNSUPPORTED, "node not attached to any beam element");
-        if (M.hub >= 0) return fail(err, KYN_ERR_UNSUPPORTED, "more than one hub node in a model");
-        M.hub = n;
+    // A node outside every beam element is allowed only as the hub of a rotor
+    // (the base node of the joints, held by one single-node BC) or as a node
+    // of a drive train: shaft base (held by one BC) -> revolute joint ->
+    // azimuth [-> rigid joint -> hub], whose last node is the joints' base.
+    const int ncon = (d->num_constraints > 0 && d->constraint_type) ? d->num_constraints : 0;
+    auto base_of = [&](int c) { return d->constraint_base_node ? d->constraint_base_node[c] : -1; };
+    for (int c = 0; c < ncon; ++c) {
+        if (d->constraint_type[c] != KYN_CONSTRAINT_REVOLUTE_JOINT) continue;
+        if (M.rev_con >= 0) return fail(err, KYN_ERR_UNSUPPORTED, "more than one revolute joint in a model");
+        M.rev_con = c;
     }
+    if (M.rev_con >= 0) {
+        const int sb = base_of(M.rev_con), az = d->constraint_target_node[M.rev_con];
+        if (sb < 0 || sb >= nn || az < 0 || az >= nn || sb == az)
+            return fail(err, KYN_ERR_INVALID, "revolute joint nodes out of range");
+        if (M.node_beam[sb] >= 0 || M.node_beam[az] >= 0)
+            return fail(err, KYN_ERR_UNSUPPORTED, "a revolute joint must join two nodes outside the beams");
+        if (M.beams.size() != 1)
+            return fail(err, KYN_ERR_UNSUPPORTED, "a drive train turns one beam system in this path");
+        M.chain = {sb, az};
+        for (int c = 0; c < ncon; ++c) {
+            const int t = d->constraint_target_node[c];
+            if (d->constraint_type[c] == KYN_CONSTRAINT_RIGID_JOINT && base_of(c) == az && t >= 0 && t < nn &&
+                M.node_beam[t] < 0) {
+                if (M.ah_con >= 0) return fail(err, KYN_ERR_UNSUPPORTED, "drive train branches after the azimuth");
+                M.ah_con = c;
+            }
+        }
+        if (M.ah_con >= 0) M.chain.push_back(d->constraint_target_node[M.ah_con]);
+        M.hub = sb;
+        for (int n = 0; n < nn; ++n)
+            if (M.node_beam[n] < 0 && std::find(M.chain.begin(), M.chain.end(), n) == M.chain.end())
+                return fail(err, KYN_ERR_UNSUPPORTED, "node not attached to any beam element");
+    } else {
+        for (int n = 0; n < nn; ++n) {
+            if (M.node_beam[n] >= 0) continue;
+            bool is_hub = false;
+            for (int c = 0; c < ncon; ++c)
+                is_hub |= is_hub_joint(d->constraint_type[c]) && base_of(c) == n;
+            if (!is_hub) return fail(err, KYN_ERR_UNSUPPORTED, "node not attached to any beam element");
+            if (M.hub >= 0) return fail(err, KYN_ERR_UNSUPPORTED, "more than one hub node in a model");
+            M.hub = n;
+        }
+        if (M.hub >= 0) M.chain = {M.hub};
+    }
+    const int jbase = M.chain.empty() ? -1 : M.chain.back();  // base node of the root joints
 
     // constraints (src/constraints/constraints.hpp:76-266)
     M.con_beam.assign(d->num_constraints, -1);
@@ -359,20 +393,31 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
     int joints = 0;
     for (int c = 0; c < d->num_constraints; ++c) {
         const int t = d->constraint_type[c];
-        if (t != KYN_CONSTRAINT_FIXED_BC && t != KYN_CONSTRAINT_PRESCRIBED_BC && !is_hub_joint(t))
+        if (t != KYN_CONSTRAINT_FIXED_BC && t != KYN_CONSTRAINT_PRESCRIBED_BC && !is_hub_joint(t) &&
+            t != KYN_CONSTRAINT_REVOLUTE_JOINT)
             return fail(err, KYN_ERR_UNSUPPORTED,
-                        "only FixedBC, PrescribedBC, RigidJoint and RotationControl constraints");
+                        "only FixedBC, PrescribedBC, RigidJoint, RevoluteJoint and RotationControl constraints");
         const int node = d->constraint_target_node[c];
         if (node < 0 || node >= nn) return fail(err, KYN_ERR_INVALID, "constraint node out of range");
+        if (c == M.rev_con || c == M.ah_con) {  // joints inside the drive train
+            if (t == KYN_CONSTRAINT_RIGID_JOINT || t == KYN_CONSTRAINT_REVOLUTE_JOINT) {
+                node_cols[base_of(c)].push_back(c);
+                node_cols[node].push_back(c);
+                continue;
+            }
+        }
         if (is_hub_joint(t)) {
-            const int base = d->constraint_base_node ? d->constraint_base_node[c] : -1;
+            const int base = base_of(c);
             if (base < 0 || base >= nn) return fail(err, KYN_ERR_INVALID, "joint base node out of range");
-            if (base != M.hub || M.node_beam[node] < 0)
+            if (base != jbase || M.node_beam[node] < 0)
                 return fail(err, KYN_ERR_UNSUPPORTED,
                             "joints must join a hub node (in no beam) to a beam node");
             node_cols[base].push_back(c);
             ++joints;
         }
+        if (M.chain.size() > 1 && node != M.hub &&
+            std::find(M.chain.begin(), M.chain.end(), node) != M.chain.end())
+            return fail(err, KYN_ERR_UNSUPPORTED, "a drive-train node other than the shaft base holds a BC");
         if (node == M.hub) {  // the hub's own boundary condition
             if (is_hub_joint(t) || M.hub_con >= 0)
                 return fail(err, KYN_ERR_UNSUPPORTED, "the hub needs exactly one FixedBC or PrescribedBC");
@@ -405,7 +450,7 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
         } else if (is_hub_joint(t)) {
             // X0 = target x0 - base x0 (src/constraints/constraints.hpp:268-290)
             const double* x0 = d->node_x0 + node * 7;
-            const double* xb = d->node_x0 + M.hub * 7;
+            const double* xb = d->node_x0 + jbase * 7;
             for (int k = 0; k < 3; ++k) B.con_X0[slot][k] = x0[k] - xb[k];
             for (int k = 0; k < 7; ++k) B.slab[L.con_input + slot * 7 + k] = ident[k];
             if (t == KYN_CONSTRAINT_ROTATION_CONTROL) {
@@ -463,13 +508,70 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
                     ? x0[k] - (d->constraint_axis ? d->constraint_axis[c * 3 + k] : 0.) : 0.;
         }
     }
+    // drive train: records 1 and 2 (state, the joint leading into the node)
+    for (size_t r = 1; r < M.chain.size(); ++r) {
+        const int n = M.chain[r], prev = M.chain[r - 1];
+        const double* x0 = d->node_x0 + n * 7;
+        const double* u = d->node_u ? d->node_u + n * 7 : ident7;
+        double X0[3], axes[9] = {};
+        for (int k = 0; k < 3; ++k) X0[k] = x0[k] - d->node_x0[prev * 7 + k];
+        if (r == 1) {
+            // src/constraints/constraints.hpp:294-319: x_hat = unit(axis), or
+            // unit(X0) for a zero axis; rows of the rotation taking (1, 0, 0)
+            // to x_hat are the joint axes
+            const double* ax = d->constraint_axis ? d->constraint_axis + M.rev_con * 3 : nullptr;
+            const double na = ax ? std::sqrt(ax[0] * ax[0] + ax[1] * ax[1] + ax[2] * ax[2]) : 0.;
+            const double* src = na != 0. ? ax : X0;
+            const double ns = std::sqrt(src[0] * src[0] + src[1] * src[1] + src[2] * src[2]);
+            if (!(ns > 0.))
+                return fail(err, KYN_ERR_INVALID, "revolute joint needs an axis or distinct node positions");
+            const double xh[3] = {src[0] / ns, src[1] / ns, src[2] / ns};
+            const double cp[3] = {0., -xh[2], xh[1]};
+            const double dp = xh[0];
+            if (!(1. + dp > 0.))
+                return fail(err, KYN_ERR_UNSUPPORTED, "revolute joint axis along -x");
+            const double kk = 1. / (1. + dp);
+            const double R[9] = {cp[0] * cp[0] * kk + dp, cp[1] * cp[0] * kk + cp[2], cp[2] * cp[0] * kk - cp[1],
+                                 cp[0] * cp[1] * kk - cp[2], cp[1] * cp[1] * kk + dp, cp[2] * cp[1] * kk + cp[0],
+                                 cp[0] * cp[2] * kk + cp[1], cp[1] * cp[2] * kk - cp[0], cp[2] * cp[2] * kk + dp};
+            for (int k = 0; k < 9; ++k) axes[k] = R[k];
+        }
+        for (auto& B : M.beams) {
+            const SlabLayout L = make_slab_layout(B.N, B.Q);
+            double* H = B.slab.data() + L.hub + r * kHubDoubles;
+            for (int k = 0; k < 7; ++k) {
+                H[hubrec::x0 + k] = x0[k];
+                H[hubrec::q + k] = u[k];
+                H[hubrec::q_prev + k] = u[k];
+                H[hubrec::input + k] = ident7[k];
+            }
+            for (int k = 0; k < 3; ++k) H[hubrec::x + k] = x0[k] + u[k];
+            qmul(u + 3, x0 + 3, H + hubrec::x + 3);
+            for (int k = 0; k < 6; ++k) {
+                H[hubrec::v + k] = d->node_v ? d->node_v[n * 6 + k] : 0.;
+                H[hubrec::vd + k] = d->node_vd ? d->node_vd[n * 6 + k] : 0.;
+                H[hubrec::a + k] = H[hubrec::vd + k];
+            }
+            for (int k = 0; k < 3; ++k) H[hubrec::tangent + k * 4] = 1.;
+            for (int k = 0; k < 3; ++k) H[hubrec::X0 + k] = X0[k];
+            for (int k = 0; k < 9; ++k) H[hubrec::axes + k] = axes[k];
+        }
+    }
 
     // DOF map: every node carries 6 DOFs, exclusive scan in node-id order
     // (compute_node_freedom_map_table.hpp); constraint rows follow in order.
     M.fmap.resize(nn);
     for (int n = 0; n < nn; ++n) M.fmap[n] = 6 * n;
     M.nsys = 6 * nn;
-    M.ndofs = M.nsys + 6 * d->num_constraints;
+    M.con_rows.assign(d->num_constraints, 6);
+    M.con_row_first.assign(d->num_constraints, 0);
+    int crow = 0;
+    for (int c = 0; c < d->num_constraints; ++c) {
+        M.con_rows[c] = constraint_rows(d->constraint_type[c]);
+        M.con_row_first[c] = crow;
+        crow += M.con_rows[c];
+    }
+    M.ndofs = M.nsys + crow;
 
     // CRS graph: each row lists the DOFs it couples to, sorted ascending
     // (compute_row_ptrs.hpp, compute_col_inds.hpp, sort_crs_graph).
@@ -502,12 +604,13 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
                 for (int c = 0; c < 6; ++c) cols.push_back(M.fmap[other] + c);
             }
             for (int con : node_cols[node])
-                for (int c = 0; c < 6; ++c) cols.push_back(M.nsys + 6 * con + c);
+                for (int c = 0; c < M.con_rows[con]; ++c) cols.push_back(M.nsys + M.con_row_first[con] + c);
         } else {
-            const int con = (row - M.nsys) / 6;
+            int con = 0;
+            while (con + 1 < d->num_constraints && M.con_row_first[con + 1] <= row - M.nsys) ++con;
             const int node = d->constraint_target_node[con];
             for (int c = 0; c < 6; ++c) cols.push_back(M.fmap[node] + c);
-            if (is_hub_joint(d->constraint_type[con]))
+            if (is_hub_joint(d->constraint_type[con]) || d->constraint_type[con] == KYN_CONSTRAINT_REVOLUTE_JOINT)
                 for (int c = 0; c < 6; ++c) cols.push_back(M.fmap[d->constraint_base_node[con]] + c);
         }
         std::sort(cols.begin(), cols.end());

@@ -50,6 +50,14 @@ struct HostModel {
     int hub = -1;                             // hub node (in no beam) or -1
     int hub_con = -1;                         // the single-node BC holding the hub
     int hub_con_type = 0;
+    // Drive train: the hub chain (hubrec records 0..): shaft base (= hub, held
+    // by hub_con), revolute target, optional node rigidly jointed to it.  A
+    // plain hub is a chain of one.  The beam roots join chain.back().
+    std::vector<int> chain;
+    int rev_con = -1;                         // the revolute joint (chain 0 -> 1)
+    int ah_con = -1;                          // the rigid joint chain 1 -> 2, or -1
+    std::vector<int> con_row_first;           // constraint -> first row (after nsys)
+    std::vector<int> con_rows;                // constraint -> rows (5 revolute, else 6)
 };
 
 // Validates the description and builds the host model.  Returns KYN_OK or a

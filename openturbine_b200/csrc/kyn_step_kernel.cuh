@@ -39,7 +39,7 @@ __device__ __forceinline__ void quat_compose(const double* a, const double* b, d
 }
 
 // Entry (i,j) of the rotation matrix of unit quaternion q.
-__device__ __forceinline__ double rot_entry(const double* q, int i, int j) {
+__host__ __device__ __forceinline__ double rot_entry(const double* q, int i, int j) {
     const double w = q[0], x = q[1], y = q[2], z = q[3];
     switch (i * 3 + j) {
         case 0: return w * w + x * x - y * y - z * z;
@@ -115,7 +115,8 @@ __device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double
 constexpr int kGroupScratch = 256;      // doubles of per-group scratch for QP math
 constexpr int kPanel = 8;               // LU panel width
 constexpr int kConStride = 96;          // doubles per constraint record in smem
-constexpr int kHubSmem = 200;           // doubles of the hub record (hubsm)
+constexpr int kHubSmem = 208;           // doubles of the hub record (hubsm)
+constexpr int kDriveSmem = 600;         // doubles of the hub record of a drive train
 
 // Per-group scratch (doubles) of the quadrature phase.
 namespace grec {
@@ -153,7 +154,7 @@ struct Smem {
     int stage;          // double [64]  U12 tile staged by warp 0 during the LU
     int con;            // double [nc][kConStride]
     int red;            // double [2][NT/32 + 8]  (offset 0: cluster exchange)
-    int hub;            // double [kHubSmem] hub state and records, or -1
+    int hub;            // double [kHubSmem or kDriveSmem] hub state and records, or -1
     int pos;            // int [N]
     int bytes;
     int ldA;
@@ -162,6 +163,7 @@ struct Smem {
 // The system matrix and the quadrature scratch never live at the same time:
 // A is assembled after the quadrature phase and consumed by the solve, so the
 // two share one region.
+// hub: 0 none, 1 a hub node, 2 a drive train (hub chain of 2 or 3 nodes).
 __host__ __device__ inline Smem make_smem(int N, int Q, int nc, int real_bytes, int nt, int hub = 0) {
     Smem S{};
     int o = 0;
@@ -175,7 +177,7 @@ __host__ __device__ inline Smem make_smem(int N, int Q, int nc, int real_bytes, 
     // The cluster exchange areas come first, so that every CTA of a model's
     // cluster finds them at the same offset whatever its beam's size.
     S.red = take(2 * (nt / 32 + 8) * 8);
-    S.hub = hub ? take(kHubSmem * 8) : -1;
+    S.hub = hub ? take((hub > 1 ? kDriveSmem : kHubSmem) * 8) : -1;
     {
         const int a_bytes = n6 * S.ldA * real_bytes;
         const int g_bytes = (nt / 16) * kGroupScratch * 8;
@@ -242,6 +244,9 @@ constexpr int yr = 49;     // [6] constrained-row residual b_r - A_r x
 constexpr int R1X0 = 55;   // [3] rigid joint: R(hub) X0
 constexpr int Btr = 58;    // [9] rigid joint: base block tilde(R1 X0) T_hub
 constexpr int Brr = 67;    // [9] rigid joint: base block -AX(C) T_hub
+constexpr int dr = 76;     // [6] drive train: root correction per unit shaft rotation
+constexpr int wr = 82;     // [6] drive train: root test vector (G w = 0)
+constexpr int s2 = 88;     // [6] drive train: A_r x2 of the second right-hand side
 }  // namespace conrec
 
 // Shared-memory record of a model's hub (doubles): the hub state in the slab
@@ -249,11 +254,41 @@ constexpr int Brr = 67;    // [9] rigid joint: base block -AX(C) T_hub
 // hub multiplier correction, and the per-beam contributions exchanged over
 // the cluster (double-buffered by iteration parity).
 namespace hubsm {
-constexpr int bc = 80;     // [kConStride] constraint record of the hub BC
-constexpr int xh = 176;    // [6] hub correction
-constexpr int xlh = 182;   // [6] hub multiplier correction (unconditioned)
-constexpr int pub = 188;   // [2][6] sum over this beam's joints of G_base^T (lambda + x_lambda)
+constexpr int bc = 88;     // [kConStride] constraint record of the hub BC
+constexpr int xh = 184;    // [6] hub correction
+constexpr int xlh = 190;   // [6] hub multiplier correction (unconditioned)
+constexpr int pub = 196;   // [2][6] sum over this beam's joints of G_base^T (lambda + x_lambda)
+// drive train (records 1 and 2 of the hub chain, the revolute and rigid joints
+// between them, and the vectors of the shaft-rotation elimination)
+constexpr int n1 = 208;    // [kHubDoubles] chain record 1 (azimuth node)
+constexpr int n2 = 296;    // [kHubDoubles] chain record 2 (hub node), if any
+constexpr int rev = 384;   // [64] revolute joint record (revrec)
+constexpr int ah = 448;    // [kConStride] rigid joint record 1 -> 2
+constexpr int cA = 544;    // [6] record-1 correction at zero shaft rotation
+constexpr int nA = 550;    // [6] record-1 correction per unit shaft rotation
+constexpr int cH = 556;    // [6] record-2 correction at zero shaft rotation
+constexpr int dH = 562;    // [6] record-2 correction per unit shaft rotation
+constexpr int wA = 568;    // [6] record-1 test vector
+constexpr int wH = 574;    // [6] record-2 test vector
+constexpr int theta = 580; // shaft rotation of the Newton correction
 }  // namespace hubsm
+
+// Revolute joint record (doubles, at hubsm::rev).
+namespace revrec {
+constexpr int Phi = 0;     // [5] residual
+constexpr int x = 5;       // [3] R(base) x0: joint axis
+constexpr int y = 8;       // [3] R(target) y0
+constexpr int z = 11;      // [3] R(target) z0
+constexpr int xcz = 14;    // [3] x cross z
+constexpr int xcy = 17;    // [3] x cross y
+constexpr int Bt = 20;     // [2][3] rotational rows of G_target T_target
+constexpr int Bb = 26;     // [2][3] rotational rows of G_base T_base
+constexpr int sys = 32;    // [3] torque about R(target) x0
+constexpr int lam = 35;    // [6] multipliers (5 used)
+constexpr int xl = 41;     // [6] multiplier correction (unconditioned)
+constexpr int GtL = 47;    // [6] G_target^T lambda
+constexpr int GbL = 53;    // [6] G_base^T lambda
+}  // namespace revrec
 
 // TF32 tensor-core product D += A B for one 16x8x8 tile (mma.sync m16n8k8).
 // Fragment layout per lane l (g = l/4, t = l%4): a = {A[g][t], A[g+8][t],
@@ -500,6 +535,30 @@ __device__ __forceinline__ void update_tile(TR* A, int ldA, int m, int k0, int k
     }
 }
 
+// Solves L U y = r for the right-hand side in column rc (rows [0, m)) by one
+// warp, in place, with the factors as the LU leaves them (unit L below the
+// diagonal, U with its pivots on it, reciprocal pivots in rpiv): forward then
+// back substitution, one column per step.
+template <typename TR>
+__device__ void solve_factored_column(TR* A, int ldA, int m, int rc, const double* rpiv, int lane) {
+    for (int j = 0; j < m; ++j) {
+        const double yj = static_cast<double>(A[j * ldA + rc]);
+        for (int i = j + 1 + lane; i < m; i += 32)
+            A[i * ldA + rc] = static_cast<TR>(static_cast<double>(A[i * ldA + rc]) -
+                                              static_cast<double>(A[i * ldA + j]) * yj);
+        __syncwarp();
+    }
+    for (int j = m - 1; j >= 0; --j) {
+        const double yj = static_cast<double>(A[j * ldA + rc]) * rpiv[j];
+        __syncwarp();
+        if (lane == 0) A[j * ldA + rc] = static_cast<TR>(yj);
+        for (int i = lane; i < j; i += 32)
+            A[i * ldA + rc] = static_cast<TR>(static_cast<double>(A[i * ldA + rc]) -
+                                              static_cast<double>(A[i * ldA + j]) * yj);
+        __syncwarp();
+    }
+}
+
 // Replaces the kb x kb upper-triangular diagonal block of panel p0 (pivots in
 // rpiv) by its inverse; lane j < kb computes column j by back substitution
 // (lanes >= kb compute on padding and store nothing).
@@ -657,6 +716,104 @@ __device__ inline void joint_base_transpose_add(const double* cr, const double* 
         for (int k = 0; k < 3; ++k) acc += tilde_e(r, k, i) * w[k] - AX[k * 3 + i] * w[3 + k];
         out[3 + i] += acc;
     }
+}
+
+// ---- drive train: revolute joint between hub-chain records 0 and 1 -------------------
+// Residual, gradient rows and G^T lambda of the revolute joint
+// (calculate_revolute_joint_constraint.hpp:19-113, calculate_revolute_joint_force.hpp:19-45,
+// branch :388-465 of calculate_constraint_residual_gradient.hpp).  Rows 0-2:
+// u2 + X0 - u1 - R1 X0 with gradients I (target) and -I (base); rows 3-4:
+// (R2 z0).(R1 x0) and (R2 y0).(R1 x0) with gradients -(x cross z), -(x cross y)
+// on the target's rotation and +(x cross z), +(x cross y) on the base's.
+// `b` and `t` are hub-chain records (state at hubrec offsets).
+__device__ inline void revolute_record(double* rr, const double* b, const double* t) {
+    const double* X0 = t + hubrec::X0;
+    const double* ax = t + hubrec::axes;
+    const double* bq = b + hubrec::q;
+    const double* tq = t + hubrec::q;
+    double R1X0[3], x[3], y[3], z[3], ta[3];
+    for (int i = 0; i < 3; ++i) {
+        R1X0[i] = x[i] = y[i] = z[i] = ta[i] = 0.;
+        for (int j = 0; j < 3; ++j) {
+            R1X0[i] += rot_entry(bq + 3, i, j) * X0[j];
+            x[i] += rot_entry(bq + 3, i, j) * ax[j];
+            y[i] += rot_entry(tq + 3, i, j) * ax[3 + j];
+            z[i] += rot_entry(tq + 3, i, j) * ax[6 + j];
+            ta[i] += rot_entry(tq + 3, i, j) * ax[j];
+        }
+    }
+    for (int i = 0; i < 3; ++i) rr[revrec::Phi + i] = tq[i] + X0[i] - bq[i] - R1X0[i];
+    rr[revrec::Phi + 3] = z[0] * x[0] + z[1] * x[1] + z[2] * x[2];
+    rr[revrec::Phi + 4] = y[0] * x[0] + y[1] * x[1] + y[2] * x[2];
+    const double xcz[3] = {x[1] * z[2] - x[2] * z[1], x[2] * z[0] - x[0] * z[2], x[0] * z[1] - x[1] * z[0]};
+    const double xcy[3] = {x[1] * y[2] - x[2] * y[1], x[2] * y[0] - x[0] * y[2], x[0] * y[1] - x[1] * y[0]};
+    for (int i = 0; i < 3; ++i) {
+        rr[revrec::x + i] = x[i];
+        rr[revrec::y + i] = y[i];
+        rr[revrec::z + i] = z[i];
+        rr[revrec::xcz + i] = xcz[i];
+        rr[revrec::xcy + i] = xcy[i];
+        rr[revrec::sys + i] = ta[i] * t[hubrec::input];
+    }
+    // B = G T on the rotational columns (stored tangent blocks, row-major)
+    const double* Tt = t + hubrec::tangent;
+    const double* Tb = b + hubrec::tangent;
+    for (int j = 0; j < 3; ++j) {
+        double a0 = 0., a1 = 0., b0 = 0., b1 = 0.;
+        for (int k = 0; k < 3; ++k) {
+            a0 -= xcz[k] * Tt[k * 3 + j];
+            a1 -= xcy[k] * Tt[k * 3 + j];
+            b0 += xcz[k] * Tb[k * 3 + j];
+            b1 += xcy[k] * Tb[k * 3 + j];
+        }
+        rr[revrec::Bt + j] = a0;
+        rr[revrec::Bt + 3 + j] = a1;
+        rr[revrec::Bb + j] = b0;
+        rr[revrec::Bb + 3 + j] = b1;
+    }
+    const double* l = rr + revrec::lam;
+    for (int i = 0; i < 3; ++i) {
+        rr[revrec::GtL + i] = l[i];
+        rr[revrec::GbL + i] = -l[i];
+        rr[revrec::GtL + 3 + i] = -xcz[i] * l[3] - xcy[i] * l[4];
+        rr[revrec::GbL + 3 + i] = xcz[i] * l[3] + xcy[i] * l[4];
+    }
+}
+
+// Target correction of a six-row joint (constraint record cr, base blocks
+// Btr/Brr, target block Brot) from its base correction xb: B_t x = -s Phi -
+// B_base xb, with s = 1 for the correction and 0 for its part per unit shaft
+// rotation.
+__device__ inline bool joint_target_correction(const double* cr, const double* xb, double s, double* x) {
+    double rr[3];
+    for (int i = 0; i < 3; ++i) {
+        x[i] = -s * cr[conrec::Phi + i] + xb[i];
+        rr[i] = -s * cr[conrec::Phi + 3 + i];
+        for (int k = 0; k < 3; ++k) {
+            x[i] -= cr[conrec::Btr + i * 3 + k] * xb[3 + k];
+            rr[i] -= cr[conrec::Brr + i * 3 + k] * xb[3 + k];
+        }
+    }
+    return solve3(cr + conrec::Brot, rr, x + 3);
+}
+
+// Target test vector of a six-row joint from its base test vector: G_t w =
+// -G_base wb with the gradients (not B = G T): G_t = [I 0; 0 AX^T],
+// G_base = [-I tilde(R1 X0); 0 -AX].
+__device__ inline bool joint_target_test(const double* cr, const double* wb, double* w) {
+    const double* r = cr + conrec::R1X0;
+    const double* AX = cr + conrec::AX;
+    double rhs[3], AXt[9];
+    for (int i = 0; i < 3; ++i) {
+        w[i] = wb[i];
+        rhs[i] = 0.;
+        for (int k = 0; k < 3; ++k) {
+            w[i] -= tilde_e(r, i, k) * wb[3 + k];
+            rhs[i] += AX[i * 3 + k] * wb[3 + k];
+            AXt[i * 3 + k] = AX[k * 3 + i];
+        }
+    }
+    return solve3(AXt, rhs, w + 3);
 }
 
 // ---- point masses and springs at the nodes of one CTA's system ---------------------
@@ -833,8 +990,17 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
     const int n6 = 6 * N;
     const int m = 6 * (N - nc);   // free-node block size
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const bool hub = KB.hub != 0;
-    const Smem S = make_smem(N, Q, nc, sizeof(TR), NT, hub ? 1 : 0);
+    const int chain = KB.hub;  // hub chain length (0: no hub)
+    const bool hub = chain != 0;
+    const bool drive = LUMP && chain > 1;  // drive trains run in the LUMP instance only
+    if (!LUMP && chain > 1) {  // launch-plan error: refuse rather than solve without the chain
+        if (tid == 0 && KB.rank == 0) {
+            status_out[KB.plan_model] = KYN_ERR_UNSUPPORTED;
+            iters_out[KB.plan_model] = 0;
+        }
+        return;
+    }
+    const Smem S = make_smem(N, Q, nc, sizeof(TR), NT, drive ? 2 : (hub ? 1 : 0));
     const SlabLayout L = make_slab_layout(N, Q);
     double* __restrict__ slab = KB.slab;
 
@@ -856,6 +1022,11 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
     double* sqd = reinterpret_cast<double*>(smem_raw + S.qd);
     double* sT = reinterpret_cast<double*>(smem_raw + S.T);
     double* hb = hub ? reinterpret_cast<double*>(smem_raw + S.hub) : nullptr;  // hub record
+    // drive train: chain records 1 (revolute target) and 2 (optional), and the
+    // record the beam roots join (the last of the chain)
+    double* hA = drive ? hb + hubsm::n1 : nullptr;
+    double* hH = (drive && chain == 3) ? hb + hubsm::n2 : nullptr;
+    double* hj = drive ? (hH ? hH : hA) : hb;
     double* resid = reinterpret_cast<double*>(smem_raw + S.resid);
     double* bp = reinterpret_cast<double*>(smem_raw + S.b);
     double* xs = reinterpret_cast<double*>(smem_raw + S.xs);
@@ -912,6 +1083,16 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
             for (int k = 0; k < 6; ++k) br[conrec::lam + k] = 0.;  // ResetConstraints
         }
     }
+    if (drive) {
+        for (int k = tid; k < (chain - 1) * kHubDoubles; k += NT)
+            hb[hubsm::n1 + (k / kHubDoubles) * (hubsm::n2 - hubsm::n1) + k % kHubDoubles] =
+                slab[L.hub + kHubDoubles + k];
+        if (tid == 0)
+            for (int k = 0; k < 6; ++k) {  // ResetConstraints
+                hb[hubsm::rev + revrec::lam + k] = 0.;
+                hb[hubsm::ah + conrec::lam + k] = 0.;
+            }
+    }
     if (tid == 0) {
         // Free nodes first, constrained nodes last (in constraint order).
         int p = 0;
@@ -938,15 +1119,21 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
         sv[k] = v_p + h * (1. - P.gamma) * a_p + P.gamma * h * an;
         sqd[k] = v_p + (0.5 - P.beta) * h * a_p + P.beta * h * an;
     }
-    if (hub && tid == NT - 1) {  // the hub node: same predictor
-        for (int k = 0; k < 7; ++k) hb[hubrec::q_prev + k] = hb[hubrec::q + k];
+    // hub-chain records: thread NT-1-r owns record r (evaluated where used, so
+    // that the instances without a drive train keep no extra register live)
+    auto chain_rec = [&]() -> double* {
+        return tid == NT - 1 ? hb : (tid == NT - 2) ? hA : (tid == NT - 3) ? hH : nullptr;
+    };
+    if (hub && chain_rec()) {  // the hub node(s): same predictor
+        double* r = chain_rec();
+        for (int k = 0; k < 7; ++k) r[hubrec::q_prev + k] = r[hubrec::q + k];
         for (int k = 0; k < 6; ++k) {
-            const double v_p = hb[hubrec::v + k], vd_p = hb[hubrec::vd + k], a_p = hb[hubrec::a + k];
-            hb[hubrec::vd + k] = 0.;
+            const double v_p = r[hubrec::v + k], vd_p = r[hubrec::vd + k], a_p = r[hubrec::a + k];
+            r[hubrec::vd + k] = 0.;
             const double an = (P.alpha_f * vd_p - P.alpha_m * a_p) / (1. - P.alpha_m);
-            hb[hubrec::a + k] = an;
-            hb[hubrec::v + k] = v_p + h * (1. - P.gamma) * a_p + P.gamma * h * an;
-            hb[hubrec::q_delta + k] = v_p + (0.5 - P.beta) * h * a_p + P.beta * h * an;
+            r[hubrec::a + k] = an;
+            r[hubrec::v + k] = v_p + h * (1. - P.gamma) * a_p + P.gamma * h * an;
+            r[hubrec::q_delta + k] = v_p + (0.5 - P.beta) * h * a_p + P.beta * h * an;
         }
     }
     __syncthreads();
@@ -960,10 +1147,10 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
             quat_compose(qd4, sqp + n * 7 + 3, qn);
             for (int c = 0; c < 4; ++c) sq[n * 7 + 3 + c] = qn[c];
         }
-        if (hub && tid == NT - 1) {
-            double* hq = hb + hubrec::q;
-            const double* hqp = hb + hubrec::q_prev;
-            const double* hqd = hb + hubrec::q_delta;
+        if (hub && chain_rec()) {
+            double* hq = chain_rec() + hubrec::q;
+            const double* hqp = chain_rec() + hubrec::q_prev;
+            const double* hqd = chain_rec() + hubrec::q_delta;
             for (int c = 0; c < 3; ++c) hq[c] = hqp[c] + h * hqd[c];
             const double d[3] = {h * hqd[3], h * hqd[4], h * hqd[5]};
             double qd4[4], qn[4];
@@ -1002,7 +1189,7 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
             }
         };
         for (int n = tid; n < N; n += NT) tangent_op(sqd + n * 6, sT + n * 9);
-        if (hub && tid == NT - 1) tangent_op(hb + hubrec::q_delta, hb + hubrec::tangent);
+        if (hub && chain_rec()) tangent_op(chain_rec() + hubrec::q_delta, chain_rec() + hubrec::tangent);
 
         // ---- quadrature-point values (calculate_quadrature_point_values.hpp) ---
         // 16 threads per quadrature point; a CTA covers NT/16 points per pass.  Each
@@ -1363,12 +1550,17 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
         if (warp == NW - 1 && lane < nc) {
             const int tn = KB.con_node[lane];
             constraint_record(con + lane * kConStride, KB.con_type[lane], sq + tn * 7, KB.con_X0[lane],
-                              sT + tn * 9, hub ? hb + hubrec::q : nullptr,
-                              hub ? hb + hubrec::tangent : nullptr, KB.con_axis[lane]);
+                              sT + tn * 9, hub ? hj + hubrec::q : nullptr,
+                              hub ? hj + hubrec::tangent : nullptr, KB.con_axis[lane]);
         }
         if (hub && warp == NW - 1 && lane == nc)  // the hub's own boundary condition
             constraint_record(hb + hubsm::bc, KB.hub_con_type, hb + hubrec::q, hb + hubrec::X0,
                               hb + hubrec::tangent, nullptr, nullptr, nullptr);
+        if (drive && warp == NW - 1 && lane == nc + 1)  // revolute joint record 0 -> 1
+            revolute_record(hb + hubsm::rev, hb, hA);
+        if (drive && hH && warp == NW - 1 && lane == nc + 2)  // rigid joint record 1 -> 2
+            constraint_record(hb + hubsm::ah, KYN_CONSTRAINT_RIGID_JOINT, hH + hubrec::q, hH + hubrec::X0,
+                              hH + hubrec::tangent, hA + hubrec::q, hA + hubrec::tangent, nullptr);
         __syncthreads();
 
         // ---- right-hand side: b = -cond (-f + R + G^T lambda) (assemble_system_residual.hpp,
@@ -1429,10 +1621,83 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
                 double y[3] = {0., 0., 0.};
                 if (!solve3(br + conrec::Brot, rhs, y)) atomicOr(&s_flag, 2);
                 for (int k = 0; k < 3; ++k) xh[3 + k] = y[k];
+                if (drive) {
+                    // Drive train: the revolute rows fix record 1's translation and
+                    // two of its rotation components; the third, the shaft rotation
+                    // theta, stays free.  x_1 = cA + theta nA, nA spanning the null
+                    // space of B_t; the chain's later corrections are affine in
+                    // theta as well (cH + theta dH).  Test vectors w (G w = 0 with
+                    // the gradients G, not G T) project the equilibrium rows onto
+                    // the free rotation: w_1 = [0, joint axis].
+                    const double* rv = hb + hubsm::rev;
+                    double* cA = hb + hubsm::cA;
+                    double* nA = hb + hubsm::nA;
+                    double* wA = hb + hubsm::wA;
+                    for (int k = 0; k < 3; ++k) {
+                        cA[k] = -rv[revrec::Phi + k] + xh[k];
+                        nA[k] = 0.;
+                        wA[k] = 0.;
+                        wA[3 + k] = rv[revrec::x + k];
+                    }
+                    const double* b0 = rv + revrec::Bt;
+                    const double* b1 = rv + revrec::Bt + 3;
+                    double r2[2];
+                    for (int i = 0; i < 2; ++i) {
+                        r2[i] = -rv[revrec::Phi + 3 + i];
+                        for (int k = 0; k < 3; ++k) r2[i] -= rv[revrec::Bb + i * 3 + k] * xh[3 + k];
+                    }
+                    // minimum-norm particular solution B_t^T (B_t B_t^T)^-1 r2
+                    const double g00 = b0[0] * b0[0] + b0[1] * b0[1] + b0[2] * b0[2];
+                    const double g01 = b0[0] * b1[0] + b0[1] * b1[1] + b0[2] * b1[2];
+                    const double g11 = b1[0] * b1[0] + b1[1] * b1[1] + b1[2] * b1[2];
+                    const double det = g00 * g11 - g01 * g01;
+                    if (!(fabs(det) > 0.)) atomicOr(&s_flag, 2);
+                    const double l0 = (g11 * r2[0] - g01 * r2[1]) / det;
+                    const double l1 = (g00 * r2[1] - g01 * r2[0]) / det;
+                    for (int k = 0; k < 3; ++k) cA[3 + k] = b0[k] * l0 + b1[k] * l1;
+                    nA[3] = b0[1] * b1[2] - b0[2] * b1[1];
+                    nA[4] = b0[2] * b1[0] - b0[0] * b1[2];
+                    nA[5] = b0[0] * b1[1] - b0[1] * b1[0];
+                    if (hH) {
+                        const double* ah = hb + hubsm::ah;
+                        bool ok = joint_target_correction(ah, cA, 1., hb + hubsm::cH);
+                        ok &= joint_target_correction(ah, nA, 0., hb + hubsm::dH);
+                        ok &= joint_target_test(ah, wA, hb + hubsm::wH);
+                        if (!ok) atomicOr(&s_flag, 2);
+                    }
+                }
             }
             __syncthreads();
         }
-        if (tid < nc) {
+        if (drive && tid < nc) {
+            // roots: x_root = c_r + theta d_r from the corrections of the record
+            // they join; d_r waits in rpiv's constrained rows (the LU uses rpiv
+            // below m only) for the second right-hand side
+            double* cr = con + tid * kConStride;
+            const int pr = 6 * pos[KB.con_node[tid]];
+            double c6[6], d6[6];
+            if (is_hub_joint(KB.con_type[tid])) {
+                const double* cb = hb + (hH ? hubsm::cH : hubsm::cA);
+                const double* db = hb + (hH ? hubsm::dH : hubsm::nA);
+                bool ok = joint_target_correction(cr, cb, 1., c6);
+                ok &= joint_target_correction(cr, db, 0., d6);
+                ok &= joint_target_test(cr, hb + (hH ? hubsm::wH : hubsm::wA), cr + conrec::wr);
+                if (!ok) atomicOr(&s_flag, 2);
+            } else {
+                for (int k = 0; k < 3; ++k) {
+                    c6[k] = -cr[conrec::Phi + k];
+                    d6[k] = d6[3 + k] = 0.;
+                }
+                const double rr[3] = {-cr[conrec::Phi + 3], -cr[conrec::Phi + 4], -cr[conrec::Phi + 5]};
+                if (!solve3(cr + conrec::Brot, rr, c6 + 3)) atomicOr(&s_flag, 2);
+                for (int k = 0; k < 6; ++k) cr[conrec::wr + k] = 0.;
+            }
+            for (int k = 0; k < 6; ++k) {
+                xs[pr + k] = c6[k];
+                rpiv[pr + k] = d6[k];
+                cr[conrec::dr + k] = d6[k];
+            }
+        } else if (tid < nc) {
             const double* cr = con + tid * kConStride;
             const int pr = 6 * pos[KB.con_node[tid]];
             double rt[3], rr[3];
@@ -1456,11 +1721,16 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
             for (int k = 0; k < 3; ++k) xs[pr + 3 + k] = y[k];
         }
         __syncthreads();
-        // (S2) free-row right-hand side, folded into column m of A
+        // (S2) free-row right-hand side, folded into column m of A; a drive
+        //      train adds the second right-hand side -A_fr d_r in column m + 1
         for (int i = tid; i < m; i += NT) {
-            double r = bp[i];
-            for (int j = m; j < n6; ++j) r -= static_cast<double>(A[i * ldA + j]) * xs[j];
+            double r = bp[i], r2 = 0.;
+            for (int j = m; j < n6; ++j) {
+                r -= static_cast<double>(A[i * ldA + j]) * xs[j];
+                if (drive) r2 -= static_cast<double>(A[i * ldA + j]) * rpiv[j];
+            }
             A[i * ldA + m] = static_cast<TR>(r);
+            if (drive) A[i * ldA + m + 1] = static_cast<TR>(r2);
         }
         __syncthreads();
         mark(kPhaseEliminate);
@@ -1516,10 +1786,75 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
         }
         // (S4) back substitution U x = y (y in column m): every warp inverts some
         //      diagonal blocks, then warp 0 substitutes block by block.
+        if (drive) {  // second right-hand side (column m + 1) before U's blocks are inverted
+            if (warp == 0 && m > 0) solve_factored_column(A, ldA, m, m + 1, rpiv, lane);
+            __syncthreads();
+        }
         for (int b = warp; b * kPanel < m; b += NW) invert_diag_block(A, ldA, m, b * kPanel, rpiv, lane);
         __syncthreads();
         if (warp == 0 && m > 0) back_substitute_blocked(A, ldA, m, xs, lane);
         __syncthreads();
+        if (drive) {
+            // Shaft rotation theta: x = x1 + theta x2 (x1 = (y1, c_r), x2 = (y2, d_r)).
+            // The equilibrium rows projected on the test vectors lose every
+            // multiplier term (G w = 0 joint by joint), leaving
+            //   sum_roots w_r.(b_r - A_r x) + sum_chain w_n.b_n = 0,
+            // b_n = -cond (sum of G^T lambda at the node + torque); chain nodes
+            // carry no element terms.
+            for (int rowi = warp; rowi < 6 * nc; rowi += NW) {
+                const int c = rowi / 6, k = rowi % 6;
+                const int pr = 6 * pos[KB.con_node[c]];
+                double a1 = 0., a2 = 0.;
+                for (int j = lane; j < n6; j += 32) {
+                    const double arj = static_cast<double>(A[(pr + k) * ldA + j]);
+                    a1 += arj * xs[j];
+                    a2 += arj * (j < m ? static_cast<double>(A[j * ldA + m + 1]) : rpiv[j]);
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+                    a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+                }
+                if (lane == 0) {
+                    con[c * kConStride + conrec::yr + k] = bp[pr + k] - a1;
+                    con[c * kConStride + conrec::s2 + k] = a2;
+                }
+            }
+            __syncthreads();
+            if (tid == 0) {
+                double num = 0., den = 0.;
+                double gj[6] = {0., 0., 0., 0., 0., 0.};  // roots' G_base^T lambda
+                for (int c = 0; c < nc; ++c) {
+                    const double* cr = con + c * kConStride;
+                    for (int k = 0; k < 6; ++k) {
+                        num += cr[conrec::wr + k] * cr[conrec::yr + k];
+                        den += cr[conrec::wr + k] * cr[conrec::s2 + k];
+                    }
+                    if (is_hub_joint(KB.con_type[c])) joint_base_transpose_add(cr, cr + conrec::lam, gj);
+                }
+                const double* rv = hb + hubsm::rev;
+                double bA[6];
+                for (int k = 0; k < 6; ++k) bA[k] = rv[revrec::GtL + k] + (k >= 3 ? rv[revrec::sys + k - 3] : 0.);
+                if (hH) {
+                    const double* ah = hb + hubsm::ah;
+                    joint_base_transpose_add(ah, ah + conrec::lam, bA);
+                    for (int k = 0; k < 6; ++k)
+                        num -= hb[hubsm::wH + k] * P.conditioner * (ah[conrec::Gl + k] + gj[k]);
+                } else {
+                    for (int k = 0; k < 6; ++k) bA[k] += gj[k];
+                }
+                for (int k = 0; k < 6; ++k) num -= hb[hubsm::wA + k] * P.conditioner * bA[k];
+                if (!(fabs(den) > 0.)) atomicOr(&s_flag, 2);
+                hb[hubsm::theta] = num / den;
+            }
+            __syncthreads();
+            const double th = hb[hubsm::theta];
+            for (int i = tid; i < m; i += NT) xs[i] += th * static_cast<double>(A[i * ldA + m + 1]);
+            for (int t = tid; t < 6 * nc; t += NT) {
+                const int pr = 6 * pos[KB.con_node[t / 6]];
+                xs[pr + t % 6] += th * rpiv[pr + t % 6];
+            }
+            __syncthreads();
+        }
         // (S5) multipliers from the constrained rows: grad^T x_l = b_r - A_r x
         for (int rowi = warp; rowi < 6 * nc; rowi += NW) {
             const int c = rowi / 6, k = rowi % 6;
@@ -1614,6 +1949,65 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
                                                : hb + hubsm::pub + 6 * (iter & 1);
                 for (int k = 0; k < 6; ++k) sum[k] += peer[k];
             }
+            if (drive) {
+                // Drive train, from the roots back to the BC: record 2's rows give
+                // the rigid joint's multipliers, record 1's rows (with the torque)
+                // the revolute's five (least squares on the three rotation rows,
+                // consistent once theta balances them), and G_rev,base^T L_rev
+                // is what record 0's BC carries.
+                double sumA[6];
+                if (hH) {
+                    const double* ah = hb + hubsm::ah;
+                    double L[6];
+                    for (int k = 0; k < 3; ++k) L[k] = -sum[k];
+                    const double rr[3] = {-sum[3], -sum[4], -sum[5]};
+                    if (!solve3(ah + conrec::AX, rr, L + 3)) flags = 1.;
+                    for (int k = 0; k < 6; ++k) sumA[k] = 0.;
+                    joint_base_transpose_add(ah, L, sumA);
+                    for (int k = 0; k < 6; ++k) {
+                        const double xl = L[k] - ah[conrec::lam + k];
+                        const double e = xl / (P.atol + P.rtol * fabs(ah[conrec::lam + k]));
+                        total += e * e;
+                        if (tid == NT - 3) hb[hubsm::ah + conrec::xl + k] = xl;
+                    }
+                } else {
+                    for (int k = 0; k < 6; ++k) sumA[k] = sum[k];
+                }
+                const double* rv = hb + hubsm::rev;
+                double g[6];
+                for (int k = 0; k < 6; ++k) g[k] = -sumA[k] - (k >= 3 ? rv[revrec::sys + k - 3] : 0.);
+                const double* u = rv + revrec::xcz;
+                const double* w = rv + revrec::xcy;
+                const double a00 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+                const double a01 = u[0] * w[0] + u[1] * w[1] + u[2] * w[2];
+                const double a11 = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
+                const double r0 = -(u[0] * g[3] + u[1] * g[4] + u[2] * g[5]);
+                const double r1 = -(w[0] * g[3] + w[1] * g[4] + w[2] * g[5]);
+                const double det = a00 * a11 - a01 * a01;
+                if (!(fabs(det) > 0.)) flags = 1.;
+                const double L[5] = {g[0], g[1], g[2], (a11 * r0 - a01 * r1) / det, (a00 * r1 - a01 * r0) / det};
+                for (int k = 0; k < 5; ++k) {
+                    const double xl = L[k] - rv[revrec::lam + k];
+                    const double e = xl / (P.atol + P.rtol * fabs(rv[revrec::lam + k]));
+                    total += e * e;
+                    if (tid == NT - 2) hb[hubsm::rev + revrec::xl + k] = xl;
+                }
+                for (int k = 0; k < 3; ++k) {
+                    sum[k] = -L[k];
+                    sum[3 + k] = u[k] * L[3] + w[k] * L[4];
+                }
+                // the chain nodes' terms of the error sum
+                const double th = hb[hubsm::theta];
+                for (int r = 1; r < chain; ++r) {
+                    const double* rec = r == 1 ? hA : hH;
+                    const double* c0 = hb + (r == 1 ? hubsm::cA : hubsm::cH);
+                    const double* d0 = hb + (r == 1 ? hubsm::nA : hubsm::dH);
+                    for (int k = 0; k < 6; ++k) {
+                        const double e = (c0[k] + th * d0[k]) / (P.atol + P.rtol * fabs(rec[hubrec::q_delta + k] * h));
+                        total += e * e;
+                    }
+                }
+            }
             const double* br = hb + hubsm::bc;
             for (int k = 0; k < 3; ++k) xlh[k] = -br[conrec::lam + k] - sum[k];
             double yr[3] = {0., 0., 0.};
@@ -1657,6 +2051,24 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
                 hb[hubsm::bc + conrec::lam + k] += xlh[k];
             }
         }
+        if (drive && (tid == NT - 2 || tid == NT - 3) && chain_rec()) {
+            double* my_rec = chain_rec();
+            const double th = hb[hubsm::theta];
+            const double* c0 = hb + (tid == NT - 2 ? hubsm::cA : hubsm::cH);
+            const double* d0 = hb + (tid == NT - 2 ? hubsm::nA : hubsm::dH);
+            for (int k = 0; k < 6; ++k) {
+                const double x = c0[k] + th * d0[k];
+                my_rec[hubrec::q_delta + k] += x / h;
+                if (P.dynamic) {
+                    my_rec[hubrec::v + k] += P.gamma_prime * x;
+                    my_rec[hubrec::vd + k] += P.beta_prime * x;
+                }
+            }
+            if (tid == NT - 2)
+                for (int k = 0; k < 5; ++k) hb[hubsm::rev + revrec::lam + k] += hb[hubsm::rev + revrec::xl + k];
+            else
+                for (int k = 0; k < 6; ++k) hb[hubsm::ah + conrec::lam + k] += hb[hubsm::ah + conrec::xl + k];
+        }
         __syncthreads();
         displacement();
         __syncthreads();
@@ -1685,20 +2097,26 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
         const double fac = (1. - P.alpha_f) / (1. - P.alpha_m);
         for (int t = tid; t < n6; t += NT) sa[t] += fac * svd[t];
     }
-    if (hub && tid == NT - 1) {
+    if (hub && chain_rec()) {
+        double* r = chain_rec();
         if (status == KYN_OK) {
             const double fac = (1. - P.alpha_f) / (1. - P.alpha_m);
-            for (int k = 0; k < 6; ++k) hb[hubrec::a + k] += fac * hb[hubrec::vd + k];
-            const double* x0 = hb + hubrec::x0;
-            for (int c = 0; c < 3; ++c) hb[hubrec::x + c] = x0[c] + hb[hubrec::q + c];
-            quat_compose(hb + hubrec::q + 3, x0 + 3, hb + hubrec::x + 3);
+            for (int k = 0; k < 6; ++k) r[hubrec::a + k] += fac * r[hubrec::vd + k];
+            const double* x0 = r + hubrec::x0;
+            for (int c = 0; c < 3; ++c) r[hubrec::x + c] = x0[c] + r[hubrec::q + c];
+            quat_compose(r + hubrec::q + 3, x0 + 3, r + hubrec::x + 3);
         }
-        for (int k = 0; k < 6; ++k) hb[hubrec::lambda + k] = hb[hubsm::bc + conrec::lam + k];
+        const double* lam = (tid == NT - 1) ? hb + hubsm::bc + conrec::lam
+                           : (tid == NT - 2) ? hb + hubsm::rev + revrec::lam : hb + hubsm::ah + conrec::lam;
+        for (int k = 0; k < 6; ++k) r[hubrec::lambda + k] = (tid == NT - 2 && k == 5) ? 0. : lam[k];
     }
     __syncthreads();
     if (hub)  // every beam keeps its copy of the hub state (the input is the caller's)
-        for (int k = tid; k < kHubDoubles; k += NT)
-            if (k < hubrec::input || k >= hubrec::input + 7) slab[L.hub + k] = hb[k];
+        for (int k = tid; k < (drive ? chain : 1) * kHubDoubles; k += NT) {
+            const int r = k / kHubDoubles, e = k % kHubDoubles;
+            const double* src = r == 0 ? hb : r == 1 ? hA : hH;
+            if (e < hubrec::input || e >= hubrec::input + 7) slab[L.hub + k] = src[e];
+        }
     for (int k = tid; k < N * 7; k += NT) {
         slab[L.q + k] = sq[k];
         slab[L.q_prev + k] = sqp[k];

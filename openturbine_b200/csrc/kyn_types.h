@@ -37,7 +37,7 @@ struct SlabLayout {
     int32_t tangent;            // [N][9]  rotational block of the stored tangent
     int32_t con_input;          // [kMaxBeamConstraints][7]
     int32_t lambda;             // [kMaxBeamConstraints][6]
-    int32_t hub;                // [kHubDoubles] hub node of a jointed model (see hubrec)
+    int32_t hub;                // [kHubChain][kHubDoubles] hub chain of a jointed model (hubrec)
     int32_t total;
 };
 
@@ -45,6 +45,14 @@ struct SlabLayout {
 // no beam element, held by one FixedBC / PrescribedBC.  Every beam of the
 // model keeps an identical copy of the hub's state in its slab; every CTA of
 // the model's cluster updates its copy with the same arithmetic.
+//
+// A drive train extends the hub to a chain of up to kHubChain massless nodes:
+// record 0 is the node held by the BC (shaft base), record 1 the target of a
+// revolute joint from it (azimuth), record 2 an optional node rigidly jointed
+// to record 1 (hub).  The beam roots join the last record.  Each record holds
+// its node's state and the constraint that leads into the node: the BC
+// (record 0), the revolute joint with its frame in `axes` and its torque in
+// input[0] (record 1), the rigid joint (record 2).
 namespace hubrec {
 constexpr int x0 = 0;       // [7]
 constexpr int q = 7;        // [7]
@@ -55,11 +63,13 @@ constexpr int vd = 34;      // [6]
 constexpr int a = 40;       // [6]
 constexpr int q_delta = 46; // [6]
 constexpr int tangent = 52; // [9] rotational block of the stored tangent
-constexpr int input = 61;   // [7] hub BC input (PrescribedBC displacement)
-constexpr int lambda = 68;  // [6] hub BC multipliers
-constexpr int X0 = 74;      // [3] hub BC X0 (FixedBC)
+constexpr int input = 61;   // [7] hub BC input (PrescribedBC displacement); revolute torque
+constexpr int lambda = 68;  // [6] multipliers of the constraint leading into the node
+constexpr int X0 = 74;      // [3] hub BC X0 (FixedBC); joints: node x0 - previous node x0
+constexpr int axes = 77;    // [9] revolute joint frame, row 0 = joint axis
 }  // namespace hubrec
-constexpr int kHubDoubles = 78;
+constexpr int kHubDoubles = 86;  // one record
+constexpr int kHubChain = 3;
 
 KYN_HD inline SlabLayout make_slab_layout(int N, int Q) {
     SlabLayout L{};
@@ -90,7 +100,7 @@ KYN_HD inline SlabLayout make_slab_layout(int N, int Q) {
     L.tangent = take(N * 9);
     L.con_input = take(kMaxBeamConstraints * 7);
     L.lambda = take(kMaxBeamConstraints * 6);
-    L.hub = take(kHubDoubles);
+    L.hub = take(kHubChain * kHubDoubles);
     L.total = o;
     return L;
 }
@@ -105,6 +115,8 @@ constexpr int kSpringRec = 7;
 // Joints between the hub node and a target node (six rows, base blocks on the
 // hub): KYN_CONSTRAINT_RIGID_JOINT (3) and KYN_CONSTRAINT_ROTATION_CONTROL (5).
 KYN_HD inline bool is_hub_joint(int type) { return type == 3 || type == 5; }
+// Rows of a constraint (src/constraints/constraint_type.hpp NumRowsForConstraint).
+KYN_HD inline int constraint_rows(int type) { return type == 4 ? 5 : 6; }
 
 struct KBeam {
     double* slab;             // device slab of this beam
@@ -120,7 +132,7 @@ struct KBeam {
     double con_axis[kMaxBeamConstraints][3]; // RotationControl: unit rotation axis
     const double* lumped;     // point masses then springs at this beam's nodes, or null
     int32_t n_mass, n_spring; // (records of kMassRec / kSpringRec doubles, node-local indices)
-    int32_t hub;              // 1: the model has a hub (joints in con_type)
+    int32_t hub;              // hub chain length: 0 none, 1 hub, 2-3 drive train
     int32_t hub_con_type;     // KYN_CONSTRAINT_FIXED_BC / PRESCRIBED_BC on the hub
     double gravity[3];
     double* conv;             // [kMaxNewtonIters] model convergence history (rank 0)

@@ -1,6 +1,7 @@
 // The reference's regression drivers written against the C++ shim (kynema_b200.hpp):
-// test_cantilever_beam.cpp:31-138, test_rotating_beam.cpp:93-150 and :390-456
-// (rotation control), test_spring_mass_system.cpp:23-96, same inputs, same golden
+// test_cantilever_beam.cpp:31-138, test_rotating_beam.cpp:93-150, :390-456
+// (rotation control) and :581-680 (generator torque on a revolute joint),
+// test_spring_mass_system.cpp:23-96, same inputs, same golden
 // tolerances.  Exit code 0 on success.
 #include <cmath>
 #include <cstdio>
@@ -110,6 +111,41 @@ static void rotation_control(const Context& ctx) {
     for (int c = 0; c < 7; ++c) expect_near(q[5 * 7 + c], tip[c], 1e-6, "rotation control tip q");
 }
 
+// test_rotating_beam.cpp:581-680 (GeneratorTorqueWithAxisTilt): shaft base (fixed) ->
+// revolute joint about the tilted shaft -> azimuth -> rigid -> hub -> rigid -> blade
+// root, generator torque read through the pointer before each Step; azimuth q, v and
+// the joint output after 10 steps at the test's 1e-6
+static void generator_torque(const Context& ctx, double tilt, const double (&az_q)[7],
+                             const double (&az_v)[6], const double (&out)[3]) {
+    const std::vector<double> node_s{0., 0.11747233803526763, 0.35738424175967748, 0.64261575824032247, 0.88252766196473242, 1.};
+    Model model;
+    model.SetGravity(0., 0., 0.);
+    std::vector<size_t> ids;
+    for (double s : node_s) ids.push_back(model.AddNode().SetElemLocation(s).SetPosition(10 * s, 0., 0., 1., 0., 0., 0.).Build());
+    const std::vector<BeamSection> sections{BeamSection(0., kMass, kStiff), BeamSection(1., kMass, kStiff)};
+    model.AddBeamElement(ids, sections, kGauss7);
+    model.TranslateBeam(0, {2., 0., 0.});
+    model.RotateBeamAboutPoint(0, RotationVectorToQuaternion({tilt, 0., 0.}), {0., 0., 0.});
+    const size_t shaft = model.AddNode().SetPosition(0., 0., 0., 1., 0., 0., 0.).Build();
+    const size_t azimuth = model.AddNode().SetPosition(0., 0., 0., 1., 0., 0., 0.).Build();
+    const size_t hub = model.AddNode().SetPosition(0., std::sin(tilt), std::cos(tilt), 1., 0., 0., 0.).Build();
+    model.AddFixedBC(shaft);
+    double torque = 100.;
+    const size_t rj = model.AddRevoluteJointConstraint({shaft, azimuth}, {0., std::sin(tilt), std::cos(tilt)}, &torque);
+    model.AddRigidJointConstraint({azimuth, hub});
+    model.AddRigidJointConstraint({hub, ids.front()});
+    auto [state, elements, constraints, solver] = model.CreateSystemWithSolver(ctx);
+    auto parameters = StepParameters(true, 5, 0.01, 0.);
+    for (int i = 0; i < 10; ++i)
+        if (!Step(parameters, solver, elements, state, constraints)) { std::printf("FAIL generator torque step %d\n", i); ++failures; }
+    const auto q = state.q();
+    const auto v = state.v();
+    const auto o = constraints.output();
+    for (int c = 0; c < 7; ++c) expect_near(q[azimuth * 7 + c], az_q[c], 1e-6, "generator torque azimuth q");
+    for (int c = 0; c < 6; ++c) expect_near(v[azimuth * 6 + c], az_v[c], 1e-6, "generator torque azimuth v");
+    for (int c = 0; c < 3; ++c) expect_near(o[rj * 3 + c], out[c], 1e-6, "generator torque joint output");
+}
+
 // test_spring_mass_system.cpp:23-96: a mass on a spring to a fixed node, no beam element
 static void spring_mass(const Context& ctx) {
     Model model;
@@ -135,6 +171,10 @@ int main() {
         cantilever(ctx);
         rotating_beam(ctx);
         rotation_control(ctx);
+        generator_torque(ctx, 0., {0., 0., 0., 0.99998634, 0., 0., -0.0052267}, {0., 0., 0., 0., 0., -0.18978539},
+                         {-0.01045353, -0.18978539, -0.566558});
+        generator_torque(ctx, 3.14159265358979323846 / 2., {0., 0., 0., 0.99998634, 0., -0.0052267, 0.},
+                         {0., 0., 0., 0., -0.18978539, 0.}, {-0.01045353, -0.18978539, -0.566560});
         spring_mass(ctx);
     } catch (const std::exception& e) {
         std::printf("FAIL exception: %s\n", e.what());

@@ -1,0 +1,129 @@
+"""Drive train with a revolute joint (test_rotating_beam.cpp:516-680): a blade
+on a hub that turns freely about a shaft axis, held by a revolute joint from a
+fixed shaft base, with or without an azimuth node between them and with a
+generator torque.  The GPU path eliminates the shaft rotation from the beam's
+system (second right-hand side, one projected equation); the oracle solves the
+whole bordered system densely.  Same CRS graph, same Newton decisions, states
+and multipliers within the parity tolerances, and the reference's golden
+values."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle.oracle_py import OracleModel
+from tests.test_gpu_hub import HubTwin
+from tests.test_gpu_parity import FIELDS, assert_state_close
+from tests.workloads_ref import generator_torque_model, load_golden, revolute_joint_test_model
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from openturbine_b200.runtime import Context
+    c = Context(0)
+    yield c
+    c.close()
+
+
+def _crs_equal(ctx, pm):
+    mid = ctx.create_model(pm)
+    rp, ci, _ = ctx.crs(mid, values=False)
+    orp, oci, _ = OracleModel(pm).crs()
+    assert np.array_equal(rp, orp) and np.array_equal(ci, oci)
+    return mid
+
+
+# Multipliers are reaction forces and moments: the beam's internal force at the
+# root is the axial stiffness times a strain formed as a difference of O(1)
+# terms, so any FP64 evaluation carries an absolute rounding floor of about
+# EA x machine epsilon on them, whatever the summation order (the oracle's
+# reversed-quadrature twin shares the per-point arithmetic and does not see it).
+# With the 0.1 rad/s spin of the revolute test the reactions are ~5e-3, where
+# that floor (EA = 1.368e6 N: 3e-10) dominates a relative bound.
+EA = 1.36817e6
+EPS = np.finfo(np.float64).eps
+
+
+def assert_multipliers_close(ctx, mid, tw):
+    lg, lo = ctx.state(mid, "lambda"), tw.state("lambda")
+    tol = max(10.0 * tw.floor("lambda") * np.abs(lo).max(), 1e-10 * np.abs(lo).max(), 10.0 * EA * EPS)
+    assert np.abs(lg - lo).max() <= tol, (np.abs(lg - lo).max(), tol)
+
+
+def _run(ctx, mid, tw, p, rj, torque, steps):
+    for _ in range(steps):
+        ctx.set_control(mid, rj, torque)
+        tw.set_prescribed(rj, [torque, 0., 0., 1., 0., 0., 0.])
+        st, it = ctx.step([mid], p)
+        ost, oit = tw.step(p)
+        assert (st[0], it[0]) == (ost, oit) == (0, oit)
+        gc, oc = ctx.convergence(mid), tw.convergence()
+        assert len(gc) == len(oc)
+        for a, b in zip(gc, oc):
+            assert (a <= 1.0) == (b <= 1.0)
+            if b > 1.0:
+                assert abs(a - b) <= 1e-6 * b, (a, b)
+
+
+def test_revolute_joint_matches_oracle_and_golden(ctx):
+    """RevoluteJointConstraint: ground (fixed) -> revolute about z -> hub ->
+    rigid joint -> blade root, zero torque, 5 steps; q of all 8 nodes against
+    the golden values at the test's 1e-6."""
+    g = load_golden("revolute_joint.json")["revolute"]
+    m, p, rj = revolute_joint_test_model()
+    pm = m.pack()
+    mid = _crs_equal(ctx, pm)
+    info = ctx.info(mid)
+    assert info.num_dofs == 8 * 6 + 6 + 5 + 6
+    tw = HubTwin(pm)
+    _run(ctx, mid, tw, p, rj, 0.0, g["steps"])
+    assert_state_close(ctx, mid, tw, fields=FIELDS, lam=False)
+    assert_multipliers_close(ctx, mid, tw)
+    np.testing.assert_allclose(ctx.state(mid, "q").ravel(), g["q"], rtol=0, atol=g["tolerance"])
+    ctx.destroy_model(mid)
+
+
+@pytest.mark.parametrize("key", ["tilt0", "tilt90"])
+def test_generator_torque_matches_oracle_and_golden(ctx, key):
+    """GeneratorTorque_Tilt0 / _Tilt90: shaft base (fixed) -> revolute about
+    the tilted shaft -> azimuth -> rigid -> hub -> rigid -> blade root under a
+    100 N m torque, 10 steps; azimuth q and v and the joint output (rotation,
+    rate, acceleration about the shaft) against the golden values at 1e-6."""
+    g = load_golden("revolute_joint.json")["generator_torque"]
+    m, p, rj, az = generator_torque_model(0.0 if key == "tilt0" else math.pi / 2.)
+    pm = m.pack()
+    mid = _crs_equal(ctx, pm)
+    tw = HubTwin(pm)
+    _run(ctx, mid, tw, p, rj, g["torque"], g["steps"])
+    assert_state_close(ctx, mid, tw, fields=FIELDS, lam=False)
+    assert_multipliers_close(ctx, mid, tw)
+    out = ctx.state(mid, "output")
+    np.testing.assert_allclose(out, tw.o.state("output"), rtol=0, atol=1e-12)
+    np.testing.assert_allclose(ctx.state(mid, "q")[az], g[key]["azimuth_q"], rtol=0, atol=g["tolerance"])
+    np.testing.assert_allclose(ctx.state(mid, "v")[az], g[key]["azimuth_v"], rtol=0, atol=g["tolerance"])
+    np.testing.assert_allclose(out[rj], g[key]["output"], rtol=0, atol=g["tolerance"])
+    ctx.destroy_model(mid)
+
+
+def test_drive_train_restart_and_state_copy(ctx):
+    """The drive-train records travel with the state: a copy made after 3
+    steps and stepped 2 more matches the original stepped 2 more."""
+    m, p, rj, _ = generator_torque_model(0.0)
+    pm = m.pack()
+    a = ctx.create_model(pm)
+    b = ctx.create_model(pm)
+    for _ in range(3):
+        ctx.set_control(a, rj, 100.0)
+        ctx.step([a], p)
+    ctx.copy_state(b, a)
+    for _ in range(2):
+        for mid in (a, b):
+            ctx.set_control(mid, rj, 100.0)
+        st, _ = ctx.step([a, b], p)
+        assert list(st) == [0, 0]
+    for f in ("q", "v", "vd", "a", "lambda"):
+        np.testing.assert_array_equal(ctx.state(a, f), ctx.state(b, f))
+    ctx.destroy_model(a)
+    ctx.destroy_model(b)
