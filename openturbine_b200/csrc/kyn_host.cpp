@@ -352,8 +352,6 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
             return fail(err, KYN_ERR_INVALID, "revolute joint nodes out of range");
         if (M.node_beam[sb] >= 0 || M.node_beam[az] >= 0)
             return fail(err, KYN_ERR_UNSUPPORTED, "a revolute joint must join two nodes outside the beams");
-        if (M.beams.size() != 1)
-            return fail(err, KYN_ERR_UNSUPPORTED, "a drive train turns one beam system in this path");
         M.chain = {sb, az};
         for (int c = 0; c < ncon; ++c) {
             const int t = d->constraint_target_node[c];

@@ -271,6 +271,8 @@ constexpr int dH = 562;    // [6] record-2 correction per unit shaft rotation
 constexpr int wA = 568;    // [6] record-1 test vector
 constexpr int wH = 574;    // [6] record-2 test vector
 constexpr int theta = 580; // shaft rotation of the Newton correction
+constexpr int xt = 584;    // [2][8] this beam's part of the shaft equation (num, den,
+                           // G_base^T lambda of its joints), exchanged over the cluster
 }  // namespace hubsm
 
 // Revolute joint record (doubles, at hubsm::rev).
@@ -1820,16 +1822,28 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
                 }
             }
             __syncthreads();
-            if (tid == 0) {
-                double num = 0., den = 0.;
-                double gj[6] = {0., 0., 0., 0., 0., 0.};  // roots' G_base^T lambda
+            double* xt = hb + hubsm::xt + 8 * (iter & 1);
+            if (tid == 0) {  // this beam's roots: w.s1, w.s2 and G_base^T lambda
+                for (int k = 0; k < 8; ++k) xt[k] = 0.;
                 for (int c = 0; c < nc; ++c) {
                     const double* cr = con + c * kConStride;
                     for (int k = 0; k < 6; ++k) {
-                        num += cr[conrec::wr + k] * cr[conrec::yr + k];
-                        den += cr[conrec::wr + k] * cr[conrec::s2 + k];
+                        xt[0] += cr[conrec::wr + k] * cr[conrec::yr + k];
+                        xt[1] += cr[conrec::wr + k] * cr[conrec::s2 + k];
                     }
-                    if (is_hub_joint(KB.con_type[c])) joint_base_transpose_add(cr, cr + conrec::lam, gj);
+                    if (is_hub_joint(KB.con_type[c])) joint_base_transpose_add(cr, cr + conrec::lam, xt + 2);
+                }
+            }
+            if (clustered) cluster.sync(); else __syncthreads();
+            if (tid == 0) {
+                // every CTA sums the beams' parts in rank order, so all find the same theta
+                double num = 0., den = 0.;
+                double gj[6] = {0., 0., 0., 0., 0., 0.};  // roots' G_base^T lambda
+                for (int r = 0; r < KB.model_beams; ++r) {
+                    const double* peer = clustered ? cluster.map_shared_rank(xt, r) : xt;
+                    num += peer[0];
+                    den += peer[1];
+                    for (int k = 0; k < 6; ++k) gj[k] += peer[2 + k];
                 }
                 const double* rv = hb + hubsm::rev;
                 double bA[6];
