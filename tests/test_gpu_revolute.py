@@ -11,6 +11,7 @@ import math
 import numpy as np
 import pytest
 
+from openturbine_b200.model import StepParameters
 from oracle.oracle_py import OracleModel
 from tests.test_gpu_hub import HubTwin
 from tests.test_gpu_parity import FIELDS, assert_state_close
@@ -175,3 +176,71 @@ def test_drive_train_restart_and_state_copy(ctx):
         np.testing.assert_array_equal(ctx.state(a, f), ctx.state(b, f))
     ctx.destroy_model(a)
     ctx.destroy_model(b)
+
+
+def test_drive_trains_batched_with_beams(ctx):
+    """Drive-train models batched with plain cantilevers and hub rotors in one
+    step call (one launch bucket per instance and size class): every model's
+    state equals the state it reaches stepped alone."""
+    from openturbine_b200 import workloads as W
+    from tests.workloads_ref import rotation_control_test_model
+    specs = [("gen", generator_torque_model(0.0)), ("three", _three_blade_drive_train(True)),
+             ("rev", revolute_joint_test_model())]
+    beams = [W.batch_cantilever_model(d) for d in W.draw_batch(6, first_id=900)]
+    rc_model, rc_p, rc, _ = rotation_control_test_model(False)
+    p = W.batch_params(6)
+
+    def build():
+        ids, ctl = [], []
+        for _, sp in specs:
+            ids.append(ctx.create_model(sp[0].pack()))
+            ctl.append(sp[2])
+        for b in beams:
+            ids.append(ctx.create_model(b.pack()))
+        ids.append(ctx.create_model(rc_model.pack()))
+        return ids, ctl
+
+    def advance(ids, ctl, k, together):
+        for mid, cid in zip(ids, ctl):
+            ctx.set_control(mid, cid, 20.0)
+        ctx.set_control(ids[-1], rc, 0.01 * (k + 1))
+        if together:
+            return list(ctx.step(ids, p)[0])
+        return [int(ctx.step([mid], p)[0][0]) for mid in ids]
+
+    a_ids, ctl = build()
+    b_ids, _ = build()
+    for k in range(4):
+        sa = advance(a_ids, ctl, k, True)
+        sb = advance(b_ids, ctl, k, False)
+        assert sa == sb
+    for ia, ib in zip(a_ids, b_ids):
+        for f in ("q", "v", "lambda"):
+            np.testing.assert_array_equal(ctx.state(ia, f), ctx.state(ib, f))
+    for mid in a_ids + b_ids:
+        ctx.destroy_model(mid)
+
+
+def test_drive_train_fp32_form_close_to_fp64(ctx):
+    """The FP32 form (FP32 tangent and LU, FP64 residual and update) on the
+    generator-torque drive train: same convergence, azimuth rotation and joint
+    output within 1e-8 of the FP64 form."""
+    m, p, rj, az = generator_torque_model(0.0)
+    pm = m.pack()
+    a = ctx.create_model(pm)
+    b = ctx.create_model(pm)
+    p32 = StepParameters(p.is_dynamic_solve, p.max_iter, p.h, p.rho_inf, p.absolute_convergence_tol,
+                         p.relative_convergence_tol, precision=1, refine_iters=1)
+    for _ in range(10):
+        for mid in (a, b):
+            ctx.set_control(mid, rj, 100.0)
+        sa, _ = ctx.step([a], p)
+        sb, _ = ctx.step([b], p32)
+        assert sa[0] == sb[0] == 0
+    qa, qb = ctx.state(a, "q"), ctx.state(b, "q")
+    assert np.abs(qa - qb).max() <= 1e-8 * np.abs(qa).max()
+    oa, ob = ctx.state(a, "output")[rj], ctx.state(b, "output")[rj]
+    assert np.abs(oa - ob).max() <= 1e-8 * np.abs(oa).max()
+    ctx.destroy_model(a)
+    ctx.destroy_model(b)
+
