@@ -158,7 +158,9 @@ def test_three_blade_drive_train_matches_oracle(ctx, with_azimuth):
 
 def test_drive_train_restart_and_state_copy(ctx):
     """The drive-train records travel with the state: a copy made after 3
-    steps and stepped 2 more matches the original stepped 2 more."""
+    steps and stepped 2 more matches the original stepped 2 more; so do a model
+    read from the original's restart record and a clone, and the batched
+    motion read returns the drive-train nodes' rows."""
     m, p, rj, _ = generator_torque_model(0.0)
     pm = m.pack()
     a = ctx.create_model(pm)
@@ -174,8 +176,27 @@ def test_drive_train_restart_and_state_copy(ctx):
         assert list(st) == [0, 0]
     for f in ("q", "v", "vd", "a", "lambda"):
         np.testing.assert_array_equal(ctx.state(a, f), ctx.state(b, f))
-    ctx.destroy_model(a)
-    ctx.destroy_model(b)
+    # restart record round trip and clone: both continue like the original
+    rec = ctx.write_restart(a)
+    c = ctx.create_model(pm)
+    ctx.read_restart(c, rec)
+    d = ctx.clone_model(a)
+    for _ in range(2):
+        for mid in (a, c, d):
+            ctx.set_control(mid, rj, 100.0)
+        st, _ = ctx.step([a, c, d], p)
+        assert list(st) == [0, 0, 0]
+    for f in ("q", "v", "vd", "lambda"):
+        np.testing.assert_array_equal(ctx.state(a, f), ctx.state(c, f))
+        np.testing.assert_array_equal(ctx.state(a, f), ctx.state(d, f))
+    # the batched motion read carries the drive-train nodes' rows too
+    n = ctx.info(a).num_nodes
+    q = np.zeros((2, n, 7))
+    ctx.get_state_batch(np.array([a, c], dtype=np.int32), "q", q.ctypes.data, False)
+    np.testing.assert_array_equal(q[0], ctx.state(a, "q"))
+    np.testing.assert_array_equal(q[1], ctx.state(c, "q"))
+    for mid in (a, b, c, d):
+        ctx.destroy_model(mid)
 
 
 def test_drive_trains_batched_with_beams(ctx):
