@@ -79,7 +79,12 @@ enum {
                                         slot Constraints::UpdateViews fills from the control
                                         pointer (src/constraints/constraints.hpp:345-352;
                                         src/constraints/calculate_rotation_control_constraint.hpp:17-144,
-                                        src/model/model.hpp:550-562) */
+                                        src/model/model.hpp:550-562) */,
+    KYN_CONSTRAINT_FIXED_BC_3DOF = 6,      /* three rows on a position-only node (model.hpp:570-583) */
+    KYN_CONSTRAINT_PRESCRIBED_BC_3DOF = 7, /* three rows, input = the node's displacement */
+    KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF = 8 /* three rows: a position-only target rigidly
+                                        carried by a six-DOF base (model.hpp:599-611;
+                                        src/constraints/calculate_rigid_joint_3DOF_constraint.hpp) */
 };
 
 /* Node-state fields readable with kyn_get_state (src/state/state.hpp:18-68,

@@ -32,6 +32,9 @@ PRESCRIBED_BC = 2
 RIGID_JOINT = 3
 REVOLUTE_JOINT = 4
 ROTATION_CONTROL = 5
+FIXED_BC_3DOF = 6
+PRESCRIBED_BC_3DOF = 7
+RIGID_JOINT_6DOF_TO_3DOF = 8
 INVALID_NODE_ID = 0  # Model::InvalidNodeID
 
 
@@ -472,6 +475,28 @@ class Model:
         self.constraints_.append(Constraint(cid, PRESCRIBED_BC, (INVALID_NODE_ID, int(node_id)),
                                             (0.0, 0.0, 0.0),
                                             tuple(float(x) for x in initial_displacement)))
+        return cid
+
+    def AddFixedBC3DOFs(self, node_id: int) -> int:
+        """src/model/model.hpp:570-583: fixes the position of a position-only node."""
+        cid = len(self.constraints_)
+        self.constraints_.append(Constraint(cid, FIXED_BC_3DOF, (INVALID_NODE_ID, int(node_id))))
+        return cid
+
+    def AddPrescribedBC3DOFs(self, node_id: int,
+                             initial_displacement=(0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0)) -> int:
+        """src/model/model.hpp:585-597: prescribes the position of a position-only node."""
+        cid = len(self.constraints_)
+        self.constraints_.append(Constraint(cid, PRESCRIBED_BC_3DOF, (INVALID_NODE_ID, int(node_id)),
+                                            (0.0, 0.0, 0.0),
+                                            tuple(float(x) for x in initial_displacement)))
+        return cid
+
+    def AddRigidJoint6DOFsTo3DOFs(self, node_ids) -> int:
+        """src/model/model.hpp:599-611 AddRigidJoint6DOFsTo3DOFs({base, target}):
+        a position-only target carried rigidly by a six-DOF base."""
+        cid = len(self.constraints_)
+        self.constraints_.append(Constraint(cid, RIGID_JOINT_6DOF_TO_3DOF, (int(node_ids[0]), int(node_ids[1]))))
         return cid
 
     def AddRigidJointConstraint(self, node_ids) -> int:

@@ -669,6 +669,7 @@ void update_spring(orc_model& m, OSpring& S) {
 // src/constraints/calculate_constraint_residual_gradient.hpp:60-199 (FixedBC, PrescribedBC)
 void update_rigid_joint(orc_model& m, OConstraint& C);
 void update_revolute_joint(orc_model& m, OConstraint& C);
+void update_3dof_constraint(orc_model& m, OConstraint& C);
 
 void update_constraint(orc_model& m, OConstraint& C) {
     if (C.type == KYN_CONSTRAINT_RIGID_JOINT || C.type == KYN_CONSTRAINT_ROTATION_CONTROL) {
@@ -677,6 +678,10 @@ void update_constraint(orc_model& m, OConstraint& C) {
     }
     if (C.type == KYN_CONSTRAINT_REVOLUTE_JOINT) {
         update_revolute_joint(m, C);
+        return;
+    }
+    if (C.type >= KYN_CONSTRAINT_FIXED_BC_3DOF) {
+        update_3dof_constraint(m, C);
         return;
     }
     const double* nu = &m.q[C.target * 7];
@@ -807,6 +812,49 @@ void update_revolute_joint(orc_model& m, OConstraint& C) {
     }
 }
 
+// Three-row constraints on a position-only target
+// (calculate_fixed_bc_3DOF_constraint.hpp, calculate_prescribed_bc_3DOF_constraint.hpp,
+// calculate_rigid_joint_3DOF_constraint.hpp with their branches of
+// calculate_constraint_residual_gradient.hpp:101-150, 196-248): residual
+// u2 + X0 - u1 - R1 X0 (FixedBC: u1 = 0, R1 = I; PrescribedBC: (u1, R1) = the
+// input; joint: the base node's displacement), target gradient I on the
+// translation, joint base gradient [-I, tilde(R1 X0)].
+void update_3dof_constraint(orc_model& m, OConstraint& C) {
+    const double* tu = &m.q[C.target * 7];
+    double u1[3] = {0., 0., 0.};
+    double R1[4] = {1., 0., 0., 0.};
+    if (C.type == KYN_CONSTRAINT_PRESCRIBED_BC_3DOF) {
+        for (int i = 0; i < 3; ++i) u1[i] = C.input[i];
+        for (int i = 0; i < 4; ++i) R1[i] = C.input[3 + i];
+    } else if (C.type == KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF) {
+        const double* bu = &m.q[C.base * 7];
+        for (int i = 0; i < 3; ++i) u1[i] = bu[i];
+        for (int i = 0; i < 4; ++i) R1[i] = bu[3 + i];
+    }
+    const V3 R1X0 = rotate_vec(R1, C.X0);
+    for (int c = 0; c < 3; ++c) C.res[c] = tu[c] + C.X0[c] - u1[c] - R1X0[c];
+    for (int c = 3; c < 6; ++c) C.res[c] = 0.;
+    M6 tg{}, bg{};
+    for (int c = 0; c < 3; ++c) tg[c * 7] = 1.;
+    if (C.type == KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF) {
+        for (int c = 0; c < 3; ++c) bg[c * 7] = -1.;
+        const double tl[9] = {0., -R1X0[2], R1X0[1], R1X0[2], 0., -R1X0[0], -R1X0[1], R1X0[0], 0.};
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) bg[i * 6 + 3 + j] = tl[i * 3 + j];
+    }
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) {
+            C.t_grad_trans[i * 6 + j] = tg[j * 6 + i];
+            C.b_grad_trans[i * 6 + j] = bg[j * 6 + i];
+        }
+    gemm(false, false, 6, 6, 6, 1., tg.data(), 6, &m.tangent[C.target * 36], 6, 0., C.t_grad_tan, 6);
+    gemv(false, 6, 6, 1., C.t_grad_trans, 6, C.lambda, 0., C.t_lambda_res);
+    if (C.type == KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF) {
+        gemm(false, false, 6, 6, 6, 1., bg.data(), 6, &m.tangent[C.base * 36], 6, 0., C.b_grad_tan, 6);
+        gemv(false, 6, 6, 1., C.b_grad_trans, 6, C.lambda, 0., C.b_lambda_res);
+    }
+}
+
 // src/constraints/calculate_revolute_joint_output.hpp:24-85: rotation about
 // the joint axis (axis turned by the target's rotation, dotted with the
 // rotation vector of that rotation), angular velocity and acceleration about
@@ -837,9 +885,10 @@ void revolute_output(const orc_model& m, OConstraint& C) {
 void solve_eliminated(orc_model& m);
 
 void solve_dense(orc_model& m) {
-    bool revolute = false;
-    for (auto& C : m.cons) revolute = revolute || C.type == KYN_CONSTRAINT_REVOLUTE_JOINT;
-    if ((m.solver_mode & 1) && !revolute) {
+    bool special = false;  // rows the single-node elimination does not cover
+    for (auto& C : m.cons)
+        special = special || C.type == KYN_CONSTRAINT_REVOLUTE_JOINT || C.type >= KYN_CONSTRAINT_FIXED_BC_3DOF;
+    if ((m.solver_mode & 1) && !special) {
         solve_eliminated(m);
         return;
     }
@@ -1416,8 +1465,10 @@ orc_model* orc_model_create(const kyn_model_desc* d, char* err, int errlen) {
         OConstraint& C = m->cons[c];
         C.type = d->constraint_type[c];
         const bool joint = C.type == KYN_CONSTRAINT_RIGID_JOINT || C.type == KYN_CONSTRAINT_ROTATION_CONTROL ||
-                           C.type == KYN_CONSTRAINT_REVOLUTE_JOINT;
-        if (C.type != KYN_CONSTRAINT_FIXED_BC && C.type != KYN_CONSTRAINT_PRESCRIBED_BC && !joint) {
+                           C.type == KYN_CONSTRAINT_REVOLUTE_JOINT ||
+                           C.type == KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF;
+        const bool three = C.type >= KYN_CONSTRAINT_FIXED_BC_3DOF && C.type <= KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF;
+        if (C.type != KYN_CONSTRAINT_FIXED_BC && C.type != KYN_CONSTRAINT_PRESCRIBED_BC && !joint && !three) {
             bad(err, errlen, "constraint type outside this path");
             delete m;
             return nullptr;
@@ -1435,16 +1486,17 @@ orc_model* orc_model_create(const kyn_model_desc* d, char* err, int errlen) {
             return nullptr;
         }
         C.base_active = joint ? 6 : 0;
-        C.target_active = 6;
-        // src/constraints/constraint_type.hpp NumRowsForConstraint: 5 for a revolute joint
-        const int rows = C.type == KYN_CONSTRAINT_REVOLUTE_JOINT ? 5 : 6;
+        C.target_active = three ? 3 : 6;
+        // src/constraints/constraint_type.hpp NumRowsForConstraint: 5 for a revolute
+        // joint, 3 for the three-row constraints on position-only nodes
+        const int rows = C.type == KYN_CONSTRAINT_REVOLUTE_JOINT ? 5 : three ? 3 : 6;
         C.row_first = start_row;
         C.row_last = start_row + rows;
         start_row += rows;
         const double axis[3] = {d->constraint_axis ? d->constraint_axis[c * 3] : 0.,
                                 d->constraint_axis ? d->constraint_axis[c * 3 + 1] : 0.,
                                 d->constraint_axis ? d->constraint_axis[c * 3 + 2] : 0.};
-        if (C.type == KYN_CONSTRAINT_FIXED_BC) {
+        if (C.type == KYN_CONSTRAINT_FIXED_BC || C.type == KYN_CONSTRAINT_FIXED_BC_3DOF) {
             for (int k = 0; k < 3; ++k) C.X0[k] = m->x0[C.target * 7 + k] - axis[k];
         } else if (joint) {
             // src/constraints/constraints.hpp:268-290: relative position target - base
@@ -1510,7 +1562,8 @@ orc_model* orc_model_create(const kyn_model_desc* d, char* err, int errlen) {
         m->sig[S.n2] |= 0b111000U;
     }
     for (auto& C : m->cons) {
-        m->sig[C.target] |= 0b111111U;
+        // FreedomSignature: JustPosition on the target of a three-row constraint
+        m->sig[C.target] |= (C.target_active == 3) ? 0b111000U : 0b111111U;
         if (C.base_active) m->sig[C.base] |= 0b111111U;
     }
     m->active.resize(nn);

@@ -18,6 +18,8 @@ Sources (paths relative to the reference project root):
   tests/unit_tests/system/beams/test_curved_beam.hpp         kernel-level data
   tests/regression_tests/interfaces/test_blade_interface.cpp + its WindIO file
                                                              IEA-15 blade input, tip
+  tests/regression_tests/regression/test_heavy_top.cpp         heavy top q (three-row
+                                                             constraints)
   tests/regression_tests/regression/test_masses.cpp,
     test_precession.cpp, test_spring_mass_system.cpp          point masses, springs
 """
@@ -207,6 +209,15 @@ def main(ref: str) -> None:
                "revolute": {"steps": 5, "q": view_after(rb[j0:j1], "state.q,"), "tolerance": 1e-6},
                "generator_torque": dict(gen, steps=10, torque=100.0, tolerance=1e-6)},
               open(os.path.join(out_dir, "revolute_joint.json"), "w"), indent=1)
+
+    # ---- heavy top (three-row constraints on a position-only ground node) -----------
+    ht = strip_comments(open(os.path.join(reg, "test_heavy_top.cpp")).read())
+    qv = [(int(m.group(1)), float(m.group(2)), float(m.group(3))) for m in
+          re.finditer(r"EXPECT_NEAR\(\s*q\[0\]\[(\d)\],\s*(" + NUM + r"),\s*(" + NUM + r")\)", ht)]
+    json.dump({"source": "tests/regression_tests/regression/test_heavy_top.cpp",
+               "steps": 400, "q_mass_node": [v for _, v, _ in sorted(qv)],
+               "tolerance": max(t for _, _, t in qv)},
+              open(os.path.join(out_dir, "heavy_top.json"), "w"), indent=1)
 
     # ---- point masses and springs -------------------------------------------------
     def near_calls(text: str, name: str):

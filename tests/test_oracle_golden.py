@@ -197,6 +197,20 @@ def test_generator_torque(key):
     np.testing.assert_allclose(o.state("output")[rj], g[key]["output"], rtol=0, atol=g["tolerance"])
 
 
+def test_heavy_top_final_rotation():
+    """test_heavy_top.cpp:9-75: the top's q after 400 steps (0.8 s) at the
+    test's 1e-10; the ground node carries three DOFs (15 DOFs in all)."""
+    from tests.workloads_ref import heavy_top_model
+    g = load_golden("heavy_top.json")
+    m, p, _ = heavy_top_model()
+    o = OracleModel(m.pack())
+    assert o.info.num_dofs == 6 + 3 + 3 + 3
+    for _ in range(g["steps"]):
+        st, _ = o.step(p)
+        assert st == 0
+    np.testing.assert_allclose(o.state("q")[0], g["q_mass_node"], rtol=0, atol=g["tolerance"])
+
+
 def test_mass_external_force_velocity():
     """test_masses.cpp:79-144: v after 1000 steps at the test's 1e-12."""
     from tests.workloads_ref import mass_external_force_model

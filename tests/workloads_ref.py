@@ -173,6 +173,30 @@ def generator_torque_model(tilt: float):
     return m, StepParameters(True, 5, 0.01, 0.0), rj, azimuth
 
 
+def heavy_top_model():
+    """tests/regression_tests/regression/test_heavy_top.cpp:9-75: a 15 kg top
+    (inertia diag(0.234375, 0.46875, 0.234375)) at (0, 1, 0) spinning at
+    (0, 150, -4.61538) rad/s, held at the origin by a rigid joint to a
+    position-only ground node with a prescribed (zero) position; gravity
+    -9.81 z; h = 0.002, rho_inf 0.9, tolerances 1e-5 / 1e-3.  Returns (model,
+    params, ground BC id)."""
+    m = Model()
+    m.SetGravity(0., 0., -9.81)
+    mass, inertia = 15., (0.234375, 0.46875, 0.234375)
+    x, omega = (0., 1., 0.), (0., 150., -4.61538)
+    x_dot = (omega[1] * x[2] - omega[2] * x[1], omega[2] * x[0] - omega[0] * x[2],
+             omega[0] * x[1] - omega[1] * x[0])
+    omega_dot = (661.3461692307691919, 0., 0.)
+    x_ddot = (0., -21.3017325444000001, -30.9608307692308244)
+    top = (m.AddNode().SetPosition(x[0], x[1], x[2], 1., 0., 0., 0.)
+           .SetVelocity(*x_dot, *omega).SetAcceleration(*x_ddot, *omega_dot).Build())
+    m.AddMassElement(top, np.diag([mass, mass, mass, *inertia]))
+    ground = m.AddNode().SetPosition(0., 0., 0., 1., 0., 0., 0.).Build()
+    m.AddRigidJoint6DOFsTo3DOFs([top, ground])
+    bc = m.AddPrescribedBC3DOFs(ground)
+    return m, StepParameters(True, 10, 0.002, 0.9, a_tol=1e-5, r_tol=1e-3), bc
+
+
 def rotation_control_inputs(i: int, h: float = 0.01):
     """Pitch angle and hub displacement before step i (0-based) of the two
     rotation-control tests: pitch = t pi/2, azimuth = 0.5 t pi/2 about z."""
