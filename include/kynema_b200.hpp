@@ -309,6 +309,20 @@ public:
         cons_.push_back({KYN_CONSTRAINT_PRESCRIBED_BC, node, u0});
         return cons_.size() - 1;
     }
+    // three-row constraints on position-only nodes (src/model/model.hpp:570-611);
+    // models without beam elements that use them run as their dense system
+    size_t AddFixedBC3DOFs(size_t node) {
+        cons_.push_back({KYN_CONSTRAINT_FIXED_BC_3DOF, node, {0., 0., 0., 1., 0., 0., 0.}});
+        return cons_.size() - 1;
+    }
+    size_t AddPrescribedBC3DOFs(size_t node, const std::array<double, 7>& u0 = {0., 0., 0., 1., 0., 0., 0.}) {
+        cons_.push_back({KYN_CONSTRAINT_PRESCRIBED_BC_3DOF, node, u0});
+        return cons_.size() - 1;
+    }
+    size_t AddRigidJoint6DOFsTo3DOFs(const std::array<size_t, 2>& nodes) {
+        cons_.push_back({KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF, nodes[1], {0., 0., 0., 1., 0., 0., 0.}, nodes[0]});
+        return cons_.size() - 1;
+    }
     // {base (hub), target} (src/model/model.hpp AddRigidJointConstraint)
     size_t AddRigidJointConstraint(const std::array<size_t, 2>& nodes) {
         cons_.push_back({KYN_CONSTRAINT_RIGID_JOINT, nodes[1], {0., 0., 0., 1., 0., 0., 0.}, nodes[0]});

@@ -44,7 +44,8 @@ struct DevModel {
     int def_nt[2] = {0, 0};          // default threads per CTA, FP64 / FP32 form
     int tuned_nt[2] = {0, 0};        // tuned threads per CTA (0: none), cached per form
     unsigned long long tuned_gen[2] = {~0ull, ~0ull};  // tuned-table generation of that cache
-    bool lump = false;               // some beam carries point masses or springs
+    int lump = 0;                    // kernel kind: 0 beams, 1 with masses / springs /
+                                     // drive train (LUMP instance), 2 dense model
     int smem_nt[2][3] = {};          // dynamic smem for 128 / 256 / 512 threads, per form
     double work = 0.;                // largest beam's N^2 Q + 72 (N-1)^3 (ordering in buckets)
     double* d_conv = nullptr;        // [kMaxNewtonIters]
@@ -65,7 +66,7 @@ struct Entry {
     int smem;
     double work;
     DevModel* m;
-    bool lump;
+    int lump;
 };
 
 struct ClassKey {
@@ -82,7 +83,7 @@ struct ClassKey {
 struct Bucket {
     int cluster = 1;
     int nt = 256;      // threads per CTA (step_kernel instance)
-    bool lump = false; // some beam carries point masses or springs
+    int lump = 0;      // kernel kind (DevModel::lump)
     int smem = 0;
     int first = 0;     // first beam in the plan's beam array
     int count = 0;     // beams
@@ -326,14 +327,20 @@ void prepare_model(DevModel* m) {
     m->lay.clear();
     m->kt.clear();
     m->work = 0.;
-    // masses, springs and drive trains run in the LUMP instance
-    m->lump = H.chain.size() > 1;
-    for (const HostBeam& hb : H.beams) m->lump |= hb.n_mass + hb.n_spring > 0;
+    // masses, springs, drive trains and dense models run in the LUMP instance
+    bool lump = H.chain.size() > 1;
+    for (const HostBeam& hb : H.beams) lump |= hb.n_mass + hb.n_spring > 0;
+    m->lump = (!H.beams.empty() && H.beams[0].dense) ? 2 : lump ? 1 : 0;
     for (int f = 0; f < 2; ++f) {
         const int rb = f ? 4 : 8;
         m->def_nt[f] = 128;
         for (int k = 0; k < 3; ++k) m->smem_nt[f][k] = 0;
         for (const HostBeam& hb : H.beams) {
+            if (hb.dense) {  // the dense bordered system: 128 threads, FP64 in both forms
+                for (int k = 0; k < 3; ++k)
+                    m->smem_nt[f][k] = std::max(m->smem_nt[f][k], make_dense_smem(hb.N, H.ndofs).bytes);
+                continue;
+            }
             m->def_nt[f] = std::max(m->def_nt[f], beam_threads(hb.N, hb.Q, hb.nc, rb, hubf));
             for (int k = 0; k < 3; ++k)
                 m->smem_nt[f][k] = std::max(m->smem_nt[f][k], beam_smem(hb.N, hb.Q, hb.nc, rb, 128 << k, hubf));
@@ -373,6 +380,8 @@ void prepare_model(DevModel* m) {
         k.conv = m->d_conv;
         k.hub = static_cast<int>(H.chain.size());
         k.hub_con_type = H.hub_con_type;
+        k.dense = hb.dense ? 1 : 0;
+        for (int s2 = 0; s2 < kMaxBeamConstraints; ++s2) k.con_base[s2] = hb.con_base[s2];
         m->kt.push_back(k);
     }
 }
@@ -464,14 +473,15 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
         const int cluster = static_cast<int>(m->kt.size());
         const int cls = ctas_per_sm(rbytes, nt, smem);
         all.push_back({i, cluster, nt, cls, smem, m->work, m, m->lump});
-        // one 64-bit sort key: masses/springs last, larger clusters first, more
-        // threads first, fewer CTAs per SM first, more work first, then model order
-        const uint64_t work = static_cast<uint64_t>(std::min(m->work, 4194303.));
-        keys.push_back((static_cast<uint64_t>(m->lump) << 63) |
-                       (static_cast<uint64_t>(15 - std::min(cluster, 15)) << 59) |
-                       (static_cast<uint64_t>(2 - nt_index(nt)) << 57) |
-                       (static_cast<uint64_t>(std::min(cls, 15)) << 53) |
-                       ((4194303ull - work) << 31) | static_cast<uint64_t>(i));
+        // one 64-bit sort key: kernel kind (beams, masses/springs, dense models),
+        // larger clusters first, more threads first, fewer CTAs per SM first,
+        // more work first, then model order
+        const uint64_t work = static_cast<uint64_t>(std::min(m->work, 2097151.));
+        keys.push_back((static_cast<uint64_t>(m->lump) << 62) |
+                       (static_cast<uint64_t>(15 - std::min(cluster, 15)) << 58) |
+                       (static_cast<uint64_t>(2 - nt_index(nt)) << 56) |
+                       (static_cast<uint64_t>(std::min(cls, 15)) << 52) |
+                       ((2097151ull - work) << 31) | static_cast<uint64_t>(i));
         nbeams += m->kt.size();
     }
     std::sort(keys.begin(), keys.end());
@@ -559,9 +569,11 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
 
 using StepKernelFn = void (*)(const KBeam*, StepCoeffs, int, int*, int*);
 
-// The step kernel instance for an arithmetic form, a thread count and whether
-// point masses or springs are present.
-StepKernelFn pick_kernel(bool fp32, int nt, bool lump) {
+// The step kernel instance for an arithmetic form, a thread count and the
+// kernel kind (0 beams, 1 with point masses / springs / a drive train, 2 a
+// dense model, which runs in FP64 in both forms).
+StepKernelFn pick_kernel(bool fp32, int nt, int lump) {
+    if (lump == 2) return nt == 128 ? dense_kernel<128> : nt == 256 ? dense_kernel<256> : dense_kernel<512>;
     if (lump) {
         if (fp32) return nt == 128 ? step_kernel<float, 128, true>
                        : nt == 256 ? step_kernel<float, 256, true> : step_kernel<float, 512, true>;
@@ -581,8 +593,8 @@ cudaError_t set_smem_attr(K kernel) {
 
 int configure_smem(kyn_ctx* c) {
     if (c->smem_configured < kMaxDynSmem) {
-        for (int k = 0; k < 12; ++k)
-            KYN_CUDA(c, set_smem_attr(pick_kernel(k & 1, 128 << ((k >> 1) % 3), k >= 6)));
+        for (int k = 0; k < 18; ++k)
+            KYN_CUDA(c, set_smem_attr(pick_kernel(k & 1, 128 << ((k >> 1) % 3), k / 6)));
         c->smem_configured = kMaxDynSmem;
     }
     return KYN_OK;
@@ -915,9 +927,10 @@ int kyn_model_create(kyn_ctx* c, const kyn_model_desc* desc) {
     size_t bytes = kMaxNewtonIters * sizeof(double);
     for (auto& b : m->host.beams) {
         const int hubf = hub_kind(m->host);
-        const int nt = beam_threads(b.N, b.Q, b.nc, sizeof(double), hubf);
-        const int sm = std::max(beam_smem(b.N, b.Q, b.nc, sizeof(double), 512, hubf),
-                                beam_smem(b.N, b.Q, b.nc, sizeof(double), nt, hubf));
+        const int nt = b.dense ? 128 : beam_threads(b.N, b.Q, b.nc, sizeof(double), hubf);
+        const int sm = b.dense ? make_dense_smem(b.N, m->host.ndofs).bytes
+                               : std::max(beam_smem(b.N, b.Q, b.nc, sizeof(double), 512, hubf),
+                                          beam_smem(b.N, b.Q, b.nc, sizeof(double), nt, hubf));
         if (sm > kMaxDynSmem)
             return set_err(c, KYN_ERR_UNSUPPORTED, "beam system does not fit in shared memory");
         m->nt.push_back(nt);
@@ -1683,7 +1696,9 @@ extern "C" int kyn_autotune(kyn_ctx* c, const int* ids, int n, const kyn_step_pa
         float best_ms = 0.f, def_ms = -1.f;
         for (int nt : {128, 256, 512}) {
             bool fits = true;
-            for (const HostBeam& b : h.beams) fits &= beam_smem(b.N, b.Q, b.nc, rb, nt, hub_kind(h)) <= kMaxDynSmem;
+            for (const HostBeam& b : h.beams)
+                fits &= (b.dense ? make_dense_smem(b.N, h.ndofs).bytes
+                                 : beam_smem(b.N, b.Q, b.nc, rb, nt, hub_kind(h))) <= kMaxDynSmem;
             if (!fits || (key.beams > 1 && key.beams * nt > 1024 * 8)) continue;
             c->tuned[key] = nt;
             ++c->tuned_gen;

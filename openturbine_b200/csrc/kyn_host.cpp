@@ -389,7 +389,64 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
     std::vector<std::vector<int>> node_cols(nn);   // constraint row blocks coupled to a node
     static const double ident7[7] = {0., 0., 0., 1., 0., 0., 0.};
     int joints = 0;
-    for (int c = 0; c < d->num_constraints; ++c) {
+    // A lumped model with three-row constraints or joints between its nodes is
+    // solved as the reference's dense bordered system (one CTA, pivoted LU).
+    bool dense = false;
+    for (int c = 0; c < d->num_constraints && lumped; ++c)
+        dense |= is_hub_joint(d->constraint_type[c]) || d->constraint_type[c] >= KYN_CONSTRAINT_FIXED_BC_3DOF;
+    if (!lumped)
+        for (int c = 0; c < d->num_constraints; ++c)
+            if (d->constraint_type[c] >= KYN_CONSTRAINT_FIXED_BC_3DOF)
+                return fail(err, KYN_ERR_UNSUPPORTED,
+                            "three-row constraints are supported in models without beam elements");
+    if (dense) {
+        HostBeam& B = M.beams[0];
+        B.dense = true;
+        if (d->num_constraints > kMaxBeamConstraints)
+            return fail(err, KYN_ERR_UNSUPPORTED, "more than 4 constraints in a dense model");
+        const SlabLayout L = make_slab_layout(B.N, 0);
+        for (int c = 0; c < d->num_constraints; ++c) {
+            const int t = d->constraint_type[c];
+            const int node = d->constraint_target_node[c];
+            if (node < 0 || node >= nn) return fail(err, KYN_ERR_INVALID, "constraint node out of range");
+            const bool joint = is_hub_joint(t) || t == KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF;
+            if (t < KYN_CONSTRAINT_FIXED_BC || t > KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF ||
+                t == KYN_CONSTRAINT_REVOLUTE_JOINT)
+                return fail(err, KYN_ERR_UNSUPPORTED, "constraint type outside the dense-model path");
+            const int base = joint ? base_of(c) : -1;
+            if (joint && (base < 0 || base >= nn || base == node))
+                return fail(err, KYN_ERR_INVALID, "joint base node out of range");
+            const int slot = B.nc++;
+            M.con_beam[c] = 0;
+            M.con_slot[c] = slot;
+            B.con_node[slot] = node;
+            B.con_base[slot] = base;
+            B.con_type[slot] = t;
+            B.con_row[slot] = c;
+            node_cols[node].push_back(c);
+            if (joint) node_cols[base].push_back(c);
+            const double* x0 = d->node_x0 + node * 7;
+            const double* ax = d->constraint_axis ? d->constraint_axis + c * 3 : nullptr;
+            const double* u = (d->constraint_initial_displacement &&
+                               (t == KYN_CONSTRAINT_PRESCRIBED_BC || t == KYN_CONSTRAINT_PRESCRIBED_BC_3DOF))
+                                  ? d->constraint_initial_displacement + c * 7 : ident7;
+            for (int k = 0; k < 7; ++k) B.slab[L.con_input + slot * 7 + k] = u[k];
+            for (int k = 0; k < 3; ++k) {  // X0 (src/constraints/constraints.hpp:224-233, 268-290)
+                if (t == KYN_CONSTRAINT_FIXED_BC || t == KYN_CONSTRAINT_FIXED_BC_3DOF)
+                    B.con_X0[slot][k] = x0[k] - (ax ? ax[k] : 0.);
+                else if (joint)
+                    B.con_X0[slot][k] = x0[k] - d->node_x0[base * 7 + k];
+                else
+                    B.con_X0[slot][k] = 0.;
+            }
+            if (t == KYN_CONSTRAINT_ROTATION_CONTROL) {
+                const double nrm = ax ? std::sqrt(ax[0] * ax[0] + ax[1] * ax[1] + ax[2] * ax[2]) : 0.;
+                if (!(nrm > 0.)) return fail(err, KYN_ERR_INVALID, "rotation control needs a nonzero axis");
+                for (int k = 0; k < 3; ++k) B.con_axis[slot][k] = ax[k] / nrm;
+            }
+        }
+    }
+    for (int c = 0; c < d->num_constraints && !dense; ++c) {
         const int t = d->constraint_type[c];
         if (t != KYN_CONSTRAINT_FIXED_BC && t != KYN_CONSTRAINT_PRESCRIBED_BC && !is_hub_joint(t) &&
             t != KYN_CONSTRAINT_REVOLUTE_JOINT)
@@ -468,7 +525,7 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
         }
     }
 
-    if (lumped)  // every node of a lumped model needs its 6 DOFs from a mass or a BC
+    if (lumped && !dense)  // every node of a lumped model needs its 6 DOFs from a mass or a BC
         for (int n = 0; n < nn; ++n)
             if (!node_mass[n] && node_con[n] < 0)
                 return fail(err, KYN_ERR_UNSUPPORTED,
@@ -556,11 +613,36 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
         }
     }
 
-    // DOF map: every node carries 6 DOFs, exclusive scan in node-id order
+    // DOF map: exclusive scan of the nodes' DOFs in node-id order
     // (compute_node_freedom_map_table.hpp); constraint rows follow in order.
+    // Every node carries 6 DOFs except, in a dense model, the position-only
+    // nodes (FreedomSignature JustPosition: springs' nodes and targets of
+    // three-row constraints, in no mass or six-DOF constraint).
+    M.active.assign(nn, 6);
+    if (dense) {
+        std::vector<int> sig(nn, 0);
+        for (int e = 0; e < n_mass; ++e) sig[d->mass_node[e]] |= 63;
+        for (int e = 0; e < n_spring; ++e) {
+            sig[d->spring_nodes[2 * e]] |= 56;
+            sig[d->spring_nodes[2 * e + 1]] |= 56;
+        }
+        for (int c = 0; c < d->num_constraints; ++c) {
+            const int t = d->constraint_type[c];
+            sig[d->constraint_target_node[c]] |= t >= KYN_CONSTRAINT_FIXED_BC_3DOF ? 56 : 63;
+            if (is_hub_joint(t) || t == KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF) sig[base_of(c)] |= 63;
+        }
+        for (int n = 0; n < nn; ++n) {
+            if (sig[n] != 63 && sig[n] != 56)
+                return fail(err, KYN_ERR_UNSUPPORTED, "dense-model node without six or three DOFs");
+            M.active[n] = sig[n] == 63 ? 6 : 3;
+        }
+    }
     M.fmap.resize(nn);
-    for (int n = 0; n < nn; ++n) M.fmap[n] = 6 * n;
-    M.nsys = 6 * nn;
+    M.nsys = 0;
+    for (int n = 0; n < nn; ++n) {
+        M.fmap[n] = M.nsys;
+        M.nsys += M.active[n];
+    }
     M.con_rows.assign(d->num_constraints, 6);
     M.con_row_first.assign(d->num_constraints, 0);
     int crow = 0;
@@ -570,19 +652,24 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
         crow += M.con_rows[c];
     }
     M.ndofs = M.nsys + crow;
+    if (dense && M.ndofs > kDenseModelMaxDofs)
+        return fail(err, KYN_ERR_UNSUPPORTED, "dense model larger than 120 DOFs");
 
     // CRS graph: each row lists the DOFs it couples to, sorted ascending
     // (compute_row_ptrs.hpp, compute_col_inds.hpp, sort_crs_graph).
     M.row_ptrs.assign(M.ndofs + 1, 0);
     M.col_inds.clear();
     std::vector<int> cols;
+    std::vector<int> row_node(M.nsys);
+    for (int n = 0; n < nn; ++n)
+        for (int c = 0; c < M.active[n]; ++c) row_node[M.fmap[n] + c] = n;
     for (int row = 0; row < M.ndofs; ++row) {
         cols.clear();
         if (row < M.nsys) {
-            const int node = row / 6;
+            const int node = row_node[row];
             // own block first (compute_system_row_entries.hpp starts every row
             // with it), then the other nodes of every element holding the node
-            for (int c = 0; c < 6; ++c) cols.push_back(M.fmap[node] + c);
+            for (int c = 0; c < M.active[node]; ++c) cols.push_back(M.fmap[node] + c);
             if (M.node_beam[node] >= 0 && !M.beams[M.node_beam[node]].lumped) {
                 const HostBeam& B = M.beams[M.node_beam[node]];
                 const int ln = M.node_local[node];
@@ -599,7 +686,7 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
                 const int n1 = M.spring_nodes[e], n2 = M.spring_nodes[e + 1];
                 if (n1 != node && n2 != node) continue;
                 const int other = (n1 == node) ? n2 : n1;
-                for (int c = 0; c < 6; ++c) cols.push_back(M.fmap[other] + c);
+                for (int c = 0; c < M.active[other]; ++c) cols.push_back(M.fmap[other] + c);
             }
             for (int con : node_cols[node])
                 for (int c = 0; c < M.con_rows[con]; ++c) cols.push_back(M.nsys + M.con_row_first[con] + c);
@@ -607,8 +694,9 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
             int con = 0;
             while (con + 1 < d->num_constraints && M.con_row_first[con + 1] <= row - M.nsys) ++con;
             const int node = d->constraint_target_node[con];
-            for (int c = 0; c < 6; ++c) cols.push_back(M.fmap[node] + c);
-            if (is_hub_joint(d->constraint_type[con]) || d->constraint_type[con] == KYN_CONSTRAINT_REVOLUTE_JOINT)
+            const int t = d->constraint_type[con];
+            for (int c = 0; c < (t >= KYN_CONSTRAINT_FIXED_BC_3DOF ? 3 : 6); ++c) cols.push_back(M.fmap[node] + c);
+            if (is_hub_joint(t) || t == KYN_CONSTRAINT_REVOLUTE_JOINT || t == KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF)
                 for (int c = 0; c < 6; ++c) cols.push_back(M.fmap[d->constraint_base_node[con]] + c);
         }
         std::sort(cols.begin(), cols.end());

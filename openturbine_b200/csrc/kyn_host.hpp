@@ -30,6 +30,8 @@ struct HostBeam {
     double con_X0[kMaxBeamConstraints][3] = {};
     double con_axis[kMaxBeamConstraints][3] = {};  // RotationControl: unit axis
     bool lumped = false;              // all nodes of a model without beam elements (Q = 0)
+    bool dense = false;               // lumped, solved as the dense bordered system
+    int con_base[kMaxBeamConstraints] = {-1, -1, -1, -1};  // dense: joint base node (local)
     int n_mass = 0, n_spring = 0;     // point masses / springs at this beam's nodes
     int lumped_off = 0;               // their records' offset in the slab (kMassRec, kSpringRec)
 };
@@ -44,6 +46,7 @@ struct HostModel {
     std::vector<int> con_beam, con_slot;      // constraint -> (beam, slot)
     std::vector<int> spring_nodes;            // [springs][2] global node ids
     std::vector<int> fmap;                    // node -> first DOF
+    std::vector<int> active;                  // node -> DOFs (6, or 3 for position-only nodes)
     int nsys = 0, ndofs = 0;
     std::vector<int> row_ptrs, col_inds;      // reference CRS graph (sorted rows)
     double gravity[3] = {0., 0., 0.};

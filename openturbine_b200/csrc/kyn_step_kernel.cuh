@@ -826,14 +826,16 @@ __device__ inline bool joint_target_test(const double* cr, const double* wb, dou
 // +-f, translational blocks +-a) to resid[n] and to node n's block row of A
 // (scaled by the conditioner).  One thread per node: each writes only its own
 // rows, and takes its elements in element order.
+// Node n's rows and columns start at pos_mul * pos[n] (6 x the node's position
+// in a beam system; the first-DOF map itself in a dense model).
 template <typename TR>
 __device__ void add_lumped_terms(int n, const double* __restrict__ rec, int n_mass, int n_spring,
                                  const double* sq, const double* sv, const double* svd,
                                  const double* sT, const double* grav, double bprime,
                                  double gprime, double cond, const int* pos, TR* A, int ldA,
-                                 double* resid) {
-    TR* Arow = A + (6 * pos[n]) * ldA;
-    const int cn = 6 * pos[n];
+                                 double* resid, int pos_mul = 6) {
+    TR* Arow = A + (pos_mul * pos[n]) * ldA;
+    const int cn = pos_mul * pos[n];
     for (int e = 0; e < n_mass; ++e) {
         const double* mr = rec + e * kMassRec;
         if (static_cast<int>(mr[0]) != n) continue;
@@ -952,7 +954,7 @@ __device__ void add_lumped_terms(int n, const double* __restrict__ rec, int n_ma
         const double sgn = (n == n1) ? 1. : -1.;
         for (int c = 0; c < 3; ++c) resid[n * 6 + c] += sgn * (c1 * r[c]);
         const int other = (n == n1) ? n2 : n1;
-        const int co = 6 * pos[other];
+        const int co = pos_mul * pos[other];
         for (int i = 0; i < 3; ++i)
             for (int j = 0; j < 3; ++j) {
                 double rr = 0.;
@@ -964,6 +966,434 @@ __device__ void add_lumped_terms(int n, const double* __restrict__ rec, int n_ma
                 *o = static_cast<TR>(static_cast<double>(*o) - a * cond);
             }
     }
+}
+
+// ---- dense models: masses, springs and constraints of any row count ---------------
+// A model without beam elements whose constraints are not all single-node
+// six-DOF BCs (three-row constraints on position-only nodes, joints between
+// its nodes) runs the reference's own bordered system in one CTA: nodes carry
+// the DOFs of their freedom signature (six, or three for position-only nodes),
+// constraint rows follow, and the system is solved by LU with partial
+// pivoting (src/step/step.hpp:42-124 with solve_system.hpp; the order of
+// operations of the dense solve follows the row-pivoting Doolittle LU).  FP64
+// in both precision forms: these systems have at most kDenseModelMaxDofs unknowns.
+
+struct DenseSmem {
+    int M, b, x, q, qp, v, vd, a, qd, T, resid, con, act, fmap, piv, bytes;
+};
+__host__ __device__ inline DenseSmem make_dense_smem(int N, int nd) {
+    DenseSmem S{};
+    int o = 0;
+    auto take = [&](int bytes) {
+        const int r = o;
+        o += (bytes + 15) & ~15;
+        return r;
+    };
+    S.M = take(nd * nd * 8);
+    S.b = take(nd * 8);
+    S.x = take(nd * 8);
+    S.q = take(N * 7 * 8);
+    S.qp = take(N * 7 * 8);
+    S.v = take(N * 6 * 8);
+    S.vd = take(N * 6 * 8);
+    S.a = take(N * 6 * 8);
+    S.qd = take(N * 6 * 8);
+    S.T = take(N * 9 * 8);
+    S.resid = take(N * 6 * 8);
+    S.con = take(kMaxBeamConstraints * kConStride * 8);
+    S.act = take(N * 4);
+    S.fmap = take(N * 4);
+    S.piv = take(64 * 8);
+    S.bytes = o;
+    return S;
+}
+
+template <int NT>
+__device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoeffs& P, int record, int* status_out,
+                                 int* iters_out, unsigned char* smem_raw) {
+    constexpr int NW = NT / 32;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int N = KB.N, nc = KB.nc;
+    const SlabLayout L = make_slab_layout(N, 0);
+    double* __restrict__ slab = KB.slab;
+    const int nd = KB.model_dofs;
+    const DenseSmem S = make_dense_smem(N, nd);
+    double* Md = reinterpret_cast<double*>(smem_raw + S.M);
+    double* b = reinterpret_cast<double*>(smem_raw + S.b);
+    double* x = reinterpret_cast<double*>(smem_raw + S.x);
+    double* sq = reinterpret_cast<double*>(smem_raw + S.q);
+    double* sqp = reinterpret_cast<double*>(smem_raw + S.qp);
+    double* sv = reinterpret_cast<double*>(smem_raw + S.v);
+    double* svd = reinterpret_cast<double*>(smem_raw + S.vd);
+    double* sa = reinterpret_cast<double*>(smem_raw + S.a);
+    double* sqd = reinterpret_cast<double*>(smem_raw + S.qd);
+    double* sT = reinterpret_cast<double*>(smem_raw + S.T);
+    double* resid = reinterpret_cast<double*>(smem_raw + S.resid);
+    double* con = reinterpret_cast<double*>(smem_raw + S.con);
+    int* act = reinterpret_cast<int*>(smem_raw + S.act);
+    int* fmap = reinterpret_cast<int*>(smem_raw + S.fmap);
+    double* red = reinterpret_cast<double*>(smem_raw + S.piv);
+    __shared__ int s_flag, s_nsys, s_piv;
+    const double h = P.h;
+
+    // state, constraint inputs, multipliers reset (ResetConstraints)
+    for (int k = tid; k < N * 7; k += NT) sq[k] = slab[L.q + k];
+    for (int k = tid; k < N * 6; k += NT) {
+        sv[k] = slab[L.v + k];
+        svd[k] = slab[L.vd + k];
+        sa[k] = slab[L.a + k];
+    }
+    if (tid < nc) {
+        double* c = con + tid * kConStride;
+        for (int k = 0; k < 7; ++k) c[conrec::inp + k] = slab[L.con_input + tid * 7 + k];
+        for (int k = 0; k < 6; ++k) c[conrec::lam + k] = 0.;
+    }
+    if (tid == 0) {
+        // FreedomSignature per node (assemble_node_freedom_allocation_table.hpp):
+        // masses six, springs position only, constraint targets six or three,
+        // joint bases six; DOF map = exclusive scan (compute_node_freedom_map_table.hpp)
+        for (int n = 0; n < N; ++n) act[n] = 0;
+        const double* mrec = KB.lumped;
+        for (int e = 0; e < KB.n_mass; ++e) act[static_cast<int>(mrec[e * kMassRec])] |= 63;
+        const double* srec = KB.lumped + KB.n_mass * kMassRec;
+        for (int e = 0; e < KB.n_spring; ++e) {
+            act[static_cast<int>(srec[e * kSpringRec])] |= 56;
+            act[static_cast<int>(srec[e * kSpringRec + 1])] |= 56;
+        }
+        for (int c = 0; c < nc; ++c) {
+            const int t = KB.con_type[c];
+            act[KB.con_node[c]] |= (t >= KYN_CONSTRAINT_FIXED_BC_3DOF) ? 56 : 63;
+            if (KB.con_base[c] >= 0) act[KB.con_base[c]] |= 63;
+        }
+        int o = 0;
+        for (int n = 0; n < N; ++n) {
+            act[n] = (act[n] == 63) ? 6 : (act[n] == 56) ? 3 : 0;
+            fmap[n] = o;
+            o += act[n];
+        }
+        s_nsys = o;
+        s_flag = (o > nd) ? 2 : 0;
+    }
+    __syncthreads();
+    const int nsys = s_nsys;
+    // PredictNextState (src/step/predict_next_state.hpp:14-47)
+    for (int k = tid; k < N * 7; k += NT) sqp[k] = sq[k];
+    for (int k = tid; k < N * 6; k += NT) {
+        const double v_p = sv[k], vd_p = svd[k], a_p = sa[k];
+        svd[k] = 0.;
+        const double an = (P.alpha_f * vd_p - P.alpha_m * a_p) / (1. - P.alpha_m);
+        sa[k] = an;
+        sv[k] = v_p + h * (1. - P.gamma) * a_p + P.gamma * h * an;
+        sqd[k] = v_p + (0.5 - P.beta) * h * a_p + P.beta * h * an;
+    }
+    __syncthreads();
+    auto displacement = [&]() {
+        for (int n = tid; n < N; n += NT) {
+            for (int c = 0; c < 3; ++c) sq[n * 7 + c] = sqp[n * 7 + c] + h * sqd[n * 6 + c];
+            const double d[3] = {h * sqd[n * 6 + 3], h * sqd[n * 6 + 4], h * sqd[n * 6 + 5]};
+            double qd4[4], qn[4];
+            rotvec_to_quat(d, qd4);
+            quat_compose(qd4, sqp + n * 7 + 3, qn);
+            for (int c = 0; c < 4; ++c) sq[n * 7 + 3 + c] = qn[c];
+        }
+    };
+    displacement();
+    __syncthreads();
+
+    int status = KYN_NOT_CONVERGED, iters = 0;
+    const double cond = P.conditioner;
+    for (int iter = 0; iter < P.max_iter && s_flag == 0; ++iter) {
+        // tangent operator, rotational block (src/system/calculate_tangent_operator.hpp)
+        for (int n = tid; n < N; n += NT) {
+            const double rv[3] = {h * sqd[n * 6 + 3], h * sqd[n * 6 + 4], h * sqd[n * 6 + 5]};
+            const double ph = sqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
+            double sn, cs;
+            sincos(ph, &sn, &cs);
+            const double t1 = (ph > 1.e-16) ? (cs - 1.) / (ph * ph) : 0.;
+            const double t2 = (ph > 1.e-16) ? (1. - sn / ph) / (ph * ph) : 0.;
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    double rr = 0.;
+                    for (int k = 0; k < 3; ++k) rr += tilde_e(rv, j, k) * tilde_e(rv, k, i);
+                    sT[n * 9 + i * 3 + j] = (i == j ? 1. : 0.) + (t1 * tilde_e(rv, j, i) + t2 * rr);
+                }
+        }
+        for (int k = tid; k < nd * nd; k += NT) Md[k] = 0.;
+        for (int k = tid; k < nd; k += NT) b[k] = 0.;
+        for (int k = tid; k < N * 6; k += NT) resid[k] = 0.;
+        __syncthreads();
+        // masses and springs (residual into resid, conditioned blocks into Md)
+        for (int n = tid; n < N; n += NT)
+            add_lumped_terms(n, KB.lumped, KB.n_mass, KB.n_spring, sq, sv, svd, sT, KB.gravity,
+                             P.beta_prime, P.gamma_prime, cond, fmap, Md, nd, resid, 1);
+        // constraints: residual, gradients and G^T lambda
+        if (tid < nc) {
+            double* cr = con + tid * kConStride;
+            const int t = KB.con_type[tid], tn = KB.con_node[tid], bn = KB.con_base[tid];
+            if (t >= KYN_CONSTRAINT_FIXED_BC_3DOF) {
+                // three rows (calculate_*_3DOF_constraint.hpp): u2 + X0 - u1 - R1 X0
+                double u1[3] = {0., 0., 0.}, R1[4] = {1., 0., 0., 0.};
+                if (t == KYN_CONSTRAINT_PRESCRIBED_BC_3DOF) {
+                    for (int k = 0; k < 3; ++k) u1[k] = cr[conrec::inp + k];
+                    for (int k = 0; k < 4; ++k) R1[k] = cr[conrec::inp + 3 + k];
+                } else if (t == KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF) {
+                    for (int k = 0; k < 3; ++k) u1[k] = sq[bn * 7 + k];
+                    for (int k = 0; k < 4; ++k) R1[k] = sq[bn * 7 + 3 + k];
+                }
+                const double* X0 = KB.con_X0[tid];
+                double r1x0[3];
+                for (int i = 0; i < 3; ++i) {
+                    r1x0[i] = 0.;
+                    for (int j = 0; j < 3; ++j) r1x0[i] += rot_entry(R1, i, j) * X0[j];
+                }
+                for (int i = 0; i < 3; ++i) {
+                    cr[conrec::Phi + i] = sq[tn * 7 + i] + X0[i] - u1[i] - r1x0[i];
+                    cr[conrec::Gl + i] = cr[conrec::lam + i];
+                    cr[conrec::R1X0 + i] = r1x0[i];
+                }
+                if (t == KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF)  // base block tilde(R1 X0) T_base
+                    for (int i = 0; i < 3; ++i)
+                        for (int j = 0; j < 3; ++j) {
+                            double bt = 0.;
+                            for (int k = 0; k < 3; ++k) bt += tilde_e(r1x0, i, k) * sT[bn * 9 + k * 3 + j];
+                            cr[conrec::Btr + i * 3 + j] = bt;
+                        }
+            } else {
+                constraint_record(cr, t, sq + tn * 7, KB.con_X0[tid], sT + tn * 9,
+                                  bn >= 0 ? sq + bn * 7 : nullptr, bn >= 0 ? sT + bn * 9 : nullptr,
+                                  KB.con_axis[tid]);
+            }
+        }
+        __syncthreads();
+        // scatter: rows of B = G T, columns G^T, residuals (assemble_constraints_matrix.hpp,
+        // assemble_constraints_residual.hpp, assemble_system_residual.hpp)
+        if (tid == 0) {
+            int rf = nsys;
+            for (int c = 0; c < nc; ++c) {
+                const double* cr = con + c * kConStride;
+                const int t = KB.con_type[c], tn = KB.con_node[c], bn = KB.con_base[c];
+                const int rows = t >= KYN_CONSTRAINT_FIXED_BC_3DOF ? 3 : 6;
+                const int ft = fmap[tn];
+                for (int r = 0; r < rows; ++r) {
+                    double* row = Md + (rf + r) * nd;
+                    if (r < 3) {
+                        row[ft + r] += 1.;
+                        Md[(ft + r) * nd + rf + r] += 1.;
+                    } else {
+                        for (int j = 0; j < 3; ++j) {
+                            row[ft + 3 + j] += cr[conrec::Brot + (r - 3) * 3 + j];
+                            Md[(ft + 3 + j) * nd + rf + r] += cr[conrec::AX + j * 3 + (r - 3)];
+                        }
+                    }
+                    b[rf + r] += cr[conrec::Phi + r];
+                }
+                for (int e = 0; e < (rows == 3 ? 3 : 6); ++e) b[ft + e] += cr[conrec::Gl + e];
+                if (bn >= 0) {  // joint base blocks: B_b = [-I, Btr; 0, Brr], G_b = [-I, tilde; 0, -AX]
+                    const int fb = fmap[bn];
+                    const double* r1x0 = cr + conrec::R1X0;
+                    for (int r = 0; r < rows; ++r) {
+                        double* row = Md + (rf + r) * nd;
+                        if (r < 3) {
+                            row[fb + r] -= 1.;
+                            Md[(fb + r) * nd + rf + r] -= 1.;
+                            for (int j = 0; j < 3; ++j) {
+                                row[fb + 3 + j] += cr[conrec::Btr + r * 3 + j];
+                                Md[(fb + 3 + j) * nd + rf + r] += tilde_e(r1x0, r, j);
+                            }
+                        } else {
+                            for (int j = 0; j < 3; ++j) {
+                                row[fb + 3 + j] += cr[conrec::Brr + (r - 3) * 3 + j];
+                                Md[(fb + 3 + j) * nd + rf + r] -= cr[conrec::AX + (r - 3) * 3 + j];
+                            }
+                        }
+                    }
+                    double gb[6] = {0., 0., 0., 0., 0., 0.};
+                    double lam6[6] = {0., 0., 0., 0., 0., 0.};
+                    for (int k = 0; k < rows; ++k) lam6[k] = cr[conrec::lam + k];
+                    if (rows == 3) {
+                        for (int i = 0; i < 3; ++i) {
+                            gb[i] = -lam6[i];
+                            for (int k = 0; k < 3; ++k) gb[3 + i] += tilde_e(r1x0, k, i) * lam6[k];
+                        }
+                    } else {
+                        joint_base_transpose_add(cr, lam6, gb);
+                    }
+                    for (int e = 0; e < 6; ++e) b[fb + e] += gb[e];
+                }
+                rf += rows;
+            }
+        }
+        __syncthreads();
+        // b = -(cond (R - f) on the system rows, Phi on the constraint rows)
+        for (int n = tid; n < N; n += NT)  // position-only nodes: components 0..2
+            for (int c = 0; c < act[n]; ++c) b[fmap[n] + c] += resid[n * 6 + c] - slab[L.f + n * 6 + c];
+        __syncthreads();
+        for (int k = tid; k < nd; k += NT) b[k] = -(k < nsys ? b[k] * cond : b[k]);
+        __syncthreads();
+        // LU with partial pivoting, in place (the oracle's dense solve)
+        for (int k = 0; k < nd; ++k) {
+            if (warp == 0) {
+                double best = -1.;
+                int p = k;
+                for (int i = k + lane; i < nd; i += 32) {
+                    const double v = fabs(Md[i * nd + k]);
+                    if (v > best) {
+                        best = v;
+                        p = i;
+                    }
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                    const int op = __shfl_xor_sync(0xffffffffu, p, o);
+                    if (ob > best || (ob == best && op < p)) {
+                        best = ob;
+                        p = op;
+                    }
+                }
+                if (lane == 0) {
+                    s_piv = p;
+                    if (!(best > 0.)) s_flag |= 2;
+                }
+            }
+            __syncthreads();
+            const int p = s_piv;
+            if (p != k) {
+                for (int j = tid; j < nd; j += NT) {
+                    const double t0 = Md[k * nd + j];
+                    Md[k * nd + j] = Md[p * nd + j];
+                    Md[p * nd + j] = t0;
+                }
+                if (tid == 0) {
+                    const double t0 = b[k];
+                    b[k] = b[p];
+                    b[p] = t0;
+                }
+            }
+            __syncthreads();
+            const double d = Md[k * nd + k];
+            for (int i = k + 1 + tid; i < nd; i += NT) Md[i * nd + k] /= d;
+            __syncthreads();
+            const int w = nd - k - 1;
+            for (int e = tid; e < w * (w + 1); e += NT) {
+                const int i = k + 1 + e / (w + 1), j = e % (w + 1);
+                const double l = Md[i * nd + k];
+                if (j < w)
+                    Md[i * nd + k + 1 + j] -= l * Md[k * nd + k + 1 + j];
+                else
+                    b[i] -= l * b[k];
+            }
+            __syncthreads();
+        }
+        if (warp == 0) {  // back substitution
+            for (int i = nd - 1; i >= 0; --i) {
+                double s2 = 0.;
+                for (int j = i + 1 + lane; j < nd; j += 32) s2 += Md[i * nd + j] * x[j];
+                for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+                if (lane == 0) x[i] = (b[i] - s2) / Md[i * nd + i];
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        // multipliers unconditioned; convergence error (calculate_convergence_error.hpp)
+        for (int k = nsys + tid; k < nd; k += NT) x[k] /= cond;
+        __syncthreads();
+        double part = 0.;
+        for (int n = tid; n < N; n += NT)
+            for (int c = 0; c < act[n]; ++c) {
+                const double e = x[fmap[n] + c] / (P.atol + P.rtol * fabs(sqd[n * 6 + c] * h));
+                part += e * e;
+            }
+        if (tid < nc) {
+            const double* cr = con + tid * kConStride;
+            int rf = nsys;
+            for (int c = 0; c < tid; ++c) rf += KB.con_type[c] >= KYN_CONSTRAINT_FIXED_BC_3DOF ? 3 : 6;
+            const int rows = KB.con_type[tid] >= KYN_CONSTRAINT_FIXED_BC_3DOF ? 3 : 6;
+            for (int r = 0; r < rows; ++r) {
+                const double e = x[rf + r] / (P.atol + P.rtol * fabs(cr[conrec::lam + r]));
+                part += e * e;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+        if (lane == 0) red[warp] = part;
+        __syncthreads();
+        double total = 0.;
+        for (int w2 = 0; w2 < NW; ++w2) total += red[w2];
+        const double err = sqrt(total / static_cast<double>(nd));
+        if (tid == 0 && iter < kMaxNewtonIters) KB.conv[iter] = err;
+        iters = iter + 1;
+        // update (update_state_prediction.hpp, update_lambda_prediction.hpp)
+        for (int n = tid; n < N; n += NT)
+            for (int c = 0; c < act[n]; ++c) {
+                const double delta = x[fmap[n] + c];
+                sqd[n * 6 + c] += delta / h;
+                if (P.dynamic) {
+                    sv[n * 6 + c] += P.gamma_prime * delta;
+                    svd[n * 6 + c] += P.beta_prime * delta;
+                }
+            }
+        if (tid < nc) {
+            double* cr = con + tid * kConStride;
+            int rf = nsys;
+            for (int c = 0; c < tid; ++c) rf += KB.con_type[c] >= KYN_CONSTRAINT_FIXED_BC_3DOF ? 3 : 6;
+            const int rows = KB.con_type[tid] >= KYN_CONSTRAINT_FIXED_BC_3DOF ? 3 : 6;
+            for (int r = 0; r < rows; ++r) cr[conrec::lam + r] += x[rf + r];
+        }
+        __syncthreads();
+        displacement();
+        __syncthreads();
+        if (s_flag != 0) {
+            status = KYN_ERR_SINGULAR;
+            break;
+        }
+        if (!(err == err) || isinf(err)) {
+            status = KYN_ERR_NONFINITE;
+            break;
+        }
+        if (err <= 1.) {
+            status = KYN_OK;
+            break;
+        }
+    }
+    if (s_flag != 0 && status == KYN_NOT_CONVERGED) status = KYN_ERR_INVALID;
+    // post-step (step.hpp:86-121) and the resident state
+    if (status == KYN_OK) {
+        const double fac = (1. - P.alpha_f) / (1. - P.alpha_m);
+        for (int k = tid; k < N * 6; k += NT) sa[k] += fac * svd[k];
+    }
+    __syncthreads();
+    for (int k = tid; k < N * 7; k += NT) {
+        slab[L.q + k] = sq[k];
+        slab[L.q_prev + k] = sqp[k];
+    }
+    for (int k = tid; k < N * 6; k += NT) {
+        slab[L.v + k] = sv[k];
+        slab[L.vd + k] = svd[k];
+        slab[L.a + k] = sa[k];
+        slab[L.q_delta + k] = sqd[k];
+    }
+    if (status == KYN_OK)
+        for (int n = tid; n < N; n += NT) {
+            const double* x0 = slab + L.x0 + n * 7;
+            for (int c = 0; c < 3; ++c) slab[L.x + n * 7 + c] = x0[c] + sq[n * 7 + c];
+            double r[4];
+            quat_compose(sq + n * 7 + 3, x0 + 3, r);
+            for (int c = 0; c < 4; ++c) slab[L.x + n * 7 + 3 + c] = r[c];
+        }
+    for (int k = tid; k < N * 9; k += NT) slab[L.tangent + k] = sT[k];
+    if (tid < 6 * nc) slab[L.lambda + tid] = con[(tid / 6) * kConStride + conrec::lam + tid % 6];
+    if (tid == 0) {
+        status_out[KB.plan_model] = status;
+        iters_out[KB.plan_model] = iters;
+    }
+    (void)record;
+}
+
+// One CTA per dense model.
+template <int NT>
+__global__ void __launch_bounds__(NT) dense_kernel(const KBeam* __restrict__ beams, StepCoeffs P, int record,
+                                                   int* __restrict__ status_out, int* __restrict__ iters_out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    dense_model_step<NT>(beams[blockIdx.x], P, record, status_out, iters_out, smem_raw);
 }
 
 // ---- the kernel ------------------------------------------------------------------

@@ -20,6 +20,7 @@ namespace kyn {
 constexpr int kMaxBeamConstraints = 4;   // FixedBC / PrescribedBC / joints per beam
 constexpr int kMaxClusterBeams = 8;      // beams per model (portable cluster size)
 constexpr int kMaxNewtonIters = 64;      // convergence-history capacity
+constexpr int kDenseModelMaxDofs = 120;  // unknowns of a model solved as a dense bordered system
 constexpr int kThreads = 256;            // threads per CTA of the step kernel
 
 // Offsets (in doubles) of the arrays inside one beam slab.
@@ -116,7 +117,7 @@ constexpr int kSpringRec = 7;
 // hub): KYN_CONSTRAINT_RIGID_JOINT (3) and KYN_CONSTRAINT_ROTATION_CONTROL (5).
 KYN_HD inline bool is_hub_joint(int type) { return type == 3 || type == 5; }
 // Rows of a constraint (src/constraints/constraint_type.hpp NumRowsForConstraint).
-KYN_HD inline int constraint_rows(int type) { return type == 4 ? 5 : 6; }
+KYN_HD inline int constraint_rows(int type) { return type == 4 ? 5 : type >= 6 ? 3 : 6; }
 
 struct KBeam {
     double* slab;             // device slab of this beam
@@ -133,6 +134,8 @@ struct KBeam {
     const double* lumped;     // point masses then springs at this beam's nodes, or null
     int32_t n_mass, n_spring; // (records of kMassRec / kSpringRec doubles, node-local indices)
     int32_t hub;              // hub chain length: 0 none, 1 hub, 2-3 drive train
+    int32_t dense;            // 1: a model without beams solved as its dense bordered system
+    int32_t con_base[kMaxBeamConstraints];   // dense models: joint base node (local), or -1
     int32_t hub_con_type;     // KYN_CONSTRAINT_FIXED_BC / PRESCRIBED_BC on the hub
     double gravity[3];
     double* conv;             // [kMaxNewtonIters] model convergence history (rank 0)

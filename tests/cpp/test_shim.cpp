@@ -1,7 +1,7 @@
 // The reference's regression drivers written against the C++ shim (kynema_b200.hpp):
 // test_cantilever_beam.cpp:31-138, test_rotating_beam.cpp:93-150, :390-456
 // (rotation control) and :581-680 (generator torque on a revolute joint),
-// test_spring_mass_system.cpp:23-96, same inputs, same golden
+// test_spring_mass_system.cpp:23-96, test_heavy_top.cpp:9-75, same inputs, same golden
 // tolerances.  Exit code 0 on success.
 #include <cmath>
 #include <cstdio>
@@ -146,6 +146,35 @@ static void generator_torque(const Context& ctx, double tilt, const double (&az_
     for (int c = 0; c < 3; ++c) expect_near(o[rj * 3 + c], out[c], 1e-6, "generator torque joint output");
 }
 
+// test_heavy_top.cpp:9-75: a top held at a point (RigidJoint6DOFsTo3DOFs to a
+// position-only ground node with PrescribedBC3DOFs), q after 400 steps at 1e-10
+static void heavy_top(const Context& ctx) {
+    Model model;
+    model.SetGravity(0., 0., -9.81);
+    const double omega[3] = {0., 150., -4.61538};
+    const double x[3] = {0., 1., 0.};
+    const double xd[3] = {omega[1] * x[2] - omega[2] * x[1], omega[2] * x[0] - omega[0] * x[2],
+                          omega[0] * x[1] - omega[1] * x[0]};
+    const size_t top = model.AddNode()
+                           .SetPosition(x[0], x[1], x[2], 1., 0., 0., 0.)
+                           .SetVelocity(xd[0], xd[1], xd[2], omega[0], omega[1], omega[2])
+                           .SetAcceleration(0., -21.3017325444000001, -30.9608307692308244, 661.3461692307691919, 0., 0.)
+                           .Build();
+    model.AddMassElement(top, {{{15., 0., 0., 0., 0., 0.}, {0., 15., 0., 0., 0., 0.}, {0., 0., 15., 0., 0., 0.},
+                                {0., 0., 0., 0.234375, 0., 0.}, {0., 0., 0., 0., 0.46875, 0.}, {0., 0., 0., 0., 0., 0.234375}}});
+    const size_t ground = model.AddNode().SetPosition(0., 0., 0., 1., 0., 0., 0.).Build();
+    model.AddRigidJoint6DOFsTo3DOFs({top, ground});
+    model.AddPrescribedBC3DOFs(ground);
+    auto parameters = StepParameters(true, 10, 0.002, 0.9, 1e-5, 1e-3);
+    auto [state, elements, constraints, solver] = model.CreateSystemWithSolver(ctx);
+    for (int i = 0; i < 400; ++i)
+        if (!Step(parameters, solver, elements, state, constraints)) { std::printf("FAIL heavy top step %d\n", i); ++failures; }
+    const double expect[7] = {-0.42217802273894345, -0.09458263530050703, -0.04455460488952848, -0.17919607435565366,
+                              0.21677896640311572, -0.9594776960853596, -0.017268392381761217};
+    const auto q = state.q();
+    for (int c = 0; c < 7; ++c) expect_near(q[c], expect[c], 1e-10, "heavy top q");
+}
+
 // test_spring_mass_system.cpp:23-96: a mass on a spring to a fixed node, no beam element
 static void spring_mass(const Context& ctx) {
     Model model;
@@ -176,6 +205,7 @@ int main() {
         generator_torque(ctx, 3.14159265358979323846 / 2., {0., 0., 0., 0.99998634, 0., -0.0052267, 0.},
                          {0., 0., 0., 0., -0.18978539, 0.}, {-0.01045353, -0.18978539, -0.566560});
         spring_mass(ctx);
+        heavy_top(ctx);
     } catch (const std::exception& e) {
         std::printf("FAIL exception: %s\n", e.what());
         return 2;

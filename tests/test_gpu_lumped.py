@@ -6,7 +6,8 @@ import numpy as np
 import pytest
 
 from oracle.oracle_py import OracleModel
-from tests.test_gpu_parity import FIELDS, Twin, assert_convergence_close, assert_state_close
+from tests.test_gpu_parity import (ACCEL_REL, FIELDS, Twin, assert_convergence_close,
+                                   assert_state_close)
 from tests.workloads_ref import (cantilever_test_loads, cantilever_test_model,
                                  load_golden, mass_external_force_model, precession_model,
                                  spring_mass_chain_model, spring_mass_model)
@@ -155,3 +156,69 @@ def test_lumped_models_batched_with_beams(ctx):
         np.testing.assert_array_equal(ctx.state(mid, "q"), qa)
     for mid in [alone] + mixed + beams:
         ctx.destroy_model(mid)
+
+
+def test_heavy_top_dense_model(ctx):
+    """test_heavy_top.cpp:9-75: a top held at a point by a rigid joint to a
+    position-only ground node with a prescribed position (RigidJoint6DOFsTo3DOFs,
+    PrescribedBC3DOFs; 15 DOFs).  The model runs as its dense bordered system
+    (one CTA, pivoted LU): same CRS, Newton decisions and states as the oracle
+    over 400 steps, and the golden q at the test's 1e-10."""
+    from tests.workloads_ref import heavy_top_model
+    g = load_golden("heavy_top.json")
+    m, p, _ = heavy_top_model()
+    pm = m.pack()
+    mid = ctx.create_model(pm)
+    assert ctx.info(mid).num_dofs == 15
+    rp, ci, _ = ctx.crs(mid, values=False)
+    tw = LumpedTwin(pm)
+    orp, oci, _ = tw.crs()
+    assert np.array_equal(rp, orp) and np.array_equal(ci, oci)
+    for _ in range(g["steps"]):
+        st, it = ctx.step([mid], p)
+        ost, oit = tw.step(p)
+        assert (st[0], it[0]) == (ost, oit) == (0, oit)
+        # The top spins at 150 rad/s: a step's first correction is ~1e8 times its
+        # last, so rounding in the first (1e-16 of it) reaches the later error
+        # norms; they are compared to 1e-12 of the step's largest norm.
+        gc, oc = ctx.convergence(mid), tw.convergence()
+        assert len(gc) == len(oc)
+        for a, b in zip(gc, oc):
+            assert (a <= 1.0) == (b <= 1.0)
+            assert abs(a - b) <= max(1e-6 * b, 1e-12 * max(oc)), (a, b)
+    assert_state_close(ctx, mid, tw, fields=FIELDS, lam=False)
+    # The multipliers are unconditioned by 1/(beta h^2) ~ 8e5 at h = 0.002, the
+    # amplification the accelerations see: they are held to the same 1e-7 bound
+    # as vd and a (the run measures ~2e-10).
+    lg, lo = ctx.state(mid, "lambda"), tw.state("lambda")
+    assert np.abs(lg - lo).max() <= ACCEL_REL * np.abs(lo).max()
+    np.testing.assert_allclose(ctx.state(mid, "q")[0], g["q_mass_node"], rtol=0, atol=g["tolerance"])
+    ctx.destroy_model(mid)
+
+
+def test_dense_models_batched_with_beams_and_fp32_form(ctx):
+    """Dense models (heavy tops) stepped in the same kyn_step call as beams
+    and spring-mass models advance exactly as they do alone, in both
+    precision forms (dense models compute in FP64 in either)."""
+    from openturbine_b200 import workloads as W
+    from tests.workloads_ref import heavy_top_model
+    m, p, _ = heavy_top_model()
+    sm, _ = spring_mass_model()
+    pm = m.pack()
+    for precision in (0, 1):
+        pp = type(p)(p.is_dynamic_solve, p.max_iter, p.h, p.rho_inf, p.absolute_convergence_tol,
+                     p.relative_convergence_tol, precision=precision)
+        alone = ctx.create_model(pm)
+        mixed = [ctx.create_model(pm) for _ in range(2)]
+        others = [ctx.create_model(sm.pack())] + [
+            ctx.create_model(W.batch_cantilever_model(d).pack()) for d in W.draw_batch(4, first_id=950)]
+        ids = np.array(mixed[:1] + others[:3] + mixed[1:] + others[3:], dtype=np.int32)
+        for _ in range(20):
+            st, _ = ctx.step([alone], pp)
+            ctx.step(ids, pp)
+            assert st[0] == 0
+        for mid in mixed:
+            for f in ("q", "v", "lambda"):
+                np.testing.assert_array_equal(ctx.state(mid, f), ctx.state(alone, f))
+        for mid in [alone] + mixed + others:
+            ctx.destroy_model(mid)
