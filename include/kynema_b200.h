@@ -57,9 +57,10 @@ enum {
 /* Constraint types: same numbering as constraints::ConstraintType
  * (src/constraints/constraint_type.hpp:9-24).  This path implements the two
  * single-node boundary conditions used by beams and rotors, the two six-row
- * joints that tie blade roots to a hub node, and the five-row revolute joint
- * that lets a drive train (hub, or azimuth node rigidly holding the hub) turn
- * about a shaft held by a boundary condition. */
+ * joints that tie blade roots to a hub node, the five-row revolute joint that
+ * lets a drive train (hub, or azimuth node rigidly holding the hub) turn about
+ * a shaft held by a boundary condition, and the three-row constraints on
+ * position-only nodes of models without beam elements. */
 enum {
     KYN_CONSTRAINT_FIXED_BC = 1,
     KYN_CONSTRAINT_PRESCRIBED_BC = 2,
