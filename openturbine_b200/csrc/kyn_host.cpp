@@ -403,7 +403,7 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
         HostBeam& B = M.beams[0];
         B.dense = true;
         if (d->num_constraints > kMaxBeamConstraints)
-            return fail(err, KYN_ERR_UNSUPPORTED, "more than 4 constraints in a dense model");
+            return fail(err, KYN_ERR_UNSUPPORTED, "more than 8 constraints in a dense model");
         const SlabLayout L = make_slab_layout(B.N, 0);
         for (int c = 0; c < d->num_constraints; ++c) {
             const int t = d->constraint_type[c];
@@ -488,7 +488,7 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
         const int e = M.node_beam[node];
         HostBeam& B = M.beams[e];
         if (B.nc >= kMaxBeamConstraints)
-            return fail(err, KYN_ERR_UNSUPPORTED, "more than 4 constraints on one beam");
+            return fail(err, KYN_ERR_UNSUPPORTED, "more than 8 constraints on one beam");
         const int slot = B.nc++;
         M.con_beam[c] = e;
         M.con_slot[c] = slot;

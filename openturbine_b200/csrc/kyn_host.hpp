@@ -31,7 +31,7 @@ struct HostBeam {
     double con_axis[kMaxBeamConstraints][3] = {};  // RotationControl: unit axis
     bool lumped = false;              // all nodes of a model without beam elements (Q = 0)
     bool dense = false;               // lumped, solved as the dense bordered system
-    int con_base[kMaxBeamConstraints] = {-1, -1, -1, -1};  // dense: joint base node (local)
+    int con_base[kMaxBeamConstraints] = {-1, -1, -1, -1, -1, -1, -1, -1};  // dense: joint base (local)
     int n_mass = 0, n_spring = 0;     // point masses / springs at this beam's nodes
     int lumped_off = 0;               // their records' offset in the slab (kMassRec, kSpringRec)
 };

@@ -17,7 +17,7 @@
 
 namespace kyn {
 
-constexpr int kMaxBeamConstraints = 4;   // FixedBC / PrescribedBC / joints per beam
+constexpr int kMaxBeamConstraints = 8;   // FixedBC / PrescribedBC / joints per beam system
 constexpr int kMaxClusterBeams = 8;      // beams per model (portable cluster size)
 constexpr int kMaxNewtonIters = 64;      // convergence-history capacity
 constexpr int kDenseModelMaxDofs = 120;  // unknowns of a model solved as a dense bordered system

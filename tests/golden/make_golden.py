@@ -18,6 +18,8 @@ Sources (paths relative to the reference project root):
   tests/unit_tests/system/beams/test_curved_beam.hpp         kernel-level data
   tests/regression_tests/interfaces/test_blade_interface.cpp + its WindIO file
                                                              IEA-15 blade input, tip
+  tests/regression_tests/interfaces/test_cfd_interface.cpp    floating platform q
+                                                             (mass, mooring springs)
   tests/regression_tests/regression/test_heavy_top.cpp         heavy top q (three-row
                                                              constraints)
   tests/regression_tests/regression/test_masses.cpp,
@@ -218,6 +220,23 @@ def main(ref: str) -> None:
                "steps": 400, "q_mass_node": [v for _, v, _ in sorted(qv)],
                "tolerance": max(t for _, _, t in qv)},
               open(os.path.join(out_dir, "heavy_top.json"), "w"), indent=1)
+
+    # ---- CFD interface: floating platform (mass + mooring springs, three-row constraints)
+    cf = strip_comments(open(os.path.join(ref, "tests", "regression_tests", "interfaces",
+                                          "test_cfd_interface.cpp")).read())
+    c0 = cf.index("TEST(CFDInterfaceTest, PrecessionTest)")
+    c1 = cf.index("TEST(CFDInterfaceTest, FloatingPlatform)")
+    c2 = cf.index("TEST(CFDInterfaceTest, Restart)")
+    pat = r"EXPECT_NEAR\(\s*platform_node\.displacement\[(\d)\],\s*(" + NUM + r"),\s*(" + NUM + r")\)"
+    pre = [(int(m.group(1)), float(m.group(2)), float(m.group(3))) for m in re.finditer(pat, cf[c0:c1])]
+    pat2 = r"EXPECT_NEAR\(\s*platform_u\[(\d)\],\s*(" + NUM + r"),\s*(" + NUM + r")\)"
+    fpl = [(int(m.group(1)), float(m.group(2)), float(m.group(3))) for m in re.finditer(pat2, cf[c1:c2])]
+    json.dump({"source": "tests/regression_tests/interfaces/test_cfd_interface.cpp",
+               "precession": {"q_500": [v for _, v, _ in pre[0:7]], "q_600": [v for _, v, _ in pre[7:14]],
+                              "tolerance": max(t for _, _, t in pre)},
+               "floating_platform": {"step": 100, "q": [v for _, v, _ in fpl],
+                                     "tolerance": max(t for _, _, t in fpl)}},
+              open(os.path.join(out_dir, "cfd_platform.json"), "w"), indent=1)
 
     # ---- point masses and springs -------------------------------------------------
     def near_calls(text: str, name: str):

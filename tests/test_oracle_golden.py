@@ -211,6 +211,39 @@ def test_heavy_top_final_rotation():
     np.testing.assert_allclose(o.state("q")[0], g["q_mass_node"], rtol=0, atol=g["tolerance"])
 
 
+def test_cfd_platform_precession():
+    """test_cfd_interface.cpp:12-124 (PrecessionTest): the platform node's q
+    after 500 and 600 steps at the test's 1e-12."""
+    from tests.workloads_ref import cfd_platform_model
+    g = load_golden("cfd_platform.json")["precession"]
+    m, p, plat = cfd_platform_model(False)
+    o = OracleModel(m.pack())
+    for i in range(600):
+        st, _ = o.step(p)
+        assert st == 0
+        if i + 1 == 500:
+            np.testing.assert_allclose(o.state("q")[plat], g["q_500"], rtol=0, atol=g["tolerance"])
+    np.testing.assert_allclose(o.state("q")[plat], g["q_600"], rtol=0, atol=g["tolerance"])
+
+
+def test_cfd_floating_platform():
+    """test_cfd_interface.cpp:126-222 (FloatingPlatform): three mooring lines
+    (position-only fairleads and anchors, 42 DOFs); the platform's q after
+    step 100 at the test's 1e-12."""
+    from tests.workloads_ref import cfd_platform_loads, cfd_platform_model
+    g = load_golden("cfd_platform.json")["floating_platform"]
+    m, p, plat = cfd_platform_model(True)
+    o = OracleModel(m.pack())
+    assert o.info.num_dofs == 6 + 6 * 3 + 6 * 3
+    f = np.zeros((o.info.num_nodes, 6))
+    for i in range(g["step"] + 1):
+        f[plat] = cfd_platform_loads(i)
+        o.set_state_f(f)
+        st, _ = o.step(p)
+        assert st == 0
+    np.testing.assert_allclose(o.state("q")[plat], g["q"], rtol=0, atol=g["tolerance"])
+
+
 def test_mass_external_force_velocity():
     """test_masses.cpp:79-144: v after 1000 steps at the test's 1e-12."""
     from tests.workloads_ref import mass_external_force_model

@@ -197,6 +197,52 @@ def heavy_top_model():
     return m, StepParameters(True, 10, 0.002, 0.9, a_tol=1e-5, r_tol=1e-3), bc
 
 
+PLATFORM_MASS = 1.419625e7
+PLATFORM_MOI = (1.2898e10, 1.2851e10, 1.4189e10)
+MOORING = [((-40.87, 0.0, -14.), (-105.47, 0.0, -58.4)), ((20.43, -35.39, -14.), (52.73, -91.34, -58.4)),
+           ((20.43, 35.39, -14.), (52.73, 91.34, -58.4))]
+
+
+def cfd_platform_model(mooring: bool):
+    """src/interfaces/cfd/interface.cpp:47-115 (CreateFloatingPlatform) with the
+    inputs of tests/regression_tests/interfaces/test_cfd_interface.cpp: the
+    platform node with its mass, then per mooring line a position-only fairlead
+    (RigidJoint6DOFsTo3DOFs from the platform) and anchor (FixedBC3DOFs) joined
+    by a spring.  mooring=False: PrecessionTest (unit mass, inertia diag(1, 1,
+    0.5), spin (0.5, 0.5, 1), no gravity, rho_inf 1); True: FloatingPlatform
+    (14,196 t platform at z = -7.53, three lines of k = 48.9 kN, l0 = 55.432 m,
+    gravity -9.8124, rho_inf 0).  Returns (model, params, platform node id)."""
+    m = Model()
+    if mooring:
+        m.SetGravity(0., 0., -9.8124)
+        pos, vel = (0., 0., -7.53), (0., 0., 0., 0., 0., 0.)
+        mass = np.diag([PLATFORM_MASS] * 3 + list(PLATFORM_MOI))
+    else:
+        pos, vel = (0., 0., 0.), (0., 0., 0., 0.5, 0.5, 1.)
+        mass = np.diag([1., 1., 1., 1., 1., .5])
+    plat = m.AddNode().SetPosition(*pos, 1., 0., 0., 0.).SetVelocity(*vel).Build()
+    m.AddMassElement(plat, mass)
+    for fair, anch in (MOORING if mooring else []):
+        f = m.AddNode().SetPosition(*fair, 1., 0., 0., 0.).Build()
+        a = m.AddNode().SetPosition(*anch, 1., 0., 0., 0.).Build()
+        m.AddFixedBC3DOFs(a)
+        m.AddRigidJoint6DOFsTo3DOFs([plat, f])
+        m.AddSpringElement(f, a, 48.9e3, 55.432)
+    return m, StepParameters(True, 5, 0.01, 0.0 if mooring else 1.0), plat
+
+
+def cfd_platform_loads(i: int, h: float = 0.01) -> np.ndarray:
+    """Platform loads before step i of the FloatingPlatform test (t = i h):
+    buoyancy balancing gravity and the initial spring forces plus a sway force
+    and three moments, all sinusoidal."""
+    t = i * h
+    spring0 = 1907514.4912628897
+    buoy = spring0 + 9.8124 * PLATFORM_MASS
+    w = 2. * math.pi
+    return np.array([0., 1e6 * math.sin(w / 20. * t), buoy + 0.5 * spring0 * math.sin(w / 20. * t),
+                     5.0e5 * math.sin(w / 15. * t), 1.0e6 * math.sin(w / 30. * t), 2.0e7 * math.sin(w / 60. * t)])
+
+
 def rotation_control_inputs(i: int, h: float = 0.01):
     """Pitch angle and hub displacement before step i (0-based) of the two
     rotation-control tests: pitch = t pi/2, azimuth = 0.5 t pi/2 about z."""
