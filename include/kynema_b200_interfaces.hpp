@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cstdio>
 #include <limits>
 #include <memory>
 #include <numbers>
@@ -575,5 +576,264 @@ private:
     components::SolutionBuilder solution_;
     components::BeamBuilder blade_;
 };
+
+// ---- CFD interface: floating platform with mooring lines --------------------------
+// src/interfaces/cfd/: a platform node with its mass, and per mooring line a
+// position-only fairlead rigidly carried by the platform
+// (RigidJoint6DOFsTo3DOFs), a position-only anchor (FixedBC3DOFs) and a spring
+// between them.  Platform loads in (NodeData::loads -> state.f), motion of every
+// node out after each Step(), SaveState / RestoreState and restart files.  The
+// model has no beam element and runs as a dense model.
+namespace cfd {
+
+using components::NodeData;
+
+// src/interfaces/cfd/mooring_line_input.hpp
+struct MooringLineInput {
+    double stiffness = 0.;
+    double undeformed_length = 0.;
+    std::array<double, 3> fairlead_position{0., 0., 0.};
+    std::array<double, 3> fairlead_velocity{0., 0., 0.};
+    std::array<double, 3> fairlead_acceleration{0., 0., 0.};
+    std::array<double, 3> anchor_position{0., 0., 0.};
+    std::array<double, 3> anchor_velocity{0., 0., 0.};
+    std::array<double, 3> anchor_acceleration{0., 0., 0.};
+};
+
+// src/interfaces/cfd/floating_platform_input.hpp
+struct FloatingPlatformInput {
+    bool enable = false;
+    std::array<double, 7> position{0., 0., 0., 1., 0., 0., 0.};
+    std::array<double, 6> velocity{0., 0., 0., 0., 0., 0.};
+    std::array<double, 6> acceleration{0., 0., 0., 0., 0., 0.};
+    std::array<std::array<double, 6>, 6> mass_matrix{};
+    std::vector<MooringLineInput> mooring_lines;
+};
+
+// src/interfaces/cfd/interface_input.hpp, turbine_input.hpp
+struct InterfaceInput {
+    std::array<double, 3> gravity{0., 0., 0.};
+    double time_step = 0.01;
+    double rho_inf = 0.;
+    size_t max_iter = 5;
+    FloatingPlatformInput floating_platform;
+    std::string output_file;
+};
+
+// src/interfaces/cfd/mooring_line.hpp, floating_platform.hpp, turbine.hpp
+struct MooringLine {
+    NodeData fairlead_node;
+    NodeData anchor_node;
+    size_t fixed_constraint_id;
+    size_t rigid_constraint_id;
+    size_t spring_element_id;
+};
+struct FloatingPlatform {
+    bool active = false;
+    NodeData node{0};
+    size_t mass_element_id = 0;
+    std::vector<MooringLine> mooring_lines;
+};
+struct Turbine {
+    FloatingPlatform floating_platform;
+};
+
+// src/interfaces/cfd/interface.cpp:47-115 (CreateFloatingPlatform)
+inline FloatingPlatform CreateFloatingPlatform(const FloatingPlatformInput& in, Model& model) {
+    FloatingPlatform p;
+    if (!in.enable) return p;
+    const auto& x = in.position;
+    const auto& v = in.velocity;
+    const auto& a = in.acceleration;
+    const size_t id = model.AddNode()
+                          .SetPosition(x[0], x[1], x[2], x[3], x[4], x[5], x[6])
+                          .SetVelocity(v[0], v[1], v[2], v[3], v[4], v[5])
+                          .SetAcceleration(a[0], a[1], a[2], a[3], a[4], a[5])
+                          .Build();
+    p.active = true;
+    p.node = NodeData(id);
+    p.mass_element_id = model.AddMassElement(id, in.mass_matrix);
+    for (const auto& ml : in.mooring_lines) {
+        const auto& fp = ml.fairlead_position;
+        const auto& fv = ml.fairlead_velocity;
+        const auto& fa = ml.fairlead_acceleration;
+        const size_t fair = model.AddNode()
+                                .SetPosition(fp[0], fp[1], fp[2], 1., 0., 0., 0.)
+                                .SetVelocity(fv[0], fv[1], fv[2], 0., 0., 0.)
+                                .SetAcceleration(fa[0], fa[1], fa[2], 0., 0., 0.)
+                                .Build();
+        const auto& ap = ml.anchor_position;
+        const auto& av = ml.anchor_velocity;
+        const auto& aa = ml.anchor_acceleration;
+        const size_t anch = model.AddNode()
+                                .SetPosition(ap[0], ap[1], ap[2], 1., 0., 0., 0.)
+                                .SetVelocity(av[0], av[1], av[2], 0., 0., 0.)
+                                .SetAcceleration(aa[0], aa[1], aa[2], 0., 0., 0.)
+                                .Build();
+        const size_t fixed = model.AddFixedBC3DOFs(anch);
+        const size_t rigid = model.AddRigidJoint6DOFsTo3DOFs({id, fair});
+        const size_t spring = model.AddSpringElement(fair, anch, ml.stiffness, ml.undeformed_length);
+        p.mooring_lines.push_back({NodeData(fair), NodeData(anch), fixed, rigid, spring});
+    }
+    return p;
+}
+
+// src/interfaces/cfd/interface.hpp
+class Interface {
+public:
+    Interface(const Context& ctx, const InterfaceInput& in)
+        : ctx_(ctx), model_(in.gravity), parameters_(true, in.max_iter, in.time_step, in.rho_inf) {
+        turbine.floating_platform = CreateFloatingPlatform(in.floating_platform, model_);
+        auto [state, elements, constraints, solver] = model_.CreateSystemWithSolver(ctx_);
+        state_ = std::make_unique<State>(state);
+        elements_ = std::make_unique<Elements>(elements);
+        constraints_ = std::make_unique<Constraints>(constraints);
+        solver_ = std::make_unique<Solver>(solver);
+        saved_ = kyn_model_clone(ctx_.get(), solver_->model()->id);  // state_save (CloneState)
+        check(ctx_.get(), saved_);
+        loads_.assign(solver_->model()->info.num_nodes * 6, 0.);
+        GetMotion();
+    }
+    Interface(const Interface&) = delete;
+    Interface& operator=(const Interface&) = delete;
+    Interface(Interface&& o) noexcept
+        : turbine(std::move(o.turbine)), ctx_(o.ctx_), model_(std::move(o.model_)), parameters_(o.parameters_),
+          state_(std::move(o.state_)), elements_(std::move(o.elements_)), constraints_(std::move(o.constraints_)),
+          solver_(std::move(o.solver_)), saved_(o.saved_), loads_(std::move(o.loads_)) {
+        o.saved_ = -1;
+    }
+    ~Interface() {
+        if (saved_ >= 0) kyn_model_destroy(ctx_.get(), saved_);
+    }
+
+    Turbine turbine;
+
+    // Platform loads -> state.f, one step, motion back (interface.cpp:270-296).
+    bool Step() {
+        const auto& p = turbine.floating_platform;
+        if (p.active)
+            for (int c = 0; c < 6; ++c) loads_[p.node.id * 6 + c] = p.node.loads[c];
+        state_->SetExternalForces(loads_);
+        if (!kynema_b200::Step(parameters_, *solver_, *elements_, *state_, *constraints_)) return false;
+        GetMotion();
+        return true;
+    }
+    void SaveState() { check(ctx_.get(), kyn_state_copy(ctx_.get(), saved_, solver_->model()->id)); }
+    void RestoreState() {
+        check(ctx_.get(), kyn_state_copy(ctx_.get(), solver_->model()->id, saved_));
+        GetMotion();
+    }
+    // WriteStateToFile / ReadStateFromFile records (interface.cpp:249-262)
+    void WriteRestart(const std::string& filename) const {
+        size_t bytes = 0;
+        check(ctx_.get(), kyn_state_write(ctx_.get(), solver_->model()->id, nullptr, 0, &bytes));
+        std::vector<char> buf(bytes);
+        check(ctx_.get(), kyn_state_write(ctx_.get(), solver_->model()->id, buf.data(), buf.size(), &bytes));
+        FILE* f = std::fopen(filename.c_str(), "wb");
+        if (!f) throw std::runtime_error("cannot open restart file for writing: " + filename);
+        const size_t w = std::fwrite(buf.data(), 1, buf.size(), f);
+        std::fclose(f);
+        if (w != buf.size()) throw std::runtime_error("short write of restart file: " + filename);
+    }
+    void ReadRestart(const std::string& filename) {
+        FILE* f = std::fopen(filename.c_str(), "rb");
+        if (!f) throw std::runtime_error("cannot open restart file: " + filename);
+        std::vector<char> buf;
+        char chunk[4096];
+        size_t r = 0;
+        while ((r = std::fread(chunk, 1, sizeof(chunk), f)) > 0) buf.insert(buf.end(), chunk, chunk + r);
+        std::fclose(f);
+        check(ctx_.get(), kyn_state_read(ctx_.get(), solver_->model()->id, buf.data(), buf.size()));
+        GetMotion();
+    }
+
+private:
+    void GetMotion() {
+        auto& p = turbine.floating_platform;
+        if (!p.active) return;
+        const auto x = state_->Get(KYN_FIELD_X), q = state_->q(), v = state_->v(), vd = state_->vd();
+        auto fill = [&](NodeData& n) {
+            for (int c = 0; c < 7; ++c) {
+                n.position[c] = x[n.id * 7 + c];
+                n.displacement[c] = q[n.id * 7 + c];
+            }
+            for (int c = 0; c < 6; ++c) {
+                n.velocity[c] = v[n.id * 6 + c];
+                n.acceleration[c] = vd[n.id * 6 + c];
+            }
+        };
+        fill(p.node);
+        for (auto& ml : p.mooring_lines) {
+            fill(ml.fairlead_node);
+            fill(ml.anchor_node);
+        }
+    }
+
+    Context ctx_;
+    Model model_;
+    StepParameters parameters_;
+    std::unique_ptr<State> state_;
+    std::unique_ptr<Elements> elements_;
+    std::unique_ptr<Constraints> constraints_;
+    std::unique_ptr<Solver> solver_;
+    int saved_ = -1;
+    std::vector<double> loads_;
+};
+
+// src/interfaces/cfd/interface_builder.hpp
+class InterfaceBuilder {
+public:
+    InterfaceBuilder& SetGravity(const std::array<double, 3>& g) { in_.gravity = g; return *this; }
+    InterfaceBuilder& SetTimeStep(double h) { in_.time_step = h; return *this; }
+    InterfaceBuilder& SetDampingFactor(double rho) { in_.rho_inf = rho; return *this; }
+    InterfaceBuilder& SetMaximumNonlinearIterations(size_t n) { in_.max_iter = n; return *this; }
+    InterfaceBuilder& EnableFloatingPlatform(bool on) { in_.floating_platform.enable = on; return *this; }
+    InterfaceBuilder& SetFloatingPlatformPosition(const std::array<double, 7>& p) {
+        in_.floating_platform.position = p;
+        return *this;
+    }
+    InterfaceBuilder& SetFloatingPlatformVelocity(const std::array<double, 6>& v) {
+        in_.floating_platform.velocity = v;
+        return *this;
+    }
+    InterfaceBuilder& SetFloatingPlatformAcceleration(const std::array<double, 6>& a) {
+        in_.floating_platform.acceleration = a;
+        return *this;
+    }
+    InterfaceBuilder& SetFloatingPlatformMassMatrix(const std::array<std::array<double, 6>, 6>& m) {
+        in_.floating_platform.mass_matrix = m;
+        return *this;
+    }
+    InterfaceBuilder& SetNumberOfMooringLines(size_t n) {
+        in_.floating_platform.mooring_lines.resize(n);
+        return *this;
+    }
+    InterfaceBuilder& SetMooringLineStiffness(size_t i, double k) { line(i).stiffness = k; return *this; }
+    InterfaceBuilder& SetMooringLineUndeformedLength(size_t i, double l) {
+        line(i).undeformed_length = l;
+        return *this;
+    }
+    InterfaceBuilder& SetMooringLineFairleadPosition(size_t i, const std::array<double, 3>& p) {
+        line(i).fairlead_position = p;
+        return *this;
+    }
+    InterfaceBuilder& SetMooringLineAnchorPosition(size_t i, const std::array<double, 3>& p) {
+        line(i).anchor_position = p;
+        return *this;
+    }
+    // NetCDF output is not part of this path; the path is recorded only
+    InterfaceBuilder& SetOutputFile(const std::string& f) { in_.output_file = f; return *this; }
+    Interface Build(const Context& ctx = Context(0)) const { return Interface(ctx, in_); }
+
+private:
+    MooringLineInput& line(size_t i) {
+        if (i >= in_.floating_platform.mooring_lines.size())
+            throw std::out_of_range("mooring line index beyond SetNumberOfMooringLines");
+        return in_.floating_platform.mooring_lines[i];
+    }
+    InterfaceInput in_;
+};
+
+}  // namespace cfd
 
 }  // namespace kynema_b200::interfaces

@@ -18,6 +18,7 @@ LIB_DIR = os.path.join(ROOT, "openturbine_b200", "_lib")
 
 
 BLADE_SRC = os.path.join(ROOT, "tests", "cpp", "test_blade_interface.cpp")
+CFD_SRC = os.path.join(ROOT, "tests", "cpp", "test_cfd_interface.cpp")
 
 
 def _compile(src: str = SRC, name: str = "test_shim") -> str:
@@ -34,6 +35,7 @@ def _compile(src: str = SRC, name: str = "test_shim") -> str:
 def test_shim_compiles():
     assert os.path.exists(_compile())
     assert os.path.exists(_compile(BLADE_SRC, "test_blade_interface"))
+    assert os.path.exists(_compile(CFD_SRC, "test_cfd_interface"))
 
 
 def test_interface_geometry_helpers():
@@ -99,3 +101,16 @@ def test_shim_cantilever_and_rotating_beam():
     print(r.stdout)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "OK (0 failures)" in r.stdout
+
+
+@pytest.mark.gpu
+def test_cfd_interface_floating_platform(tmp_path):
+    """CFD interface (include/kynema_b200_interfaces.hpp, namespace cfd) on the
+    reference's CFDInterfaceTest.PrecessionTest (with SaveState/RestoreState),
+    FloatingPlatform (three mooring lines) and Restart, at the tests' 1e-12."""
+    exe = _compile(CFD_SRC, "test_cfd_interface")
+    r = subprocess.run([exe, str(tmp_path / "restart.dat")], capture_output=True, text=True, timeout=300)
+    print(r.stdout)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "OK (0 failures)" in r.stdout
+

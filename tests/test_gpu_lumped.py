@@ -222,3 +222,39 @@ def test_dense_models_batched_with_beams_and_fp32_form(ctx):
                 np.testing.assert_array_equal(ctx.state(mid, f), ctx.state(alone, f))
         for mid in [alone] + mixed + others:
             ctx.destroy_model(mid)
+
+
+def test_cfd_floating_platform_models(ctx):
+    """The CFD interface's platform models (test_cfd_interface.cpp): the
+    spinning platform (mass only, the beam-free lumped path, 600 steps) and the
+    moored platform (three position-only fairleads and anchors, six three-row
+    constraints: a dense model of 42 DOFs, 101 steps under the test's loads).
+    Same Newton decisions and states as the oracle, goldens at 1e-12."""
+    from tests.workloads_ref import cfd_platform_loads, cfd_platform_model
+    g = load_golden("cfd_platform.json")
+    m, p, plat = cfd_platform_model(False)
+    mid = _run(ctx, m, p, 600)
+    np.testing.assert_allclose(ctx.state(mid, "q")[plat], g["precession"]["q_600"], rtol=0, atol=1e-12)
+    ctx.destroy_model(mid)
+
+    m, p, plat = cfd_platform_model(True)
+    pm = m.pack()
+    mid = ctx.create_model(pm)
+    assert ctx.info(mid).num_dofs == 42
+    rp, ci, _ = ctx.crs(mid, values=False)
+    tw = LumpedTwin(pm)
+    orp, oci, _ = tw.crs()
+    assert np.array_equal(rp, orp) and np.array_equal(ci, oci)
+    f = np.zeros((ctx.info(mid).num_nodes, 6))
+    for i in range(g["floating_platform"]["step"] + 1):
+        f[plat] = cfd_platform_loads(i)
+        ctx.set_state_f(mid, f)
+        tw.set_state_f(f)
+        st, it = ctx.step([mid], p)
+        ost, oit = tw.step(p)
+        assert (st[0], it[0]) == (ost, oit) == (0, oit)
+    assert_state_close(ctx, mid, tw, fields=FIELDS, lam=False)
+    lg, lo = ctx.state(mid, "lambda"), tw.state("lambda")
+    assert np.abs(lg - lo).max() <= ACCEL_REL * np.abs(lo).max()
+    np.testing.assert_allclose(ctx.state(mid, "q")[plat], g["floating_platform"]["q"], rtol=0, atol=1e-12)
+    ctx.destroy_model(mid)
