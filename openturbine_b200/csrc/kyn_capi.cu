@@ -1271,8 +1271,9 @@ int kyn_get_crs(kyn_ctx* c, int id, int* row_ptrs, int* col_inds, double* values
     if (row_ptrs) std::copy(H.row_ptrs.begin(), H.row_ptrs.end(), row_ptrs);
     if (col_inds) std::copy(H.col_inds.begin(), H.col_inds.end(), col_inds);
     if (!values) return KYN_OK;
-    if (m->host.hub >= 0)
-        return set_err(c, KYN_ERR_UNSUPPORTED, "system values are not recorded for models with a hub");
+    if (m->host.hub >= 0 || m->host.beams[0].dense)
+        return set_err(c, KYN_ERR_UNSUPPORTED,
+                       "system values are not recorded for models with a hub or dense models");
     if (!m->d_dump) return set_err(c, KYN_ERR_INVALID, "KYN_OPT_RECORD_SYSTEM was not set");
     KYN_CUDA(c, cudaStreamSynchronize(c->stream));
     std::fill(values, values + H.col_inds.size(), 0.);
@@ -1307,8 +1308,9 @@ int kyn_get_system_vectors(kyn_ctx* c, int id, double* rhs, double* solution) {
     if (!c) return KYN_ERR_INVALID;
     DevModel* m = find_model(c, id);
     if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
-    if (m->host.hub >= 0)
-        return set_err(c, KYN_ERR_UNSUPPORTED, "system values are not recorded for models with a hub");
+    if (m->host.hub >= 0 || m->host.beams[0].dense)
+        return set_err(c, KYN_ERR_UNSUPPORTED,
+                       "system values are not recorded for models with a hub or dense models");
     if (!m->d_dump) return set_err(c, KYN_ERR_INVALID, "KYN_OPT_RECORD_SYSTEM was not set");
     KYN_CUDA(c, cudaStreamSynchronize(c->stream));
     const HostModel& H = m->host;

@@ -979,7 +979,7 @@ __device__ void add_lumped_terms(int n, const double* __restrict__ rec, int n_ma
 // in both precision forms: these systems have at most kDenseModelMaxDofs unknowns.
 
 struct DenseSmem {
-    int M, b, x, q, qp, v, vd, a, qd, T, resid, con, act, fmap, piv, bytes;
+    int M, b, x, q, qp, v, vd, a, qd, T, resid, con, act, fmap, red, bytes;
 };
 __host__ __device__ inline DenseSmem make_dense_smem(int N, int nd) {
     DenseSmem S{};
@@ -1003,7 +1003,7 @@ __host__ __device__ inline DenseSmem make_dense_smem(int N, int nd) {
     S.con = take(kMaxBeamConstraints * kConStride * 8);
     S.act = take(N * 4);
     S.fmap = take(N * 4);
-    S.piv = take(64 * 8);
+    S.red = take(64 * 8);  // per-warp partial sums of the error
     S.bytes = o;
     return S;
 }
@@ -1032,7 +1032,7 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
     double* con = reinterpret_cast<double*>(smem_raw + S.con);
     int* act = reinterpret_cast<int*>(smem_raw + S.act);
     int* fmap = reinterpret_cast<int*>(smem_raw + S.fmap);
-    double* red = reinterpret_cast<double*>(smem_raw + S.piv);
+    double* red = reinterpret_cast<double*>(smem_raw + S.red);
     __shared__ int s_flag, s_nsys, s_piv;
     const double h = P.h;
 
@@ -1385,7 +1385,7 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
         status_out[KB.plan_model] = status;
         iters_out[KB.plan_model] = iters;
     }
-    (void)record;
+    (void)record;  // dense models keep no system dump (kyn_get_system refuses them)
 }
 
 // One CTA per dense model.
