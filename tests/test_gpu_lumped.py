@@ -258,3 +258,44 @@ def test_cfd_floating_platform_models(ctx):
     assert np.abs(lg - lo).max() <= ACCEL_REL * np.abs(lo).max()
     np.testing.assert_allclose(ctx.state(mid, "q")[plat], g["floating_platform"]["q"], rtol=0, atol=1e-12)
     ctx.destroy_model(mid)
+
+
+def test_dense_model_with_six_row_joints(ctx):
+    """Beam-free models whose nodes are joined by six-row joints run as dense
+    models: a spinning body (mass B) carried by a RigidJoint from a body (mass
+    A) that hangs from a fixed, position-only pivot (RigidJoint6DOFsTo3DOFs +
+    FixedBC3DOFs), and the same with the rigid joint replaced by a
+    RotationControl turning B about the joint axis.  Same CRS, Newton
+    decisions and states as the oracle over 60 steps."""
+    from openturbine_b200.model import Model, StepParameters
+    for control in (False, True):
+        m = Model()
+        m.SetGravity(0., 0., -9.81)
+        a = m.AddNode().SetPosition(0., 1., 0., 1., 0., 0., 0.).SetVelocity(0., 0., 0., 0., 0., 2.).Build()
+        b = m.AddNode().SetPosition(0., 2., 0., 1., 0., 0., 0.).SetVelocity(-2., 0., 0., 0., 0., 2.).Build()
+        pivot = m.AddNode().SetPosition(0., 0., 0., 1., 0., 0., 0.).Build()
+        m.AddMassElement(a, np.diag([5., 5., 5., 0.2, 0.1, 0.2]))
+        m.AddMassElement(b, np.diag([2., 2., 2., 0.05, 0.05, 0.08]))
+        m.AddRigidJoint6DOFsTo3DOFs([a, pivot])
+        m.AddFixedBC3DOFs(pivot)
+        rc = (m.AddRotationControl([a, b], [0., 1., 0.]) if control else m.AddRigidJointConstraint([a, b]))
+        p = StepParameters(True, 8, 0.005, 0.8, a_tol=1e-6, r_tol=1e-3)
+        pm = m.pack()
+        mid = ctx.create_model(pm)
+        assert ctx.info(mid).num_dofs == 6 + 6 + 3 + 3 + 3 + 6
+        rp, ci, _ = ctx.crs(mid, values=False)
+        tw = LumpedTwin(pm)
+        orp, oci, _ = tw.crs()
+        assert np.array_equal(rp, orp) and np.array_equal(ci, oci)
+        for k in range(60):
+            if control:
+                ang = 0.5 * 0.005 * (k + 1)
+                ctx.set_control(mid, rc, ang)
+                tw.set_prescribed(rc, [ang, 0., 0., 1., 0., 0., 0.])
+            st, it = ctx.step([mid], p)
+            ost, oit = tw.step(p)
+            assert (st[0], it[0]) == (ost, oit) == (0, oit)
+        assert_state_close(ctx, mid, tw, fields=FIELDS, lam=False)
+        lg, lo = ctx.state(mid, "lambda"), tw.state("lambda")
+        assert np.abs(lg - lo).max() <= ACCEL_REL * np.abs(lo).max()
+        ctx.destroy_model(mid)
