@@ -9,6 +9,8 @@
 // form a thread-block cluster and sum the model's convergence error through
 // distributed shared memory, so every beam of a model takes the same Newton
 // iterations as the reference's model-wide loop (src/step/step.hpp:54-83).
+// Models without beam elements whose constraints are more than single-node
+// BCs run in dense_kernel (the bordered system with a pivoted LU).
 //
 // Linear solve: the reference factors the whole bordered system with a
 // sparse direct solver (src/step/solve_system.hpp:27-31).  Here the

@@ -1,10 +1,13 @@
 // kyn_types.h -- data structures shared by the host setup and the CUDA kernels.
 //
-// Layout in HBM: every beam element owns one contiguous "slab" of doubles
-// holding its constant geometry (shape tables, quadrature data, sectional
-// 6x6 matrices) followed by its resident node state in beam-local node order.
-// A model is a set of independent beam blocks (no node shared between beams),
-// so one beam's slab is everything its CTA reads and writes during a step.
+// Layout in HBM: every beam system (an element, or elements sharing nodes, or
+// the nodes of a model without beam elements) owns one contiguous "slab" of
+// doubles holding its constant geometry (shape tables, quadrature data,
+// sectional 6x6 matrices) followed by its resident node state in local node
+// order, its constraints' inputs and multipliers, and the hub-chain records
+// of a jointed model.  Beam systems share no nodes, so one slab is everything
+// its CTA reads and writes during a step; what couples the systems of a model
+// (its hub chain) is kept as identical copies in every slab of the model.
 #pragma once
 
 #include <cstdint>
