@@ -230,6 +230,17 @@ KYN_API int kyn_model_create(kyn_ctx* ctx, const kyn_model_desc* desc);
 KYN_API int kyn_model_destroy(kyn_ctx* ctx, int model_id);
 KYN_API int kyn_model_info_get(kyn_ctx* ctx, int model_id, kyn_model_info* info);
 
+/* Host only (no device, no context): validates a description as
+ * kyn_model_create does and reports its sizes and, when row_ptrs / col_inds are
+ * not NULL, its CRS graph (row_ptrs [num_dofs + 1], col_inds [nnz]; the graph of
+ * Model::CreateSystemWithSolver, src/solver/create_full_matrix.hpp:27-73).
+ * info->device_bytes is the slab footprint a model would take.  err (errlen
+ * bytes, may be NULL) receives the reason of a negative return code.  No
+ * counterpart in the reference: lets a caller check a model, and tests check the
+ * DOF map and CRS graph of every model type, without a GPU. */
+KYN_API int kyn_model_describe(const kyn_model_desc* desc, kyn_model_info* info, int32_t* row_ptrs,
+                               int32_t* col_inds, char* err, int errlen);
+
 /* A new model that is a copy of an existing one in its current state (same
  * description, node state, multipliers and loads; its own device memory,
  * counted against the HBM budget).  No counterpart in the reference: a server

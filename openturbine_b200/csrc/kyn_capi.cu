@@ -1015,6 +1015,39 @@ int kyn_model_info_get(kyn_ctx* c, int id, kyn_model_info* info) {
     return KYN_OK;
 }
 
+int kyn_model_describe(const kyn_model_desc* desc, kyn_model_info* info, int32_t* row_ptrs,
+                       int32_t* col_inds, char* err, int errlen) {
+    if (!info) return KYN_ERR_INVALID;
+    HostModel h;
+    std::string msg;
+    const int rc = build_host_model(desc, h, msg);
+    if (rc != KYN_OK) {
+        if (err && errlen > 0) std::snprintf(err, static_cast<size_t>(errlen), "%s", msg.c_str());
+        return rc;
+    }
+    const bool lumped = !h.beams.empty() && h.beams[0].lumped;
+    info->num_nodes = h.num_nodes;
+    info->num_beams = lumped ? 0 : h.num_elements;
+    info->num_constraints = h.num_constraints;
+    info->num_system_dofs = h.nsys;
+    info->num_dofs = h.ndofs;
+    info->nnz = static_cast<int32_t>(h.col_inds.size());
+    int mn = 0, mq = 0;
+    int64_t bytes = kMaxNewtonIters * static_cast<int64_t>(sizeof(double));
+    for (auto& b : h.beams) {
+        bytes += static_cast<int64_t>(b.slab.size() * sizeof(double));
+        if (b.lumped) continue;
+        mn = std::max(mn, b.N);
+        mq = std::max(mq, b.Q);
+    }
+    info->max_beam_nodes = mn;
+    info->max_beam_qps = mq;
+    info->device_bytes = bytes;
+    if (row_ptrs) std::copy(h.row_ptrs.begin(), h.row_ptrs.end(), row_ptrs);
+    if (col_inds) std::copy(h.col_inds.begin(), h.col_inds.end(), col_inds);
+    return KYN_OK;
+}
+
 int kyn_model_set_loads(kyn_ctx* c, int id, int which, const double* values) {
     if (!c || !values) return KYN_ERR_INVALID;
     DevModel* m = find_model(c, id);

@@ -47,6 +47,8 @@ def load_library():
             f"{LIB_PATH} is missing: build it with `python -m openturbine_b200.build` "
             "(nvcc, sm_100a); there is no CPU fallback")
     L = ctypes.CDLL(LIB_PATH)
+    L.kyn_model_describe.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_int), ctypes.c_char_p, ctypes.c_int]
     L.kyn_ctx_create.restype = ctypes.c_void_p
     L.kyn_ctx_create.argtypes = [ctypes.c_int, ctypes.c_size_t]
     L.kyn_ctx_destroy.argtypes = [ctypes.c_void_p]
@@ -88,6 +90,27 @@ def load_library():
     L.kyn_ctx_stream.argtypes = [ctypes.c_void_p]
     _lib = L
     return L
+
+
+def describe(model: Model | PackedModel):
+    """Host-only check of a model description (kyn_model_describe): the sizes
+    and the CRS graph (row_ptrs, col_inds) that kyn_model_create would build,
+    without a GPU.  Raises RuntimeError with the library's reason when the
+    description is invalid or outside this path."""
+    L = load_library()
+    pm = model.pack() if isinstance(model, Model) else model
+    info = KynModelInfo()
+    err = ctypes.create_string_buffer(256)
+    rc = L.kyn_model_describe(ctypes.byref(pm.desc), ctypes.byref(info), None, None, err, 256)
+    if rc < 0:
+        raise RuntimeError(f"kyn_model_describe: {ERR.get(rc, rc)}: {err.value.decode()}")
+    rp = np.zeros(info.num_dofs + 1, dtype=np.int32)
+    ci = np.zeros(info.nnz, dtype=np.int32)
+    rc = L.kyn_model_describe(ctypes.byref(pm.desc), ctypes.byref(info), rp.ctypes.data_as(_ip),
+                              ci.ctypes.data_as(_ip), err, 256)
+    if rc < 0:
+        raise RuntimeError(f"kyn_model_describe: {ERR.get(rc, rc)}: {err.value.decode()}")
+    return info, rp, ci
 
 
 class Context:
