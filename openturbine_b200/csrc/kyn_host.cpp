@@ -621,20 +621,20 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
     M.active.assign(nn, 6);
     if (dense) {
         std::vector<int> sig(nn, 0);
-        for (int e = 0; e < n_mass; ++e) sig[d->mass_node[e]] |= 63;
+        for (int e = 0; e < n_mass; ++e) sig[d->mass_node[e]] |= kSigAll;
         for (int e = 0; e < n_spring; ++e) {
-            sig[d->spring_nodes[2 * e]] |= 56;
-            sig[d->spring_nodes[2 * e + 1]] |= 56;
+            sig[d->spring_nodes[2 * e]] |= kSigPosition;
+            sig[d->spring_nodes[2 * e + 1]] |= kSigPosition;
         }
         for (int c = 0; c < d->num_constraints; ++c) {
             const int t = d->constraint_type[c];
-            sig[d->constraint_target_node[c]] |= t >= KYN_CONSTRAINT_FIXED_BC_3DOF ? 56 : 63;
-            if (is_hub_joint(t) || t == KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF) sig[base_of(c)] |= 63;
+            sig[d->constraint_target_node[c]] |= t >= KYN_CONSTRAINT_FIXED_BC_3DOF ? kSigPosition : kSigAll;
+            if (is_hub_joint(t) || t == KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF) sig[base_of(c)] |= kSigAll;
         }
         for (int n = 0; n < nn; ++n) {
-            if (sig[n] != 63 && sig[n] != 56)
+            if (sig[n] != kSigAll && sig[n] != kSigPosition)
                 return fail(err, KYN_ERR_UNSUPPORTED, "dense-model node without six or three DOFs");
-            M.active[n] = sig[n] == 63 ? 6 : 3;
+            M.active[n] = sig[n] == kSigAll ? 6 : 3;
         }
     }
     M.fmap.resize(nn);

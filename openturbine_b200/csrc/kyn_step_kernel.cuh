@@ -1056,20 +1056,20 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
         // joint bases six; DOF map = exclusive scan (compute_node_freedom_map_table.hpp)
         for (int n = 0; n < N; ++n) act[n] = 0;
         const double* mrec = KB.lumped;
-        for (int e = 0; e < KB.n_mass; ++e) act[static_cast<int>(mrec[e * kMassRec])] |= 63;
+        for (int e = 0; e < KB.n_mass; ++e) act[static_cast<int>(mrec[e * kMassRec])] |= kSigAll;
         const double* srec = KB.lumped + KB.n_mass * kMassRec;
         for (int e = 0; e < KB.n_spring; ++e) {
-            act[static_cast<int>(srec[e * kSpringRec])] |= 56;
-            act[static_cast<int>(srec[e * kSpringRec + 1])] |= 56;
+            act[static_cast<int>(srec[e * kSpringRec])] |= kSigPosition;
+            act[static_cast<int>(srec[e * kSpringRec + 1])] |= kSigPosition;
         }
         for (int c = 0; c < nc; ++c) {
             const int t = KB.con_type[c];
-            act[KB.con_node[c]] |= (t >= KYN_CONSTRAINT_FIXED_BC_3DOF) ? 56 : 63;
-            if (KB.con_base[c] >= 0) act[KB.con_base[c]] |= 63;
+            act[KB.con_node[c]] |= (t >= KYN_CONSTRAINT_FIXED_BC_3DOF) ? kSigPosition : kSigAll;
+            if (KB.con_base[c] >= 0) act[KB.con_base[c]] |= kSigAll;
         }
         int o = 0;
         for (int n = 0; n < N; ++n) {
-            act[n] = (act[n] == 63) ? 6 : (act[n] == 56) ? 3 : 0;
+            act[n] = (act[n] == kSigAll) ? 6 : (act[n] == kSigPosition) ? 3 : 0;
             fmap[n] = o;
             o += act[n];
         }

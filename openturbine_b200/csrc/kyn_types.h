@@ -119,6 +119,10 @@ constexpr int kSpringRec = 7;
 // Joints between the hub node and a target node (six rows, base blocks on the
 // hub): KYN_CONSTRAINT_RIGID_JOINT (3) and KYN_CONSTRAINT_ROTATION_CONTROL (5).
 KYN_HD inline bool is_hub_joint(int type) { return type == 3 || type == 5; }
+// Node freedom signatures (src/dof_management/freedom_signature.hpp): all six
+// components, or the three positions of a position-only node.
+constexpr int kSigAll = 0b111111;
+constexpr int kSigPosition = 0b111000;
 // Rows of a constraint (src/constraints/constraint_type.hpp NumRowsForConstraint).
 KYN_HD inline int constraint_rows(int type) { return type == 4 ? 5 : type >= 6 ? 3 : 6; }
 
