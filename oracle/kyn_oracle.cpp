@@ -1967,4 +1967,52 @@ void orc_tangent_operator(double h, const double qdelta[6], double t_stored[36])
     tangent_operator(h, qdelta, t_stored);
 }
 
+// Kernel-level forms of the revolute joint's residual and gradients, torque
+// and output (the oracle's update_revolute_joint / revolute_output on a
+// two-node model: base node 0, target node 1, identity tangents), for the
+// reference's unit tests test_calculate_revolute_joint_{constraint,force,output}.cpp.
+void orc_revolute_joint(const double X0[3], const double axes[9], const double base_u[7],
+                        const double target_u[7], double torque, double res[6], double base_grad[36],
+                        double target_grad[36], double sys_res[6]) {
+    orc_model m;
+    m.num_nodes = 2;
+    m.q.assign(base_u, base_u + 7);
+    m.q.insert(m.q.end(), target_u, target_u + 7);
+    m.tangent.assign(72, 0.);
+    for (int n = 0; n < 2; ++n)
+        for (int c = 0; c < 6; ++c) m.tangent[n * 36 + c * 7] = 1.;
+    OConstraint C;
+    C.type = KYN_CONSTRAINT_REVOLUTE_JOINT;
+    C.base = 0;
+    C.target = 1;
+    for (int k = 0; k < 3; ++k) C.X0[k] = X0[k];
+    for (int k = 0; k < 9; ++k) C.axes[k] = axes[k];
+    C.input[0] = torque;
+    update_revolute_joint(m, C);
+    for (int k = 0; k < 6; ++k) {
+        res[k] = C.res[k];
+        sys_res[k] = C.sys_res[k];
+    }
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) {
+            base_grad[i * 6 + j] = C.b_grad_trans[j * 6 + i];
+            target_grad[i * 6 + j] = C.t_grad_trans[j * 6 + i];
+        }
+}
+
+void orc_revolute_output(const double axes[9], const double u[7], const double udot[6],
+                         const double uddot[6], double out[3]) {
+    orc_model m;
+    m.num_nodes = 1;
+    m.q.assign(u, u + 7);
+    m.v.assign(udot, udot + 6);
+    m.vd.assign(uddot, uddot + 6);
+    OConstraint C;
+    C.type = KYN_CONSTRAINT_REVOLUTE_JOINT;
+    C.target = 0;
+    for (int k = 0; k < 9; ++k) C.axes[k] = axes[k];
+    revolute_output(m, C);
+    for (int k = 0; k < 3; ++k) out[k] = C.output[k];
+}
+
 }  // extern "C"

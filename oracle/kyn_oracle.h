@@ -66,6 +66,11 @@ void orc_lagrange_interp_weights(double x, const double* xs, int n, double* w);
 void orc_lagrange_deriv_weights(double x, const double* xs, int n, double* w);
 void orc_gll_points(int order, double* pts);
 void orc_rotate_section(const double xr[4], const double cstar[36], double out[36]);
+void orc_revolute_joint(const double X0[3], const double axes[9], const double base_u[7],
+                        const double target_u[7], double torque, double res[6], double base_grad[36],
+                        double target_grad[36], double sys_res[6]);
+void orc_revolute_output(const double axes[9], const double u[7], const double udot[6],
+                         const double uddot[6], double out[3]);
 void orc_calc_strain(const double x0p[3], const double up[3], const double r[4],
                      const double rp[4], double strain[6]);
 void orc_calc_fc(const double cuu[36], const double strain[6], double fc[6]);

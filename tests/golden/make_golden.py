@@ -18,6 +18,8 @@ Sources (paths relative to the reference project root):
   tests/unit_tests/system/beams/test_curved_beam.hpp         kernel-level data
   tests/regression_tests/interfaces/test_blade_interface.cpp + its WindIO file
                                                              IEA-15 blade input, tip
+  tests/unit_tests/constraints/test_calculate_revolute_joint_*.cpp
+                                                             revolute joint kernels
   tests/regression_tests/interfaces/test_cfd_interface.cpp    floating platform q
                                                              (mass, mooring springs)
   tests/regression_tests/regression/test_heavy_top.cpp         heavy top q (three-row
@@ -237,6 +239,25 @@ def main(ref: str) -> None:
                "floating_platform": {"step": 100, "q": [v for _, v, _ in fpl],
                                      "tolerance": max(t for _, _, t in fpl)}},
               open(os.path.join(out_dir, "cfd_platform.json"), "w"), indent=1)
+
+    # ---- revolute joint kernels (unit tests: residual/gradients, torque, output) ----
+    ut = os.path.join(ref, "tests", "unit_tests", "constraints")
+
+    def views(text):
+        out = {}
+        for mm in re.finditer(r'CreateView<[^>]*>\(\s*"(\w+)",\s*std::array(?:<[^>]*>)?\{', text):
+            out[mm.group(1)] = [float(x) for x in re.findall(NUM, _block(text, mm.end() - 1))]
+        for mm in re.finditer(r"(\w+_exact_data)\s*=\s*std::array\{", text):
+            out[mm.group(1)] = [float(x) for x in re.findall(NUM, _block(text, mm.end() - 1))]
+        return out
+    rj = {}
+    for key, fname in (("constraint", "test_calculate_revolute_joint_constraint.cpp"),
+                       ("force", "test_calculate_revolute_joint_force.cpp"),
+                       ("output", "test_calculate_revolute_joint_output.cpp")):
+        rj[key] = views(strip_comments(open(os.path.join(ut, fname)).read()))
+    rj["source"] = "tests/unit_tests/constraints/test_calculate_revolute_joint_{constraint,force,output}.cpp"
+    rj["tolerance"] = 1e-15
+    json.dump(rj, open(os.path.join(out_dir, "revolute_unit.json"), "w"), indent=1)
 
     # ---- point masses and springs -------------------------------------------------
     def near_calls(text: str, name: str):

@@ -104,3 +104,31 @@ def test_tangent_operator_small_angle():
     T = np.zeros(36)
     L.orc_tangent_operator(ctypes.c_double(0.01), p(np.zeros(6)), T.ctypes.data_as(D))
     np.testing.assert_array_equal(T.reshape(6, 6), np.eye(6))
+
+
+def test_revolute_joint_kernels():
+    """The oracle's revolute joint (residual and gradients, generator torque,
+    output) against the reference's unit tests
+    test_calculate_revolute_joint_{constraint,force,output}.cpp at their 1e-15
+    (unnormalised quaternions: the formulas, not rotations, are checked)."""
+    L = lib()
+    g = load_golden("revolute_unit.json")
+    c = g["constraint"]
+    res, bg, tg, sr = np.zeros(6), np.zeros(36), np.zeros(36), np.zeros(6)
+    L.orc_revolute_joint(p(c["X0"]), p(c["axes"]), p(c["base_node_u"]), p(c["target_node_u"]),
+                         ctypes.c_double(0.), res.ctypes.data_as(D), bg.ctypes.data_as(D),
+                         tg.ctypes.data_as(D), sr.ctypes.data_as(D))
+    np.testing.assert_allclose(res, c["residual_terms_exact_data"], rtol=0, atol=g["tolerance"])
+    np.testing.assert_allclose(bg, c["base_gradient_terms_exact_data"], rtol=0, atol=g["tolerance"])
+    np.testing.assert_allclose(tg, -np.array(c["base_gradient_terms_exact_data"]), rtol=0,
+                               atol=g["tolerance"])
+    f = g["force"]
+    L.orc_revolute_joint(p([0., 0., 0.]), p(f["axes"]), p([0., 0., 0., 1., 0., 0., 0.]), p(f["node_u"]),
+                         ctypes.c_double(f["constraint_inputs"][0]), res.ctypes.data_as(D),
+                         bg.ctypes.data_as(D), tg.ctypes.data_as(D), sr.ctypes.data_as(D))
+    np.testing.assert_allclose(sr, f["residual_terms_exact_data"], rtol=0, atol=g["tolerance"])
+    o = g["output"]
+    out = np.zeros(3)
+    L.orc_revolute_output(p(o["axes"]), p(o["node_u"][7:]), p(o["node_udot"][6:]), p(o["node_uddot"][6:]),
+                          out.ctypes.data_as(D))
+    np.testing.assert_allclose(out, o["outputs_exact_data"], rtol=0, atol=g["tolerance"])
