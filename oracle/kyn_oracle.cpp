@@ -2000,6 +2000,38 @@ void orc_revolute_joint(const double X0[3], const double axes[9], const double b
         }
 }
 
+// Kernel-level form of the six-row constraints (FixedBC, PrescribedBC,
+// RigidJoint, RotationControl with its raw axis) on a two-node model (base 0,
+// target 1, identity tangents): residual and gradients, for the reference's
+// unit tests test_calculate_{fixed_bc,prescribed_bc,rigid_joint,rotation_control}_constraint.cpp.
+void orc_constraint_kernel(int type, const double X0[3], const double axis[3], const double input[7],
+                           const double base_u[7], const double target_u[7], double res[6],
+                           double base_grad[36], double target_grad[36]) {
+    orc_model m;
+    m.num_nodes = 2;
+    m.q.assign(base_u, base_u + 7);
+    m.q.insert(m.q.end(), target_u, target_u + 7);
+    m.tangent.assign(72, 0.);
+    for (int n = 0; n < 2; ++n)
+        for (int c = 0; c < 6; ++c) m.tangent[n * 36 + c * 7] = 1.;
+    OConstraint C;
+    C.type = type;
+    C.base = 0;
+    C.target = 1;
+    for (int k = 0; k < 3; ++k) {
+        C.X0[k] = X0[k];
+        C.axis[k] = axis[k];
+    }
+    for (int k = 0; k < 7; ++k) C.input[k] = input[k];
+    update_constraint(m, C);
+    for (int k = 0; k < 6; ++k) res[k] = C.res[k];
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) {
+            base_grad[i * 6 + j] = C.b_grad_trans[j * 6 + i];
+            target_grad[i * 6 + j] = C.t_grad_trans[j * 6 + i];
+        }
+}
+
 void orc_revolute_output(const double axes[9], const double u[7], const double udot[6],
                          const double uddot[6], double out[3]) {
     orc_model m;

@@ -69,6 +69,9 @@ void orc_rotate_section(const double xr[4], const double cstar[36], double out[3
 void orc_revolute_joint(const double X0[3], const double axes[9], const double base_u[7],
                         const double target_u[7], double torque, double res[6], double base_grad[36],
                         double target_grad[36], double sys_res[6]);
+void orc_constraint_kernel(int type, const double X0[3], const double axis[3], const double input[7],
+                           const double base_u[7], const double target_u[7], double res[6],
+                           double base_grad[36], double target_grad[36]);
 void orc_revolute_output(const double axes[9], const double u[7], const double udot[6],
                          const double uddot[6], double out[3]);
 void orc_calc_strain(const double x0p[3], const double up[3], const double r[4],

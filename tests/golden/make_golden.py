@@ -258,6 +258,14 @@ def main(ref: str) -> None:
     rj["source"] = "tests/unit_tests/constraints/test_calculate_revolute_joint_{constraint,force,output}.cpp"
     rj["tolerance"] = 1e-15
     json.dump(rj, open(os.path.join(out_dir, "revolute_unit.json"), "w"), indent=1)
+    cu = {}
+    for key, fname in (("fixed_bc", "test_calculate_fixed_bc_constraint.cpp"),
+                       ("prescribed_bc", "test_calculate_prescribed_bc_constraint.cpp"),
+                       ("rigid_joint", "test_calculate_rigid_joint_constraint.cpp"),
+                       ("rotation_control", "test_calculate_rotation_control_constraint.cpp")):
+        cu[key] = views(strip_comments(open(os.path.join(ut, fname)).read()))
+    cu["source"] = "tests/unit_tests/constraints/test_calculate_{fixed_bc,prescribed_bc,rigid_joint,rotation_control}_constraint.cpp"
+    json.dump(cu, open(os.path.join(out_dir, "constraint_unit.json"), "w"), indent=1)
 
     # ---- point masses and springs -------------------------------------------------
     def near_calls(text: str, name: str):
