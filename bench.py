@@ -151,26 +151,29 @@ def cpu_baseline(draws, params, steps: int, threads: int) -> dict:
 
 def run_reference(args) -> None:
     """--impl reference: the reference's CPU path (the oracle port: the reference
-    itself needs Kokkos/KokkosKernels/a sparse solver, absent here) on the host
-    cores, each step a bounded sample of the batch."""
+    itself needs Kokkos/KokkosKernels/a sparse solver, absent here) on all host
+    cores, on the same configuration as the GPU arm: every step advances the
+    whole batch (`--beams`, 4096 by default) one time step, with the same load
+    schedule (time index k of the warm-up and timed steps)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from oracle.oracle_py import OracleModel, run_batch
+    from oracle.oracle_py import OracleModel, run_batch_record
     threads = os.cpu_count() or 1
-    sample = args.ref_sample
-    draws = W.draw_batch(sample)
+    draws = W.draw_batch(args.beams)
+    if args.nodes:
+        draws = [W.BeamDraw(d.model_id, args.nodes, d.length, d.amp, d.freq) for d in draws]
     models = [OracleModel(W.batch_cantilever_model(d).pack()) for d in draws]
     params = W.batch_params()
     amp = [d.amp for d in draws]
     freq = [d.freq for d in draws]
-    # warm-up steps, then K timed steps; each step advances the sample one step
-    for _ in range(args.warmup):
-        run_batch(models, params, 1, amp, freq, threads)
-    total_conv, total_secs, lat = 0, 0.0, []
-    for _ in range(args.steps):
-        conv, secs, _ = run_batch(models, params, 1, amp, freq, threads)
-        total_conv += conv
+    for k in range(args.warmup):
+        run_batch_record(models, params, k, 1, amp, freq, threads)
+    total_conv, total_secs, lat, iters = 0, 0.0, [], 0
+    for j in range(args.steps):
+        st, it, secs = run_batch_record(models, params, args.warmup + j, 1, amp, freq, threads)
+        total_conv += int((st == 0).sum())
+        iters += int(it.sum())
         total_secs += secs
         lat.append(secs * 1e3)
     value = total_conv / total_secs
@@ -179,11 +182,18 @@ def run_reference(args) -> None:
         "unit": "beam-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_secs * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"4096-beam batch, sample of {sample} beams per step (CPU)",
-                   "beams": sample, "h": 0.01},
+        "config": {"workload": (f"{args.beams}-beam batch of uneven cantilevers (nodes U{{5..21}}, "
+                                "Gauss nodes+2, L U(5,100) m, tip A sin(2 pi f t)), every beam "
+                                "one time step per bench step (CPU)"),
+                   "beams_per_gpu": args.beams, "h": 0.01, "rho_inf": 0.9,
+                   "max_iter": params.max_iter, "a_tol": 1e-7, "r_tol": 1e-3,
+                   "precision": "plain FP64", "same_config": True},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "converged_fraction": total_conv / (args.steps * len(models)),
+        "newton_iters_per_beam_step": iters / (args.steps * len(models)),
         "cpu_baseline": {"value": value, "unit": "beam-steps/s", "cores": threads, "kind": "port",
-                         "sample": f"{sample} beams x {args.steps} steps"},
+                         "sample": f"the whole {len(models)}-beam batch x {args.steps} timed steps "
+                                   f"after {args.warmup} warm-up steps"},
         "e2e": {"value": value, "unit": "beam-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -197,9 +207,10 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--beams", type=int, default=4096)
-    ap.add_argument("--ref-sample", type=int, default=512)
     ap.add_argument("--cpu-sample", type=int, default=1024)
     ap.add_argument("--cpu-steps", type=int, default=150)
+    ap.add_argument("--oracle-sample", type=int, default=512,
+                    help="beams of the EI-swept batch run on the FP64 oracle for the accuracy leg")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32 + refinement form")
     ap.add_argument("--no-graph", action="store_true", help="launch steps directly (no CUDA graph)")
@@ -210,6 +221,9 @@ def main() -> None:
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="request arrivals per second")
     ap.add_argument("--refine", type=int, default=0,
                     help="refinement corrections of the FP32 form after convergence")
+    ap.add_argument("--solver", type=int, default=1,
+                    help="free-block solve of the headline legs: 1 panel LU (default), 0 Gauss-Jordan "
+                         "in registers (panel LU where the block does not fit)")
     ap.add_argument("--nodes", type=int, default=0,
                     help="uniform nodes per beam (0: the batch's U{5..21}); for profiling one bucket")
     args = ap.parse_args()
@@ -238,6 +252,7 @@ def main() -> None:
     if args.nodes:
         draws = [W.BeamDraw(d.model_id, args.nodes, d.length, d.amp, d.freq) for d in draws]
     ctx = Context(local)
+    ctx.set_linear_solver(args.solver)
     if not args.no_graph:
         ctx.set_cuda_graph(True)   # each step replays the captured bucket launches
     t_setup = time.perf_counter()
@@ -335,71 +350,135 @@ def main() -> None:
     conv_all = int(S.sum_over_ranks(conv_v, dist, dev))
     value = conv_all / (t_value_ms * 1e-3)
 
-    # ---- the FP32 + refinement form on its own copy of the batch ---------------
+    # ---- the FP32 forms on their own copies of the batch ------------------------
+    # (a) FP32 tangent and panel LU; (b) FP32 tangent, FP32 Gauss-Jordan inverse
+    # and FP64-residual refinement of every Newton correction to a 1e-10
+    # backward error.  Both keep the FP64 residual, convergence test and update.
     prec = None
     if not args.no_fp32:
-        ids32 = np.array([ctx.create_model(W.batch_cantilever_model(d).pack()) for d in draws],
-                         dtype=np.int32)
-        p32 = W.batch_params()
-        p32.precision, p32.refine_iters = 1, args.refine
-        tuned32 = tune(ids32, p32)
-        r32 = device_leg(ids32, p32, False)
-        t32 = S.max_over_ranks(float(sum(r32["ms"])), dist, dev)
-        v32 = S.sum_over_ranks(r32["conv"], dist, dev) / (t32 * 1e-3)
         tips = np.cumsum(nodes) - 1
-        a, b = r64["q"][tips, :3], r32["q"][tips, :3]
-        rel = np.abs(b - a).max(axis=1) / np.maximum(np.abs(a).max(axis=1), 1e-300)
-        rel = rel[r64["ok_all"] & r32["ok_all"]]   # beams converged at every step in both forms
-        prec = {"form": "FP32 tangent/LU (3xTF32 integration GEMM) + FP64 residual, update "
-                        f"and {args.refine} refinement correction(s)",
-                "value": v32, "unit": "beam-steps/s", "ratio_vs_fp64": v32 / value,
-                "threads_per_cta_by_nodes": tuned32,
-                "ms_per_step": t32 / args.steps,
-                "newton_iters_per_beam_step": r32["iters"] / (args.steps * len(ids32)),
-                "fp64_newton_iters_per_beam_step": r64["iters"] / (args.steps * len(ids)),
-                "converged_fraction": r32["conv"] / (args.steps * len(ids32)),
-                "tip_rel_err_vs_fp64": {"beams": int(rel.size), "median": float(np.median(rel)) if rel.size else None,
-                                        "p99": float(np.percentile(rel, 99)) if rel.size else None,
-                                        "max": float(rel.max()) if rel.size else None},
-                "latency_ms": {"p50": float(np.percentile(r32["ms"], 50)),
-                               "p99": float(np.percentile(r32["ms"], 99))}}
-        for i in ids32:
-            ctx.destroy_model(int(i))
 
-        # accuracy of the FP32 form on the EI-swept batch (EA/EI over three
-        # decades, conditioned tangents ~2e7..3e9): the same steps in both forms,
-        # per-beam tip-displacement and root-load errors against the FP64 form
-        # (which reproduces the FP64 oracle to 1e-10, tests/test_gpu_parity.py)
-        acc_ids = {}
-        for form in (0, 1):
-            acc_ids[form] = np.array([ctx.create_model(W.precision_cantilever_model(d).pack())
-                                      for d in draws], dtype=np.int32)
-        pa = {}
-        for form in (0, 1):
-            pp = W.batch_params()
-            pp.precision, pp.refine_iters = form, args.refine
-            pa[form] = device_leg(acc_ids[form], pp, False)
-        both = pa[0]["ok_all"] & pa[1]["ok_all"]
-        a, b = pa[0]["q"][tips, :3], pa[1]["q"][tips, :3]
-        tip_rel = (np.abs(b - a).max(axis=1) / np.maximum(np.abs(a).max(axis=1), 1e-300))[both]
-        root_rel = []
-        for i in np.flatnonzero(both):
-            la = ctx.state(int(acc_ids[0][i]), "lambda")
-            lb = ctx.state(int(acc_ids[1][i]), "lambda")
-            root_rel.append(float(np.abs(lb - la).max() / max(np.abs(la).max(), 1e-300)))
-        root_rel = np.array(root_rel)
+        def tip_rel_vs(qa, qb, ok):
+            a, b = qa[tips, :3], qb[tips, :3]
+            rel = np.abs(b - a).max(axis=1) / np.maximum(np.abs(a).max(axis=1), 1e-300)
+            return rel[ok]
 
         def stats(x):
-            return {"median": float(np.median(x)), "p99": float(np.percentile(x, 99)),
-                    "max": float(x.max())} if x.size else None
-        prec["accuracy_ei_swept_batch"] = {
-            "workload": f"{args.beams} beams of the batch with bending/torsion stiffness x 10^U(-1,2)",
-            "beams_converged_in_both": int(both.sum()),
-            "ratio_vs_fp64": (pa[1]["conv"] / sum(pa[1]["ms"])) / max(pa[0]["conv"] / sum(pa[0]["ms"]), 1e-300),
-            "tip_rel_err_vs_fp64": stats(tip_rel),
-            "root_load_rel_err_vs_fp64": stats(root_rel)}
-        for form in (0, 1):
-            for i in acc_ids[form]:
+            x = np.asarray(x)
+            return {"beams": int(x.size), "median": float(np.median(x)),
+                    "p99": float(np.percentile(x, 99)), "max": float(x.max())} if x.size else None
+
+        def fp32_leg(solver):
+            ids32 = np.array([ctx.create_model(W.batch_cantilever_model(d).pack()) for d in draws],
+                             dtype=np.int32)
+            p32 = W.batch_params()
+            p32.precision, p32.refine_iters = 1, args.refine
+            ctx.set_linear_solver(solver)
+            tuned32 = tune(ids32, p32)
+            ctx.reset_solve_stats()
+            before = ctx.solve_stats()
+            r32 = device_leg(ids32, p32, False)
+            after = ctx.solve_stats()
+            ctx.set_linear_solver(args.solver)
+            t32 = S.max_over_ranks(float(sum(r32["ms"])), dist, dev)
+            v32 = S.sum_over_ranks(r32["conv"], dist, dev) / (t32 * 1e-3)
+            solves = after["checked"] - before["checked"]
+            out = {"value": v32, "unit": "beam-steps/s", "ratio_vs_fp64": v32 / value,
+                   "threads_per_cta_by_nodes": tuned32,
+                   "ms_per_step": t32 / args.steps,
+                   "newton_iters_per_beam_step": r32["iters"] / (args.steps * len(ids32)),
+                   "fp64_newton_iters_per_beam_step": r64["iters"] / (args.steps * len(ids)),
+                   "converged_fraction": r32["conv"] / (args.steps * len(ids32)),
+                   "tip_rel_err_vs_fp64_form": stats(tip_rel_vs(r64["q"], r32["q"],
+                                                                r64["ok_all"] & r32["ok_all"])),
+                   "latency_ms": {"p50": float(np.percentile(r32["ms"], 50)),
+                                  "p99": float(np.percentile(r32["ms"], 99))}}
+            if solves:
+                out["refinement"] = {
+                    "solves": solves,
+                    "sweeps_per_solve": (after["refine_sweeps"] - before["refine_sweeps"]) / solves,
+                    "solves_above_1e-10_after_8_sweeps": after["refine_short"] - before["refine_short"],
+                    "largest_backward_error": after["max_backward_error"]}
+            for i in ids32:
+                ctx.destroy_model(int(i))
+            return out
+
+        prec = {"form": "FP32 tangent (3xTF32 integration GEMM) and FP32 panel LU (pivot chains FP32, "
+                        "trailing updates on FP64 tensor cores), FP64 residual, convergence test and "
+                        "rotation update"
+                        + (f", {args.refine} extra Newton correction(s) after convergence"
+                           if args.refine else "")}
+        prec.update(fp32_leg(1))
+        prec["refined"] = {"form": "FP32 tangent, FP32 Gauss-Jordan inverse of the free block in "
+                                   "registers, every Newton correction refined with FP64 residuals "
+                                   "of the assembled system to a 1e-10 backward error (at most 8 "
+                                   "sweeps)"}
+        prec["refined"].update(fp32_leg(0))
+
+        # accuracy on the EI-swept batch (bending/torsion stiffness x 10^U(-1,2),
+        # conditioned tangents ~2e7..3e9): the same steps in every form, per-beam
+        # tip-displacement and root-load errors against the FP64 oracle on a
+        # sample, and against the FP64 form on every beam; the FP64 Gauss-Jordan
+        # leg measures the backward error of every unpivoted solve
+        forms = {"fp64": (0, 1), "fp32": (1, 1), "fp32_refined": (1, 0), "fp64_gauss_jordan": (0, 0)}
+        acc_ids, pa, guard = {}, {}, None
+        for name, (form, solver) in forms.items():
+            acc_ids[name] = np.array([ctx.create_model(W.precision_cantilever_model(d).pack())
+                                      for d in draws], dtype=np.int32)
+            pp = W.batch_params()
+            pp.precision, pp.refine_iters = form, args.refine
+            ctx.set_linear_solver(solver)
+            ctx.reset_solve_stats()
+            before = ctx.solve_stats()
+            pa[name] = device_leg(acc_ids[name], pp, False)
+            after = ctx.solve_stats()
+            if name == "fp64_gauss_jordan":
+                guard = {"solves": after["checked"] - before["checked"],
+                         "backward_error_above_1e-10": after["guard_trips"] - before["guard_trips"],
+                         "largest_backward_error": after["max_backward_error"]}
+        ctx.set_linear_solver(args.solver)
+
+        def root_err(la, lb):
+            return float(np.abs(lb - la).max() / max(np.abs(la).max(), 1e-300))
+
+        ns = min(args.oracle_sample, len(draws))
+        vs_oracle = None
+        if ns > 0:
+            from oracle.oracle_py import OracleModel, run_batch_record
+            orcs = [OracleModel(W.precision_cantilever_model(d).pack()) for d in draws[:ns]]
+            ost, _, osecs = run_batch_record(orcs, W.batch_params(), 0, args.warmup + args.steps,
+                                             [d.amp for d in draws[:ns]], [d.freq for d in draws[:ns]],
+                                             os.cpu_count() or 1)
+            oracle_ok = (ost == 0).all(axis=1)
+            row0 = np.concatenate([[0], np.cumsum(nodes)[:-1]])
+            vs_oracle = {}
+            for name in forms:
+                okf = oracle_ok & pa[name]["ok_all"][:ns]
+                te, re_ = [], []
+                for i in np.flatnonzero(okf):
+                    oq = orcs[i].state("q")
+                    gq = pa[name]["q"][row0[i]:row0[i] + nodes[i]]
+                    te.append(np.abs(gq[-1, :3] - oq[-1, :3]).max() / max(np.abs(oq[-1, :3]).max(), 1e-300))
+                    re_.append(root_err(orcs[i].state("lambda"),
+                                        ctx.state(int(acc_ids[name][i]), "lambda")))
+                vs_oracle[name] = {"tip_rel_err": stats(te), "root_load_rel_err": stats(re_)}
+            vs_oracle["sample"] = (f"first {ns} beams, {args.warmup + args.steps} steps, beams "
+                                   f"converged at every step in the oracle and the form "
+                                   f"(oracle: {osecs:.1f} s on {os.cpu_count()} threads)")
+        acc = {"workload": f"{args.beams} beams of the batch with bending/torsion stiffness x 10^U(-1,2)",
+               "vs_fp64_oracle": vs_oracle, "fp64_gauss_jordan_backward_error": guard}
+        for name in ("fp32", "fp32_refined"):
+            both = pa["fp64"]["ok_all"] & pa[name]["ok_all"]
+            rr = [root_err(ctx.state(int(acc_ids["fp64"][i]), "lambda"),
+                           ctx.state(int(acc_ids[name][i]), "lambda")) for i in np.flatnonzero(both)]
+            acc[name] = {"beams_converged_in_both": int(both.sum()),
+                         "ratio_vs_fp64": ((pa[name]["conv"] / sum(pa[name]["ms"])) /
+                                           max(pa["fp64"]["conv"] / sum(pa["fp64"]["ms"]), 1e-300)),
+                         "tip_rel_err_vs_fp64_form": stats(tip_rel_vs(pa["fp64"]["q"], pa[name]["q"], both)),
+                         "root_load_rel_err_vs_fp64_form": stats(rr)}
+        prec["accuracy_ei_swept_batch"] = acc
+        for name in forms:
+            for i in acc_ids[name]:
                 ctx.destroy_model(int(i))
 
     # ---- e2e: host buffers through the C ABI, wall time per step --------------
@@ -429,6 +508,7 @@ def main() -> None:
                    "hbm_budget_gb": 150}
         for name, form in (("fp64", 0), ("fp32_refined", 1)):
             sctx = Context(local, 150 * 10**9)
+            sctx.set_linear_solver(args.solver)
             sp = W.batch_params()
             sp.precision = form
             if not args.no_autotune:   # size classes of the request pool, tuned before serving
@@ -460,6 +540,10 @@ def main() -> None:
                        "beams_per_gpu": args.beams, "h": 0.01, "rho_inf": 0.9,
                        "max_iter": params.max_iter, "a_tol": 1e-7, "r_tol": 1e-3,
                        "precision": "plain FP64", "l2": "flushed (256 MB write) before each step",
+                       "linear_solver": ("Gauss-Jordan in registers (panel LU where the block "
+                                         "exceeds the register grid)" if args.solver == 0 else
+                                         "panel LU (8-column look-ahead panels, FP64 tensor-core "
+                                         "trailing updates)"),
                        "launch": "direct" if args.no_graph else "CUDA graph replay per step",
                        "threads_per_cta_by_nodes": tuned64,
                        "parallelism": f"independent beam shards x{world}"},

@@ -295,9 +295,13 @@ KYN_API int kyn_get_state_batch(kyn_ctx* ctx, const int* model_ids, int n, int f
  * device does a one-time set-up (looks up the array's device address, which
  * may load the library's device code): make it before any stream capture.
  * The array is shared by every call and context on the device and keeps the
- * last call's contents: calls that overlap in time (two host threads, or two
- * contexts' streams) race on it; serialise them.  Results equal those of
- * kyn_set_loads_batch. */
+ * last call's contents: calls that overlap on the device race on it.  A call
+ * returns before its copy kernel runs, so calls from two contexts (two streams)
+ * race even when the host makes them one after the other: order them on the
+ * device (synchronise the first stream, or make the second wait on an event
+ * recorded after the first call).  The device address found at set-up is kept
+ * for the life of the process; do not call this again on a device after
+ * cudaDeviceReset.  Results equal those of kyn_set_loads_batch. */
 KYN_API int kyn_set_loads_batch_static(kyn_ctx* ctx, const int* model_ids, int n, int which,
                                        const double* values, int on_device);
 
@@ -358,20 +362,50 @@ KYN_API int kyn_get_system_vectors(kyn_ctx* ctx, int model_id, double* rhs, doub
 enum {
     KYN_OPT_RECORD_SYSTEM = 1, /* keep the last assembled system for kyn_get_crs */
     KYN_OPT_PHASE_TIMING = 2,  /* count SM cycles per step-kernel phase (tracing) */
-    KYN_OPT_CUDA_GRAPH = 3     /* capture each model set's step launches in a CUDA
+    KYN_OPT_CUDA_GRAPH = 3,    /* capture each model set's step launches in a CUDA
                                   graph and replay it (re-captured when the model
                                   set or the step coefficients change) */
+    KYN_OPT_LINEAR_SOLVER = 4, /* KYN_SOLVER_*: how the step kernel solves a beam's
+                                  free block (default KYN_SOLVER_PANEL_LU) */
+    KYN_OPT_RESET_SOLVE_STATS = 5 /* any value: zero the KYN_STAT_SOLVES_CHECKED ..
+                                     KYN_STAT_REFINE_SHORT counters */
 };
+
+/* Free-block solves of the step kernel (the reference's sparse direct solve,
+ * src/step/solve_system.hpp:27-31, after the boundary conditions are
+ * eliminated).  Neither pivots.
+ * PANEL_LU (default): right-looking LU in shared memory, 8-column look-ahead
+ *   panels, trailing updates on the FP64 tensor cores, block back substitution.
+ * GAUSS_JORDAN: the block held in registers across the CTA, one barrier per
+ *   2x2 pivot block.  FP64 form: the backward error
+ *   max|b - A x| / (|A| |x| + |b|) of every solve is measured and counted
+ *   (KYN_STAT_SOLVES_CHECKED, _GUARD_TRIPS above 1e-10, _MAX_BACKWARD_ERROR).
+ *   FP32 form: the block is inverted in FP32 and every Newton correction is
+ *   refined with FP64 residuals of the assembled system until that backward
+ *   error is at most 1e-10 (at most 8 sweeps; KYN_STAT_REFINE_*).  Blocks
+ *   larger than the register grid of their thread count take PANEL_LU. */
+enum { KYN_SOLVER_GAUSS_JORDAN = 0, KYN_SOLVER_PANEL_LU = 1 };
 KYN_API int kyn_ctx_set_option(kyn_ctx* ctx, int option, int64_t value);
 
 /* Context counters (diagnostics; no counterpart in the reference). */
 enum {
     KYN_STAT_KERNEL_LAUNCHES = 1,  /* kernels launched by this context so far */
     KYN_STAT_STEP_BUCKETS = 2,     /* step-kernel launches of the last step call */
-    KYN_STAT_PHASE_CYCLES = 100    /* + phase (0..8): SM cycles summed over beams since
+    KYN_STAT_ALLOCATIONS = 3,      /* device (cudaMalloc, cudaMallocAsync) and pinned host
+                                      (cudaMallocHost) allocations made by this context */
+    /* Gauss-Jordan solves (KYN_SOLVER_GAUSS_JORDAN), summed since the context
+       was created or KYN_OPT_RESET_SOLVE_STATS: */
+    KYN_STAT_SOLVES_CHECKED = 4,   /* solves whose backward error was measured */
+    KYN_STAT_GUARD_TRIPS = 5,      /* FP64 solves with a backward error above 1e-10 */
+    KYN_STAT_MAX_BACKWARD_ERROR = 6, /* largest backward error seen: the bits of a double */
+    KYN_STAT_REFINE_SWEEPS = 7,    /* FP32 form: refinement sweeps taken */
+    KYN_STAT_REFINE_SHORT = 8,     /* FP32 form: solves above 1e-10 after the last sweep */
+    KYN_STAT_PHASE_CYCLES = 100    /* + phase (0..12): SM cycles summed over beams since
                                       KYN_OPT_PHASE_TIMING was set: load/predict,
                                       quadrature, integrate, constraints, eliminate,
-                                      factor, substitute, update, store */
+                                      factor, substitute, update, store, then the
+                                      panel LU's sub-phases (9..11) and the FP32
+                                      form's refinement sweeps (12) */
 };
 KYN_API int kyn_ctx_stat(kyn_ctx* ctx, int stat, int64_t* value);
 

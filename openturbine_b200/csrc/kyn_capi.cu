@@ -198,6 +198,7 @@ struct kyn_ctx {
     std::vector<int> pending;             // models of the last kyn_step_async
     int smem_configured = 0;
     bool use_graph = false;               // KYN_OPT_CUDA_GRAPH
+    int solver = KYN_SOLVER_PANEL_LU;     // KYN_OPT_LINEAR_SOLVER
     double* h_stage = nullptr;            // pinned staging for loads
     size_t h_stage_len = 0;
     std::unique_ptr<XferPlan> xfer[4];    // cached transfer plans
@@ -206,8 +207,10 @@ struct kyn_ctx {
     double* d_stage = nullptr;            // device staging for batched transfers
     size_t d_stage_len = 0;
     int64_t launches = 0;                 // kernels launched so far
+    int64_t allocations = 0;              // device and pinned allocations so far
     int64_t last_buckets = 0;
     unsigned long long* d_prof = nullptr; // phase timing counters (KYN_OPT_PHASE_TIMING)
+    unsigned long long* d_diag = nullptr; // solve counters (kDiag*, KYN_STAT_SOLVE_*)
     std::map<ClassKey, int> tuned;        // threads per CTA chosen by kyn_autotune
     // Plan buffers, grown on demand and reused by every plan (one step in
     // flight at a time), so rebuilding a plan for a changed model set (the
@@ -248,6 +251,14 @@ int set_err(kyn_ctx* c, int code, const std::string& msg) {
                            std::string(#call) + ": " + cudaGetErrorString(e_));          \
     } while (0)
 
+// A device or pinned-host allocation by the context, counted for
+// KYN_STAT_ALLOCATIONS.
+#define KYN_ALLOC(ctx, call)        \
+    do {                            \
+        (ctx)->allocations++;       \
+        KYN_CUDA(ctx, call);        \
+    } while (0)
+
 DevModel* find_model(kyn_ctx* c, int id) {
     return (id >= 0 && static_cast<size_t>(id) < c->by_id.size()) ? c->by_id[id] : nullptr;
 }
@@ -258,8 +269,13 @@ void register_model(kyn_ctx* c, int id, std::unique_ptr<DevModel> m) {
     c->models[id] = std::move(m);
 }
 
-StepCoeffs make_coeffs(const kyn_step_params* p) {
+StepCoeffs make_coeffs(const kyn_ctx* c, const kyn_step_params* p) {
     StepCoeffs P{};
+    P.solver = c->solver;
+    P.diag = c->d_diag;
+    const bool fp32 = p->precision == KYN_PRECISION_FP32_REFINED;
+    P.refine_sweeps = fp32 ? kRefineSweeps : 0;
+    P.refine_tol = fp32 ? kRefineTol : 0.;
     const double rho = p->rho_inf;
     P.h = p->h;
     P.alpha_m = (2. * rho - 1.) / (rho + 1.);
@@ -392,7 +408,7 @@ int nt_index(int nt) { return nt == 128 ? 0 : nt == 256 ? 1 : 2; }
 // (stream-ordered; the host copy m->kt stays alive with the model).
 int upload_templates(kyn_ctx* c, DevModel* m) {
     const size_t len = sizeof(KBeam) * m->kt.size();
-    KYN_CUDA(c, cudaMallocAsync(reinterpret_cast<void**>(&m->d_kt), len, c->stream));
+    KYN_ALLOC(c, cudaMallocAsync(reinterpret_cast<void**>(&m->d_kt), len, c->stream));
     KYN_CUDA(c, cudaMemcpyAsync(m->d_kt, m->kt.data(), len, cudaMemcpyHostToDevice, c->stream));
     m->bytes += len;
     c->used += len;
@@ -409,7 +425,7 @@ int grow_device(kyn_ctx* c, T*& p, size_t& cap, size_t need, size_t floor) {
     while (nc < need) nc *= 2;
     if (p) KYN_CUDA(c, cudaFreeAsync(p, c->stream));
     p = nullptr;
-    KYN_CUDA(c, cudaMallocAsync(reinterpret_cast<void**>(&p), sizeof(T) * nc, c->stream));
+    KYN_ALLOC(c, cudaMallocAsync(reinterpret_cast<void**>(&p), sizeof(T) * nc, c->stream));
     cap = nc;
     return KYN_OK;
 }
@@ -426,7 +442,7 @@ int grow_pinned(kyn_ctx* c, T*& p, size_t& cap, size_t need, size_t floor) {
         KYN_CUDA(c, cudaFreeHost(p));
     }
     p = nullptr;
-    KYN_CUDA(c, cudaMallocHost(reinterpret_cast<void**>(&p), sizeof(T) * nc));
+    KYN_ALLOC(c, cudaMallocHost(reinterpret_cast<void**>(&p), sizeof(T) * nc));
     cap = nc;
     return KYN_OK;
 }
@@ -601,7 +617,7 @@ int configure_smem(kyn_ctx* c) {
 }
 
 int launch_plan(kyn_ctx* c, Plan* plan, const kyn_step_params* p) {
-    const StepCoeffs P = make_coeffs(p);
+    const StepCoeffs P = make_coeffs(c, p);
     int rc = configure_smem(c);
     if (rc != KYN_OK) return rc;
     KYN_CUDA(c, cudaEventRecord(c->fork, c->stream));
@@ -804,6 +820,11 @@ kyn_ctx* kyn_ctx_create(int device, size_t hbm_budget_bytes) {
     }
     ok = ok && cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) == cudaSuccess;
     ok = ok && cudaEventCreateWithFlags(&c->plan_uploaded, cudaEventDisableTiming) == cudaSuccess;
+    if (ok) {
+        c->allocations++;
+        ok = cudaMalloc(&c->d_diag, kNumDiag * sizeof(unsigned long long)) == cudaSuccess &&
+             cudaMemset(c->d_diag, 0, kNumDiag * sizeof(unsigned long long)) == cudaSuccess;
+    }
     // Slabs come from the device's stream-ordered pool; keep freed blocks in
     // the pool instead of returning them at each synchronisation, so that
     // models created and destroyed every serving iteration reuse memory.
@@ -843,6 +864,7 @@ void kyn_ctx_destroy(kyn_ctx* c) {
     if (c->h_stage) cudaFreeHost(c->h_stage);
     for (auto& x : c->xfer) x.reset();
     if (c->d_stage) cudaFree(c->d_stage);
+    if (c->d_diag) cudaFree(c->d_diag);
     for (int i = 0; i < kBucketStreams; ++i) {
         if (c->bstream[i]) cudaStreamDestroy(c->bstream[i]);
         if (c->join[i]) cudaEventDestroy(c->join[i]);
@@ -863,6 +885,19 @@ int kyn_ctx_stat(kyn_ctx* c, int stat, int64_t* value) {
     if (!c || !value) return KYN_ERR_INVALID;
     if (stat == KYN_STAT_KERNEL_LAUNCHES) *value = c->launches;
     else if (stat == KYN_STAT_STEP_BUCKETS) *value = c->last_buckets;
+    else if (stat == KYN_STAT_ALLOCATIONS) *value = c->allocations;
+    else if (stat >= KYN_STAT_SOLVES_CHECKED && stat <= KYN_STAT_REFINE_SHORT) {
+        static_assert(KYN_STAT_GUARD_TRIPS - KYN_STAT_SOLVES_CHECKED == kDiagGuardTrips &&
+                          KYN_STAT_MAX_BACKWARD_ERROR - KYN_STAT_SOLVES_CHECKED == kDiagMaxBackwardError &&
+                          KYN_STAT_REFINE_SWEEPS - KYN_STAT_SOLVES_CHECKED == kDiagRefineSweeps &&
+                          KYN_STAT_REFINE_SHORT - KYN_STAT_SOLVES_CHECKED == kDiagRefineShort,
+                      "KYN_STAT_SOLVE* follow kDiag*");
+        unsigned long long v = 0;
+        KYN_CUDA(c, cudaStreamSynchronize(c->stream));
+        KYN_CUDA(c, cudaMemcpy(&v, c->d_diag + (stat - KYN_STAT_SOLVES_CHECKED), sizeof(v),
+                               cudaMemcpyDeviceToHost));
+        *value = static_cast<int64_t>(v);
+    }
     else if (stat >= KYN_STAT_PHASE_CYCLES && stat < KYN_STAT_PHASE_CYCLES + kNumPhases) {
         if (!c->d_prof) return set_err(c, KYN_ERR_INVALID, "KYN_OPT_PHASE_TIMING is not set");
         unsigned long long v = 0;
@@ -889,11 +924,21 @@ int kyn_ctx_set_option(kyn_ctx* c, int option, int64_t value) {
                     m->dump_off.push_back(tot);
                     tot += nl * nl + 2 * nl;
                 }
-                KYN_CUDA(c, cudaMalloc(&m->d_dump, tot * sizeof(double)));
+                KYN_ALLOC(c, cudaMalloc(&m->d_dump, tot * sizeof(double)));
                 KYN_CUDA(c, cudaMemset(m->d_dump, 0, tot * sizeof(double)));
             }
         }
         c->plan.reset();
+        return KYN_OK;
+    }
+    if (option == KYN_OPT_RESET_SOLVE_STATS) {
+        KYN_CUDA(c, cudaMemsetAsync(c->d_diag, 0, kNumDiag * sizeof(unsigned long long), c->stream));
+        return KYN_OK;
+    }
+    if (option == KYN_OPT_LINEAR_SOLVER) {
+        if (value != KYN_SOLVER_GAUSS_JORDAN && value != KYN_SOLVER_PANEL_LU)
+            return set_err(c, KYN_ERR_INVALID, "unknown linear solver");
+        c->solver = static_cast<int>(value);
         return KYN_OK;
     }
     if (option == KYN_OPT_CUDA_GRAPH) {
@@ -904,7 +949,7 @@ int kyn_ctx_set_option(kyn_ctx* c, int option, int64_t value) {
     if (option == KYN_OPT_PHASE_TIMING) {
         KYN_CUDA(c, cudaStreamSynchronize(c->stream));
         if (value && !c->d_prof) {
-            KYN_CUDA(c, cudaMalloc(&c->d_prof, 16 * sizeof(unsigned long long)));
+            KYN_ALLOC(c, cudaMalloc(&c->d_prof, 16 * sizeof(unsigned long long)));
         }
         if (c->d_prof) KYN_CUDA(c, cudaMemset(c->d_prof, 0, 16 * sizeof(unsigned long long)));
         if (!value && c->d_prof) {
@@ -940,12 +985,12 @@ int kyn_model_create(kyn_ctx* c, const kyn_model_desc* desc) {
         return set_err(c, KYN_ERR_BUDGET, "HBM budget exceeded");
     for (auto& b : m->host.beams) {
         double* p = nullptr;
-        KYN_CUDA(c, cudaMallocAsync(&p, b.slab.size() * sizeof(double), c->stream));
+        KYN_ALLOC(c, cudaMallocAsync(&p, b.slab.size() * sizeof(double), c->stream));
         KYN_CUDA(c, cudaMemcpyAsync(p, b.slab.data(), b.slab.size() * sizeof(double),
                                     cudaMemcpyHostToDevice, c->stream));
         m->d_slab.push_back(p);
     }
-    KYN_CUDA(c, cudaMallocAsync(&m->d_conv, kMaxNewtonIters * sizeof(double), c->stream));
+    KYN_ALLOC(c, cudaMallocAsync(&m->d_conv, kMaxNewtonIters * sizeof(double), c->stream));
     KYN_CUDA(c, cudaMemsetAsync(m->d_conv, 0, kMaxNewtonIters * sizeof(double), c->stream));
     if (c->record) {
         size_t tot = 0;
@@ -954,7 +999,7 @@ int kyn_model_create(kyn_ctx* c, const kyn_model_desc* desc) {
             m->dump_off.push_back(tot);
             tot += nl * nl + 2 * nl;
         }
-        KYN_CUDA(c, cudaMallocAsync(&m->d_dump, tot * sizeof(double), c->stream));
+        KYN_ALLOC(c, cudaMallocAsync(&m->d_dump, tot * sizeof(double), c->stream));
         KYN_CUDA(c, cudaMemsetAsync(m->d_dump, 0, tot * sizeof(double), c->stream));
     }
     // Stream-ordered: the uploads (from the model's own host copy, which it
@@ -1065,7 +1110,7 @@ int kyn_model_set_loads(kyn_ctx* c, int id, int which, const double* values) {
             KYN_CUDA(c, cudaStreamSynchronize(c->stream));
             cudaFreeHost(c->h_stage);
         }
-        KYN_CUDA(c, cudaMallocHost(&c->h_stage, need * sizeof(double)));
+        KYN_ALLOC(c, cudaMallocHost(&c->h_stage, need * sizeof(double)));
         c->h_stage_len = need;
     }
     KYN_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -1148,7 +1193,7 @@ int kyn_step_async(kyn_ctx* c, const int* ids, int n, const kyn_step_params* p) 
     if (!c->use_graph) return launch_plan(c, plan, p);
     // CUDA graph: capture the step's launch sequence (fork, bucket kernels,
     // join, status copies) once per plan and coefficient set, then replay it.
-    const StepCoeffs P = make_coeffs(p);
+    const StepCoeffs P = make_coeffs(c, p);
     if (!plan->graph || std::memcmp(&P, &plan->graph_coeffs, sizeof(P)) != 0) {
         rc = configure_smem(c);
         if (rc != KYN_OK) return rc;
@@ -1647,11 +1692,11 @@ int clone_model(kyn_ctx* c, int id) {
     for (size_t bi = 0; bi < m->host.beams.size(); ++bi) {
         double* p = nullptr;
         const size_t len = m->host.beams[bi].slab.size() * sizeof(double);
-        KYN_CUDA(c, cudaMallocAsync(&p, len, c->stream));
+        KYN_ALLOC(c, cudaMallocAsync(&p, len, c->stream));
         KYN_CUDA(c, cudaMemcpyAsync(p, src->d_slab[bi], len, cudaMemcpyDeviceToDevice, c->stream));
         m->d_slab.push_back(p);
     }
-    KYN_CUDA(c, cudaMallocAsync(&m->d_conv, kMaxNewtonIters * sizeof(double), c->stream));
+    KYN_ALLOC(c, cudaMallocAsync(&m->d_conv, kMaxNewtonIters * sizeof(double), c->stream));
     KYN_CUDA(c, cudaMemcpyAsync(m->d_conv, src->d_conv, kMaxNewtonIters * sizeof(double),
                                 cudaMemcpyDeviceToDevice, c->stream));
     if (src->d_dump) {  // the recorded-system buffer, when the source has one
@@ -1661,7 +1706,7 @@ int clone_model(kyn_ctx* c, int id) {
             const size_t nl = 6 * m->host.beams[bi].N + 6 * m->host.beams[bi].nc;
             tot += nl * nl + 2 * nl;
         }
-        KYN_CUDA(c, cudaMallocAsync(&m->d_dump, tot * sizeof(double), c->stream));
+        KYN_ALLOC(c, cudaMallocAsync(&m->d_dump, tot * sizeof(double), c->stream));
         KYN_CUDA(c, cudaMemsetAsync(m->d_dump, 0, tot * sizeof(double), c->stream));
     }
     m->last_status = src->last_status;

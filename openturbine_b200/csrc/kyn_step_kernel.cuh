@@ -162,6 +162,25 @@ struct Smem {
     int ldA;
 };
 
+// Entries of one slot of the Gauss-Jordan pivot buffers for (storage bytes,
+// threads): 2 (RT * NT/16 + CT * 16) with the tile sizes GJTile below (the
+// pivot pair's column and row entries).
+__host__ __device__ constexpr int gj_slot_entries(int real_bytes, int nt) {
+    return 2 * (real_bytes == 8 ? (nt == 128 ? 7 * 8 + 4 * 16 : nt == 256 ? 6 * 16 + 6 * 16 : 4 * 32 + 8 * 16)
+                                : (nt == 128 ? 8 * 8 + 5 * 16 : nt == 256 ? 8 * 16 + 8 * 16 : 4 * 32 + 8 * 16));
+}
+
+// Bytes of the solve-phase scratch that lives in the G region (dead after the
+// integration): the two pivot-buffer slots, then FP64 vectors of n6 entries
+// (residual, second right-hand side, its solution, correction) and 4 * 16
+// doubles of reductions.
+__host__ __device__ inline int gj_vec_offset(int real_bytes, int nt) {
+    return (2 * gj_slot_entries(real_bytes, nt) * real_bytes + 15) & ~15;
+}
+__host__ __device__ inline int gj_scratch_bytes(int N, int real_bytes, int nt) {
+    return gj_vec_offset(real_bytes, nt) + 4 * 6 * N * 8 + 64 * 8;
+}
+
 // The system matrix and the quadrature scratch never live at the same time:
 // A is assembled after the quadrature phase and consumed by the solve, so the
 // two share one region.
@@ -187,7 +206,11 @@ __host__ __device__ inline Smem make_smem(int N, int Q, int nc, int real_bytes, 
     }
     // FP64 form: G in FP64, one k-step per point.  FP32 form: G in FP32 and
     // k-steps of two points (m16n8k8), so an odd Q gets one zero pad point.
-    S.G = take(4 * (real_bytes == 4 ? (Q + 1) & ~1 : Q) * 56 * real_bytes);
+    {
+        const int g_bytes = 4 * (real_bytes == 4 ? (Q + 1) & ~1 : Q) * 56 * real_bytes;
+        const int s_bytes = gj_scratch_bytes(N, real_bytes, nt);
+        S.G = take(g_bytes > s_bytes ? g_bytes : s_bytes);
+    }
     S.Fc = take(Q * 6 * 8);
     S.Fdig = take(Q * 6 * 8);
     S.phi = take(Q * N * 8);
@@ -622,6 +645,271 @@ __device__ __forceinline__ void back_substitute_blocked(const TR* A, int ldA, in
             xs[i] = static_cast<double>(acc);
         }
         __syncwarp();
+    }
+}
+
+// ---- register-resident Gauss-Jordan solve of the free block ----------------------
+// The free block A[0:m][0:m] and its right-hand-side columns are spread over a
+// (NT/16) x 16 grid of threads: thread (ri, cj) = (tid / 16, tid % 16) keeps the
+// entries (ri + a*(NT/16), cj + 16*b), a < RT, b < CT, in registers (cyclic in
+// both directions, so every thread keeps work until the last pivot).  Each
+// pivot step is one CTA barrier: every thread reads the pivot column and row
+// from a double-buffered shared-memory slot, forms the reciprocal pivot itself
+// and updates its entries; the owners of the next pivot's column and row
+// publish them into the other slot.  No single warp runs a serial panel, and
+// the triangular solves of an LU disappear (Gauss-Jordan eliminates above the
+// pivot as well), so the chain is m steps of ~one barrier each.
+// Tile sizes per (type, threads): the registers a thread can spend on the block
+// within its launch budget.  Blocks that do not fit take the panel LU.
+template <typename TR, int NT>
+struct GJTile;
+template <> struct GJTile<double, 128> { static constexpr int RT = 7, CT = 4; };
+template <> struct GJTile<double, 256> { static constexpr int RT = 6, CT = 6; };
+template <> struct GJTile<double, 512> { static constexpr int RT = 4, CT = 8; };
+template <> struct GJTile<float, 128> { static constexpr int RT = 8, CT = 5; };
+template <> struct GJTile<float, 256> { static constexpr int RT = 8, CT = 8; };
+template <> struct GJTile<float, 512> { static constexpr int RT = 4, CT = 8; };
+
+constexpr int kGJCols = 16;  // column groups of the register grid
+// Largest backward error an FP64 Gauss-Jordan solve may leave (rounding gives
+// ~n eps); above it the unpivoted elimination has lost accuracy to growth.
+constexpr double kGJBackwardErrorMax = 1e-10;
+
+template <typename TR, int NT>
+__host__ __device__ constexpr int gj_slot() {
+    return 2 * (GJTile<TR, NT>::RT * (NT / kGJCols) + GJTile<TR, NT>::CT * kGJCols);
+}
+static_assert(gj_slot<double, 128>() == gj_slot_entries(8, 128) &&
+                  gj_slot<double, 256>() == gj_slot_entries(8, 256) &&
+                  gj_slot<double, 512>() == gj_slot_entries(8, 512) &&
+                  gj_slot<float, 128>() == gj_slot_entries(4, 128) &&
+                  gj_slot<float, 256>() == gj_slot_entries(4, 256) &&
+                  gj_slot<float, 512>() == gj_slot_entries(4, 512),
+              "gj_slot_entries must follow GJTile");
+
+// Whether the free block (m rows, m + nrhs columns; INV: m x m) fits the grid.
+template <typename TR, int NT>
+__host__ __device__ inline bool gj_fits(int m, int ncols) {
+    return m <= GJTile<TR, NT>::RT * (NT / kGJCols) && ncols <= GJTile<TR, NT>::CT * kGJCols;
+}
+
+// Pair of TR values for vectorised shared-memory access.
+template <typename TR> struct Pair2;
+template <> struct Pair2<double> { using type = double2; };
+template <> struct Pair2<float> { using type = float2; };
+
+// Rank-2 update R[a][b] -= x0[a] u0[b] + x1[a] u1[b] of the column blocks
+// b >= b0 (one uniform test per column block, none per entry: padding rows and
+// columns hold zeros, so their updates change nothing).
+template <int B, typename TR, int RT, int CT>
+__device__ __forceinline__ void gj_rank2_from(TR (&R)[RT][CT], const TR (&x0)[RT], const TR (&x1)[RT],
+                                              const TR (&u0)[CT], const TR (&u1)[CT], int b0) {
+    if constexpr (B < CT) {
+        if (B >= b0) {
+#pragma unroll
+            for (int a = 0; a < RT; ++a) R[a][B] = fma(-x1[a], u1[B], fma(-x0[a], u0[B], R[a][B]));
+        }
+        gj_rank2_from<B + 1>(R, x0, x1, u0, u1, b0);
+    }
+}
+
+// Row a of R (a chosen at run time, the same in the whole warp) becomes
+// p u0 + q u1 in the column blocks b >= b0.
+template <typename TR, int RT, int CT>
+__device__ __forceinline__ void gj_set_row(TR (&R)[RT][CT], int a_sel, TR p, const TR (&u0)[CT], TR q,
+                                           const TR (&u1)[CT], int b0) {
+#pragma unroll
+    for (int a = 0; a < RT; ++a)
+        if (a == a_sel) {
+#pragma unroll
+            for (int b = 0; b < CT; ++b)
+                if (b >= b0) R[a][b] = fma(p, u0[b], q * u1[b]);
+        }
+}
+
+// Gauss-Jordan elimination without pivoting of the free block, held in R, two
+// pivots per step (2x2 pivot blocks D, inverted through their determinant), so
+// one CTA barrier serves two pivots.  Rows of a pivot pair are normalised
+// (D^-1 applied), so on exit the block is the identity:
+//   INV = false (solve): columns [0, m + nrhs) are loaded (only column blocks
+//     that still hold a column right of the pair are updated); on exit column
+//     m + r of row i holds x_i.
+//   INV = true (inverse): columns [0, m) are loaded and replaced in place by
+//     the inverse (pivot rows D^-1 A_K, pivot columns -A_iK D^-1, pivot block
+//     D^-1).
+// m must be even (free blocks are 6 per node).  buf: 2 slots of
+// gj_slot<TR, NT>() entries in shared memory: the pivot pair's two columns,
+// paired per row, then its two rows, paired per column; D is the pair of the
+// pivot rows.  Every thread forms D^-1 and its rows' multipliers itself; the
+// pivot rows' own update (multipliers ~ identity) is overwritten by their
+// normalisation.  The pivot pair's block indices are the same in every
+// thread, so the owners of the pivot rows and columns branch on them
+// (warp-uniform) instead of selecting among their registers.  A zero or
+// non-finite determinant sets bit 2 of *flag.
+template <typename TR, int NT, bool INV>
+__device__ __forceinline__ void gj_eliminate(const TR* A, int ldA, int m, int nrhs, TR* buf, int* flag,
+                                             TR (&R)[GJTile<TR, NT>::RT][GJTile<TR, NT>::CT]) {
+    using P2 = typename Pair2<TR>::type;
+    constexpr int RT = GJTile<TR, NT>::RT, CT = GJTile<TR, NT>::CT;
+    constexpr int PR = NT / kGJCols, PC = kGJCols;
+    constexpr int SLOT = gj_slot<TR, NT>();
+    constexpr int ROWS = 2 * RT * PR;
+    const int tid = threadIdx.x, ri = tid / PC, cj = tid % PC;
+    const int ncols = INV ? m : m + nrhs;
+#pragma unroll
+    for (int a = 0; a < RT; ++a) {
+        const int i = ri + a * PR;
+#pragma unroll
+        for (int b = 0; b < CT; ++b) {
+            const int j = cj + b * PC;
+            R[a][b] = (i < m && j < ncols) ? A[i * ldA + j] : TR(0);
+        }
+    }
+    // slot 0: columns 0, 1 and rows 0, 1; padding of both slots stays zero
+    for (int t = tid; t < 2 * SLOT; t += NT) {
+        const int e = t % SLOT;
+        TR v = TR(0);
+        if (t < SLOT) {
+            if (e < ROWS) {
+                const int i = e >> 1, h = e & 1;
+                v = (i < m) ? A[i * ldA + h] : TR(0);
+            } else {
+                const int j = (e - ROWS) >> 1, h = (e - ROWS) & 1;
+                v = (j < ncols) ? A[h * ldA + j] : TR(0);
+            }
+        }
+        buf[t] = v;
+    }
+    __syncthreads();
+    for (int k = 0; k < m; k += 2) {
+        const TR* cb = buf + ((k >> 1) & 1) * SLOT;
+        TR* nb = buf + (((k >> 1) + 1) & 1) * SLOT;
+        const P2 dA = *reinterpret_cast<const P2*>(cb + 2 * k);
+        const P2 dB = *reinterpret_cast<const P2*>(cb + 2 * k + 2);
+        const TR det = fma(dA.x, dB.y, -(dA.y * dB.x));
+        const TR rd = pivot_rcp(det);
+        if (tid == 0 && (!(fabs(det) > TR(0)) || !isfinite(rd))) atomicOr(flag, 2);
+        const TR i00 = dB.y * rd, i01 = -dA.y * rd, i10 = -dB.x * rd, i11 = dA.x * rd;
+        TR x0[RT], x1[RT], u0[CT], u1[CT];
+#pragma unroll
+        for (int a = 0; a < RT; ++a) {
+            const P2 c = *reinterpret_cast<const P2*>(cb + 2 * (ri + a * PR));
+            x0[a] = fma(c.x, i00, c.y * i10);
+            x1[a] = fma(c.x, i01, c.y * i11);
+        }
+#pragma unroll
+        for (int b = 0; b < CT; ++b) {
+            const P2 w = *reinterpret_cast<const P2*>(cb + ROWS + 2 * (cj + b * PC));
+            u0[b] = w.x;
+            u1[b] = w.y;
+        }
+        // solve form: column blocks left of b0 hold only eliminated columns
+        const int b0 = INV ? 0 : (k + 2) / PC;
+        gj_rank2_from<0>(R, x0, x1, u0, u1, b0);
+        // the pivot rows: D^-1 [row k; row k+1]
+        const int ak = k / PR;
+        const bool r0 = ri == k % PR, r1 = ri == (k + 1) % PR;
+        if (r0 || r1) gj_set_row(R, ak, r0 ? i00 : i10, u0, r0 ? i01 : i11, u1, b0);
+        if (INV) {  // the pivot columns: -A_iK D^-1, and D^-1 in the pivot rows
+            const int bk = k / PC;
+            const bool c0 = cj == k % PC, c1 = cj == (k + 1) % PC;
+            if (c0 || c1) {
+#pragma unroll
+                for (int b = 0; b < CT; ++b)
+                    if (b == bk) {
+#pragma unroll
+                        for (int a = 0; a < RT; ++a) {
+                            TR v = c0 ? -x0[a] : -x1[a];
+                            if (a == ak && r0) v = c0 ? i00 : i01;
+                            if (a == ak && r1) v = c0 ? i10 : i11;
+                            R[a][b] = v;
+                        }
+                    }
+            }
+        }
+        // publish the next pair's columns and rows
+        const int kn = k + 2;
+        if (kn < m) {
+            const int an = kn / PR, bn = kn / PC;
+            const bool c0 = cj == kn % PC, c1 = cj == (kn + 1) % PC;
+            if (c0 || c1) {
+                TR* dst = nb + 2 * ri + (c0 ? 0 : 1);
+#pragma unroll
+                for (int b = 0; b < CT; ++b)
+                    if (b == bn) {
+#pragma unroll
+                        for (int a = 0; a < RT; ++a) dst[2 * a * PR] = R[a][b];
+                    }
+            }
+            const bool w0 = ri == kn % PR, w1 = ri == (kn + 1) % PR;
+            if (w0 || w1) {
+                TR* dst = nb + ROWS + 2 * cj + (w0 ? 0 : 1);
+#pragma unroll
+                for (int a = 0; a < RT; ++a)
+                    if (a == an) {
+#pragma unroll
+                        for (int b = 0; b < CT; ++b) dst[2 * b * PC] = R[a][b];
+                    }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Column `col` (col >= m) of the register grid after the solve form: the
+// solution for that right-hand side, into out[0:m].
+template <typename TR, int NT, typename Out>
+__device__ __forceinline__ void gj_extract(const TR (&R)[GJTile<TR, NT>::RT][GJTile<TR, NT>::CT], int m,
+                                           int col, Out* out) {
+    constexpr int RT = GJTile<TR, NT>::RT, CT = GJTile<TR, NT>::CT;
+    constexpr int PR = NT / kGJCols, PC = kGJCols;
+    const int tid = threadIdx.x, ri = tid / PC, cj = tid % PC;
+    if (cj != col % PC) return;
+    const int bc = col / PC;
+#pragma unroll
+    for (int b = 0; b < CT; ++b)
+        if (b == bc) {
+#pragma unroll
+            for (int a = 0; a < RT; ++a) {
+                const int i = ri + a * PR;
+                if (i < m) out[i] = static_cast<Out>(R[a][b]);
+            }
+        }
+}
+
+// y = M v for the free block, with M either the register grid (from_regs) or
+// the block in shared memory (A, FP64 accumulation in both); v, y in FP64
+// shared memory.  With `bvec`, y = bvec - M v and amax gets max |y| (lane 0 of
+// each row group, reduced by the caller).  The 16 threads of a row group sit
+// in one half-warp and sum their columns by shuffles.
+template <typename TR, int NT, bool from_regs>
+__device__ __forceinline__ void gj_matvec(const TR (&R)[GJTile<TR, NT>::RT][GJTile<TR, NT>::CT], const TR* A,
+                                          int ldA, int m, const double* v, const double* bvec, double* y,
+                                          double& amax) {
+    constexpr int RT = GJTile<TR, NT>::RT, CT = GJTile<TR, NT>::CT;
+    constexpr int PR = NT / kGJCols, PC = kGJCols;
+    const int tid = threadIdx.x, ri = tid / PC, cj = tid % PC;
+    amax = 0.;
+#pragma unroll
+    for (int a = 0; a < RT; ++a) {
+        const int i = ri + a * PR;
+        if (a * PR >= m) break;  // uniform: no row of this block is in range
+        double acc = 0.;
+#pragma unroll
+        for (int b = 0; b < CT; ++b) {
+            const int j = cj + b * PC;
+            if (j < m && i < m) {
+                const double mij = from_regs ? static_cast<double>(R[a][b]) : static_cast<double>(A[i * ldA + j]);
+                acc = fma(mij, v[j], acc);
+            }
+        }
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (cj == 0 && i < m) {
+            const double val = bvec ? bvec[i] - acc : acc;
+            y[i] = val;
+            amax = fmax(amax, fabs(val));
+        }
     }
 }
 
@@ -2155,8 +2443,14 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
             for (int k = 0; k < 3; ++k) xs[pr + 3 + k] = y[k];
         }
         __syncthreads();
-        // (S2) free-row right-hand side, folded into column m of A; a drive
-        //      train adds the second right-hand side -A_fr d_r in column m + 1
+        // (S2) free-row right-hand side, folded into column m of A (and kept in
+        //      FP64 in bp[0:m]); a drive train adds the second right-hand side
+        //      -A_fr d_r in column m + 1 (FP64 copy in rhs2)
+        double* gjv = reinterpret_cast<double*>(smem_raw + S.G + gj_vec_offset(sizeof(TR), NT));
+        double* r64 = gjv;                 // [n6] residual of the linear solve
+        double* rhs2 = gjv + n6;           // [n6] second right-hand side (drive train)
+        double* x2 = gjv + 2 * n6;         // [n6] its solution
+        double* red4 = gjv + 4 * n6;       // [64] reductions of the refinement
         for (int i = tid; i < m; i += NT) {
             double r = bp[i], r2 = 0.;
             for (int j = m; j < n6; ++j) {
@@ -2164,70 +2458,212 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
                 if (drive) r2 -= static_cast<double>(A[i * ldA + j]) * rpiv[j];
             }
             A[i * ldA + m] = static_cast<TR>(r);
-            if (drive) A[i * ldA + m + 1] = static_cast<TR>(r2);
+            bp[i] = r;
+            if (drive) {
+                A[i * ldA + m + 1] = static_cast<TR>(r2);
+                rhs2[i] = r2;
+            }
         }
         __syncthreads();
         mark(kPhaseEliminate);
-        // (S3) LU without pivoting of the free block A[0:m][0:m]; the right-hand
-        //      side in column m is eliminated with it.  Right-looking, panels of
-        //      kPanel columns, two CTA barriers per panel:
-        //      phase 1 - warp 0 applies panel k to the next panel's diagonal rows
-        //                (its U12 tile goes to a stage) and factors the next
-        //                diagonal block; the other warps apply panel k to the rows
-        //                below it and to every other column tile;
-        //      phase 2 - the stage is copied into A and all threads solve the next
-        //                panel's L21 rows (one row per thread).
-        //      Multipliers are stored scaled; rpiv keeps the reciprocal pivots.
-        if (m > 0) {
-            if (warp == 0) factor_diag(A, ldA, m, 0, rpiv, lane, &s_flag);
-            __syncthreads();
-            solve_l21(A, ldA, m, 0, rpiv, min(kPanel, m), tid, NT);
-            __syncthreads();
-            for (int k0 = 0; k0 < m; k0 += kPanel) {
-                const int kb = min(kPanel, m - k0);
-                const int r0 = k0 + kb;
-                const int nct = (m + 1 - r0 + 7) / 8;  // column tiles of [r0, m], rhs included
-                const int top = min(r0 + kPanel, m);   // rows of the next diagonal block
-                if (warp == 0) {
-                    update_tile<kU12ToStage>(A, ldA, m, k0, kb, r0, r0, top, stage, lane);
-                    mark(kPhaseLUDiag);
-                    if (r0 < m) {
-                        __syncwarp();
-                        factor_diag(A, ldA, m, r0, rpiv, lane, &s_flag);
-                    }
-                    mark(kPhaseLUPanel);
-                } else {
-                    // unit 0: tile 0 below the next diagonal block; unit u >= 1: tile u
-                    for (int u = warp - 1; u < nct; u += NW - 1) {
-                        if (u == 0) {
-                            if (top < m)
-                                update_tile<kU12InRegs>(A, ldA, m, k0, kb, r0, top, m, nullptr, lane);
-                        } else {
-                            update_tile<kU12InPlace>(A, ldA, m, k0, kb, r0 + 8 * u, r0, m, nullptr, lane);
+        // (S3) the free block: Gauss-Jordan in registers where it fits the grid
+        //      (FP64 form: solve; FP32 form: inverse, then FP64-residual
+        //      refinement), else the panel LU.  x1 -> xs[0:m], x2 -> x2[0:m].
+        constexpr bool kInv = sizeof(TR) == 4;
+        const int nrhs = drive ? 2 : 1;
+        const bool use_gj = P.solver == KYN_SOLVER_GAUSS_JORDAN && m > 0 && (m & 1) == 0 &&
+                            gj_fits<TR, NT>(m, kInv ? m : m + nrhs);
+        if (use_gj) {
+            TR R[GJTile<TR, NT>::RT][GJTile<TR, NT>::CT];
+            gj_eliminate<TR, NT, kInv>(A, ldA, m, nrhs, reinterpret_cast<TR*>(smem_raw + S.G), &s_flag, R);
+            mark(kPhaseFactor);
+            // Backward error of a solve: max|b - A x| / (||A|| ||x|| + ||b||),
+            // infinity norms, FP64, A as assembled (its FP32 rounding in the
+            // FP32 form).  Returns the same value in every thread.
+            auto backward_error = [&](const double* x, const double* b, double* res) -> double {
+                double ra = 0., xa = 0., ba = 0., aa = 0.;
+                constexpr int PR = NT / kGJCols;
+                const int ri = tid / kGJCols, cj = tid % kGJCols;
+#pragma unroll
+                for (int a = 0; a < GJTile<TR, NT>::RT; ++a) {
+                    const int i = ri + a * PR;
+                    if (a * PR >= m) break;
+                    double acc = 0., asum = 0.;
+#pragma unroll
+                    for (int bb = 0; bb < GJTile<TR, NT>::CT; ++bb) {
+                        const int j = cj + bb * kGJCols;
+                        if (j < m && i < m) {
+                            const double aij = static_cast<double>(A[i * ldA + j]);
+                            acc = fma(aij, x[j], acc);
+                            asum += fabs(aij);
+                            if (a == 0) xa = fmax(xa, fabs(x[j]));
                         }
                     }
+#pragma unroll
+                    for (int o = 8; o > 0; o >>= 1) {
+                        acc += __shfl_xor_sync(0xffffffffu, acc, o);
+                        asum += __shfl_xor_sync(0xffffffffu, asum, o);
+                    }
+                    if (i < m) {
+                        const double rv = b[i] - acc;
+                        if (cj == 0) res[i] = rv;
+                        ra = fmax(ra, fabs(rv));
+                        ba = fmax(ba, fabs(b[i]));
+                        aa = fmax(aa, asum);
+                    }
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    ra = fmax(ra, __shfl_xor_sync(0xffffffffu, ra, o));
+                    xa = fmax(xa, __shfl_xor_sync(0xffffffffu, xa, o));
+                    ba = fmax(ba, __shfl_xor_sync(0xffffffffu, ba, o));
+                    aa = fmax(aa, __shfl_xor_sync(0xffffffffu, aa, o));
+                }
+                if (lane == 0) {
+                    red4[4 * warp] = ra;
+                    red4[4 * warp + 1] = xa;
+                    red4[4 * warp + 2] = ba;
+                    red4[4 * warp + 3] = aa;
                 }
                 __syncthreads();
-                mark(kPhaseFactor);
-                if (tid < 64) {  // tile 0 of U12 (rows k0+1 .. k0+kb-1) from the stage
-                    const int j = tid >> 3, c = r0 + (tid & 7);
-                    if (j >= 1 && j < kb && c <= m) A[(k0 + j) * ldA + c] = static_cast<TR>(stage[tid]);
+                ra = xa = ba = aa = 0.;
+                for (int w2 = 0; w2 < NW; ++w2) {
+                    ra = fmax(ra, red4[4 * w2]);
+                    xa = fmax(xa, red4[4 * w2 + 1]);
+                    ba = fmax(ba, red4[4 * w2 + 2]);
+                    aa = fmax(aa, red4[4 * w2 + 3]);
                 }
-                if (top < m) solve_l21(A, ldA, m, r0, rpiv, top, tid, NT);
+                __syncthreads();  // red4 is reused by the next call
+                const double den = aa * xa + ba;
+                return den > 0. ? ra / den : 0.;
+            };
+            if constexpr (!kInv) {
+                gj_extract<TR, NT>(R, m, m, xs);
+                if (drive) gj_extract<TR, NT>(R, m, m + 1, x2);
                 __syncthreads();
-                mark(kPhaseIntEpilogue);
+                // guard of the unpivoted elimination: the backward error of the
+                // solve, counted (checked, above kGJBackwardErrorMax, largest)
+                for (int rhs = 0; rhs < nrhs; ++rhs) {
+                    const double eta = backward_error(rhs ? x2 : xs, rhs ? rhs2 : bp, r64);
+                    if (tid == 0 && P.diag) {
+                        atomicAdd(P.diag + kDiagChecked, 1ull);
+                        if (!(eta <= kGJBackwardErrorMax)) atomicAdd(P.diag + kDiagGuardTrips, 1ull);
+                        if (eta == eta)
+                            atomicMax(P.diag + kDiagMaxBackwardError,
+                                      static_cast<unsigned long long>(__double_as_longlong(eta)));
+                    }
+                }
+            } else {
+                // FP32 inverse in R; x = R b, then sweeps x += R (b - A x) with
+                // the residual in FP64 until its backward error is at most
+                // refine_tol (or refine_sweeps sweeps)
+                for (int rhs = 0; rhs < nrhs; ++rhs) {
+                    double* x = rhs ? x2 : xs;
+                    const double* b = rhs ? rhs2 : bp;
+                    double amax;
+                    gj_matvec<TR, NT, true>(R, A, ldA, m, b, nullptr, x, amax);
+                    __syncthreads();
+                    for (int sweep = 1;; ++sweep) {
+                        const double eta = backward_error(x, b, r64);
+                        const bool done = eta <= P.refine_tol;
+                        if (tid == 0 && P.diag) {
+                            if (done || sweep > P.refine_sweeps) {
+                                atomicAdd(P.diag + kDiagChecked, 1ull);
+                                if (eta == eta)
+                                    atomicMax(P.diag + kDiagMaxBackwardError,
+                                              static_cast<unsigned long long>(__double_as_longlong(eta)));
+                            }
+                            if (!done && sweep > P.refine_sweeps) atomicAdd(P.diag + kDiagRefineShort, 1ull);
+                            if (!done && sweep <= P.refine_sweeps) atomicAdd(P.diag + kDiagRefineSweeps, 1ull);
+                        }
+                        if (done || sweep > P.refine_sweeps) break;
+                        // x += R r: one row group's 16 threads sum their columns
+                        constexpr int PR = NT / kGJCols;
+                        const int ri = tid / kGJCols, cj = tid % kGJCols;
+#pragma unroll
+                        for (int a = 0; a < GJTile<TR, NT>::RT; ++a) {
+                            const int i = ri + a * PR;
+                            if (a * PR >= m) break;
+                            double acc = 0.;
+#pragma unroll
+                            for (int bb = 0; bb < GJTile<TR, NT>::CT; ++bb) {
+                                const int j = cj + bb * kGJCols;
+                                if (j < m) acc = fma(static_cast<double>(R[a][bb]), r64[j], acc);
+                            }
+#pragma unroll
+                            for (int o = 8; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+                            if (cj == 0 && i < m) x[i] += acc;
+                        }
+                        __syncthreads();
+                    }
+                }
+                mark(kPhaseRefine);
             }
-        }
-        // (S4) back substitution U x = y (y in column m): every warp inverts some
-        //      diagonal blocks, then warp 0 substitutes block by block.
-        if (drive) {  // second right-hand side (column m + 1) before U's blocks are inverted
-            if (warp == 0 && m > 0) solve_factored_column(A, ldA, m, m + 1, rpiv, lane);
+        } else {
+            // (S3) LU without pivoting of the free block A[0:m][0:m]; the right-hand
+            //      side in column m is eliminated with it.  Right-looking, panels of
+            //      kPanel columns, two CTA barriers per panel:
+            //      phase 1 - warp 0 applies panel k to the next panel's diagonal rows
+            //                (its U12 tile goes to a stage) and factors the next
+            //                diagonal block; the other warps apply panel k to the rows
+            //                below it and to every other column tile;
+            //      phase 2 - the stage is copied into A and all threads solve the next
+            //                panel's L21 rows (one row per thread).
+            //      Multipliers are stored scaled; rpiv keeps the reciprocal pivots.
+            if (m > 0) {
+                if (warp == 0) factor_diag(A, ldA, m, 0, rpiv, lane, &s_flag);
+                __syncthreads();
+                solve_l21(A, ldA, m, 0, rpiv, min(kPanel, m), tid, NT);
+                __syncthreads();
+                for (int k0 = 0; k0 < m; k0 += kPanel) {
+                    const int kb = min(kPanel, m - k0);
+                    const int r0 = k0 + kb;
+                    const int nct = (m + 1 - r0 + 7) / 8;  // column tiles of [r0, m], rhs included
+                    const int top = min(r0 + kPanel, m);   // rows of the next diagonal block
+                    if (warp == 0) {
+                        update_tile<kU12ToStage>(A, ldA, m, k0, kb, r0, r0, top, stage, lane);
+                        mark(kPhaseLUDiag);
+                        if (r0 < m) {
+                            __syncwarp();
+                            factor_diag(A, ldA, m, r0, rpiv, lane, &s_flag);
+                        }
+                        mark(kPhaseLUPanel);
+                    } else {
+                        // unit 0: tile 0 below the next diagonal block; unit u >= 1: tile u
+                        for (int u = warp - 1; u < nct; u += NW - 1) {
+                            if (u == 0) {
+                                if (top < m)
+                                    update_tile<kU12InRegs>(A, ldA, m, k0, kb, r0, top, m, nullptr, lane);
+                            } else {
+                                update_tile<kU12InPlace>(A, ldA, m, k0, kb, r0 + 8 * u, r0, m, nullptr, lane);
+                            }
+                        }
+                    }
+                    __syncthreads();
+                    mark(kPhaseFactor);
+                    if (tid < 64) {  // tile 0 of U12 (rows k0+1 .. k0+kb-1) from the stage
+                        const int j = tid >> 3, c = r0 + (tid & 7);
+                        if (j >= 1 && j < kb && c <= m) A[(k0 + j) * ldA + c] = static_cast<TR>(stage[tid]);
+                    }
+                    if (top < m) solve_l21(A, ldA, m, r0, rpiv, top, tid, NT);
+                    __syncthreads();
+                    mark(kPhaseIntEpilogue);
+                }
+            }
+            // (S4) back substitution U x = y (y in column m): every warp inverts some
+            //      diagonal blocks, then warp 0 substitutes block by block.
+            if (drive) {  // second right-hand side (column m + 1) before U's blocks are inverted
+                if (warp == 0 && m > 0) solve_factored_column(A, ldA, m, m + 1, rpiv, lane);
+                __syncthreads();
+            }
+            for (int b = warp; b * kPanel < m; b += NW) invert_diag_block(A, ldA, m, b * kPanel, rpiv, lane);
+            __syncthreads();
+            if (warp == 0 && m > 0) back_substitute_blocked(A, ldA, m, xs, lane);
+            __syncthreads();
+            if (drive)
+                for (int i = tid; i < m; i += NT) x2[i] = static_cast<double>(A[i * ldA + m + 1]);
             __syncthreads();
         }
-        for (int b = warp; b * kPanel < m; b += NW) invert_diag_block(A, ldA, m, b * kPanel, rpiv, lane);
-        __syncthreads();
-        if (warp == 0 && m > 0) back_substitute_blocked(A, ldA, m, xs, lane);
-        __syncthreads();
         if (drive) {
             // Shaft rotation theta: x = x1 + theta x2 (x1 = (y1, c_r), x2 = (y2, d_r)).
             // The equilibrium rows projected on the test vectors lose every
@@ -2242,7 +2678,7 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
                 for (int j = lane; j < n6; j += 32) {
                     const double arj = static_cast<double>(A[(pr + k) * ldA + j]);
                     a1 += arj * xs[j];
-                    a2 += arj * (j < m ? static_cast<double>(A[j * ldA + m + 1]) : rpiv[j]);
+                    a2 += arj * (j < m ? x2[j] : rpiv[j]);
                 }
                 for (int o = 16; o > 0; o >>= 1) {
                     a1 += __shfl_xor_sync(0xffffffffu, a1, o);
@@ -2294,7 +2730,7 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
             }
             __syncthreads();
             const double th = hb[hubsm::theta];
-            for (int i = tid; i < m; i += NT) xs[i] += th * static_cast<double>(A[i * ldA + m + 1]);
+            for (int i = tid; i < m; i += NT) xs[i] += th * x2[i];
             for (int t = tid; t < 6 * nc; t += NT) {
                 const int pr = 6 * pos[KB.con_node[t / 6]];
                 xs[pr + t % 6] += th * rpiv[pr + t % 6];

@@ -23,6 +23,8 @@ namespace kyn {
 constexpr int kMaxBeamConstraints = 8;   // FixedBC / PrescribedBC / joints per beam system
 constexpr int kMaxClusterBeams = 8;      // beams per model (portable cluster size)
 constexpr int kMaxNewtonIters = 64;      // convergence-history capacity
+constexpr int kRefineSweeps = 8;         // FP32 form: most refinement sweeps per linear solve
+constexpr double kRefineTol = 1e-10;     // FP32 form: backward error the sweeps aim for
 constexpr int kDenseModelMaxDofs = 120;  // unknowns of a model solved as a dense bordered system
 constexpr int kThreads = 256;            // threads per CTA of the step kernel
 
@@ -164,7 +166,8 @@ enum Phase {
     kPhaseLUDiag = 9,       // LU: diagonal-block factorisation (part of the factor phase)
     kPhaseLUPanel = 10,     // LU: panel solves (part of the factor phase)
     kPhaseIntEpilogue = 11, // LU: L21 rows solved by all threads (part of the factor phase)
-    kNumPhases = 12
+    kPhaseRefine = 12,      // FP32 form: FP64-residual refinement sweeps of the correction
+    kNumPhases = 13
 };
 
 // Step coefficients (src/step/step_parameters.hpp:37-52).
@@ -174,6 +177,25 @@ struct StepCoeffs {
     int32_t max_iter;
     int32_t dynamic;
     int32_t refine_iters;  // extra corrections after convergence (FP32 form)
+    int32_t solver;        // KYN_SOLVER_*: free-block solve (register Gauss-Jordan or panel LU)
+    int32_t refine_sweeps; // FP32 form: most refinement sweeps of one linear solve
+    double refine_tol;     // FP32 form: target relative FP64 residual of the linear solve
+    unsigned long long* diag;  // solve counters (kDiag*), or null
+};
+
+// Solve counters of a context (StepCoeffs::diag), summed over the beams of
+// every step: Gauss-Jordan solves whose backward error was checked, those
+// above kGJBackwardErrorMax, the largest backward error seen (bits of a
+// non-negative double, so integer max orders them), FP32 refinement sweeps
+// taken, and FP32 solves still above the refinement tolerance after the last
+// sweep.
+enum : int {
+    kDiagChecked = 0,
+    kDiagGuardTrips = 1,
+    kDiagMaxBackwardError = 2,
+    kDiagRefineSweeps = 3,
+    kDiagRefineShort = 4,
+    kNumDiag = 8
 };
 
 }  // namespace kyn

@@ -5,7 +5,9 @@
 Creates a batch of cantilevers (uniform node count, or the mixed batch with
 --nodes 0), takes two untimed steps, switches on KYN_OPT_PHASE_TIMING and
 prints the SM cycles per beam and Newton iteration of each kernel phase (one
-CTA's clock, summed over beams by the kernel).
+CTA's clock, summed over beams by the kernel).  Phase "factor" is the whole
+Gauss-Jordan elimination (--solver 0) or the panel LU's barrier wait
+(--solver 1, whose own sub-phases follow as lu_*).
 """
 from __future__ import annotations
 
@@ -15,11 +17,11 @@ import json
 import numpy as np
 
 from . import workloads as W
-from .runtime import LOAD_NODE_FX, OPT_PHASE_TIMING, Context
+from .runtime import LOAD_NODE_FX, OPT_LINEAR_SOLVER, OPT_PHASE_TIMING, Context
 
 PHASES = ["load_predict", "quadrature", "integrate_gemm", "constraints", "eliminate",
-          "lu_barrier_wait", "substitute", "update", "store", "lu_warp0_next_rows",
-          "lu_warp0_diag_factor", "lu_l21_all_threads"]
+          "factor", "substitute", "update", "store", "lu_warp0_next_rows",
+          "lu_warp0_diag_factor", "lu_l21_all_threads", "refine"]
 
 
 def main() -> None:
@@ -28,8 +30,11 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--nodes", type=int, default=13, help="0: the mixed batch (U{5..21})")
     ap.add_argument("--precision", type=int, default=0)
+    ap.add_argument("--solver", type=int, default=0,
+                    help="0: Gauss-Jordan in registers where it fits, 1: panel LU")
     args = ap.parse_args()
     ctx = Context(0)
+    ctx.lib.kyn_ctx_set_option(ctx.h, OPT_LINEAR_SOLVER, args.solver)
     draws = W.draw_batch(args.beams)
     if args.nodes:
         draws = [W.BeamDraw(d.model_id, args.nodes, d.length, d.amp, d.freq) for d in draws]
@@ -52,7 +57,8 @@ def main() -> None:
         iters += int(it.sum())
     cyc = [ctx.stat(100 + i) for i in range(len(PHASES))]
     print(json.dumps({"beams": args.beams, "nodes": args.nodes or "mixed",
-                      "precision": args.precision, "beam_iterations": iters,
+                      "precision": args.precision, "solver": args.solver,
+                      "beam_iterations": iters,
                       "cycles_per_beam_iteration": {n: round(c / max(iters, 1))
                                                     for n, c in zip(PHASES, cyc)}}))
     ctx.close()

@@ -24,7 +24,9 @@ FIELD = {"x0": 0, "x": 1, "q": 2, "q_prev": 3, "q_delta": 4, "v": 5, "vd": 6, "a
 WIDTH = {"x0": 7, "x": 7, "q": 7, "q_prev": 7, "q_delta": 6, "v": 6, "vd": 6, "a": 6, "f": 6,
          "lambda": 6, "tangent": 36, "output": 3}
 LOAD_NODE_FX, LOAD_STATE_F = 0, 1
-OPT_RECORD_SYSTEM, OPT_PHASE_TIMING, OPT_CUDA_GRAPH = 1, 2, 3
+OPT_RECORD_SYSTEM, OPT_PHASE_TIMING, OPT_CUDA_GRAPH, OPT_LINEAR_SOLVER = 1, 2, 3, 4
+OPT_RESET_SOLVE_STATS = 5
+SOLVER_GAUSS_JORDAN, SOLVER_PANEL_LU = 0, 1
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -145,6 +147,11 @@ class Context:
         """Replay each model set's step launches from a captured CUDA graph."""
         self._check(self.lib.kyn_ctx_set_option(self.h, OPT_CUDA_GRAPH, int(on)))
 
+    def set_linear_solver(self, solver: int) -> None:
+        """SOLVER_GAUSS_JORDAN (registers, default) or SOLVER_PANEL_LU for the
+        free-block solve of the step kernel."""
+        self._check(self.lib.kyn_ctx_set_option(self.h, OPT_LINEAR_SOLVER, int(solver)))
+
     def set_record_system(self, on: bool = True) -> None:
         self._check(self.lib.kyn_ctx_set_option(self.h, OPT_RECORD_SYSTEM, int(on)))
 
@@ -233,16 +240,34 @@ class Context:
     def kernel_launches(self) -> int:
         return self.stat(1)
 
+    @property
+    def allocations(self) -> int:
+        """Device and pinned-host allocations made by this context so far."""
+        return self.stat(3)
+
+    def reset_solve_stats(self) -> None:
+        self._check(self.lib.kyn_ctx_set_option(self.h, OPT_RESET_SOLVE_STATS, 1))
+
+    def solve_stats(self) -> dict:
+        """Gauss-Jordan solve counters since the context was created (backward
+        errors of FP64 solves, FP32 refinement sweeps)."""
+        import struct
+        mx = struct.unpack("<d", struct.pack("<q", self.stat(6)))[0]
+        return {"checked": self.stat(4), "guard_trips": self.stat(5), "max_backward_error": mx,
+                "refine_sweeps": self.stat(7), "refine_short": self.stat(8)}
+
     def batch_ids(self, ids) -> np.ndarray:
         return np.ascontiguousarray(ids, dtype=np.int32)
 
     def set_loads_batch(self, ids: np.ndarray, which: int, ptr: int, on_device: bool) -> None:
         """Loads for many models from one array at address `ptr` (host or device)."""
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
         self._check(self.lib.kyn_set_loads_batch(self.h, ids.ctypes.data_as(_ip), ids.shape[0],
                                                  which, ctypes.c_void_p(ptr), int(on_device)))
 
     def set_prescribed_batch(self, ids: np.ndarray, ptr: int, on_device: bool) -> None:
         """Prescribed motion [constraints of the listed models][7] from one array."""
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
         self._check(self.lib.kyn_set_prescribed_batch(self.h, ids.ctypes.data_as(_ip), ids.shape[0],
                                                       ctypes.c_void_p(ptr), int(on_device)))
 
@@ -279,11 +304,13 @@ class Context:
                                on_device: bool) -> None:
         """set_loads_batch that allocates nothing: staging in the library's fixed
         device array (limits and sharing rules in include/kynema_b200.h)."""
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
         self._check(self.lib.kyn_set_loads_batch_static(
             self.h, ids.ctypes.data_as(_ip), ids.shape[0], which, ctypes.c_void_p(ptr),
             int(on_device)))
 
     def get_state_batch(self, ids: np.ndarray, field: str, ptr: int, on_device: bool) -> None:
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
         self._check(self.lib.kyn_get_state_batch(self.h, ids.ctypes.data_as(_ip), ids.shape[0],
                                                  FIELD[field], ctypes.c_void_p(ptr),
                                                  int(on_device)))

@@ -1765,35 +1765,46 @@ int orc_get_element_terms(const orc_model* m, int e, double* residual, double* s
     return KYN_OK;
 }
 
-long orc_run_batch(orc_model** models, int n, const kyn_step_params* p, int steps,
-                   const double* amp, const double* freq, int nthreads, double* seconds,
-                   int* iters_total) {
+long orc_run_batch_record(orc_model** models, int n, const kyn_step_params* p, int first_step,
+                          int steps, const double* amp, const double* freq, int nthreads,
+                          double* seconds, int* status, int* iters_out) {
     const Params P = make_params(p);
     long converged = 0;
-    long iters = 0;
 #ifdef _OPENMP
     if (nthreads > 0) omp_set_num_threads(nthreads);
 #endif
     const auto t0 = std::chrono::steady_clock::now();
-#pragma omp parallel for schedule(dynamic, 1) reduction(+ : converged, iters)
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : converged)
     for (int i = 0; i < n; ++i) {
         orc_model& m = *models[i];
         for (int k = 0; k < steps; ++k) {
             if (amp && freq && !m.beams.empty()) {
                 OBeam& B = m.beams[0];
-                const double t = P.h * static_cast<double>(k + 1);
+                const double t = P.h * static_cast<double>(first_step + k + 1);
                 B.fx[(B.N - 1) * 6 + 2] = amp[i] * std::sin(2. * M_PI * freq[i] * t);
             }
             int it = 0;
             const int st = step_impl(m, P, &it);
-            iters += it;
+            if (status) status[static_cast<long>(i) * steps + k] = st;
+            if (iters_out) iters_out[static_cast<long>(i) * steps + k] = it;
             if (st == KYN_OK) ++converged;
         }
     }
     const auto t1 = std::chrono::steady_clock::now();
     if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
-    if (iters_total) *iters_total = static_cast<int>(iters);
     return converged;
+}
+
+long orc_run_batch(orc_model** models, int n, const kyn_step_params* p, int steps,
+                   const double* amp, const double* freq, int nthreads, double* seconds,
+                   int* iters_total) {
+    std::vector<int> it(static_cast<size_t>(n) * (steps > 0 ? steps : 0), 0);
+    const long conv = orc_run_batch_record(models, n, p, 0, steps, amp, freq, nthreads, seconds,
+                                           nullptr, it.data());
+    long total = 0;
+    for (int v : it) total += v;
+    if (iters_total) *iters_total = static_cast<int>(total);
+    return conv;
 }
 
 // ---- kernel-level entry points --------------------------------------------

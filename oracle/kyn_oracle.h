@@ -61,6 +61,14 @@ long orc_run_batch(orc_model** models, int n, const kyn_step_params* p, int step
                    const double* amp, const double* freq, int nthreads,
                    double* seconds, int* iters_total);
 
+/* The same schedule starting at time step `first_step` (the tip load of step k
+ * uses t = h (first_step + k + 1)), recording every model's status and Newton
+ * iterations per step: status[i*steps + k], iters[i*steps + k] (either may be
+ * NULL).  Returns the number of converged model-steps. */
+long orc_run_batch_record(orc_model** models, int n, const kyn_step_params* p, int first_step,
+                          int steps, const double* amp, const double* freq, int nthreads,
+                          double* seconds, int* status, int* iters);
+
 /* ---- kernel-level restatements (curved-beam and unit known-answer tests) -- */
 void orc_lagrange_interp_weights(double x, const double* xs, int n, double* w);
 void orc_lagrange_deriv_weights(double x, const double* xs, int n, double* w);

@@ -56,6 +56,10 @@ def lib():
         L.orc_run_batch.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
                                     ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.c_int,
                                     _dp, _ip]
+        L.orc_run_batch_record.restype = ctypes.c_long
+        L.orc_run_batch_record.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                                           ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp,
+                                           ctypes.c_int, _dp, _ip, _ip]
         L.orc_crs_build.restype = ctypes.c_long
         L.orc_crs_build.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _lp, _lp,
                                     ctypes.c_int, ctypes.c_int, _lp, _lp, ctypes.c_int, _lp,
@@ -160,6 +164,24 @@ def run_batch(models: list, params, steps: int, amp=None, freq=None, nthreads: i
                                _d(f) if f is not None else None, nthreads,
                                ctypes.byref(secs), ctypes.byref(iters))
     return int(conv), secs.value, iters.value
+
+
+def run_batch_record(models: list, params, first_step: int, steps: int, amp, freq,
+                     nthreads: int = 0):
+    """Advance every model `steps` steps from time step `first_step` (tip load
+    amp sin(2 pi freq t)) with OpenMP over models; returns (status, iters,
+    seconds) with status/iters of shape (models, steps)."""
+    n = len(models)
+    arr = (ctypes.c_void_p * n)(*[m.h.value for m in models])
+    secs = ctypes.c_double(0.0)
+    st = np.zeros((n, steps), dtype=np.int32)
+    it = np.zeros((n, steps), dtype=np.int32)
+    c = params.to_c()
+    a = np.ascontiguousarray(amp, dtype=np.float64)
+    f = np.ascontiguousarray(freq, dtype=np.float64)
+    lib().orc_run_batch_record(arr, n, ctypes.byref(c), first_step, steps, _d(a), _d(f), nthreads,
+                               ctypes.byref(secs), st.ctypes.data_as(_ip), it.ctypes.data_as(_ip))
+    return st, it, secs.value
 
 
 def crs_build(num_system_dofs, num_dofs, active_dofs, fmap, elem_nodes, constraints=None,

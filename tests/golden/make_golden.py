@@ -1,7 +1,8 @@
 """Extract the reference's golden vectors into JSON fixtures.
 
-Run in the build container (where the reference tree is mounted):
-    python tests/golden/make_golden.py /root/reference
+Run where the reference tree is present, giving its root directory:
+    python tests/golden/make_golden.py <reference root>
+(or set KYN_REFERENCE_ROOT instead of the argument).
 It reads the reference's own test sources as text, pulls the numeric
 literals of the named initialisers, and writes tests/golden/*.json.  The GPU
 box never reads the reference; tests use only the committed JSON.
@@ -352,4 +353,7 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("KYN_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_golden.py <reference root>  (or set KYN_REFERENCE_ROOT)")
+    main(root)

@@ -5,6 +5,7 @@ states within 1e-10 relative (max-abs difference over max-abs value of the
 field) of the FP64 oracle, and the reference's own golden tolerances.
 """
 import math
+import os
 
 import numpy as np
 import pytest
@@ -103,18 +104,32 @@ def assert_convergence_close(gpu, orc):
             assert abs(a - b) <= 1e-6 * b, (a, b)
 
 
+# Measured errors and oracle twin floors of every state comparison (in every
+# module that uses assert_state_close); tests/conftest.py writes them as JSON
+# lines to $KYN_PARITY_REPORT at the end of the session when that is set.
+REPORT: list = []
+
+
+def _test_name() -> str:
+    return os.environ.get("PYTEST_CURRENT_TEST", "?").split(" ")[0].split("::")[-1]
+
+
 def assert_state_close(ctx, mid, orc, fields=FIELDS, rel=REL, lam=True):
     """q, v, q_delta, x within `rel`; vd, a within ACCEL_REL; lambda (reaction
-    loads) within max(rel, 10 x the oracle's own noise floor) when `orc` is a
-    Twin."""
+    loads) within `rel` flat, unless the oracle's own twin floor (two FP64
+    operation orders of the same algorithm, `Twin`) is above it, then within
+    10 x that floor.  Every comparison is recorded with its floor."""
     fl = list(fields) + (["lambda"] if lam and orc.info.num_constraints else [])
     for f in fl:
         e = rel_err(ctx.state(mid, f), orc.state(f))
         tol = rel
+        floor = orc.floor(f) if isinstance(orc, Twin) else None
         if f in ACCEL:
             tol = ACCEL_REL
-        elif f not in STRICT and isinstance(orc, Twin):
-            tol = max(rel, 10.0 * orc.floor(f))
+        elif f not in STRICT and floor is not None:
+            tol = max(rel, 10.0 * floor)
+        REPORT.append({"test": _test_name(), "model": int(mid), "field": f, "err": e,
+                       "twin_floor": floor, "tol": tol})
         assert e <= tol, (f, e, tol)
 
 
@@ -247,7 +262,7 @@ def test_config_rotor_with_gravity(ctx):
     mid = ctx.create_model(pm)
     o = Twin(pm)
     p = W.rotor_params()
-    for k in range(40):
+    for k in range(1000):
         for c, u in zip(bcs, W.rotor_root_inputs(m, bcs, k)):
             ctx.set_prescribed(mid, c, u)
             o.set_prescribed(c, u)
@@ -285,6 +300,55 @@ def test_batch_uneven_cantilevers(ctx):
     assert checked >= 32
     for i in ids:
         ctx.destroy_model(i)
+
+
+def test_batch_256_beams_200_steps(ctx):
+    """The first 256 beams of the 4096-beam batch for its full 200 steps, all
+    stepped together through the batched load path; the oracle (and its twin
+    for the noise floors) advances the same beams with OpenMP over beams.
+    Statuses and iteration counts agree step by step up to each beam's first
+    non-converged step (the iterate left after max_iter is not a converged
+    state); states agree every 50 steps for the beams converged so far."""
+    from oracle.oracle_py import run_batch_record
+    from openturbine_b200.runtime import LOAD_NODE_FX
+    n, steps, every = 256, 200, 50
+    draws = W.draw_batch(n)
+    pms = [W.batch_cantilever_model(d).pack() for d in draws]
+    ids = np.array([ctx.create_model(pm) for pm in pms], dtype=np.int32)
+    orcs = [Twin(pm) for pm in pms]
+    p = W.batch_params()
+    amp = [d.amp for d in draws]
+    freq = [d.freq for d in draws]
+    nodes = np.array([d.num_nodes for d in draws])
+    tips = np.cumsum(nodes) - 1
+    fx = np.zeros((int(nodes.sum()), 6))
+    ost = np.zeros((n, steps), dtype=np.int32)
+    oit = np.zeros((n, steps), dtype=np.int32)
+    gst = np.zeros((n, steps), dtype=np.int32)
+    git = np.zeros((n, steps), dtype=np.int32)
+    checked = []
+    for k0 in range(0, steps, every):
+        seg = slice(k0, k0 + every)
+        ost[:, seg], oit[:, seg], _ = run_batch_record([o.o for o in orcs], p, k0, every, amp, freq)
+        run_batch_record([o.alt for o in orcs], p, k0, every, amp, freq)
+        for k in range(k0, k0 + every):
+            fx[tips, 2] = W.tip_loads(draws, k)
+            ctx.set_loads_batch(ids, LOAD_NODE_FX, fx.ctypes.data, False)
+            gst[:, k], git[:, k] = ctx.step(ids, p)
+        done = k0 + every
+        for i in range(n):
+            bad = np.flatnonzero(ost[i, :done] != 0)
+            last = int(bad[0]) + 1 if bad.size else done
+            assert np.array_equal(gst[i, :last], ost[i, :last]), (i, gst[i, :last], ost[i, :last])
+            assert np.array_equal(git[i, :last], oit[i, :last]), (i, git[i, :last], oit[i, :last])
+        alive = np.flatnonzero((ost[:, :done] == 0).all(axis=1))
+        for i in alive:
+            assert_state_close(ctx, int(ids[i]), orcs[i])
+        checked.append(alive.size)
+    # beams converged at every step so far, at steps 50, 100, 150, 200
+    assert checked[0] >= 128 and checked[-1] >= 64, checked
+    for i in ids:
+        ctx.destroy_model(int(i))
 
 
 def test_batched_transfers(ctx):
@@ -359,3 +423,61 @@ def test_budget_admission():
         assert e.value.code == -4
     finally:
         c.close()
+
+
+def test_gauss_jordan_and_panel_lu_agree(ctx):
+    """The two free-block solves (registers, and the panel LU that takes blocks
+    too large for the register grid) give the same Newton decisions and states
+    within the parity bar on uneven beams, in both precision forms."""
+    from openturbine_b200.runtime import SOLVER_GAUSS_JORDAN, SOLVER_PANEL_LU
+    draws = W.draw_batch(48, first_id=3000)
+    pms = [W.batch_cantilever_model(d).pack() for d in draws]
+    for precision in (0, 1):
+        ids = {s: [ctx.create_model(pm) for pm in pms] for s in (SOLVER_GAUSS_JORDAN, SOLVER_PANEL_LU)}
+        p = W.batch_params()
+        p.precision = precision
+        res = {}
+        for solver, mids in ids.items():
+            ctx.set_linear_solver(solver)
+            ctx.reset_solve_stats()
+            before = ctx.solve_stats()
+            out = []
+            for k in range(6):
+                fz = W.tip_loads(draws, k)
+                for i, d in enumerate(draws):
+                    ctx.set_node_fx(mids[i], W.node_fx_for(d, fz[i]))
+                out.append(ctx.step(mids, p))
+            res[solver] = out
+            after = ctx.solve_stats()
+            if solver == SOLVER_GAUSS_JORDAN:
+                # every Gauss-Jordan solve measured its backward error; the
+                # unpivoted FP64 solves stay at rounding level, the FP32 ones
+                # are refined below 1e-10
+                assert after["checked"] > before["checked"]
+                if precision == 0:
+                    assert after["guard_trips"] == before["guard_trips"]
+                    assert after["max_backward_error"] <= 1e-10, after
+                else:
+                    # a few corrections of heavily loaded beams stay above 1e-10
+                    # after 8 sweeps (FP32 inverse of a tangent too ill-conditioned
+                    # for FP32 refinement); they are counted, not hidden
+                    solves = after["checked"] - before["checked"]
+                    assert after["refine_sweeps"] > before["refine_sweeps"]
+                    assert after["refine_short"] - before["refine_short"] <= 0.01 * solves, after
+        ctx.set_linear_solver(SOLVER_PANEL_LU)
+        ok = np.ones(len(draws), dtype=bool)
+        for (sa, ia), (sb, ib) in zip(res[SOLVER_GAUSS_JORDAN], res[SOLVER_PANEL_LU]):
+            live = ok & (sb == 0)
+            if precision == 0:
+                assert np.array_equal(sa[ok], sb[ok]) and np.array_equal(ia[ok], ib[ok])
+            ok = live & (sa == 0)
+        assert ok.sum() >= len(draws) // 2
+        rel = REL if precision == 0 else 1e-6
+        for i in np.flatnonzero(ok):
+            for f in ("q", "v"):
+                a = ctx.state(ids[SOLVER_GAUSS_JORDAN][i], f)
+                b = ctx.state(ids[SOLVER_PANEL_LU][i], f)
+                assert rel_err(a, b) <= rel, (precision, i, f, rel_err(a, b))
+        for mids in ids.values():
+            for m in mids:
+                ctx.destroy_model(m)
