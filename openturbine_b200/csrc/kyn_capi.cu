@@ -354,7 +354,9 @@ void prepare_model(DevModel* m) {
         for (const HostBeam& hb : H.beams) {
             if (hb.dense) {  // the dense bordered system: 128 threads, FP64 in both forms
                 for (int k = 0; k < 3; ++k)
-                    m->smem_nt[f][k] = std::max(m->smem_nt[f][k], make_dense_smem(hb.N, H.ndofs).bytes);
+                    m->smem_nt[f][k] = std::max(
+                        m->smem_nt[f][k],
+                        make_dense_smem(hb.N, H.ndofs, 128 << k, hb.comp_maxN, hb.comp_maxQ).bytes);
                 continue;
             }
             m->def_nt[f] = std::max(m->def_nt[f], beam_threads(hb.N, hb.Q, hb.nc, rb, hubf));
@@ -397,6 +399,10 @@ void prepare_model(DevModel* m) {
         k.hub = static_cast<int>(H.chain.size());
         k.hub_con_type = H.hub_con_type;
         k.dense = hb.dense ? 1 : 0;
+        k.n_comps = hb.n_comps;
+        k.comps = hb.n_comps > 0 ? m->d_slab[b] + hb.comps_off : nullptr;
+        k.comp_maxN = hb.comp_maxN;
+        k.comp_maxQ = hb.comp_maxQ;
         for (int s2 = 0; s2 < kMaxBeamConstraints; ++s2) k.con_base[s2] = hb.con_base[s2];
         m->kt.push_back(k);
     }
@@ -588,8 +594,14 @@ using StepKernelFn = void (*)(const KBeam*, StepCoeffs, int, int*, int*);
 // The step kernel instance for an arithmetic form, a thread count and the
 // kernel kind (0 beams, 1 with point masses / springs / a drive train, 2 a
 // dense model, which runs in FP64 in both forms).
-StepKernelFn pick_kernel(bool fp32, int nt, int lump) {
+StepKernelFn pick_kernel(bool fp32, int nt, int lump, bool gauss_jordan = false) {
     if (lump == 2) return nt == 128 ? dense_kernel<128> : nt == 256 ? dense_kernel<256> : dense_kernel<512>;
+    if (!lump && gauss_jordan) {
+        if (fp32) return nt == 128 ? step_kernel<float, 128, false, true>
+                       : nt == 256 ? step_kernel<float, 256, false, true> : step_kernel<float, 512, false, true>;
+        return nt == 128 ? step_kernel<double, 128, false, true>
+             : nt == 256 ? step_kernel<double, 256, false, true> : step_kernel<double, 512, false, true>;
+    }
     if (lump) {
         if (fp32) return nt == 128 ? step_kernel<float, 128, true>
                        : nt == 256 ? step_kernel<float, 256, true> : step_kernel<float, 512, true>;
@@ -609,8 +621,8 @@ cudaError_t set_smem_attr(K kernel) {
 
 int configure_smem(kyn_ctx* c) {
     if (c->smem_configured < kMaxDynSmem) {
-        for (int k = 0; k < 18; ++k)
-            KYN_CUDA(c, set_smem_attr(pick_kernel(k & 1, 128 << ((k >> 1) % 3), k / 6)));
+        for (int k = 0; k < 24; ++k)
+            KYN_CUDA(c, set_smem_attr(pick_kernel(k & 1, 128 << ((k >> 1) % 3), (k / 6) % 3, k >= 18)));
         c->smem_configured = kMaxDynSmem;
     }
     return KYN_OK;
@@ -643,7 +655,8 @@ int launch_plan(kyn_ctx* c, Plan* plan, const kyn_step_params* p) {
         const KBeam* beams = plan->d_kbeams + bk.first;
         const int rec = plan->record ? 1 : 0;
         const bool fp32 = plan->precision == KYN_PRECISION_FP32_REFINED;
-        KYN_CUDA(c, cudaLaunchKernelEx(&cfg, pick_kernel(fp32, bk.nt, bk.lump), beams, P, rec,
+        KYN_CUDA(c, cudaLaunchKernelEx(&cfg, pick_kernel(fp32, bk.nt, bk.lump, P.solver == KYN_SOLVER_GAUSS_JORDAN),
+                                       beams, P, rec,
                                        plan->d_status, plan->d_iters));
         c->launches++;
     }
@@ -740,7 +753,7 @@ int get_xfer(kyn_ctx* c, const int* ids, int n, int kind, XferPlan** out) {
             xb.map_off = static_cast<int>(map.size());
             int width = 6, fo;
             if (kind == KYN_LOAD_NODE_FX) {
-                if (b.elem_ids.size() != 1)
+                if (b.elem_ids.size() != 1 || b.dense)
                     return set_err(c, KYN_ERR_UNSUPPORTED,
                                    "batched node_FX needs single-element beams (use kyn_model_set_loads)");
                 fo = L.fx;
@@ -973,7 +986,7 @@ int kyn_model_create(kyn_ctx* c, const kyn_model_desc* desc) {
     for (auto& b : m->host.beams) {
         const int hubf = hub_kind(m->host);
         const int nt = b.dense ? 128 : beam_threads(b.N, b.Q, b.nc, sizeof(double), hubf);
-        const int sm = b.dense ? make_dense_smem(b.N, m->host.ndofs).bytes
+        const int sm = b.dense ? make_dense_smem(b.N, m->host.ndofs, nt, b.comp_maxN, b.comp_maxQ).bytes
                                : std::max(beam_smem(b.N, b.Q, b.nc, sizeof(double), 512, hubf),
                                           beam_smem(b.N, b.Q, b.nc, sizeof(double), nt, hubf));
         if (sm > kMaxDynSmem)
@@ -1118,7 +1131,7 @@ int kyn_model_set_loads(kyn_ctx* c, int id, int which, const double* values) {
     for (size_t bi = 0; bi < m->host.beams.size(); ++bi) {
         const HostBeam& b = m->host.beams[bi];
         const SlabLayout L = make_slab_layout(b.N, b.Q);
-        if (which == KYN_LOAD_NODE_FX && b.elem_ids.size() > 1) {
+        if (which == KYN_LOAD_NODE_FX && (b.elem_ids.size() > 1 || b.dense)) {
             for (int k = 0; k < 6 * b.N; ++k) c->h_stage[off + k] = 0.;
             for (size_t ei = 0; ei < b.elem_ids.size(); ++ei) {
                 const int row = m->host.elem_row[b.elem_ids[ei]];
@@ -1777,7 +1790,7 @@ extern "C" int kyn_autotune(kyn_ctx* c, const int* ids, int n, const kyn_step_pa
         for (int nt : {128, 256, 512}) {
             bool fits = true;
             for (const HostBeam& b : h.beams)
-                fits &= (b.dense ? make_dense_smem(b.N, h.ndofs).bytes
+                fits &= (b.dense ? make_dense_smem(b.N, h.ndofs, nt, b.comp_maxN, b.comp_maxQ).bytes
                                  : beam_smem(b.N, b.Q, b.nc, rb, nt, hub_kind(h))) <= kMaxDynSmem;
             if (!fits || (key.beams > 1 && key.beams * nt > 1024 * 8)) continue;
             c->tuned[key] = nt;
@@ -1919,7 +1932,7 @@ int kyn_set_loads_batch_static(kyn_ctx* c, const int* ids, int n, int which,
             xb.N = b.N;
             xb.map_off = rows;
             if (which == KYN_LOAD_NODE_FX) {
-                if (b.elem_ids.size() != 1)
+                if (b.elem_ids.size() != 1 || b.dense)
                     return set_err(c, KYN_ERR_UNSUPPORTED,
                                    "batched node_FX needs single-element beams (use kyn_model_set_loads)");
                 xb.slab_field = m->d_slab[bi] + L.fx;

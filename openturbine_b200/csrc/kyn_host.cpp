@@ -293,6 +293,52 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
         init_node_state(d, B, L, B.slab.data());
     }
 
+    // A model with beam elements whose constraints the per-beam systems cannot
+    // take -- a joint whose base node is a beam node (beams coupled to each
+    // other, or a beam carrying a position-only node), or three-row
+    // constraints -- is solved as one dense bordered system (dense_kernel),
+    // as the reference assembles it (src/solver/create_full_matrix.hpp).  Its
+    // beam components keep their constant data (appended to the dense slab
+    // below); every node joins the one system record.
+    bool dense_beams = false;
+    std::vector<HostBeam> comps;
+    if (!lumped && d->num_constraints > 0 && d->constraint_type)
+        for (int c = 0; c < d->num_constraints; ++c) {
+            const int t = d->constraint_type[c];
+            const int base = d->constraint_base_node ? d->constraint_base_node[c] : -1;
+            if (t >= KYN_CONSTRAINT_FIXED_BC_3DOF) dense_beams = true;
+            if ((is_hub_joint(t) || t == KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF) && base >= 0 && base < nn &&
+                M.node_beam[base] >= 0)
+                dense_beams = true;
+        }
+    if (dense_beams) {
+        if (M.beams.size() > static_cast<size_t>(kMaxDenseComps))
+            return fail(err, KYN_ERR_UNSUPPORTED, "more than 8 beams in a dense model");
+        comps = std::move(M.beams);
+        M.beams.assign(1, HostBeam{});
+        HostBeam& B = M.beams[0];
+        B.N = nn;
+        B.Q = 0;
+        for (int n = 0; n < nn; ++n) {
+            B.node_ids.push_back(n);
+            M.node_beam[n] = 0;
+            M.node_local[n] = n;
+        }
+        for (int e = 0; e < d->num_beams; ++e) {
+            B.elem_ids.push_back(e);
+            B.elem_local.emplace_back(d->beam_node_ids + d->beam_node_offsets[e],
+                                      d->beam_node_ids + d->beam_node_offsets[e + 1]);
+        }
+        const SlabLayout L = make_slab_layout(nn, 0);
+        B.slab.assign(L.total, 0.);
+        init_node_state(d, B, L, B.slab.data());
+        B.n_comps = static_cast<int>(comps.size());
+        for (const HostBeam& cb : comps) {
+            B.comp_maxN = std::max(B.comp_maxN, cb.N);
+            B.comp_maxQ = std::max(B.comp_maxQ, cb.Q);
+        }
+    }
+
     // point masses and springs join the beam that holds their nodes
     // (src/elements/masses/create_masses.hpp, src/elements/springs/create_springs.hpp)
     std::vector<std::vector<double>> lrec_mass(M.beams.size()), lrec_spring(M.beams.size());
@@ -334,6 +380,28 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
         B.lumped_off = static_cast<int>(B.slab.size());
         B.slab.insert(B.slab.end(), lrec_mass[b].begin(), lrec_mass[b].end());
         B.slab.insert(B.slab.end(), lrec_spring[b].begin(), lrec_spring[b].end());
+    }
+    if (dense_beams) {
+        // [header: kCompHead doubles per component][component slabs], every
+        // slab at an even double offset (its arrays are 16-byte aligned)
+        HostBeam& B = M.beams[0];
+        if (B.slab.size() & 1) B.slab.push_back(0.);
+        B.comps_off = static_cast<int>(B.slab.size());
+        std::vector<double> head(kCompHead * comps.size(), 0.);
+        size_t at = (head.size() + 1) & ~static_cast<size_t>(1);
+        std::vector<double> body;
+        for (size_t ci = 0; ci < comps.size(); ++ci) {
+            const HostBeam& cb = comps[ci];
+            head[ci * kCompHead + 0] = static_cast<double>(at + body.size());
+            head[ci * kCompHead + 1] = cb.N;
+            head[ci * kCompHead + 2] = cb.Q;
+            for (int k = 0; k < cb.N; ++k) head[ci * kCompHead + 3 + k] = cb.node_ids[k];
+            body.insert(body.end(), cb.slab.begin(), cb.slab.end());
+            if (body.size() & 1) body.push_back(0.);
+        }
+        head.resize(at, 0.);
+        B.slab.insert(B.slab.end(), head.begin(), head.end());
+        B.slab.insert(B.slab.end(), body.begin(), body.end());
     }
     // A node outside every beam element is allowed only as the hub of a rotor
     // (the base node of the joints, held by one single-node BC) or as a node
@@ -391,10 +459,10 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
     int joints = 0;
     // A lumped model with three-row constraints or joints between its nodes is
     // solved as the reference's dense bordered system (one CTA, pivoted LU).
-    bool dense = false;
+    bool dense = dense_beams;
     for (int c = 0; c < d->num_constraints && lumped; ++c)
         dense |= is_hub_joint(d->constraint_type[c]) || d->constraint_type[c] >= KYN_CONSTRAINT_FIXED_BC_3DOF;
-    if (!lumped)
+    if (!lumped && !dense_beams)
         for (int c = 0; c < d->num_constraints; ++c)
             if (d->constraint_type[c] >= KYN_CONSTRAINT_FIXED_BC_3DOF)
                 return fail(err, KYN_ERR_UNSUPPORTED,
@@ -631,6 +699,8 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
             sig[d->constraint_target_node[c]] |= t >= KYN_CONSTRAINT_FIXED_BC_3DOF ? kSigPosition : kSigAll;
             if (is_hub_joint(t) || t == KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF) sig[base_of(c)] |= kSigAll;
         }
+        for (int k = 0; dense_beams && k < d->beam_node_offsets[d->num_beams]; ++k)
+            sig[d->beam_node_ids[k]] |= kSigAll;  // beam nodes (FreedomSignature AllComponents)
         for (int n = 0; n < nn; ++n) {
             if (sig[n] != kSigAll && sig[n] != kSigPosition)
                 return fail(err, KYN_ERR_UNSUPPORTED, "dense-model node without six or three DOFs");

@@ -30,7 +30,10 @@ struct HostBeam {
     double con_X0[kMaxBeamConstraints][3] = {};
     double con_axis[kMaxBeamConstraints][3] = {};  // RotationControl: unit axis
     bool lumped = false;              // all nodes of a model without beam elements (Q = 0)
-    bool dense = false;               // lumped, solved as the dense bordered system
+    bool dense = false;               // solved as the dense bordered system (one CTA, pivoted LU)
+    int n_comps = 0;                  // dense model with beams: beam components in the slab
+    int comps_off = 0;                // their header's offset in the slab (kCompHead records)
+    int comp_maxN = 0, comp_maxQ = 0; // largest component
     int con_base[kMaxBeamConstraints] = {-1, -1, -1, -1, -1, -1, -1, -1};  // dense: joint base (local)
     int n_mass = 0, n_spring = 0;     // point masses / springs at this beam's nodes
     int lumped_off = 0;               // their records' offset in the slab (kMassRec, kSpringRec)

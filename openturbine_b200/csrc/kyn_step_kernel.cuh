@@ -700,30 +700,36 @@ template <> struct Pair2<float> { using type = float2; };
 
 // Rank-2 update R[a][b] -= x0[a] u0[b] + x1[a] u1[b] of the column blocks
 // b >= b0 (one uniform test per column block, none per entry: padding rows and
-// columns hold zeros, so their updates change nothing).
+// columns hold zeros, so their updates change nothing).  (u0, u1) of column
+// block b is read from the pivot pair's row buffer `rp` (pairs per column).
 template <int B, typename TR, int RT, int CT>
 __device__ __forceinline__ void gj_rank2_from(TR (&R)[RT][CT], const TR (&x0)[RT], const TR (&x1)[RT],
-                                              const TR (&u0)[CT], const TR (&u1)[CT], int b0) {
+                                              const TR* rp, int b0) {
+    using P2 = typename Pair2<TR>::type;
     if constexpr (B < CT) {
         if (B >= b0) {
+            const P2 w = *reinterpret_cast<const P2*>(rp + 2 * B * kGJCols);
 #pragma unroll
-            for (int a = 0; a < RT; ++a) R[a][B] = fma(-x1[a], u1[B], fma(-x0[a], u0[B], R[a][B]));
+            for (int a = 0; a < RT; ++a) R[a][B] = fma(-x1[a], w.y, fma(-x0[a], w.x, R[a][B]));
         }
-        gj_rank2_from<B + 1>(R, x0, x1, u0, u1, b0);
+        gj_rank2_from<B + 1>(R, x0, x1, rp, b0);
     }
 }
 
 // Row a of R (a chosen at run time, the same in the whole warp) becomes
-// p u0 + q u1 in the column blocks b >= b0.
+// p u0 + q u1 in the column blocks b >= b0, (u0, u1) from the row buffer `rp`.
 template <typename TR, int RT, int CT>
-__device__ __forceinline__ void gj_set_row(TR (&R)[RT][CT], int a_sel, TR p, const TR (&u0)[CT], TR q,
-                                           const TR (&u1)[CT], int b0) {
+__device__ __forceinline__ void gj_set_row(TR (&R)[RT][CT], int a_sel, TR p, TR q, const TR* rp, int b0) {
+    using P2 = typename Pair2<TR>::type;
 #pragma unroll
     for (int a = 0; a < RT; ++a)
         if (a == a_sel) {
 #pragma unroll
             for (int b = 0; b < CT; ++b)
-                if (b >= b0) R[a][b] = fma(p, u0[b], q * u1[b]);
+                if (b >= b0) {
+                    const P2 w = *reinterpret_cast<const P2*>(rp + 2 * b * kGJCols);
+                    R[a][b] = fma(p, w.x, q * w.y);
+                }
         }
 }
 
@@ -790,26 +796,21 @@ __device__ __forceinline__ void gj_eliminate(const TR* A, int ldA, int m, int nr
         const TR rd = pivot_rcp(det);
         if (tid == 0 && (!(fabs(det) > TR(0)) || !isfinite(rd))) atomicOr(flag, 2);
         const TR i00 = dB.y * rd, i01 = -dA.y * rd, i10 = -dB.x * rd, i11 = dA.x * rd;
-        TR x0[RT], x1[RT], u0[CT], u1[CT];
+        TR x0[RT], x1[RT];
 #pragma unroll
         for (int a = 0; a < RT; ++a) {
             const P2 c = *reinterpret_cast<const P2*>(cb + 2 * (ri + a * PR));
             x0[a] = fma(c.x, i00, c.y * i10);
             x1[a] = fma(c.x, i01, c.y * i11);
         }
-#pragma unroll
-        for (int b = 0; b < CT; ++b) {
-            const P2 w = *reinterpret_cast<const P2*>(cb + ROWS + 2 * (cj + b * PC));
-            u0[b] = w.x;
-            u1[b] = w.y;
-        }
+        const TR* rp = cb + ROWS + 2 * cj;  // this thread's columns in the row pair
         // solve form: column blocks left of b0 hold only eliminated columns
         const int b0 = INV ? 0 : (k + 2) / PC;
-        gj_rank2_from<0>(R, x0, x1, u0, u1, b0);
+        gj_rank2_from<0>(R, x0, x1, rp, b0);
         // the pivot rows: D^-1 [row k; row k+1]
         const int ak = k / PR;
         const bool r0 = ri == k % PR, r1 = ri == (k + 1) % PR;
-        if (r0 || r1) gj_set_row(R, ak, r0 ? i00 : i10, u0, r0 ? i01 : i11, u1, b0);
+        if (r0 || r1) gj_set_row(R, ak, r0 ? i00 : i10, r0 ? i01 : i11, rp, b0);
         if (INV) {  // the pivot columns: -A_iK D^-1, and D^-1 in the pivot rows
             const int bk = k / PC;
             const bool c0 = cj == k % PC, c1 = cj == (k + 1) % PC;
@@ -1269,9 +1270,15 @@ __device__ void add_lumped_terms(int n, const double* __restrict__ rec, int n_ma
 // in both precision forms: these systems have at most kDenseModelMaxDofs unknowns.
 
 struct DenseSmem {
-    int M, b, x, q, qp, v, vd, a, qd, T, resid, con, act, fmap, red, bytes;
+    int M, b, x, q, qp, v, vd, a, qd, T, resid, con, act, fmap, red;
+    // beam components (dense models with beams): shape tables, weights and
+    // node state of one component at a time, its quadrature-point outputs and
+    // the quadrature phase's group scratch
+    int cphi, cdphi, cdphiJ, cqpw, cq, cv, cvd, cG, cFc, cFd, cgs;
+    int bytes;
 };
-__host__ __device__ inline DenseSmem make_dense_smem(int N, int nd) {
+// nt, cN, cQ: threads per CTA and the largest beam component (0: none).
+__host__ __device__ inline DenseSmem make_dense_smem(int N, int nd, int nt = 128, int cN = 0, int cQ = 0) {
     DenseSmem S{};
     int o = 0;
     auto take = [&](int bytes) {
@@ -1294,8 +1301,376 @@ __host__ __device__ inline DenseSmem make_dense_smem(int N, int nd) {
     S.act = take(N * 4);
     S.fmap = take(N * 4);
     S.red = take(64 * 8);  // per-warp partial sums of the error
+    S.cphi = S.cdphi = S.cdphiJ = S.cqpw = S.cq = S.cv = S.cvd = S.cG = S.cFc = S.cFd = S.cgs = -1;
+    if (cN > 0) {
+        S.cphi = take(cQ * cN * 8);
+        S.cdphi = take(cQ * cN * 8);
+        S.cdphiJ = take(cQ * cN * 8);
+        S.cqpw = take(cQ * 4 * 8);
+        S.cq = take(cN * 7 * 8);
+        S.cv = take(cN * 6 * 8);
+        S.cvd = take(cN * 6 * 8);
+        S.cG = take(4 * cQ * 56 * 8);
+        S.cFc = take(cQ * 6 * 8);
+        S.cFd = take(cQ * 6 * 8);
+        S.cgs = take((nt / 16) * kGroupScratch * 8);
+    }
     S.bytes = o;
     return S;
+}
+
+
+// Quadrature-point physics of one beam system (calculate_quadrature_point_values.hpp:
+// a6-a10 of the step path): 16 threads per quadrature point, NT/16 points per
+// pass.  Each stage gives every lane of a group the same formula on its own
+// entries, so the half-warps run without divergence.  Inputs: shape tables
+// phi / dphiJ [Q][N], weights qpw [Q][4], node state q [N][7], v, vd [N][6]
+// (shared memory), the system's slab for the sections and reference frames
+// (layout L).  Outputs: Fc, Fd + Fi - Fg [Q][6] and the weighted blocks of the
+// integration GEMM G [4Q][56] (column layout gcol).  gscr: NT/16 groups of
+// kGroupScratch doubles.
+template <typename TG, int NT>
+__device__ __forceinline__ void qp_phase(int N, int Q, const double* phi, const double* dphiJ,
+                                         const double* qpw, const double* sq, const double* sv,
+                                         const double* svd, const double* __restrict__ slab,
+                                         const SlabLayout& L, const double* gravity, double beta_prime,
+                                         double gamma_prime, double* gscr, TG* G, double* Fc, double* Fdig) {
+    constexpr int NG = NT / 16;
+    const int tid = threadIdx.x;
+    const int grp = tid >> 4;
+    const int g = tid & 15;
+    double* gs = gscr + grp * kGroupScratch;
+    double* rn = gs + grec::rn;
+    double* Rx = gs + grec::Rx;
+    double* Rr = gs + grec::Rr;
+    double* st = gs + grec::st;
+    double* Mu = gs + grec::Mu;
+    double* ms = gs + grec::ms;
+    double* O12 = gs + grec::O12;
+    double* Gu = gs + grec::Gu;
+    double* Kk = gs + grec::Kk;
+    double* fcv = gs + grec::fcv;
+    double* Cu = gs + grec::Cu;
+    const double* mst = gs + grec::mstar;
+    const double* cst = gs + grec::cstar;
+    const double* r0 = gs + grec::r0;
+    const double* x0p = gs + grec::x0p;
+    for (int q0 = 0; q0 < Q; q0 += NG) {
+        const int qp = q0 + grp;
+        const bool act = qp < Q;
+        const double* ph_q = phi + qp * N;
+        if (act) {
+            // stage this point's sections and reference frame from the slab
+            // (read early: the loads overlap the interpolation below)
+            for (int k = g; k < 79; k += 16) {
+                double v;
+                if (k < 36) v = slab[L.mstar + qp * 36 + k];
+                else if (k < 72) v = slab[L.cstar + qp * 36 + (k - 36)];
+                else if (k < 76) v = slab[L.r0 + qp * 4 + (k - 72)];
+                else v = slab[L.x0p + qp * 3 + (k - 76)];
+                gs[grec::mstar + k] = v;
+            }
+            // this point's G rows start at zero (structural zeros, padding)
+            TG* Gq = G + 4 * qp * 56;
+            for (int t = g; t < 4 * 56; t += 16) Gq[t] = TG(0);
+        }
+        // (1) interpolation: r, u_ddot, omega, omega_dot, u', r'
+        if (act) {
+            for (int k = g; k < 20; k += 16) {
+                // source column of node state and shape table for sum k
+                const double* src = (k < 4) ? sq + 3 + k
+                                  : (k < 7) ? svd + (k - 4)
+                                  : (k < 10) ? sv + 3 + (k - 7)
+                                  : (k < 13) ? svd + 3 + (k - 10)
+                                  : (k < 16) ? sq + (k - 13)
+                                             : sq + 3 + (k - 16);
+                const int stride = (k < 4 || k >= 13) ? 7 : 6;
+                const double* shp = (k < 13) ? ph_q : dphiJ + qp * N;
+                double acc = 0.;
+                for (int n = 0; n < N; ++n) acc += src[n * stride] * shp[n];
+                gs[k] = acc;
+            }
+        }
+        __syncwarp();
+        if (act && g < 4) {
+            const double nr = sqrt(gs[0] * gs[0] + gs[1] * gs[1] + gs[2] * gs[2] + gs[3] * gs[3]);
+            rn[g] = gs[g] / nr;
+        }
+        __syncwarp();
+        // (2) R(xr), R(r), rotational strain 2 E(r) r', s = x0' + u'
+        if (act) {
+            for (int k = g; k < 24; k += 16) {
+                if (k < 9) {
+                    double xr[4];
+                    quat_compose(rn, r0, xr);
+                    Rx[k] = rot_entry(xr, k / 3, k % 3);
+                } else if (k < 18) {
+                    Rr[k - 9] = rot_entry(rn, (k - 9) / 3, (k - 9) % 3);
+                } else if (k < 21) {
+                    // 2 E(r) r' with E = QuaternionDerivative (3x4)
+                    const int i = k - 18;
+                    const double* rp = gs + 16;
+                    double e;
+                    if (i == 0) e = -rn[1] * rp[0] + rn[0] * rp[1] - rn[3] * rp[2] + rn[2] * rp[3];
+                    else if (i == 1) e = -rn[2] * rp[0] + rn[3] * rp[1] + rn[0] * rp[2] - rn[1] * rp[3];
+                    else e = -rn[3] * rp[0] - rn[2] * rp[1] + rn[1] * rp[2] + rn[0] * rp[3];
+                    st[3 + i] = 2. * e;
+                } else {
+                    ms[4 + (k - 21)] = x0p[k - 21] + gs[13 + (k - 21)];
+                }
+            }
+        }
+        __syncwarp();
+        // (3) Muu = R M* R^T, Cuu = R C* R^T; translational strain
+        if (act) {
+            for (int o = g; o < 75; o += 16) {
+                if (o < 72) {
+                    const int e = o % 36;
+                    const int i = e / 6, j = e % 6;
+                    const int bi = i / 3, bj = j / 3, ii = i % 3, jj = j % 3;
+                    const double* Cs = (o < 36) ? mst : cst;
+                    double acc = 0.;
+                    for (int pp = 0; pp < 3; ++pp) {
+                        double t = 0.;
+                        for (int ss = 0; ss < 3; ++ss)
+                            t += Cs[(3 * bi + pp) * 6 + 3 * bj + ss] * Rx[jj * 3 + ss];
+                        acc += Rx[ii * 3 + pp] * t;
+                    }
+                    if (o < 36) Mu[e] = acc;
+                    else Cu[e] = acc;
+                } else {
+                    // strain[i] = x0' + u' - R(r) x0'  (calculate_strain.hpp:27-46)
+                    const int i = o - 72;
+                    double rx = 0.;
+                    for (int j = 0; j < 3; ++j) rx += Rr[i * 3 + j] * x0p[j];
+                    st[i] = x0p[i] + gs[13 + i] - rx;
+                }
+            }
+        }
+        __syncwarp();
+        // (4) FC = Cuu eps (calculate_force_FC.hpp); mass and eta (CalculateEta)
+        if (act && g < 6) {
+            double f = 0.;
+            for (int j = 0; j < 6; ++j) f += Cu[g * 6 + j] * st[j];
+            fcv[g] = f;
+            Fc[qp * 6 + g] = f;
+        } else if (act && g == 6) {
+            const double mass = Mu[0];
+            ms[0] = mass;
+            ms[1] = Mu[5 * 6 + 1] / mass;
+            ms[2] = -Mu[5 * 6 + 0] / mass;
+            ms[3] = Mu[4 * 6 + 0] / mass;
+        }
+        __syncwarp();
+        const double* ud = gs + 4;
+        const double* om = gs + 7;
+        const double* omd = gs + 10;
+        const double* sv3 = ms + 4;  // x0' + u'
+        if (act && g < 9) {
+            // (5) entry (i,j) of every 3x3 block: Ouu, Puu (calculate_Ouu/Puu.hpp),
+            //     Guu (calculate_gyroscopic_matrix.hpp), Kuu
+            //     (calculate_inertia_stiffness_matrix.hpp)
+            const int i = g / 3, j = g % 3;
+            const double mass = ms[0];
+            const double meta[3] = {mass * ms[1], mass * ms[2], mass * ms[3]};
+            double rw[3], rwd[3], wme[3];
+            for (int r = 0; r < 3; ++r) {
+                rw[r] = Mu[(3 + r) * 6 + 3] * om[0] + Mu[(3 + r) * 6 + 4] * om[1] +
+                        Mu[(3 + r) * 6 + 5] * om[2];
+                rwd[r] = Mu[(3 + r) * 6 + 3] * omd[0] + Mu[(3 + r) * 6 + 4] * omd[1] +
+                         Mu[(3 + r) * 6 + 5] * omd[2];
+            }
+            cross3(om, meta, wme);
+            double o12 = -tilde_e(fcv, i, j), o22 = -tilde_e(fcv + 3, i, j);
+            double p21 = tilde_e(fcv, i, j), p22 = 0.;
+            double g12 = -tilde_e(wme, i, j), g22 = -tilde_e(rw, i, j);
+            double k12 = 0., k22 = -tilde_e(rwd, i, j);
+            for (int k = 0; k < 3; ++k) {
+                const double s_kj = tilde_e(sv3, k, j);
+                const double s_ki = tilde_e(sv3, k, i);
+                o12 += Cu[i * 6 + k] * s_kj;
+                o22 += Cu[(3 + i) * 6 + k] * s_kj;
+                p21 += s_ki * Cu[k * 6 + j];
+                p22 += s_ki * Cu[k * 6 + 3 + j];
+                const double w_ik = tilde_e(om, i, k);
+                const double me_kj = tilde_e(meta, k, j);
+                g12 -= w_ik * me_kj;
+                g22 += w_ik * Mu[(3 + k) * 6 + 3 + j];
+                double ww = 0.;
+                for (int l = 0; l < 3; ++l) ww += tilde_e(om, i, l) * tilde_e(om, l, k);
+                k12 -= (tilde_e(omd, i, k) + ww) * me_kj;
+                k22 += Mu[(3 + i) * 6 + 3 + k] * tilde_e(omd, k, j);
+                k22 += tilde_e(ud, i, k) * me_kj;
+                double inner = -tilde_e(rw, k, j);
+                for (int l = 0; l < 3; ++l) inner += Mu[(3 + k) * 6 + 3 + l] * tilde_e(om, l, j);
+                k22 += w_ik * inner;
+            }
+            // G rows of this quadrature point (see the integration GEMM):
+            //   4q+1: w [Puu left | Puu right | 0], 4q+3: w [0 | Ouu right | 0]
+            const double w = qpw[qp * 4], wJ = qpw[qp * 4 + 2];
+            TG* G1 = G + (4 * qp + 1) * 56;
+            TG* G3 = G + (4 * qp + 3) * 56;
+            O12[g] = o12;
+            G3[gcol(18 + g)] = static_cast<TG>(w * o12);
+            G3[gcol(18 + 9 + g)] = static_cast<TG>(w * o22);
+            G1[gcol(9 + g)] = static_cast<TG>(w * p21);
+            G1[gcol(18 + 9 + g)] = static_cast<TG>(w * p22);
+            Gu[g] = g12;
+            Gu[9 + g] = g22;
+            G[(4 * qp) * 56 + gcol(18 + g)] = static_cast<TG>(wJ * k12);
+            Kk[g] = k22;
+        } else if (act && g < 15) {
+            // Fd + Fi - Fe - Fg (calculate_force_FD.hpp, calculate_inertial_force.hpp,
+            // calculate_gravity_force.hpp; Fe = 0)
+            const int c = g - 9;
+            const double mass = ms[0];
+            const double eta[3] = {ms[1], ms[2], ms[3]};
+            double fd = 0., fi, fgv;
+            if (c < 3) {
+                double wxe[3], wxwxe[3], wdxe[3];
+                cross3(om, eta, wxe);
+                cross3(om, wxe, wxwxe);
+                cross3(omd, eta, wdxe);
+                fi = mass * ud[c] + mass * (wxwxe[c] + wdxe[c]);
+                fgv = mass * gravity[c];
+            } else {
+                const int i = c - 3;
+                for (int k = 0; k < 3; ++k) fd += tilde_e(sv3, k, i) * fcv[k];
+                double exu[3], rw[3], rwd[3], wxrw[3];
+                cross3(eta, ud, exu);
+                for (int r = 0; r < 3; ++r) {
+                    rw[r] = Mu[(3 + r) * 6 + 3] * om[0] + Mu[(3 + r) * 6 + 4] * om[1] +
+                            Mu[(3 + r) * 6 + 5] * om[2];
+                    rwd[r] = Mu[(3 + r) * 6 + 3] * omd[0] + Mu[(3 + r) * 6 + 4] * omd[1] +
+                             Mu[(3 + r) * 6 + 5] * omd[2];
+                }
+                cross3(om, rw, wxrw);
+                fi = mass * exu[i] + rwd[i] + wxrw[i];
+                const double mg[3] = {mass * gravity[0], mass * gravity[1],
+                                      mass * gravity[2]};
+                double exg[3];
+                cross3(eta, mg, exg);
+                fgv = exg[i];
+            }
+            Fdig[qp * 6 + c] = fd + fi - fgv;
+        }
+        __syncwarp();
+        // (6) Quu_22 = SS^T (C11 SS - N~) joins Kuu_22; XI = beta' Muu + gamma' Guu;
+        //     G rows 4q+0: wJ [XI left | XK right | XI right], 4q+2: (w/J) [Cuu]
+        if (act) {
+            const double wJ = qpw[qp * 4 + 2], wdJ = qpw[qp * 4 + 3];
+            TG* G0 = G + (4 * qp) * 56;
+            TG* G2 = G + (4 * qp + 2) * 56;
+            if (g < 9) {
+                const int i = g / 3, j = g % 3;
+                double qv = 0.;
+                for (int k = 0; k < 3; ++k) qv += tilde_e(sv3, k, i) * O12[k * 3 + j];
+                G0[gcol(18 + 9 + g)] = static_cast<TG>(wJ * (Kk[g] + qv));
+            }
+            for (int e = g; e < 36; e += 16) {
+                const int i = e / 6, j = e % 6;
+                double gg = 0.;
+                if (j >= 3) gg = Gu[(i < 3 ? 0 : 9) + (i % 3) * 3 + (j - 3)];
+                const double xi = beta_prime * Mu[e] + gamma_prime * gg;
+                const int col = (j < 3) ? i * 3 + j : 36 + i * 3 + (j - 3);
+                G0[gcol(col)] = static_cast<TG>(wJ * xi);
+                G2[gcol((j < 3) ? i * 3 + j : 18 + i * 3 + (j - 3))] = static_cast<TG>(wdJ * Cu[e]);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Beam element terms of the components of a dense model (the step path's
+// a5-a14 for elements whose nodes sit in a dense bordered system): for each
+// component, the quadrature-point physics (qp_phase, on the component's local
+// nodes), the residual (integrate_residual_vector.hpp:33-50) into resid of
+// the model nodes, and SM_ij = S_ij T_j + I_ij (integrate_stiffness_matrix.hpp,
+// integrate_inertia_matrix.hpp, calculate_system_matrix.hpp) times the
+// conditioner added into the dense matrix Md at the nodes' DOF rows and
+// columns (contribute_beams_to_sparse_matrix.hpp).  Components run one after
+// the other, so shared nodes sum without races.
+template <int NT>
+__device__ void dense_beam_terms(const KBeam& KB, const StepCoeffs& P, const DenseSmem& S, unsigned char* smem_raw,
+                                 const double* sq, const double* sv, const double* svd, const double* sT,
+                                 const int* fmap, double* Md, int nd, double* resid) {
+    const int tid = threadIdx.x;
+    double* phi = reinterpret_cast<double*>(smem_raw + S.cphi);
+    double* dphi = reinterpret_cast<double*>(smem_raw + S.cdphi);
+    double* dphiJ = reinterpret_cast<double*>(smem_raw + S.cdphiJ);
+    double* qpw = reinterpret_cast<double*>(smem_raw + S.cqpw);
+    double* cq = reinterpret_cast<double*>(smem_raw + S.cq);
+    double* cv = reinterpret_cast<double*>(smem_raw + S.cv);
+    double* cvd = reinterpret_cast<double*>(smem_raw + S.cvd);
+    double* G = reinterpret_cast<double*>(smem_raw + S.cG);
+    double* Fc = reinterpret_cast<double*>(smem_raw + S.cFc);
+    double* Fd = reinterpret_cast<double*>(smem_raw + S.cFd);
+    double* gscr = reinterpret_cast<double*>(smem_raw + S.cgs);
+    const double cond = P.conditioner;
+    for (int ci = 0; ci < KB.n_comps; ++ci) {
+        const double* hd = KB.comps + ci * kCompHead;
+        const double* cs = KB.comps + static_cast<long>(hd[0]);
+        const int N = static_cast<int>(hd[1]), Q = static_cast<int>(hd[2]);
+        const double* node = hd + 3;  // model node of each local node
+        const SlabLayout L = make_slab_layout(N, Q);
+        for (int k = tid; k < Q * N; k += NT) {
+            phi[k] = cs[L.phi + k];
+            dphi[k] = cs[L.dphi + k];
+            dphiJ[k] = cs[L.dphiJ + k];
+        }
+        for (int k = tid; k < Q * 4; k += NT) qpw[k] = cs[L.qpw + k];
+        for (int k = tid; k < N * 7; k += NT) cq[k] = sq[static_cast<int>(node[k / 7]) * 7 + k % 7];
+        for (int k = tid; k < N * 6; k += NT) {
+            const int n = static_cast<int>(node[k / 6]);
+            cv[k] = sv[n * 6 + k % 6];
+            cvd[k] = svd[n * 6 + k % 6];
+        }
+        __syncthreads();
+        qp_phase<double, NT>(N, Q, phi, dphiJ, qpw, cq, cv, cvd, cs, L, KB.gravity, P.beta_prime, P.gamma_prime,
+                             gscr, G, Fc, Fd);
+        __syncthreads();
+        for (int t = tid; t < N * 6; t += NT) {
+            const int n = t / 6, c = t % 6;
+            double acc = 0.;
+            for (int qp = 0; qp < Q; ++qp) {
+                const double w = qpw[qp * 4], wJ = qpw[qp * 4 + 2];
+                acc += (w * dphi[qp * N + n]) * Fc[qp * 6 + c] + (wJ * phi[qp * N + n]) * Fd[qp * 6 + c];
+            }
+            resid[static_cast<int>(node[n]) * 6 + c] += acc;
+        }
+        // one thread per (node pair, row): C_ij[r] = sum_q sum_m coef_m(i, j, q) G[4q+m]
+        // with coef = (phi_i phi_j, phi_i phi'_j, phi'_i phi'_j, phi'_i phi_j)
+        for (int t = tid; t < N * N * 6; t += NT) {
+            const int pr = t / 6, r = t % 6;
+            const int i = pr / N, j = pr % N;
+            double Lr[3] = {0., 0., 0.}, RS[3] = {0., 0., 0.}, RI[3] = {0., 0., 0.};
+            for (int qp = 0; qp < Q; ++qp) {
+                const double pi = phi[qp * N + i], pj = phi[qp * N + j];
+                const double di = dphi[qp * N + i], dj = dphi[qp * N + j];
+                const double coef[4] = {pi * pj, pi * dj, di * dj, di * pj};
+#pragma unroll
+                for (int mm = 0; mm < 4; ++mm) {
+                    const double* g = G + (4 * qp + mm) * 56;
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        Lr[c] += coef[mm] * g[gcol(r * 3 + c)];
+                        RS[c] += coef[mm] * g[gcol(18 + r * 3 + c)];
+                        RI[c] += coef[mm] * g[gcol(36 + r * 3 + c)];
+                    }
+                }
+            }
+            const int nj = static_cast<int>(node[j]);
+            const double* Tj = sT + nj * 9;
+            double* row = Md + (fmap[static_cast<int>(node[i])] + r) * nd + fmap[nj];
+            for (int c = 0; c < 3; ++c) row[c] += cond * Lr[c];
+            for (int c = 0; c < 3; ++c) {
+                double v = RI[c];
+                for (int k = 0; k < 3; ++k) v += RS[k] * Tj[k * 3 + c];
+                row[3 + c] += cond * v;
+            }
+        }
+        __syncthreads();
+    }
 }
 
 template <int NT>
@@ -1307,7 +1682,7 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
     const SlabLayout L = make_slab_layout(N, 0);
     double* __restrict__ slab = KB.slab;
     const int nd = KB.model_dofs;
-    const DenseSmem S = make_dense_smem(N, nd);
+    const DenseSmem S = make_dense_smem(N, nd, NT, KB.n_comps > 0 ? KB.comp_maxN : 0, KB.comp_maxQ);
     double* Md = reinterpret_cast<double*>(smem_raw + S.M);
     double* b = reinterpret_cast<double*>(smem_raw + S.b);
     double* x = reinterpret_cast<double*>(smem_raw + S.x);
@@ -1354,6 +1729,10 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
             const int t = KB.con_type[c];
             act[KB.con_node[c]] |= (t >= KYN_CONSTRAINT_FIXED_BC_3DOF) ? kSigPosition : kSigAll;
             if (KB.con_base[c] >= 0) act[KB.con_base[c]] |= kSigAll;
+        }
+        for (int ci = 0; ci < KB.n_comps; ++ci) {  // beam nodes: all six components
+            const double* hd = KB.comps + ci * kCompHead;
+            for (int k = 0; k < static_cast<int>(hd[1]); ++k) act[static_cast<int>(hd[3 + k])] |= kSigAll;
         }
         int o = 0;
         for (int n = 0; n < N; ++n) {
@@ -1416,6 +1795,11 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
         for (int n = tid; n < N; n += NT)
             add_lumped_terms(n, KB.lumped, KB.n_mass, KB.n_spring, sq, sv, svd, sT, KB.gravity,
                              P.beta_prime, P.gamma_prime, cond, fmap, Md, nd, resid, 1);
+        if (KB.n_comps > 0) {  // beam elements, then their node_FX (summed per node)
+            __syncthreads();
+            dense_beam_terms<NT>(KB, P, S, smem_raw, sq, sv, svd, sT, fmap, Md, nd, resid);
+            for (int t = tid; t < N * 6; t += NT) resid[t] -= slab[L.fx + t];
+        }
         // constraints: residual, gradients and G^T lambda
         if (tid < nc) {
             double* cr = con + tid * kConStride;
@@ -1699,7 +2083,10 @@ __host__ __device__ constexpr int step_min_blocks(int real_bytes, int nt) {
 // LUMP: the instance that also adds point masses and springs (KBeam::lumped);
 // beams without them run the instance compiled without that code, whose
 // registers it would otherwise crowd.
-template <typename TR, int NT, bool LUMP>
+// GJ: the instance that also carries the register Gauss-Jordan solve
+// (KYN_SOLVER_GAUSS_JORDAN); the default instances carry only the panel LU,
+// whose register allocation the Gauss-Jordan tile would otherwise crowd.
+template <typename TR, int NT, bool LUMP, bool GJ = false>
 __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
     step_kernel(const KBeam* __restrict__ beams, StepCoeffs P, int record,
                 int* __restrict__ status_out, int* __restrict__ iters_out) {
@@ -1914,253 +2301,8 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
         if (hub && chain_rec()) tangent_op(chain_rec() + hubrec::q_delta, chain_rec() + hubrec::tangent);
 
         // ---- quadrature-point values (calculate_quadrature_point_values.hpp) ---
-        // 16 threads per quadrature point; a CTA covers NT/16 points per pass.  Each
-        // stage gives every lane of a group the same formula on its own entries,
-        // so the half-warps run without divergence.
-        {
-            const int grp = tid >> 4;
-            const int g = tid & 15;
-            double* gs = gscr + grp * kGroupScratch;
-            double* rn = gs + grec::rn;
-            double* Rx = gs + grec::Rx;
-            double* Rr = gs + grec::Rr;
-            double* st = gs + grec::st;
-            double* Mu = gs + grec::Mu;
-            double* ms = gs + grec::ms;
-            double* O12 = gs + grec::O12;
-            double* Gu = gs + grec::Gu;
-            double* Kk = gs + grec::Kk;
-            double* fcv = gs + grec::fcv;
-            double* Cu = gs + grec::Cu;
-            const double* mst = gs + grec::mstar;
-            const double* cst = gs + grec::cstar;
-            const double* r0 = gs + grec::r0;
-            const double* x0p = gs + grec::x0p;
-            for (int q0 = 0; q0 < Q; q0 += NG) {
-                const int qp = q0 + grp;
-                const bool act = qp < Q;
-                const double* ph_q = phi + qp * N;
-                if (act) {
-                    // stage this point's sections and reference frame from the slab
-                    // (read early: the loads overlap the interpolation below)
-                    for (int k = g; k < 79; k += 16) {
-                        double v;
-                        if (k < 36) v = slab[L.mstar + qp * 36 + k];
-                        else if (k < 72) v = slab[L.cstar + qp * 36 + (k - 36)];
-                        else if (k < 76) v = slab[L.r0 + qp * 4 + (k - 72)];
-                        else v = slab[L.x0p + qp * 3 + (k - 76)];
-                        gs[grec::mstar + k] = v;
-                    }
-                    // this point's G rows start at zero (structural zeros, padding)
-                    TG* Gq = G + 4 * qp * 56;
-                    for (int t = g; t < 4 * 56; t += 16) Gq[t] = TG(0);
-                }
-                // (1) interpolation: r, u_ddot, omega, omega_dot, u', r'
-                if (act) {
-                    for (int k = g; k < 20; k += 16) {
-                        // source column of node state and shape table for sum k
-                        const double* src = (k < 4) ? sq + 3 + k
-                                          : (k < 7) ? svd + (k - 4)
-                                          : (k < 10) ? sv + 3 + (k - 7)
-                                          : (k < 13) ? svd + 3 + (k - 10)
-                                          : (k < 16) ? sq + (k - 13)
-                                                     : sq + 3 + (k - 16);
-                        const int stride = (k < 4 || k >= 13) ? 7 : 6;
-                        const double* shp = (k < 13) ? ph_q : dphiJ + qp * N;
-                        double acc = 0.;
-                        for (int n = 0; n < N; ++n) acc += src[n * stride] * shp[n];
-                        gs[k] = acc;
-                    }
-                }
-                __syncwarp();
-                if (act && g < 4) {
-                    const double nr = sqrt(gs[0] * gs[0] + gs[1] * gs[1] + gs[2] * gs[2] + gs[3] * gs[3]);
-                    rn[g] = gs[g] / nr;
-                }
-                __syncwarp();
-                // (2) R(xr), R(r), rotational strain 2 E(r) r', s = x0' + u'
-                if (act) {
-                    for (int k = g; k < 24; k += 16) {
-                        if (k < 9) {
-                            double xr[4];
-                            quat_compose(rn, r0, xr);
-                            Rx[k] = rot_entry(xr, k / 3, k % 3);
-                        } else if (k < 18) {
-                            Rr[k - 9] = rot_entry(rn, (k - 9) / 3, (k - 9) % 3);
-                        } else if (k < 21) {
-                            // 2 E(r) r' with E = QuaternionDerivative (3x4)
-                            const int i = k - 18;
-                            const double* rp = gs + 16;
-                            double e;
-                            if (i == 0) e = -rn[1] * rp[0] + rn[0] * rp[1] - rn[3] * rp[2] + rn[2] * rp[3];
-                            else if (i == 1) e = -rn[2] * rp[0] + rn[3] * rp[1] + rn[0] * rp[2] - rn[1] * rp[3];
-                            else e = -rn[3] * rp[0] - rn[2] * rp[1] + rn[1] * rp[2] + rn[0] * rp[3];
-                            st[3 + i] = 2. * e;
-                        } else {
-                            ms[4 + (k - 21)] = x0p[k - 21] + gs[13 + (k - 21)];
-                        }
-                    }
-                }
-                __syncwarp();
-                // (3) Muu = R M* R^T, Cuu = R C* R^T; translational strain
-                if (act) {
-                    for (int o = g; o < 75; o += 16) {
-                        if (o < 72) {
-                            const int e = o % 36;
-                            const int i = e / 6, j = e % 6;
-                            const int bi = i / 3, bj = j / 3, ii = i % 3, jj = j % 3;
-                            const double* Cs = (o < 36) ? mst : cst;
-                            double acc = 0.;
-                            for (int pp = 0; pp < 3; ++pp) {
-                                double t = 0.;
-                                for (int ss = 0; ss < 3; ++ss)
-                                    t += Cs[(3 * bi + pp) * 6 + 3 * bj + ss] * Rx[jj * 3 + ss];
-                                acc += Rx[ii * 3 + pp] * t;
-                            }
-                            if (o < 36) Mu[e] = acc;
-                            else Cu[e] = acc;
-                        } else {
-                            // strain[i] = x0' + u' - R(r) x0'  (calculate_strain.hpp:27-46)
-                            const int i = o - 72;
-                            double rx = 0.;
-                            for (int j = 0; j < 3; ++j) rx += Rr[i * 3 + j] * x0p[j];
-                            st[i] = x0p[i] + gs[13 + i] - rx;
-                        }
-                    }
-                }
-                __syncwarp();
-                // (4) FC = Cuu eps (calculate_force_FC.hpp); mass and eta (CalculateEta)
-                if (act && g < 6) {
-                    double f = 0.;
-                    for (int j = 0; j < 6; ++j) f += Cu[g * 6 + j] * st[j];
-                    fcv[g] = f;
-                    Fc[qp * 6 + g] = f;
-                } else if (act && g == 6) {
-                    const double mass = Mu[0];
-                    ms[0] = mass;
-                    ms[1] = Mu[5 * 6 + 1] / mass;
-                    ms[2] = -Mu[5 * 6 + 0] / mass;
-                    ms[3] = Mu[4 * 6 + 0] / mass;
-                }
-                __syncwarp();
-                const double* ud = gs + 4;
-                const double* om = gs + 7;
-                const double* omd = gs + 10;
-                const double* sv3 = ms + 4;  // x0' + u'
-                if (act && g < 9) {
-                    // (5) entry (i,j) of every 3x3 block: Ouu, Puu (calculate_Ouu/Puu.hpp),
-                    //     Guu (calculate_gyroscopic_matrix.hpp), Kuu
-                    //     (calculate_inertia_stiffness_matrix.hpp)
-                    const int i = g / 3, j = g % 3;
-                    const double mass = ms[0];
-                    const double meta[3] = {mass * ms[1], mass * ms[2], mass * ms[3]};
-                    double rw[3], rwd[3], wme[3];
-                    for (int r = 0; r < 3; ++r) {
-                        rw[r] = Mu[(3 + r) * 6 + 3] * om[0] + Mu[(3 + r) * 6 + 4] * om[1] +
-                                Mu[(3 + r) * 6 + 5] * om[2];
-                        rwd[r] = Mu[(3 + r) * 6 + 3] * omd[0] + Mu[(3 + r) * 6 + 4] * omd[1] +
-                                 Mu[(3 + r) * 6 + 5] * omd[2];
-                    }
-                    cross3(om, meta, wme);
-                    double o12 = -tilde_e(fcv, i, j), o22 = -tilde_e(fcv + 3, i, j);
-                    double p21 = tilde_e(fcv, i, j), p22 = 0.;
-                    double g12 = -tilde_e(wme, i, j), g22 = -tilde_e(rw, i, j);
-                    double k12 = 0., k22 = -tilde_e(rwd, i, j);
-                    for (int k = 0; k < 3; ++k) {
-                        const double s_kj = tilde_e(sv3, k, j);
-                        const double s_ki = tilde_e(sv3, k, i);
-                        o12 += Cu[i * 6 + k] * s_kj;
-                        o22 += Cu[(3 + i) * 6 + k] * s_kj;
-                        p21 += s_ki * Cu[k * 6 + j];
-                        p22 += s_ki * Cu[k * 6 + 3 + j];
-                        const double w_ik = tilde_e(om, i, k);
-                        const double me_kj = tilde_e(meta, k, j);
-                        g12 -= w_ik * me_kj;
-                        g22 += w_ik * Mu[(3 + k) * 6 + 3 + j];
-                        double ww = 0.;
-                        for (int l = 0; l < 3; ++l) ww += tilde_e(om, i, l) * tilde_e(om, l, k);
-                        k12 -= (tilde_e(omd, i, k) + ww) * me_kj;
-                        k22 += Mu[(3 + i) * 6 + 3 + k] * tilde_e(omd, k, j);
-                        k22 += tilde_e(ud, i, k) * me_kj;
-                        double inner = -tilde_e(rw, k, j);
-                        for (int l = 0; l < 3; ++l) inner += Mu[(3 + k) * 6 + 3 + l] * tilde_e(om, l, j);
-                        k22 += w_ik * inner;
-                    }
-                    // G rows of this quadrature point (see the integration GEMM):
-                    //   4q+1: w [Puu left | Puu right | 0], 4q+3: w [0 | Ouu right | 0]
-                    const double w = qpw[qp * 4], wJ = qpw[qp * 4 + 2];
-                    TG* G1 = G + (4 * qp + 1) * 56;
-                    TG* G3 = G + (4 * qp + 3) * 56;
-                    O12[g] = o12;
-                    G3[gcol(18 + g)] = static_cast<TG>(w * o12);
-                    G3[gcol(18 + 9 + g)] = static_cast<TG>(w * o22);
-                    G1[gcol(9 + g)] = static_cast<TG>(w * p21);
-                    G1[gcol(18 + 9 + g)] = static_cast<TG>(w * p22);
-                    Gu[g] = g12;
-                    Gu[9 + g] = g22;
-                    G[(4 * qp) * 56 + gcol(18 + g)] = static_cast<TG>(wJ * k12);
-                    Kk[g] = k22;
-                } else if (act && g < 15) {
-                    // Fd + Fi - Fe - Fg (calculate_force_FD.hpp, calculate_inertial_force.hpp,
-                    // calculate_gravity_force.hpp; Fe = 0)
-                    const int c = g - 9;
-                    const double mass = ms[0];
-                    const double eta[3] = {ms[1], ms[2], ms[3]};
-                    double fd = 0., fi, fgv;
-                    if (c < 3) {
-                        double wxe[3], wxwxe[3], wdxe[3];
-                        cross3(om, eta, wxe);
-                        cross3(om, wxe, wxwxe);
-                        cross3(omd, eta, wdxe);
-                        fi = mass * ud[c] + mass * (wxwxe[c] + wdxe[c]);
-                        fgv = mass * KB.gravity[c];
-                    } else {
-                        const int i = c - 3;
-                        for (int k = 0; k < 3; ++k) fd += tilde_e(sv3, k, i) * fcv[k];
-                        double exu[3], rw[3], rwd[3], wxrw[3];
-                        cross3(eta, ud, exu);
-                        for (int r = 0; r < 3; ++r) {
-                            rw[r] = Mu[(3 + r) * 6 + 3] * om[0] + Mu[(3 + r) * 6 + 4] * om[1] +
-                                    Mu[(3 + r) * 6 + 5] * om[2];
-                            rwd[r] = Mu[(3 + r) * 6 + 3] * omd[0] + Mu[(3 + r) * 6 + 4] * omd[1] +
-                                     Mu[(3 + r) * 6 + 5] * omd[2];
-                        }
-                        cross3(om, rw, wxrw);
-                        fi = mass * exu[i] + rwd[i] + wxrw[i];
-                        const double mg[3] = {mass * KB.gravity[0], mass * KB.gravity[1],
-                                              mass * KB.gravity[2]};
-                        double exg[3];
-                        cross3(eta, mg, exg);
-                        fgv = exg[i];
-                    }
-                    Fdig[qp * 6 + c] = fd + fi - fgv;
-                }
-                __syncwarp();
-                // (6) Quu_22 = SS^T (C11 SS - N~) joins Kuu_22; XI = beta' Muu + gamma' Guu;
-                //     G rows 4q+0: wJ [XI left | XK right | XI right], 4q+2: (w/J) [Cuu]
-                if (act) {
-                    const double wJ = qpw[qp * 4 + 2], wdJ = qpw[qp * 4 + 3];
-                    TG* G0 = G + (4 * qp) * 56;
-                    TG* G2 = G + (4 * qp + 2) * 56;
-                    if (g < 9) {
-                        const int i = g / 3, j = g % 3;
-                        double qv = 0.;
-                        for (int k = 0; k < 3; ++k) qv += tilde_e(sv3, k, i) * O12[k * 3 + j];
-                        G0[gcol(18 + 9 + g)] = static_cast<TG>(wJ * (Kk[g] + qv));
-                    }
-                    for (int e = g; e < 36; e += 16) {
-                        const int i = e / 6, j = e % 6;
-                        double gg = 0.;
-                        if (j >= 3) gg = Gu[(i < 3 ? 0 : 9) + (i % 3) * 3 + (j - 3)];
-                        const double xi = P.beta_prime * Mu[e] + P.gamma_prime * gg;
-                        const int col = (j < 3) ? i * 3 + j : 36 + i * 3 + (j - 3);
-                        G0[gcol(col)] = static_cast<TG>(wJ * xi);
-                        G2[gcol((j < 3) ? i * 3 + j : 18 + i * 3 + (j - 3))] = static_cast<TG>(wdJ * Cu[e]);
-                    }
-                }
-                __syncwarp();
-            }
-        }
+        qp_phase<TG, NT>(N, Q, phi, dphiJ, qpw, sq, sv, svd, slab, L, KB.gravity, P.beta_prime,
+                         P.gamma_prime, gscr, G, Fc, Fdig);
         __syncthreads();
         mark(kPhaseQuadrature);
 
@@ -2471,9 +2613,10 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
         //      refinement), else the panel LU.  x1 -> xs[0:m], x2 -> x2[0:m].
         constexpr bool kInv = sizeof(TR) == 4;
         const int nrhs = drive ? 2 : 1;
-        const bool use_gj = P.solver == KYN_SOLVER_GAUSS_JORDAN && m > 0 && (m & 1) == 0 &&
+        const bool use_gj = GJ && P.solver == KYN_SOLVER_GAUSS_JORDAN && m > 0 && (m & 1) == 0 &&
                             gj_fits<TR, NT>(m, kInv ? m : m + nrhs);
         if (use_gj) {
+          if constexpr (GJ) {
             TR R[GJTile<TR, NT>::RT][GJTile<TR, NT>::CT];
             gj_eliminate<TR, NT, kInv>(A, ldA, m, nrhs, reinterpret_cast<TR*>(smem_raw + S.G), &s_flag, R);
             mark(kPhaseFactor);
@@ -2599,6 +2742,7 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
                 }
                 mark(kPhaseRefine);
             }
+          }
         } else {
             // (S3) LU without pivoting of the free block A[0:m][0:m]; the right-hand
             //      side in column m is eliminated with it.  Right-looking, panels of

@@ -26,6 +26,12 @@ constexpr int kMaxNewtonIters = 64;      // convergence-history capacity
 constexpr int kRefineSweeps = 8;         // FP32 form: most refinement sweeps per linear solve
 constexpr double kRefineTol = 1e-10;     // FP32 form: backward error the sweeps aim for
 constexpr int kDenseModelMaxDofs = 120;  // unknowns of a model solved as a dense bordered system
+// A dense model with beam elements keeps each beam component's constant data
+// (a slab in SlabLayout(Nc, Qc)) after its own records; a header of
+// kCompHead doubles per component precedes them: [offset of the component's
+// slab from the header start, Nc, Qc, model node of each local node (32)].
+constexpr int kCompHead = 35;
+constexpr int kMaxDenseComps = 8;
 constexpr int kThreads = 256;            // threads per CTA of the step kernel
 
 // Offsets (in doubles) of the arrays inside one beam slab.
@@ -147,6 +153,9 @@ struct KBeam {
     int32_t con_base[kMaxBeamConstraints];   // dense models: joint base node (local), or -1
     int32_t hub_con_type;     // KYN_CONSTRAINT_FIXED_BC / PRESCRIBED_BC on the hub
     double gravity[3];
+    const double* comps;      // dense models with beams: component records (kCompHead), or null
+    int32_t n_comps;          // beam components (connected element groups) of a dense model
+    int32_t comp_maxN, comp_maxQ;  // their largest node and quadrature-point counts
     double* conv;             // [kMaxNewtonIters] model convergence history (rank 0)
     double* dump;             // optional: last assembled system (see kyn_capi.cu)
     unsigned long long* prof; // optional: per-phase SM cycles, summed over beams

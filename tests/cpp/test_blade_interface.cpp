@@ -135,10 +135,50 @@ static void static_curled_beam() {
     }
 }
 
+// TwoBeams (test_blade_interface.cpp:312-372): two order-3 beams built by
+// BeamBuilder from a straight axis, the second moved 10 m along x, a
+// PrescribedBC at the first root and a RigidJoint from the first tip to the
+// second root (one dense bordered system); every one of 1000 steps converges.
+static void two_beams() {
+    components::BeamBuilder builder;
+    const int n_nodes = 4;
+    builder.SetElementOrder(n_nodes - 1).PrescribedRootMotion(false)
+        .SetRootPosition({0., 0., 0., 1., 0., 0., 0.}).AddRefAxisTwist(0., 0.).AddRefAxisTwist(1., 0.);
+    const int n_kps = 12;
+    for (int i = 0; i < n_kps; ++i) {
+        const double s = static_cast<double>(i) / (n_kps - 1);
+        builder.AddRefAxisPoint(s, {10. * s, 0., 0.}, components::ReferenceAxisOrientation::X);
+    }
+    for (int i = 0; i <= 20; ++i)
+        builder.AddSection(
+            0.05 * i,
+            {{{8.538e-2, 0., 0., 0., 0., 0.}, {0., 8.538e-2, 0., 0., 0., 0.}, {0., 0., 8.538e-2, 0., 0., 0.},
+              {0., 0., 0., 1.4433e-2, 0., 0.}, {0., 0., 0., 0., 0.40972e-2, 0.}, {0., 0., 0., 0., 0., 1.0336e-2}}},
+            {{{1368.17e3, 0., 0., 0., 0., 0.}, {0., 88.56e3, 0., 0., 0., 0.}, {0., 0., 38.78e3, 0., 0., 0.},
+              {0., 0., 0., 16.9600e3, 17.6100e3, -0.3510e3}, {0., 0., 0., 17.6100e3, 59.1200e3, -0.3700e3},
+              {0., 0., 0., -0.3510e3, -0.3700e3, 141.470e3}}},
+            components::ReferenceAxisOrientation::X);
+    Model model({0., 0., -9.81});
+    components::Beam beam_1(builder.Input(), model);
+    components::Beam beam_2(builder.Input(), model);
+    for (auto& node : beam_2.nodes) model.GetNode(node.id).x0[0] += 10.;
+    model.AddPrescribedBC(beam_1.nodes[0].id);
+    model.AddRigidJointConstraint({beam_1.nodes[n_nodes - 1].id, beam_2.nodes[0].id});
+    const StepParameters parameters(true, 6, 0.01, 0.);
+    auto [state, elements, constraints, solver] = model.CreateSystemWithSolver(Context(0));
+    for (int i = 0; i < 1000; ++i)
+        if (!Step(parameters, solver, elements, state, constraints)) {
+            std::printf("FAIL two beams: step %d did not converge\n", i);
+            ++failures;
+            return;
+        }
+}
+
 int main(int argc, char** argv) {
     try {
         if (argc > 1) blade_windio(argv[1]);
         static_curled_beam();
+        two_beams();
         const double time_step = 0.01;
         const std::array<double, 3> omega{0., 0., 1.};
         const std::array<double, 3> x0_root{2., 0., 0.};

@@ -37,6 +37,9 @@ MODELS = {
     "spring_mass": lambda: R.spring_mass_model(),
     "spring_mass_chain": lambda: R.spring_mass_chain_model(),
     "two_element_cantilever": lambda: R.two_element_cantilever_model(),
+    "two_beams_rigid_joint": lambda: R.two_beams_model(),
+    "moored_cantilever": lambda: R.moored_cantilever_model(),
+    "three_row_bc_on_a_beam": lambda: _cantilever_with(lambda m: m.AddFixedBC3DOFs(4)),
     "batch_rotor": lambda: W.rotor_model(3),
     "batch_cantilever": lambda: W.batch_cantilever_model(W.draw_batch(1, first_id=77)[0]),
 }
@@ -60,13 +63,11 @@ def _cantilever_with(extra):
     return m
 
 
-@pytest.mark.parametrize("case", ["three_row_bc_on_a_beam", "two_revolute_joints",
+@pytest.mark.parametrize("case", ["two_revolute_joints",
                                   "revolute_between_beam_nodes", "revolute_in_a_dense_model",
                                   "free_node_outside_the_beams"])
 def test_topologies_outside_the_path_are_refused(case):
-    if case == "three_row_bc_on_a_beam":
-        m = _cantilever_with(lambda m: m.AddFixedBC3DOFs(4))
-    elif case == "two_revolute_joints":
+    if case == "two_revolute_joints":
         m = R.generator_torque_model(0.0)[0]
         n = m.AddNode().SetPosition(0., 0., 5., 1., 0., 0., 0.).Build()
         m.AddRevoluteJointConstraint([len(m.nodes_) - 4, n], [0., 0., 1.], np.zeros(1))

@@ -11,8 +11,9 @@ import os
 
 import numpy as np
 
-from openturbine_b200.model import (BeamSection, Model, RotateVectorByQuaternion,
-                                    RotationVectorToQuaternion, StepParameters)
+from openturbine_b200.model import (BeamSection, CreateTrapezoidalQuadrature, GenerateGLLPoints,
+                                    Model, RotateVectorByQuaternion, RotationVectorToQuaternion,
+                                    StepParameters)
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
@@ -405,3 +406,51 @@ def two_element_cantilever_loads(step: int) -> np.ndarray:
     fx = np.zeros((6, 6))
     fx[3, 2] = 100. * math.sin(10.0 * 0.005 * (step + 1))
     return fx
+
+
+# ---- beams in one dense bordered system --------------------------------------------
+def two_beams_model():
+    """BladeInterfaceTest.TwoBeams (tests/regression_tests/interfaces/
+    test_blade_interface.cpp:312-372): two straight 10 m beams of order 3 along
+    x, built like components::BeamBuilder builds them from a straight reference
+    axis (GLL nodes, 21 sections at s = 0, 0.05, ..., 1 with the test's
+    diagonal mass and coupled stiffness, trapezoidal quadrature at the
+    sections), the second moved 10 m along x; a PrescribedBC at the first
+    beam's root and a RigidJoint from its tip to the second beam's root;
+    gravity -9.81 z; StepParameters(true, 6, 0.01, 0)."""
+    section_s = [0.05 * k for k in range(21)]
+    mass = np.diag([8.538e-2, 8.538e-2, 8.538e-2, 1.4433e-2, 0.40972e-2, 1.0336e-2])
+    stiff = np.diag([1368.17e3, 88.56e3, 38.78e3, 16.96e3, 59.12e3, 141.47e3])
+    stiff[3, 4] = stiff[4, 3] = 17.61e3
+    stiff[3, 5] = stiff[5, 3] = -0.351e3
+    stiff[4, 5] = stiff[5, 4] = -0.37e3
+    secs = [BeamSection(s, mass, stiff) for s in section_s]
+    quad = CreateTrapezoidalQuadrature(section_s)
+    m = Model()
+    m.SetGravity(0., 0., -9.81)
+    beams = []
+    for b in range(2):
+        ids = [m.AddNode().SetElemLocation(s).SetPosition(10. * s + 10. * b, 0., 0., 1., 0., 0., 0.).Build()
+               for s in [(x + 1.) / 2. for x in GenerateGLLPoints(3)]]
+        m.AddBeamElement(ids, secs, quad)
+        beams.append(ids)
+    m.AddPrescribedBC(beams[0][0])
+    m.AddRigidJointConstraint([beams[0][-1], beams[1][0]])
+    return m, StepParameters(True, 6, 0.01, 0.)
+
+
+def moored_cantilever_model():
+    """The cantilever of test_cantilever_beam.cpp with a mooring line at its
+    tip (the floating platform's line of test_cfd_interface.cpp on a beam): a
+    position-only fairlead node carried by a RigidJoint6DOFsTo3DOFs from the tip,
+    a spring to a position-only anchor held by a FixedBC3DOFs; the tip also
+    carries a point mass.  Solved as one dense system."""
+    m, p = cantilever_test_model()
+    tip = 4
+    fair = m.AddNode().SetPosition(10., 0., -1., 1., 0., 0., 0.).Build()
+    anchor = m.AddNode().SetPosition(10., 0., -21., 1., 0., 0., 0.).Build()
+    m.AddRigidJoint6DOFsTo3DOFs([tip, fair])
+    m.AddSpringElement(fair, anchor, 5.0e3, 19.0)
+    m.AddFixedBC3DOFs(anchor)
+    m.AddMassElement(tip, np.diag([50., 50., 50., 5., 5., 5.]))
+    return m, p
