@@ -224,6 +224,8 @@ def main() -> None:
     ap.add_argument("--solver", type=int, default=1,
                     help="free-block solve of the headline legs: 1 panel LU (default), 0 Gauss-Jordan "
                          "in registers (panel LU where the block does not fit)")
+    ap.add_argument("--bulk-sections", type=int, default=1,
+                    help="1: sections staged by one bulk copy per Newton iteration, 0: per-point loads")
     ap.add_argument("--nodes", type=int, default=0,
                     help="uniform nodes per beam (0: the batch's U{5..21}); for profiling one bucket")
     args = ap.parse_args()
@@ -253,6 +255,7 @@ def main() -> None:
         draws = [W.BeamDraw(d.model_id, args.nodes, d.length, d.amp, d.freq) for d in draws]
     ctx = Context(local)
     ctx.set_linear_solver(args.solver)
+    ctx.set_bulk_sections(bool(args.bulk_sections))
     if not args.no_graph:
         ctx.set_cuda_graph(True)   # each step replays the captured bucket launches
     t_setup = time.perf_counter()

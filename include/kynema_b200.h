@@ -367,8 +367,12 @@ enum {
                                   set or the step coefficients change) */
     KYN_OPT_LINEAR_SOLVER = 4, /* KYN_SOLVER_*: how the step kernel solves a beam's
                                   free block (default KYN_SOLVER_PANEL_LU) */
-    KYN_OPT_RESET_SOLVE_STATS = 5 /* any value: zero the KYN_STAT_SOLVES_CHECKED ..
-                                     KYN_STAT_REFINE_SHORT counters */
+    KYN_OPT_RESET_SOLVE_STATS = 5, /* any value: zero the KYN_STAT_SOLVES_CHECKED ..
+                                      KYN_STAT_REFINE_SHORT counters */
+    KYN_OPT_BULK_SECTIONS = 6  /* 1 (default): each Newton iteration's sectional
+                                  data (x0', r0, M*, C*) reach shared memory in one
+                                  bulk copy issued during the previous iteration;
+                                  0: every quadrature point loads its own */
 };
 
 /* Free-block solves of the step kernel (the reference's sparse direct solve,

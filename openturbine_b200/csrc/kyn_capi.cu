@@ -199,6 +199,7 @@ struct kyn_ctx {
     int smem_configured = 0;
     bool use_graph = false;               // KYN_OPT_CUDA_GRAPH
     int solver = KYN_SOLVER_PANEL_LU;     // KYN_OPT_LINEAR_SOLVER
+    int bulk_sections = 1;                // KYN_OPT_BULK_SECTIONS
     double* h_stage = nullptr;            // pinned staging for loads
     size_t h_stage_len = 0;
     std::unique_ptr<XferPlan> xfer[4];    // cached transfer plans
@@ -273,6 +274,7 @@ StepCoeffs make_coeffs(const kyn_ctx* c, const kyn_step_params* p) {
     StepCoeffs P{};
     P.solver = c->solver;
     P.diag = c->d_diag;
+    P.bulk_sections = c->bulk_sections;
     const bool fp32 = p->precision == KYN_PRECISION_FP32_REFINED;
     P.refine_sweeps = fp32 ? kRefineSweeps : 0;
     P.refine_tol = fp32 ? kRefineTol : 0.;
@@ -942,6 +944,10 @@ int kyn_ctx_set_option(kyn_ctx* c, int option, int64_t value) {
             }
         }
         c->plan.reset();
+        return KYN_OK;
+    }
+    if (option == KYN_OPT_BULK_SECTIONS) {
+        c->bulk_sections = value != 0;
         return KYN_OK;
     }
     if (option == KYN_OPT_RESET_SOLVE_STATS) {

@@ -108,6 +108,54 @@ __device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double
                  : "d"(a), "d"(b));
 }
 
+// ---- bulk copies into shared memory (cp.async.bulk, completion on an mbarrier) --
+// One thread arms the barrier with the byte count and issues the copy; every
+// thread that reads the data waits on the barrier's phase parity.  The copy
+// is a plain (non-multicast) global -> own-CTA shared-memory transfer.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+// src, dst 16-byte aligned, bytes a multiple of 16.  Every thread that
+// accessed the destination through ordinary loads and stores runs
+// proxy_fence_async_smem() before the CTA barrier that precedes this call.
+__device__ __forceinline__ void proxy_fence_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+// Waits for phase `parity` of the barrier, at most kBulkWaitTries polls;
+// false when it gave up.
+constexpr int kBulkWaitTries = 1 << 22;
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    const uint32_t b = smem_u32(bar);
+    for (int i = 0; i < kBulkWaitTries; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(b), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Doubles of one beam system's per-point section data as it lies in the slab
+// from x0' on: x0' [Q][3] (padded to even), r0 [Q][4], M* [Q][36], C* [Q][36]
+// (SlabLayout keeps them contiguous); staged per Newton iteration.
+__host__ __device__ inline int sec_doubles(int Q) { return ((3 * Q + 1) & ~1) + 76 * Q; }
+
 // ---- shared-memory plan of one CTA --------------------------------------------
 // The kernel runs with NT = 128, 256 or 512 threads (up to four, two or one
 // CTAs per SM within the 128-register budget); NT/16 quadrature points are
@@ -158,6 +206,9 @@ struct Smem {
     int red;            // double [2][NT/32 + 8]  (offset 0: cluster exchange)
     int hub;            // double [kHubSmem or kDriveSmem] hub state and records, or -1
     int pos;            // int [N]
+    int sec;            // double [sec_doubles(Q)] staged sections, inside A's region after
+                        // the group scratch (quadrature phase only)
+    int bar;            // uint64 mbarrier of the section copies
     int bytes;
     int ldA;
 };
@@ -183,7 +234,8 @@ __host__ __device__ inline int gj_scratch_bytes(int N, int real_bytes, int nt) {
 
 // The system matrix and the quadrature scratch never live at the same time:
 // A is assembled after the quadrature phase and consumed by the solve, so the
-// two share one region.
+// two share one region; so do the sections staged for the next quadrature
+// phase, copied in once the solve has read A for the last time.
 // hub: 0 none, 1 a hub node, 2 a drive train (hub chain of 2 or 3 nodes).
 __host__ __device__ inline Smem make_smem(int N, int Q, int nc, int real_bytes, int nt, int hub = 0) {
     Smem S{};
@@ -202,7 +254,9 @@ __host__ __device__ inline Smem make_smem(int N, int Q, int nc, int real_bytes, 
     {
         const int a_bytes = n6 * S.ldA * real_bytes;
         const int g_bytes = (nt / 16) * kGroupScratch * 8;
-        S.A = take(a_bytes > g_bytes ? a_bytes : g_bytes);
+        const int q_bytes = g_bytes + sec_doubles(Q) * 8;
+        S.A = take(a_bytes > q_bytes ? a_bytes : q_bytes);
+        S.sec = S.A + g_bytes;
     }
     // FP64 form: G in FP64, one k-step per point.  FP32 form: G in FP32 and
     // k-steps of two points (m16n8k8), so an odd Q gets one zero pad point.
@@ -231,6 +285,7 @@ __host__ __device__ inline Smem make_smem(int N, int Q, int nc, int real_bytes, 
     S.stage = take(64 * 8);
     S.con = take((nc > 0 ? nc : 1) * kConStride * 8);
     S.pos = take(N * 4);
+    S.bar = take(8);
     S.bytes = o;
     return S;
 }
@@ -1328,13 +1383,15 @@ __host__ __device__ inline DenseSmem make_dense_smem(int N, int nd, int nt = 128
 // (shared memory), the system's slab for the sections and reference frames
 // (layout L).  Outputs: Fc, Fd + Fi - Fg [Q][6] and the weighted blocks of the
 // integration GEMM G [4Q][56] (column layout gcol).  gscr: NT/16 groups of
-// kGroupScratch doubles.
+// kGroupScratch doubles.  sec: the sections already staged in shared memory
+// (sec_doubles(Q), slab order from x0'), or null to read them from the slab.
 template <typename TG, int NT>
 __device__ __forceinline__ void qp_phase(int N, int Q, const double* phi, const double* dphiJ,
                                          const double* qpw, const double* sq, const double* sv,
                                          const double* svd, const double* __restrict__ slab,
                                          const SlabLayout& L, const double* gravity, double beta_prime,
-                                         double gamma_prime, double* gscr, TG* G, double* Fc, double* Fdig) {
+                                         double gamma_prime, double* gscr, TG* G, double* Fc, double* Fdig,
+                                         const double* sec = nullptr) {
     constexpr int NG = NT / 16;
     const int tid = threadIdx.x;
     const int grp = tid >> 4;
@@ -1359,10 +1416,18 @@ __device__ __forceinline__ void qp_phase(int N, int Q, const double* phi, const 
         const int qp = q0 + grp;
         const bool act = qp < Q;
         const double* ph_q = phi + qp * N;
+        if (sec) {  // staged by the bulk copy: this point's entries in place
+            const int qc = act ? qp : 0;
+            const int o_r0 = (3 * Q + 1) & ~1;
+            x0p = sec + qc * 3;
+            r0 = sec + o_r0 + qc * 4;
+            mst = sec + o_r0 + 4 * Q + qc * 36;
+            cst = mst + 36 * Q;
+        }
         if (act) {
             // stage this point's sections and reference frame from the slab
             // (read early: the loads overlap the interpolation below)
-            for (int k = g; k < 79; k += 16) {
+            for (int k = g; k < 79 && !sec; k += 16) {
                 double v;
                 if (k < 36) v = slab[L.mstar + qp * 36 + k];
                 else if (k < 72) v = slab[L.cstar + qp * 36 + (k - 36)];
@@ -2147,6 +2212,25 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
     int* pos = reinterpret_cast<int*>(smem_raw + S.pos);
     __shared__ int s_flag;
     __shared__ unsigned long long s_ph[kNumPhases];
+    // sections of the next quadrature phase: one bulk copy per Newton
+    // iteration (slab from x0' on -> the A region after the group scratch)
+    uint64_t* sec_bar = reinterpret_cast<uint64_t*>(smem_raw + S.bar);
+    double* sec = reinterpret_cast<double*>(smem_raw + S.sec);
+    const uint32_t sec_bytes = static_cast<uint32_t>(sec_doubles(Q)) * 8u;
+    uint32_t sec_issued = 0, sec_waited = 0;  // copies issued / completed (thread 0 issues)
+    const bool bulk = P.bulk_sections != 0;
+    auto sec_prefetch = [&]() {  // all threads, once every use of the region has ended
+        if (!bulk) return;
+        proxy_fence_async_smem();
+        __syncthreads();
+        if (tid == 0) bulk_copy_g2s(sec, slab + L.x0p, sec_bytes, sec_bar);
+        ++sec_issued;
+    };
+    auto sec_wait = [&]() {  // all threads
+        if (!bulk) return;
+        if (!mbar_wait(sec_bar, sec_waited & 1u) && tid == 0) atomicOr(&s_flag, 8);
+        ++sec_waited;
+    };
 
     const double h = P.h;
     // Optional phase timing: thread 0 reads the SM clock at phase boundaries
@@ -2212,8 +2296,10 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
         }
         for (int c = 0; c < nc; ++c) pos[KB.con_node[c]] = p++;
         s_flag = 0;
+        mbar_init(sec_bar);
     }
     __syncthreads();
+    sec_prefetch();
 
     if (sizeof(TR) == 4 && (Q & 1))  // zero pad point of the FP32 integration GEMM
         for (int k = tid; k < 4 * 56; k += NT) G[4 * Q * 56 + k] = TG(0);
@@ -2301,8 +2387,9 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
         if (hub && chain_rec()) tangent_op(chain_rec() + hubrec::q_delta, chain_rec() + hubrec::tangent);
 
         // ---- quadrature-point values (calculate_quadrature_point_values.hpp) ---
+        sec_wait();
         qp_phase<TG, NT>(N, Q, phi, dphiJ, qpw, sq, sv, svd, slab, L, KB.gravity, P.beta_prime,
-                         P.gamma_prime, gscr, G, Fc, Fdig);
+                         P.gamma_prime, gscr, G, Fc, Fdig, bulk ? sec : nullptr);
         __syncthreads();
         mark(kPhaseQuadrature);
 
@@ -2923,6 +3010,7 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
         }
 
         __syncthreads();
+        sec_prefetch();  // A is not read again in this iteration
         mark(kPhaseSubstitute);
 
         // ---- convergence error (calculate_error_sum_squares.hpp:33-79) --------------
@@ -3117,6 +3205,11 @@ __global__ void __launch_bounds__(NT, step_min_blocks(sizeof(TR), NT))
             break;
         }
     }
+
+    // the copy issued in the last iteration lands before the region is released
+    while (sec_waited < sec_issued) sec_wait();
+    __syncthreads();
+    if (s_flag & 8) status = KYN_ERR_CUDA;  // a section copy did not complete in time
 
     // ---- post-step (step.hpp:86-121) ---------------------------------------------------
     if (status == KYN_OK) {

@@ -190,6 +190,7 @@ struct StepCoeffs {
     int32_t refine_sweeps; // FP32 form: most refinement sweeps of one linear solve
     double refine_tol;     // FP32 form: target relative FP64 residual of the linear solve
     unsigned long long* diag;  // solve counters (kDiag*), or null
+    int32_t bulk_sections;     // 1: stage each iteration's sections with one bulk copy
 };
 
 // Solve counters of a context (StepCoeffs::diag), summed over the beams of

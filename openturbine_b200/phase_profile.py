@@ -30,11 +30,14 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--nodes", type=int, default=13, help="0: the mixed batch (U{5..21})")
     ap.add_argument("--precision", type=int, default=0)
-    ap.add_argument("--solver", type=int, default=0,
-                    help="0: Gauss-Jordan in registers where it fits, 1: panel LU")
+    ap.add_argument("--solver", type=int, default=1,
+                    help="1: panel LU (default), 0: Gauss-Jordan in registers where it fits")
+    ap.add_argument("--bulk-sections", type=int, default=1,
+                    help="1: sections staged by one bulk copy per iteration, 0: per-point loads")
     args = ap.parse_args()
     ctx = Context(0)
     ctx.lib.kyn_ctx_set_option(ctx.h, OPT_LINEAR_SOLVER, args.solver)
+    ctx.set_bulk_sections(bool(args.bulk_sections))
     draws = W.draw_batch(args.beams)
     if args.nodes:
         draws = [W.BeamDraw(d.model_id, args.nodes, d.length, d.amp, d.freq) for d in draws]
@@ -58,6 +61,7 @@ def main() -> None:
     cyc = [ctx.stat(100 + i) for i in range(len(PHASES))]
     print(json.dumps({"beams": args.beams, "nodes": args.nodes or "mixed",
                       "precision": args.precision, "solver": args.solver,
+                      "bulk_sections": args.bulk_sections,
                       "beam_iterations": iters,
                       "cycles_per_beam_iteration": {n: round(c / max(iters, 1))
                                                     for n, c in zip(PHASES, cyc)}}))

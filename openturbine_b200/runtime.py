@@ -25,7 +25,7 @@ WIDTH = {"x0": 7, "x": 7, "q": 7, "q_prev": 7, "q_delta": 6, "v": 6, "vd": 6, "a
          "lambda": 6, "tangent": 36, "output": 3}
 LOAD_NODE_FX, LOAD_STATE_F = 0, 1
 OPT_RECORD_SYSTEM, OPT_PHASE_TIMING, OPT_CUDA_GRAPH, OPT_LINEAR_SOLVER = 1, 2, 3, 4
-OPT_RESET_SOLVE_STATS = 5
+OPT_RESET_SOLVE_STATS, OPT_BULK_SECTIONS = 5, 6
 SOLVER_GAUSS_JORDAN, SOLVER_PANEL_LU = 0, 1
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -244,6 +244,11 @@ class Context:
     def allocations(self) -> int:
         """Device and pinned-host allocations made by this context so far."""
         return self.stat(3)
+
+    def set_bulk_sections(self, on: bool) -> None:
+        """Stage each iteration's sections with one bulk copy (default) or let
+        every quadrature point load its own."""
+        self._check(self.lib.kyn_ctx_set_option(self.h, OPT_BULK_SECTIONS, int(on)))
 
     def reset_solve_stats(self) -> None:
         self._check(self.lib.kyn_ctx_set_option(self.h, OPT_RESET_SOLVE_STATS, 1))
