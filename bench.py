@@ -53,15 +53,42 @@ def _hbm_peak() -> float | None:
         return None
 
 
-def algorithmic_flops(N: int, Q: int, iters: int, f_qp: float) -> float:
+# FLOPs of the quadrature-point physics (interpolation, sections rotated,
+# inertial and elastic forces and blocks) per point of an N-node beam, counted
+# in the oracle's operation order by its counting build (ORC_COUNT_FLOPS;
+# tests/test_flop_count.py re-derives both constants).
+QP_FLOPS_FIXED = 3112.0
+QP_FLOPS_PER_NODE = 55.0
+
+
+def qp_flops(N: int) -> float:
+    return QP_FLOPS_FIXED + QP_FLOPS_PER_NODE * N
+
+
+def algorithmic_flops(N: int, Q: int, iters: int) -> float:
     """FLOPs of one beam for `iters` Newton iterations (per-iteration count:
-    Q*F_qp + 410 N^2 Q + 468 N^2 + 48 N Q + (2/3) n^3 + 2 n^2, n = 6N + 6)."""
+    Q*F_qp(N) + 410 N^2 Q + 468 N^2 + 48 N Q + (2/3) n^3 + 2 n^2, n = 6N + 6)."""
     n = 6 * N + 6
-    per = Q * f_qp + 410.0 * N * N * Q + 468.0 * N * N + 48.0 * N * Q + (2.0 / 3.0) * n ** 3 + 2.0 * n * n
+    per = (Q * qp_flops(N) + 410.0 * N * N * Q + 468.0 * N * N + 48.0 * N * Q + (2.0 / 3.0) * n ** 3
+           + 2.0 * n * n)
     return per * iters
 
 
-F_QP = 2500.0  # flops of the quadrature-point physics per point (frozen estimate)
+def rank_draws(rank: int, beams: int, nodes: int = 0) -> list:
+    """This rank's batch under weak scaling: its own `beams` beams of the
+    workload (model ids rank*beams ...), every node count `nodes` if nonzero."""
+    draws = W.draw_batch(beams, first_id=S.weak_shard_first_id(rank, beams))
+    if nodes:
+        draws = [W.BeamDraw(d.model_id, nodes, d.length, d.amp, d.freq) for d in draws]
+    return draws
+
+
+def job_rate(local_ms: float, local_units: float, dist=None, device=None) -> tuple:
+    """Whole-job throughput of a timed region: (slowest rank's time in ms,
+    units of all ranks, units / s); the time is the max over ranks."""
+    t_ms = S.max_over_ranks(float(local_ms), dist, device)
+    units = S.sum_over_ranks(float(local_units), dist, device)
+    return t_ms, units, units / (t_ms * 1e-3)
 
 
 class ClockSampler:
@@ -200,6 +227,73 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_single_models(args) -> None:
+    """--single-models: per-step latency of the two single-model configurations
+    -- the 5-node cantilever (100 steps, tip load 1e4 sin(2 pi t)) and the
+    three-blade rotor with gravity (1000 steps, prescribed hub rotation) --
+    through kyn_step (one model per call, results on the host after each
+    call), beside the FP64 oracle on one host core.  Prints one JSON line."""
+    import torch
+    from oracle.oracle_py import OracleModel
+    from openturbine_b200.runtime import Context
+    torch.cuda.set_device(0)
+    ctx = Context(0)
+    out = {"metric": "step latency of single models", "unit": "ms", "higher_is_better": False,
+           "n_gpus": 1, "dtype": "f64", "data": "synthetic", "configs": {}}
+
+    def cantilever():
+        m = W.cantilever_model()
+        p = W.cantilever_params()
+
+        def inputs(k, setter):
+            fx = np.zeros((5, 6))
+            fx[4, 2] = W.cantilever_tip_load(k)
+            setter(fx)
+        return m, p, 100, inputs
+
+    def rotor():
+        m, bcs = W.rotor_model(3)
+        p = W.rotor_params()
+
+        def inputs(k, setter):
+            for c, u in zip(bcs, W.rotor_root_inputs(m, bcs, k)):
+                setter(c, u)
+        return m, p, 1000, inputs
+
+    for name, make in (("cantilever 5 nodes, 100 steps", cantilever),
+                       ("three-blade rotor 11 nodes per blade, gravity, 1000 steps", rotor)):
+        m, p, steps, inputs = make()
+        pm = m.pack()
+        mid = ctx.create_model(pm)
+        orc = OracleModel(pm)
+        gpu_ms, cpu_ms, iters = [], [], 0
+        for k in range(steps):
+            if name.startswith("cantilever"):
+                inputs(k, lambda fx: ctx.set_node_fx(mid, fx))
+                inputs(k, orc.set_node_fx)
+            else:
+                inputs(k, lambda c, u: ctx.set_prescribed(mid, c, u))
+                inputs(k, orc.set_prescribed)
+            t0 = time.perf_counter()
+            st, it = ctx.step([mid], p)
+            gpu_ms.append((time.perf_counter() - t0) * 1e3)
+            t0 = time.perf_counter()
+            orc.step(p)
+            cpu_ms.append((time.perf_counter() - t0) * 1e3)
+            iters += int(it[0])
+        g = np.array(gpu_ms[3:])
+        c = np.array(cpu_ms[3:])
+        out["configs"][name] = {
+            "gpu_ms": {"p50": float(np.percentile(g, 50)), "p99": float(np.percentile(g, 99))},
+            "oracle_1_core_ms": {"p50": float(np.percentile(c, 50)), "p99": float(np.percentile(c, 99))},
+            "newton_iters_per_step": iters / steps,
+            "tip_rel_err_vs_oracle": float(np.abs(ctx.state(mid, "q") - orc.state("q")).max()
+                                           / max(np.abs(orc.state("q")).max(), 1e-300))}
+        ctx.destroy_model(mid)
+    ctx.close()
+    print(json.dumps(out), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -224,6 +318,8 @@ def main() -> None:
     ap.add_argument("--solver", type=int, default=1,
                     help="free-block solve of the headline legs: 1 panel LU (default), 0 Gauss-Jordan "
                          "in registers (panel LU where the block does not fit)")
+    ap.add_argument("--single-models", action="store_true",
+                    help="time the single cantilever and rotor configurations instead")
     ap.add_argument("--bulk-sections", type=int, default=1,
                     help="1: sections staged by one bulk copy per Newton iteration, 0: per-point loads")
     ap.add_argument("--nodes", type=int, default=0,
@@ -233,6 +329,9 @@ def main() -> None:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.single_models:
+        run_single_models(args)
         return
 
     import torch
@@ -250,9 +349,7 @@ def main() -> None:
     from openturbine_b200.runtime import LOAD_NODE_FX, Context
 
     # ---- build the shard: weak scaling, each rank owns its own 4096 beams ----
-    draws = W.draw_batch(args.beams, first_id=S.weak_shard_first_id(rank, args.beams))
-    if args.nodes:
-        draws = [W.BeamDraw(d.model_id, args.nodes, d.length, d.amp, d.freq) for d in draws]
+    draws = rank_draws(rank, args.beams, args.nodes)
     ctx = Context(local)
     ctx.set_linear_solver(args.solver)
     ctx.set_bulk_sections(bool(args.bulk_sections))
@@ -330,7 +427,7 @@ def main() -> None:
             conv += int((st == 0).sum())
             ok_all &= st == 0
             iters += int(it.sum())
-            flops += sum(algorithmic_flops(int(nodes[i]), int(qps[i]), int(it[i]), F_QP)
+            flops += sum(algorithmic_flops(int(nodes[i]), int(qps[i]), int(it[i]))
                          for i in range(len(step_ids)))
         torch.cuda.synchronize()
         if dist:
@@ -349,9 +446,7 @@ def main() -> None:
     tuned64 = tune(ids, params)
     r64 = device_leg(ids, params, True)
     dev_ms, conv_v, flops_v, launches = r64["ms"], r64["conv"], r64["flops"], r64["launches"]
-    t_value_ms = S.max_over_ranks(float(sum(dev_ms)), dist, dev)
-    conv_all = int(S.sum_over_ranks(conv_v, dist, dev))
-    value = conv_all / (t_value_ms * 1e-3)
+    t_value_ms, conv_all, value = job_rate(sum(dev_ms), conv_v, dist, dev)
 
     # ---- the FP32 forms on their own copies of the batch ------------------------
     # (a) FP32 tangent and panel LU; (b) FP32 tangent, FP32 Gauss-Jordan inverse
@@ -383,8 +478,7 @@ def main() -> None:
             r32 = device_leg(ids32, p32, False)
             after = ctx.solve_stats()
             ctx.set_linear_solver(args.solver)
-            t32 = S.max_over_ranks(float(sum(r32["ms"])), dist, dev)
-            v32 = S.sum_over_ranks(r32["conv"], dist, dev) / (t32 * 1e-3)
+            t32, _, v32 = job_rate(sum(r32["ms"]), r32["conv"], dist, dev)
             solves = after["checked"] - before["checked"]
             out = {"value": v32, "unit": "beam-steps/s", "ratio_vs_fp64": v32 / value,
                    "threads_per_cta_by_nodes": tuned32,
@@ -496,9 +590,7 @@ def main() -> None:
         ctx.get_state_batch(ids, "q", q_host.data_ptr(), False)
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
         conv_e += int((st == 0).sum())
-    t_e2e_ms = S.max_over_ranks(float(sum(e2e_ms)), dist, dev)
-    conv_e = int(S.sum_over_ranks(conv_e, dist, dev))
-    e2e = conv_e / (t_e2e_ms * 1e-3)
+    t_e2e_ms, conv_e, e2e = job_rate(sum(e2e_ms), conv_e, dist, dev)
 
     # ---- serving: Poisson request stream, continuous batching, both forms --------
     serving = None
@@ -509,7 +601,7 @@ def main() -> None:
                                "90% single beams (nodes U{5..21}), 10% three-blade rotors (11 nodes "
                                "per blade, prescribed hub rotation), U{50..500} steps per request",
                    "hbm_budget_gb": 150}
-        for name, form in (("fp64", 0), ("fp32_refined", 1)):
+        for name, form in (("fp64", 0), ("fp32", 1)):
             sctx = Context(local, 150 * 10**9)
             sctx.set_linear_solver(args.solver)
             sp = W.batch_params()
@@ -526,7 +618,7 @@ def main() -> None:
             serving[name] = srv.summary()
             sctx.close()
         if serving["fp64"]["converged_beam_steps_per_s"] > 0:
-            serving["fp32_vs_fp64"] = (serving["fp32_refined"]["converged_beam_steps_per_s"] /
+            serving["fp32_vs_fp64"] = (serving["fp32"]["converged_beam_steps_per_s"] /
                                        serving["fp64"]["converged_beam_steps_per_s"])
 
     if rank == 0:

@@ -33,6 +33,19 @@
 
 namespace {
 
+// Floating-point operation tally of the quadrature-point physics (a6-a10),
+// compiled in only with -DORC_COUNT_FLOPS (oracle/_build/libkyn_oracle_flops.so):
+// every add, subtract, multiply, divide and square root of the functions below
+// in their operation order, so that the per-point count the roofline uses is
+// counted from this restatement of the reference rather than estimated.
+#ifdef ORC_COUNT_FLOPS
+long long g_flops = 0;     // every counted operation
+long long g_qp_flops = 0;  // those of the quadrature-point loops of update_beam
+#define ORC_FLOPS(n) (g_flops += static_cast<long long>(n))
+#else
+#define ORC_FLOPS(n) ((void)0)
+#endif
+
 using V3 = std::array<double, 3>;
 using V4 = std::array<double, 4>;
 using M3 = std::array<double, 9>;
@@ -41,6 +54,7 @@ using M6 = std::array<double, 36>;
 // KokkosBatched::SerialGemm restated (row-major, strided, optional transposes).
 void gemm(bool ta, bool tb, int m, int n, int k, double alpha, const double* A, int lda,
           const double* B, int ldb, double beta, double* C, int ldc) {
+    ORC_FLOPS((beta != 0. && beta != 1. ? m * n : 0) + (alpha != 0. ? 2 * m * n * k + 2 * m * n : 0));
     if (beta == 0.) {
         for (int i = 0; i < m; ++i)
             for (int j = 0; j < n; ++j) C[i * ldc + j] = 0.;
@@ -65,6 +79,7 @@ void gemm(bool ta, bool tb, int m, int n, int k, double alpha, const double* A, 
 // KokkosBlas::SerialGemv restated: y = beta*y; y(i) += alpha * sum_j op(A)(i,j) x(j).
 void gemv(bool ta, int m, int n, double alpha, const double* A, int lda, const double* x,
           double beta, double* y) {
+    ORC_FLOPS((beta != 0. && beta != 1. ? m : 0) + (alpha != 0. ? 2 * m * n + 2 * m : 0));
     if (beta == 0.) {
         for (int i = 0; i < m; ++i) y[i] = 0.;
     } else if (beta != 1.) {
@@ -85,6 +100,7 @@ M3 tilde(const double* v) {
 
 // src/math/quaternion_operations.hpp:20-32 QuaternionToRotationMatrix
 M3 quat_to_rot(const double* q) {
+    ORC_FLOPS(45);  // 3 diagonal entries x 7, 6 off-diagonal x 4
     return M3{q[0] * q[0] + q[1] * q[1] - q[2] * q[2] - q[3] * q[3],
               2. * (q[1] * q[2] - q[0] * q[3]),
               2. * (q[1] * q[3] + q[0] * q[2]),
@@ -98,6 +114,7 @@ M3 quat_to_rot(const double* q) {
 
 // src/math/quaternion_operations.hpp:118-129 RotateVectorByQuaternion
 V3 rotate_vec(const double* q, const double* v) {
+    ORC_FLOPS(60);  // per component: 8 (diagonal term) + 2 x 5 (off-diagonal) + 2 adds
     V3 r;
     r[0] = (q[0] * q[0] + q[1] * q[1] - q[2] * q[2] - q[3] * q[3]) * v[0] +
            2. * (q[1] * q[2] - q[0] * q[3]) * v[1] + 2. * (q[1] * q[3] + q[0] * q[2]) * v[2];
@@ -111,6 +128,7 @@ V3 rotate_vec(const double* q, const double* v) {
 
 // src/math/quaternion_operations.hpp:204-211 QuaternionCompose
 V4 quat_compose(const double* a, const double* b) {
+    ORC_FLOPS(28);  // 16 multiplies, 12 adds
     return V4{a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3],
               a[0] * b[1] + a[1] * b[0] + a[2] * b[3] - a[3] * b[2],
               a[0] * b[2] - a[1] * b[3] + a[2] * b[0] + a[3] * b[1],
@@ -155,6 +173,7 @@ V3 axial(const M3& m) {
 }
 
 double nrm2(const double* v, int n) {
+    ORC_FLOPS(2 * n + 1);
     double s = 0.;
     for (int i = 0; i < n; ++i) s += v[i] * v[i];
     return std::sqrt(s);
@@ -177,6 +196,7 @@ void inertial_force(double mass, const double* uddot, const double* omega, const
     M3 M1{};
     V3 V1{};
     gemm(false, false, 3, 3, 3, mass, om_t.data(), 3, om_t.data(), 3, 0., M1.data(), 3);
+    ORC_FLOPS(18 + 6 + 6);  // the three axpy loops of this function
     for (int i = 0; i < 9; ++i) M1[i] += mass * omd_t[i];
     gemv(false, 3, 3, 1., M1.data(), 3, eta, 0., FI);
     for (int i = 0; i < 3; ++i) FI[i] += mass * uddot[i];
@@ -189,6 +209,7 @@ void inertial_force(double mass, const double* uddot, const double* omega, const
 
 // src/system/masses/calculate_gravity_force.hpp:15-27 CalculateGravityForce
 void gravity_force(double mass, const double* g, const M3& eta_t, double* FG) {
+    ORC_FLOPS(6);
     for (int i = 0; i < 6; ++i) FG[i] = 0.;
     for (int i = 0; i < 3; ++i) FG[i] += mass * g[i];
     gemv(false, 3, 3, 1., eta_t.data(), 3, FG, 0., FG + 3);
@@ -198,6 +219,7 @@ void gravity_force(double mass, const double* g, const M3& eta_t, double* FG) {
 void gyroscopic_matrix(double mass, const double* omega, const double* eta, const M3& rho,
                        const M3& om_t, double* Guu) {
     V3 V1{}, V2{};
+    ORC_FLOPS(6);
     for (int i = 0; i < 36; ++i) Guu[i] = 0.;
     for (int i = 0; i < 3; ++i) V1[i] += mass * eta[i];
     gemv(false, 3, 3, 1., om_t.data(), 3, V1.data(), 0., V2.data());
@@ -219,6 +241,7 @@ void inertia_stiffness_matrix(double mass, const double* uddot, const double* om
                               const M3& om_t, const M3& omd_t, double* Kuu) {
     V3 V1{};
     M3 M1{}, M2{};
+    ORC_FLOPS(18 + 6 + 18);  // the three axpy loops of this function
     for (int i = 0; i < 36; ++i) Kuu[i] = 0.;
     for (int i = 0; i < 9; ++i) M1[i] += 1. * omd_t[i];
     gemm(false, false, 3, 3, 3, 1., om_t.data(), 3, om_t.data(), 3, 1., M1.data(), 3);
@@ -246,6 +269,7 @@ void inertial_qp(const double* mstar, const double* r0, const double* r, const d
     const V4 xr = quat_compose(r, r0);
     rotate_section(xr.data(), mstar, Muu);
     const double mass = Muu[0];
+    ORC_FLOPS(3);  // eta
     // src/system/masses/calculate_mass_matrix_components.hpp CalculateEta / CalculateRho
     const V3 eta{Muu[5 * 6 + 1] / mass, -Muu[5 * 6 + 0] / mass, Muu[4 * 6 + 0] / mass};
     const M3 eta_t = tilde(eta.data());
@@ -264,6 +288,7 @@ void inertial_qp(const double* mstar, const double* r0, const double* r, const d
 void calc_strain(const double* x0p, const double* up, const double* r, const double* rp,
                  double* strain) {
     V3 R = rotate_vec(r, x0p);
+    ORC_FLOPS(12);
     for (int i = 0; i < 3; ++i) R[i] += -1. * up[i];
     for (int i = 0; i < 3; ++i) R[i] += -1. * x0p[i];
     const auto E = quat_derivative(r);
@@ -280,6 +305,7 @@ void calc_strain(const double* x0p, const double* up, const double* r, const dou
 // src/system/beams/calculate_Ouu.hpp:17-37
 void calc_ouu(const double* cuu, const double* ss, const double* mt, const double* nt,
               double* O) {
+    ORC_FLOPS(36);
     for (int i = 0; i < 36; ++i) O[i] = 0.;
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j) O[i * 6 + 3 + j] += 1. * nt[i * 3 + j];
@@ -291,6 +317,7 @@ void calc_ouu(const double* cuu, const double* ss, const double* mt, const doubl
 
 // src/system/beams/calculate_Puu.hpp:17-36
 void calc_puu(const double* cuu, const double* ss, const double* nt, double* P) {
+    ORC_FLOPS(18);
     for (int i = 0; i < 36; ++i) P[i] = 0.;
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j) P[(3 + i) * 6 + j] += 1. * nt[i * 3 + j];
@@ -301,6 +328,7 @@ void calc_puu(const double* cuu, const double* ss, const double* nt, double* P) 
 // src/system/beams/calculate_Quu.hpp:17-38
 void calc_quu(const double* cuu, const double* ss, const double* nt, double* Qm) {
     M3 M1{};
+    ORC_FLOPS(18);
     for (int i = 0; i < 36; ++i) Qm[i] = 0.;
     for (int i = 0; i < 9; ++i) M1[i] += 1. * nt[i];
     gemm(false, false, 3, 3, 3, 1., cuu, 6, ss, 3, -1., M1.data(), 3);
@@ -317,6 +345,7 @@ void stiffness_qp(const double* cstar, const double* r0, const double* x0p, cons
     calc_strain(x0p, up, r, rp, strain);
     // calculate_temporary_variables.hpp:17-28
     double x0pup[3] = {x0p[0], x0p[1], x0p[2]};
+    ORC_FLOPS(6);
     for (int i = 0; i < 3; ++i) x0pup[i] += 1. * up[i];
     const M3 ss = tilde(x0pup);
     // calculate_force_FC.hpp / calculate_force_FD.hpp
@@ -540,9 +569,13 @@ void update_beam(orc_model& m, OBeam& B, double beta_prime, double gamma_prime) 
     std::vector<double> Fc(Q * 6), Fd(Q * 6), Fi(Q * 6), Fg(Q * 6);
     std::vector<double> Kuu(Q * 36), Puu(Q * 36), Cuu(Q * 36), Ouu(Q * 36), Quu(Q * 36),
         Muu(Q * 36), Guu(Q * 36);
+#ifdef ORC_COUNT_FLOPS
+    const long long qp_flops0 = g_flops;
+#endif
     for (int qp = 0; qp < Q; ++qp) {
         // interpolate_to_quadrature_point_for_inertia.hpp:19-40
         double r[4] = {0, 0, 0, 0}, ud[3] = {0, 0, 0}, om[3] = {0, 0, 0}, omd[3] = {0, 0, 0};
+        ORC_FLOPS(26 * N + 4);  // interpolation sums; the 4 divisions of the normalisation
         for (int n = 0; n < N; ++n) {
             const int s = B.node_ids[n];
             const double phi = B.phi[n * Q + qp];
@@ -559,6 +592,7 @@ void update_beam(orc_model& m, OBeam& B, double beta_prime, double gamma_prime) 
                     &Fg[qp * 6], &Muu[qp * 36], &Guu[qp * 36], &Kuu[qp * 36]);
         // interpolate_to_quadrature_point_for_stiffness.hpp:19-41
         double u[3] = {0, 0, 0}, up[3] = {0, 0, 0}, r2[4] = {0, 0, 0, 0}, rp[4] = {0, 0, 0, 0};
+        ORC_FLOPS(29 * N + 4);  // dphi / J and the interpolation sums; normalisation divisions
         for (int n = 0; n < N; ++n) {
             const int s = B.node_ids[n];
             const double phi = B.phi[n * Q + qp];
@@ -577,6 +611,9 @@ void update_beam(orc_model& m, OBeam& B, double beta_prime, double gamma_prime) 
         stiffness_qp(&B.cstar[qp * 36], &B.r0[qp * 4], &B.x0p[qp * 3], up, r2, rp, &Fc[qp * 6],
                      &Fd[qp * 6], &Cuu[qp * 36], &Ouu[qp * 36], &Puu[qp * 36], &Quu[qp * 36]);
     }
+#ifdef ORC_COUNT_FLOPS
+    g_qp_flops += g_flops - qp_flops0;
+#endif
     std::vector<double> S(N * N * 36), I(N * N * 36);
     if (m.solver_mode & 2) {
         // Cross-check ordering: the same sums with the quadrature points reversed.
@@ -1765,6 +1802,23 @@ int orc_get_element_terms(const orc_model* m, int e, double* residual, double* s
     return KYN_OK;
 }
 
+// FLOP tally of the counting build (0 in the normal one): reset, then read
+// after a call to count the operations it made.
+void orc_flops_reset() {
+#ifdef ORC_COUNT_FLOPS
+    g_flops = 0;
+    g_qp_flops = 0;
+#endif
+}
+long long orc_flops_read(int qp_only) {
+#ifdef ORC_COUNT_FLOPS
+    return qp_only ? g_qp_flops : g_flops;
+#else
+    (void)qp_only;
+    return 0;
+#endif
+}
+
 long orc_run_batch_record(orc_model** models, int n, const kyn_step_params* p, int first_step,
                           int steps, const double* amp, const double* freq, int nthreads,
                           double* seconds, int* status, int* iters_out) {
@@ -1784,7 +1838,13 @@ long orc_run_batch_record(orc_model** models, int n, const kyn_step_params* p, i
                 B.fx[(B.N - 1) * 6 + 2] = amp[i] * std::sin(2. * M_PI * freq[i] * t);
             }
             int it = 0;
-            const int st = step_impl(m, P, &it);
+            int st = step_impl(m, P, &it);
+            // The reference's Newton loop runs while err > 1, so a NaN error
+            // ends it and Step() returns true (src/step/step.hpp:54); the state
+            // evolves exactly as there, but for counting converged beam-steps a
+            // step whose last error is not finite is reported non-finite, as
+            // the GPU path reports it.
+            if (st == KYN_OK && !m.conv.empty() && !std::isfinite(m.conv.back())) st = KYN_ERR_NONFINITE;
             if (status) status[static_cast<long>(i) * steps + k] = st;
             if (iters_out) iters_out[static_cast<long>(i) * steps + k] = it;
             if (st == KYN_OK) ++converged;

@@ -64,10 +64,18 @@ long orc_run_batch(orc_model** models, int n, const kyn_step_params* p, int step
 /* The same schedule starting at time step `first_step` (the tip load of step k
  * uses t = h (first_step + k + 1)), recording every model's status and Newton
  * iterations per step: status[i*steps + k], iters[i*steps + k] (either may be
- * NULL).  Returns the number of converged model-steps. */
+ * NULL).  A step the reference's loop ends because its error norm is NaN
+ * (Step() returns true) is recorded as KYN_ERR_NONFINITE and not counted.
+ * Returns the number of converged model-steps. */
 long orc_run_batch_record(orc_model** models, int n, const kyn_step_params* p, int first_step,
                           int steps, const double* amp, const double* freq, int nthreads,
                           double* seconds, int* status, int* iters);
+
+/* FLOP tally of the counting build (-DORC_COUNT_FLOPS, libkyn_oracle_flops.so;
+ * always 0 in the normal build): reset, then read all counted operations or
+ * (qp_only) those of the quadrature-point physics of every beam update. */
+void orc_flops_reset(void);
+long long orc_flops_read(int qp_only);
 
 /* ---- kernel-level restatements (curved-beam and unit known-answer tests) -- */
 void orc_lagrange_interp_weights(double x, const double* xs, int n, double* w);

@@ -27,8 +27,10 @@ WIDTH = {"x0": 7, "x": 7, "q": 7, "q_prev": 7, "q_delta": 6, "v": 6, "vd": 6, "a
 
 
 def build(force: bool = False) -> str:
-    """Compile the oracle with its Makefile (g++, no GPU needed)."""
-    if force or not os.path.exists(_LIB_PATH):
+    """Compile the oracle (and its FLOP-counting build) with its Makefile (g++,
+    no GPU needed)."""
+    flops = os.path.join(_HERE, "_build", "libkyn_oracle_flops.so")
+    if force or not os.path.exists(_LIB_PATH) or not os.path.exists(flops):
         subprocess.run(["make", "-s", "-C", _HERE], check=True)
     return _LIB_PATH
 

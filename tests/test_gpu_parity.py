@@ -93,6 +93,23 @@ def rel_err(a, b):
     return float(np.abs(a - b).max() / scale)
 
 
+def assert_failure_agrees(gst, git, ost, oit, tag=None):
+    """Statuses and Newton iteration counts equal at every step before the
+    oracle's first non-converged step; at that step both fail.  There the
+    Newton iteration diverges: whether its error stays finite until max_iter
+    (status 1) or overflows first (KYN_ERR_NONFINITE, a step the reference's
+    `while err > 1` loop would end and report converged) is set by the last
+    bits of rounding of either FP64 implementation."""
+    bad = np.flatnonzero(np.asarray(ost) != 0)
+    first = int(bad[0]) if bad.size else len(ost)
+    assert np.array_equal(gst[:first], ost[:first]), (tag, gst[:first], ost[:first])
+    assert np.array_equal(git[:first], oit[:first]), (tag, git[:first], oit[:first])
+    if first < len(ost):
+        assert gst[first] != 0, (tag, first, gst[first], ost[first])
+        if gst[first] == 1 and ost[first] == 1:
+            assert git[first] == oit[first], (tag, first, git[first], oit[first])
+
+
 def assert_convergence_close(gpu, orc):
     """Same Newton history: equal length, same converge decision at every
     iteration, and equal error norms wherever the norm is above rounding noise
@@ -289,7 +306,7 @@ def test_batch_uneven_cantilevers(ctx):
         for i in range(len(draws)):
             ost, oit = orcs[i].step(p)
             if alive[i]:
-                assert (st[i], it[i]) == (ost, oit), (i, k, st[i], it[i], ost, oit)
+                assert_failure_agrees([st[i]], [it[i]], [ost], [oit], (i, k))
                 if ost != 0:
                     alive[i] = False
     checked = 0
@@ -307,8 +324,9 @@ def test_batch_256_beams_200_steps(ctx):
     stepped together through the batched load path; the oracle (and its twin
     for the noise floors) advances the same beams with OpenMP over beams.
     Statuses and iteration counts agree step by step up to each beam's first
-    non-converged step (the iterate left after max_iter is not a converged
-    state); states agree every 50 steps for the beams converged so far."""
+    non-converged step, where both fail (assert_failure_agrees; the iterate
+    left after it is not a converged state); states agree every 50 steps for
+    the beams converged so far."""
     from oracle.oracle_py import run_batch_record
     from openturbine_b200.runtime import LOAD_NODE_FX
     n, steps, every = 256, 200, 50
@@ -337,10 +355,7 @@ def test_batch_256_beams_200_steps(ctx):
             gst[:, k], git[:, k] = ctx.step(ids, p)
         done = k0 + every
         for i in range(n):
-            bad = np.flatnonzero(ost[i, :done] != 0)
-            last = int(bad[0]) + 1 if bad.size else done
-            assert np.array_equal(gst[i, :last], ost[i, :last]), (i, gst[i, :last], ost[i, :last])
-            assert np.array_equal(git[i, :last], oit[i, :last]), (i, git[i, :last], oit[i, :last])
+            assert_failure_agrees(gst[i, :done], git[i, :done], ost[i, :done], oit[i, :done], i)
         alive = np.flatnonzero((ost[:, :done] == 0).all(axis=1))
         for i in alive:
             assert_state_close(ctx, int(ids[i]), orcs[i])

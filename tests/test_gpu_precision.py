@@ -122,12 +122,17 @@ def test_autotune_keeps_results(ctx):
             for i, d in enumerate(draws):
                 c.set_node_fx(int(ids[i]), W.node_fx_for(d, fz[i]))
             res.append(c.step(ids, p))
-        out.append((res, np.concatenate([c.state(int(i), "q") for i in ids])))
+        out.append((res, [c.state(int(i), "q") for i in ids]))
         c.close()
     (r0, q0), (r1, q1) = out
     for (s0, i0), (s1, i1) in zip(r0, r1):
         assert np.array_equal(s0, s1) and np.array_equal(i0, i1)
-    assert np.abs(q0 - q1).max() <= 1e-12 * max(1.0, np.abs(q0).max())
+    # states of the beams converged at every step (a diverging iterate left by
+    # max_iter is not a result: another thread count's reduction order moves it)
+    ok = np.all([s == 0 for s, _ in r0], axis=0)
+    assert ok.sum() >= len(draws) // 2
+    for i in np.flatnonzero(ok):
+        assert np.abs(q0[i] - q1[i]).max() <= 1e-12 * max(1.0, np.abs(q0[i]).max())
 
 
 def test_cuda_graph_replay_matches_direct_launches():

@@ -72,3 +72,48 @@ def test_sharded_oracle_equals_single_process(tmp_path):
     assert res["total"] == conv
     for i, m in enumerate(models):
         np.testing.assert_array_equal(res[f"q{i}"], m.state("q"))
+
+
+def _bench_worker(rank, world, port, out_path):
+    """The benchmark's own multi-rank pieces on gloo: each rank takes its weak-
+    scaling batch (bench.rank_draws), advances it on the oracle and reduces its
+    timed region and converged beam-steps with bench.job_rate, as bench.py does
+    with NCCL under torchrun."""
+    import sys
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    if root not in sys.path:
+        sys.path.insert(0, root)
+    import bench
+    from oracle.oracle_py import OracleModel, run_batch
+    from openturbine_b200 import workloads as W
+    draws = bench.rank_draws(rank, 6, nodes=7)
+    models = [OracleModel(W.batch_cantilever_model(d).pack()) for d in draws]
+    conv, _, _ = run_batch(models, W.batch_params(), 2, [d.amp for d in draws],
+                           [d.freq for d in draws], 1)
+    local_ms = 10.0 * (rank + 1)          # a stand-in timed region per rank
+    t_ms, units, rate = bench.job_rate(local_ms, conv, dist)
+    ids = [d.model_id for d in draws]
+    gathered = [None] * world
+    dist.all_gather_object(gathered, (ids, conv))
+    if rank == 0:
+        np.savez(out_path, t_ms=t_ms, units=units, rate=rate,
+                 ids=np.array([i for g in gathered for i in g[0]]),
+                 convs=np.array([g[1] for g in gathered]))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_bench_multirank_reduction_and_shards(tmp_path):
+    out = str(tmp_path / "bench_ranks.npz")
+    mp.spawn(_bench_worker, args=(2, _free_port(), out), nprocs=2, join=True)
+    res = np.load(out)
+    # the slowest rank's time, the units of every rank, their ratio
+    assert res["t_ms"] == 20.0
+    assert res["units"] == res["convs"].sum()
+    assert res["rate"] == res["convs"].sum() / 0.02
+    # weak scaling: each rank has its own batch, no model twice
+    assert sorted(res["ids"].tolist()) == list(range(12))
