@@ -203,6 +203,12 @@ typedef struct kyn_model_info {
     int32_t max_beam_nodes;
     int32_t max_beam_qps;
     int64_t device_bytes;   /* HBM held by this model's resident state */
+    /* Condensed models (a multi-element beam longer than one FP64 beam system,
+     * or beams coupled by joints beyond 120 unknowns): unknowns of the
+     * bordered system left after each element's interior nodes are eliminated
+     * inside the element; 0 for every other model.  No reference counterpart
+     * (the reference factors the whole sparse system). */
+    int32_t condensed_dofs;
 } kyn_model_info;
 
 typedef struct kyn_ctx kyn_ctx;

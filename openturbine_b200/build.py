@@ -38,23 +38,46 @@ def needs_build() -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(verbose: bool = False, force: bool = False) -> str:
-    if not force and not needs_build():
-        return LIB
-    os.makedirs(OUT_DIR, exist_ok=True)
-    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-           "-Xcompiler", "-fvisibility=hidden", "-shared", "-o", LIB + ".tmp"]
-    if verbose:
-        cmd += ["-Xptxas", "-v"]
-    cmd += [os.path.join(CSRC, s) for s in SOURCES]
-    host_cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else None
-    if host_cxx:
-        cmd += ["-ccbin", host_cxx]
+# Headers each source depends on (an object is rebuilt when one is newer).
+DEPS = {
+    "kyn_capi.cu": HEADERS,
+    "kyn_host.cpp": ["kyn_types.h", "kyn_host.hpp"],
+}
+
+
+def _run(cmd: list[str], verbose: bool) -> None:
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)
     if verbose:
         sys.stdout.write(res.stdout + res.stderr)
+
+
+def build(verbose: bool = False, force: bool = False) -> str:
+    """Compiles each source to an object (only those older than the source,
+    its headers or include/kynema_b200.h, unless forced) and links the
+    library."""
+    if not force and not needs_build():
+        return LIB
+    obj_dir = os.path.join(OUT_DIR, "obj")
+    os.makedirs(obj_dir, exist_ok=True)
+    base = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+            "-Xcompiler", "-fvisibility=hidden"]
+    if os.path.exists("/usr/bin/g++"):
+        base += ["-ccbin", "/usr/bin/g++"]
+    api = os.path.join(HERE, "..", "include", "kynema_b200.h")
+    objs = []
+    for src in SOURCES:
+        obj = os.path.join(obj_dir, src + ".o")
+        deps = [os.path.join(CSRC, f) for f in [src] + DEPS[src]] + [api]
+        stale = force or not os.path.exists(obj) or any(
+            os.path.getmtime(d) > os.path.getmtime(obj) for d in deps)
+        if stale:
+            cmd = base + (["-Xptxas", "-v"] if verbose else []) + ["-c", os.path.join(CSRC, src), "-o", obj + ".tmp"]
+            _run(cmd, verbose)
+            os.replace(obj + ".tmp", obj)
+        objs.append(obj)
+    _run(base + ["-shared", "-o", LIB + ".tmp"] + objs, verbose)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -338,6 +338,11 @@ ClassKey class_key(const HostModel& h, int precision) {
     return k;
 }
 
+// Dynamic shared memory of a dense model's CTA.
+int dense_smem(const HostModel& H, const HostBeam& hb, int nt) {
+    return make_dense_smem(hb.N, H.ndofs, nt, hb.comp_maxN, hb.comp_maxQ, hb.cond_nd, hb.cond_md_off >= 0).bytes;
+}
+
 // Fills the per-model values that plans and transfer plans reuse.
 void prepare_model(DevModel* m) {
     const HostModel& H = m->host;
@@ -358,7 +363,7 @@ void prepare_model(DevModel* m) {
                 for (int k = 0; k < 3; ++k)
                     m->smem_nt[f][k] = std::max(
                         m->smem_nt[f][k],
-                        make_dense_smem(hb.N, H.ndofs, 128 << k, hb.comp_maxN, hb.comp_maxQ).bytes);
+                        dense_smem(H, hb, 128 << k));
                 continue;
             }
             m->def_nt[f] = std::max(m->def_nt[f], beam_threads(hb.N, hb.Q, hb.nc, rb, hubf));
@@ -405,6 +410,8 @@ void prepare_model(DevModel* m) {
         k.comps = hb.n_comps > 0 ? m->d_slab[b] + hb.comps_off : nullptr;
         k.comp_maxN = hb.comp_maxN;
         k.comp_maxQ = hb.comp_maxQ;
+        k.cond_nd = hb.cond_nd;
+        k.cond_md = hb.cond_md_off >= 0 ? m->d_slab[b] + hb.cond_md_off : nullptr;
         for (int s2 = 0; s2 < kMaxBeamConstraints; ++s2) k.con_base[s2] = hb.con_base[s2];
         m->kt.push_back(k);
     }
@@ -992,7 +999,13 @@ int kyn_model_create(kyn_ctx* c, const kyn_model_desc* desc) {
     for (auto& b : m->host.beams) {
         const int hubf = hub_kind(m->host);
         const int nt = b.dense ? 128 : beam_threads(b.N, b.Q, b.nc, sizeof(double), hubf);
-        const int sm = b.dense ? make_dense_smem(b.N, m->host.ndofs, nt, b.comp_maxN, b.comp_maxQ).bytes
+        if (b.cond_nd > 0 && dense_smem(m->host, b, nt) > kMaxDynSmem) {
+            // the condensed model's bordered system moves to device memory (the slab's tail)
+            if (b.slab.size() & 1) b.slab.push_back(0.);
+            b.cond_md_off = static_cast<int>(b.slab.size());
+            b.slab.resize(b.slab.size() + static_cast<size_t>(b.cond_nd) * b.cond_nd, 0.);
+        }
+        const int sm = b.dense ? dense_smem(m->host, b, nt)
                                : std::max(beam_smem(b.N, b.Q, b.nc, sizeof(double), 512, hubf),
                                           beam_smem(b.N, b.Q, b.nc, sizeof(double), nt, hubf));
         if (sm > kMaxDynSmem)
@@ -1076,6 +1089,7 @@ int kyn_model_info_get(kyn_ctx* c, int id, kyn_model_info* info) {
     info->max_beam_nodes = mn;
     info->max_beam_qps = mq;
     info->device_bytes = static_cast<int64_t>(m->bytes);
+    info->condensed_dofs = m->host.beams.empty() ? 0 : m->host.beams[0].cond_nd;
     return KYN_OK;
 }
 
@@ -1107,6 +1121,7 @@ int kyn_model_describe(const kyn_model_desc* desc, kyn_model_info* info, int32_t
     info->max_beam_nodes = mn;
     info->max_beam_qps = mq;
     info->device_bytes = bytes;
+    info->condensed_dofs = h.beams.empty() ? 0 : h.beams[0].cond_nd;
     if (row_ptrs) std::copy(h.row_ptrs.begin(), h.row_ptrs.end(), row_ptrs);
     if (col_inds) std::copy(h.col_inds.begin(), h.col_inds.end(), col_inds);
     return KYN_OK;
@@ -1796,7 +1811,7 @@ extern "C" int kyn_autotune(kyn_ctx* c, const int* ids, int n, const kyn_step_pa
         for (int nt : {128, 256, 512}) {
             bool fits = true;
             for (const HostBeam& b : h.beams)
-                fits &= (b.dense ? make_dense_smem(b.N, h.ndofs, nt, b.comp_maxN, b.comp_maxQ).bytes
+                fits &= (b.dense ? dense_smem(h, b, nt)
                                  : beam_smem(b.N, b.Q, b.nc, rb, nt, hub_kind(h))) <= kMaxDynSmem;
             if (!fits || (key.beams > 1 && key.beams * nt > 1024 * 8)) continue;
             c->tuned[key] = nt;

@@ -151,6 +151,63 @@ static void init_node_state(const kyn_model_desc* d, const HostBeam& B, const Sl
     }
 }
 
+// A model with beam elements whose constraints the per-beam systems cannot
+// take: three-row constraints, or a joint whose base node is a beam node
+// (beams coupled to each other, a beam carrying a position-only node).
+static bool needs_dense_beams(const kyn_model_desc* d) {
+    if (d->num_beams <= 0 || d->num_constraints <= 0 || !d->constraint_type) return false;
+    std::vector<char> in_beam(d->num_nodes, 0);
+    for (int k = 0; k < d->beam_node_offsets[d->num_beams]; ++k) {
+        const int id = d->beam_node_ids[k];
+        if (id >= 0 && id < d->num_nodes) in_beam[id] = 1;
+    }
+    for (int c = 0; c < d->num_constraints; ++c) {
+        const int t = d->constraint_type[c];
+        const int base = d->constraint_base_node ? d->constraint_base_node[c] : -1;
+        if (t >= KYN_CONSTRAINT_FIXED_BC_3DOF) return true;
+        if ((is_hub_joint(t) || t == KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF) && base >= 0 &&
+            base < d->num_nodes && in_beam[base])
+            return true;
+    }
+    return false;
+}
+
+// FreedomSignature bits of every node in a dense model
+// (assemble_node_freedom_allocation_table.hpp): masses and six-row
+// constraints all six components, springs and three-row constraints the
+// positions; with_beams adds the beam nodes (all six).  Out-of-range ids are
+// skipped (the model is validated elsewhere).
+static std::vector<int> node_signatures(const kyn_model_desc* d, bool with_beams) {
+    const int nn = d->num_nodes;
+    std::vector<int> sig(nn, 0);
+    auto set = [&](int n, int bits) {
+        if (n >= 0 && n < nn) sig[n] |= bits;
+    };
+    for (int e = 0; e < d->num_masses && d->mass_node; ++e) set(d->mass_node[e], kSigAll);
+    for (int e = 0; e < d->num_springs && d->spring_nodes; ++e) {
+        set(d->spring_nodes[2 * e], kSigPosition);
+        set(d->spring_nodes[2 * e + 1], kSigPosition);
+    }
+    for (int c = 0; c < d->num_constraints && d->constraint_type && d->constraint_target_node; ++c) {
+        const int t = d->constraint_type[c];
+        set(d->constraint_target_node[c], t >= KYN_CONSTRAINT_FIXED_BC_3DOF ? kSigPosition : kSigAll);
+        if ((is_hub_joint(t) || t == KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF || t == KYN_CONSTRAINT_REVOLUTE_JOINT) &&
+            d->constraint_base_node)
+            set(d->constraint_base_node[c], kSigAll);
+    }
+    for (int k = 0; with_beams && d->num_beams > 0 && k < d->beam_node_offsets[d->num_beams]; ++k)
+        set(d->beam_node_ids[k], kSigAll);
+    return sig;
+}
+
+// Unknowns of the dense bordered system over all nodes and constraint rows.
+static int dense_unknowns(const kyn_model_desc* d, bool with_beams) {
+    int n = 0;
+    for (int s : node_signatures(d, with_beams)) n += s == kSigAll ? 6 : s == kSigPosition ? 3 : 0;
+    for (int c = 0; c < d->num_constraints && d->constraint_type; ++c) n += constraint_rows(d->constraint_type[c]);
+    return n;
+}
+
 int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
     if (!d) return fail(err, KYN_ERR_INVALID, "null model description");
     if (d->num_nodes <= 0 || !d->node_x0 || !d->node_s)
@@ -211,6 +268,31 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
             }
         }
     }
+    // Condensed dense model: a multi-element beam larger than one FP64 system
+    // (kMaxFP64SystemNodes), or a model that needs the dense bordered system
+    // (below) but has more than kDenseModelMaxDofs unknowns.  Every element is
+    // then its own component; the interior nodes of each are eliminated inside
+    // the component (kyn_step_kernel.cuh, cond_component_terms).
+    bool condense = false;
+    if (d->num_beams > 0) {
+        std::vector<int> group_nodes(d->num_beams, 0), group_elems(d->num_beams, 0);
+        std::vector<int> seen(nn, -1);
+        for (int e = 0; e < d->num_beams; ++e) {
+            ++group_elems[find(e)];
+            for (int k = d->beam_node_offsets[e]; k < d->beam_node_offsets[e + 1]; ++k) {
+                const int id = d->beam_node_ids[k], r = find(e);
+                if (seen[id] != r) {
+                    seen[id] = r;
+                    ++group_nodes[r];
+                }
+            }
+        }
+        for (int e = 0; e < d->num_beams; ++e)
+            condense |= group_elems[e] > 1 && group_nodes[e] > kMaxFP64SystemNodes;
+        if (!condense && needs_dense_beams(d) && dense_unknowns(d, true) > kDenseModelMaxDofs) condense = true;
+        if (condense)
+            for (int e = 0; e < d->num_beams; ++e) comp[e] = e;
+    }
     std::vector<int> comp_index(d->num_beams > 0 ? d->num_beams : 0, -1);
     std::vector<std::vector<int>> comp_elems;
     for (int e = 0; e < d->num_beams; ++e) {
@@ -229,26 +311,30 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
         M.elem_row[e + 1] = M.elem_row[e] + d->beam_node_offsets[e + 1] - d->beam_node_offsets[e];
     M.beams.resize(comp_elems.size());
 
+    std::vector<int> local_of(nn, -1);
     for (size_t ci = 0; ci < comp_elems.size(); ++ci) {
         HostBeam& B = M.beams[ci];
-        // local nodes in order of first appearance, element by element
+        // local nodes in order of first appearance, element by element (the
+        // elements of a condensed model share nodes across components)
         int qtot = 0;
         for (int e : comp_elems[ci]) {
             const int n0 = d->beam_node_offsets[e], n1 = d->beam_node_offsets[e + 1];
             std::vector<int> loc;
             for (int k = n0; k < n1; ++k) {
                 const int id = d->beam_node_ids[k];
-                if (M.node_beam[id] < 0) {
-                    M.node_beam[id] = static_cast<int>(ci);
-                    M.node_local[id] = static_cast<int>(B.node_ids.size());
+                if (local_of[id] < 0) {
+                    local_of[id] = static_cast<int>(B.node_ids.size());
                     B.node_ids.push_back(id);
                 }
-                loc.push_back(M.node_local[id]);
+                M.node_beam[id] = static_cast<int>(ci);
+                M.node_local[id] = local_of[id];
+                loc.push_back(local_of[id]);
             }
             B.elem_ids.push_back(e);
             B.elem_local.push_back(loc);
             qtot += d->beam_qp_offsets[e + 1] - d->beam_qp_offsets[e];
         }
+        for (int id : B.node_ids) local_of[id] = -1;
         B.N = static_cast<int>(B.node_ids.size());
         B.Q = qtot;
         if (B.N > 32 || B.Q > 64)
@@ -300,17 +386,8 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
     // as the reference assembles it (src/solver/create_full_matrix.hpp).  Its
     // beam components keep their constant data (appended to the dense slab
     // below); every node joins the one system record.
-    bool dense_beams = false;
+    const bool dense_beams = !lumped && (condense || needs_dense_beams(d));
     std::vector<HostBeam> comps;
-    if (!lumped && d->num_constraints > 0 && d->constraint_type)
-        for (int c = 0; c < d->num_constraints; ++c) {
-            const int t = d->constraint_type[c];
-            const int base = d->constraint_base_node ? d->constraint_base_node[c] : -1;
-            if (t >= KYN_CONSTRAINT_FIXED_BC_3DOF) dense_beams = true;
-            if ((is_hub_joint(t) || t == KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF) && base >= 0 && base < nn &&
-                M.node_beam[base] >= 0)
-                dense_beams = true;
-        }
     if (dense_beams) {
         if (M.beams.size() > static_cast<size_t>(kMaxDenseComps))
             return fail(err, KYN_ERR_UNSUPPORTED, "more than 8 beams in a dense model");
@@ -336,6 +413,20 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
         for (const HostBeam& cb : comps) {
             B.comp_maxN = std::max(B.comp_maxN, cb.N);
             B.comp_maxQ = std::max(B.comp_maxQ, cb.Q);
+        }
+        if (condense) {
+            // bordered-system unknowns: the nodes that are not interior to one
+            // component, then the constraint rows
+            std::vector<int> ncomp(nn, 0);
+            for (const HostBeam& cb : comps)
+                for (int id : cb.node_ids) ++ncomp[id];
+            const std::vector<int> other = node_signatures(d, false);
+            B.cond_nd = 0;
+            for (int n = 0; n < nn; ++n)
+                if (!(ncomp[n] == 1 && other[n] == 0)) B.cond_nd += 6;
+            for (int c = 0; c < d->num_constraints; ++c) B.cond_nd += constraint_rows(d->constraint_type[c]);
+            if (B.cond_nd > kCondMaxDofs)
+                return fail(err, KYN_ERR_UNSUPPORTED, "condensed model with more than 160 bordered-system unknowns");
         }
     }
 
@@ -399,6 +490,13 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
             body.insert(body.end(), cb.slab.begin(), cb.slab.end());
             if (body.size() & 1) body.push_back(0.);
         }
+        if (B.cond_nd > 0)  // condensation workspaces [6Nc][6Nc + 1]
+            for (size_t ci = 0; ci < comps.size(); ++ci) {
+                const int mc = 6 * comps[ci].N;
+                head[ci * kCompHead + kCompWork] = static_cast<double>(at + body.size());
+                body.insert(body.end(), static_cast<size_t>(mc) * (mc + 1), 0.);
+                if (body.size() & 1) body.push_back(0.);
+            }
         head.resize(at, 0.);
         B.slab.insert(B.slab.end(), head.begin(), head.end());
         B.slab.insert(B.slab.end(), body.begin(), body.end());
@@ -555,7 +653,7 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
         node_cols[node].push_back(c);
         const int e = M.node_beam[node];
         HostBeam& B = M.beams[e];
-        if (B.nc >= kMaxBeamConstraints)
+        if (B.nc >= kMaxBeamSystemConstraints)
             return fail(err, KYN_ERR_UNSUPPORTED, "more than 8 constraints on one beam");
         const int slot = B.nc++;
         M.con_beam[c] = e;
@@ -722,7 +820,7 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
         crow += M.con_rows[c];
     }
     M.ndofs = M.nsys + crow;
-    if (dense && M.ndofs > kDenseModelMaxDofs)
+    if (dense && !condense && M.ndofs > kDenseModelMaxDofs)
         return fail(err, KYN_ERR_UNSUPPORTED, "dense model larger than 120 DOFs");
 
     // CRS graph: each row lists the DOFs it couples to, sorted ascending

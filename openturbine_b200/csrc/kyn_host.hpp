@@ -34,7 +34,10 @@ struct HostBeam {
     int n_comps = 0;                  // dense model with beams: beam components in the slab
     int comps_off = 0;                // their header's offset in the slab (kCompHead records)
     int comp_maxN = 0, comp_maxQ = 0; // largest component
-    int con_base[kMaxBeamConstraints] = {-1, -1, -1, -1, -1, -1, -1, -1};  // dense: joint base (local)
+    int con_base[kMaxBeamConstraints] = {-1, -1, -1, -1, -1, -1, -1, -1,
+                                         -1, -1, -1, -1, -1, -1, -1, -1};  // dense: joint base (local)
+    int cond_nd = 0;                  // condensed dense model: bordered-system unknowns, else 0
+    int cond_md_off = -1;             // offset of that system in the slab when it lives in device memory
     int n_mass = 0, n_spring = 0;     // point masses / springs at this beam's nodes
     int lumped_off = 0;               // their records' offset in the slab (kMassRec, kSpringRec)
 };

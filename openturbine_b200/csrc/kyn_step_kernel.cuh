@@ -1330,10 +1330,22 @@ struct DenseSmem {
     // node state of one component at a time, its quadrature-point outputs and
     // the quadrature phase's group scratch
     int cphi, cdphi, cdphiJ, cqpw, cq, cv, cvd, cG, cFc, cFd, cgs;
+    // condensed models: interior solution [6N], interior DOF map [N], the
+    // bordered system's right-hand-side corrections [nd], one component's
+    // local order (position of each local node, node at each position [32
+    // each]) and its solution [6 cN]; M is -1 when the bordered system lives
+    // in device memory (KBeam::cond_md)
+    int xi, imap, bc, lpos, lnode, cx;
+    int cW;  // condensed models: one component's system (inside M's region when M is shared)
     int bytes;
 };
-// nt, cN, cQ: threads per CTA and the largest beam component (0: none).
-__host__ __device__ inline DenseSmem make_dense_smem(int N, int nd, int nt = 128, int cN = 0, int cQ = 0) {
+// Quadrature points per pass of a condensed component's assembly.
+constexpr int kCondChunk = 16;
+// nt, cN, cQ: threads per CTA and the largest beam component (0: none);
+// cond_nd > 0: a condensed model whose bordered system has cond_nd unknowns
+// (md_global: kept in device memory instead of shared memory).
+__host__ __device__ inline DenseSmem make_dense_smem(int N, int nd, int nt = 128, int cN = 0, int cQ = 0,
+                                                     int cond_nd = 0, bool md_global = false) {
     DenseSmem S{};
     int o = 0;
     auto take = [&](int bytes) {
@@ -1341,7 +1353,16 @@ __host__ __device__ inline DenseSmem make_dense_smem(int N, int nd, int nt = 128
         o += (bytes + 15) & ~15;
         return r;
     };
-    S.M = take(nd * nd * 8);
+    if (cond_nd > 0) nd = cond_nd;
+    // condensed models: the bordered system's region also holds, before the
+    // system is assembled, one component's system [6cN][6cN + 1] and the G
+    // rows of one chunk of its quadrature points
+    const int w_bytes = cond_nd > 0 ? (cN * 6 * (cN * 6 + 1) * 8 + 15) & ~15 : 0;
+    const int g_bytes = cond_nd > 0 ? 4 * kCondChunk * 56 * 8 : 0;
+    const int m_bytes = md_global ? 0 : nd * nd * 8;
+    const int region = take(m_bytes > w_bytes + g_bytes ? m_bytes : w_bytes + g_bytes);
+    S.M = md_global ? -1 : region;
+    S.cW = cond_nd > 0 ? region : -1;
     S.b = take(nd * 8);
     S.x = take(nd * 8);
     S.q = take(N * 7 * 8);
@@ -1365,10 +1386,20 @@ __host__ __device__ inline DenseSmem make_dense_smem(int N, int nd, int nt = 128
         S.cq = take(cN * 7 * 8);
         S.cv = take(cN * 6 * 8);
         S.cvd = take(cN * 6 * 8);
-        S.cG = take(4 * cQ * 56 * 8);
+        S.cG = cond_nd > 0 ? -1 : take(4 * cQ * 56 * 8);  // condensed: set below
         S.cFc = take(cQ * 6 * 8);
         S.cFd = take(cQ * 6 * 8);
         S.cgs = take((nt / 16) * kGroupScratch * 8);
+    }
+    S.xi = S.imap = S.bc = S.lpos = S.lnode = S.cx = -1;
+    if (cond_nd > 0) {
+        S.cG = S.cW + w_bytes;
+        S.xi = take(N * 6 * 8);
+        S.imap = take(N * 4);
+        S.bc = take(nd * 8);
+        S.lpos = take(32 * 4);
+        S.lnode = take(32 * 4);
+        S.cx = take(cN * 6 * 8);
     }
     S.bytes = o;
     return S;
@@ -1738,6 +1769,230 @@ __device__ void dense_beam_terms(const KBeam& KB, const StepCoeffs& P, const Den
     }
 }
 
+// ---- condensed beam components of a dense model (KBeam::cond_nd > 0) -------------
+// A component's local order: its interior nodes first (fmap < 0: nodes of this
+// component only, without masses, springs or constraints), then its boundary
+// nodes; lpos[k] = position of local node k, lnode[p] = local node at p.
+// Returns the number of interior nodes.
+template <int NT>
+__device__ int cond_local_order(const double* node, int N, const int* fmap, int* lpos, int* lnode) {
+    if (threadIdx.x == 0) {
+        int o = 0;
+        for (int pass = 0; pass < 2; ++pass)
+            for (int k = 0; k < N; ++k)
+                if ((fmap[static_cast<int>(node[k])] < 0) == (pass == 0)) {
+                    lpos[k] = o;
+                    lnode[o] = k;
+                    ++o;
+                }
+    }
+    int ni = 0;
+    for (int k = 0; k < N; ++k) ni += fmap[static_cast<int>(node[k])] < 0;
+    __syncthreads();
+    return ni;
+}
+
+// Each component's system over its own local nodes, with the element terms of
+// dense_beam_terms (residual, S_ij T_j + I_ij times the conditioner) taken
+// kCondChunk quadrature points at a time.  The interior rows carry their
+// complete right-hand side -conditioner (R - node_FX - f); the boundary
+// nodes' residual goes to resid like the other nodes of the bordered system.
+// Unpivoted elimination of the interior rows (the beam systems' LU) leaves in
+// the boundary rows the Schur complement A_bb - A_bi A_ii^-1 A_ib and the
+// right-hand-side correction -A_bi A_ii^-1 b_i.  The eliminated system is
+// saved to the component's workspace for cond_add_schur and
+// cond_back_substitute.  This is the static condensation of the element
+// groups that the reference's sparse direct solve factors as one matrix
+// (src/solver/compute_system_row_entries.hpp:83-97 gives their overlap).
+template <int NT>
+__device__ void cond_component_terms(const KBeam& KB, const StepCoeffs& P, const DenseSmem& S,
+                                     unsigned char* smem_raw, const double* sq, const double* sv,
+                                     const double* svd, const double* sT, const int* fmap,
+                                     const double* mslab, const SlabLayout& ML, double* resid, int* flag) {
+    const int tid = threadIdx.x;
+    double* phi = reinterpret_cast<double*>(smem_raw + S.cphi);
+    double* dphi = reinterpret_cast<double*>(smem_raw + S.cdphi);
+    double* dphiJ = reinterpret_cast<double*>(smem_raw + S.cdphiJ);
+    double* qpw = reinterpret_cast<double*>(smem_raw + S.cqpw);
+    double* cq = reinterpret_cast<double*>(smem_raw + S.cq);
+    double* cv = reinterpret_cast<double*>(smem_raw + S.cv);
+    double* cvd = reinterpret_cast<double*>(smem_raw + S.cvd);
+    double* G = reinterpret_cast<double*>(smem_raw + S.cG);
+    double* Fc = reinterpret_cast<double*>(smem_raw + S.cFc);
+    double* Fd = reinterpret_cast<double*>(smem_raw + S.cFd);
+    double* gscr = reinterpret_cast<double*>(smem_raw + S.cgs);
+    double* W = reinterpret_cast<double*>(smem_raw + S.cW);
+    int* lpos = reinterpret_cast<int*>(smem_raw + S.lpos);
+    int* lnode = reinterpret_cast<int*>(smem_raw + S.lnode);
+    const double cond = P.conditioner;
+    for (int ci = 0; ci < KB.n_comps; ++ci) {
+        const double* hd = KB.comps + ci * kCompHead;
+        const double* cs = KB.comps + static_cast<long>(hd[0]);
+        double* work = const_cast<double*>(KB.comps) + static_cast<long>(hd[kCompWork]);
+        const int N = static_cast<int>(hd[1]), Q = static_cast<int>(hd[2]);
+        const double* node = hd + 3;
+        const SlabLayout L = make_slab_layout(N, Q);
+        const int mc = 6 * N, ldw = mc + 1;
+        for (int k = tid; k < Q * N; k += NT) {
+            phi[k] = cs[L.phi + k];
+            dphi[k] = cs[L.dphi + k];
+            dphiJ[k] = cs[L.dphiJ + k];
+        }
+        for (int k = tid; k < Q * 4; k += NT) qpw[k] = cs[L.qpw + k];
+        for (int k = tid; k < N * 7; k += NT) cq[k] = sq[static_cast<int>(node[k / 7]) * 7 + k % 7];
+        for (int k = tid; k < N * 6; k += NT) {
+            const int n = static_cast<int>(node[k / 6]);
+            cv[k] = sv[n * 6 + k % 6];
+            cvd[k] = svd[n * 6 + k % 6];
+        }
+        const int mi = 6 * cond_local_order<NT>(node, N, fmap, lpos, lnode);
+        for (int k = tid; k < mc * ldw; k += NT) {
+            const int r = k / ldw, c = k % ldw;
+            double v = 0.;
+            if (c == mc && r < mi) {  // interior right-hand side before the element residual
+                const int n = static_cast<int>(node[lnode[r / 6]]) * 6 + r % 6;
+                v = cond * (mslab[ML.fx + n] + mslab[ML.f + n]);
+            }
+            W[k] = v;
+        }
+        __syncthreads();
+        for (int q0 = 0; q0 < Q; q0 += kCondChunk) {
+            const int qn = min(kCondChunk, Q - q0);
+            SlabLayout Lc = L;
+            Lc.mstar += 36 * q0;
+            Lc.cstar += 36 * q0;
+            Lc.r0 += 4 * q0;
+            Lc.x0p += 3 * q0;
+            qp_phase<double, NT>(N, qn, phi + q0 * N, dphiJ + q0 * N, qpw + q0 * 4, cq, cv, cvd, cs, Lc,
+                                 KB.gravity, P.beta_prime, P.gamma_prime, gscr, G, Fc, Fd);
+            __syncthreads();
+            for (int t = tid; t < N * 6; t += NT) {
+                const int n = t / 6, c = t % 6;
+                double acc = 0.;
+                for (int qp = 0; qp < qn; ++qp) {
+                    const int qa = q0 + qp;
+                    const double w = qpw[qa * 4], wJ = qpw[qa * 4 + 2];
+                    acc += (w * dphi[qa * N + n]) * Fc[qp * 6 + c] + (wJ * phi[qa * N + n]) * Fd[qp * 6 + c];
+                }
+                const int mn = static_cast<int>(node[n]);
+                if (fmap[mn] < 0) W[(lpos[n] * 6 + c) * ldw + mc] -= cond * acc;
+                else resid[mn * 6 + c] += acc;
+            }
+            for (int t = tid; t < N * N * 6; t += NT) {
+                const int pr = t / 6, r = t % 6;
+                const int i = pr / N, j = pr % N;
+                double Lr[3] = {0., 0., 0.}, RS[3] = {0., 0., 0.}, RI[3] = {0., 0., 0.};
+                for (int qp = 0; qp < qn; ++qp) {
+                    const int qa = q0 + qp;
+                    const double pi = phi[qa * N + i], pj = phi[qa * N + j];
+                    const double di = dphi[qa * N + i], dj = dphi[qa * N + j];
+                    const double coef[4] = {pi * pj, pi * dj, di * dj, di * pj};
+#pragma unroll
+                    for (int mm = 0; mm < 4; ++mm) {
+                        const double* g = G + (4 * qp + mm) * 56;
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            Lr[c] += coef[mm] * g[gcol(r * 3 + c)];
+                            RS[c] += coef[mm] * g[gcol(18 + r * 3 + c)];
+                            RI[c] += coef[mm] * g[gcol(36 + r * 3 + c)];
+                        }
+                    }
+                }
+                const double* Tj = sT + static_cast<int>(node[j]) * 9;
+                double* row = W + (lpos[i] * 6 + r) * ldw + lpos[j] * 6;
+                for (int c = 0; c < 3; ++c) row[c] += cond * Lr[c];
+                for (int c = 0; c < 3; ++c) {
+                    double v = RI[c];
+                    for (int k = 0; k < 3; ++k) v += RS[k] * Tj[k * 3 + c];
+                    row[3 + c] += cond * v;
+                }
+            }
+            __syncthreads();
+        }
+        // unpivoted elimination of the interior rows, right-hand side included
+        for (int k = 0; k < mi; ++k) {
+            const double d = W[k * ldw + k];
+            if (tid == 0 && !(fabs(d) > 0. && isfinite(d))) *flag |= 2;
+            for (int i = k + 1 + tid; i < mc; i += NT) W[i * ldw + k] /= d;
+            __syncthreads();
+            const int w = mc - k - 1;
+            for (int e = tid; e < w * (w + 1); e += NT) {
+                const int i = k + 1 + e / (w + 1), j = k + 1 + e % (w + 1);
+                W[i * ldw + j] -= W[i * ldw + k] * W[k * ldw + j];
+            }
+            __syncthreads();
+        }
+        for (int k = tid; k < mc * ldw; k += NT) work[k] = W[k];
+        __syncthreads();
+    }
+}
+
+// Adds each condensed component's Schur complement (its workspace rows and
+// columns of the boundary nodes) into the bordered system Md and its
+// right-hand-side correction into bc, at the boundary nodes' DOF rows.
+template <int NT>
+__device__ void cond_add_schur(const KBeam& KB, const DenseSmem& S, unsigned char* smem_raw, const int* fmap,
+                               double* Md, int md, double* bc) {
+    const int tid = threadIdx.x;
+    int* lpos = reinterpret_cast<int*>(smem_raw + S.lpos);
+    int* lnode = reinterpret_cast<int*>(smem_raw + S.lnode);
+    for (int ci = 0; ci < KB.n_comps; ++ci) {
+        const double* hd = KB.comps + ci * kCompHead;
+        const double* work = KB.comps + static_cast<long>(hd[kCompWork]);
+        const int N = static_cast<int>(hd[1]);
+        const double* node = hd + 3;
+        const int mc = 6 * N, ldw = mc + 1;
+        const int mi = 6 * cond_local_order<NT>(node, N, fmap, lpos, lnode);
+        const int mb = mc - mi;
+        for (int e = tid; e < mb * (mb + 1); e += NT) {
+            const int t = mi + e / (mb + 1), u = mi + e % (mb + 1);
+            const int rt = fmap[static_cast<int>(node[lnode[t / 6]])] + t % 6;
+            const double v = work[t * ldw + u];
+            if (u == mc) bc[rt] += v;
+            else Md[rt * md + fmap[static_cast<int>(node[lnode[u / 6]])] + u % 6] += v;
+        }
+        __syncthreads();
+    }
+}
+
+// Interior corrections of each condensed component from the bordered
+// system's solution x at its boundary nodes: U_ii x_i = y_i - U_ib x_b by one
+// warp, rows of the eliminated system (staged back into shared memory in W)
+// from the last up; the corrections go to xi at the nodes' interior DOFs.
+template <int NT>
+__device__ void cond_back_substitute(const KBeam& KB, const DenseSmem& S, unsigned char* smem_raw,
+                                     const int* fmap, const int* imap, const double* x, double* xi) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double* W = reinterpret_cast<double*>(smem_raw + S.cW);
+    double* cx = reinterpret_cast<double*>(smem_raw + S.cx);
+    int* lpos = reinterpret_cast<int*>(smem_raw + S.lpos);
+    int* lnode = reinterpret_cast<int*>(smem_raw + S.lnode);
+    for (int ci = 0; ci < KB.n_comps; ++ci) {
+        const double* hd = KB.comps + ci * kCompHead;
+        const double* work = KB.comps + static_cast<long>(hd[kCompWork]);
+        const int N = static_cast<int>(hd[1]);
+        const double* node = hd + 3;
+        const int mc = 6 * N, ldw = mc + 1;
+        const int mi = 6 * cond_local_order<NT>(node, N, fmap, lpos, lnode);
+        for (int k = tid; k < mi * ldw; k += NT) W[k] = work[k];
+        for (int p = mi + tid; p < mc; p += NT) cx[p] = x[fmap[static_cast<int>(node[lnode[p / 6]])] + p % 6];
+        __syncthreads();
+        if (warp == 0) {
+            for (int k = mi - 1; k >= 0; --k) {
+                const double* row = W + k * ldw;
+                double acc = 0.;
+                for (int j = k + 1 + lane; j < mc; j += 32) acc += row[j] * cx[j];
+                for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+                if (lane == 0) cx[k] = (row[mc] - acc) / row[k];
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        for (int p = tid; p < mi; p += NT) xi[imap[static_cast<int>(node[lnode[p / 6]])] + p % 6] = cx[p];
+        __syncthreads();
+    }
+}
+
 template <int NT>
 __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoeffs& P, int record, int* status_out,
                                  int* iters_out, unsigned char* smem_raw) {
@@ -1746,9 +2001,12 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
     const int N = KB.N, nc = KB.nc;
     const SlabLayout L = make_slab_layout(N, 0);
     double* __restrict__ slab = KB.slab;
-    const int nd = KB.model_dofs;
-    const DenseSmem S = make_dense_smem(N, nd, NT, KB.n_comps > 0 ? KB.comp_maxN : 0, KB.comp_maxQ);
-    double* Md = reinterpret_cast<double*>(smem_raw + S.M);
+    const int nd = KB.model_dofs;                       // the reference's unknowns
+    const bool cnd = KB.cond_nd > 0;                    // condensed beam components
+    const int md = cnd ? KB.cond_nd : nd;               // unknowns of the bordered system
+    const DenseSmem S = make_dense_smem(N, nd, NT, KB.n_comps > 0 ? KB.comp_maxN : 0, KB.comp_maxQ, KB.cond_nd,
+                                        KB.cond_md != nullptr);
+    double* Md = KB.cond_md ? KB.cond_md : reinterpret_cast<double*>(smem_raw + S.M);
     double* b = reinterpret_cast<double*>(smem_raw + S.b);
     double* x = reinterpret_cast<double*>(smem_raw + S.x);
     double* sq = reinterpret_cast<double*>(smem_raw + S.q);
@@ -1763,6 +2021,9 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
     int* act = reinterpret_cast<int*>(smem_raw + S.act);
     int* fmap = reinterpret_cast<int*>(smem_raw + S.fmap);
     double* red = reinterpret_cast<double*>(smem_raw + S.red);
+    double* xi = cnd ? reinterpret_cast<double*>(smem_raw + S.xi) : nullptr;
+    int* imap = cnd ? reinterpret_cast<int*>(smem_raw + S.imap) : nullptr;
+    double* bc = cnd ? reinterpret_cast<double*>(smem_raw + S.bc) : nullptr;
     __shared__ int s_flag, s_nsys, s_piv;
     const double h = P.h;
 
@@ -1783,6 +2044,8 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
         // masses six, springs position only, constraint targets six or three,
         // joint bases six; DOF map = exclusive scan (compute_node_freedom_map_table.hpp)
         for (int n = 0; n < N; ++n) act[n] = 0;
+        if (cnd)
+            for (int n = 0; n < N; ++n) imap[n] = 0;
         const double* mrec = KB.lumped;
         for (int e = 0; e < KB.n_mass; ++e) act[static_cast<int>(mrec[e * kMassRec])] |= kSigAll;
         const double* srec = KB.lumped + KB.n_mass * kMassRec;
@@ -1795,18 +2058,34 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
             act[KB.con_node[c]] |= (t >= KYN_CONSTRAINT_FIXED_BC_3DOF) ? kSigPosition : kSigAll;
             if (KB.con_base[c] >= 0) act[KB.con_base[c]] |= kSigAll;
         }
+        // condensed models: a node of one component only, with no mass, spring
+        // or constraint, is interior (fmap -1, imap its first interior DOF)
+        if (cnd)
+            for (int n = 0; n < N; ++n) fmap[n] = act[n];
         for (int ci = 0; ci < KB.n_comps; ++ci) {  // beam nodes: all six components
             const double* hd = KB.comps + ci * kCompHead;
-            for (int k = 0; k < static_cast<int>(hd[1]); ++k) act[static_cast<int>(hd[3 + k])] |= kSigAll;
+            for (int k = 0; k < static_cast<int>(hd[1]); ++k) {
+                act[static_cast<int>(hd[3 + k])] |= kSigAll;
+                if (cnd) ++imap[static_cast<int>(hd[3 + k])];
+            }
         }
-        int o = 0;
+        int o = 0, oi = 0;
         for (int n = 0; n < N; ++n) {
             act[n] = (act[n] == kSigAll) ? 6 : (act[n] == kSigPosition) ? 3 : 0;
-            fmap[n] = o;
-            o += act[n];
+            if (cnd && imap[n] == 1 && fmap[n] == 0) {
+                fmap[n] = -1;
+                imap[n] = oi;
+                oi += act[n];
+            } else {
+                fmap[n] = o;
+                if (cnd) imap[n] = -1;
+                o += act[n];
+            }
         }
+        int rows = 0;
+        for (int c = 0; c < nc; ++c) rows += KB.con_type[c] >= KYN_CONSTRAINT_FIXED_BC_3DOF ? 3 : 6;
         s_nsys = o;
-        s_flag = (o > nd) ? 2 : 0;
+        s_flag = cnd ? ((o + rows != md || o + oi + rows != nd) ? 2 : 0) : (o > nd) ? 2 : 0;
     }
     __syncthreads();
     const int nsys = s_nsys;
@@ -1852,17 +2131,24 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
                     sT[n * 9 + i * 3 + j] = (i == j ? 1. : 0.) + (t1 * tilde_e(rv, j, i) + t2 * rr);
                 }
         }
-        for (int k = tid; k < nd * nd; k += NT) Md[k] = 0.;
-        for (int k = tid; k < nd; k += NT) b[k] = 0.;
         for (int k = tid; k < N * 6; k += NT) resid[k] = 0.;
+        if (cnd) {  // components first: their systems share the bordered system's region
+            __syncthreads();
+            cond_component_terms<NT>(KB, P, S, smem_raw, sq, sv, svd, sT, fmap, slab, L, resid, &s_flag);
+        }
+        for (int k = tid; k < md * md; k += NT) Md[k] = 0.;
+        for (int k = tid; k < md; k += NT) b[k] = 0.;
+        if (cnd)
+            for (int k = tid; k < md; k += NT) bc[k] = 0.;
         __syncthreads();
         // masses and springs (residual into resid, conditioned blocks into Md)
         for (int n = tid; n < N; n += NT)
             add_lumped_terms(n, KB.lumped, KB.n_mass, KB.n_spring, sq, sv, svd, sT, KB.gravity,
-                             P.beta_prime, P.gamma_prime, cond, fmap, Md, nd, resid, 1);
+                             P.beta_prime, P.gamma_prime, cond, fmap, Md, md, resid, 1);
         if (KB.n_comps > 0) {  // beam elements, then their node_FX (summed per node)
             __syncthreads();
-            dense_beam_terms<NT>(KB, P, S, smem_raw, sq, sv, svd, sT, fmap, Md, nd, resid);
+            if (cnd) cond_add_schur<NT>(KB, S, smem_raw, fmap, Md, md, bc);
+            else dense_beam_terms<NT>(KB, P, S, smem_raw, sq, sv, svd, sT, fmap, Md, nd, resid);
             for (int t = tid; t < N * 6; t += NT) resid[t] -= slab[L.fx + t];
         }
         // constraints: residual, gradients and G^T lambda
@@ -1914,14 +2200,14 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
                 const int rows = t >= KYN_CONSTRAINT_FIXED_BC_3DOF ? 3 : 6;
                 const int ft = fmap[tn];
                 for (int r = 0; r < rows; ++r) {
-                    double* row = Md + (rf + r) * nd;
+                    double* row = Md + (rf + r) * md;
                     if (r < 3) {
                         row[ft + r] += 1.;
-                        Md[(ft + r) * nd + rf + r] += 1.;
+                        Md[(ft + r) * md + rf + r] += 1.;
                     } else {
                         for (int j = 0; j < 3; ++j) {
                             row[ft + 3 + j] += cr[conrec::Brot + (r - 3) * 3 + j];
-                            Md[(ft + 3 + j) * nd + rf + r] += cr[conrec::AX + j * 3 + (r - 3)];
+                            Md[(ft + 3 + j) * md + rf + r] += cr[conrec::AX + j * 3 + (r - 3)];
                         }
                     }
                     b[rf + r] += cr[conrec::Phi + r];
@@ -1931,18 +2217,18 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
                     const int fb = fmap[bn];
                     const double* r1x0 = cr + conrec::R1X0;
                     for (int r = 0; r < rows; ++r) {
-                        double* row = Md + (rf + r) * nd;
+                        double* row = Md + (rf + r) * md;
                         if (r < 3) {
                             row[fb + r] -= 1.;
-                            Md[(fb + r) * nd + rf + r] -= 1.;
+                            Md[(fb + r) * md + rf + r] -= 1.;
                             for (int j = 0; j < 3; ++j) {
                                 row[fb + 3 + j] += cr[conrec::Btr + r * 3 + j];
-                                Md[(fb + 3 + j) * nd + rf + r] += tilde_e(r1x0, r, j);
+                                Md[(fb + 3 + j) * md + rf + r] += tilde_e(r1x0, r, j);
                             }
                         } else {
                             for (int j = 0; j < 3; ++j) {
                                 row[fb + 3 + j] += cr[conrec::Brr + (r - 3) * 3 + j];
-                                Md[(fb + 3 + j) * nd + rf + r] -= cr[conrec::AX + (r - 3) * 3 + j];
+                                Md[(fb + 3 + j) * md + rf + r] -= cr[conrec::AX + (r - 3) * 3 + j];
                             }
                         }
                     }
@@ -1965,17 +2251,18 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
         __syncthreads();
         // b = -(cond (R - f) on the system rows, Phi on the constraint rows)
         for (int n = tid; n < N; n += NT)  // position-only nodes: components 0..2
-            for (int c = 0; c < act[n]; ++c) b[fmap[n] + c] += resid[n * 6 + c] - slab[L.f + n * 6 + c];
+            if (fmap[n] >= 0)
+                for (int c = 0; c < act[n]; ++c) b[fmap[n] + c] += resid[n * 6 + c] - slab[L.f + n * 6 + c];
         __syncthreads();
-        for (int k = tid; k < nd; k += NT) b[k] = -(k < nsys ? b[k] * cond : b[k]);
+        for (int k = tid; k < md; k += NT) b[k] = -(k < nsys ? b[k] * cond : b[k]) + (cnd ? bc[k] : 0.);
         __syncthreads();
         // LU with partial pivoting, in place (the oracle's dense solve)
-        for (int k = 0; k < nd; ++k) {
+        for (int k = 0; k < md; ++k) {
             if (warp == 0) {
                 double best = -1.;
                 int p = k;
-                for (int i = k + lane; i < nd; i += 32) {
-                    const double v = fabs(Md[i * nd + k]);
+                for (int i = k + lane; i < md; i += 32) {
+                    const double v = fabs(Md[i * md + k]);
                     if (v > best) {
                         best = v;
                         p = i;
@@ -1997,10 +2284,10 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
             __syncthreads();
             const int p = s_piv;
             if (p != k) {
-                for (int j = tid; j < nd; j += NT) {
-                    const double t0 = Md[k * nd + j];
-                    Md[k * nd + j] = Md[p * nd + j];
-                    Md[p * nd + j] = t0;
+                for (int j = tid; j < md; j += NT) {
+                    const double t0 = Md[k * md + j];
+                    Md[k * md + j] = Md[p * md + j];
+                    Md[p * md + j] = t0;
                 }
                 if (tid == 0) {
                     const double t0 = b[k];
@@ -2009,37 +2296,40 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
                 }
             }
             __syncthreads();
-            const double d = Md[k * nd + k];
-            for (int i = k + 1 + tid; i < nd; i += NT) Md[i * nd + k] /= d;
+            const double d = Md[k * md + k];
+            for (int i = k + 1 + tid; i < md; i += NT) Md[i * md + k] /= d;
             __syncthreads();
-            const int w = nd - k - 1;
+            const int w = md - k - 1;
             for (int e = tid; e < w * (w + 1); e += NT) {
                 const int i = k + 1 + e / (w + 1), j = e % (w + 1);
-                const double l = Md[i * nd + k];
+                const double l = Md[i * md + k];
                 if (j < w)
-                    Md[i * nd + k + 1 + j] -= l * Md[k * nd + k + 1 + j];
+                    Md[i * md + k + 1 + j] -= l * Md[k * md + k + 1 + j];
                 else
                     b[i] -= l * b[k];
             }
             __syncthreads();
         }
         if (warp == 0) {  // back substitution
-            for (int i = nd - 1; i >= 0; --i) {
+            for (int i = md - 1; i >= 0; --i) {
                 double s2 = 0.;
-                for (int j = i + 1 + lane; j < nd; j += 32) s2 += Md[i * nd + j] * x[j];
+                for (int j = i + 1 + lane; j < md; j += 32) s2 += Md[i * md + j] * x[j];
                 for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-                if (lane == 0) x[i] = (b[i] - s2) / Md[i * nd + i];
+                if (lane == 0) x[i] = (b[i] - s2) / Md[i * md + i];
                 __syncwarp();
             }
         }
         __syncthreads();
         // multipliers unconditioned; convergence error (calculate_convergence_error.hpp)
-        for (int k = nsys + tid; k < nd; k += NT) x[k] /= cond;
+        for (int k = nsys + tid; k < md; k += NT) x[k] /= cond;
         __syncthreads();
+        if (cnd) cond_back_substitute<NT>(KB, S, smem_raw, fmap, imap, x, xi);
+        // correction of component c of node n
+        auto delta_of = [&](int n, int c) { return fmap[n] >= 0 ? x[fmap[n] + c] : xi[imap[n] + c]; };
         double part = 0.;
         for (int n = tid; n < N; n += NT)
             for (int c = 0; c < act[n]; ++c) {
-                const double e = x[fmap[n] + c] / (P.atol + P.rtol * fabs(sqd[n * 6 + c] * h));
+                const double e = delta_of(n, c) / (P.atol + P.rtol * fabs(sqd[n * 6 + c] * h));
                 part += e * e;
             }
         if (tid < nc) {
@@ -2063,7 +2353,7 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
         // update (update_state_prediction.hpp, update_lambda_prediction.hpp)
         for (int n = tid; n < N; n += NT)
             for (int c = 0; c < act[n]; ++c) {
-                const double delta = x[fmap[n] + c];
+                const double delta = delta_of(n, c);
                 sqd[n * 6 + c] += delta / h;
                 if (P.dynamic) {
                     sv[n * 6 + c] += P.gamma_prime * delta;

@@ -20,7 +20,9 @@
 
 namespace kyn {
 
-constexpr int kMaxBeamConstraints = 8;   // FixedBC / PrescribedBC / joints per beam system
+constexpr int kMaxBeamConstraints = 16;  // constraint records of one system (dense models)
+constexpr int kMaxBeamSystemConstraints = 8;  // FixedBC / PrescribedBC / joints per beam system
+constexpr int kMaxFP64SystemNodes = 21;  // nodes of one beam system in the FP64 form (shared memory)
 constexpr int kMaxClusterBeams = 8;      // beams per model (portable cluster size)
 constexpr int kMaxNewtonIters = 64;      // convergence-history capacity
 constexpr int kRefineSweeps = 8;         // FP32 form: most refinement sweeps per linear solve
@@ -29,9 +31,19 @@ constexpr int kDenseModelMaxDofs = 120;  // unknowns of a model solved as a dens
 // A dense model with beam elements keeps each beam component's constant data
 // (a slab in SlabLayout(Nc, Qc)) after its own records; a header of
 // kCompHead doubles per component precedes them: [offset of the component's
-// slab from the header start, Nc, Qc, model node of each local node (32)].
-constexpr int kCompHead = 35;
+// slab from the header start, Nc, Qc, model node of each local node (32),
+// offset of the component's condensation workspace from the header start].
+constexpr int kCompHead = 36;
+constexpr int kCompWork = 35;
 constexpr int kMaxDenseComps = 8;
+// A condensed dense model (KBeam::cond_nd > 0) eliminates the interior nodes
+// of each beam component -- nodes of one component only, without masses,
+// springs or constraints -- inside the component's own system, and solves
+// the bordered system of the remaining nodes and the constraints (at most
+// kCondMaxDofs unknowns).  The workspace of a component holds its system
+// [6Nc][6Nc + 1] during the condensation and its factored interior rows for
+// the back substitution.
+constexpr int kCondMaxDofs = 160;
 constexpr int kThreads = 256;            // threads per CTA of the step kernel
 
 // Offsets (in doubles) of the arrays inside one beam slab.
@@ -156,6 +168,8 @@ struct KBeam {
     const double* comps;      // dense models with beams: component records (kCompHead), or null
     int32_t n_comps;          // beam components (connected element groups) of a dense model
     int32_t comp_maxN, comp_maxQ;  // their largest node and quadrature-point counts
+    int32_t cond_nd;          // condensed dense models: unknowns of the bordered system, else 0
+    double* cond_md;          // condensed dense models: that system in device memory, or null (shared)
     double* conv;             // [kMaxNewtonIters] model convergence history (rank 0)
     double* dump;             // optional: last assembled system (see kyn_capi.cu)
     unsigned long long* prof; // optional: per-phase SM cycles, summed over beams

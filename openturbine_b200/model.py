@@ -341,7 +341,7 @@ class KynModelInfo(ctypes.Structure):
         ("num_constraints", ctypes.c_int32), ("num_system_dofs", ctypes.c_int32),
         ("num_dofs", ctypes.c_int32), ("nnz", ctypes.c_int32),
         ("max_beam_nodes", ctypes.c_int32), ("max_beam_qps", ctypes.c_int32),
-        ("device_bytes", ctypes.c_int64),
+        ("device_bytes", ctypes.c_int64), ("condensed_dofs", ctypes.c_int32),
     ]
 
 

@@ -1700,6 +1700,7 @@ int orc_model_info(const orc_model* m, kyn_model_info* info) {
     info->max_beam_nodes = mn;
     info->max_beam_qps = mq;
     info->device_bytes = 0;
+    info->condensed_dofs = 0;
     return KYN_OK;
 }
 

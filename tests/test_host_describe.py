@@ -39,6 +39,9 @@ MODELS = {
     "two_element_cantilever": lambda: R.two_element_cantilever_model(),
     "two_beams_rigid_joint": lambda: R.two_beams_model(),
     "moored_cantilever": lambda: R.moored_cantilever_model(),
+    "condensed_four_element_cantilever": lambda: R.four_element_cantilever_model(),
+    "condensed_tower": lambda: R.tower_model(),
+    "condensed_two_long_beams": lambda: R.two_long_beams_model(),
     "three_row_bc_on_a_beam": lambda: _cantilever_with(lambda m: m.AddFixedBC3DOFs(4)),
     "batch_rotor": lambda: W.rotor_model(3),
     "batch_cantilever": lambda: W.batch_cantilever_model(W.draw_batch(1, first_id=77)[0]),

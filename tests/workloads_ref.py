@@ -454,3 +454,125 @@ def moored_cantilever_model():
     m.AddFixedBC3DOFs(anchor)
     m.AddMassElement(tip, np.diag([50., 50., 50., 5., 5., 5.]))
     return m, p
+
+
+# ---- condensed dense models (beams longer than one FP64 beam system) ---------------
+def chain_beam(m: Model, n_elem: int, order: int, length: float, q_axis, sections, quad, origin=(0., 0., 0.)):
+    """Adds a straight beam of n_elem elements of the given order along the
+    local x axis rotated by q_axis, the elements sharing their end nodes.
+    Node::s is one value per node, so the elements alternate direction: odd
+    elements are parametrised from their far end back to the shared node,
+    which then sits at the same s in both elements.  Returns the node ids in
+    order along the beam and the element node lists."""
+    gll = [(x + 1.) / 2. for x in GenerateGLLPoints(order)]
+    le = length / n_elem
+    ends = []
+    for e in range(n_elem + 1):
+        s = 0. if e % 2 == 0 else 1.
+        p = RotateVectorByQuaternion(q_axis, [le * e, 0., 0.])
+        ends.append(m.AddNode().SetElemLocation(s).SetPosition(
+            origin[0] + p[0], origin[1] + p[1], origin[2] + p[2], *q_axis).Build())
+    along = [ends[0]]
+    elems = []
+    for e in range(n_elem):
+        fwd = e % 2 == 0
+        inner = []
+        for s in gll[1:-1]:
+            xl = le * e + le * (s if fwd else 1. - s)
+            p = RotateVectorByQuaternion(q_axis, [xl, 0., 0.])
+            inner.append(m.AddNode().SetElemLocation(s).SetPosition(
+                origin[0] + p[0], origin[1] + p[1], origin[2] + p[2], *q_axis).Build())
+        nodes = [ends[e]] + inner + [ends[e + 1]] if fwd else [ends[e + 1]] + inner + [ends[e]]
+        m.AddBeamElement(nodes, sections, quad)
+        elems.append(nodes)
+        along += (inner if fwd else inner[::-1]) + [ends[e + 1]]
+    return along, elems
+
+
+def four_element_cantilever_model():
+    """A 40 m cantilever of four order-10 elements (41 nodes) with the
+    composite section of test_cantilever_beam.cpp and 12 Gauss points per
+    element, FixedBC at the root, no gravity: larger than one FP64 beam
+    system, so each element's interior nodes are condensed inside the
+    element and the four shared end nodes form the bordered system."""
+    m = Model()
+    m.SetGravity(0., 0., 0.)
+    secs = [BeamSection(0., COMPOSITE_MASS, COMPOSITE_STIFF), BeamSection(1., COMPOSITE_MASS, COMPOSITE_STIFF)]
+    g12 = [[x, w] for x, w in zip(*np.polynomial.legendre.leggauss(12))]
+    along, elems = chain_beam(m, 4, 10, 40., [1., 0., 0., 0.], secs, g12)
+    m.AddFixedBC(along[0])
+    return m, StepParameters(True, 6, 0.005, 0.0), along, elems
+
+
+def chain_tip_loads(elems, tip: int, step: int, h: float = 0.005) -> np.ndarray:
+    """node_FX rows per element node (elements in order) with a tip force
+    100 sin(10 t) along z and a tip moment about x."""
+    rows = sum(len(e) for e in elems)
+    fx = np.zeros((rows, 6))
+    at = 0
+    for nodes in elems:
+        if tip in nodes:
+            r = at + nodes.index(tip)
+            fx[r, 2] = 100. * math.sin(10.0 * h * (step + 1))
+            fx[r, 3] = 20. * math.sin(7.0 * h * (step + 1))
+            break
+        at += len(nodes)
+    return fx
+
+
+def hollow_circle_section(s: float, E: float, G: float, rho: float, D: float, t: float, nu: float):
+    """Mass and stiffness of a thin-walled circular tube in the beam's frame
+    (axial direction first): the properties of hollow_circle_properties.hpp
+    (area, I, J, Timoshenko shear factor 6(1 + nu)/(7 + 6 nu)), placed on
+    the diagonal as [EA, kGA, kGA, GJ, EI, EI] and [m, m, m, Ip, I, I]."""
+    ro, ri = D / 2., D / 2. - t
+    A = math.pi * (ro ** 2 - ri ** 2)
+    I = math.pi * (ro ** 4 - ri ** 4) / 4.
+    J = 2. * I
+    k = 6. * (1. + nu) / (7. + 6. * nu)
+    mass = np.diag([rho * A, rho * A, rho * A, rho * 2. * I, rho * I, rho * I])
+    stiff = np.diag([E * A, k * G * A, k * G * A, G * J, E * I, E * I])
+    return BeamSection(s, mass, stiff)
+
+
+def tower_model():
+    """A 90 m steel tower along z of three order-10 elements (31 nodes; 6 m
+    tube, 30 mm wall, 12 Gauss points per element) with a PrescribedBC at
+    its base, a nacelle point mass at its top and gravity -9.81 z; the top
+    node (a point mass) and the shared element ends form the bordered
+    system of the condensed model."""
+    m = Model()
+    m.SetGravity(0., 0., -9.81)
+    secs = [hollow_circle_section(s, 200e9, 79.3e9, 7850., 6., 0.03, 0.3) for s in (0., 1.)]
+    g12 = [[x, w] for x, w in zip(*np.polynomial.legendre.leggauss(12))]
+    qz = [math.sqrt(0.5), 0., -math.sqrt(0.5), 0.]   # local x -> global z
+    along, elems = chain_beam(m, 3, 10, 90., qz, secs, g12)
+    m.AddPrescribedBC(along[0])
+    m.AddMassElement(along[-1], np.diag([2.0e5, 2.0e5, 2.0e5, 4.0e6, 3.0e6, 3.0e6]))
+    return m, StepParameters(True, 6, 0.01, 0.0), along, elems
+
+
+def two_long_beams_model():
+    """BladeInterfaceTest.TwoBeams with two order-20 beams (21 nodes each):
+    joined by a RigidJoint they need 264 unknowns as one dense system, so the
+    model is condensed (each beam's 19 interior nodes eliminated inside the
+    beam)."""
+    section_s = [0.05 * k for k in range(21)]
+    mass = np.diag([8.538e-2, 8.538e-2, 8.538e-2, 1.4433e-2, 0.40972e-2, 1.0336e-2])
+    stiff = np.diag([1368.17e3, 88.56e3, 38.78e3, 16.96e3, 59.12e3, 141.47e3])
+    stiff[3, 4] = stiff[4, 3] = 17.61e3
+    stiff[3, 5] = stiff[5, 3] = -0.351e3
+    stiff[4, 5] = stiff[5, 4] = -0.37e3
+    secs = [BeamSection(s, mass, stiff) for s in section_s]
+    quad = CreateTrapezoidalQuadrature(section_s)
+    m = Model()
+    m.SetGravity(0., 0., -9.81)
+    beams = []
+    for b in range(2):
+        ids = [m.AddNode().SetElemLocation(s).SetPosition(10. * s + 10. * b, 0., 0., 1., 0., 0., 0.).Build()
+               for s in [(x + 1.) / 2. for x in GenerateGLLPoints(20)]]
+        m.AddBeamElement(ids, secs, quad)
+        beams.append(ids)
+    m.AddPrescribedBC(beams[0][0])
+    m.AddRigidJointConstraint([beams[0][-1], beams[1][0]])
+    return m, StepParameters(True, 6, 0.01, 0.), beams
