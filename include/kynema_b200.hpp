@@ -348,6 +348,28 @@ public:
     }
 
     std::tuple<State, Elements, Constraints, Solver> CreateSystemWithSolver(const Context& ctx) const {
+        auto m = std::make_shared<DeviceModel>(ctx);
+        WithDescription([&](const kyn_model_desc& d) {
+            const int id = kyn_model_create(ctx.get(), &d);
+            check(ctx.get(), id);
+            m->id = id;
+        });
+        check(ctx.get(), kyn_model_info_get(ctx.get(), m->id, &m->info));
+        size_t elem_nodes = 0;
+        for (const auto& b : beams_) {
+            m->elem_offset.push_back(elem_nodes);
+            elem_nodes += b.nodes.size();
+        }
+        for (size_t k = 0; k < cons_.size(); ++k)
+            if (cons_[k].control) m->controls.emplace_back(static_cast<int>(k), cons_[k].control);
+        m->node_fx.assign(elem_nodes * 6, 0.);
+        return {State(m), Elements(m), Constraints(m), Solver(m)};
+    }
+
+    // Calls f with the plain-array description of this model (kyn_model_desc,
+    // valid during the call), the input of kyn_model_create.
+    template <typename F>
+    void WithDescription(F&& f) const {
         std::vector<double> x0, u, v, vd, s, spos, smass, sstiff, qxi, qw, cinit, caxis;
         std::vector<int32_t> bno{0}, bni, bso{0}, bqo{0}, ctype, cbase, ctarget;
         for (const auto& n : nodes_) {
@@ -357,11 +379,7 @@ public:
             vd.insert(vd.end(), n.vd.begin(), n.vd.end());
             s.push_back(n.s);
         }
-        auto m = std::make_shared<DeviceModel>(ctx);
-        size_t elem_nodes = 0;
         for (const auto& b : beams_) {
-            m->elem_offset.push_back(elem_nodes);
-            elem_nodes += b.nodes.size();
             for (auto n : b.nodes) bni.push_back(static_cast<int32_t>(n));
             bno.push_back(static_cast<int32_t>(bni.size()));
             for (const auto& sec : b.sections) {
@@ -382,7 +400,6 @@ public:
             ctarget.push_back(static_cast<int32_t>(c.node));
             cinit.insert(cinit.end(), c.u0.begin(), c.u0.end());
             caxis.insert(caxis.end(), c.axis.begin(), c.axis.end());
-            if (c.control) m->controls.emplace_back(static_cast<int>(ctype.size() - 1), c.control);
         }
         kyn_model_desc d{};
         d.num_nodes = static_cast<int32_t>(nodes_.size());
@@ -414,12 +431,7 @@ public:
         d.mass_node = mnode.data(); d.mass_matrix = mmat.data();
         d.num_springs = static_cast<int32_t>(springs_.size());
         d.spring_nodes = snodes.data(); d.spring_stiffness = sk.data(); d.spring_length = sl.data();
-        const int id = kyn_model_create(ctx.get(), &d);
-        check(ctx.get(), id);
-        m->id = id;
-        check(ctx.get(), kyn_model_info_get(ctx.get(), id, &m->info));
-        m->node_fx.assign(elem_nodes * 6, 0.);
-        return {State(m), Elements(m), Constraints(m), Solver(m)};
+        f(static_cast<const kyn_model_desc&>(d));
     }
 
 private:

@@ -577,6 +577,440 @@ private:
     components::BeamBuilder blade_;
 };
 
+// ---- sectional properties of a hollow circular tube ---------------------------------
+// src/elements/beams/generate_sectional_properties.hpp and
+// hollow_circle_properties.hpp: the 6x6 stiffness and mass matrices of a
+// section about its reference point (the beam axis along z of the section
+// frame, WindIO convention), from its stiffnesses, inertias, offsets of the
+// elastic centre, shear centre and centre of gravity, and principal-axis angles.
+namespace beams {
+
+inline math::M6 GenerateStiffnessMatrix(double EA, double EI_x, double EI_y, double GKt, double GA, double kxs,
+                                        double kys, double x_C, double y_C, double theta_p, double x_S,
+                                        double y_S, double theta_s) {
+    const double cp = std::cos(theta_p), sp = std::sin(theta_p);
+    const double cs = std::cos(theta_s), ss = std::sin(theta_s);
+    const double bxx = EI_x * cp * cp + EI_y * sp * sp;
+    const double byy = EI_x * sp * sp + EI_y * cp * cp;
+    const double bxy = (EI_y - EI_x) * sp * cp;
+    const double sxx = GA * (kxs * cs * cs + kys * ss * ss);
+    const double syy = GA * (kxs * ss * ss + kys * cs * cs);
+    const double sxy = GA * (kys - kxs) * ss * cs;
+    math::M6 k{};
+    k[0][0] = sxx;
+    k[0][1] = k[1][0] = -sxy;
+    k[1][1] = syy;
+    k[2][2] = EA;
+    k[2][3] = k[3][2] = EA * y_C;
+    k[2][4] = k[4][2] = -EA * x_C;
+    k[3][3] = bxx + EA * y_C * y_C;
+    k[3][4] = k[4][3] = -bxy - EA * x_C * y_C;
+    k[4][4] = byy + EA * x_C * x_C;
+    k[0][5] = k[5][0] = -sxx * y_S - sxy * x_S;
+    k[1][5] = k[5][1] = sxy * y_S + syy * x_S;
+    k[5][5] = GKt + sxx * y_S * y_S + 2. * sxy * x_S * y_S + syy * x_S * x_S;
+    return k;
+}
+
+inline math::M6 GenerateMassMatrix(double m, double I_x, double I_y, double I_p, double x_G = 0., double y_G = 0.,
+                                   double theta_i = 0.) {
+    const double ci = std::cos(theta_i), si = std::sin(theta_i);
+    const double ixx = I_x * ci * ci + I_y * si * si;
+    const double iyy = I_x * si * si + I_y * ci * ci;
+    const double ixy = (I_y - I_x) * si * ci;
+    math::M6 M{};
+    M[0][0] = M[1][1] = M[2][2] = m;
+    M[0][5] = M[5][0] = -m * y_G;
+    M[1][5] = M[5][1] = m * x_G;
+    M[2][3] = M[3][2] = m * y_G;
+    M[2][4] = M[4][2] = -m * x_G;
+    M[3][3] = ixx + m * y_G * y_G;
+    M[3][4] = M[4][3] = -ixy - m * x_G * y_G;
+    M[4][4] = iyy + m * x_G * x_G;
+    M[5][5] = I_p + m * (x_G * x_G + y_G * y_G);
+    return M;
+}
+
+struct HollowCircleProperties {
+    double area, Ixx, Iyy, J, kx, ky;
+};
+
+// Area, second moments and polar moment of a tube of outer diameter D and
+// wall t, Timoshenko shear factor 6 (1 + nu) / (7 + 6 nu).
+inline HollowCircleProperties CalculateHollowCircleProperties(double D, double t, double nu = 0.33) {
+    if (t >= D / 2.) throw std::invalid_argument("wall thickness must be less than the outer radius");
+    const double ro = D / 2., ri = ro - t;
+    const double area = std::numbers::pi * (ro * ro - ri * ri);
+    const double I = std::numbers::pi * (std::pow(ro, 4) - std::pow(ri, 4)) / 4.;
+    const double k = 6. * (1. + nu) / (7. + 6. * nu);
+    return {area, I, I, 2. * I, k, k};
+}
+
+inline BeamSection GenerateHollowCircleSection(double s, double E, double G, double rho, double D, double t,
+                                               double nu, double x_C = 0., double y_C = 0., double theta_p = 0.,
+                                               double x_S = 0., double y_S = 0., double theta_s = 0.,
+                                               double x_G = 0., double y_G = 0., double theta_i = 0.) {
+    const auto p = CalculateHollowCircleProperties(D, t, nu);
+    const double Ix = rho * p.Ixx, Iy = rho * p.Iyy;
+    return {s, GenerateMassMatrix(rho * p.area, Ix, Iy, Ix + Iy, x_G, y_G, theta_i),
+            GenerateStiffnessMatrix(E * p.area, E * p.Ixx, E * p.Iyy, G * p.J, G * p.area, p.kx, p.ky, x_C, y_C,
+                                    theta_p, x_S, y_S, theta_s)};
+}
+
+}  // namespace beams
+
+// ---- turbine: tower, drive train, hub, blades -----------------------------------------
+namespace components {
+
+// src/interfaces/components/turbine_input.hpp
+struct TurbineInput {
+    std::vector<BeamInput> blades;
+    BeamInput tower;
+    math::M6 yaw_bearing_inertia_matrix{};
+    math::M6 hub_inertia_matrix{};
+    std::array<double, 7> tower_base_position{0., 0., 0., 1., 0., 0., 0.};
+    double tower_axis_to_rotor_apex = 0.;
+    double tower_top_to_rotor_apex = 0.;
+    double rotor_apex_to_hub = 0.;
+    double hub_diameter = 1e-7;
+    double nacelle_yaw_angle = 0.;
+    double shaft_tilt_angle = 0.;
+    double cone_angle = 0.;
+    double blade_pitch_angle = 0.;
+    double azimuth_angle = 0.;
+    double rotor_speed = 0.;
+};
+
+struct ConstraintData {
+    size_t id;
+};
+
+// src/interfaces/components/turbine.cpp: the blades and the tower as beam
+// components; a yaw bearing at the tower top (nacelle mass), a shaft base, an
+// azimuth node, a hub (hub mass) and one apex node per blade, placed by the
+// turbine's geometry (tower axis to z, blades to z at the hub radius, cone,
+// azimuth spacing, shaft tilt, rotor apex); the joints tower top -> yaw
+// bearing (RotationControl about z, yaw), yaw bearing -> shaft base (rigid),
+// shaft base -> azimuth (revolute about the shaft axis, generator torque),
+// azimuth -> hub (rigid), hub -> apex (rigid) and blade root -> apex
+// (RotationControl about the pitch axis); initial pitch, yaw and tower-base
+// displacements, a PrescribedBC at the tower base and the rotor's initial
+// speed about the shaft.  The constraints read blade_pitch_control,
+// yaw_control and torque_control before every step, so a Turbine stays where
+// it was built.
+class Turbine {
+public:
+    static constexpr size_t invalid_id = static_cast<size_t>(-1);
+    static constexpr double kMinHubDiameter = 1e-8;
+    static constexpr double kZeroTolerance = 1e-12;
+
+    std::vector<Beam> blades;
+    Beam tower;
+    size_t hub_mass_element_id = invalid_id;
+    size_t yaw_bearing_mass_element_id = invalid_id;
+    std::vector<NodeData> apex_nodes;
+    NodeData hub_node{invalid_id};
+    NodeData azimuth_node{invalid_id};
+    NodeData shaft_base_node{invalid_id};
+    NodeData yaw_bearing_node{invalid_id};
+    ConstraintData tower_base{invalid_id};
+    ConstraintData tower_top_to_yaw_bearing{invalid_id};
+    ConstraintData yaw_bearing_to_shaft_base{invalid_id};
+    ConstraintData shaft_base_to_azimuth{invalid_id};
+    ConstraintData azimuth_to_hub{invalid_id};
+    std::vector<ConstraintData> blade_pitch;
+    std::vector<ConstraintData> apex_to_hub;
+    std::vector<double> blade_pitch_control;
+    double torque_control = 0.;
+    double yaw_control = 0.;
+
+    Turbine(const TurbineInput& in, Model& model)
+        : blades(CreateBlades(in.blades, model)), tower(in.tower, model),
+          blade_pitch_control(in.blades.size(), in.blade_pitch_angle) {
+        if (in.hub_diameter <= kMinHubDiameter) throw std::invalid_argument("hub diameter must be > 1e-8");
+        if (in.rotor_speed < 0.) throw std::invalid_argument("rotor speed must be >= 0");
+        if (blades.empty()) throw std::invalid_argument("a turbine needs at least one blade");
+        PositionNodes(in, model);
+        yaw_bearing_mass_element_id = model.AddMassElement(yaw_bearing_node.id, in.yaw_bearing_inertia_matrix);
+        hub_mass_element_id = model.AddMassElement(hub_node.id, in.hub_inertia_matrix);
+        AddConstraints(in, model);
+        SetInitialDisplacements(in, model);
+        SetInitialRotorVelocity(in, model);
+    }
+    Turbine(const Turbine&) = delete;
+    Turbine& operator=(const Turbine&) = delete;
+
+private:
+    std::vector<size_t> tower_node_ids_, nacelle_node_ids_, rotor_node_ids_, blade_node_ids_;
+
+    static std::vector<Beam> CreateBlades(const std::vector<BeamInput>& inputs, Model& model) {
+        std::vector<Beam> out;
+        for (const auto& b : inputs) out.emplace_back(b, model);
+        return out;
+    }
+
+    void PositionNodes(const TurbineInput& in, Model& model) {
+        const std::array<double, 3> origin{0., 0., 0.};
+        const double blade_angle = 2. * std::numbers::pi / static_cast<double>(blades.size());
+        const auto q_x_to_z = RotationVectorToQuaternion({0., -std::numbers::pi / 2., 0.});
+        const auto q_cone = RotationVectorToQuaternion({0., -in.cone_angle, 0.});
+        model.RotateBeamAboutPoint(tower.beam_element_id, q_x_to_z, origin);
+        const auto& top = model.GetNode(tower.nodes.back().id);
+        const std::array<double, 3> apex{top.x0[0] - in.tower_axis_to_rotor_apex, top.x0[1],
+                                         top.x0[2] + in.tower_top_to_rotor_apex};
+        CreateIntermediateNodes(in, model);
+        for (size_t b = 0; b < blades.size(); ++b) {
+            std::vector<size_t> ids;
+            for (const auto& n : blades[b].nodes) ids.push_back(n.id);
+            for (size_t id : ids) {
+                model.GetNode(id).RotateAboutPoint(q_x_to_z, origin);
+                model.GetNode(id).Translate({0., 0., in.hub_diameter / 2.});
+            }
+            ids.push_back(apex_nodes[b].id);
+            const auto q_az = RotationVectorToQuaternion({static_cast<double>(b) * blade_angle, 0., 0.});
+            for (size_t id : ids) {
+                model.GetNode(id).RotateAboutPoint(q_cone, origin);
+                model.GetNode(id).RotateAboutPoint(q_az, origin);
+            }
+        }
+        const auto q_tilt = RotationVectorToQuaternion({0., in.shaft_tilt_angle, 0.});
+        for (size_t id : rotor_node_ids_) {
+            model.GetNode(id).RotateAboutPoint(q_tilt, origin);
+            model.GetNode(id).Translate(apex);
+        }
+    }
+
+    void CreateIntermediateNodes(const TurbineInput& in, Model& model) {
+        const double shaft_length = in.tower_axis_to_rotor_apex / std::cos(in.shaft_tilt_angle);
+        const auto top = model.GetNode(tower.nodes.back().id).x0;
+        hub_node = NodeData(model.AddNode().SetPosition(-in.rotor_apex_to_hub, 0., 0., 1., 0., 0., 0.).Build());
+        azimuth_node = NodeData(model.AddNode().SetPosition(shaft_length, 0., 0., 1., 0., 0., 0.).Build());
+        shaft_base_node = NodeData(model.AddNode().SetPosition(shaft_length, 0., 0., 1., 0., 0., 0.).Build());
+        yaw_bearing_node = NodeData(model.AddNode().SetPosition(top[0], top[1], top[2], 1., 0., 0., 0.).Build());
+        for (size_t b = 0; b < blades.size(); ++b)
+            apex_nodes.emplace_back(model.AddNode().SetPosition(0., 0., 0., 1., 0., 0., 0.).Build());
+        for (const auto& n : tower.nodes) tower_node_ids_.push_back(n.id);
+        for (size_t b = 0; b < blades.size(); ++b) {
+            for (const auto& n : blades[b].nodes) blade_node_ids_.push_back(n.id);
+            blade_node_ids_.push_back(apex_nodes[b].id);
+        }
+        rotor_node_ids_ = {hub_node.id, azimuth_node.id, shaft_base_node.id};
+        rotor_node_ids_.insert(rotor_node_ids_.end(), blade_node_ids_.begin(), blade_node_ids_.end());
+        nacelle_node_ids_ = {yaw_bearing_node.id, shaft_base_node.id, azimuth_node.id, hub_node.id};
+        nacelle_node_ids_.insert(nacelle_node_ids_.end(), blade_node_ids_.begin(), blade_node_ids_.end());
+    }
+
+    void AddConstraints(const TurbineInput& in, Model& model) {
+        for (size_t b = 0; b < blades.size(); ++b) {
+            const auto& apex = model.GetNode(apex_nodes[b].id);
+            const auto& root = model.GetNode(blades[b].nodes[0].id);
+            const std::array<double, 3> pitch_axis{root.x0[0] - apex.x0[0], root.x0[1] - apex.x0[1],
+                                                   root.x0[2] - apex.x0[2]};
+            blade_pitch.push_back({model.AddRotationControl({root.id, apex.id}, pitch_axis, &blade_pitch_control[b])});
+            apex_to_hub.push_back({model.AddRigidJointConstraint({hub_node.id, apex_nodes[b].id})});
+        }
+        azimuth_to_hub = {model.AddRigidJointConstraint({azimuth_node.id, hub_node.id})};
+        const std::array<double, 3> shaft_axis{-std::cos(in.shaft_tilt_angle), 0., std::sin(in.shaft_tilt_angle)};
+        shaft_base_to_azimuth = {
+            model.AddRevoluteJointConstraint({shaft_base_node.id, azimuth_node.id}, shaft_axis, &torque_control)};
+        yaw_bearing_to_shaft_base = {model.AddRigidJointConstraint({yaw_bearing_node.id, shaft_base_node.id})};
+        yaw_control = in.nacelle_yaw_angle;
+        tower_top_to_yaw_bearing = {
+            model.AddRotationControl({tower.nodes.back().id, yaw_bearing_node.id}, {0., 0., 1.}, &yaw_control)};
+    }
+
+    // Node::RotateDisplacementAboutPoint (src/model/node.hpp:152-187)
+    static void RotateDisplacement(Node& n, const std::array<double, 4>& q, const std::array<double, 3>& p) {
+        const auto d = n.DisplacedPosition();
+        const auto r = RotateVectorByQuaternion(q, {d[0] - p[0], d[1] - p[1], d[2] - p[2]});
+        for (int k = 0; k < 3; ++k) n.u[k] = r[k] + p[k] - n.x0[k];
+        const auto qn = QuaternionCompose(q, {n.u[3], n.u[4], n.u[5], n.u[6]});
+        for (int k = 0; k < 4; ++k) n.u[3 + k] = qn[k];
+    }
+
+    void SetInitialDisplacements(const TurbineInput& in, Model& model) {
+        for (size_t b = 0; b < blades.size(); ++b) {
+            const auto& root = model.GetNode(blades[b].nodes.front().id);
+            const auto& apex = model.GetNode(apex_nodes[b].id);
+            const auto axis = math::Unit({root.x0[0] - apex.x0[0], root.x0[1] - apex.x0[1], root.x0[2] - apex.x0[2]});
+            const auto q_pitch = RotationVectorToQuaternion(
+                {in.blade_pitch_angle * axis[0], in.blade_pitch_angle * axis[1], in.blade_pitch_angle * axis[2]});
+            const std::array<double, 3> center{apex.x0[0], apex.x0[1], apex.x0[2]};
+            for (const auto& n : blades[b].nodes) RotateDisplacement(model.GetNode(n.id), q_pitch, center);
+        }
+        if (std::abs(in.nacelle_yaw_angle) > kZeroTolerance) {
+            const auto& top = model.GetNode(tower.nodes.back().id);
+            const std::array<double, 3> center{top.x0[0], top.x0[1], top.x0[2]};
+            const auto q_yaw = RotationVectorToQuaternion({0., 0., in.nacelle_yaw_angle});
+            for (size_t id : nacelle_node_ids_) RotateDisplacement(model.GetNode(id), q_yaw, center);
+        }
+        auto& base = model.GetNode(tower.nodes.front().id);
+        const std::array<double, 3> ref{base.x0[0], base.x0[1], base.x0[2]};
+        const std::array<double, 3> d{in.tower_base_position[0] - ref[0], in.tower_base_position[1] - ref[1],
+                                      in.tower_base_position[2] - ref[2]};
+        const std::array<double, 4> qb{in.tower_base_position[3], in.tower_base_position[4],
+                                       in.tower_base_position[5], in.tower_base_position[6]};
+        const bool identity = std::abs(qb[0] - 1.) <= kZeroTolerance && std::abs(qb[1]) <= kZeroTolerance &&
+                              std::abs(qb[2]) <= kZeroTolerance && std::abs(qb[3]) <= kZeroTolerance;
+        if (std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) > kZeroTolerance || !identity) {
+            std::vector<size_t> all = tower_node_ids_;
+            all.insert(all.end(), nacelle_node_ids_.begin(), nacelle_node_ids_.end());
+            for (size_t id : all) {
+                auto& n = model.GetNode(id);
+                RotateDisplacement(n, qb, ref);
+                for (int k = 0; k < 3; ++k) n.u[k] += d[k];
+            }
+        }
+        tower_base = {model.AddPrescribedBC(base.id, base.u)};
+    }
+
+    void SetInitialRotorVelocity(const TurbineInput& in, Model& model) {
+        const auto hp = model.GetNode(hub_node.id).DisplacedPosition();
+        const auto sp = model.GetNode(shaft_base_node.id).DisplacedPosition();
+        const auto axis = math::Unit({hp[0] - sp[0], hp[1] - sp[1], hp[2] - sp[2]});
+        std::vector<size_t> ids{hub_node.id, azimuth_node.id};
+        for (size_t b = 0; b < blades.size(); ++b) {
+            for (const auto& n : blades[b].nodes) ids.push_back(n.id);
+            ids.push_back(apex_nodes[b].id);
+        }
+        const std::array<double, 6> vel{0., 0., 0., in.rotor_speed * axis[0], in.rotor_speed * axis[1],
+                                        in.rotor_speed * axis[2]};
+        for (size_t id : ids) model.GetNode(id).SetVelocityAboutPoint(vel, {hp[0], hp[1], hp[2]});
+    }
+};
+
+// src/interfaces/components/turbine_builder.hpp
+class TurbineBuilder {
+public:
+    BeamBuilder& Blade(size_t i) {
+        if (i >= blades_.size()) blades_.resize(i + 1);
+        return blades_[i];
+    }
+    BeamBuilder& Tower() { return tower_; }
+    TurbineBuilder& SetYawBearingInertiaMatrix(const math::M6& m) { in_.yaw_bearing_inertia_matrix = m; return *this; }
+    TurbineBuilder& SetHubInertiaMatrix(const math::M6& m) { in_.hub_inertia_matrix = m; return *this; }
+    TurbineBuilder& SetTowerBasePosition(const std::array<double, 7>& p) { in_.tower_base_position = p; return *this; }
+    TurbineBuilder& SetTowerAxisToRotorApex(double d) { in_.tower_axis_to_rotor_apex = d; return *this; }
+    TurbineBuilder& SetTowerTopToRotorApex(double h) { in_.tower_top_to_rotor_apex = h; return *this; }
+    TurbineBuilder& SetRotorApexToHub(double d) { in_.rotor_apex_to_hub = d; return *this; }
+    TurbineBuilder& SetHubDiameter(double d) { in_.hub_diameter = d; return *this; }
+    TurbineBuilder& SetShaftTiltAngle(double a) { in_.shaft_tilt_angle = a; return *this; }
+    TurbineBuilder& SetNacelleYawAngle(double a) { in_.nacelle_yaw_angle = a; return *this; }
+    TurbineBuilder& SetConeAngle(double a) { in_.cone_angle = a; return *this; }
+    TurbineBuilder& SetBladePitchAngle(double a) { in_.blade_pitch_angle = a; return *this; }
+    TurbineBuilder& SetAzimuthAngle(double a) { in_.azimuth_angle = a; return *this; }
+    TurbineBuilder& SetRotorSpeed(double w) { in_.rotor_speed = w; return *this; }
+    TurbineInput Input() const {
+        TurbineInput in = in_;
+        in.blades.clear();
+        for (const auto& b : blades_) in.blades.push_back(b.Input());
+        in.tower = tower_.Input();
+        return in;
+    }
+
+private:
+    TurbineInput in_;
+    std::vector<BeamBuilder> blades_;
+    BeamBuilder tower_;
+};
+
+}  // namespace components
+
+// src/interfaces/turbine/turbine_interface.hpp: the turbine with node loads in
+// (state.f) and the motion of the blade and tower nodes out after each step,
+// a saved state for predictor-corrector coupling.  The aerodynamics, the
+// controller library and the NetCDF outputs of the reference's interface are
+// outside this path.
+class TurbineInterface {
+public:
+    TurbineInterface(const Context& ctx, const components::SolutionInput& sol, const components::TurbineInput& in)
+        : ctx_(ctx), model_(sol.gravity), turbine_(in, model_), parameters_(sol.Parameters()) {
+        auto [state, elements, constraints, solver] = model_.CreateSystemWithSolver(ctx_);
+        state_ = std::make_unique<State>(state);
+        elements_ = std::make_unique<Elements>(elements);
+        constraints_ = std::make_unique<Constraints>(constraints);
+        solver_ = std::make_unique<Solver>(solver);
+        saved_ = kyn_model_clone(ctx_.get(), solver_->model()->id);
+        check(ctx_.get(), saved_);
+        loads_.assign(solver_->model()->info.num_nodes * 6, 0.);
+        GetMotion();
+    }
+    TurbineInterface(const TurbineInterface&) = delete;
+    TurbineInterface& operator=(const TurbineInterface&) = delete;
+    ~TurbineInterface() {
+        if (saved_ >= 0) kyn_model_destroy(ctx_.get(), saved_);
+    }
+
+    components::Turbine& Turbine() { return turbine_; }
+    const Model& GetModel() const { return model_; }
+    const Solver& GetSolver() const { return *solver_; }
+
+    // Node loads of the blades and the tower -> state.f, the controls into
+    // their constraints, one step, motion back (false: max_iter reached).
+    bool Step() {
+        std::fill(loads_.begin(), loads_.end(), 0.);
+        auto put = [&](const components::Beam& b) {
+            for (const auto& n : b.nodes)
+                for (int c = 0; c < 6; ++c) loads_[n.id * 6 + c] = n.loads[c];
+        };
+        for (const auto& b : turbine_.blades) put(b);
+        put(turbine_.tower);
+        state_->SetExternalForces(loads_);
+        if (!kynema_b200::Step(parameters_, *solver_, *elements_, *state_, *constraints_)) return false;
+        GetMotion();
+        return true;
+    }
+    void SaveState() { check(ctx_.get(), kyn_state_copy(ctx_.get(), saved_, solver_->model()->id)); }
+    void RestoreState() {
+        check(ctx_.get(), kyn_state_copy(ctx_.get(), solver_->model()->id, saved_));
+        GetMotion();
+    }
+
+private:
+    void GetMotion() {
+        const auto x = state_->Get(KYN_FIELD_X), q = state_->q(), v = state_->v(), vd = state_->vd();
+        auto get = [&](components::Beam& b) {
+            for (auto& n : b.nodes) {
+                for (int c = 0; c < 7; ++c) {
+                    n.position[c] = x[n.id * 7 + c];
+                    n.displacement[c] = q[n.id * 7 + c];
+                }
+                for (int c = 0; c < 6; ++c) {
+                    n.velocity[c] = v[n.id * 6 + c];
+                    n.acceleration[c] = vd[n.id * 6 + c];
+                }
+            }
+        };
+        for (auto& b : turbine_.blades) get(b);
+        get(turbine_.tower);
+    }
+
+    Context ctx_;
+    Model model_;
+    components::Turbine turbine_;
+    StepParameters parameters_;
+    std::unique_ptr<State> state_;
+    std::unique_ptr<Elements> elements_;
+    std::unique_ptr<Constraints> constraints_;
+    std::unique_ptr<Solver> solver_;
+    int saved_ = -1;
+    std::vector<double> loads_;
+};
+
+// src/interfaces/turbine/turbine_interface_builder.hpp
+class TurbineInterfaceBuilder {
+public:
+    components::SolutionBuilder& Solution() { return solution_; }
+    components::TurbineBuilder& Turbine() { return turbine_; }
+    TurbineInterface Build(const Context& ctx = Context(0)) const {
+        return TurbineInterface(ctx, solution_.Input(), turbine_.Input());
+    }
+
+private:
+    components::SolutionBuilder solution_;
+    components::TurbineBuilder turbine_;
+};
+
 // ---- CFD interface: floating platform with mooring lines --------------------------
 // src/interfaces/cfd/: a platform node with its mass, and per mooring line a
 // position-only fairlead rigidly carried by the platform

@@ -412,6 +412,7 @@ void prepare_model(DevModel* m) {
         k.comp_maxQ = hb.comp_maxQ;
         k.cond_nd = hb.cond_nd;
         k.cond_md = hb.cond_md_off >= 0 ? m->d_slab[b] + hb.cond_md_off : nullptr;
+        k.con_frames = hb.frames_off >= 0 ? m->d_slab[b] + hb.frames_off : nullptr;
         for (int s2 = 0; s2 < kMaxBeamConstraints; ++s2) k.con_base[s2] = hb.con_base[s2];
         m->kt.push_back(k);
     }

@@ -151,9 +151,30 @@ static void init_node_state(const kyn_model_desc* d, const HostBeam& B, const Sl
     }
 }
 
+// Frame of a revolute joint (src/constraints/constraints.hpp:294-319): x_hat =
+// unit(axis), or unit(X0) for a zero axis; the rows of the rotation taking
+// (1, 0, 0) to x_hat are the joint axes x0, y0, z0.
+static int revolute_frame(const double* ax, const double X0[3], double axes[9], std::string& err) {
+    const double na = ax ? std::sqrt(ax[0] * ax[0] + ax[1] * ax[1] + ax[2] * ax[2]) : 0.;
+    const double* src = na != 0. ? ax : X0;
+    const double ns = std::sqrt(src[0] * src[0] + src[1] * src[1] + src[2] * src[2]);
+    if (!(ns > 0.)) return fail(err, KYN_ERR_INVALID, "revolute joint needs an axis or distinct node positions");
+    const double xh[3] = {src[0] / ns, src[1] / ns, src[2] / ns};
+    const double cp[3] = {0., -xh[2], xh[1]};
+    const double dp = xh[0];
+    if (!(1. + dp > 0.)) return fail(err, KYN_ERR_UNSUPPORTED, "revolute joint axis along -x");
+    const double kk = 1. / (1. + dp);
+    const double R[9] = {cp[0] * cp[0] * kk + dp, cp[1] * cp[0] * kk + cp[2], cp[2] * cp[0] * kk - cp[1],
+                         cp[0] * cp[1] * kk - cp[2], cp[1] * cp[1] * kk + dp, cp[2] * cp[1] * kk + cp[0],
+                         cp[0] * cp[2] * kk + cp[1], cp[1] * cp[2] * kk - cp[0], cp[2] * cp[2] * kk + dp};
+    for (int k = 0; k < 9; ++k) axes[k] = R[k];
+    return KYN_OK;
+}
+
 // A model with beam elements whose constraints the per-beam systems cannot
-// take: three-row constraints, or a joint whose base node is a beam node
-// (beams coupled to each other, a beam carrying a position-only node).
+// take: three-row constraints, a joint whose base node is a beam node (beams
+// coupled to each other, a beam carrying a position-only node), or more than
+// one revolute joint (the per-beam systems take one, in a drive train).
 static bool needs_dense_beams(const kyn_model_desc* d) {
     if (d->num_beams <= 0 || d->num_constraints <= 0 || !d->constraint_type) return false;
     std::vector<char> in_beam(d->num_nodes, 0);
@@ -161,15 +182,17 @@ static bool needs_dense_beams(const kyn_model_desc* d) {
         const int id = d->beam_node_ids[k];
         if (id >= 0 && id < d->num_nodes) in_beam[id] = 1;
     }
+    int revolute = 0;
     for (int c = 0; c < d->num_constraints; ++c) {
         const int t = d->constraint_type[c];
         const int base = d->constraint_base_node ? d->constraint_base_node[c] : -1;
         if (t >= KYN_CONSTRAINT_FIXED_BC_3DOF) return true;
-        if ((is_hub_joint(t) || t == KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF) && base >= 0 &&
-            base < d->num_nodes && in_beam[base])
+        if ((is_hub_joint(t) || t == KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF || t == KYN_CONSTRAINT_REVOLUTE_JOINT) &&
+            base >= 0 && base < d->num_nodes && in_beam[base])
             return true;
+        revolute += t == KYN_CONSTRAINT_REVOLUTE_JOINT;
     }
-    return false;
+    return revolute > 1;
 }
 
 // FreedomSignature bits of every node in a dense model
@@ -507,7 +530,16 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
     // azimuth [-> rigid joint -> hub], whose last node is the joints' base.
     const int ncon = (d->num_constraints > 0 && d->constraint_type) ? d->num_constraints : 0;
     auto base_of = [&](int c) { return d->constraint_base_node ? d->constraint_base_node[c] : -1; };
-    for (int c = 0; c < ncon; ++c) {
+    // A lumped model with three-row constraints or joints between its nodes is
+    // solved as the reference's dense bordered system (one CTA, pivoted LU);
+    // a dense model takes its revolute joints as constraint rows, not as a
+    // drive train.
+    bool dense = dense_beams;
+    for (int c = 0; c < ncon && lumped; ++c) {
+        const int t = d->constraint_type[c];
+        dense |= is_hub_joint(t) || t >= KYN_CONSTRAINT_FIXED_BC_3DOF || t == KYN_CONSTRAINT_REVOLUTE_JOINT;
+    }
+    for (int c = 0; c < ncon && !dense; ++c) {
         if (d->constraint_type[c] != KYN_CONSTRAINT_REVOLUTE_JOINT) continue;
         if (M.rev_con >= 0) return fail(err, KYN_ERR_UNSUPPORTED, "more than one revolute joint in a model");
         M.rev_con = c;
@@ -555,11 +587,6 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
     std::vector<std::vector<int>> node_cols(nn);   // constraint row blocks coupled to a node
     static const double ident7[7] = {0., 0., 0., 1., 0., 0., 0.};
     int joints = 0;
-    // A lumped model with three-row constraints or joints between its nodes is
-    // solved as the reference's dense bordered system (one CTA, pivoted LU).
-    bool dense = dense_beams;
-    for (int c = 0; c < d->num_constraints && lumped; ++c)
-        dense |= is_hub_joint(d->constraint_type[c]) || d->constraint_type[c] >= KYN_CONSTRAINT_FIXED_BC_3DOF;
     if (!lumped && !dense_beams)
         for (int c = 0; c < d->num_constraints; ++c)
             if (d->constraint_type[c] >= KYN_CONSTRAINT_FIXED_BC_3DOF)
@@ -569,15 +596,17 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
         HostBeam& B = M.beams[0];
         B.dense = true;
         if (d->num_constraints > kMaxBeamConstraints)
-            return fail(err, KYN_ERR_UNSUPPORTED, "more than 8 constraints in a dense model");
+            return fail(err, KYN_ERR_UNSUPPORTED, "more than 16 constraints in a dense model");
         const SlabLayout L = make_slab_layout(B.N, 0);
+        std::vector<double> frames(static_cast<size_t>(d->num_constraints) * 9, 0.);
+        bool any_revolute = false;
         for (int c = 0; c < d->num_constraints; ++c) {
             const int t = d->constraint_type[c];
             const int node = d->constraint_target_node[c];
             if (node < 0 || node >= nn) return fail(err, KYN_ERR_INVALID, "constraint node out of range");
-            const bool joint = is_hub_joint(t) || t == KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF;
-            if (t < KYN_CONSTRAINT_FIXED_BC || t > KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF ||
-                t == KYN_CONSTRAINT_REVOLUTE_JOINT)
+            const bool joint = is_hub_joint(t) || t == KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF ||
+                               t == KYN_CONSTRAINT_REVOLUTE_JOINT;
+            if (t < KYN_CONSTRAINT_FIXED_BC || t > KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF)
                 return fail(err, KYN_ERR_UNSUPPORTED, "constraint type outside the dense-model path");
             const int base = joint ? base_of(c) : -1;
             if (joint && (base < 0 || base >= nn || base == node))
@@ -610,6 +639,16 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
                 if (!(nrm > 0.)) return fail(err, KYN_ERR_INVALID, "rotation control needs a nonzero axis");
                 for (int k = 0; k < 3; ++k) B.con_axis[slot][k] = ax[k] / nrm;
             }
+            if (t == KYN_CONSTRAINT_REVOLUTE_JOINT) {
+                const int rc = revolute_frame(ax, B.con_X0[slot], frames.data() + slot * 9, err);
+                if (rc != KYN_OK) return rc;
+                any_revolute = true;
+            }
+        }
+        if (any_revolute) {  // the joints' frames after the slab's other records
+            if (B.slab.size() & 1) B.slab.push_back(0.);
+            B.frames_off = static_cast<int>(B.slab.size());
+            B.slab.insert(B.slab.end(), frames.begin(), frames.begin() + B.nc * 9);
         }
     }
     for (int c = 0; c < d->num_constraints && !dense; ++c) {
@@ -737,25 +776,9 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
         double X0[3], axes[9] = {};
         for (int k = 0; k < 3; ++k) X0[k] = x0[k] - d->node_x0[prev * 7 + k];
         if (r == 1) {
-            // src/constraints/constraints.hpp:294-319: x_hat = unit(axis), or
-            // unit(X0) for a zero axis; rows of the rotation taking (1, 0, 0)
-            // to x_hat are the joint axes
-            const double* ax = d->constraint_axis ? d->constraint_axis + M.rev_con * 3 : nullptr;
-            const double na = ax ? std::sqrt(ax[0] * ax[0] + ax[1] * ax[1] + ax[2] * ax[2]) : 0.;
-            const double* src = na != 0. ? ax : X0;
-            const double ns = std::sqrt(src[0] * src[0] + src[1] * src[1] + src[2] * src[2]);
-            if (!(ns > 0.))
-                return fail(err, KYN_ERR_INVALID, "revolute joint needs an axis or distinct node positions");
-            const double xh[3] = {src[0] / ns, src[1] / ns, src[2] / ns};
-            const double cp[3] = {0., -xh[2], xh[1]};
-            const double dp = xh[0];
-            if (!(1. + dp > 0.))
-                return fail(err, KYN_ERR_UNSUPPORTED, "revolute joint axis along -x");
-            const double kk = 1. / (1. + dp);
-            const double R[9] = {cp[0] * cp[0] * kk + dp, cp[1] * cp[0] * kk + cp[2], cp[2] * cp[0] * kk - cp[1],
-                                 cp[0] * cp[1] * kk - cp[2], cp[1] * cp[1] * kk + dp, cp[2] * cp[1] * kk + cp[0],
-                                 cp[0] * cp[2] * kk + cp[1], cp[1] * cp[2] * kk - cp[0], cp[2] * cp[2] * kk + dp};
-            for (int k = 0; k < 9; ++k) axes[k] = R[k];
+            const int rc = revolute_frame(d->constraint_axis ? d->constraint_axis + M.rev_con * 3 : nullptr, X0,
+                                          axes, err);
+            if (rc != KYN_OK) return rc;
         }
         for (auto& B : M.beams) {
             const SlabLayout L = make_slab_layout(B.N, B.Q);
@@ -795,7 +818,8 @@ int build_host_model(const kyn_model_desc* d, HostModel& M, std::string& err) {
         for (int c = 0; c < d->num_constraints; ++c) {
             const int t = d->constraint_type[c];
             sig[d->constraint_target_node[c]] |= t >= KYN_CONSTRAINT_FIXED_BC_3DOF ? kSigPosition : kSigAll;
-            if (is_hub_joint(t) || t == KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF) sig[base_of(c)] |= kSigAll;
+            if (is_hub_joint(t) || t == KYN_CONSTRAINT_RIGID_JOINT_6DOF_TO_3DOF || t == KYN_CONSTRAINT_REVOLUTE_JOINT)
+                sig[base_of(c)] |= kSigAll;
         }
         for (int k = 0; dense_beams && k < d->beam_node_offsets[d->num_beams]; ++k)
             sig[d->beam_node_ids[k]] |= kSigAll;  // beam nodes (FreedomSignature AllComponents)

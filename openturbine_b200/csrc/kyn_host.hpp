@@ -38,6 +38,7 @@ struct HostBeam {
                                          -1, -1, -1, -1, -1, -1, -1, -1};  // dense: joint base (local)
     int cond_nd = 0;                  // condensed dense model: bordered-system unknowns, else 0
     int cond_md_off = -1;             // offset of that system in the slab when it lives in device memory
+    int frames_off = -1;              // dense model with revolute joints: [nc][9] joint frames in the slab
     int n_mass = 0, n_spring = 0;     // point masses / springs at this beam's nodes
     int lumped_off = 0;               // their records' offset in the slab (kMassRec, kSpringRec)
 };

@@ -1769,6 +1769,69 @@ __device__ void dense_beam_terms(const KBeam& KB, const StepCoeffs& P, const Den
     }
 }
 
+// Record of a revolute joint in a dense model (constraint record layout drev;
+// multipliers at conrec::lam, torque at conrec::inp): residual, the gradient
+// rows B = G T on both nodes' rotations, G^T lambda and the torque about the
+// target's joint axis (calculate_revolute_joint_constraint.hpp:19-113,
+// calculate_revolute_joint_force.hpp:19-45, branch :388-465 of
+// calculate_constraint_residual_gradient.hpp), as revolute_record computes it
+// for the drive train's hub chain.  frame: x0, y0, z0 of the joint (rows).
+namespace drev {
+constexpr int Phi = 0;    // [5]
+constexpr int Bt = 5;     // [2][3] rows 3-4 of G_target T_target (rotation)
+constexpr int Bb = 11;    // [2][3] rows 3-4 of G_base T_base (rotation)
+constexpr int sys = 17;   // [3] torque about R(target) x0
+constexpr int GtL = 20;   // [6] G_target^T lambda
+constexpr int GbL = 26;   // [6] G_base^T lambda
+constexpr int xcz = 50;   // [3] x cross z
+constexpr int xcy = 53;   // [3] x cross y
+}  // namespace drev
+__device__ inline void revolute_dense_record(double* cr, const double* bq, const double* tq, const double* frame,
+                                             const double* X0, const double* Tb, const double* Tt) {
+    double R1X0[3], x[3], y[3], z[3], ta[3];
+    for (int i = 0; i < 3; ++i) {
+        R1X0[i] = x[i] = y[i] = z[i] = ta[i] = 0.;
+        for (int j = 0; j < 3; ++j) {
+            R1X0[i] += rot_entry(bq + 3, i, j) * X0[j];
+            x[i] += rot_entry(bq + 3, i, j) * frame[j];
+            y[i] += rot_entry(tq + 3, i, j) * frame[3 + j];
+            z[i] += rot_entry(tq + 3, i, j) * frame[6 + j];
+            ta[i] += rot_entry(tq + 3, i, j) * frame[j];
+        }
+    }
+    for (int i = 0; i < 3; ++i) cr[drev::Phi + i] = tq[i] + X0[i] - bq[i] - R1X0[i];
+    cr[drev::Phi + 3] = z[0] * x[0] + z[1] * x[1] + z[2] * x[2];
+    cr[drev::Phi + 4] = y[0] * x[0] + y[1] * x[1] + y[2] * x[2];
+    const double xcz[3] = {x[1] * z[2] - x[2] * z[1], x[2] * z[0] - x[0] * z[2], x[0] * z[1] - x[1] * z[0]};
+    const double xcy[3] = {x[1] * y[2] - x[2] * y[1], x[2] * y[0] - x[0] * y[2], x[0] * y[1] - x[1] * y[0]};
+    const double torque = cr[conrec::inp];
+    for (int i = 0; i < 3; ++i) {
+        cr[drev::xcz + i] = xcz[i];
+        cr[drev::xcy + i] = xcy[i];
+        cr[drev::sys + i] = ta[i] * torque;
+    }
+    for (int j = 0; j < 3; ++j) {
+        double a0 = 0., a1 = 0., b0 = 0., b1 = 0.;
+        for (int k = 0; k < 3; ++k) {
+            a0 -= xcz[k] * Tt[k * 3 + j];
+            a1 -= xcy[k] * Tt[k * 3 + j];
+            b0 += xcz[k] * Tb[k * 3 + j];
+            b1 += xcy[k] * Tb[k * 3 + j];
+        }
+        cr[drev::Bt + j] = a0;
+        cr[drev::Bt + 3 + j] = a1;
+        cr[drev::Bb + j] = b0;
+        cr[drev::Bb + 3 + j] = b1;
+    }
+    const double* l = cr + conrec::lam;
+    for (int i = 0; i < 3; ++i) {
+        cr[drev::GtL + i] = l[i];
+        cr[drev::GbL + i] = -l[i];
+        cr[drev::GtL + 3 + i] = -xcz[i] * l[3] - xcy[i] * l[4];
+        cr[drev::GbL + 3 + i] = xcz[i] * l[3] + xcy[i] * l[4];
+    }
+}
+
 // ---- condensed beam components of a dense model (KBeam::cond_nd > 0) -------------
 // A component's local order: its interior nodes first (fmap < 0: nodes of this
 // component only, without masses, springs or constraints), then its boundary
@@ -2083,7 +2146,7 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
             }
         }
         int rows = 0;
-        for (int c = 0; c < nc; ++c) rows += KB.con_type[c] >= KYN_CONSTRAINT_FIXED_BC_3DOF ? 3 : 6;
+        for (int c = 0; c < nc; ++c) rows += constraint_rows(KB.con_type[c]);
         s_nsys = o;
         s_flag = cnd ? ((o + rows != md || o + oi + rows != nd) ? 2 : 0) : (o > nd) ? 2 : 0;
     }
@@ -2183,6 +2246,9 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
                             for (int k = 0; k < 3; ++k) bt += tilde_e(r1x0, i, k) * sT[bn * 9 + k * 3 + j];
                             cr[conrec::Btr + i * 3 + j] = bt;
                         }
+            } else if (t == KYN_CONSTRAINT_REVOLUTE_JOINT) {
+                revolute_dense_record(cr, sq + bn * 7, sq + tn * 7, KB.con_frames + tid * 9, KB.con_X0[tid],
+                                      sT + bn * 9, sT + tn * 9);
             } else {
                 constraint_record(cr, t, sq + tn * 7, KB.con_X0[tid], sT + tn * 9,
                                   bn >= 0 ? sq + bn * 7 : nullptr, bn >= 0 ? sT + bn * 9 : nullptr,
@@ -2197,8 +2263,35 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
             for (int c = 0; c < nc; ++c) {
                 const double* cr = con + c * kConStride;
                 const int t = KB.con_type[c], tn = KB.con_node[c], bn = KB.con_base[c];
-                const int rows = t >= KYN_CONSTRAINT_FIXED_BC_3DOF ? 3 : 6;
+                const int rows = constraint_rows(t);
                 const int ft = fmap[tn];
+                if (t == KYN_CONSTRAINT_REVOLUTE_JOINT) {  // five rows, gradients on both nodes
+                    const int fb = fmap[bn];
+                    for (int r = 0; r < 5; ++r) {
+                        double* row = Md + (rf + r) * md;
+                        if (r < 3) {
+                            row[ft + r] += 1.;
+                            Md[(ft + r) * md + rf + r] += 1.;
+                            row[fb + r] -= 1.;
+                            Md[(fb + r) * md + rf + r] -= 1.;
+                        } else {
+                            const double* v = cr + (r == 3 ? drev::xcz : drev::xcy);
+                            for (int j = 0; j < 3; ++j) {
+                                row[ft + 3 + j] += cr[drev::Bt + (r - 3) * 3 + j];
+                                row[fb + 3 + j] += cr[drev::Bb + (r - 3) * 3 + j];
+                                Md[(ft + 3 + j) * md + rf + r] -= v[j];
+                                Md[(fb + 3 + j) * md + rf + r] += v[j];
+                            }
+                        }
+                        b[rf + r] += cr[drev::Phi + r];
+                    }
+                    for (int e = 0; e < 6; ++e) {
+                        b[ft + e] += cr[drev::GtL + e] + (e >= 3 ? cr[drev::sys + e - 3] : 0.);
+                        b[fb + e] += cr[drev::GbL + e];
+                    }
+                    rf += 5;
+                    continue;
+                }
                 for (int r = 0; r < rows; ++r) {
                     double* row = Md + (rf + r) * md;
                     if (r < 3) {
@@ -2335,8 +2428,8 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
         if (tid < nc) {
             const double* cr = con + tid * kConStride;
             int rf = nsys;
-            for (int c = 0; c < tid; ++c) rf += KB.con_type[c] >= KYN_CONSTRAINT_FIXED_BC_3DOF ? 3 : 6;
-            const int rows = KB.con_type[tid] >= KYN_CONSTRAINT_FIXED_BC_3DOF ? 3 : 6;
+            for (int c = 0; c < tid; ++c) rf += constraint_rows(KB.con_type[c]);
+            const int rows = constraint_rows(KB.con_type[tid]);
             for (int r = 0; r < rows; ++r) {
                 const double e = x[rf + r] / (P.atol + P.rtol * fabs(cr[conrec::lam + r]));
                 part += e * e;
@@ -2363,8 +2456,8 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
         if (tid < nc) {
             double* cr = con + tid * kConStride;
             int rf = nsys;
-            for (int c = 0; c < tid; ++c) rf += KB.con_type[c] >= KYN_CONSTRAINT_FIXED_BC_3DOF ? 3 : 6;
-            const int rows = KB.con_type[tid] >= KYN_CONSTRAINT_FIXED_BC_3DOF ? 3 : 6;
+            for (int c = 0; c < tid; ++c) rf += constraint_rows(KB.con_type[c]);
+            const int rows = constraint_rows(KB.con_type[tid]);
             for (int r = 0; r < rows; ++r) cr[conrec::lam + r] += x[rf + r];
         }
         __syncthreads();

@@ -170,6 +170,7 @@ struct KBeam {
     int32_t comp_maxN, comp_maxQ;  // their largest node and quadrature-point counts
     int32_t cond_nd;          // condensed dense models: unknowns of the bordered system, else 0
     double* cond_md;          // condensed dense models: that system in device memory, or null (shared)
+    const double* con_frames; // dense models: [nc][9] frame (x0, y0, z0) of each revolute joint, or null
     double* conv;             // [kMaxNewtonIters] model convergence history (rank 0)
     double* dump;             // optional: last assembled system (see kyn_capi.cu)
     unsigned long long* prof; // optional: per-phase SM cycles, summed over beams

@@ -30,7 +30,11 @@ def build(force: bool = False) -> str:
     """Compile the oracle (and its FLOP-counting build) with its Makefile (g++,
     no GPU needed)."""
     flops = os.path.join(_HERE, "_build", "libkyn_oracle_flops.so")
-    if force or not os.path.exists(_LIB_PATH) or not os.path.exists(flops):
+    deps = [os.path.join(_HERE, f) for f in ("kyn_oracle.cpp", "kyn_oracle.h")]
+    deps.append(os.path.join(_HERE, "..", "include", "kynema_b200.h"))
+    stale = any(not os.path.exists(x) or any(os.path.getmtime(d) > os.path.getmtime(x) for d in deps)
+                for x in (_LIB_PATH, flops))
+    if force or stale:
         subprocess.run(["make", "-s", "-C", _HERE], check=True)
     return _LIB_PATH
 

@@ -329,6 +329,48 @@ def main(ref: str) -> None:
                 "# axis points (grid x y z), twist (grid deg), sections (grid inertia[21] stiffness[21]),\n"
                 "# expected tip position [7]\n" + "\n".join(lines) + "\n")
 
+    # ---- IEA-15 turbine through the turbine interface (WindIO input) ----------------
+    # tests/regression_tests/interfaces/test_turbine_interface.cpp:17-285 builds
+    # the whole turbine from the same WindIO file: the blade input above, the
+    # tower (reference axis, outer diameter and wall thickness of its first
+    # layer, isotropic material), the hub and the nacelle; the expected tower
+    # top position of the test closes the file.
+    tt = strip_comments(open(os.path.join(itf, "test_turbine_interface.cpp")).read())
+    t0 = tt.index("TEST(TurbineInterfaceTest, IEA15_Structure)")
+    top = [float(m.group(2)) for m in
+           re.finditer(r"EXPECT_NEAR\(\s*tower_top_node\.position\[(\d)\],\s*(" + NUM + r"),", tt[t0:])]
+    assert len(top) == 7
+    tower = wio["components"]["tower"]
+    tra = tower["outer_shape_bem"]["reference_axis"]
+    tdia = tower["outer_shape_bem"]["outer_diameter"]
+    layer = tower["internal_structure_2d_fem"]["layers"][0]
+    mat = next(m for m in wio["materials"] if m.get("name") == layer["material"])
+    hub = wio["components"]["hub"]
+    nac = wio["components"]["nacelle"]
+    tl = [str(len(tra["x"]["grid"]))]
+    for i, g in enumerate(tra["x"]["grid"]):
+        tl.append(" ".join(repr(float(v)) for v in (g, tra["x"]["values"][i], tra["y"]["values"][i],
+                                                     tra["z"]["values"][i])))
+    tl.append(str(len(tdia["grid"])))
+    for i, g in enumerate(tdia["grid"]):
+        tl.append(" ".join(repr(float(v)) for v in (g, tdia["values"][i], layer["thickness"]["values"][i])))
+    tl.append(" ".join(repr(float(mat[k])) for k in ("E", "G", "rho", "nu")))
+    tl.append(" ".join(repr(float(v)) for v in [hub["diameter"], hub["cone_angle"],
+                                                  hub["elastic_properties_mb"]["system_mass"]]
+                       + list(hub["elastic_properties_mb"]["system_inertia"])))
+    dt = nac["drivetrain"]
+    ep = nac["elastic_properties_mb"]
+    tl.append(" ".join(repr(float(v)) for v in [dt["uptilt"], dt["overhang"], dt["distance_tt_hub"],
+                                                  ep["system_mass"], ep["yaw_mass"]]
+                       + list(ep["system_inertia_tt"])))
+    tl.append(" ".join(repr(v) for v in top))
+    with open(os.path.join(out_dir, "iea15_turbine_windio.txt"), "w") as f:
+        f.write("# IEA-15-240-RWT tower, hub and nacelle (WindIO) for TurbineInterfaceTest.IEA15_Structure\n"
+                "# (the blades use iea15_blade_windio.txt): tower axis points (grid x y z), tower stations\n"
+                "# (grid outer_diameter wall_thickness), tower material (E G rho nu), hub (diameter\n"
+                "# cone_angle mass inertia[6]), nacelle (uptilt overhang distance_tt_hub system_mass\n"
+                "# yaw_mass inertia_tt[6]), expected tower top position [7]\n" + "\n".join(tl) + "\n")
+
     # ---- curved beam (kernel level) --------------------------------------------
     cb = strip_comments(open(os.path.join(unit, "test_curved_beam.hpp")).read())
     names = ["kCurvedBeamNodes_data", "kGaussQuadraturePoints", "kGaussQuadratureWeights",

@@ -19,15 +19,22 @@ LIB_DIR = os.path.join(ROOT, "openturbine_b200", "_lib")
 
 BLADE_SRC = os.path.join(ROOT, "tests", "cpp", "test_blade_interface.cpp")
 CFD_SRC = os.path.join(ROOT, "tests", "cpp", "test_cfd_interface.cpp")
+TURBINE_SRC = os.path.join(ROOT, "tests", "cpp", "test_turbine_interface.cpp")
 
 
-def _compile(src: str = SRC, name: str = "test_shim") -> str:
+def _compile(src: str = SRC, name: str = "test_shim", with_oracle: bool = False) -> str:
+    """g++ build of a driver against the shim (and, for the cross-checking
+    drivers, the oracle library: test infrastructure)."""
     kbuild.build()
     os.makedirs(OUT_DIR, exist_ok=True)
     exe = os.path.join(OUT_DIR, name)
     gxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
     cmd = [gxx, "-std=c++20", "-O1", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), src,
            "-L", LIB_DIR, "-lkynema_b200", "-Wl,-rpath," + LIB_DIR, "-o", exe]
+    if with_oracle:
+        from oracle import oracle_py
+        odir = os.path.dirname(oracle_py.build())
+        cmd[-2:-2] = ["-I", os.path.join(ROOT, "oracle"), "-L", odir, "-lkyn_oracle", "-Wl,-rpath," + odir]
     subprocess.run(cmd, check=True)
     return exe
 
@@ -36,6 +43,7 @@ def test_shim_compiles():
     assert os.path.exists(_compile())
     assert os.path.exists(_compile(BLADE_SRC, "test_blade_interface"))
     assert os.path.exists(_compile(CFD_SRC, "test_cfd_interface"))
+    assert os.path.exists(_compile(TURBINE_SRC, "test_turbine_interface", with_oracle=True))
 
 
 def test_interface_geometry_helpers():
@@ -114,3 +122,20 @@ def test_cfd_interface_floating_platform(tmp_path):
     assert r.returncode == 0, r.stdout + r.stderr
     assert "OK (0 failures)" in r.stdout
 
+
+
+@pytest.mark.gpu
+def test_turbine_interface_iea15_structure():
+    """TurbineInterface (include/kynema_b200_interfaces.hpp) on the reference's
+    TurbineInterfaceTest.IEA15_Structure: the IEA-15-240-RWT tower, drive train,
+    hub and three blades (a condensed dense model), 9 steps under a tower-top
+    load, generator torque, pitch and yaw ramps, tower top position at the
+    test's 1e-10, and the oracle stepping the same model beside it."""
+    exe = _compile(TURBINE_SRC, "test_turbine_interface", with_oracle=True)
+    golden = os.path.join(ROOT, "tests", "golden")
+    r = subprocess.run([exe, os.path.join(golden, "iea15_blade_windio.txt"),
+                        os.path.join(golden, "iea15_turbine_windio.txt")],
+                       capture_output=True, text=True, timeout=600)
+    print(r.stdout)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.strip().endswith("OK")

@@ -15,8 +15,8 @@ import numpy as np
 import pytest
 
 from tests.test_gpu_parity import FIELDS, Twin, assert_convergence_close, assert_state_close, rel_err
-from tests.workloads_ref import (chain_tip_loads, four_element_cantilever_model, tower_model,
-                                 two_long_beams_model)
+from tests.workloads_ref import (chain_tip_loads, four_element_cantilever_model, revolute_pendulum_model,
+                                 tower_model, two_long_beams_model)
 
 pytestmark = pytest.mark.gpu
 
@@ -121,3 +121,27 @@ def test_condensed_models_in_both_forms_and_batched(ctx):
         assert rel_err(ctx.state(x, "q"), ctx.state(y, "q")) == 0.0
     for mid in [a, b] + mixed + alone:
         ctx.destroy_model(mid)
+
+
+def test_revolute_joint_in_a_dense_model(ctx):
+    """A revolute joint as five constraint rows of a dense bordered system (the
+    turbine's shaft joint sits between nodes of such a system): a pendulum on a
+    revolute joint about x, swung by gravity and driven by the joint torque,
+    against the oracle for 200 steps."""
+    m, p = revolute_pendulum_model()
+    pm = m.pack()
+    mid = ctx.create_model(pm)
+    tw = Twin(pm)
+    for k in range(200):
+        torque = 30.0 * np.sin(0.05 * k)
+        u = np.array([torque, 0., 0., 1., 0., 0., 0.])
+        ctx.set_prescribed(mid, 1, u)
+        tw.set_prescribed(1, u)
+        st, it = ctx.step([mid], p)
+        ost, oit = tw.step(p)
+        assert (st[0], it[0]) == (ost, oit) == (0, oit), (k, st[0], it[0], ost, oit)
+        assert_convergence_close(ctx.convergence(mid), tw.convergence())
+    assert_state_close(ctx, mid, tw, fields=FIELDS)
+    q = ctx.state(mid, "q")
+    assert abs(q[2, 2]) > 1e-2   # the bob swung
+    ctx.destroy_model(mid)

@@ -42,6 +42,7 @@ MODELS = {
     "condensed_four_element_cantilever": lambda: R.four_element_cantilever_model(),
     "condensed_tower": lambda: R.tower_model(),
     "condensed_two_long_beams": lambda: R.two_long_beams_model(),
+    "dense_revolute_pendulum": lambda: R.revolute_pendulum_model(),
     "three_row_bc_on_a_beam": lambda: _cantilever_with(lambda m: m.AddFixedBC3DOFs(4)),
     "batch_rotor": lambda: W.rotor_model(3),
     "batch_cantilever": lambda: W.batch_cantilever_model(W.draw_batch(1, first_id=77)[0]),
@@ -66,21 +67,52 @@ def _cantilever_with(extra):
     return m
 
 
-@pytest.mark.parametrize("case", ["two_revolute_joints",
-                                  "revolute_between_beam_nodes", "revolute_in_a_dense_model",
-                                  "free_node_outside_the_beams"])
+def _two_revolute_joints():
+    m = R.generator_torque_model(0.0)[0]
+    n = m.AddNode().SetPosition(0., 0., 5., 1., 0., 0., 0.).Build()
+    m.AddMassElement(n, np.eye(6))
+    m.AddRevoluteJointConstraint([len(m.nodes_) - 4, n], [0., 0., 1.], np.zeros(1))
+    return m
+
+
+def _revolute_in_a_dense_model():
+    m = R.heavy_top_model()[0]
+    n = m.AddNode().SetPosition(0., 2., 0., 1., 0., 0., 0.).Build()
+    m.AddMassElement(n, np.eye(6))
+    m.AddRevoluteJointConstraint([0, n], [0., 0., 1.], np.zeros(1))
+    return m
+
+
+# Revolute joints outside a drive train (a second joint, a joint between beam
+# nodes, a joint in a beam-free dense model) make the model a dense bordered
+# system, where each revolute joint is five constraint rows.
+MODELS.update({
+    "two_revolute_joints": _two_revolute_joints,
+    "revolute_between_beam_nodes": lambda: _cantilever_with(
+        lambda m: m.AddRevoluteJointConstraint([1, 2], [1., 0., 0.], np.zeros(1))),
+    "revolute_in_a_dense_model": _revolute_in_a_dense_model,
+})
+
+
+@pytest.mark.parametrize("name", ["two_revolute_joints", "revolute_between_beam_nodes",
+                                  "revolute_in_a_dense_model"])
+def test_revolute_joints_outside_a_drive_train_go_dense(name):
+    pm = _first(MODELS[name]()).pack()
+    info, rp, ci = describe(pm)
+    o = OracleModel(pm)
+    orp, oci, _ = o.crs()
+    assert info.num_dofs == o.info.num_dofs
+    assert np.array_equal(rp, orp) and np.array_equal(ci, oci)
+
+
+@pytest.mark.parametrize("case", ["free_node_outside_the_beams", "seventeen_constraints_in_a_dense_model"])
 def test_topologies_outside_the_path_are_refused(case):
-    if case == "two_revolute_joints":
-        m = R.generator_torque_model(0.0)[0]
-        n = m.AddNode().SetPosition(0., 0., 5., 1., 0., 0., 0.).Build()
-        m.AddRevoluteJointConstraint([len(m.nodes_) - 4, n], [0., 0., 1.], np.zeros(1))
-    elif case == "revolute_between_beam_nodes":
-        m = _cantilever_with(lambda m: m.AddRevoluteJointConstraint([1, 2], [1., 0., 0.], np.zeros(1)))
-    elif case == "revolute_in_a_dense_model":
+    if case == "seventeen_constraints_in_a_dense_model":
         m = R.heavy_top_model()[0]
-        n = m.AddNode().SetPosition(0., 2., 0., 1., 0., 0., 0.).Build()
-        m.AddMassElement(n, np.eye(6))
-        m.AddRevoluteJointConstraint([0, n], [0., 0., 1.], np.zeros(1))
+        for k in range(17):
+            n = m.AddNode().SetPosition(0., 2. + k, 0., 1., 0., 0., 0.).Build()
+            m.AddMassElement(n, np.eye(6))
+            m.AddRigidJointConstraint([0, n])
     else:
         m = _cantilever_with(lambda m: m.AddNode().SetPosition(0., 5., 0., 1., 0., 0., 0.).Build())
     with pytest.raises(RuntimeError, match="UNSUPPORTED"):

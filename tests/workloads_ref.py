@@ -576,3 +576,23 @@ def two_long_beams_model():
     m.AddPrescribedBC(beams[0][0])
     m.AddRigidJointConstraint([beams[0][-1], beams[1][0]])
     return m, StepParameters(True, 6, 0.01, 0.), beams
+
+
+def revolute_pendulum_model():
+    """A beam-free dense model with a revolute joint: a shaft base held by a
+    FixedBC, a revolute joint about x to a light hub node carrying a point
+    mass, and a heavy point mass rigidly jointed to the hub 0.5 m off the
+    axis; gravity -9.81 z swings it about the joint while the joint's torque
+    drives it.  Solved as one dense bordered system (the revolute joint as
+    five constraint rows, not a drive train)."""
+    m = Model()
+    m.SetGravity(0., 0., -9.81)
+    base = m.AddNode().SetPosition(0., 0., 0., 1., 0., 0., 0.).Build()
+    hub = m.AddNode().SetPosition(1., 0., 0., 1., 0., 0., 0.).Build()
+    bob = m.AddNode().SetPosition(1., 0.5, 0., 1., 0., 0., 0.).Build()
+    m.AddFixedBC(base)
+    m.AddRevoluteJointConstraint([base, hub], [1., 0., 0.])
+    m.AddRigidJointConstraint([hub, bob])
+    m.AddMassElement(hub, np.diag([2., 2., 2., 0.5, 0.4, 0.4]))
+    m.AddMassElement(bob, np.diag([20., 20., 20., 1., 1., 1.]))
+    return m, StepParameters(True, 8, 0.005, 0.5)
