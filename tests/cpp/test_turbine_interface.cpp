@@ -8,6 +8,7 @@
 // test's 1e-10.  The oracle (test infrastructure, oracle/kyn_oracle.h) steps the
 // same model description beside it: same Newton iteration counts at every step,
 // displacements within 1e-10 relative.  Exit code 0 on success.
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <fstream>
@@ -178,13 +179,16 @@ int main(int argc, char** argv) {
         t.tower.nodes.back().loads = {1e5, 0., 0., 0., 0., 0.};
         t.torque_control = 1e8;
         const auto n_steps = static_cast<size_t>(duration / time_step);
-        double worst = 0.;
+        double worst = 0., gpu_s = 0., orc_s = 0.;
         for (size_t i = 1; i < n_steps; ++i) {
             const double time = static_cast<double>(i) * time_step;
             t.blade_pitch_control[2] = time * 0.5;
             t.yaw_control = time * 0.3;
             if (i % 500 == 0) t.torque_control = 0.;
-            if (!interface.Step()) {
+            const auto g0 = std::chrono::steady_clock::now();
+            const bool converged = interface.Step();
+            gpu_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - g0).count();
+            if (!converged) {
                 std::printf("FAIL step %zu did not converge\n", i);
                 ++failures;
                 break;
@@ -201,7 +205,9 @@ int main(int argc, char** argv) {
             control(t.tower_top_to_yaw_bearing.id, t.yaw_control);
             control(t.shaft_base_to_azimuth.id, t.torque_control);
             int oit = 0;
+            const auto o0 = std::chrono::steady_clock::now();
             const int ost = orc_step(orc, &op, &oit);
+            orc_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - o0).count();
             const int git = static_cast<int>(interface.GetSolver().convergence_err().size());
             if (ost != KYN_OK || oit != git) {
                 std::printf("FAIL step %zu: oracle status %d iterations %d, GPU iterations %d\n", i, ost, oit, git);
@@ -220,11 +226,41 @@ int main(int argc, char** argv) {
             worst = std::max(worst, diff / scale);
         }
         std::printf("oracle: largest relative difference of q over the steps %.3g\n", worst);
+        // wall time per step: TurbineInterface::Step (loads and controls in, one
+        // condensed dense step on the GPU, motion out) and the oracle's step (one core)
+        std::printf("time per step: interface %.3f ms, oracle %.3f ms\n", 1e3 * gpu_s / (n_steps - 1),
+                    1e3 * orc_s / (n_steps - 1));
         if (!(worst <= 1e-10)) {
             std::printf("FAIL q differs from the oracle by %.3g relative\n", worst);
             ++failures;
         }
         orc_model_destroy(orc);
+
+        // throughput: 148 copies of the turbine (one per SM of a B200) stepped by
+        // one batched call, from the state the test left
+        {
+            const auto dm = interface.GetSolver().model();
+            kyn_ctx* c = dm->ctx.get();
+            std::vector<int> ids;
+            for (int k = 0; k < 148; ++k) {
+                const int cid = kyn_model_clone(c, dm->id);
+                check(c, cid);
+                ids.push_back(cid);
+            }
+            const kyn_step_params bp = sp.c();
+            std::vector<int> st(ids.size()), it(ids.size());
+            check(c, kyn_step(c, ids.data(), static_cast<int>(ids.size()), &bp, st.data(), it.data()));
+            const int reps = 5;
+            const auto b0 = std::chrono::steady_clock::now();
+            for (int r = 0; r < reps; ++r)
+                check(c, kyn_step(c, ids.data(), static_cast<int>(ids.size()), &bp, st.data(), it.data()));
+            const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - b0).count();
+            int converged = 0;
+            for (int s2 : st) converged += s2 == KYN_OK;
+            std::printf("batch of %zu turbines: %.3f ms per batched step, %.0f turbine-steps/s (%d converged)\n",
+                        ids.size(), 1e3 * sec / reps, ids.size() * reps / sec, converged);
+            for (int cid : ids) kyn_model_destroy(c, cid);
+        }
 
         const auto& top = t.tower.nodes.back();
         for (int c = 0; c < 7; ++c) expect_near(top.position[c], expected[c], 1e-10, "tower top position", c);

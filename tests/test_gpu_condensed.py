@@ -145,3 +145,35 @@ def test_revolute_joint_in_a_dense_model(ctx):
     q = ctx.state(mid, "q")
     assert abs(q[2, 2]) > 1e-2   # the bob swung
     ctx.destroy_model(mid)
+
+
+def test_condensed_tower_under_base_motion_and_state_f(ctx):
+    """The condensed tower with its base moved by its PrescribedBC (a lateral
+    ground motion) and external forces given as state.f at an interior node of
+    the middle element (eliminated inside that element) and at the top (a
+    boundary node), against the oracle for 40 steps."""
+    m, p, along, elems = tower_model()
+    pm = m.pack()
+    mid = ctx.create_model(pm)
+    tw = Twin(pm)
+    interior = elems[1][4]   # a node of the middle element only
+    nn = len(m.nodes_)
+    for k in range(40):
+        t = (k + 1) * p.h
+        u = np.array([0.05 * np.sin(6.0 * t), 0.02 * np.sin(4.0 * t), 0., 1., 0., 0., 0.])
+        ctx.set_prescribed(mid, 0, u)
+        tw.set_prescribed(0, u)
+        f = np.zeros((nn, 6))
+        f[interior, 1] = 5.0e4 * np.cos(5.0 * t)
+        f[along[-1], 0] = 1.0e5 * np.sin(3.0 * t)
+        ctx.set_state_f(mid, f)
+        tw.o.set_state_f(f)
+        tw.alt.set_state_f(f)
+        st, it = ctx.step([mid], p)
+        ost, oit = tw.step(p)
+        assert (st[0], it[0]) == (ost, oit) == (0, oit), (k, st[0], it[0], ost, oit)
+        assert_convergence_close(ctx.convergence(mid), tw.convergence())
+    assert_state_close(ctx, mid, tw, fields=FIELDS)
+    q = ctx.state(mid, "q")
+    assert abs(q[interior, 1]) > 1e-5   # the interior node moved sideways
+    ctx.destroy_model(mid)
