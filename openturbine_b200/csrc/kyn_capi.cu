@@ -359,11 +359,19 @@ void prepare_model(DevModel* m) {
         m->def_nt[f] = 128;
         for (int k = 0; k < 3; ++k) m->smem_nt[f][k] = 0;
         for (const HostBeam& hb : H.beams) {
-            if (hb.dense) {  // the dense bordered system: 128 threads, FP64 in both forms
+            if (hb.dense) {  // the dense bordered system, FP64 in both forms
                 for (int k = 0; k < 3; ++k)
                     m->smem_nt[f][k] = std::max(
                         m->smem_nt[f][k],
                         dense_smem(H, hb, 128 << k));
+                // 128 threads, or for a condensed model (elements assembled and
+                // eliminated one after the other in one CTA) the most that fit
+                if (hb.cond_nd > 0)
+                    for (int nt : {512, 256})
+                        if (dense_smem(H, hb, nt) <= kMaxDynSmem) {
+                            m->def_nt[f] = nt;
+                            break;
+                        }
                 continue;
             }
             m->def_nt[f] = std::max(m->def_nt[f], beam_threads(hb.N, hb.Q, hb.nc, rb, hubf));

@@ -1355,12 +1355,18 @@ __host__ __device__ inline DenseSmem make_dense_smem(int N, int nd, int nt = 128
     };
     if (cond_nd > 0) nd = cond_nd;
     // condensed models: the bordered system's region also holds, before the
-    // system is assembled, one component's system [6cN][6cN + 1] and the G
-    // rows of one chunk of its quadrature points
-    const int w_bytes = cond_nd > 0 ? (cN * 6 * (cN * 6 + 1) * 8 + 15) & ~15 : 0;
+    // system is assembled, one component's system [6cN][6cN + 1], the G rows
+    // of one chunk of its quadrature points, the quadrature phase's group
+    // scratch and the component's tables and node state (cond_tables)
+    auto r16 = [](int b) { return (b + 15) & ~15; };
+    const int w_bytes = cond_nd > 0 ? r16(cN * 6 * (cN * 6 + 1) * 8) : 0;
     const int g_bytes = cond_nd > 0 ? 4 * kCondChunk * 56 * 8 : 0;
+    const int s_bytes = cond_nd > 0 ? (nt / 16) * kGroupScratch * 8 : 0;
+    const int t_bytes = cond_nd > 0 ? 3 * r16(cQ * cN * 8) + r16(cQ * 4 * 8) + r16(cN * 7 * 8) +
+                                          2 * r16(cN * 6 * 8) + 2 * r16(cQ * 6 * 8) : 0;
+    const int c_bytes = w_bytes + g_bytes + s_bytes + t_bytes;
     const int m_bytes = md_global ? 0 : nd * nd * 8;
-    const int region = take(m_bytes > w_bytes + g_bytes ? m_bytes : w_bytes + g_bytes);
+    const int region = take(m_bytes > c_bytes ? m_bytes : c_bytes);
     S.M = md_global ? -1 : region;
     S.cW = cond_nd > 0 ? region : -1;
     S.b = take(nd * 8);
@@ -1378,7 +1384,25 @@ __host__ __device__ inline DenseSmem make_dense_smem(int N, int nd, int nt = 128
     S.fmap = take(N * 4);
     S.red = take(64 * 8);  // per-warp partial sums of the error
     S.cphi = S.cdphi = S.cdphiJ = S.cqpw = S.cq = S.cv = S.cvd = S.cG = S.cFc = S.cFd = S.cgs = -1;
-    if (cN > 0) {
+    if (cN > 0 && cond_nd > 0) {  // inside the bordered system's region, after the component's system
+        int t = region + w_bytes;
+        auto at = [&](int bytes) {
+            const int r = t;
+            t += r16(bytes);
+            return r;
+        };
+        S.cG = at(g_bytes);
+        S.cgs = at(s_bytes);
+        S.cphi = at(cQ * cN * 8);
+        S.cdphi = at(cQ * cN * 8);
+        S.cdphiJ = at(cQ * cN * 8);
+        S.cqpw = at(cQ * 4 * 8);
+        S.cq = at(cN * 7 * 8);
+        S.cv = at(cN * 6 * 8);
+        S.cvd = at(cN * 6 * 8);
+        S.cFc = at(cQ * 6 * 8);
+        S.cFd = at(cQ * 6 * 8);
+    } else if (cN > 0) {
         S.cphi = take(cQ * cN * 8);
         S.cdphi = take(cQ * cN * 8);
         S.cdphiJ = take(cQ * cN * 8);
@@ -1386,14 +1410,13 @@ __host__ __device__ inline DenseSmem make_dense_smem(int N, int nd, int nt = 128
         S.cq = take(cN * 7 * 8);
         S.cv = take(cN * 6 * 8);
         S.cvd = take(cN * 6 * 8);
-        S.cG = cond_nd > 0 ? -1 : take(4 * cQ * 56 * 8);  // condensed: set below
+        S.cG = take(4 * cQ * 56 * 8);
         S.cFc = take(cQ * 6 * 8);
         S.cFd = take(cQ * 6 * 8);
         S.cgs = take((nt / 16) * kGroupScratch * 8);
     }
     S.xi = S.imap = S.bc = S.lpos = S.lnode = S.cx = -1;
     if (cond_nd > 0) {
-        S.cG = S.cW + w_bytes;
         S.xi = take(N * 6 * 8);
         S.imap = take(N * 4);
         S.bc = take(nd * 8);
