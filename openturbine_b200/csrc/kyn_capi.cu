@@ -1285,6 +1285,40 @@ int kyn_get_state(kyn_ctx* c, int id, int field, double* out) {
         // (src/constraints/calculate_revolute_joint_output.hpp:24-85), from beam
         // 0's copy of the azimuth record; zero for the other constraints.
         for (int k = 0; k < 3 * HM.num_constraints; ++k) out[k] = 0.;
+        if (!HM.beams.empty() && HM.beams[0].dense && HM.beams[0].frames_off >= 0) {
+            // dense models: every revolute joint, from its target node's state
+            // in the one dense record and the joint frame kept in its slab
+            const HostBeam& b0 = HM.beams[0];
+            const SlabLayout L0 = make_slab_layout(b0.N, 0);
+            for (int cid = 0; cid < HM.num_constraints; ++cid) {
+                const int slot = HM.con_slot[cid];
+                if (slot < 0 || b0.con_type[slot] != KYN_CONSTRAINT_REVOLUTE_JOINT) continue;
+                const int n = b0.con_node[slot];
+                double qv[7], w[6], wd[6];
+                KYN_CUDA(c, cudaMemcpy(qv, m->d_slab[0] + L0.q + n * 7, sizeof(qv), cudaMemcpyDeviceToHost));
+                KYN_CUDA(c, cudaMemcpy(w, m->d_slab[0] + L0.v + n * 6, sizeof(w), cudaMemcpyDeviceToHost));
+                KYN_CUDA(c, cudaMemcpy(wd, m->d_slab[0] + L0.vd + n * 6, sizeof(wd), cudaMemcpyDeviceToHost));
+                const double* q = qv + 3;
+                const double* a0 = b0.slab.data() + b0.frames_off + slot * 9;
+                double ax[3], rv[3] = {0., 0., 0.};
+                for (int i = 0; i < 3; ++i) {
+                    ax[i] = 0.;
+                    for (int j = 0; j < 3; ++j) ax[i] += rot_entry(q, i, j) * a0[j];
+                }
+                const double sh = std::sqrt(1. - q[0] * q[0]);
+                if (sh > 1e-12) {  // QuaternionToRotationVector (src/math/quaternion_operations.hpp:248-262)
+                    const double th = 2. * std::acos(q[0]);
+                    for (int i = 0; i < 3; ++i) rv[i] = th * q[1 + i] / sh;
+                }
+                double* o = out + 3 * cid;
+                for (int i = 0; i < 3; ++i) {
+                    o[0] += ax[i] * rv[i];
+                    o[1] += ax[i] * w[3 + i];
+                    o[2] += ax[i] * wd[3 + i];
+                }
+            }
+            return KYN_OK;
+        }
         if (HM.rev_con < 0) return KYN_OK;
         const HostBeam& b0 = HM.beams[0];
         const SlabLayout L0 = make_slab_layout(b0.N, b0.Q);

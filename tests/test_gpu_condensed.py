@@ -127,7 +127,7 @@ def test_revolute_joint_in_a_dense_model(ctx):
     """A revolute joint as five constraint rows of a dense bordered system (the
     turbine's shaft joint sits between nodes of such a system): a pendulum on a
     revolute joint about x, swung by gravity and driven by the joint torque,
-    against the oracle for 200 steps."""
+    against the oracle for 200 steps, states and the joint's output."""
     m, p = revolute_pendulum_model()
     pm = m.pack()
     mid = ctx.create_model(pm)
@@ -141,6 +141,10 @@ def test_revolute_joint_in_a_dense_model(ctx):
         ost, oit = tw.step(p)
         assert (st[0], it[0]) == (ost, oit) == (0, oit), (k, st[0], it[0], ost, oit)
         assert_convergence_close(ctx.convergence(mid), tw.convergence())
+        if k % 50 == 49:  # the joint output (rotation, rate, acceleration about its axis)
+            out = ctx.state(mid, "output")
+            np.testing.assert_allclose(out, tw.o.state("output"), rtol=1e-9, atol=1e-10)
+            assert abs(out[1, 0]) > 1e-3
     assert_state_close(ctx, mid, tw, fields=FIELDS)
     q = ctx.state(mid, "q")
     assert abs(q[2, 2]) > 1e-2   # the bob swung
