@@ -965,6 +965,15 @@ public:
         check(ctx_.get(), kyn_state_copy(ctx_.get(), solver_->model()->id, saved_));
         GetMotion();
     }
+    // Rotation of the shaft joint about its axis, wrapped to [0, 2 pi), and the
+    // rotor speed about it (TurbineInterface::CalculateAzimuthAngle /
+    // CalculateRotorSpeed, src/interfaces/turbine/turbine_interface.cpp:206-222)
+    double CalculateAzimuthAngle() const {
+        double azimuth = constraints_->output()[turbine_.shaft_base_to_azimuth.id * 3];
+        azimuth = std::fmod(azimuth, 2. * std::numbers::pi);
+        return azimuth < 0. ? azimuth + 2. * std::numbers::pi : azimuth;
+    }
+    double CalculateRotorSpeed() const { return constraints_->output()[turbine_.shaft_base_to_azimuth.id * 3 + 1]; }
 
 private:
     void GetMotion() {

@@ -238,6 +238,22 @@ int main(int argc, char** argv) {
             std::printf("FAIL q differs from the oracle by %.3g relative\n", worst);
             ++failures;
         }
+        {  // the shaft joint's output: azimuth angle and rotor speed
+            std::vector<double> oo(static_cast<size_t>(oinfo.num_constraints) * 3);
+            orc_get_state(orc, KYN_FIELD_CONSTRAINT_OUTPUT, oo.data());
+            const size_t rj = t.shaft_base_to_azimuth.id;
+            double az = std::fmod(oo[rj * 3], 2. * std::numbers::pi);
+            if (az < 0.) az += 2. * std::numbers::pi;
+            expect_near(interface.CalculateAzimuthAngle(), az, 1e-10, "azimuth angle", 0);
+            expect_near(interface.CalculateRotorSpeed(), oo[rj * 3 + 1], 1e-10 * (1. + std::abs(oo[rj * 3 + 1])),
+                        "rotor speed", 0);
+            if (!(std::abs(interface.CalculateRotorSpeed()) > 1e-3)) {
+                std::printf("FAIL the generator torque did not turn the rotor\n");
+                ++failures;
+            }
+            std::printf("azimuth %.6g rad, rotor speed %.6g rad/s\n", interface.CalculateAzimuthAngle(),
+                        interface.CalculateRotorSpeed());
+        }
         orc_model_destroy(orc);
 
         // throughput: 148 copies of the turbine (one per SM of a B200) stepped by
