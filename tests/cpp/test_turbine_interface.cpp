@@ -162,6 +162,39 @@ int main(int argc, char** argv) {
         turbine_builder.SetYawBearingInertiaMatrix(point_inertia(system_mass + yaw_mass, inertia_tt));
         turbine_builder.SetHubInertiaMatrix(point_inertia(hub_mass, hub_inertia));
 
+        if (argc > 3 && std::string(argv[3]) == "--describe") {
+            // host only (no device): the turbine's model description through
+            // kyn_model_describe, its DOF counts and CRS graph against the oracle's
+            Model model(builder.Solution().Input().gravity);
+            components::Turbine turbine(builder.Turbine().Input(), model);
+            model.WithDescription([&](const kyn_model_desc& d) {
+                kyn_model_info info{};
+                char e[256] = {};
+                if (kyn_model_describe(&d, &info, nullptr, nullptr, e, 256) != KYN_OK)
+                    throw std::runtime_error(std::string("describe: ") + e);
+                std::vector<int32_t> rp(static_cast<size_t>(info.num_dofs) + 1), ci(static_cast<size_t>(info.nnz));
+                kyn_model_describe(&d, &info, rp.data(), ci.data(), e, 256);
+                orc_model* o = orc_model_create(&d, e, 256);
+                if (!o) throw std::runtime_error(std::string("oracle: ") + e);
+                kyn_model_info oi{};
+                orc_model_info(o, &oi);
+                std::vector<int> orp(static_cast<size_t>(oi.num_dofs) + 1), oci(static_cast<size_t>(oi.nnz));
+                orc_get_crs(o, orp.data(), oci.data(), nullptr);
+                orc_model_destroy(o);
+                std::printf("describe: %d nodes, %d constraints, %d unknowns, %d in the condensed system, nnz %d\n",
+                            info.num_nodes, info.num_constraints, info.num_dofs, info.condensed_dofs, info.nnz);
+                bool same = info.num_dofs == oi.num_dofs && info.nnz == oi.nnz;
+                for (size_t k = 0; same && k < rp.size(); ++k) same = rp[k] == orp[k];
+                for (size_t k = 0; same && k < ci.size(); ++k) same = ci[k] == oci[k];
+                if (!same || info.num_dofs != 371 || info.condensed_dofs != 137) {
+                    std::printf("FAIL the turbine's DOF counts or CRS graph differ from the oracle's\n");
+                    ++failures;
+                }
+            });
+            std::printf("%s\n", failures ? "FAILED" : "OK");
+            return failures ? 1 : 0;
+        }
+
         auto interface = builder.Build(Context(0));
 
         // the oracle on the same model description

@@ -124,6 +124,20 @@ def test_cfd_interface_floating_platform(tmp_path):
 
 
 
+def test_turbine_model_description_without_a_gpu():
+    """The IEA-15 turbine's model, built by the turbine component on the host
+    and described by kyn_model_describe (no device): 371 unknowns condensed to
+    a bordered system of 137, DOF counts and CRS graph equal to the oracle's."""
+    exe = _compile(TURBINE_SRC, "test_turbine_interface", with_oracle=True)
+    golden = os.path.join(ROOT, "tests", "golden")
+    r = subprocess.run([exe, os.path.join(golden, "iea15_blade_windio.txt"),
+                        os.path.join(golden, "iea15_turbine_windio.txt"), "--describe"],
+                       capture_output=True, text=True, timeout=300)
+    print(r.stdout)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.strip().endswith("OK")
+
+
 @pytest.mark.gpu
 def test_turbine_interface_iea15_structure():
     """TurbineInterface (include/kynema_b200_interfaces.hpp) on the reference's
