@@ -1337,6 +1337,7 @@ struct DenseSmem {
     // in device memory (KBeam::cond_md)
     int xi, imap, bc, lpos, lnode, cx;
     int cW;  // condensed models: one component's system (inside M's region when M is shared)
+    int cR;  // condensed models: bytes of that region
     int bytes;
 };
 // Quadrature points per pass of a condensed component's assembly.
@@ -1369,6 +1370,7 @@ __host__ __device__ inline DenseSmem make_dense_smem(int N, int nd, int nt = 128
     const int region = take(m_bytes > c_bytes ? m_bytes : c_bytes);
     S.M = md_global ? -1 : region;
     S.cW = cond_nd > 0 ? region : -1;
+    S.cR = cond_nd > 0 ? (m_bytes > c_bytes ? m_bytes : c_bytes) : 0;
     S.b = take(nd * 8);
     S.x = take(nd * 8);
     S.q = take(N * 7 * 8);
@@ -1995,16 +1997,19 @@ __device__ void cond_component_terms(const KBeam& KB, const StepCoeffs& P, const
             }
             __syncthreads();
         }
-        // unpivoted elimination of the interior rows, right-hand side included
+        // unpivoted elimination of the interior rows, right-hand side included:
+        // rows over the warps, columns over the lanes, one barrier per pivot
+        // (each row's warp stores its own multiplier after using it)
+        const int wid = tid >> 5, wl = tid & 31;
         for (int k = 0; k < mi; ++k) {
             const double d = W[k * ldw + k];
             if (tid == 0 && !(fabs(d) > 0. && isfinite(d))) *flag |= 2;
-            for (int i = k + 1 + tid; i < mc; i += NT) W[i * ldw + k] /= d;
-            __syncthreads();
-            const int w = mc - k - 1;
-            for (int e = tid; e < w * (w + 1); e += NT) {
-                const int i = k + 1 + e / (w + 1), j = k + 1 + e % (w + 1);
-                W[i * ldw + j] -= W[i * ldw + k] * W[k * ldw + j];
+            const double rd = 1. / d;
+            for (int i = k + 1 + wid; i < mc; i += NT / 32) {
+                const double l = W[i * ldw + k] * rd;
+                for (int j = k + 1 + wl; j <= mc; j += 32) W[i * ldw + j] -= l * W[k * ldw + j];
+                __syncwarp();
+                if (wl == 0) W[i * ldw + k] = l;
             }
             __syncthreads();
         }
@@ -2041,6 +2046,82 @@ __device__ void cond_add_schur(const KBeam& KB, const DenseSmem& S, unsigned cha
     }
 }
 
+// The back substitution of cond_back_substitute for all components at once,
+// one warp per component, when every component's eliminated rows and a map
+// of its DOFs fit the condensed region (dead once the bordered system is
+// solved): the rows are staged there together, map[p] is the position of local
+// DOF p in xi (>= 0, interior) or -1 - its position in x (boundary), and each
+// warp sweeps its rows with the sums of the sequential form.  Returns false,
+// having done nothing, when they do not fit.
+template <int NT>
+__device__ bool cond_back_substitute_warps(const KBeam& KB, const DenseSmem& S, unsigned char* smem_raw,
+                                           const int* fmap, const int* imap, const double* x, double* xi) {
+    constexpr int NW = NT / 32;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    long need = 0;
+    for (int ci = 0; ci < KB.n_comps; ++ci) {
+        const int N = static_cast<int>(KB.comps[ci * kCompHead + 1]);
+        int ni = 0;
+        for (int k = 0; k < N; ++k) ni += fmap[static_cast<int>(KB.comps[ci * kCompHead + 3 + k])] < 0;
+        need += 8L * (6 * ni) * (6 * N + 1) + 4L * 6 * N + 16;
+    }
+    if (need > S.cR) return false;
+    unsigned char* base = smem_raw + S.cW;
+    // per component: rows at a double offset, map at an int offset (tid 0 lays them out)
+    __shared__ int s_roff[kMaxDenseComps], s_moff[kMaxDenseComps], s_mi[kMaxDenseComps];
+    if (tid == 0) {
+        long o = 0;
+        for (int ci = 0; ci < KB.n_comps; ++ci) {
+            const double* hd = KB.comps + ci * kCompHead;
+            const int N = static_cast<int>(hd[1]), mc = 6 * N;
+            int ni = 0;
+            for (int k = 0; k < N; ++k) ni += fmap[static_cast<int>(hd[3 + k])] < 0;
+            s_roff[ci] = static_cast<int>(o / 8);
+            s_mi[ci] = 6 * ni;
+            o += 8L * (6 * ni) * (mc + 1);
+            s_moff[ci] = static_cast<int>(o / 4);
+            int* map = reinterpret_cast<int*>(base) + s_moff[ci];
+            int pi = 0, pb = 6 * ni;  // interior nodes first, then boundary, in local order
+            for (int k = 0; k < N; ++k) {
+                const int n = static_cast<int>(hd[3 + k]);
+                if (fmap[n] < 0)
+                    for (int c = 0; c < 6; ++c) map[pi++] = imap[n] + c;
+                else
+                    for (int c = 0; c < 6; ++c) map[pb++] = -1 - (fmap[n] + c);
+            }
+            o += 4L * mc;
+            o = (o + 15) & ~15L;
+        }
+    }
+    __syncthreads();
+    for (int ci = 0; ci < KB.n_comps; ++ci) {
+        const double* hd = KB.comps + ci * kCompHead;
+        const double* work = KB.comps + static_cast<long>(hd[kCompWork]);
+        const int ldw = 6 * static_cast<int>(hd[1]) + 1;
+        double* R = reinterpret_cast<double*>(base) + s_roff[ci];
+        for (int k = tid; k < s_mi[ci] * ldw; k += NT) R[k] = work[k];
+    }
+    __syncthreads();
+    for (int ci = warp; ci < KB.n_comps; ci += NW) {
+        const int mc = 6 * static_cast<int>(KB.comps[ci * kCompHead + 1]), ldw = mc + 1, mi = s_mi[ci];
+        const double* R = reinterpret_cast<const double*>(base) + s_roff[ci];
+        const int* map = reinterpret_cast<const int*>(base) + s_moff[ci];
+        for (int k = mi - 1; k >= 0; --k) {
+            const double* row = R + k * ldw;
+            double acc = 0.;
+            for (int j = k + 1 + lane; j < mc; j += 32) {
+                const int mj = map[j];
+                acc += row[j] * (mj >= 0 ? xi[mj] : x[-1 - mj]);
+            }
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0) xi[map[k]] = (row[mc] - acc) / row[k];
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    return true;
+}
+
 // Interior corrections of each condensed component from the bordered
 // system's solution x at its boundary nodes: U_ii x_i = y_i - U_ib x_b by one
 // warp, rows of the eliminated system (staged back into shared memory in W)
@@ -2049,6 +2130,7 @@ template <int NT>
 __device__ void cond_back_substitute(const KBeam& KB, const DenseSmem& S, unsigned char* smem_raw,
                                      const int* fmap, const int* imap, const double* x, double* xi) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (cond_back_substitute_warps<NT>(KB, S, smem_raw, fmap, imap, x, xi)) return;
     double* W = reinterpret_cast<double*>(smem_raw + S.cW);
     double* cx = reinterpret_cast<double*>(smem_raw + S.cx);
     int* lpos = reinterpret_cast<int*>(smem_raw + S.lpos);
@@ -2111,6 +2193,21 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
     int* imap = cnd ? reinterpret_cast<int*>(smem_raw + S.imap) : nullptr;
     double* bc = cnd ? reinterpret_cast<double*>(smem_raw + S.bc) : nullptr;
     __shared__ int s_flag, s_nsys, s_piv;
+    // phase timers (KYN_OPT_PHASE_TIMING): one CTA's clock, thread 0
+    __shared__ unsigned long long s_ph[kNumPhases];
+    const bool timing = KB.prof != nullptr;
+    long long ph_t = 0;
+    if (timing && tid == 0) {
+        for (int k = 0; k < kNumPhases; ++k) s_ph[k] = 0ull;
+        ph_t = clock64();
+    }
+    auto mark = [&](int phase) {
+        if (timing && tid == 0) {
+            const long long t = clock64();
+            s_ph[phase] += static_cast<unsigned long long>(t - ph_t);
+            ph_t = t;
+        }
+    };
     const double h = P.h;
 
     // state, constraint inputs, multipliers reset (ResetConstraints)
@@ -2218,10 +2315,12 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
                 }
         }
         for (int k = tid; k < N * 6; k += NT) resid[k] = 0.;
+        mark(kPhaseLoadPredict);
         if (cnd) {  // components first: their systems share the bordered system's region
             __syncthreads();
             cond_component_terms<NT>(KB, P, S, smem_raw, sq, sv, svd, sT, fmap, slab, L, resid, &s_flag);
         }
+        mark(kPhaseIntegrate);
         for (int k = tid; k < md * md; k += NT) Md[k] = 0.;
         for (int k = tid; k < md; k += NT) b[k] = 0.;
         if (cnd)
@@ -2372,6 +2471,7 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
         __syncthreads();
         for (int k = tid; k < md; k += NT) b[k] = -(k < nsys ? b[k] * cond : b[k]) + (cnd ? bc[k] : 0.);
         __syncthreads();
+        mark(kPhaseConstraints);
         // LU with partial pivoting, in place (the oracle's dense solve)
         for (int k = 0; k < md; ++k) {
             if (warp == 0) {
@@ -2412,20 +2512,23 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
                 }
             }
             __syncthreads();
-            const double d = Md[k * md + k];
-            for (int i = k + 1 + tid; i < md; i += NT) Md[i * md + k] /= d;
-            __syncthreads();
-            const int w = md - k - 1;
-            for (int e = tid; e < w * (w + 1); e += NT) {
-                const int i = k + 1 + e / (w + 1), j = e % (w + 1);
-                const double l = Md[i * md + k];
-                if (j < w)
-                    Md[i * md + k + 1 + j] -= l * Md[k * md + k + 1 + j];
-                else
+            // rows below the pivot over the warps, their columns over the lanes;
+            // each row's warp forms its multiplier (times the pivot's reciprocal),
+            // updates the row and the right-hand side, then stores the multiplier
+            // (no other warp reads it)
+            const double rd = 1. / Md[k * md + k];
+            for (int i = k + 1 + warp; i < md; i += NW) {
+                const double l = Md[i * md + k] * rd;
+                for (int j = k + 1 + lane; j < md; j += 32) Md[i * md + j] -= l * Md[k * md + j];
+                __syncwarp();
+                if (lane == 0) {
+                    Md[i * md + k] = l;
                     b[i] -= l * b[k];
+                }
             }
             __syncthreads();
         }
+        mark(kPhaseFactor);
         if (warp == 0) {  // back substitution
             for (int i = md - 1; i >= 0; --i) {
                 double s2 = 0.;
@@ -2440,6 +2543,7 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
         for (int k = nsys + tid; k < md; k += NT) x[k] /= cond;
         __syncthreads();
         if (cnd) cond_back_substitute<NT>(KB, S, smem_raw, fmap, imap, x, xi);
+        mark(kPhaseSubstitute);
         // correction of component c of node n
         auto delta_of = [&](int n, int c) { return fmap[n] >= 0 ? x[fmap[n] + c] : xi[imap[n] + c]; };
         double part = 0.;
@@ -2486,6 +2590,7 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
         __syncthreads();
         displacement();
         __syncthreads();
+        mark(kPhaseUpdate);
         if (s_flag != 0) {
             status = KYN_ERR_SINGULAR;
             break;
@@ -2529,6 +2634,8 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
     if (tid == 0) {
         status_out[KB.plan_model] = status;
         iters_out[KB.plan_model] = iters;
+        if (timing)
+            for (int k = 0; k < kNumPhases; ++k) atomicAdd(KB.prof + k, s_ph[k]);
     }
     (void)record;  // dense models keep no system dump (kyn_get_system refuses them)
 }

@@ -312,6 +312,22 @@ int main(int argc, char** argv) {
             for (int s2 : st) converged += s2 == KYN_OK;
             std::printf("batch of %zu turbines: %.3f ms per batched step, %.0f turbine-steps/s (%d converged)\n",
                         ids.size(), 1e3 * sec / reps, ids.size() * reps / sec, converged);
+            // per-phase SM cycles of one more batched step (KYN_OPT_PHASE_TIMING),
+            // per turbine and Newton iteration
+            check(c, kyn_ctx_set_option(c, KYN_OPT_PHASE_TIMING, 1));
+            check(c, kyn_step(c, ids.data(), static_cast<int>(ids.size()), &bp, st.data(), it.data()));
+            long iters = 0;
+            for (int v : it) iters += v;
+            const char* names[] = {"predict+tangent", "", "elements", "bordered assembly", "", "bordered LU",
+                                   "back substitution", "update"};
+            std::printf("phase cycles per turbine-iteration (%ld iterations):", iters);
+            for (int ph : {0, 2, 3, 5, 6, 7}) {
+                int64_t v = 0;
+                check(c, kyn_ctx_stat(c, KYN_STAT_PHASE_CYCLES + ph, &v));
+                std::printf(" %s %.0f,", names[ph], static_cast<double>(v) / static_cast<double>(iters));
+            }
+            std::printf("\n");
+            check(c, kyn_ctx_set_option(c, KYN_OPT_PHASE_TIMING, 0));
             for (int cid : ids) kyn_model_destroy(c, cid);
         }
 
