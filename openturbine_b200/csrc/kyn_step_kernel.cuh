@@ -1896,8 +1896,20 @@ template <int NT>
 __device__ void cond_component_terms(const KBeam& KB, const StepCoeffs& P, const DenseSmem& S,
                                      unsigned char* smem_raw, const double* sq, const double* sv,
                                      const double* svd, const double* sT, const int* fmap,
-                                     const double* mslab, const SlabLayout& ML, double* resid, int* flag) {
+                                     const double* mslab, const SlabLayout& ML, double* resid, int* flag,
+                                     unsigned long long* ph = nullptr) {
     const int tid = threadIdx.x;
+    // optional sub-phase timers (thread 0): quadrature physics, assembly,
+    // elimination, save, in the slots kPhaseQuadrature, kPhaseLUDiag,
+    // kPhaseLUPanel, kPhaseIntEpilogue of ph
+    long long pt = (ph && tid == 0) ? clock64() : 0;
+    auto sub = [&](int slot) {
+        if (ph && tid == 0) {
+            const long long t = clock64();
+            ph[slot] += static_cast<unsigned long long>(t - pt);
+            pt = t;
+        }
+    };
     double* phi = reinterpret_cast<double*>(smem_raw + S.cphi);
     double* dphi = reinterpret_cast<double*>(smem_raw + S.cdphi);
     double* dphiJ = reinterpret_cast<double*>(smem_raw + S.cdphiJ);
@@ -1954,6 +1966,7 @@ __device__ void cond_component_terms(const KBeam& KB, const StepCoeffs& P, const
             qp_phase<double, NT>(N, qn, phi + q0 * N, dphiJ + q0 * N, qpw + q0 * 4, cq, cv, cvd, cs, Lc,
                                  KB.gravity, P.beta_prime, P.gamma_prime, gscr, G, Fc, Fd);
             __syncthreads();
+            sub(kPhaseQuadrature);
             for (int t = tid; t < N * 6; t += NT) {
                 const int n = t / 6, c = t % 6;
                 double acc = 0.;
@@ -1996,6 +2009,7 @@ __device__ void cond_component_terms(const KBeam& KB, const StepCoeffs& P, const
                 }
             }
             __syncthreads();
+            sub(kPhaseLUDiag);
         }
         // unpivoted elimination of the interior rows, right-hand side included:
         // rows over the warps, columns over the lanes, one barrier per pivot
@@ -2013,8 +2027,10 @@ __device__ void cond_component_terms(const KBeam& KB, const StepCoeffs& P, const
             }
             __syncthreads();
         }
+        sub(kPhaseLUPanel);
         for (int k = tid; k < mc * ldw; k += NT) work[k] = W[k];
         __syncthreads();
+        sub(kPhaseIntEpilogue);
     }
 }
 
@@ -2318,7 +2334,8 @@ __device__ __forceinline__ void dense_model_step(const KBeam& KB, const StepCoef
         mark(kPhaseLoadPredict);
         if (cnd) {  // components first: their systems share the bordered system's region
             __syncthreads();
-            cond_component_terms<NT>(KB, P, S, smem_raw, sq, sv, svd, sT, fmap, slab, L, resid, &s_flag);
+            cond_component_terms<NT>(KB, P, S, smem_raw, sq, sv, svd, sT, fmap, slab, L, resid, &s_flag,
+                                     timing ? s_ph : nullptr);
         }
         mark(kPhaseIntegrate);
         for (int k = tid; k < md * md; k += NT) Md[k] = 0.;

@@ -318,10 +318,11 @@ int main(int argc, char** argv) {
             check(c, kyn_step(c, ids.data(), static_cast<int>(ids.size()), &bp, st.data(), it.data()));
             long iters = 0;
             for (int v : it) iters += v;
-            const char* names[] = {"predict+tangent", "", "elements", "bordered assembly", "", "bordered LU",
-                                   "back substitution", "update"};
+            const char* names[] = {"predict+tangent", "(elements: quadrature)", "elements", "bordered assembly", "",
+                                   "bordered LU", "back substitution", "update", "", "(elements: assembly)",
+                                   "(elements: elimination)", "(elements: save)"};
             std::printf("phase cycles per turbine-iteration (%ld iterations):", iters);
-            for (int ph : {0, 2, 3, 5, 6, 7}) {
+            for (int ph : {0, 2, 1, 9, 10, 11, 3, 5, 6, 7}) {
                 int64_t v = 0;
                 check(c, kyn_ctx_stat(c, KYN_STAT_PHASE_CYCLES + ph, &v));
                 std::printf(" %s %.0f,", names[ph], static_cast<double>(v) / static_cast<double>(iters));
