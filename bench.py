@@ -382,15 +382,24 @@ def main() -> None:
             ctx.set_loads_batch(ids, LOAD_NODE_FX, loads_host[k].data_ptr(), False)
         return ctx.step(ids, params)
 
+    tuned_solvers: dict = {}
+
     def tune(step_ids, step_params) -> dict:
-        """Autotune threads per CTA per size class (timed on clones, before the
-        timed region); returns the choice per node count."""
+        """Autotune threads per CTA (and in the FP64 form the free-block solver)
+        per size class, timed on clones before the timed region; returns the
+        threads per node count and keeps the solvers in tuned_solvers."""
         if args.no_autotune:
             return {}
+        # the clones carry their sources' loads: tune on loaded steps (the
+        # first step's tip loads), whose Newton iterations are the timed ones'
+        ctx.set_loads_batch(step_ids, LOAD_NODE_FX, loads_dev[0].data_ptr(), True)
         ctx.autotune(step_ids, step_params)
-        out = {}
+        out, sv = {}, {}
         for i, d in enumerate(draws):
             out.setdefault(int(d.num_nodes), ctx.tuned_threads(int(step_ids[i]), step_params.precision))
+            sv.setdefault(int(d.num_nodes), "gauss-jordan" if ctx.tuned_solver(
+                int(step_ids[i]), step_params.precision) == 0 else "panel LU")
+        tuned_solvers[step_params.precision] = dict(sorted(sv.items()))
         return dict(sorted(out.items()))
 
     def device_leg(step_ids, step_params, clocks_on: bool):
@@ -641,6 +650,7 @@ def main() -> None:
                                          "trailing updates)"),
                        "launch": "direct" if args.no_graph else "CUDA graph replay per step",
                        "threads_per_cta_by_nodes": tuned64,
+                       "solver_by_nodes": tuned_solvers.get(0, {}),
                        "parallelism": f"independent beam shards x{world}"},
             "latency_ms": {"p50": float(np.percentile(dev_ms, 50)),
                            "p99": float(np.percentile(dev_ms, 99)),

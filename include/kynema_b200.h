@@ -313,14 +313,23 @@ KYN_API int kyn_set_loads_batch_static(kyn_ctx* ctx, const int* model_ids, int n
 
 /* Autotuner (no counterpart in the reference): for every size class of the
  * listed models (beams per model, nodes, quadrature points, constraints,
- * precision), times the step kernel with 128, 256 and 512 threads per CTA on
- * temporary copies of up to 8 x SMs models of that class (two steps after one
- * warm-up step) and keeps the fastest for later kyn_step calls on this
- * context.  The listed models' states are not changed. */
+ * precision), times the step kernel with 128, 256 and 512 threads per CTA --
+ * in the FP64 form, for beam systems, each with the panel LU and with the
+ * register Gauss-Jordan solve of the free block (the same FP64 accuracy
+ * class; Gauss-Jordan is the faster for small beams) -- on temporary copies
+ * of all the class's models (repeated up to 4 x SMs copies, at most 16384;
+ * four steps after one warm-up step)
+ * and keeps the fastest for later kyn_step calls on this context.  The
+ * listed models' states are not changed. */
 KYN_API int kyn_autotune(kyn_ctx* ctx, const int* model_ids, int n, const kyn_step_params* params);
 
 /* Threads per CTA kyn_step uses for a model at a precision (tuned or default). */
 KYN_API int kyn_tuned_threads(kyn_ctx* ctx, int model_id, int precision);
+
+/* Free-block solver (KYN_SOLVER_*) kyn_step uses for a model at a precision:
+ * the tuned one, else the context's KYN_OPT_LINEAR_SOLVER.  No counterpart in
+ * the reference. */
+KYN_API int kyn_tuned_solver(kyn_ctx* ctx, int model_id, int precision);
 
 /* Batched Constraints::UpdateDisplacement for many models: values holds
  * [sum of the listed models' constraints][7] (model order, then constraint

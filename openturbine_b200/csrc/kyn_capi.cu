@@ -43,6 +43,7 @@ struct DevModel {
     std::vector<int> node_base;      // per beam: first global node when its nodes are contiguous, else -1
     int def_nt[2] = {0, 0};          // default threads per CTA, FP64 / FP32 form
     int tuned_nt[2] = {0, 0};        // tuned threads per CTA (0: none), cached per form
+    int tuned_sv[2] = {-1, -1};      // tuned free-block solver (-1: the context's), cached per form
     unsigned long long tuned_gen[2] = {~0ull, ~0ull};  // tuned-table generation of that cache
     int lump = 0;                    // kernel kind: 0 beams, 1 with masses / springs /
                                      // drive train (LUMP instance), 2 dense model
@@ -67,6 +68,7 @@ struct Entry {
     double work;
     DevModel* m;
     int lump;
+    int solver;  // KYN_SOLVER_* of the free-block solve (tuned per size class, or the context's)
 };
 
 struct ClassKey {
@@ -84,6 +86,7 @@ struct Bucket {
     int cluster = 1;
     int nt = 256;      // threads per CTA (step_kernel instance)
     int lump = 0;      // kernel kind (DevModel::lump)
+    int solver = KYN_SOLVER_PANEL_LU;  // free-block solve of this bucket's launch
     int smem = 0;
     int first = 0;     // first beam in the plan's beam array
     int count = 0;     // beams
@@ -213,6 +216,7 @@ struct kyn_ctx {
     unsigned long long* d_prof = nullptr; // phase timing counters (KYN_OPT_PHASE_TIMING)
     unsigned long long* d_diag = nullptr; // solve counters (kDiag*, KYN_STAT_SOLVE_*)
     std::map<ClassKey, int> tuned;        // threads per CTA chosen by kyn_autotune
+    std::map<ClassKey, int> tuned_solver; // free-block solver chosen by kyn_autotune (FP64 form)
     // Plan buffers, grown on demand and reused by every plan (one step in
     // flight at a time), so rebuilding a plan for a changed model set (the
     // serving loop does it every iteration) allocates nothing in steady state.
@@ -503,25 +507,30 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
         int nt = m->def_nt[f];
         if (!c->tuned.empty()) {
             if (m->tuned_gen[f] != c->tuned_gen) {  // per-model cache of the tuned table
-                const auto tuned = c->tuned.find(class_key(m->host, precision));
+                const ClassKey ck = class_key(m->host, precision);
+                const auto tuned = c->tuned.find(ck);
                 m->tuned_nt[f] = (tuned != c->tuned.end()) ? tuned->second : 0;
+                const auto tsv = c->tuned_solver.find(ck);
+                m->tuned_sv[f] = (tsv != c->tuned_solver.end()) ? tsv->second : -1;
                 m->tuned_gen[f] = c->tuned_gen;
             }
             if (m->tuned_nt[f] > 0) nt = m->tuned_nt[f];
         }
+        const int solver = (!c->tuned.empty() && m->tuned_sv[f] >= 0) ? m->tuned_sv[f] : c->solver;
         const int smem = m->smem_nt[f][nt_index(nt)];
         const int cluster = static_cast<int>(m->kt.size());
         const int cls = ctas_per_sm(rbytes, nt, smem);
-        all.push_back({i, cluster, nt, cls, smem, m->work, m, m->lump});
+        all.push_back({i, cluster, nt, cls, smem, m->work, m, m->lump, solver});
         // one 64-bit sort key: kernel kind (beams, masses/springs, dense models),
         // larger clusters first, more threads first, fewer CTAs per SM first,
         // more work first, then model order
-        const uint64_t work = static_cast<uint64_t>(std::min(m->work, 2097151.));
+        const uint64_t work = static_cast<uint64_t>(std::min(m->work, 1048575.));
         keys.push_back((static_cast<uint64_t>(m->lump) << 62) |
                        (static_cast<uint64_t>(15 - std::min(cluster, 15)) << 58) |
                        (static_cast<uint64_t>(2 - nt_index(nt)) << 56) |
                        (static_cast<uint64_t>(std::min(cls, 15)) << 52) |
-                       ((2097151ull - work) << 31) | static_cast<uint64_t>(i));
+                       (static_cast<uint64_t>(solver == KYN_SOLVER_GAUSS_JORDAN ? 1 : 0) << 51) |
+                       ((1048575ull - work) << 31) | static_cast<uint64_t>(i));
         nbeams += m->kt.size();
     }
     std::sort(keys.begin(), keys.end());
@@ -545,11 +554,13 @@ int get_plan(kyn_ctx* c, const int* ids, int n, int precision, Plan** out) {
         const Entry& en = entries[e];
         if (plan->buckets.empty() || plan->buckets.back().cluster != en.cluster ||
             plan->buckets.back().nt != en.nt || plan->buckets.back().lump != en.lump ||
+            plan->buckets.back().solver != en.solver ||
             ctas_per_sm(rbytes, en.nt, plan->buckets.back().smem) != en.cls) {
             Bucket bk;
             bk.cluster = en.cluster;
             bk.nt = en.nt;
             bk.lump = en.lump;
+            bk.solver = en.solver;
             bk.first = static_cast<int>(nk);
             plan->buckets.push_back(bk);
         }
@@ -673,8 +684,10 @@ int launch_plan(kyn_ctx* c, Plan* plan, const kyn_step_params* p) {
         const KBeam* beams = plan->d_kbeams + bk.first;
         const int rec = plan->record ? 1 : 0;
         const bool fp32 = plan->precision == KYN_PRECISION_FP32_REFINED;
-        KYN_CUDA(c, cudaLaunchKernelEx(&cfg, pick_kernel(fp32, bk.nt, bk.lump, P.solver == KYN_SOLVER_GAUSS_JORDAN),
-                                       beams, P, rec,
+        StepCoeffs Pb = P;
+        Pb.solver = bk.solver;
+        KYN_CUDA(c, cudaLaunchKernelEx(&cfg, pick_kernel(fp32, bk.nt, bk.lump, bk.solver == KYN_SOLVER_GAUSS_JORDAN),
+                                       beams, Pb, rec,
                                        plan->d_status, plan->d_iters));
         c->launches++;
     }
@@ -973,6 +986,7 @@ int kyn_ctx_set_option(kyn_ctx* c, int option, int64_t value) {
     if (option == KYN_OPT_LINEAR_SOLVER) {
         if (value != KYN_SOLVER_GAUSS_JORDAN && value != KYN_SOLVER_PANEL_LU)
             return set_err(c, KYN_ERR_INVALID, "unknown linear solver");
+        if (c->solver != static_cast<int>(value)) c->plan.reset();  // buckets carry their solver
         c->solver = static_cast<int>(value);
         return KYN_OK;
     }
@@ -1817,7 +1831,7 @@ extern "C" int kyn_autotune(kyn_ctx* c, const int* ids, int n, const kyn_step_pa
     const int rb = (p->precision == KYN_PRECISION_FP32_REFINED) ? 4 : 8;
     int sms = 148;
     KYN_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-    const size_t sample_max = static_cast<size_t>(8) * sms;
+    const size_t sample_max = 16384;  // copies timed per class at most
     std::map<ClassKey, std::vector<int>> classes;
     for (int i = 0; i < n; ++i) {
         DevModel* m = find_model(c, ids[i]);
@@ -1830,9 +1844,13 @@ extern "C" int kyn_autotune(kyn_ctx* c, const int* ids, int n, const kyn_step_pa
     int rc = KYN_OK;
     for (auto& kv : classes) {
         const ClassKey& key = kv.first;
+        // copies of all the class's models (the batch being tuned), repeated up
+        // to 4 x SMs so that a small class is timed on full waves of CTAs
         std::vector<int> clones;
-        for (size_t j = 0; j < std::min(kv.second.size(), sample_max); ++j) {
-            const int cid = clone_model(c, kv.second[j]);
+        const size_t nsrc = kv.second.size();
+        const size_t want = std::min(std::max(nsrc, static_cast<size_t>(4) * sms), sample_max);
+        for (size_t j = 0; j < want; ++j) {
+            const int cid = clone_model(c, kv.second[j % nsrc]);
             if (cid < 0) break;
             clones.push_back(cid);
         }
@@ -1844,12 +1862,17 @@ extern "C" int kyn_autotune(kyn_ctx* c, const int* ids, int n, const kyn_step_pa
         // timed steps), so that Newton iteration counts match across candidates.
         auto reset = [&]() {
             for (size_t j = 0; j < clones.size(); ++j) {
-                const int r2 = kyn_state_copy(c, clones[j], kv.second[j]);
+                const int r2 = kyn_state_copy(c, clones[j], kv.second[j % nsrc]);
                 if (r2 != KYN_OK) return r2;
             }
             return static_cast<int>(KYN_OK);
         };
-        int best_nt = -1;
+        // candidates: threads per CTA, and in the FP64 form for plain beam
+        // systems also the free-block solver (panel LU or register
+        // Gauss-Jordan: the same FP64 accuracy class, different speeds by size)
+        const bool try_solver = p->precision == KYN_PRECISION_FP64 && find_model(c, clones[0])->lump == 0;
+        const int other = c->solver == KYN_SOLVER_PANEL_LU ? KYN_SOLVER_GAUSS_JORDAN : KYN_SOLVER_PANEL_LU;
+        int best_nt = -1, best_sv = c->solver;
         float best_ms = 0.f, def_ms = -1.f;
         for (int nt : {128, 256, 512}) {
             bool fits = true;
@@ -1857,33 +1880,47 @@ extern "C" int kyn_autotune(kyn_ctx* c, const int* ids, int n, const kyn_step_pa
                 fits &= (b.dense ? dense_smem(h, b, nt)
                                  : beam_smem(b.N, b.Q, b.nc, rb, nt, hub_kind(h))) <= kMaxDynSmem;
             if (!fits || (key.beams > 1 && key.beams * nt > 1024 * 8)) continue;
-            c->tuned[key] = nt;
-            ++c->tuned_gen;
-            c->plan.reset();
-            Plan* plan = nullptr;
-            rc = get_plan(c, clones.data(), static_cast<int>(clones.size()), p->precision, &plan);
-            if (rc == KYN_OK) rc = reset();
-            if (rc == KYN_OK) rc = launch_plan(c, plan, p);  // warm-up step
-            if (rc == KYN_OK) rc = finish_plan(c, plan, nullptr, nullptr);
-            if (rc == KYN_OK) rc = reset();
-            if (rc != KYN_OK) break;
-            KYN_CUDA(c, cudaEventRecord(e0, c->stream));
-            for (int r = 0; r < 2 && rc == KYN_OK; ++r) rc = launch_plan(c, plan, p);
-            KYN_CUDA(c, cudaEventRecord(e1, c->stream));
-            if (rc == KYN_OK) rc = finish_plan(c, plan, nullptr, nullptr);
-            if (rc != KYN_OK) break;
-            float ms = 0.f;
-            KYN_CUDA(c, cudaEventElapsedTime(&ms, e0, e1));
-            if (nt == def_nt) def_ms = ms;
-            if (best_nt < 0 || ms < best_ms) {
-                best_nt = nt;
-                best_ms = ms;
+            for (int sv : {c->solver, other}) {
+                if (sv != c->solver && !try_solver) continue;
+                c->tuned[key] = nt;
+                c->tuned_solver[key] = sv;
+                ++c->tuned_gen;
+                c->plan.reset();
+                Plan* plan = nullptr;
+                rc = get_plan(c, clones.data(), static_cast<int>(clones.size()), p->precision, &plan);
+                if (rc == KYN_OK) rc = reset();
+                if (rc == KYN_OK) rc = launch_plan(c, plan, p);  // warm-up step
+                if (rc == KYN_OK) rc = finish_plan(c, plan, nullptr, nullptr);
+                if (rc == KYN_OK) rc = reset();
+                if (rc != KYN_OK) break;
+                KYN_CUDA(c, cudaEventRecord(e0, c->stream));
+                for (int r = 0; r < 4 && rc == KYN_OK; ++r) rc = launch_plan(c, plan, p);
+                KYN_CUDA(c, cudaEventRecord(e1, c->stream));
+                if (rc == KYN_OK) rc = finish_plan(c, plan, nullptr, nullptr);
+                if (rc != KYN_OK) break;
+                float ms = 0.f;
+                KYN_CUDA(c, cudaEventElapsedTime(&ms, e0, e1));
+                if (nt == def_nt && sv == c->solver) def_ms = ms;
+                if (best_nt < 0 || ms < best_ms) {
+                    best_nt = nt;
+                    best_sv = sv;
+                    best_ms = ms;
+                }
             }
+            if (rc != KYN_OK) break;
         }
         // keep the default unless another choice is clearly faster (timing noise)
-        if (def_ms > 0.f && best_nt != def_nt && best_ms > 0.97f * def_ms) best_nt = def_nt;
-        if (best_nt > 0) c->tuned[key] = best_nt;
-        else c->tuned.erase(key);
+        if (def_ms > 0.f && (best_nt != def_nt || best_sv != c->solver) && best_ms > 0.97f * def_ms) {
+            best_nt = def_nt;
+            best_sv = c->solver;
+        }
+        if (best_nt > 0) {
+            c->tuned[key] = best_nt;
+            c->tuned_solver[key] = best_sv;
+        } else {
+            c->tuned.erase(key);
+            c->tuned_solver.erase(key);
+        }
         ++c->tuned_gen;
         c->plan.reset();
         for (int cid : clones) kyn_model_destroy(c, cid);
@@ -1905,6 +1942,14 @@ extern "C" int kyn_tuned_threads(kyn_ctx* c, int model_id, int precision) {
     int nt = 128;
     for (const HostBeam& b : m->host.beams) nt = std::max(nt, beam_threads(b.N, b.Q, b.nc, rb, hub_kind(m->host)));
     return nt;
+}
+
+extern "C" int kyn_tuned_solver(kyn_ctx* c, int model_id, int precision) {
+    if (!c) return KYN_ERR_INVALID;
+    DevModel* m = find_model(c, model_id);
+    if (!m) return set_err(c, KYN_ERR_NOT_FOUND, "unknown model id");
+    const auto it = c->tuned_solver.find(class_key(m->host, precision));
+    return it != c->tuned_solver.end() ? it->second : c->solver;
 }
 
 // ---- batched load scatter through a static staging array (no allocation) ----

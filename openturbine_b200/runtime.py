@@ -85,6 +85,7 @@ def load_library():
     L.kyn_state_copy.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     L.kyn_autotune.argtypes = [ctypes.c_void_p, _ip, ctypes.c_int, ctypes.c_void_p]
     L.kyn_tuned_threads.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    L.kyn_tuned_solver.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     L.kyn_set_loads_batch_static.argtypes = [ctypes.c_void_p, _ip, ctypes.c_int, ctypes.c_int,
                                              ctypes.c_void_p, ctypes.c_int]
     L.kyn_ctx_stat.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
@@ -304,6 +305,10 @@ class Context:
 
     def tuned_threads(self, mid: int, precision: int = 0) -> int:
         return self._check(self.lib.kyn_tuned_threads(self.h, mid, precision))
+
+    def tuned_solver(self, mid: int, precision: int = 0) -> int:
+        """KYN_SOLVER_* the step uses for the model (tuned, else the context's)."""
+        return self._check(self.lib.kyn_tuned_solver(self.h, mid, precision))
 
     def set_loads_batch_static(self, ids: np.ndarray, which: int, ptr: int,
                                on_device: bool) -> None:
