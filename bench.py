@@ -10,7 +10,8 @@ Metric: converged beam-steps/s (non-converged beam-steps are excluded), with
 p50/p99 step latency.  `value` is measured with the loads already resident in
 HBM (device-timed with CUDA events on the library's stream); `e2e` goes
 through the public C ABI with host buffers: per step one pinned H2D of every
-beam's loads, the step, and one D2H of every node's displacement.
+beam's loads, the step, and one D2H of every node's displacement, over the
+same steps as `value` (a twin batch taken through the same warm-up steps).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -364,7 +365,7 @@ def main() -> None:
     qps = nodes + 2
     elem_nodes = int(nodes.sum())
     tip_index = np.cumsum(nodes) - 1          # element-node row of each tip
-    total_steps = args.warmup + 2 * args.steps
+    total_steps = args.warmup + args.steps
     # loads for every step (resident on the device for `value`, pinned host for e2e)
     loads_host = torch.zeros((total_steps, elem_nodes, 6), dtype=torch.float64).pin_memory()
     for k in range(total_steps):
@@ -374,13 +375,6 @@ def main() -> None:
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     ext = torch.cuda.ExternalStream(ctx.stream_handle, device=dev)
     fp64_peak = measured_fp64_peak(torch, dev)
-
-    def do_step(k: int, device_loads: bool):
-        if device_loads:
-            ctx.set_loads_batch(ids, LOAD_NODE_FX, loads_dev[k].data_ptr(), True)
-        else:
-            ctx.set_loads_batch(ids, LOAD_NODE_FX, loads_host[k].data_ptr(), False)
-        return ctx.step(ids, params)
 
     tuned_solvers: dict = {}
 
@@ -588,18 +582,33 @@ def main() -> None:
                 ctx.destroy_model(int(i))
 
     # ---- e2e: host buffers through the C ABI, wall time per step --------------
+    # A twin of the batch, built from the same draws and taken through the same
+    # W warm-up steps, is timed over the steps `value` timed (W .. W+K-1, the
+    # reference arm's steps too), so both numbers cover the same work: the
+    # twin's states, statuses and iteration counts are the batch's own.
+    e_ids = np.array([ctx.create_model(W.batch_cantilever_model(d).pack()) for d in draws],
+                     dtype=np.int32)
+    for k in range(args.warmup):
+        ctx.set_loads_batch(e_ids, LOAD_NODE_FX, loads_dev[k].data_ptr(), True)
+        ctx.step(e_ids, params)
     e2e_ms, conv_e = [], 0
+    if dist:
+        dist.barrier()
     for j in range(args.steps):
-        k = args.warmup + args.steps + j
+        k = args.warmup + j
         with torch.cuda.stream(ext):
             flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        st, it = do_step(k, False)
-        ctx.get_state_batch(ids, "q", q_host.data_ptr(), False)
+        ctx.set_loads_batch(e_ids, LOAD_NODE_FX, loads_host[k].data_ptr(), False)
+        st, it = ctx.step(e_ids, params)
+        ctx.get_state_batch(e_ids, "q", q_host.data_ptr(), False)
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
         conv_e += int((st == 0).sum())
-    t_e2e_ms, conv_e, e2e = job_rate(sum(e2e_ms), conv_e, dist, dev)
+    e2e_same_q = bool(np.array_equal(q_host.numpy(), r64["q"], equal_nan=True))
+    for i in e_ids:
+        ctx.destroy_model(int(i))
+    t_e2e_ms, conv_e_all, e2e = job_rate(sum(e2e_ms), conv_e, dist, dev)
 
     # ---- serving: Poisson request stream, continuous batching, both forms --------
     serving = None
@@ -659,7 +668,10 @@ def main() -> None:
             "converged_fraction": conv_v / (args.steps * len(ids)),
             "e2e": {"value": e2e, "unit": "beam-steps/s",
                     "h2d_bytes_per_step": int(elem_nodes * 6 * 8),
-                    "d2h_bytes_per_step": int(elem_nodes * 7 * 8 + 2 * 4 * len(ids))},
+                    "d2h_bytes_per_step": int(elem_nodes * 7 * 8 + 2 * 4 * len(ids)),
+                    "steps": f"{args.warmup}..{args.warmup + args.steps - 1} (value's steps) on a twin batch",
+                    "converged_fraction": conv_e / (args.steps * len(ids)),
+                    "final_q_equals_value_leg": e2e_same_q},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": fp64_peak,
                          "unit": "TFLOP/s", "frac": achieved / fp64_peak,
                          "traffic": DRAM_BYTES_PER_BEAM_STEP * len(ids),
